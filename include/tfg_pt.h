@@ -1,0 +1,313 @@
+/*
+ * tfg_pt.h -- C ABI of the B200 path-tracing hot path (CWBVH traversal,
+ * wavefront shading / next-event estimation / Russian roulette, neural
+ * radiance cache kernels).
+ *
+ * Every struct below is byte-for-byte layout compatible with the structure
+ * of the same (Spanish) name in the reference project, so a caller can pass
+ * its existing device buffers by reinterpret_cast.  Sizes are checked with
+ * static asserts in the implementation (tfg_b200/csrc/pt_common.cuh).
+ *
+ * Every entry point returns 0 on success or a non-zero code (a cudaError_t
+ * value, or one of the TFG_E_* codes below).  tfgGetLastErrorString() gives
+ * a readable message for the last failure on the calling thread.  The
+ * reference's launch wrappers returned void and left error polling to the
+ * caller (reference main.cpp:576-594); here each call checks its own launch.
+ *
+ * All device pointers are caller-owned unless a function says otherwise.
+ * `stream` is a cudaStream_t passed as void* (0 = legacy default stream,
+ * which is where the reference launched its render kernels,
+ * RenderKernel.cu:270).
+ */
+#ifndef TFG_PT_H
+#define TFG_PT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ */
+/* Scene value types (reference L0/L1 structs)                         */
+/* ------------------------------------------------------------------ */
+
+/* vector3d.h:14-16 -- three doubles, 24 B. */
+typedef struct TfgVec3d { double x, y, z; } TfgVec3d;
+
+/* color.h:13-15 -- three floats, 12 B. */
+typedef struct TfgColor { float r, g, b; } TfgColor;
+
+/* primitiva.h:17 enum TipoPrimitiva. */
+enum { TFG_ESFERA = 0, TFG_PLANO = 1, TFG_TRIANGULO = 2 };
+
+/* primitiva.h:19-41 -- tagged union, 200 B, union at offset 56. */
+typedef struct TfgPrimitiva {
+    int32_t  tipo;
+    TfgColor emision;
+    TfgColor difuso;
+    TfgColor especular;
+    TfgColor transmision;
+    float    indice_refraccion;
+    union {
+        struct { TfgVec3d centro; float radio; } esfera;
+        struct { TfgVec3d normal; float distancia; } plano;
+        struct { TfgVec3d v0, v1, v2, v0_normal, v1_normal, v2_normal; } triangulo;
+    } u;
+} TfgPrimitiva;
+
+/* luzPuntual.h:14-17 -- 40 B. */
+typedef struct TfgLuzPuntual { TfgVec3d posicion; TfgColor intensidad; } TfgLuzPuntual;
+
+/* camara.h:15-21 -- 112 B.  `izquierda` = frente x arriba (camera right). */
+typedef struct TfgCamara {
+    TfgVec3d posicion, frente, arriba, izquierda;
+    float ancho_plano, alto_plano, distancia_focal;
+} TfgCamara;
+
+/* imagen_gpu.h:14-16 -- passed by value in the reference; 16 B. */
+typedef struct TfgImagenGPU { int32_t anchura, altura; TfgColor* datos; } TfgImagenGPU;
+
+/* mlp_types.h:14-23 -- 112 B. */
+typedef struct TfgDatosMLP {
+    TfgVec3d posicion, direccion, normal;
+    TfgColor difuso, especular, color;
+} TfgDatosMLP;
+
+/* mlp_types.h:26-29 -- 48 B. */
+typedef struct TfgSceneBounds { TfgVec3d min, max; } TfgSceneBounds;
+
+/* mlp_types.h:32-38 -- 96 B. */
+typedef struct TfgDatosGeometricos {
+    TfgVec3d posicion, direccion, normal;
+    TfgColor difuso, especular;
+} TfgDatosGeometricos;
+
+/* mlp_types.h:41-54 -- 232 B (bool at 228, padded). */
+typedef struct TfgRegistroEntrenamiento {
+    TfgDatosGeometricos head, tail;
+    TfgColor luz_acumulada_sufijo, throughput_sufijo, factor_normalizacion;
+    uint8_t  valido;
+} TfgRegistroEntrenamiento;
+
+/* tinybvh_wrapper.h:15-21 -- device descriptor of a CWBVH, passed by value
+ * in the reference.  d_nodos: 5 float4 (80 B) per node; d_tris: 4 float4
+ * (64 B) per triangle in the reference's transform layout. */
+typedef struct TfgTinyBVHD_GPU {
+    float*   d_nodos;
+    float*   d_tris;
+    uint32_t num_nodos;
+    uint32_t num_tris;
+} TfgTinyBVHD_GPU;
+
+/* ------------------------------------------------------------------ */
+/* Error handling                                                      */
+/* ------------------------------------------------------------------ */
+
+enum {
+    TFG_OK = 0,
+    TFG_E_INVALID = 10001,     /* bad argument (null pointer, size out of range) */
+    TFG_E_UNSUPPORTED = 10002, /* device is not sm_100 or feature not built */
+    TFG_E_TIMEOUT = 10003,     /* a bounded device-side wait ran out */
+    TFG_E_BUILD = 10004        /* BVH build failed (e.g. out of memory) */
+};
+
+/* Message for the last non-zero return on this thread ("" if none). */
+const char* tfgGetLastErrorString(void);
+
+/* ------------------------------------------------------------------ */
+/* CWBVH build hand-off (replaces TinyBVH::construirBVH,               */
+/* tinybvh_wrapper.cpp:30-83)                                          */
+/* ------------------------------------------------------------------ */
+
+/* Host result of a CWBVH build.  Node and reference-triangle arrays use the
+ * layout the reference traversal decodes (traverse_cwbvh.cuh:77-209):
+ *   node  = 20 floats (80 B): p.xyz, {e.x,e.y,e.z,imask} bytes,
+ *           child base (node units), triangle base (float4 units),
+ *           meta[0..7], q_lo_x[8], q_lo_y[8], q_lo_z[8], q_hi_x[8], q_hi_y[8], q_hi_z[8]
+ *   tris_ref = 16 floats (64 B) per triangle: rows u, v, plane of the
+ *           world-to-triangle transform, then (0,0,0,prim id bits)
+ *   tris_wt  = 12 floats (48 B) per triangle: v0.xyz, prim id bits,
+ *           v1.xyz, 0, v2.xyz, 0  (watertight-test layout)
+ * Triangle k of the BVH order lives at tris_*[k]; node field "triangle base"
+ * is 4*k so both layouts are addressed from the same nodes. */
+typedef struct TfgCWBVHHost {
+    float*    nodes;
+    float*    tris_ref;
+    float*    tris_wt;
+    uint32_t  num_nodes;
+    uint32_t  num_tris;
+    uint32_t  max_depth;  /* deepest node level (root = 1) */
+    uint32_t  reserved;
+} TfgCWBVHHost;
+
+/* Build over `num_tris` triangles given as 9 floats each (v0,v1,v2).  The
+ * prim id stored in each triangle is its index in `verts`.  Arrays in `out`
+ * are malloc'ed by the library; release with tfgCWBVHFree.  Host only. */
+int  tfgCWBVHBuild(const float* verts, uint32_t num_tris, TfgCWBVHHost* out);
+void tfgCWBVHFree(TfgCWBVHHost* bvh);
+
+/* Device-resident CWBVH plus the watertight triangle array.  `ref` is the
+ * exact TinyBVHD_GPU a reference caller passes to launchKernelRenderTiny. */
+typedef struct TfgTinyBVH {
+    TfgTinyBVHD_GPU ref;
+    float*          d_tris_wt;
+    TfgPrimitiva*   d_primitivas;   /* triangles in input order, as the reference uploads them */
+    uint32_t        num_primitivas;
+    uint32_t        max_depth;
+} TfgTinyBVH;
+
+/* TinyBVH::construirBVH: filter TRIANGULO primitives (input order kept),
+ * build, upload nodes / both triangle layouts / primitives with cudaMalloc. */
+int  tfgTinyBVHConstruir(const TfgPrimitiva* primitivas_host, int32_t n, TfgTinyBVH* out);
+/* Frees what tfgTinyBVHConstruir allocated (TinyBVH::~TinyBVH). */
+void tfgTinyBVHLiberar(TfgTinyBVH* bvh);
+
+/* ------------------------------------------------------------------ */
+/* Render entry points (RenderKernel.h:47-77)                          */
+/* ------------------------------------------------------------------ */
+
+/* Triangle test used against the CWBVH. */
+enum {
+    TFG_TRIS_REF = 0,        /* reference 64-B transform test (traverse_cwbvh.cuh:189-209) */
+    TFG_TRIS_WATERTIGHT = 1  /* 48-B vertices, watertight FP32 test (Woop, Benthin, Wald 2013) */
+};
+
+/* Path-tracer settings that the reference hard-codes. */
+typedef struct TfgRenderParams {
+    int32_t max_depth;     /* bounces; reference 20 (render.h:63) */
+    int32_t rr_min_depth;  /* Russian roulette when depth >= this; reference 11 (render.h:209: depth > 10) */
+    int32_t shadow_mesh;   /* 1: shadow rays also test the CWBVH mesh; reference kernel 0 (escenario.h:65,168) */
+    int32_t tri_format;    /* TFG_TRIS_REF or TFG_TRIS_WATERTIGHT */
+    int32_t spp;           /* samples per pixel in this call: frame_number .. frame_number+spp-1 */
+    int32_t accumulate;    /* 1: add each sample into `accum` (FP32 RGB per pixel) */
+    int32_t profile;       /* TFG_PROFILE_* bits: stage timing / traversal work counters */
+    int32_t reserved;
+} TfgRenderParams;
+
+enum {
+    TFG_PROFILE_TIMES = 1,   /* CUDA events around every stage launch */
+    TFG_PROFILE_COUNTS = 2   /* count rays, nodes visited and triangle tests (slower) */
+};
+
+/* Stage times and traversal work accumulated by passes run with `profile`
+ * set, since the last tfgRenderProfileReset on this device. */
+typedef struct TfgRenderProfile {
+    double   ms[5];          /* generate, trace, shade, shadow, resolve (sum of launch durations) */
+    uint64_t launches[5];
+    uint64_t rays;           /* closest-hit rays traced */
+    uint64_t nodes;          /* CWBVH nodes decoded by those rays */
+    uint64_t tri_tests;      /* triangle tests by those rays */
+    uint64_t shadow_rays;    /* shadow rays cast (one per light with cos > 0) */
+    uint64_t shadow_nodes;
+    uint64_t shadow_tri_tests;
+} TfgRenderProfile;
+
+int tfgRenderProfileReset(void);
+/* Synchronises the device, then fills `out`. */
+int tfgRenderProfileGet(TfgRenderProfile* out);
+
+/* Reference settings: depth 20, RR from depth 11, mesh-free shadow rays,
+ * reference triangle layout, 1 spp, no accumulation. */
+void tfgRenderParamsReference(TfgRenderParams* p);
+
+/* launchKernelRenderTiny (RenderKernel.h:55-61).  Same arguments and
+ * meaning; the grid/block arguments of the reference are dropped because the
+ * wavefront stages choose their own launch shapes.  `camara`, all arrays and
+ * the counters are device pointers.  Uses the reference settings above and
+ * the reference triangle layout in `nodos_bvh`, so a BVH built by either
+ * builder works.  Unlike the reference, pixels outside W x H are never
+ * written (RenderKernel.cu:35-46 had no bounds guard). */
+int tfgLaunchKernelRenderTiny(
+    const TfgCamara* camara, const TfgPrimitiva* primitivas, int32_t num_primitivas,
+    const TfgLuzPuntual* luces, int32_t num_luces,
+    const TfgPrimitiva* primitivas_malla, int32_t num_primitivas_malla,
+    int32_t ancho_img, int32_t alto_img, int32_t samples_per_pixel, int32_t frame_number,
+    const TfgTinyBVHD_GPU* nodos_bvh, const TfgPrimitiva* primitivas_bvh, int32_t num_nodos_bvh,
+    const TfgImagenGPU* imagen_directa,
+    uint32_t* dev_counter, TfgRegistroEntrenamiento* buffer_registros, uint32_t* counter_train,
+    int32_t max_cap_train, TfgDatosMLP* buffer_inference, TfgColor* buffer_throughput,
+    int32_t usar_red_inferencia, int32_t entrenar_red, void* stream);
+
+/* Extended render: explicit settings, optional watertight triangles
+ * (`tris_wt`, required when params->tri_format == TFG_TRIS_WATERTIGHT) and
+ * optional accumulation buffer `accum` (W*H*3 floats).  Training / inference
+ * capture arguments behave as in tfgLaunchKernelRenderTiny and may be null
+ * when both NRC flags are 0.  `imagen_directa->datos` receives the last
+ * sample's radiance. */
+int tfgRenderPass(
+    const TfgRenderParams* params,
+    const TfgCamara* camara, const TfgPrimitiva* primitivas, int32_t num_primitivas,
+    const TfgLuzPuntual* luces, int32_t num_luces,
+    int32_t ancho_img, int32_t alto_img, int32_t frame_number,
+    const TfgTinyBVHD_GPU* nodos_bvh, const float* tris_wt,
+    const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh,
+    const TfgImagenGPU* imagen_directa, float* accum,
+    TfgRegistroEntrenamiento* buffer_registros, uint32_t* counter_train, int32_t max_cap_train,
+    TfgDatosMLP* buffer_inference, TfgColor* buffer_throughput,
+    int32_t usar_red_inferencia, int32_t entrenar_red, void* stream);
+
+/* Closest-hit traversal of `n` rays (primary-ray mode).  rays: 8 floats per
+ * ray (O.x, O.y, O.z, t_max, D.x, D.y, D.z, unused).  hits: 4 floats per ray
+ * (t, u, v, prim id bits); a miss returns t = t_max and id 0xFFFFFFFF.  This
+ * is traverse_cwbvh (traverse_cwbvh.cuh:51) over a batch, with 1/D computed
+ * per ray as the reference caller does (escenario.h:339-341). */
+int tfgTraceRays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int32_t tri_format,
+                 const float* rays, int32_t n, float* hits, void* stream);
+
+/* Camera rays for one sample of a W x H image, in the reference's order and
+ * arithmetic (rng.h:25-35 seed, two jitter draws, camara.h:42-59), written
+ * in the tfgTraceRays ray layout with t_max = 1e9 (escenario.h:318). */
+int tfgGenerateCameraRays(const TfgCamara* camara, int32_t ancho_img, int32_t alto_img,
+                          int32_t frame_number, float* rays, void* stream);
+
+/* launchInicializarCamara (RenderKernel.cu:68-90): default 45-degree camera
+ * at (0,-0.75,4.25) looking down -z, written to device pointer d_camara. */
+int tfgLaunchInicializarCamara(TfgCamara* d_camara, int32_t ancho_imagen, int32_t alto_imagen,
+                               void* stream);
+
+/* launchKernelComposite (RenderKernel.cu:49-66): img += thr * pred where thr != 0. */
+int tfgLaunchKernelComposite(TfgColor* img_pt, const TfgColor* img_prediccion,
+                             const TfgColor* throughput_map, int32_t ancho, int32_t alto,
+                             void* stream);
+
+/* launchKernelCalcularTargets (RenderKernel.cu:92-137). */
+int tfgLaunchKernelCalcularTargets(const TfgRegistroEntrenamiento* buffer_registros,
+                                   const TfgColor* buffer_prediccion_tail,
+                                   TfgDatosMLP* buffer_training_final, int32_t num_elementos,
+                                   void* stream);
+
+/* launchKernelPrepararInferenciaTail (RenderKernel.cu:139-166). */
+int tfgLaunchKernelPrepararInferenciaTail(const TfgRegistroEntrenamiento* source_registros,
+                                          TfgDatosMLP* dest_inference_inputs,
+                                          int32_t num_elements, void* stream);
+
+/* ------------------------------------------------------------------ */
+/* NRC data kernels (NrcKernel.h:24-41)                                */
+/* ------------------------------------------------------------------ */
+
+/* launchGenerarIndicesAleatorios (NrcKernel.cu:10-16): idx[i] = pcg32(seed ^ i) % max_range. */
+int tfgLaunchGenerarIndicesAleatorios(int32_t* indices, int32_t max_range, int32_t count,
+                                      uint32_t seed, void* stream);
+
+/* launchPrepararDatosEntrenamiento (NrcKernel.cu:18-68): gather + 15-float rows
+ * (position normalised to `bounds` and clamped to [0,1]) + 3-float targets clamped at 1e5. */
+int tfgLaunchPrepararDatosEntrenamiento(const TfgDatosMLP* buffer, const int32_t* indices_aleatorios,
+                                        int32_t batch_size, int32_t n_in, int32_t n_out,
+                                        const TfgSceneBounds* bounds, float* input_matrix,
+                                        float* target_matrix, void* stream);
+
+/* launchPrepararDatosInferencia (NrcKernel.cu:70-97). */
+int tfgLaunchPrepararDatosInferencia(const TfgDatosMLP* datos, uint32_t n_elements, uint32_t n_in,
+                                     float* buffer_in, const TfgSceneBounds* bounds, void* stream);
+
+/* launchGuardarSalidaInferencia (NrcKernel.cu:99-126): clamp to [0,1e5], NaN -> 0, Inf -> 1e5. */
+int tfgLaunchGuardarSalidaInferencia(const float* network_output, TfgColor* buffer_color,
+                                     int32_t n_elements, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TFG_PT_H */

@@ -1,0 +1,135 @@
+"""Primary-ray traversal parity on the GPU.
+
+The product traversal (tfgTraceRays) runs on the same CWBVH as the
+reference's own traverse_cwbvh (compiled from the reference sources into
+oracle/_ref) and as the CPU restatement.  With the reference triangle layout
+the closest-hit ids must agree bit for bit; with the watertight test they
+must agree except on genuine edge hits, with t within 1e-5 relative."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import oracle as orc
+from tfg_b200 import bvh as hbvh
+from tfg_b200 import pathtracer as pt
+from tfg_b200 import scenes
+
+pytestmark = pytest.mark.gpu
+
+MISS = 0xFFFFFFFF
+
+
+@pytest.fixture(scope="module")
+def setup(built):
+    scene = scenes.box_icosphere(256, 192, subdiv=5)
+    ds = pt.DeviceScene(scene, "cuda")
+    W, H = scene.width, scene.height
+    rays = torch.zeros(W * H * 8, dtype=torch.float32, device="cuda")
+    pt.camera_rays(ds, 3, rays)
+    # plus incoherent rays from inside the box
+    rng = np.random.default_rng(0)
+    n = 60000
+    r = np.zeros((n, 8), np.float32)
+    r[:, :3] = rng.uniform([-2.5, -1.9, -3.9], [2.5, 2.3, 5.4], (n, 3))
+    d = rng.normal(size=(n, 3))
+    r[:, 4:7] = d / np.linalg.norm(d, axis=1, keepdims=True)
+    r[:, 3] = 1e9
+    rays_all = torch.cat([rays, torch.from_numpy(r.reshape(-1)).cuda()])
+    yield scene, ds, rays, rays_all
+    ds.close()
+
+
+def _trace(ds, rays, fmt):
+    hits = torch.zeros(rays.numel() // 2, dtype=torch.float32, device="cuda")
+    pt.trace_rays(ds, rays, hits, fmt)
+    torch.cuda.synchronize()
+    return hits.view(-1, 4).cpu().numpy()
+
+
+def _ref_trace(ds, rays):
+    ref = orc.ref()
+    if ref is None:
+        pytest.skip("reference kernels (oracle/_ref) not built")
+    n = rays.numel() // 8
+    hits = torch.zeros(n * 4, dtype=torch.float32, device="cuda")
+    steps = torch.zeros(n, dtype=torch.int32, device="cuda")
+    assert ref.ref_trace(ds.bvh.ref.d_nodos, ds.bvh.ref.d_tris, rays.data_ptr(), n, hits.data_ptr(),
+                         steps.data_ptr()) == 0
+    torch.cuda.synchronize()
+    return hits.view(-1, 4).cpu().numpy(), steps.cpu().numpy()
+
+
+def test_camera_rays_match_cpu_restatement(setup):
+    scene, ds, rays, _ = setup
+    got = rays.view(-1, 8).cpu().numpy()
+    want = orc.camera_rays(scene.camera, scene.width, scene.height, 3)
+    np.testing.assert_allclose(got[:, :7], want[:, :7], rtol=0, atol=2e-7)
+    assert (got[:, :7] == want[:, :7]).mean() > 0.999
+
+
+def test_ref_layout_ids_bit_exact_vs_reference_traversal(setup):
+    _, ds, _, rays = setup
+    mine = _trace(ds, rays, pt.TRIS_REF)
+    ref, _ = _ref_trace(ds, rays)
+    a, b = mine[:, 3].view(np.uint32), ref[:, 3].view(np.uint32)
+    assert (a != MISS).mean() > 0.2
+    assert np.array_equal(a, b), f"{(a != b).sum()} id mismatches"
+    hit = a != MISS
+    np.testing.assert_allclose(mine[hit, 0], ref[hit, 0], rtol=1e-6)
+
+
+def test_watertight_ids_vs_reference_traversal(setup):
+    _, ds, _, rays = setup
+    mine = _trace(ds, rays, pt.TRIS_WATERTIGHT)
+    ref, _ = _ref_trace(ds, rays)
+    a, b = mine[:, 3].view(np.uint32), ref[:, 3].view(np.uint32)
+    same = a == b
+    # mismatches must be edge / vertex hits: a barycentric within 1e-4 of an edge in
+    # either result, or both hits at the same distance (adjacent triangles)
+    def near_edge(h):
+        u, v = h[:, 1], h[:, 2]
+        return np.minimum(np.minimum(u, v), 1.0 - u - v) < 1e-4
+    tie = np.isclose(mine[:, 0], ref[:, 0], rtol=1e-5) & (a != MISS) & (b != MISS)
+    explained = near_edge(mine) | near_edge(ref) | tie
+    bad = ~same & ~explained
+    assert bad.sum() == 0, f"{bad.sum()} unexplained id mismatches of {len(a)}"
+    assert (~same).mean() < 1e-3
+    both = same & (a != MISS)
+    rel = np.abs(mine[both, 0] - ref[both, 0]) / ref[both, 0]
+    assert rel.max() <= 1e-5, f"t rel error {rel.max():.2e}"
+
+
+def test_traversal_vs_cpu_oracle(setup):
+    scene, ds, _, rays = setup
+    hb = hbvh.build_host(hbvh.triangle_vertices(scene.mesh))
+    mine = _trace(ds, rays, pt.TRIS_REF)
+    cpu, _ = orc.trace_batch(hb.nodes, hb.tris_ref, rays.view(-1, 8).cpu().numpy())
+    a, b = mine[:, 3].view(np.uint32), cpu[:, 3].view(np.uint32)
+    assert (a != b).mean() < 1e-4
+    both = (a == b) & (a != MISS)
+    np.testing.assert_allclose(mine[both, 0], cpu[both, 0], rtol=1e-5)
+
+
+def test_device_bvh_equals_host_build(setup):
+    """tfgTinyBVHConstruir uploads exactly what tfgCWBVHBuild returns."""
+    scene, ds, _, _ = setup
+    hb = hbvh.build_host(hbvh.triangle_vertices(scene.mesh))
+    assert ds.bvh.ref.num_nodos == hb.num_nodes and ds.bvh.ref.num_tris == hb.num_tris
+    from tfg_b200.devmem import view_device
+    nodes = view_device(ds.bvh.ref.d_nodos, hb.nodes.size).cpu().numpy()
+    tris = view_device(ds.bvh.ref.d_tris, hb.tris_ref.size).cpu().numpy()
+    wt = view_device(ds.bvh.d_tris_wt, hb.tris_wt.size).cpu().numpy()
+    assert np.array_equal(tris.view(np.uint32), hb.tris_ref.reshape(-1).view(np.uint32))
+    assert np.array_equal(wt.view(np.uint32), hb.tris_wt.reshape(-1).view(np.uint32))
+    assert np.array_equal(nodes.view(np.uint32), hb.nodes.reshape(-1).view(np.uint32))
+
+
+def test_empty_batch_and_all_miss(setup):
+    _, ds, _, _ = setup
+    r = torch.zeros(8 * 64, dtype=torch.float32, device="cuda").view(64, 8)
+    r[:, 0:3] = 100.0        # far outside, pointing away
+    r[:, 4] = 1.0
+    r[:, 3] = 1e9
+    h = _trace(ds, r.reshape(-1), pt.TRIS_WATERTIGHT)
+    assert (h[:, 3].view(np.uint32) == MISS).all() and (h[:, 0] == 1e9).all()
+    pt.trace_rays(ds, torch.zeros(0, device="cuda"), torch.zeros(0, device="cuda"))

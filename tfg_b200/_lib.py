@@ -1,0 +1,83 @@
+"""ctypes binding of the native library (tfg_b200/libtfgpt.so).
+
+The library is the product: there is no Python or CPU fallback.  Importing
+this module raises if the library has not been built.  Every wrapper below
+raises ``TfgError`` on a non-zero return, carrying tfgGetLastErrorString().
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_float, c_int32, c_uint32, c_void_p
+from pathlib import Path
+
+from .structs import CCWBVHHost, CImagenGPU, CRenderParams, CRenderProfile, CTinyBVH, CTinyBVHD_GPU
+
+LIB_PATH = Path(__file__).resolve().parent / "libtfgpt.so"
+
+
+class TfgError(RuntimeError):
+    def __init__(self, fn: str, code: int, msg: str):
+        super().__init__(f"{fn} failed ({code}): {msg}")
+        self.code = code
+
+
+def _load() -> ctypes.CDLL:
+    if not LIB_PATH.exists():
+        raise ImportError(f"native library missing: {LIB_PATH} (run tfg_b200/_build.py)")
+    return ctypes.CDLL(str(LIB_PATH))
+
+
+lib = _load()
+
+# name -> (restype, argtypes)
+_PROTOS = {
+    "tfgGetLastErrorString": (c_char_p, []),
+    "tfgCWBVHBuild": (c_int32, [POINTER(c_float), c_uint32, POINTER(CCWBVHHost)]),
+    "tfgCWBVHFree": (None, [POINTER(CCWBVHHost)]),
+    "tfgTinyBVHConstruir": (c_int32, [c_void_p, c_int32, POINTER(CTinyBVH)]),
+    "tfgTinyBVHLiberar": (None, [POINTER(CTinyBVH)]),
+    "tfgRenderParamsReference": (None, [POINTER(CRenderParams)]),
+    "tfgRenderProfileReset": (c_int32, []),
+    "tfgRenderProfileGet": (c_int32, [POINTER(CRenderProfile)]),
+    "tfgLaunchKernelRenderTiny": (c_int32, [
+        c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32,
+        POINTER(CTinyBVHD_GPU), c_void_p, c_int32, POINTER(CImagenGPU), c_void_p, c_void_p, c_void_p, c_int32,
+        c_void_p, c_void_p, c_int32, c_int32, c_void_p]),
+    "tfgRenderPass": (c_int32, [
+        POINTER(CRenderParams), c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32,
+        POINTER(CTinyBVHD_GPU), c_void_p, c_void_p, c_int32, POINTER(CImagenGPU), c_void_p, c_void_p, c_void_p,
+        c_int32, c_void_p, c_void_p, c_int32, c_int32, c_void_p]),
+    "tfgTraceRays": (c_int32, [POINTER(CTinyBVHD_GPU), c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_void_p]),
+    "tfgGenerateCameraRays": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
+    "tfgLaunchInicializarCamara": (c_int32, [c_void_p, c_int32, c_int32, c_void_p]),
+    "tfgLaunchKernelComposite": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p]),
+    "tfgLaunchKernelCalcularTargets": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_void_p]),
+    "tfgLaunchKernelPrepararInferenciaTail": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p]),
+    "tfgLaunchGenerarIndicesAleatorios": (c_int32, [c_void_p, c_int32, c_int32, c_uint32, c_void_p]),
+    "tfgLaunchPrepararDatosEntrenamiento": (c_int32, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p,
+                                                      c_void_p, c_void_p, c_void_p]),
+    "tfgLaunchPrepararDatosInferencia": (c_int32, [c_void_p, c_uint32, c_uint32, c_void_p, c_void_p, c_void_p]),
+    "tfgLaunchGuardarSalidaInferencia": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p]),
+}
+
+for _name, (_res, _args) in _PROTOS.items():
+    _f = getattr(lib, _name)
+    _f.restype = _res
+    _f.argtypes = _args
+
+
+def last_error() -> str:
+    return lib.tfgGetLastErrorString().decode(errors="replace")
+
+
+def check(fn: str, code: int) -> None:
+    if code != 0:
+        raise TfgError(fn, code, last_error())
+
+
+def call(name: str, *args) -> None:
+    check(name, getattr(lib, name)(*args))
+
+
+def exported_symbols() -> list[str]:
+    return list(_PROTOS)

@@ -1,0 +1,923 @@
+// Wavefront path tracer: the reference's per-pixel megakernel
+// (RenderKernel.cu:28-47 -> render.h:416-466 -> render.h:33-262) split into
+// queue stages.
+//
+//   generate   one thread per pixel: RNG seed + jitter + NRC draws, camera ray
+//   trace      persistent warps pull rays from the queue (one atomic per warp),
+//              closest hit over analytic primitives then the CWBVH
+//   shade      emission, NRC footprint / capture logic, BSDF sampling, Russian
+//              roulette; survivors are compacted into the next ray queue and
+//              diffuse hits into the shadow queue (warp ballot + one atomic)
+//   shadow     next-event estimation to every point light, in light order,
+//              added to the path's radiance
+//   resolve    per pixel: image, accumulation, inference/throughput buffers,
+//              training records
+//
+// A path's bounce count equals the queue it sits in, so no depth is stored.
+// Random numbers are drawn in the reference's order, so a path consumes the
+// same stream as in the reference.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstdio>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/tfg_pt.h"
+#include "cwbvh_traverse.cuh"
+#include "pt_common.cuh"
+#include "tfg_errors.h"
+#include "tfg_runtime.h"
+
+namespace tfg {
+
+// ------------------------------------------------------------------ state
+enum : uint32_t {
+    F_TRAIN = 1u,       // es_ruta_entrenamiento (render.h:443)
+    F_UNBIASED = 2u,    // es_ruta_insesgada (render.h:65)
+    F_CAPTURED = 4u,    // punto_entrenamiento_encontrado
+    F_INF = 8u,         // inference query written by shade
+    F_TAIL = 16u,       // tail vertex recorded
+};
+
+constexpr uint32_t kMissId = 0xFFFFFFFFu;
+
+// Traversal work totals for TFG_PROFILE_COUNTS: rays, nodes, triangle tests
+// for closest-hit rays, then the same for shadow rays.
+__device__ unsigned long long g_work[6];
+
+__device__ __forceinline__ void flush_work(int base, uint32_t rays, const TravCounts& c) {
+    unsigned long long v[3] = {rays, c.nodes, c.tris};
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        unsigned long long x = v[k];
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xFFFFFFFFu, x, o);
+        if ((threadIdx.x & 31u) == 0 && x) atomicAdd(&g_work[base + k], x);
+    }
+}
+constexpr uint32_t kAnalyticBit = 0x80000000u;
+constexpr int kMaxBounces = 64;
+constexpr int kSmemPrims = 128;
+
+struct Workspace {
+    size_t cap = 0;          // paths
+    size_t train_cap = 0;    // paths with training scratch
+    float4* ray[2] = {nullptr, nullptr};   // 2 float4 per ray: (O, tmax), (D, pixel)
+    float4* hit = nullptr;                  // (t, u, v, id)
+    float4* shadow = nullptr;               // 4 float4 per item
+    float4* thr = nullptr;                  // camino.rgb, ior
+    uint4* st = nullptr;                    // rng, flags, pdf bits, -
+    float4* lpre = nullptr;                 // L_pre.rgb, a_0
+    float4* lsuf = nullptr;                 // L_suf.rgb, a_current
+    float4* nrc = nullptr;                  // a_suffix, a_prefix
+    float4* ts = nullptr;                   // training scratch, 10 float4 per path
+    uint32_t* counters = nullptr;           // per bounce: rays, fetch, shadows, spare
+};
+
+struct PassArgs {
+    const TfgPrimitiva* prims; int nprims;
+    const TfgLuzPuntual* lights; int nlights;
+    const float4* nodes; const float4* tris; int has_bvh;
+    const TfgPrimitiva* mesh; int nmesh;
+    TfgCamara cam;
+    int W, H, frame;
+    TfgColor* img; float* accum;
+    TfgRegistroEntrenamiento* regs; uint32_t* reg_counter; int reg_cap;
+    TfgDatosMLP* infer; TfgColor* thr_out;
+    int use_inf, train;
+    int max_depth, rr_min_depth, shadow_mesh;
+    Workspace ws;
+};
+
+// ------------------------------------------------------------------ helpers
+__device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Warp-aggregated queue append: every lane with `want` gets a unique slot.
+__device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
+    const uint32_t mask = __activemask();
+    const uint32_t vote = __ballot_sync(mask, want);
+    if (!vote) return 0xFFFFFFFFu;
+    const uint32_t leader = __ffs(vote) - 1u;
+    uint32_t base = 0;
+    if (lane_id() == leader) base = atomicAdd(counter, (uint32_t)__popc(vote));
+    base = __shfl_sync(mask, base, leader);
+    return want ? base + __popc(vote & ((1u << lane_id()) - 1u)) : 0xFFFFFFFFu;
+}
+
+__device__ __forceinline__ V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
+
+__device__ __forceinline__ const TfgPrimitiva* prim_of(const PassArgs& a, uint32_t id) {
+    return (id & kAnalyticBit) ? &a.prims[id & ~kAnalyticBit] : &a.mesh[id];
+}
+
+// Closest analytic hit (escenario.h:323-334): strict t < best, t > 1e-6.
+__device__ __forceinline__ int analytic_closest(const APrim* sp, int nsm, const TfgPrimitiva* gp, int n, V3 O, V3 D,
+                                                float& best, float& bu, float& bv) {
+    int hit = -1;
+    for (int i = 0; i < n; ++i) {
+        APrim q;
+        if (i < nsm) q = sp[i];
+        else aprim_load(gp[i], q);
+        float t, u, v;
+        if (aprim_hit(q, O, D, t, u, v) && t < best && t > 1e-6f) { best = t; bu = u; bv = v; hit = i; }
+    }
+    return hit;
+}
+
+__device__ __forceinline__ bool analytic_any(const APrim* sp, int nsm, const TfgPrimitiva* gp, int n, V3 O, V3 D,
+                                             float dist) {
+    for (int i = 0; i < n; ++i) {
+        APrim q;
+        if (i < nsm) q = sp[i];
+        else aprim_load(gp[i], q);
+        float t, u, v;
+        if (aprim_hit(q, O, D, t, u, v) && t > 1e-6f && t < dist) return true;
+    }
+    return false;
+}
+
+__device__ __forceinline__ int load_aprims_smem(APrim* sp, const TfgPrimitiva* gp, int n) {
+    const int nsm = min(n, kSmemPrims);
+    for (int i = threadIdx.x; i < nsm; i += blockDim.x) aprim_load(gp[i], sp[i]);
+    __syncthreads();
+    return nsm;
+}
+
+// ------------------------------------------------------------------ generate
+// render.h:424-447: seed, jitter draws, training / unbiased draws, camera ray.
+__global__ void k_generate(PassArgs a) {
+    const uint32_t N = (uint32_t)a.W * (uint32_t)a.H;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        const int x = (int)(p % (uint32_t)a.W), y = (int)(p / (uint32_t)a.W);
+        uint32_t rng = seed_pixel(x, y, a.frame);
+        const float ox = pcg_uniform(rng);
+        const float oy = pcg_uniform(rng);
+        V3 O, D;
+        camera_ray(a.cam, x, y, a.W, a.H, ox, oy, O, D);
+        uint32_t flags = 0;
+        bool training = a.train ? (a.use_inf ? (pcg_uniform(rng) < 0.05f) : true) : false;
+        if (training) {
+            flags |= F_TRAIN;
+            if (pcg_uniform(rng) < 0.0625f) flags |= F_UNBIASED;
+        }
+        a.ws.ray[0][2 * p + 0] = make_float4(O.x, O.y, O.z, 1e9f);
+        a.ws.ray[0][2 * p + 1] = make_float4(D.x, D.y, D.z, __uint_as_float(p));
+        a.ws.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+        a.ws.st[p] = make_uint4(rng, flags, __float_as_uint(1.0f), 0u);
+        a.ws.lpre[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        if (a.use_inf || a.train) {
+            a.ws.lsuf[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            a.ws.nrc[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ws.counters[0] = N;
+}
+
+// ------------------------------------------------------------------ trace
+template <int TRI_FMT, bool STATS>
+__global__ void __launch_bounds__(128) k_trace(PassArgs a, int bounce) {
+    extern __shared__ unsigned char smem_raw[];
+    uint2* sstack = reinterpret_cast<uint2*>(smem_raw);
+    APrim* sprims = reinterpret_cast<APrim*>(smem_raw + sizeof(uint2) * kSmemStack * blockDim.x);
+    const int nsm = load_aprims_smem(sprims, a.prims, a.nprims);
+    TravStack st;
+    st.smem = sstack; st.stride = blockDim.x; st.tid = threadIdx.x;
+    const float4* rays = a.ws.ray[bounce & 1];
+    const uint32_t n = a.ws.counters[4 * bounce + 0];
+    uint32_t* fetch = &a.ws.counters[4 * bounce + 1];
+    TravCounts cnt;
+    uint32_t nrays = 0;
+    while (true) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(fetch, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane_id();
+        if (i < n) {
+            const float4 o4 = rays[2 * i], d4 = rays[2 * i + 1];
+            const V3 O = xyz(o4), D = xyz(d4);
+            float best = o4.w, bu = 0.0f, bv = 0.0f;
+            uint32_t id = kMissId;
+            const int ai = analytic_closest(sprims, nsm, a.prims, a.nprims, O, D, best, bu, bv);
+            if (ai >= 0) id = kAnalyticBit | (uint32_t)ai;
+            if (a.has_bvh) {
+                float tm = best, hu, hv;
+                uint32_t mid;
+                if (cwbvh_trace<TRI_FMT, false>(a.nodes, a.tris, O, D, 0.0f, tm, mid, hu, hv, st,
+                                                STATS ? &cnt : nullptr) &&
+                    tm < best && tm > kEps) {
+                    best = tm; bu = hu; bv = hv; id = mid;
+                }
+            }
+            a.ws.hit[i] = make_float4(best, bu, bv, __uint_as_float(id));
+            ++nrays;
+        }
+    }
+    if (STATS) flush_work(0, nrays, cnt);
+}
+
+// ------------------------------------------------------------------ shade
+__device__ __forceinline__ void put_geo(float4* dst, V3 P, V3 dir, V3 n, V3 kd, V3 ks) {
+    dst[0] = make_float4(P.x, P.y, P.z, dir.x);
+    dst[1] = make_float4(dir.y, dir.z, n.x, n.y);
+    dst[2] = make_float4(n.z, kd.x, kd.y, kd.z);
+    dst[3] = make_float4(ks.x, ks.y, ks.z, 0.0f);
+}
+
+__device__ __forceinline__ V3 map01(V3 d) { return v3(d.x * 0.5f + 0.5f, d.y * 0.5f + 0.5f, d.z * 0.5f + 0.5f); }
+
+__device__ __forceinline__ void write_datos(TfgDatosMLP* d, V3 P, V3 dir, V3 n, V3 kd, V3 ks) {
+    TfgDatosMLP r;
+    r.posicion.x = P.x; r.posicion.y = P.y; r.posicion.z = P.z;
+    r.direccion.x = dir.x; r.direccion.y = dir.y; r.direccion.z = dir.z;
+    r.normal.x = n.x; r.normal.y = n.y; r.normal.z = n.z;
+    r.difuso.r = kd.x; r.difuso.g = kd.y; r.difuso.b = kd.z;
+    r.especular.r = ks.x; r.especular.g = ks.y; r.especular.b = ks.z;
+    r.color.r = 0.0f; r.color.g = 0.0f; r.color.b = 0.0f;
+    *d = r;
+}
+
+__global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
+    const uint32_t n = a.ws.counters[4 * bounce + 0];
+    const float4* rays = a.ws.ray[bounce & 1];
+    float4* next = a.ws.ray[(bounce + 1) & 1];
+    uint32_t* next_count = &a.ws.counters[4 * (bounce + 1) + 0];
+    uint32_t* shadow_count = &a.ws.counters[4 * bounce + 2];
+    const bool nrc = a.use_inf || a.train;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    // Uniform trip count so that every lane of a warp reaches the warp-wide appends.
+    const uint32_t n_round = (n + stride - 1) / stride * stride;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+        bool live = i < n, want_shadow = false, survive = false;
+        float4 sh0, sh1, sh2, sh3, nr0, nr1;
+        uint32_t p = 0;
+        if (live) {
+            const float4 o4 = rays[2 * i], d4 = rays[2 * i + 1], h = a.ws.hit[i];
+            p = __float_as_uint(d4.w);
+            V3 O = xyz(o4), D = xyz(d4);
+            float4 thr4 = a.ws.thr[p];
+            uint4 st = a.ws.st[p];
+            V3 cam = xyz(thr4);
+            float ior = thr4.w;
+            uint32_t rng = st.x, flags = st.y;
+            float pdf_last = __uint_as_float(st.z);
+            const uint32_t id = __float_as_uint(h.w);
+            float4 lpre = a.ws.lpre[p];
+            float4 lsuf = make_float4(0, 0, 0, 0), nrc4 = make_float4(0, 0, 0, 0);
+            if (nrc) { lsuf = a.ws.lsuf[p]; nrc4 = a.ws.nrc[p]; }
+            bool end = false;
+            if (id == kMissId) {
+                end = true;   // background is black (render.h:227-239)
+            } else {
+                const TfgPrimitiva* pr = prim_of(a, id);
+                const float t = h.x;
+                const V3 P = O + D * t;
+                const V3 nrm = surface_normal(pr, P, h.y, h.z);
+                const V3 view = -D;
+                const float cos_t = fabsf(dot(nrm, -D));
+                const Material m = load_material(pr);
+                const bool es_dif = cmax(m.difuso) > kEps;
+                const bool es_esp = cmax(m.especular) > kEps;
+                const bool captured = (flags & F_CAPTURED) != 0;
+                bool foot_ok = false;
+                if (nrc) {
+                    // Footprint heuristic, render.h:86-102.
+                    const float dist_sq = t * t;
+                    if (bounce == 0) {
+                        lpre.w = dist_sq / (4.0f * kPiF * fmaxf(cos_t, 1e-4f));
+                        lsuf.w = 0.0f;
+                    } else {
+                        const float spread = dist_sq / (fmaxf(pdf_last, 1e-4f) * fmaxf(cos_t, 1e-4f));
+                        if (!captured) lsuf.w += spread;
+                        else nrc4.x += spread;
+                    }
+                    foot_ok = lsuf.w >= lpre.w * 0.01f;
+                }
+                if (cmax(m.emision) > 0.0f) {
+                    // Emission ends the path (render.h:104-123).
+                    const V3 c = mul(cam, m.emision);
+                    if (captured) {
+                        lsuf.x += c.x; lsuf.y += c.y; lsuf.z += c.z;
+                        put_geo(&a.ws.ts[10 * (size_t)p + 4], P, normalized(-D), nrm, v3(0, 0, 0), v3(0, 0, 0));
+                        a.ws.ts[10 * (size_t)p + 9] = make_float4(0, 0, 0, 0);
+                        flags |= F_TAIL;
+                    } else {
+                        lpre.x += c.x; lpre.y += c.y; lpre.z += c.z;
+                    }
+                    end = true;
+                } else {
+                    if (es_dif) {
+                        // Next-event estimation is deferred to the shadow stage (render.h:126-131).
+                        const V3 ps = P + nrm * kEps;
+                        want_shadow = true;
+                        sh0 = make_float4(ps.x, ps.y, ps.z, __uint_as_float(p));
+                        sh1 = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(captured ? 1u : 0u));
+                        sh2 = make_float4(m.difuso.x, m.difuso.y, m.difuso.z, 0.0f);
+                        sh3 = make_float4(cam.x, cam.y, cam.z, 0.0f);
+                    }
+                    if (captured) {
+                        // Suffix bootstrap termination (render.h:134-163).
+                        const bool stop = !(flags & F_UNBIASED) && (nrc4.x >= nrc4.y);
+                        if (stop) {
+                            put_geo(&a.ws.ts[10 * (size_t)p + 4], P, map01(view), map01(nrm), m.difuso, m.especular);
+                            const V3 refl = m.difuso + m.especular + m.transmision;
+                            const V3 ts = mul(cam, refl);
+                            a.ws.ts[10 * (size_t)p + 9] = make_float4(ts.x, ts.y, ts.z, 0.0f);
+                            flags |= F_TAIL;
+                            end = true;
+                        }
+                    }
+                    if (!end && es_dif && !es_esp && foot_ok) {
+                        // Cache query / training head capture (render.h:166-202).
+                        V3 refl = m.difuso + m.especular + m.transmision;
+                        refl = v3(fmaxf(refl.x, 1e-3f), fmaxf(refl.y, 1e-3f), fmaxf(refl.z, 1e-3f));
+                        const bool training = (flags & F_TRAIN) != 0;
+                        if (!training && a.use_inf) {
+                            write_datos(&a.infer[p], P, map01(view), map01(nrm), m.difuso, m.especular);
+                            const V3 tt = mul(cam, refl);
+                            a.thr_out[p] = TfgColor{tt.x, tt.y, tt.z};
+                            flags |= F_INF;
+                            end = true;
+                        } else if (training && !captured) {
+                            put_geo(&a.ws.ts[10 * (size_t)p + 0], P, map01(view), map01(nrm), m.difuso, m.especular);
+                            const V3 tt = mul(cam, refl);
+                            a.ws.ts[10 * (size_t)p + 8] = make_float4(tt.x, tt.y, tt.z, 0.0f);
+                            nrc4.y = lsuf.w;   // a_prefix = a_current
+                            flags |= F_CAPTURED;
+                            // This bounce's NEE still belongs to the prefix: sh1.w stays 0.
+                        }
+                    }
+                    if (!end) {
+                        // BSDF sampling, render.h:264-335.
+                        const float mkd = cmax(m.difuso), mks = cmax(m.especular), mkt = cmax(m.transmision);
+                        const float sum = mkd + mks + mkt;
+                        if (sum <= 0.0f) {
+                            cam = v3(0.0f, 0.0f, 0.0f);
+                        } else {
+                            const float pd = mkd / sum, ps = mks / sum, pt = 1.0f - pd - ps;
+                            const float r = pcg_uniform(rng);
+                            if (r < pd) {
+                                cam = mul(cam, m.difuso);
+                                cam = v3(cam.x / pd, cam.y / pd, cam.z / pd);
+                                const float r1 = pcg_uniform(rng);
+                                const float r2 = pcg_uniform(rng);
+                                const float phi = 2.0f * kPiF * r1;
+                                const float z = sqrtf(1.0f - r2);
+                                if (z > kEps) {
+                                    const float s = sqrtf(r2);
+                                    float sp, cp;
+                                    sincosf(phi, &sp, &cp);
+                                    const V3 wi = to_world(v3(s * cp, s * sp, z), nrm);
+                                    O = P + wi * kEps;
+                                    D = normalized(wi);
+                                    float c = fabsf(dot(wi, nrm));
+                                    if (c < 1e-4f) c = 1e-4f;
+                                    pdf_last = c / kPiF;
+                                }
+                            } else if (r < pd + ps) {
+                                const V3 wr = reflect_dir(D, nrm);
+                                cam = mul(cam, m.especular);
+                                cam = v3(cam.x / ps, cam.y / ps, cam.z / ps);
+                                O = P + wr * kEps;
+                                D = normalized(wr);
+                                pdf_last = 1e6f;
+                            } else {
+                                const V3 wt = refract_dir(D, nrm, m.ior, ior);
+                                cam = mul(cam, m.transmision);
+                                cam = v3(cam.x / pt, cam.y / pt, cam.z / pt);
+                                O = P + wt * kEps;
+                                D = normalized(wt);
+                                pdf_last = 1e6f;
+                            }
+                        }
+                        // Russian roulette, render.h:209-224.
+                        if (bounce >= a.rr_min_depth) {
+                            float prob = fmaxf(cam.x, fmaxf(cam.y, cam.z));
+                            if (prob > 0.95f) prob = 0.95f;
+                            if (pcg_uniform(rng) > prob) end = true;
+                            else cam = v3(cam.x / prob, cam.y / prob, cam.z / prob);
+                        }
+                        if (!end && bounce + 1 < a.max_depth) survive = true;
+                    }
+                }
+            }
+            a.ws.thr[p] = make_float4(cam.x, cam.y, cam.z, ior);
+            a.ws.st[p] = make_uint4(rng, flags, __float_as_uint(pdf_last), 0u);
+            a.ws.lpre[p] = lpre;
+            if (nrc) { a.ws.lsuf[p] = lsuf; a.ws.nrc[p] = nrc4; }
+            nr0 = make_float4(O.x, O.y, O.z, 1e9f);
+            nr1 = make_float4(D.x, D.y, D.z, __uint_as_float(p));
+        }
+        const uint32_t slot = warp_append(next_count, survive);
+        if (survive) { next[2 * slot] = nr0; next[2 * slot + 1] = nr1; }
+        const uint32_t sslot = warp_append(shadow_count, want_shadow);
+        if (want_shadow) {
+            float4* s = &a.ws.shadow[4 * (size_t)sslot];
+            s[0] = sh0; s[1] = sh1; s[2] = sh2; s[3] = sh3;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ shadow
+// escenario.h:144-184: every light in order, Lambert BRDF kd/pi, inverse-square
+// falloff with the distance clamped to >= 1, summed then scaled by the path
+// throughput (render.h:128-130).
+template <int TRI_FMT, bool STATS>
+__global__ void __launch_bounds__(128) k_shadow(PassArgs a, int bounce) {
+    extern __shared__ unsigned char smem_raw[];
+    uint2* sstack = reinterpret_cast<uint2*>(smem_raw);
+    APrim* sprims = reinterpret_cast<APrim*>(smem_raw + sizeof(uint2) * kSmemStack * blockDim.x);
+    const int nsm = load_aprims_smem(sprims, a.prims, a.nprims);
+    TravStack stck;
+    stck.smem = sstack; stck.stride = blockDim.x; stck.tid = threadIdx.x;
+    const uint32_t n = a.ws.counters[4 * bounce + 2];
+    TravCounts cnt;
+    uint32_t nrays = 0;
+    const uint32_t stride = gridDim.x * blockDim.x;
+    const uint32_t n_round = STATS ? (n + stride - 1) / stride * stride : n;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
+        if (STATS && i >= n) continue;
+        const float4* s = &a.ws.shadow[4 * (size_t)i];
+        const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
+        const V3 P = xyz(s0), N = xyz(s1), kd = xyz(s2), cam = xyz(s3);
+        const uint32_t p = __float_as_uint(s0.w);
+        const bool to_suffix = __float_as_uint(s1.w) != 0u;
+        V3 L = v3(0.0f, 0.0f, 0.0f);
+        for (int l = 0; l < a.nlights; ++l) {
+            const TfgLuzPuntual lz = a.lights[l];
+            V3 dl = ld3(lz.posicion) - P;
+            float dist = sqrtf(dot(dl, dl));
+            dl = normalized(dl);
+            const float c = dot(N, dl);
+            if (c <= 0.0f) continue;
+            const V3 so = P + dl * kEps;
+            if (STATS) ++nrays;
+            if (analytic_any(sprims, nsm, a.prims, a.nprims, so, dl, dist)) continue;
+            if (a.shadow_mesh && a.has_bvh) {
+                float tm = dist, hu, hv;
+                uint32_t hid;
+                if (cwbvh_trace<TRI_FMT, true>(a.nodes, a.tris, so, dl, kEps, tm, hid, hu, hv, stck,
+                                               STATS ? &cnt : nullptr)) continue;
+            }
+            const V3 kdpi = v3(kd.x / kPiF, kd.y / kPiF, kd.z / kPiF);
+            dist = fmaxf(dist, 1.0f);
+            const float d2 = dist * dist;
+            const V3 Li = v3(lz.intensidad.r / d2, lz.intensidad.g / d2, lz.intensidad.b / d2);
+            L = L + mul(Li, kdpi) * c;
+        }
+        const V3 add = mul(cam, L);
+        float4* dst = to_suffix ? &a.ws.lsuf[p] : &a.ws.lpre[p];
+        float4 v = *dst;
+        v.x += add.x; v.y += add.y; v.z += add.z;
+        *dst = v;
+    }
+    if (STATS) flush_work(3, nrays, cnt);
+}
+
+// ------------------------------------------------------------------ resolve
+__device__ __forceinline__ void get_geo(const float4* src, TfgDatosGeometricos& g) {
+    const float4 a0 = src[0], a1 = src[1], a2 = src[2], a3 = src[3];
+    g.posicion.x = a0.x; g.posicion.y = a0.y; g.posicion.z = a0.z;
+    g.direccion.x = a0.w; g.direccion.y = a1.x; g.direccion.z = a1.y;
+    g.normal.x = a1.z; g.normal.y = a1.w; g.normal.z = a2.x;
+    g.difuso = TfgColor{a2.y, a2.z, a2.w};
+    g.especular = TfgColor{a3.x, a3.y, a3.z};
+}
+
+__global__ void k_resolve(PassArgs a) {
+    const uint32_t N = (uint32_t)a.W * (uint32_t)a.H;
+    const bool nrc = a.use_inf || a.train;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        const float4 lp = a.ws.lpre[p];
+        if (a.img) a.img[p] = TfgColor{lp.x, lp.y, lp.z};
+        if (a.accum) { a.accum[3 * (size_t)p] += lp.x; a.accum[3 * (size_t)p + 1] += lp.y; a.accum[3 * (size_t)p + 2] += lp.z; }
+        const uint32_t flags = a.ws.st[p].y;
+        const bool rec = nrc && (flags & F_TRAIN) && (flags & F_CAPTURED);
+        if (a.thr_out && !(flags & F_INF) && !rec) a.thr_out[p] = TfgColor{0.0f, 0.0f, 0.0f};
+        if (!rec) continue;
+        // Training path with a head vertex: its pixel keeps the prefix radiance and
+        // asks the cache at the head (render.h:243-260); the record goes to the ring
+        // (render.h:461-464).
+        const float4* ts = &a.ws.ts[10 * (size_t)p];
+        TfgDatosGeometricos head, tail;
+        get_geo(ts, head);
+        const float4 thr_train = ts[8];
+        if (a.infer) {
+            TfgDatosMLP d;
+            d.posicion = head.posicion; d.direccion = head.direccion; d.normal = head.normal;
+            d.difuso = head.difuso; d.especular = head.especular; d.color = TfgColor{0.0f, 0.0f, 0.0f};
+            a.infer[p] = d;
+        }
+        if (a.thr_out) a.thr_out[p] = TfgColor{thr_train.x, thr_train.y, thr_train.z};
+        if (a.reg_counter && a.regs && a.reg_cap > 0) {
+            TfgRegistroEntrenamiento r;
+            r.head = head;
+            float4 thr_suf = make_float4(0, 0, 0, 0);
+            if (flags & F_TAIL) { get_geo(ts + 4, tail); thr_suf = ts[9]; }
+            else { memset(&tail, 0, sizeof(tail)); }
+            r.tail = tail;
+            const float4 ls = a.ws.lsuf[p];
+            r.luz_acumulada_sufijo = TfgColor{ls.x, ls.y, ls.z};
+            r.throughput_sufijo = TfgColor{thr_suf.x, thr_suf.y, thr_suf.z};
+            r.factor_normalizacion = TfgColor{thr_train.x, thr_train.y, thr_train.z};
+            r.valido = 1;
+            const uint32_t idx = atomicAdd(a.reg_counter, 1u);
+            a.regs[idx % (uint32_t)a.reg_cap] = r;
+        }
+    }
+}
+
+// ------------------------------------------------------------------ host side
+namespace {
+
+std::mutex g_ws_mutex;
+Workspace g_ws[16];
+
+int ensure_workspace(int dev, size_t paths, bool nrc, Workspace& out) {
+    std::lock_guard<std::mutex> lk(g_ws_mutex);
+    Workspace& w = g_ws[dev & 15];
+    auto grow = [](void** p, size_t bytes) -> cudaError_t {
+        if (*p) cudaFree(*p);
+        *p = nullptr;
+        return cudaMalloc(p, bytes);
+    };
+    cudaError_t e = cudaSuccess;
+    if (w.cap < paths) {
+        size_t cap = paths;
+        for (int k = 0; k < 2 && e == cudaSuccess; ++k) e = grow((void**)&w.ray[k], cap * 2 * sizeof(float4));
+        if (e == cudaSuccess) e = grow((void**)&w.hit, cap * sizeof(float4));
+        if (e == cudaSuccess) e = grow((void**)&w.shadow, cap * 4 * sizeof(float4));
+        if (e == cudaSuccess) e = grow((void**)&w.thr, cap * sizeof(float4));
+        if (e == cudaSuccess) e = grow((void**)&w.st, cap * sizeof(uint4));
+        if (e == cudaSuccess) e = grow((void**)&w.lpre, cap * sizeof(float4));
+        if (e == cudaSuccess) e = grow((void**)&w.lsuf, cap * sizeof(float4));
+        if (e == cudaSuccess) e = grow((void**)&w.nrc, cap * sizeof(float4));
+        if (e == cudaSuccess && !w.counters) e = cudaMalloc((void**)&w.counters, 4 * (kMaxBounces + 1) * sizeof(uint32_t));
+        if (e != cudaSuccess) { w.cap = 0; return fail((int)e, std::string("render workspace: ") + cudaGetErrorString(e)); }
+        w.cap = cap;
+    }
+    if (nrc && w.train_cap < paths) {
+        e = grow((void**)&w.ts, paths * 10 * sizeof(float4));
+        if (e != cudaSuccess) { w.train_cap = 0; return fail((int)e, std::string("training scratch: ") + cudaGetErrorString(e)); }
+        w.train_cap = paths;
+    }
+    out = w;
+    return 0;
+}
+
+struct LaunchShapes {
+    int sms = 0;
+    int trace_blocks[2] = {0, 0};
+    int shadow_blocks[2] = {0, 0};
+    int shade_blocks = 0;
+};
+LaunchShapes g_shapes[16];
+
+size_t trace_smem(int nprims) {
+    return sizeof(uint2) * kSmemStack * 128 + sizeof(APrim) * (size_t)std::min(nprims, kSmemPrims);
+}
+
+int shapes_for(int dev, LaunchShapes& s) {
+    LaunchShapes& g = g_shapes[dev & 15];
+    if (g.sms == 0) {
+        int sms = 0;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        int occ = 0;
+        size_t sm = trace_smem(kSmemPrims);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<0, false>, 128, sm);
+        g.trace_blocks[0] = sms * std::max(occ, 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<1, false>, 128, sm);
+        g.trace_blocks[1] = sms * std::max(occ, 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<0, false>, 128, sm);
+        g.shadow_blocks[0] = sms * std::max(occ, 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<1, false>, 128, sm);
+        g.shadow_blocks[1] = sms * std::max(occ, 1);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade, 256, 0);
+        g.shade_blocks = sms * std::max(occ, 1);
+        g.sms = sms;
+    }
+    s = g;
+    return 0;
+}
+
+// Stage timing with CUDA events (TFG_PROFILE_TIMES): one start/stop pair per
+// launch, summed by tfgRenderProfileGet.
+struct StageEvents {
+    cudaEvent_t start, stop;
+    int stage;
+};
+std::mutex g_prof_mutex;
+std::vector<StageEvents> g_prof_events;
+size_t g_prof_used = 0;
+double g_prof_ms[5] = {0, 0, 0, 0, 0};
+uint64_t g_prof_launches[5] = {0, 0, 0, 0, 0};
+
+StageEvents profiler_pair(int stage) {
+    std::lock_guard<std::mutex> lk(g_prof_mutex);
+    if (g_prof_used == g_prof_events.size()) {
+        StageEvents ev{};
+        cudaEventCreate(&ev.start);
+        cudaEventCreate(&ev.stop);
+        g_prof_events.push_back(ev);
+    }
+    StageEvents& ev = g_prof_events[g_prof_used++];
+    ev.stage = stage;
+    return ev;
+}
+
+}  // namespace
+
+int profile_reset() {
+    std::lock_guard<std::mutex> lk(g_prof_mutex);
+    g_prof_used = 0;
+    for (int i = 0; i < 5; ++i) { g_prof_ms[i] = 0.0; g_prof_launches[i] = 0; }
+    unsigned long long zero[6] = {0, 0, 0, 0, 0, 0};
+    cudaError_t e = cudaMemcpyToSymbol(g_work, zero, sizeof(zero));
+    if (e != cudaSuccess) return fail((int)e, std::string("profile reset: ") + cudaGetErrorString(e));
+    return ok();
+}
+
+int profile_get(TfgRenderProfile* out) {
+    if (!out) return fail(TFG_E_INVALID, "tfgRenderProfileGet: out is null");
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return fail((int)e, std::string("profile get: ") + cudaGetErrorString(e));
+    std::lock_guard<std::mutex> lk(g_prof_mutex);
+    for (size_t i = 0; i < g_prof_used; ++i) {
+        float ms = 0.0f;
+        e = cudaEventElapsedTime(&ms, g_prof_events[i].start, g_prof_events[i].stop);
+        if (e != cudaSuccess) return fail((int)e, std::string("profile events: ") + cudaGetErrorString(e));
+        g_prof_ms[g_prof_events[i].stage] += ms;
+        g_prof_launches[g_prof_events[i].stage] += 1;
+    }
+    g_prof_used = 0;
+    unsigned long long w[6];
+    e = cudaMemcpyFromSymbol(w, g_work, sizeof(w));
+    if (e != cudaSuccess) return fail((int)e, std::string("profile counters: ") + cudaGetErrorString(e));
+    for (int i = 0; i < 5; ++i) { out->ms[i] = g_prof_ms[i]; out->launches[i] = g_prof_launches[i]; }
+    out->rays = w[0]; out->nodes = w[1]; out->tri_tests = w[2];
+    out->shadow_rays = w[3]; out->shadow_nodes = w[4]; out->shadow_tri_tests = w[5];
+    return ok();
+}
+
+int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
+                const TfgLuzPuntual* lights, int nlights, int W, int H, int frame, const TfgTinyBVHD_GPU* bvh,
+                const float* tris_wt, const TfgPrimitiva* mesh, int nmesh, TfgColor* img, float* accum,
+                TfgRegistroEntrenamiento* regs, uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer,
+                TfgColor* thr_out, int use_inf, int train, cudaStream_t stream) {
+    if (W <= 0 || H <= 0 || (size_t)W * (size_t)H > (1u << 28)) return fail(TFG_E_INVALID, "render: bad image size");
+    if (!d_cam) return fail(TFG_E_INVALID, "render: camara is null");
+    if (nprims < 0 || nlights < 0 || nmesh < 0) return fail(TFG_E_INVALID, "render: negative count");
+    if ((nprims > 0 && !prims) || (nlights > 0 && !lights)) return fail(TFG_E_INVALID, "render: null scene array");
+    if (prm.max_depth < 1 || prm.max_depth > kMaxBounces) return fail(TFG_E_INVALID, "render: max_depth out of [1,64]");
+    if (prm.spp < 1) return fail(TFG_E_INVALID, "render: spp < 1");
+    if (prm.tri_format != TFG_TRIS_REF && prm.tri_format != TFG_TRIS_WATERTIGHT)
+        return fail(TFG_E_INVALID, "render: unknown tri_format");
+    const bool nrc = use_inf || train;
+    if (nrc && (!infer || !thr_out)) return fail(TFG_E_INVALID, "render: NRC flags need inference and throughput buffers");
+    const bool has_bvh = bvh && bvh->d_nodos && bvh->d_tris && nmesh > 0;
+    if (has_bvh && !mesh) return fail(TFG_E_INVALID, "render: mesh primitives are null");
+    if (has_bvh && prm.tri_format == TFG_TRIS_WATERTIGHT && !tris_wt)
+        return fail(TFG_E_INVALID, "render: watertight format needs tris_wt");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    if (int rc = require_sm100(dev)) return rc;
+    Workspace ws;
+    if (int rc = ensure_workspace(dev, (size_t)W * H, nrc, ws)) return rc;
+    LaunchShapes sh;
+    shapes_for(dev, sh);
+
+    TfgCamara cam;
+    e = cudaMemcpyAsync(&cam, d_cam, sizeof(cam), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return fail((int)e, std::string("render: camera read: ") + cudaGetErrorString(e));
+
+    PassArgs a{};
+    a.prims = prims; a.nprims = nprims; a.lights = lights; a.nlights = nlights;
+    a.nodes = has_bvh ? reinterpret_cast<const float4*>(bvh->d_nodos) : nullptr;
+    a.tris = has_bvh ? reinterpret_cast<const float4*>(prm.tri_format == TFG_TRIS_REF ? bvh->d_tris : tris_wt) : nullptr;
+    a.has_bvh = has_bvh ? 1 : 0;
+    a.mesh = mesh; a.nmesh = nmesh;
+    a.cam = cam;
+    a.W = W; a.H = H;
+    a.accum = accum;
+    a.regs = regs; a.reg_counter = reg_counter; a.reg_cap = reg_cap;
+    a.infer = infer; a.thr_out = thr_out; a.use_inf = use_inf; a.train = train;
+    a.max_depth = prm.max_depth; a.rr_min_depth = prm.rr_min_depth; a.shadow_mesh = prm.shadow_mesh;
+    a.ws = ws;
+    const int fmt = prm.tri_format;
+    const size_t smem = trace_smem(nprims);
+    const int gen_blocks = std::max(1, std::min((W * H + 255) / 256, sh.sms * 8));
+    const bool times = (prm.profile & TFG_PROFILE_TIMES) != 0;
+    const bool counts = (prm.profile & TFG_PROFILE_COUNTS) != 0;
+    auto stage = [&](int id, auto&& launch) {
+        if (times) {
+            StageEvents ev = profiler_pair(id);
+            cudaEventRecord(ev.start, stream);
+            launch();
+            cudaEventRecord(ev.stop, stream);
+        } else {
+            launch();
+        }
+    };
+    for (int s = 0; s < prm.spp; ++s) {
+        a.frame = frame + s;
+        a.img = (s == prm.spp - 1) ? img : nullptr;
+        e = cudaMemsetAsync(ws.counters, 0, 4 * (kMaxBounces + 1) * sizeof(uint32_t), stream);
+        if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+        stage(0, [&] { k_generate<<<gen_blocks, 256, 0, stream>>>(a); });
+        for (int b = 0; b < prm.max_depth; ++b) {
+            stage(1, [&] {
+                if (fmt == 0) {
+                    if (counts) k_trace<0, true><<<sh.trace_blocks[0], 128, smem, stream>>>(a, b);
+                    else k_trace<0, false><<<sh.trace_blocks[0], 128, smem, stream>>>(a, b);
+                } else {
+                    if (counts) k_trace<1, true><<<sh.trace_blocks[1], 128, smem, stream>>>(a, b);
+                    else k_trace<1, false><<<sh.trace_blocks[1], 128, smem, stream>>>(a, b);
+                }
+            });
+            stage(2, [&] { k_shade<<<sh.shade_blocks, 256, 0, stream>>>(a, b); });
+            stage(3, [&] {
+                if (fmt == 0) {
+                    if (counts) k_shadow<0, true><<<sh.shadow_blocks[0], 128, smem, stream>>>(a, b);
+                    else k_shadow<0, false><<<sh.shadow_blocks[0], 128, smem, stream>>>(a, b);
+                } else {
+                    if (counts) k_shadow<1, true><<<sh.shadow_blocks[1], 128, smem, stream>>>(a, b);
+                    else k_shadow<1, false><<<sh.shadow_blocks[1], 128, smem, stream>>>(a, b);
+                }
+            });
+        }
+        stage(4, [&] { k_resolve<<<gen_blocks, 256, 0, stream>>>(a); });
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return fail((int)e, std::string("render launch: ") + cudaGetErrorString(e));
+    }
+    return ok();
+}
+
+// ------------------------------------------------------------------ traversal-only entries
+template <int TRI_FMT>
+__global__ void __launch_bounds__(128) k_trace_rays(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                                                    const float4* __restrict__ rays, uint32_t n, float4* __restrict__ hits,
+                                                    uint32_t* fetch) {
+    __shared__ uint2 sstack[kSmemStack * 128];
+    TravStack st;
+    st.smem = sstack; st.stride = blockDim.x; st.tid = threadIdx.x;
+    while (true) {
+        uint32_t base = 0;
+        if (lane_id() == 0) base = atomicAdd(fetch, 32u);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane_id();
+        if (i < n) {
+            const float4 o4 = rays[2 * i], d4 = rays[2 * i + 1];
+            float tm = o4.w, hu = 0.0f, hv = 0.0f;
+            uint32_t id = kMissId;
+            if (!cwbvh_trace<TRI_FMT, false>(nodes, tris, xyz(o4), xyz(d4), 0.0f, tm, id, hu, hv, st, nullptr)) {
+                id = kMissId; tm = o4.w; hu = 0.0f; hv = 0.0f;
+            }
+            hits[i] = make_float4(tm, hu, hv, __uint_as_float(id));
+        }
+    }
+}
+
+__global__ void k_camera_rays(TfgCamara cam, int W, int H, int frame, float4* rays) {
+    const uint32_t N = (uint32_t)W * (uint32_t)H;
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
+        const int x = (int)(p % (uint32_t)W), y = (int)(p / (uint32_t)W);
+        uint32_t rng = seed_pixel(x, y, frame);
+        const float ox = pcg_uniform(rng);
+        const float oy = pcg_uniform(rng);
+        V3 O, D;
+        camera_ray(cam, x, y, W, H, ox, oy, O, D);
+        rays[2 * p] = make_float4(O.x, O.y, O.z, 1e9f);
+        rays[2 * p + 1] = make_float4(D.x, D.y, D.z, 0.0f);
+    }
+}
+
+namespace {
+std::mutex g_fetch_mutex;
+uint32_t* g_fetch[16] = {nullptr};
+}
+
+int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const float* rays, int n, float* hits,
+               cudaStream_t stream) {
+    if (!bvh || !bvh->d_nodos || !rays || !hits || n < 0) return fail(TFG_E_INVALID, "tfgTraceRays: null argument");
+    if (fmt == TFG_TRIS_REF && !bvh->d_tris) return fail(TFG_E_INVALID, "tfgTraceRays: d_tris is null");
+    if (fmt == TFG_TRIS_WATERTIGHT && !tris_wt) return fail(TFG_E_INVALID, "tfgTraceRays: tris_wt is null");
+    if (fmt != TFG_TRIS_REF && fmt != TFG_TRIS_WATERTIGHT) return fail(TFG_E_INVALID, "tfgTraceRays: bad format");
+    if (n == 0) return ok();
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    if (int rc = require_sm100(dev)) return rc;
+    uint32_t* fetch;
+    {
+        std::lock_guard<std::mutex> lk(g_fetch_mutex);
+        if (!g_fetch[dev & 15]) {
+            e = cudaMalloc((void**)&g_fetch[dev & 15], sizeof(uint32_t));
+            if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+        }
+        fetch = g_fetch[dev & 15];
+    }
+    LaunchShapes sh;
+    shapes_for(dev, sh);
+    e = cudaMemsetAsync(fetch, 0, sizeof(uint32_t), stream);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    const float4* tr = reinterpret_cast<const float4*>(fmt == TFG_TRIS_REF ? bvh->d_tris : tris_wt);
+    if (fmt == 0)
+        k_trace_rays<0><<<sh.trace_blocks[0], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
+                                                                 reinterpret_cast<const float4*>(rays), (uint32_t)n,
+                                                                 reinterpret_cast<float4*>(hits), fetch);
+    else
+        k_trace_rays<1><<<sh.trace_blocks[1], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
+                                                                 reinterpret_cast<const float4*>(rays), (uint32_t)n,
+                                                                 reinterpret_cast<float4*>(hits), fetch);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgTraceRays: ") + cudaGetErrorString(e));
+    return ok();
+}
+
+int camera_rays(const TfgCamara* d_cam, int W, int H, int frame, float* rays, cudaStream_t stream) {
+    if (!d_cam || !rays || W <= 0 || H <= 0) return fail(TFG_E_INVALID, "tfgGenerateCameraRays: bad argument");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    if (int rc = require_sm100(dev)) return rc;
+    TfgCamara cam;
+    e = cudaMemcpyAsync(&cam, d_cam, sizeof(cam), cudaMemcpyDeviceToHost, stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    const int blocks = std::max(1, std::min((W * H + 255) / 256, 148 * 8));
+    k_camera_rays<<<blocks, 256, 0, stream>>>(cam, W, H, frame, reinterpret_cast<float4*>(rays));
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    return ok();
+}
+
+}  // namespace tfg
+
+// ------------------------------------------------------------------ C ABI
+extern "C" void tfgRenderParamsReference(TfgRenderParams* p) {
+    if (!p) return;
+    p->max_depth = 20;
+    p->rr_min_depth = 11;
+    p->shadow_mesh = 0;
+    p->tri_format = TFG_TRIS_REF;
+    p->spp = 1;
+    p->accumulate = 0;
+    p->profile = 0;
+    p->reserved = 0;
+}
+
+extern "C" int tfgRenderProfileReset(void) { return tfg::profile_reset(); }
+
+extern "C" int tfgRenderProfileGet(TfgRenderProfile* out) { return tfg::profile_get(out); }
+
+extern "C" int tfgLaunchKernelRenderTiny(
+    const TfgCamara* camara, const TfgPrimitiva* primitivas, int32_t num_primitivas, const TfgLuzPuntual* luces,
+    int32_t num_luces, const TfgPrimitiva* primitivas_malla, int32_t num_primitivas_malla, int32_t ancho_img,
+    int32_t alto_img, int32_t samples_per_pixel, int32_t frame_number, const TfgTinyBVHD_GPU* nodos_bvh,
+    const TfgPrimitiva* primitivas_bvh, int32_t num_nodos_bvh, const TfgImagenGPU* imagen_directa,
+    uint32_t* dev_counter, TfgRegistroEntrenamiento* buffer_registros, uint32_t* counter_train, int32_t max_cap_train,
+    TfgDatosMLP* buffer_inference, TfgColor* buffer_throughput, int32_t usar_red_inferencia, int32_t entrenar_red,
+    void* stream) {
+    (void)primitivas_malla; (void)num_primitivas_malla; (void)samples_per_pixel; (void)dev_counter;
+    if (!imagen_directa) return tfg::fail(TFG_E_INVALID, "tfgLaunchKernelRenderTiny: imagen is null");
+    if (!buffer_throughput) return tfg::fail(TFG_E_INVALID, "tfgLaunchKernelRenderTiny: throughput buffer is null");
+    TfgRenderParams prm;
+    tfgRenderParamsReference(&prm);
+    // The reference kernel draws a training-pixel decision and writes the
+    // inference / throughput buffers every launch (render.h:443-458).
+    return tfg::render_pass(prm, camara, primitivas, num_primitivas, luces, num_luces, ancho_img, alto_img, frame_number,
+                            nodos_bvh, nullptr, primitivas_bvh, num_nodos_bvh, imagen_directa->datos, nullptr,
+                            buffer_registros, counter_train, max_cap_train, buffer_inference, buffer_throughput,
+                            usar_red_inferencia, entrenar_red, (cudaStream_t)stream);
+}
+
+extern "C" int tfgRenderPass(const TfgRenderParams* params, const TfgCamara* camara, const TfgPrimitiva* primitivas,
+                             int32_t num_primitivas, const TfgLuzPuntual* luces, int32_t num_luces, int32_t ancho_img,
+                             int32_t alto_img, int32_t frame_number, const TfgTinyBVHD_GPU* nodos_bvh,
+                             const float* tris_wt, const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh,
+                             const TfgImagenGPU* imagen_directa, float* accum,
+                             TfgRegistroEntrenamiento* buffer_registros, uint32_t* counter_train,
+                             int32_t max_cap_train, TfgDatosMLP* buffer_inference, TfgColor* buffer_throughput,
+                             int32_t usar_red_inferencia, int32_t entrenar_red, void* stream) {
+    if (!params) return tfg::fail(TFG_E_INVALID, "tfgRenderPass: params is null");
+    TfgColor* img = imagen_directa ? imagen_directa->datos : nullptr;
+    return tfg::render_pass(*params, camara, primitivas, num_primitivas, luces, num_luces, ancho_img, alto_img,
+                            frame_number, nodos_bvh, tris_wt, primitivas_bvh, num_prims_bvh, img,
+                            params->accumulate ? accum : nullptr, buffer_registros, counter_train, max_cap_train,
+                            buffer_inference, buffer_throughput, usar_red_inferencia, entrenar_red,
+                            (cudaStream_t)stream);
+}
+
+extern "C" int tfgTraceRays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int32_t tri_format, const float* rays,
+                            int32_t n, float* hits, void* stream) {
+    return tfg::trace_rays(bvh, tris_wt, tri_format, rays, n, hits, (cudaStream_t)stream);
+}
+
+extern "C" int tfgGenerateCameraRays(const TfgCamara* camara, int32_t ancho_img, int32_t alto_img, int32_t frame_number,
+                                     float* rays, void* stream) {
+    return tfg::camera_rays(camara, ancho_img, alto_img, frame_number, rays, (cudaStream_t)stream);
+}

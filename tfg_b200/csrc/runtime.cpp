@@ -1,0 +1,45 @@
+// Error state and device checks shared by all entry points.
+#include <cuda_runtime.h>
+
+#include <cstdio>
+#include <string>
+
+#include "../../include/tfg_pt.h"
+#include "tfg_errors.h"
+#include "tfg_runtime.h"
+
+namespace tfg {
+
+namespace {
+thread_local std::string g_last_error;
+thread_local int g_last_code = 0;
+}  // namespace
+
+void set_error(int code, const std::string& msg) {
+    g_last_code = code;
+    g_last_error = msg;
+}
+
+int fail(int code, const std::string& msg) {
+    set_error(code, msg);
+    return code;
+}
+
+int ok() { return 0; }
+
+int require_sm100(int dev) {
+    static int checked[16] = {0};   // 0 unknown, 1 ok, 2 bad
+    int& c = checked[dev & 15];
+    if (c == 0) {
+        int major = 0;
+        cudaError_t e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+        if (e != cudaSuccess) return fail((int)e, std::string("device query: ") + cudaGetErrorString(e));
+        c = (major == 10) ? 1 : 2;
+    }
+    if (c != 1) return fail(TFG_E_UNSUPPORTED, "this library is built for sm_100a (B200) only");
+    return 0;
+}
+
+}  // namespace tfg
+
+extern "C" const char* tfgGetLastErrorString(void) { return tfg::g_last_error.c_str(); }
