@@ -170,6 +170,24 @@ def reference_arm(args):
     }))
 
 
+def profile_pass():
+    """One 1-spp pass (8 bounces) of the benchmark frame: ~0.3 GB of scene
+    data (more than L2) and ~0.5 GB of queues; used for ncu captures."""
+    import torch
+
+    from tfg_b200 import pathtracer as pt
+    from tfg_b200 import scenes
+    scene = scenes.spheres_terrain(W_PX, H_PX)
+    ds = pt.DeviceScene(scene, "cuda")
+    p = pt.RenderParams(max_depth=DEPTH, rr_min_depth=RR, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT,
+                        spp=1, accumulate=1)
+    accum = torch.zeros(W_PX * H_PX * 3, dtype=torch.float32, device="cuda")
+    pt.render_pass(ds, p, 1, None, accum)
+    torch.cuda.synchronize()
+    ds.close()
+    print("profile pass done")
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -177,9 +195,14 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-pass", action="store_true",
+                    help="run one untimed 1-spp pass of the workload and exit (small case for ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
+        return
+    if args.profile_pass:
+        profile_pass()
         return
 
     import torch

@@ -802,11 +802,12 @@ uint32_t* g_fetch[16] = {nullptr};
 
 int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const float* rays, int n, float* hits,
                cudaStream_t stream) {
-    if (!bvh || !bvh->d_nodos || !rays || !hits || n < 0) return fail(TFG_E_INVALID, "tfgTraceRays: null argument");
+    if (n < 0) return fail(TFG_E_INVALID, "tfgTraceRays: negative ray count");
+    if (n == 0) return ok();
+    if (!bvh || !bvh->d_nodos || !rays || !hits) return fail(TFG_E_INVALID, "tfgTraceRays: null argument");
     if (fmt == TFG_TRIS_REF && !bvh->d_tris) return fail(TFG_E_INVALID, "tfgTraceRays: d_tris is null");
     if (fmt == TFG_TRIS_WATERTIGHT && !tris_wt) return fail(TFG_E_INVALID, "tfgTraceRays: tris_wt is null");
     if (fmt != TFG_TRIS_REF && fmt != TFG_TRIS_WATERTIGHT) return fail(TFG_E_INVALID, "tfgTraceRays: bad format");
-    if (n == 0) return ok();
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
