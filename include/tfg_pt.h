@@ -306,6 +306,55 @@ int tfgLaunchPrepararDatosInferencia(const TfgDatosMLP* datos, uint32_t n_elemen
 int tfgLaunchGuardarSalidaInferencia(const float* network_output, TfgColor* buffer_color,
                                      int32_t n_elements, void* stream);
 
+/* ------------------------------------------------------------------ */
+/* Neural radiance cache MLP (ColorMLP, mlp.h:19-70)                   */
+/* ------------------------------------------------------------------ */
+
+/* Opaque cache model: FP32 master weights, Adam moments, an exponential
+ * moving average of the weights (used for inference, as the reference's
+ * EMA(Adam) optimizer, mlp.cpp:61-69) and packed FP16 / BF16 tensor-core
+ * images of them. */
+typedef struct TfgColorMLP TfgColorMLP;
+
+/* ColorMLP(n_in=15, n_out=3, batch, config) (mlp.cpp:12-87): 12-band
+ * frequency encoding of the position + the 12 other inputs + bias -> 5 x 64
+ * ReLU -> 3.  `batch` (samples per train step, reference 16384) must be a
+ * multiple of 128.  Weights are drawn from `seed`.  Adam lr 1e-2,
+ * beta1 0.9, beta2 0.99, eps 1e-15, EMA decay 0.99. */
+int  tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, TfgColorMLP** out);
+void tfgMlpDestroy(TfgColorMLP* mlp);
+/* ColorMLP::setBounds (mlp.cpp:89-93): position normalisation box. */
+int  tfgMlpSetBounds(TfgColorMLP* mlp, const TfgSceneBounds* bounds);
+int  tfgMlpSetHyperparams(TfgColorMLP* mlp, float lr, float beta1, float beta2, float eps, float ema_decay);
+/* ColorMLP::train_step (mlp.cpp:95-125): one Adam step on `batch` samples
+ * drawn as pcg32(step ^ i) % n_available (NrcKernel.cu:10-16) from the
+ * DatosMLP training buffer (targets in .color).  No step below 100 samples
+ * (mlp.cpp:96).  When `loss_out` is not null the call synchronises the stream
+ * and returns the batch loss there (the reference always did, mlp.cpp:122);
+ * with null it stays asynchronous. */
+int  tfgMlpTrainStep(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t n_available, float* loss_out,
+                     void* stream);
+/* ColorMLP::inference (mlp.cpp:127-170): scrubbed predictions (clamped to
+ * [0, 1e5], NaN -> 0) of `count` samples into `out`.  `in` must be 16-byte
+ * aligned.  Asynchronous (the reference synchronised here). */
+int  tfgMlpInference(TfgColorMLP* mlp, const TfgDatosMLP* in, TfgColor* out, uint32_t count, void* stream);
+/* Inference fused with launchKernelComposite (RenderKernel.cu:49-66):
+ * img[i] += throughput[i] * prediction where throughput[i] != 0. */
+int  tfgMlpInferenceComposite(TfgColorMLP* mlp, const TfgDatosMLP* in, const TfgColor* throughput, TfgColor* img,
+                              uint32_t count, void* stream);
+/* FP32 parameter arrays (count = 23552, padded [out][in] per layer):
+ * which = 0 weights, 1 EMA, 2 Adam m, 3 Adam v. */
+int  tfgMlpGetParams(TfgColorMLP* mlp, int which, float* host, uint32_t count);
+/* Set weights (and EMA), reset Adam state; re-packs the tensor-core images. */
+int  tfgMlpSetParams(TfgColorMLP* mlp, const float* host, uint32_t count);
+/* d loss / d W for one batch drawn with `seed`, without updating anything
+ * (synchronous; for gradient checks). */
+int  tfgMlpComputeGradient(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
+                           float* host_grad, uint32_t count, float* loss_out);
+/* TFG_E_TIMEOUT if a bounded tensor-core wait in an MLP kernel gave up since
+ * the last call (synchronous). */
+int  tfgMlpStatus(void);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,169 @@
+"""The tensor-core cache MLP against the FP64 numpy model (oracle/mlp_oracle):
+inference (alone and fused with the composite), the loss gradient of one
+batch (same sample selection as NrcKernel.cu:10-16), one Adam step, and that
+online training on a known signal drives the loss down."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp_oracle as mo
+from oracle import oracle as orc
+from tfg_b200.nrc import ColorMLP, EMA, WEIGHTS, split_layers
+from tfg_b200.structs import DATOS_MLP
+
+pytestmark = pytest.mark.gpu
+
+LO, HI = (-6.0, -4.0, -10.0), (6.0, 6.0, 2.0)
+
+
+def _datos(rng, n, target_fn=None):
+    d = np.zeros(n, DATOS_MLP)
+    pos = rng.uniform(LO, HI, (n, 3))
+    for j, k in enumerate("xyz"):
+        d["posicion"][k] = pos[:, j]
+        d["direccion"][k] = rng.uniform(0, 1, n)
+        d["normal"][k] = rng.uniform(0, 1, n)
+    kd = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    for j, k in enumerate("rgb"):
+        d["difuso"][k] = kd[:, j]
+        d["especular"][k] = 0.0
+    y = target_fn(pos, kd) if target_fn else rng.uniform(0, 2, (n, 3))
+    for j, k in enumerate("rgb"):
+        d["color"][k] = y[:, j]
+    return d
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).cuda()
+
+
+def _f16(w):
+    return np.asarray(w, np.float32).astype(np.float16).astype(np.float64)
+
+
+@pytest.fixture(scope="module")
+def mlp(built):
+    m = ColorMLP(batch=4096, seed=7)
+    m.set_bounds(LO, HI)
+    yield m
+    m.close()
+
+
+@pytest.mark.parametrize("n", [1000, 128, 5])
+def test_inference_matches_fp64_model(mlp, n):
+    rng = np.random.default_rng(n)
+    d = _datos(rng, n)
+    out = torch.zeros(n * 3, device="cuda")
+    mlp.inference(_dev(d), out, n)
+    torch.cuda.synchronize()
+    got = out.view(n, 3).cpu().numpy()
+    W = [_f16(w) for w in split_layers(mlp.get_params(EMA))]
+    x = mo.encode(mo.rows15(d, LO, HI))
+    want = mo.scrub(mo.forward(W, x)[0])
+    scale = np.abs(mo.forward(W, x)[0]).mean() + 1e-3
+    err = np.abs(got - want) / scale
+    assert np.isfinite(got).all()
+    assert err.max() < 0.05, f"max scaled error {err.max():.3e}"
+    assert err.mean() < 0.01
+
+
+def test_inference_composite(mlp):
+    rng = np.random.default_rng(3)
+    n = 777
+    d = _datos(rng, n)
+    thr = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    thr[rng.random(n) < 0.4] = 0.0
+    img0 = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    img = torch.from_numpy(img0.reshape(-1).copy()).cuda()
+    pred = torch.zeros(n * 3, device="cuda")
+    dd = _dev(d)
+    mlp.inference(dd, pred, n)
+    mlp.inference_composite(dd, torch.from_numpy(thr.reshape(-1).copy()).cuda(), img, n)
+    torch.cuda.synchronize()
+    p = pred.view(n, 3).cpu().numpy()
+    want = img0.copy()
+    on = (thr > 0).any(axis=1)
+    want[on] = img0[on] + thr[on] * p[on]
+    np.testing.assert_allclose(img.view(n, 3).cpu().numpy(), want, rtol=1e-6, atol=1e-6)
+
+
+def test_gradient_matches_fp64_model(mlp):
+    rng = np.random.default_rng(11)
+    n_avail = 20000
+    d = _datos(rng, n_avail)
+    w = mlp.get_params(WEIGHTS)
+    g, loss = mlp.compute_gradient(_dev(d), n_avail, seed=5)
+    idx = np.zeros(mlp.batch, np.int32)
+    orc.cpu.orc_indices(orc.p(idx), n_avail, mlp.batch, 5)
+    sel = d[idx]
+    x = mo.encode(mo.rows15(sel, LO, HI))
+    y = np.stack([sel["color"][k] for k in "rgb"], 1).astype(np.float64)
+    ref_loss, ref = mo.loss_and_grad([_f16(a) for a in split_layers(w)], x, y)
+    assert abs(loss - ref_loss) / ref_loss < 0.02, (loss, ref_loss)
+    for l, (gg, rr) in enumerate(zip(split_layers(g), ref)):
+        rel = np.linalg.norm(gg - rr) / (np.linalg.norm(rr) + 1e-30)
+        assert rel < 0.05, f"layer {l}: relative gradient error {rel:.3e}"
+
+
+def test_one_adam_step(built):
+    """At t = 1 bias-corrected Adam moves every weight with a non-zero
+    gradient by exactly lr against the gradient's sign."""
+    m = ColorMLP(batch=1024, seed=3)
+    m.set_bounds(LO, HI)
+    rng = np.random.default_rng(2)
+    d = _datos(rng, 5000)
+    dd = _dev(d)
+    w0 = m.get_params(WEIGHTS)
+    g, _ = m.compute_gradient(dd, 5000, seed=0)
+    m.set_hyperparams(lr=1e-3, eps=1e-30)
+    m.train_step(dd, 5000)
+    w1 = m.get_params(WEIGHTS)
+    big = np.abs(g) > 1e-6
+    np.testing.assert_allclose(np.abs(w1 - w0)[big], 1e-3, rtol=1e-3)
+    assert (np.sign(w1 - w0)[big] == -np.sign(g[big])).mean() > 0.999
+    # the EMA moved 1% of the way (decay 0.99), debiased for inference
+    e1 = m.get_params(EMA)
+    np.testing.assert_allclose(e1, 0.99 * w0 + 0.01 * w1, rtol=1e-5, atol=1e-7)
+    m.close()
+
+
+def test_small_buffer_is_a_no_op(mlp):
+    rng = np.random.default_rng(4)
+    d = _datos(rng, 99)
+    w0 = mlp.get_params(WEIGHTS)
+    assert mlp.train_step(_dev(d), 99) == 0.0
+    assert np.array_equal(mlp.get_params(WEIGHTS), w0)
+
+
+def test_online_training_learns_a_signal(built):
+    """Radiance-like target: smooth in position, scaled by albedo."""
+    m = ColorMLP(batch=4096, seed=9)
+    m.set_bounds(LO, HI)
+    rng = np.random.default_rng(8)
+
+    def f(pos, kd):
+        base = 0.5 + 0.4 * np.sin(0.7 * pos[:, :1]) * np.cos(0.5 * pos[:, 2:3])
+        return base * (0.2 + kd)
+
+    n = 50000
+    d = _datos(rng, n, f)
+    dd = _dev(d)
+    test = _datos(np.random.default_rng(99), 4096, f)
+    y = np.stack([test["color"][k] for k in "rgb"], 1)
+
+    def held_out_error():
+        out = torch.zeros(4096 * 3, device="cuda")
+        m.inference(_dev(test), out, 4096)
+        torch.cuda.synchronize()
+        p = out.view(-1, 3).cpu().numpy()
+        return np.mean((p - y) ** 2 / (y ** 2 + 1e-2))
+
+    before = held_out_error()
+    losses = [m.train_step(dd, n) for _ in range(300)]
+    assert np.isfinite(losses).all()
+    first, last = np.mean(losses[:10]), np.mean(losses[-10:])
+    assert last < first / 5, (first, last)
+    # inference with the EMA weights tracks the signal on held-out samples
+    after = held_out_error()
+    assert after < 0.2 * before, (before, after)
+    m.close()

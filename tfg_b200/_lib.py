@@ -7,7 +7,7 @@ raises ``TfgError`` on a non-zero return, carrying tfgGetLastErrorString().
 from __future__ import annotations
 
 import ctypes
-from ctypes import POINTER, c_char_p, c_float, c_int32, c_uint32, c_void_p
+from ctypes import POINTER, c_char_p, c_float, c_int32, c_uint32, c_uint64, c_void_p
 from pathlib import Path
 
 from .structs import CCWBVHHost, CImagenGPU, CRenderParams, CRenderProfile, CTinyBVH, CTinyBVHD_GPU
@@ -58,6 +58,18 @@ _PROTOS = {
                                                       c_void_p, c_void_p, c_void_p]),
     "tfgLaunchPrepararDatosInferencia": (c_int32, [c_void_p, c_uint32, c_uint32, c_void_p, c_void_p, c_void_p]),
     "tfgLaunchGuardarSalidaInferencia": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p]),
+    "tfgMlpCreate": (c_int32, [c_uint32, c_uint32, c_uint32, c_uint64, POINTER(c_void_p)]),
+    "tfgMlpDestroy": (None, [c_void_p]),
+    "tfgMlpSetBounds": (c_int32, [c_void_p, c_void_p]),
+    "tfgMlpSetHyperparams": (c_int32, [c_void_p, c_float, c_float, c_float, c_float, c_float]),
+    "tfgMlpTrainStep": (c_int32, [c_void_p, c_void_p, c_uint32, POINTER(c_float), c_void_p]),
+    "tfgMlpInference": (c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
+    "tfgMlpInferenceComposite": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
+    "tfgMlpGetParams": (c_int32, [c_void_p, c_int32, POINTER(c_float), c_uint32]),
+    "tfgMlpSetParams": (c_int32, [c_void_p, POINTER(c_float), c_uint32]),
+    "tfgMlpComputeGradient": (c_int32, [c_void_p, c_void_p, c_uint32, c_uint32, POINTER(c_float), c_uint32,
+                                        POINTER(c_float)]),
+    "tfgMlpStatus": (c_int32, []),
 }
 
 for _name, (_res, _args) in _PROTOS.items():

@@ -1,0 +1,954 @@
+// Neural radiance cache MLP on sm_100a tensor cores: the replacement for the
+// reference's ColorMLP over tiny-cuda-nn (mlp.h:19-70, mlp.cpp:22-275).
+//
+// Network: 15 reference inputs (NrcKernel.cu:18-97 layout: position
+// normalised to the scene bounds, view direction and normal mapped to [0,1],
+// diffuse and specular albedo) -> 12-band frequency encoding of the position
+// (sin, cos of 2^b*pi*p, b = 0..11: 72 features) + the 12 other inputs + a
+// constant 1 (first-layer bias) -> 96 features -> 5 hidden layers of 64 ReLU
+// -> 3 outputs (no output activation).  FP16 weights and activations with FP32
+// accumulation for inference and the training forward pass; BF16 for the
+// backward pass (gradients exceed the FP16 range); FP32 master weights, Adam
+// and an exponential moving average of the weights (used for inference), as
+// the reference's EMA(Adam) configuration (mlp.cpp:61-69).
+// Loss: relative L2 on luminance (the reference's RelativeL2Luminance):
+// mean over samples and channels of (y_hat - y)^2 / (lum(y_hat)^2 + 0.01), the
+// denominator treated as a constant.
+//
+// Kernels (one CTA = one warpgroup of 128 threads, one thread per sample row
+// of a 128-sample tile, TMEM accumulators, SW128 K-major operands in shared
+// memory, one elected thread issues tcgen05.mma):
+//   k_infer   inputs by bulk (TMA) copy, encode, 6 chained layer GEMMs,
+//             output scrub (NrcKernel.cu:99-126) and optionally the
+//             composite img += throughput * prediction (RenderKernel.cu:49-66)
+//   k_train   gather (NrcKernel.cu:10-68 sample selection), forward, loss
+//             gradient, backward through the layers; writes transposed
+//             activation / gradient tiles for the weight gradients
+//   k_wgrad   dW = dZ^T H per layer, reduced over the batch with tcgen05
+//   k_adam    Adam + EMA on FP32 masters, re-packs the three weight images
+#include <cuda_bf16.h>
+#include <cuda_fp16.h>
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "../../include/tfg_pt.h"
+#include "pt_common.cuh"
+#include "tfg_errors.h"
+#include "tfg_runtime.h"
+#include "umma.cuh"
+
+namespace tfg {
+namespace mlp {
+
+constexpr int kTile = 128;
+constexpr int kIn = 96;          // encoded features
+constexpr int kHid = 64;
+constexpr int kLayers = 6;       // 96->64, 4 x 64->64, 64->16 (3 used)
+constexpr int kOutPad = 16;
+constexpr int kBands = 12;
+
+// FP32 master parameters, row-major [out][in] per layer with padded shapes
+// 64x96, 4 x 64x64, 16x64 (rows 3..15 of the last layer stay zero).
+__host__ __device__ constexpr int kRows(int l) { return l == kLayers - 1 ? 16 : 64; }
+__host__ __device__ constexpr int kCols(int l) { return l == 0 ? 96 : 64; }
+__host__ __device__ constexpr int kPOff(int l) { return l == 0 ? 0 : (l <= 5 ? 6144 + (l - 1) * 4096 : 23552); }
+constexpr int kParams = 23552;
+
+// Forward / inference weight image (FP16, SW128 K-major): layer 0 uses two
+// K regions (64 rows x 128 B each), layers 1-4 one region, layer 5 16 rows.
+__host__ __device__ constexpr int kFOff(int l) { return l == 0 ? 0 : (l <= 5 ? 16384 + (l - 1) * 8192 : 51200); }
+constexpr int kFwdBytes = 51200;
+// Backward image (BF16, W^T: [in rows][out K]) for layers 1..5; layer 5's
+// K = 16 occupies the first two chunks of each row.
+__host__ __device__ constexpr int kBOff(int l) { return l == 0 ? 0 : (l - 1) * 8192; }
+constexpr int kBwdBytes = 40960;
+
+// Transposed per-tile layouts written by k_train for k_wgrad: feature rows x
+// 128 samples, two 64-sample K regions of F*128 bytes.
+__host__ __device__ constexpr int kHTFeat(int l) { return l == 0 ? 96 : 64; }   // input of layer l
+__host__ __device__ constexpr int kZTFeat(int l) { return l == kLayers - 1 ? 16 : 64; }   // output gradient of layer l
+
+constexpr uint32_t kSpinLimit = 1u << 26;
+
+struct Bounds {
+    float lo[3], hi[3];
+};
+
+__device__ int g_mlp_error;   // set when a bounded wait gives up (TFG_E_TIMEOUT)
+
+// ------------------------------------------------------------------ small helpers
+__device__ __forceinline__ uint32_t pack_h2(float a, float b) {
+    __half2 h = __floats2half2_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+__device__ __forceinline__ uint32_t pack_bf2(float a, float b) {
+    __nv_bfloat162 h = __floats2bfloat162_rn(a, b);
+    return *reinterpret_cast<uint32_t*>(&h);
+}
+
+__device__ __forceinline__ float unit_clamp(float v, float lo, float hi) {   // NrcKernel.cu:5-8
+    float n = (v - lo) / (hi - lo);
+    return fminf(fmaxf(n, 0.0f), 1.0f);
+}
+
+// Encoded features of one sample, packed as 48 FP16 pairs (96 features).
+__device__ __forceinline__ void encode(const TfgDatosMLP& d, const Bounds& b, uint32_t (&w)[48]) {
+    const float p[3] = {unit_clamp((float)d.posicion.x, b.lo[0], b.hi[0]),
+                        unit_clamp((float)d.posicion.y, b.lo[1], b.hi[1]),
+                        unit_clamp((float)d.posicion.z, b.lo[2], b.hi[2])};
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        float s, c;
+        sincospif(p[j], &s, &c);
+#pragma unroll
+        for (int k = 0; k < kBands; ++k) {
+            w[12 * j + k] = pack_h2(s, c);
+            const float s2 = 2.0f * s * c;
+            const float c2 = (c - s) * (c + s);
+            s = s2;
+            c = c2;
+        }
+    }
+    w[36] = pack_h2((float)d.direccion.x, (float)d.direccion.y);
+    w[37] = pack_h2((float)d.direccion.z, (float)d.normal.x);
+    w[38] = pack_h2((float)d.normal.y, (float)d.normal.z);
+    w[39] = pack_h2(d.difuso.r, d.difuso.g);
+    w[40] = pack_h2(d.difuso.b, d.especular.r);
+    w[41] = pack_h2(d.especular.g, d.especular.b);
+    w[42] = pack_h2(1.0f, 0.0f);
+#pragma unroll
+    for (int k = 43; k < 48; ++k) w[k] = 0u;
+}
+
+// Store the 96 encoded features of row r into the two-region A buffer.
+__device__ __forceinline__ void store_encoded(uint8_t* a0, int r, const uint32_t (&w)[48]) {
+#pragma unroll
+    for (int c = 0; c < 12; ++c) {
+        uint8_t* region = a0 + (c >> 3) * (kTile * 128);
+        *reinterpret_cast<uint4*>(region + umma::sw128_offset(r, c & 7)) =
+            make_uint4(w[4 * c], w[4 * c + 1], w[4 * c + 2], w[4 * c + 3]);
+    }
+}
+
+// Store 64 values of row r (ReLU'd by the caller) as FP16 or BF16.
+template <bool BF16>
+__device__ __forceinline__ void store_row64(uint8_t* a, int r, const float (&v)[64]) {
+#pragma unroll
+    for (int c = 0; c < 8; ++c) {
+        uint32_t q[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            q[e] = BF16 ? pack_bf2(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]) : pack_h2(v[8 * c + 2 * e], v[8 * c + 2 * e + 1]);
+        *reinterpret_cast<uint4*>(a + umma::sw128_offset(r, c)) = make_uint4(q[0], q[1], q[2], q[3]);
+    }
+}
+
+__device__ __forceinline__ void tmem_row64(uint32_t tmem, int warp, int col0, float (&v)[64]) {
+    float a[32], b[32];
+    const uint32_t base = tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)col0;
+    umma::tmem_ld32(base, a);
+    umma::tmem_ld32(base + 32, b);
+#pragma unroll
+    for (int i = 0; i < 32; ++i) { v[i] = a[i]; v[32 + i] = b[i]; }
+}
+
+// Issue the MMAs of one layer: D[128 x N] = A[128 x K] * W^T, K in 16-steps.
+__device__ __forceinline__ void issue_layer(uint32_t d_tmem, const uint8_t* a, int a_region_bytes, const uint8_t* w,
+                                            int w_region_bytes, int K, int N, bool bf16) {
+    const uint32_t id = umma::idesc_f16(kTile, N, bf16);
+    const int steps = K / 16;
+    for (int s = 0; s < steps; ++s) {
+        const int reg = s >> 2, kk = s & 3;
+        const uint64_t ad = umma::sdesc_sw128(umma::smem_u32(a + reg * a_region_bytes + kk * 32));
+        const uint64_t bd = umma::sdesc_sw128(umma::smem_u32(w + reg * w_region_bytes + kk * 32));
+        umma::mma_f16(d_tmem, ad, bd, id, s > 0);
+    }
+}
+
+// Scrub a prediction as guardarSalidaInferencia (NrcKernel.cu:99-126).
+__device__ __forceinline__ float scrub(float c) {
+    if (c < 0.0f) c = 0.0f;
+    if (isnan(c)) c = 0.0f;
+    if (c > 100000.0f) c = 100000.0f;
+    if (isinf(c)) c = 100000.0f;
+    return c;
+}
+
+__device__ __forceinline__ bool all_ok(bool ok) { return __syncthreads_and(ok ? 1 : 0) != 0; }
+
+// ------------------------------------------------------------------ inference
+// Shared memory: weights 51200 | input tile 14336 | A 32768 (two regions).
+constexpr int kInferSmemW = 0;
+constexpr int kInferSmemX = 51200;
+constexpr int kInferSmemA = 51200 + 14336 + 1024;   // 1024-aligned: 66560
+constexpr int kInferSmem = kInferSmemA + 2 * kTile * 128;   // 99328
+
+__global__ void __launch_bounds__(128) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n, Bounds bounds,
+                                               const uint8_t* __restrict__ wimg, TfgColor* __restrict__ out,
+                                               TfgColor* __restrict__ img, const TfgColor* __restrict__ thr) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sw = smem + kInferSmemW;
+    uint8_t* sx = smem + kInferSmemX;
+    uint8_t* sa = smem + kInferSmemA;
+    __shared__ uint64_t mb_w, mb_x, mb_mma;
+    __shared__ uint32_t tslot;
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    if (blockIdx.x >= ntiles) return;
+    if (warp == 0) umma::tmem_alloc(&tslot, 128);
+    if (t == 0) {
+        umma::mbar_init(&mb_w, 1);
+        umma::mbar_init(&mb_x, 1);
+        umma::mbar_init(&mb_mma, 1);
+        umma::mbar_fence_init();
+    }
+    // Region 1 chunks 4..7 (features 96..127) are never written: zero them once.
+    for (int i = t; i < kTile * 4; i += blockDim.x) {
+        const int r = i >> 2, c = 4 + (i & 3);
+        *reinterpret_cast<uint4*>(sa + kTile * 128 + umma::sw128_offset(r, c)) = make_uint4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tslot;
+    if (t == 0) {
+        umma::mbar_expect_tx(&mb_w, kFwdBytes);
+        umma::bulk_g2s(sw, wimg, kFwdBytes, &mb_w);
+        const uint32_t tile = blockIdx.x;
+        const uint32_t rows = min((uint32_t)kTile, n - tile * kTile);
+        umma::mbar_expect_tx(&mb_x, rows * (uint32_t)sizeof(TfgDatosMLP));
+        umma::bulk_g2s(sx, in + (size_t)tile * kTile, rows * (uint32_t)sizeof(TfgDatosMLP), &mb_x);
+    }
+    bool ok = umma::mbar_wait(&mb_w, 0, kSpinLimit);
+    uint32_t xph = 0, mph = 0;
+    for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const uint32_t row = tile * kTile + (uint32_t)t;
+        const bool valid = row < n;
+        ok = all_ok(umma::mbar_wait(&mb_x, xph, kSpinLimit));
+        xph ^= 1u;
+        if (!ok) break;
+        {
+            uint32_t w[48];
+            TfgDatosMLP d;
+            if (valid) d = reinterpret_cast<const TfgDatosMLP*>(sx)[t];
+            else memset(&d, 0, sizeof(d));
+            encode(d, bounds, w);
+            store_encoded(sa, t, w);
+        }
+        umma::fence_smem_to_async();
+        __syncthreads();
+        if (t == 0) {
+            const uint32_t next = tile + gridDim.x;
+            if (next < ntiles) {
+                // The input tile is consumed; prefetch the next one during the GEMM chain.
+                const uint32_t rows = min((uint32_t)kTile, n - next * kTile);
+                umma::mbar_expect_tx(&mb_x, rows * (uint32_t)sizeof(TfgDatosMLP));
+                umma::bulk_g2s(sx, in + (size_t)next * kTile, rows * (uint32_t)sizeof(TfgDatosMLP), &mb_x);
+            }
+        }
+        for (int l = 0; l < kLayers && ok; ++l) {
+            const int K = kCols(l), N = (l == kLayers - 1) ? kOutPad : kHid;
+            const uint32_t dcol = (l == kLayers - 1) ? 64u : 0u;
+            if (t == 0) {
+                umma::fence_after_sync();
+                issue_layer(tmem + dcol, sa, kTile * 128, sw + kFOff(l), kRows(l) * 128, K, N, false);
+                umma::mma_commit(&mb_mma);
+            }
+            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+            mph ^= 1u;
+            if (!ok) break;
+            umma::fence_after_sync();
+            if (l < kLayers - 1) {
+                float v[64];
+                tmem_row64(tmem, warp, 0, v);
+#pragma unroll
+                for (int i = 0; i < 64; ++i) v[i] = fmaxf(v[i], 0.0f);
+                store_row64<false>(sa, t, v);
+                umma::fence_before_sync();
+                umma::fence_smem_to_async();
+                __syncthreads();
+            } else {
+                float v[16];
+                umma::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + 64u, v);
+                umma::fence_before_sync();
+                if (valid) {
+                    const float r = scrub(v[0]), g = scrub(v[1]), b = scrub(v[2]);
+                    if (img) {
+                        const TfgColor th = thr[row];
+                        if (th.r > 0 || th.g > 0 || th.b > 0) {
+                            TfgColor f = img[row];
+                            f.r = f.r + th.r * r;
+                            f.g = f.g + th.g * g;
+                            f.b = f.b + th.b * b;
+                            img[row] = f;
+                        }
+                    } else {
+                        out[row] = TfgColor{r, g, b};
+                    }
+                }
+                __syncthreads();
+            }
+        }
+    }
+    if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+// ------------------------------------------------------------------ training forward + backward
+// Shared memory: fwd weights 51200 | bwd weights 40960 | A 32768.
+constexpr int kTrainSmemF = 0;
+constexpr int kTrainSmemB = 51200 + 1024;            // 52224, 1024-aligned
+constexpr int kTrainSmemA = kTrainSmemB + 40960;      // 93184
+constexpr int kTrainSmem = kTrainSmemA + 2 * kTile * 128;   // 125952
+
+struct TrainArgs {
+    const TfgDatosMLP* buf;      // training records (targets in .color)
+    uint32_t n_avail;            // records available
+    uint32_t batch;              // samples in this step (multiple of kTile)
+    uint32_t seed;               // index stream seed (ColorMLP step counter)
+    Bounds bounds;
+    const uint8_t* fwd;          // FP16 forward image
+    const uint8_t* bwd;          // BF16 backward image
+    uint8_t* hT[kLayers];        // transposed inputs of each layer, per tile
+    uint8_t* zT[kLayers];        // transposed output gradients of each layer, per tile
+    float* loss;                 // sum of per-sample losses (unnormalised)
+};
+
+// Write 64 (or 16) values of sample s into the transposed BF16 tile layout.
+template <int F>
+__device__ __forceinline__ void store_T(uint8_t* tile, int s, const float* v) {
+    uint8_t* region = tile + (s >> 6) * (F * 128);
+    const int c = (s & 63) >> 3, e = s & 7;
+#pragma unroll
+    for (int f = 0; f < F; ++f) {
+        __nv_bfloat16 h = __float2bfloat16_rn(v[f]);
+        *reinterpret_cast<__nv_bfloat16*>(region + umma::sw128_offset(f, c) + 2 * e) = h;
+    }
+}
+
+__global__ void __launch_bounds__(128) k_train(TrainArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sf = smem + kTrainSmemF;
+    uint8_t* sb = smem + kTrainSmemB;
+    uint8_t* sa = smem + kTrainSmemA;
+    __shared__ uint64_t mb_w, mb_mma;
+    __shared__ uint32_t tslot;
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t ntiles = a.batch / kTile;
+    if (blockIdx.x >= ntiles) return;
+    if (warp == 0) umma::tmem_alloc(&tslot, 128);
+    if (t == 0) {
+        umma::mbar_init(&mb_w, 1);
+        umma::mbar_init(&mb_mma, 1);
+        umma::mbar_fence_init();
+    }
+    for (int i = t; i < kTile * 4; i += blockDim.x) {
+        const int r = i >> 2, c = 4 + (i & 3);
+        *reinterpret_cast<uint4*>(sa + kTile * 128 + umma::sw128_offset(r, c)) = make_uint4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tslot;
+    if (t == 0) {
+        umma::mbar_expect_tx(&mb_w, kFwdBytes + kBwdBytes);
+        umma::bulk_g2s(sf, a.fwd, kFwdBytes, &mb_w);
+        umma::bulk_g2s(sb, a.bwd, kBwdBytes, &mb_w);
+    }
+    bool ok = umma::mbar_wait(&mb_w, 0, kSpinLimit);
+    uint32_t mph = 0;
+    float lsum = 0.0f;
+    for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const uint32_t s = tile * kTile + (uint32_t)t;
+        // Sample selection as generarIndicesAleatorios (NrcKernel.cu:10-16).
+        uint32_t st = a.seed ^ s;
+        const uint32_t idx = pcg_next(st) % a.n_avail;
+        const TfgDatosMLP d = a.buf[idx];
+        float tgt[3] = {d.color.r, d.color.g, d.color.b};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) if (tgt[k] > 100000.0f) tgt[k] = 100000.0f;   // NrcKernel.cu:52-57
+        {
+            uint32_t w[48];
+            encode(d, a.bounds, w);
+            store_encoded(sa, t, w);
+            // transposed copy of the layer-0 input for dW0
+            float f[96];
+#pragma unroll
+            for (int k = 0; k < 48; ++k) {
+                __half2 h = *reinterpret_cast<__half2*>(&w[k]);
+                const float2 ff = __half22float2(h);
+                f[2 * k] = ff.x; f[2 * k + 1] = ff.y;
+            }
+            store_T<96>(a.hT[0] + (size_t)tile * (2 * 96 * 128), t, f);
+        }
+        umma::fence_smem_to_async();
+        __syncthreads();
+        uint32_t mask[kLayers - 1][2];
+        // forward
+        for (int l = 0; l < kLayers && ok; ++l) {
+            const int K = kCols(l), N = (l == kLayers - 1) ? kOutPad : kHid;
+            const uint32_t dcol = (l == kLayers - 1) ? 64u : 0u;
+            if (t == 0) {
+                umma::fence_after_sync();
+                issue_layer(tmem + dcol, sa, kTile * 128, sf + kFOff(l), kRows(l) * 128, K, N, false);
+                umma::mma_commit(&mb_mma);
+            }
+            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+            mph ^= 1u;
+            if (!ok) break;
+            umma::fence_after_sync();
+            if (l < kLayers - 1) {
+                float v[64];
+                tmem_row64(tmem, warp, 0, v);
+                uint32_t m0 = 0, m1 = 0;
+#pragma unroll
+                for (int i = 0; i < 64; ++i) {
+                    const bool on = v[i] > 0.0f;
+                    v[i] = on ? v[i] : 0.0f;
+                    if (i < 32) m0 |= (on ? 1u : 0u) << i;
+                    else m1 |= (on ? 1u : 0u) << (i - 32);
+                }
+                mask[l][0] = m0; mask[l][1] = m1;
+                store_row64<false>(sa, t, v);
+                store_T<64>(a.hT[l + 1] + (size_t)tile * (2 * 64 * 128), t, v);
+            } else {
+                float v[16];
+                umma::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + 64u, v);
+                // Relative L2 on luminance: the denominator is held constant.
+                const float lum = 0.299f * v[0] + 0.587f * v[1] + 0.114f * v[2];
+                const float den = lum * lum + 0.01f;
+                float g[64];
+#pragma unroll
+                for (int k = 0; k < 64; ++k) g[k] = 0.0f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float diff = v[k] - tgt[k];
+                    lsum += diff * diff / den;
+                    g[k] = 2.0f * diff / den;
+                }
+                store_row64<true>(sa, t, g);
+                store_T<16>(a.zT[kLayers - 1] + (size_t)tile * (2 * 16 * 128), t, g);
+            }
+            umma::fence_before_sync();
+            umma::fence_smem_to_async();
+            __syncthreads();
+        }
+        // backward: dH_{l-1} = dZ_l * W_l, masked by the ReLU of layer l-1
+        for (int l = kLayers - 1; l >= 1 && ok; --l) {
+            const int K = (l == kLayers - 1) ? kOutPad : kHid;
+            if (t == 0) {
+                umma::fence_after_sync();
+                issue_layer(tmem, sa, kTile * 128, sb + kBOff(l), 64 * 128, K, kHid, true);
+                umma::mma_commit(&mb_mma);
+            }
+            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+            mph ^= 1u;
+            if (!ok) break;
+            umma::fence_after_sync();
+            float v[64];
+            tmem_row64(tmem, warp, 0, v);
+#pragma unroll
+            for (int i = 0; i < 64; ++i) {
+                const uint32_t bit = (i < 32) ? (mask[l - 1][0] >> i) & 1u : (mask[l - 1][1] >> (i - 32)) & 1u;
+                v[i] = bit ? v[i] : 0.0f;
+            }
+            if (l > 1) store_row64<true>(sa, t, v);
+            store_T<64>(a.zT[l - 1] + (size_t)tile * (2 * 64 * 128), t, v);
+            umma::fence_before_sync();
+            umma::fence_smem_to_async();
+            __syncthreads();
+        }
+    }
+    // loss reduction
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xFFFFFFFFu, lsum, o);
+    if ((t & 31) == 0) atomicAdd(a.loss, lsum);
+    if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+// ------------------------------------------------------------------ weight gradients
+// dW_l[out][in] = sum_s dZ_l[s][out] * H_l[s][in].  A = dZ^T (out rows padded
+// to 128 with zeros), B = H^T (in rows), K = samples.  One CTA reduces
+// `tiles_per_cta` sample tiles of one layer into TMEM, then adds its partial
+// sums to the FP32 gradient with atomics.
+constexpr int kWgSmemA = 0;                          // 2 stages x 2 regions x 16 KB
+constexpr int kWgSmemB = 65536;                      // 2 stages x 2 x 96 x 128
+constexpr int kWgSmem = kWgSmemB + 2 * 2 * 96 * 128; // 114688
+
+struct WgradArgs {
+    const uint8_t* zT[kLayers];
+    const uint8_t* hT[kLayers];
+    float* grad;
+    uint32_t ntiles;
+    uint32_t tiles_per_cta;
+};
+
+__global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    __shared__ uint64_t mb_ld[2], mb_mma[2], mb_done;
+    __shared__ uint32_t tslot;
+    const int t = threadIdx.x, warp = t >> 5;
+    const int l = blockIdx.y;
+    const int FZ = kZTFeat(l), FH = kHTFeat(l);
+    const uint32_t t0 = blockIdx.x * a.tiles_per_cta;
+    if (t0 >= a.ntiles) return;
+    const uint32_t t1 = min(a.ntiles, t0 + a.tiles_per_cta);
+    if (warp == 0) umma::tmem_alloc(&tslot, 128);
+    if (t == 0) {
+        for (int k = 0; k < 2; ++k) { umma::mbar_init(&mb_ld[k], 1); umma::mbar_init(&mb_mma[k], 1); }
+        umma::mbar_init(&mb_done, 1);
+        umma::mbar_fence_init();
+    }
+    // Zero both A stages: rows >= FZ stay zero (padding of M to 128).
+    for (int i = t; i < 65536 / 16; i += blockDim.x) reinterpret_cast<uint4*>(smem + kWgSmemA)[i] = make_uint4(0, 0, 0, 0);
+    umma::fence_smem_to_async();
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t zbytes = (uint32_t)FZ * 128, hbytes = 2u * FH * 128;
+    auto load = [&](uint32_t tile, int stage) {
+        uint8_t* sA = smem + kWgSmemA + stage * 32768;
+        uint8_t* sB = smem + kWgSmemB + stage * (2 * 96 * 128);
+        const uint8_t* gz = a.zT[l] + (size_t)tile * 2 * zbytes;
+        const uint8_t* gh = a.hT[l] + (size_t)tile * hbytes;
+        umma::mbar_expect_tx(&mb_ld[stage], 2 * zbytes + hbytes);
+        umma::bulk_g2s(sA, gz, zbytes, &mb_ld[stage]);
+        umma::bulk_g2s(sA + 16384, gz + zbytes, zbytes, &mb_ld[stage]);
+        umma::bulk_g2s(sB, gh, hbytes, &mb_ld[stage]);
+    };
+    bool ok = true;
+    uint32_t ldph[2] = {0, 0}, mmph[2] = {0, 0};
+    if (t == 0) {
+        load(t0, 0);
+        if (t0 + 1 < t1) load(t0 + 1, 1);
+        const uint32_t id = umma::idesc_f16(kTile, FH, true);
+        for (uint32_t tile = t0; tile < t1 && ok; ++tile) {
+            const int stage = (int)((tile - t0) & 1u);
+            ok = umma::mbar_wait(&mb_ld[stage], ldph[stage], kSpinLimit);
+            ldph[stage] ^= 1u;
+            if (!ok) break;
+            umma::fence_after_sync();
+            const uint8_t* sA = smem + kWgSmemA + stage * 32768;
+            const uint8_t* sB = smem + kWgSmemB + stage * (2 * 96 * 128);
+            for (int s = 0; s < 8; ++s) {
+                const int reg = s >> 2, kk = s & 3;
+                const uint64_t ad = umma::sdesc_sw128(umma::smem_u32(sA + reg * 16384 + kk * 32));
+                const uint64_t bd = umma::sdesc_sw128(umma::smem_u32(sB + reg * (FH * 128) + kk * 32));
+                umma::mma_f16(tmem, ad, bd, id, tile > t0 || s > 0);
+            }
+            umma::mma_commit(&mb_mma[stage]);
+            if (tile + 2 < t1) {
+                // Refill this stage once its MMAs have read it.
+                ok = umma::mbar_wait(&mb_mma[stage], mmph[stage], kSpinLimit);
+                mmph[stage] ^= 1u;
+                if (!ok) break;
+                load(tile + 2, stage);
+            }
+        }
+        // One more commit tracks every MMA issued above.
+        if (ok) {
+            umma::mma_commit(&mb_done);
+            ok = umma::mbar_wait(&mb_done, 0, kSpinLimit);
+        }
+    }
+    ok = all_ok(ok);
+    umma::fence_after_sync();
+    if (ok && 32 * warp < FZ) {
+        const int row = 32 * warp + (t & 31);
+        for (int c0 = 0; c0 < FH; c0 += 32) {
+            float v[32];
+            umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
+            if (row < FZ) {
+                float* g = a.grad + kPOff(l) + row * kCols(l) + c0;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) atomicAdd(&g[i], v[i]);
+            }
+        }
+    }
+    if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
+    umma::fence_before_sync();
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+// ------------------------------------------------------------------ Adam + EMA + packing
+struct AdamArgs {
+    float* w;        // FP32 master
+    float* m;
+    float* v;
+    float* ema;      // running EMA (not debiased)
+    float* grad;     // summed gradient; reset to 0 here
+    uint8_t* fwd;    // FP16 forward image of w
+    uint8_t* bwd;    // BF16 W^T image of w
+    uint8_t* inf;    // FP16 image of the debiased EMA
+    float lr, beta1, beta2, eps, decay;
+    float grad_scale;              // 1 / (batch * 3)
+    float bc1, bc2, ema_debias;    // 1 - beta^t, 1 - decay^t
+    int update;                    // 0: only re-pack (after loading parameters)
+};
+
+__device__ __forceinline__ void layer_of(int i, int& l, int& r, int& c) {
+    l = 0;
+    while (i >= kPOff(l + 1)) ++l;
+    const int j = i - kPOff(l);
+    r = j / kCols(l);
+    c = j % kCols(l);
+}
+
+__global__ void k_adam(AdamArgs a) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= kParams) return;
+    int l, r, c;
+    layer_of(i, l, r, c);
+    // Padded entries (output rows 3..15, input columns 85..95 of layer 0) stay zero.
+    const bool live = !(l == kLayers - 1 && r >= 3) && !(l == 0 && c >= 85);
+    float w = a.w[i];
+    float e = a.ema[i];
+    if (a.update && live) {
+        const float g = a.grad[i] * a.grad_scale;
+        const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
+        const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
+        a.m[i] = m;
+        a.v[i] = v;
+        w -= a.lr * (m / a.bc1) / (sqrtf(v / a.bc2) + a.eps);
+        e = a.decay * e + (1.0f - a.decay) * w;
+        a.w[i] = w;
+        a.ema[i] = e;
+    }
+    if (!live) { w = 0.0f; e = 0.0f; }
+    a.grad[i] = 0.0f;
+    const float ew = a.ema_debias > 0.0f ? e / a.ema_debias : w;
+    // forward / inference images: row r, K index c
+    const int rows = kRows(l);
+    const uint32_t off = (uint32_t)kFOff(l) + (uint32_t)(c >> 6) * rows * 128 + umma::sw128_offset(r, (c & 63) >> 3) +
+                         2 * (c & 7);
+    *reinterpret_cast<__half*>(a.fwd + off) = __float2half_rn(w);
+    *reinterpret_cast<__half*>(a.inf + off) = __float2half_rn(ew);
+    if (l >= 1) {
+        // backward image: W^T, row = c (input unit), K index = r (output unit)
+        const uint32_t boff = (uint32_t)kBOff(l) + umma::sw128_offset(c, r >> 3) + 2 * (r & 7);
+        *reinterpret_cast<__nv_bfloat16*>(a.bwd + boff) = __float2bfloat16_rn(w);
+    }
+}
+
+}  // namespace mlp
+
+// ====================================================================== host object
+struct ColorMlp {
+    int dev = 0;
+    uint32_t batch = 16384;
+    uint32_t step = 0;           // ColorMLP::step_counter (mlp.cpp:103)
+    uint32_t adam_t = 0;
+    float lr = 1e-2f, beta1 = 0.9f, beta2 = 0.99f, eps = 1e-15f, decay = 0.99f;
+    mlp::Bounds bounds{{-1, -1, -1}, {1, 1, 1}};
+    float* w = nullptr; float* m = nullptr; float* v = nullptr; float* ema = nullptr; float* grad = nullptr;
+    uint8_t* fwd = nullptr; uint8_t* bwd = nullptr; uint8_t* inf = nullptr;
+    uint8_t* hT[mlp::kLayers] = {nullptr};
+    uint8_t* zT[mlp::kLayers] = {nullptr};
+    float* loss = nullptr;
+    uint32_t act_tiles = 0;
+    int sms = 148;
+};
+
+namespace {
+
+int cuda_fail(cudaError_t e, const char* what) {
+    return fail((int)e, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+uint64_t splitmix(uint64_t& s) {
+    uint64_t z = (s += 0x9E3779B97F4A7C15ull);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t batch_used) {
+    mlp::AdamArgs a;
+    a.w = n->w; a.m = n->m; a.v = n->v; a.ema = n->ema; a.grad = n->grad;
+    a.fwd = n->fwd; a.bwd = n->bwd; a.inf = n->inf;
+    a.lr = n->lr; a.beta1 = n->beta1; a.beta2 = n->beta2; a.eps = n->eps; a.decay = n->decay;
+    a.grad_scale = batch_used ? 1.0f / (3.0f * (float)batch_used) : 0.0f;
+    a.bc1 = 1.0f - std::pow(n->beta1, (float)std::max(1u, n->adam_t));
+    a.bc2 = 1.0f - std::pow(n->beta2, (float)std::max(1u, n->adam_t));
+    a.ema_debias = n->adam_t ? 1.0f - std::pow(n->decay, (float)n->adam_t) : 0.0f;
+    a.update = update ? 1 : 0;
+    mlp::k_adam<<<(mlp::kParams + 255) / 256, 256, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mlp adam");
+    return ok();
+}
+
+int ensure_acts(ColorMlp* n, uint32_t tiles) {
+    if (n->act_tiles >= tiles) return ok();
+    for (int l = 0; l < mlp::kLayers; ++l) {
+        if (n->hT[l]) cudaFree(n->hT[l]);
+        if (n->zT[l]) cudaFree(n->zT[l]);
+        n->hT[l] = n->zT[l] = nullptr;
+    }
+    for (int l = 0; l < mlp::kLayers; ++l) {
+        cudaError_t e = cudaMalloc((void**)&n->hT[l], (size_t)tiles * 2 * mlp::kHTFeat(l) * 128);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&n->zT[l], (size_t)tiles * 2 * mlp::kZTFeat(l) * 128);
+        if (e != cudaSuccess) { n->act_tiles = 0; return cuda_fail(e, "mlp activations"); }
+    }
+    n->act_tiles = tiles;
+    return ok();
+}
+
+int check_error_flag() {
+    int flag = 0;
+    cudaError_t e = cudaMemcpyFromSymbol(&flag, mlp::g_mlp_error, sizeof(int));
+    if (e != cudaSuccess) return cuda_fail(e, "mlp status");
+    if (flag) {
+        int zero = 0;
+        cudaMemcpyToSymbol(mlp::g_mlp_error, &zero, sizeof(int));
+        return fail(TFG_E_TIMEOUT, "mlp kernel: a bounded tensor-core wait gave up");
+    }
+    return ok();
+}
+
+}  // namespace
+}  // namespace tfg
+
+using tfg::ColorMlp;
+namespace M = tfg::mlp;
+
+extern "C" int tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, TfgColorMLP** out) {
+    if (!out) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: out is null");
+    *out = nullptr;
+    if (n_in != 15 || n_out != 3) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: the cache takes 15 inputs and 3 outputs");
+    if (batch == 0 || batch % M::kTile != 0 || batch > (1u << 24))
+        return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: batch must be a positive multiple of 128");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpCreate");
+    if (int rc = tfg::require_sm100(dev)) return rc;
+    ColorMlp* n = new ColorMlp();
+    n->dev = dev;
+    n->batch = batch;
+    cudaDeviceGetAttribute(&n->sms, cudaDevAttrMultiProcessorCount, dev);
+    const size_t pb = M::kParams * sizeof(float);
+    e = cudaMalloc((void**)&n->w, pb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->m, pb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->v, pb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->ema, pb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->grad, pb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->fwd, M::kFwdBytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->bwd, M::kBwdBytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf, M::kFwdBytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->loss, sizeof(float));
+    if (e != cudaSuccess) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return tfg::cuda_fail(e, "tfgMlpCreate"); }
+    cudaMemset(n->fwd, 0, M::kFwdBytes);
+    cudaMemset(n->bwd, 0, M::kBwdBytes);
+    cudaMemset(n->inf, 0, M::kFwdBytes);
+    // Uniform (-s, s) initialisation with s = sqrt(6 / (fan_in + fan_out)) per layer.
+    std::vector<float> h(M::kParams, 0.0f);
+    uint64_t st = seed ? seed : 0x5EEDull;
+    const int fan_in[M::kLayers] = {85, 64, 64, 64, 64, 64};
+    const int fan_out[M::kLayers] = {64, 64, 64, 64, 64, 3};
+    for (int l = 0; l < M::kLayers; ++l) {
+        const float s = std::sqrt(6.0f / (float)(fan_in[l] + fan_out[l]));
+        for (int r = 0; r < M::kRows(l); ++r)
+            for (int c = 0; c < M::kCols(l); ++c) {
+                const bool live = !(l == M::kLayers - 1 && r >= 3) && !(l == 0 && c >= 85);
+                const double u = (double)(tfg::splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
+                h[M::kPOff(l) + r * M::kCols(l) + c] = live ? (float)((2.0 * u - 1.0) * s) : 0.0f;
+            }
+    }
+    e = cudaMemcpy(n->w, h.data(), pb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(n->ema, h.data(), pb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(n->m, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(n->v, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, pb);
+    if (e != cudaSuccess) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return tfg::cuda_fail(e, "tfgMlpCreate"); }
+    if (int rc = tfg::repack(n, 0, false, 0)) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return rc; }
+    static bool attrs = false;
+    if (!attrs) {
+        cudaFuncSetAttribute(M::k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kInferSmem + 1024);
+        cudaFuncSetAttribute(M::k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kTrainSmem + 1024);
+        cudaFuncSetAttribute(M::k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
+        attrs = true;
+    }
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return tfg::cuda_fail(e, "tfgMlpCreate"); }
+    *out = reinterpret_cast<TfgColorMLP*>(n);
+    return tfg::ok();
+}
+
+extern "C" void tfgMlpDestroy(TfgColorMLP* h) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n) return;
+    for (void* p : {(void*)n->w, (void*)n->m, (void*)n->v, (void*)n->ema, (void*)n->grad, (void*)n->fwd, (void*)n->bwd,
+                    (void*)n->inf, (void*)n->loss})
+        if (p) cudaFree(p);
+    for (int l = 0; l < M::kLayers; ++l) {
+        if (n->hT[l]) cudaFree(n->hT[l]);
+        if (n->zT[l]) cudaFree(n->zT[l]);
+    }
+    delete n;
+}
+
+extern "C" int tfgMlpSetBounds(TfgColorMLP* h, const TfgSceneBounds* b) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !b) return tfg::fail(TFG_E_INVALID, "tfgMlpSetBounds: null argument");
+    n->bounds = M::Bounds{{(float)b->min.x, (float)b->min.y, (float)b->min.z}, {(float)b->max.x, (float)b->max.y, (float)b->max.z}};
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpSetHyperparams(TfgColorMLP* h, float lr, float beta1, float beta2, float eps, float ema_decay) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !(lr > 0.0f) || !(beta1 >= 0.0f && beta1 < 1.0f) || !(beta2 >= 0.0f && beta2 < 1.0f) || !(eps >= 0.0f) ||
+        !(ema_decay >= 0.0f && ema_decay < 1.0f))
+        return tfg::fail(TFG_E_INVALID, "tfgMlpSetHyperparams: value out of range");
+    n->lr = lr; n->beta1 = beta1; n->beta2 = beta2; n->eps = eps; n->decay = ema_decay;
+    return tfg::ok();
+}
+
+static int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img, const TfgColor* thr,
+                      uint32_t count, cudaStream_t s) {
+    if (count == 0) return tfg::ok();
+    if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpInference: input buffer must be 16-byte aligned");
+    const uint32_t tiles = (count + M::kTile - 1) / M::kTile;
+    const uint32_t grid = std::min<uint32_t>(tiles, 2u * (uint32_t)n->sms);
+    M::k_infer<<<grid, 128, M::kInferSmem + 1024, s>>>(in, count, n->bounds, n->inf, out, img, thr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpInference");
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpInference(TfgColorMLP* h, const TfgDatosMLP* in, TfgColor* out, uint32_t count, void* stream) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || (count && (!in || !out))) return tfg::fail(TFG_E_INVALID, "tfgMlpInference: null argument");
+    return infer_impl(n, in, out, nullptr, nullptr, count, (cudaStream_t)stream);
+}
+
+extern "C" int tfgMlpInferenceComposite(TfgColorMLP* h, const TfgDatosMLP* in, const TfgColor* throughput,
+                                        TfgColor* img, uint32_t count, void* stream) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || (count && (!in || !throughput || !img)))
+        return tfg::fail(TFG_E_INVALID, "tfgMlpInferenceComposite: null argument");
+    return infer_impl(n, in, nullptr, img, throughput, count, (cudaStream_t)stream);
+}
+
+extern "C" int tfgMlpTrainStep(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32_t n_available, float* loss_out,
+                               void* stream) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !buffer) return tfg::fail(TFG_E_INVALID, "tfgMlpTrainStep: null argument");
+    if (loss_out) *loss_out = 0.0f;
+    if (n_available < 100) return tfg::ok();   // mlp.cpp:96: too few samples, no step
+    cudaStream_t s = (cudaStream_t)stream;
+    const uint32_t tiles = n->batch / M::kTile;
+    if (int rc = tfg::ensure_acts(n, tiles)) return rc;
+    cudaError_t e = cudaMemsetAsync(n->loss, 0, sizeof(float), s);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpTrainStep");
+    M::TrainArgs ta;
+    ta.buf = buffer; ta.n_avail = n_available; ta.batch = n->batch; ta.seed = n->step++;
+    ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
+    for (int l = 0; l < M::kLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
+    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)n->sms);
+    M::k_train<<<grid, 128, M::kTrainSmem + 1024, s>>>(ta);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpTrainStep: forward/backward");
+    M::WgradArgs wa;
+    for (int l = 0; l < M::kLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
+    wa.grad = n->grad;
+    wa.ntiles = tiles;
+    wa.tiles_per_cta = std::max<uint32_t>(2u, (tiles + 15u) / 16u);
+    dim3 g((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, M::kLayers);
+    M::k_wgrad<<<g, 128, M::kWgSmem + 1024, s>>>(wa);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpTrainStep: weight gradients");
+    n->adam_t++;
+    if (int rc = tfg::repack(n, s, true, n->batch)) return rc;
+    if (loss_out) {
+        float l = 0.0f;
+        e = cudaMemcpyAsync(&l, n->loss, sizeof(float), cudaMemcpyDeviceToHost, s);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpTrainStep: loss");
+        *loss_out = l / (3.0f * (float)n->batch);
+        if (int rc = tfg::check_error_flag()) return rc;
+    }
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpGetParams(TfgColorMLP* h, int which, float* host, uint32_t count) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !host || count != (uint32_t)M::kParams) return tfg::fail(TFG_E_INVALID, "tfgMlpGetParams: bad argument");
+    const float* src = which == 0 ? n->w : which == 1 ? n->ema : which == 2 ? n->m : which == 3 ? n->v : nullptr;
+    if (!src) return tfg::fail(TFG_E_INVALID, "tfgMlpGetParams: unknown array");
+    cudaError_t e = cudaMemcpy(host, src, count * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpGetParams");
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !host || count != (uint32_t)M::kParams) return tfg::fail(TFG_E_INVALID, "tfgMlpSetParams: bad argument");
+    const size_t pb = count * sizeof(float);
+    cudaError_t e = cudaMemcpy(n->w, host, pb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(n->ema, host, pb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(n->m, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(n->v, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, pb);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetParams");
+    n->adam_t = 0;
+    if (int rc = tfg::repack(n, 0, false, 0)) return rc;
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetParams");
+    return tfg::ok();
+}
+
+// Gradient of the last step is consumed by Adam; this runs the
+// forward/backward/weight-gradient kernels alone and returns the normalised
+// gradient (d loss / d W) without updating the parameters.
+extern "C" int tfgMlpComputeGradient(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
+                                     float* host_grad, uint32_t count, float* loss_out) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !buffer || !host_grad || count != (uint32_t)M::kParams || n_available == 0)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpComputeGradient: bad argument");
+    const uint32_t tiles = n->batch / M::kTile;
+    if (int rc = tfg::ensure_acts(n, tiles)) return rc;
+    cudaError_t e = cudaMemset(n->loss, 0, sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, M::kParams * sizeof(float));
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
+    M::TrainArgs ta;
+    ta.buf = buffer; ta.n_avail = n_available; ta.batch = n->batch; ta.seed = seed;
+    ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
+    for (int l = 0; l < M::kLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
+    M::k_train<<<std::min<uint32_t>(tiles, (uint32_t)n->sms), 128, M::kTrainSmem + 1024>>>(ta);
+    M::WgradArgs wa;
+    for (int l = 0; l < M::kLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
+    wa.grad = n->grad;
+    wa.ntiles = tiles;
+    wa.tiles_per_cta = std::max<uint32_t>(2u, (tiles + 15u) / 16u);
+    M::k_wgrad<<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, M::kLayers), 128, M::kWgSmem + 1024>>>(wa);
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
+    if (int rc = tfg::check_error_flag()) return rc;
+    std::vector<float> g(M::kParams);
+    e = cudaMemcpy(g.data(), n->grad, M::kParams * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
+    const float sc = 1.0f / (3.0f * (float)n->batch);
+    for (int i = 0; i < M::kParams; ++i) host_grad[i] = g[i] * sc;
+    cudaMemset(n->grad, 0, M::kParams * sizeof(float));
+    if (loss_out) {
+        float l = 0.0f;
+        cudaMemcpy(&l, n->loss, sizeof(float), cudaMemcpyDeviceToHost);
+        *loss_out = l * sc;
+    }
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpStatus(void) {
+    return tfg::check_error_flag();
+}
