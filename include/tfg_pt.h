@@ -345,7 +345,9 @@ int  tfgMlpInferenceComposite(TfgColorMLP* mlp, const TfgDatosMLP* in, const Tfg
 /* FP32 parameter arrays (count = 23552, padded [out][in] per layer):
  * which = 0 weights, 1 EMA, 2 Adam m, 3 Adam v. */
 int  tfgMlpGetParams(TfgColorMLP* mlp, int which, float* host, uint32_t count);
-/* Set weights (and EMA), reset Adam state; re-packs the tensor-core images. */
+/* Set the weights and restart the optimiser (Adam moments and the weight
+ * average cleared, step 0, so inference uses these weights until the next
+ * step); re-packs the tensor-core images. */
 int  tfgMlpSetParams(TfgColorMLP* mlp, const float* host, uint32_t count);
 /* d loss / d W for one batch drawn with `seed`, without updating anything
  * (synchronous; for gradient checks). */
@@ -354,6 +356,56 @@ int  tfgMlpComputeGradient(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t
 /* TFG_E_TIMEOUT if a bounded tensor-core wait in an MLP kernel gave up since
  * the last call (synchronous). */
 int  tfgMlpStatus(void);
+/* Device training state (synchronous): [0] step counter, [1] Adam step,
+ * [2] records used by the last step, [3] cache-query gate (1 = open),
+ * [4] running loss (float bits), [5..7] reserved. */
+int  tfgMlpGetState(TfgColorMLP* mlp, uint32_t* out8);
+
+/* ------------------------------------------------------------------ */
+/* One cache frame (main.cpp:995-1061) without host synchronisation    */
+/* ------------------------------------------------------------------ */
+
+typedef struct TfgNrcFrameConfig {
+    int32_t  train_steps;     /* train_step calls per frame; reference 1 (main.cpp:1056) */
+    uint32_t max_records;     /* records used per frame; reference 65536 (main.cpp:1036) */
+    uint32_t min_records;     /* train only above this count; reference 1024 (main.cpp:1043) */
+    int32_t  warmup;          /* 1: no cache queries, every path is a training path (main.cpp:997) */
+    float    gate_threshold;  /* > 0: answer cache queries only once the running training loss is
+                                 below this value (0: always, as the reference) */
+    int32_t  use_graph;       /* 1: capture the frame as a CUDA graph on first use and replay it
+                                 (needs a non-default stream) */
+} TfgNrcFrameConfig;
+
+/* Reference frame settings: 1 step, 65536 records, train above 1024, no gate, no graph. */
+void tfgNrcFrameConfigReference(TfgNrcFrameConfig* cfg);
+
+/* Caller-owned device buffers of a cache frame (main.cpp:908-930). */
+typedef struct TfgNrcBuffers {
+    TfgColor*                 img;        /* W*H: frame radiance (prefix + cache) */
+    float*                    accum;      /* W*H*3 running sum, or null */
+    TfgDatosMLP*              infer;      /* W*H cache queries */
+    TfgColor*                 thr;        /* W*H throughput at the query vertex */
+    TfgRegistroEntrenamiento* regs;       /* training-record ring */
+    uint32_t*                 counter;    /* ring counter (1 word) */
+    uint32_t                  ring_cap;   /* ring capacity, >= max_records */
+    uint32_t                  reserved;
+    TfgDatosMLP*              tail_in;    /* max_records */
+    TfgColor*                 tail_pred;  /* max_records */
+    TfgDatosMLP*              train_buf;  /* max_records */
+} TfgNrcBuffers;
+
+/* Render one sample per pixel with cache queries and training records, answer
+ * the queries with the cache and composite into buffers->img (accumulating
+ * into buffers->accum if set), then bootstrap targets and take
+ * cfg->train_steps Adam steps -- all enqueued on `stream` with the record
+ * count kept in device memory.  `params` sets depth / roulette / shadows /
+ * triangle test (spp is forced to 1).  `frame` seeds the RNG
+ * (rng.h:25-35). */
+int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const TfgRenderParams* params,
+                const TfgCamara* camara, const TfgPrimitiva* primitivas, int32_t num_primitivas,
+                const TfgLuzPuntual* luces, int32_t num_luces, int32_t ancho_img, int32_t alto_img,
+                const TfgTinyBVHD_GPU* bvh, const float* tris_wt, const TfgPrimitiva* primitivas_bvh,
+                int32_t num_prims_bvh, const TfgNrcBuffers* buffers, int32_t frame, void* stream);
 
 #ifdef __cplusplus
 }

@@ -57,7 +57,8 @@ def test_inference_matches_fp64_model(mlp, n):
     mlp.inference(_dev(d), out, n)
     torch.cuda.synchronize()
     got = out.view(n, 3).cpu().numpy()
-    W = [_f16(w) for w in split_layers(mlp.get_params(EMA))]
+    # before any step inference uses the weights themselves
+    W = [_f16(w) for w in split_layers(mlp.get_params(WEIGHTS))]
     x = mo.encode(mo.rows15(d, LO, HI))
     want = mo.scrub(mo.forward(W, x)[0])
     scale = np.abs(mo.forward(W, x)[0]).mean() + 1e-3
@@ -121,9 +122,18 @@ def test_one_adam_step(built):
     big = np.abs(g) > 1e-6
     np.testing.assert_allclose(np.abs(w1 - w0)[big], 1e-3, rtol=1e-3)
     assert (np.sign(w1 - w0)[big] == -np.sign(g[big])).mean() > 0.999
-    # the EMA moved 1% of the way (decay 0.99), debiased for inference
+    # the weight average starts at zero: after one step it holds (1 - 0.99) w1,
+    # and inference uses it debiased by 1 - 0.99^1, i.e. exactly w1
     e1 = m.get_params(EMA)
-    np.testing.assert_allclose(e1, 0.99 * w0 + 0.01 * w1, rtol=1e-5, atol=1e-7)
+    np.testing.assert_allclose(e1, 0.01 * w1, rtol=1e-5, atol=1e-9)
+    d2 = _datos(np.random.default_rng(5), 300)
+    out = torch.zeros(300 * 3, device="cuda")
+    m.inference(_dev(d2), out, 300)
+    torch.cuda.synchronize()
+    x = mo.encode(mo.rows15(d2, LO, HI))
+    want = mo.scrub(mo.forward([_f16(w) for w in split_layers(w1)], x)[0])
+    scale = np.abs(want).mean() + 1e-3
+    assert np.abs(out.view(300, 3).cpu().numpy() - want).max() / scale < 0.05
     m.close()
 
 

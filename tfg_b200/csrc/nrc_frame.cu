@@ -1,0 +1,193 @@
+// One radiance-cache frame on the GPU: the reference's per-frame host loop
+// (main.cpp:995-1061) with every host synchronisation removed.
+//
+//   render (1 spp, cache queries + training records)      main.cpp:1016
+//   cache inference fused with the composite              main.cpp:1028-1029
+//   record count, capped and rounded to 4, in device memory main.cpp:1033-1039
+//   tail queries -> tail inference -> targets             main.cpp:1046-1052
+//   `train_steps` Adam steps on the targets               main.cpp:1056
+//
+// Counts and the step / Adam counters never leave the device, so the whole
+// frame can be captured once as a CUDA graph and replayed; only the frame
+// number (RNG seed) is written before each launch.
+#include <cuda_runtime.h>
+
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "../../include/tfg_pt.h"
+#include "tfg_errors.h"
+#include "tfg_runtime.h"
+
+namespace tfg {
+namespace {
+
+__global__ void k_set_frame(int32_t* frame_dev, int32_t frame) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) *frame_dev = frame;
+}
+
+struct FrameKey {
+    const void* ptrs[20];
+    int32_t ints[16];
+    float gate;
+    bool operator==(const FrameKey& o) const { return std::memcmp(this, &o, sizeof(FrameKey)) == 0; }
+};
+
+struct FrameGraph {
+    FrameKey key;
+    bool valid = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+std::mutex g_frame_mutex;
+int32_t* g_frame_dev[16] = {nullptr};
+FrameGraph g_graph[16];
+
+struct FrameCall {
+    ColorMlp* mlp;
+    TfgNrcFrameConfig cfg;
+    TfgRenderParams prm;
+    const TfgCamara* cam; const TfgPrimitiva* prims; int nprims;
+    const TfgLuzPuntual* lights; int nlights;
+    int W, H;
+    const TfgTinyBVHD_GPU* bvh; const float* tris_wt; const TfgPrimitiva* mesh; int nmesh;
+    TfgNrcBuffers b;
+    int32_t* frame_dev;
+};
+
+int enqueue_frame(const FrameCall& c, bool prepare_only, cudaStream_t s) {
+    const uint32_t npx = (uint32_t)c.W * (uint32_t)c.H;
+    const uint32_t min_n = std::max(c.cfg.min_records + 1u, 100u);
+    uint32_t* navail = mlp_navail(c.mlp);
+    const uint32_t* gate = c.cfg.gate_threshold > 0.0f ? mlp_gate(c.mlp) : nullptr;
+    if (prepare_only) {
+        if (int rc = mlp_prepare(c.mlp)) return rc;
+    } else {
+        cudaError_t e = cudaMemsetAsync(c.b.counter, 0, sizeof(uint32_t), s);
+        if (e != cudaSuccess) return fail((int)e, std::string("nrc frame: ") + cudaGetErrorString(e));
+    }
+    if (int rc = render_pass_ex(c.prm, c.cam, c.prims, c.nprims, c.lights, c.nlights, c.W, c.H, 0, c.frame_dev, gate,
+                                c.bvh, c.tris_wt, c.mesh, c.nmesh, c.b.img, nullptr, c.b.regs, c.b.counter,
+                                (int)c.b.ring_cap, c.b.infer, c.b.thr, c.cfg.warmup ? 0 : 1, 1, prepare_only, s))
+        return rc;
+    if (prepare_only) return ok();
+    if (int rc = mlp_enqueue_infer(c.mlp, c.b.infer, nullptr, c.b.img, c.b.thr, npx, nullptr, s)) return rc;
+    if (c.b.accum)
+        if (int rc = launch_nrc_frame_small(3, c.b.img, c.b.accum, nullptr, nullptr, npx, 0, s)) return rc;
+    if (int rc = launch_nrc_frame_small(2, c.b.counter, navail, nullptr, nullptr, c.cfg.max_records, 0, s)) return rc;
+    if (int rc = launch_nrc_frame_small(0, c.b.regs, c.b.tail_in, nullptr, navail, c.cfg.max_records, min_n, s))
+        return rc;
+    if (int rc = mlp_enqueue_infer(c.mlp, c.b.tail_in, c.b.tail_pred, nullptr, nullptr, c.cfg.max_records, navail, s))
+        return rc;
+    if (int rc = launch_nrc_frame_small(1, c.b.regs, c.b.train_buf, c.b.tail_pred, navail, c.cfg.max_records, min_n, s))
+        return rc;
+    for (int k = 0; k < c.cfg.train_steps; ++k)
+        if (int rc = mlp_enqueue_train(c.mlp, c.b.train_buf, min_n, s)) return rc;
+    return ok();
+}
+
+FrameKey key_of(const FrameCall& c) {
+    FrameKey k;
+    std::memset(&k, 0, sizeof(k));
+    const void* p[] = {c.mlp, c.cam, c.prims, c.lights, c.bvh ? c.bvh->d_nodos : nullptr,
+                       c.bvh ? c.bvh->d_tris : nullptr, c.tris_wt, c.mesh, c.b.img, c.b.accum, c.b.infer, c.b.thr,
+                       c.b.regs, c.b.counter, c.b.tail_in, c.b.tail_pred, c.b.train_buf, c.frame_dev};
+    std::memcpy(k.ptrs, p, sizeof(p));
+    const int32_t v[] = {c.nprims, c.nlights, c.W, c.H, c.nmesh, (int32_t)c.b.ring_cap, c.cfg.train_steps,
+                         (int32_t)c.cfg.max_records, (int32_t)c.cfg.min_records, c.cfg.warmup, c.prm.max_depth,
+                         c.prm.rr_min_depth, c.prm.shadow_mesh, c.prm.tri_format};
+    std::memcpy(k.ints, v, sizeof(v));
+    k.gate = c.cfg.gate_threshold;
+    return k;
+}
+
+}  // namespace
+}  // namespace tfg
+
+extern "C" void tfgNrcFrameConfigReference(TfgNrcFrameConfig* c) {
+    if (!c) return;
+    c->train_steps = 1;
+    c->max_records = 65536;
+    c->min_records = 1024;
+    c->warmup = 0;
+    c->gate_threshold = 0.0f;
+    c->use_graph = 0;
+}
+
+extern "C" int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const TfgRenderParams* params,
+                           const TfgCamara* camara, const TfgPrimitiva* primitivas, int32_t num_primitivas,
+                           const TfgLuzPuntual* luces, int32_t num_luces, int32_t W, int32_t H,
+                           const TfgTinyBVHD_GPU* bvh, const float* tris_wt, const TfgPrimitiva* primitivas_bvh,
+                           int32_t num_prims_bvh, const TfgNrcBuffers* buffers, int32_t frame, void* stream) {
+    using namespace tfg;
+    if (!mlp || !cfg || !params || !buffers) return fail(TFG_E_INVALID, "tfgNrcFrame: null argument");
+    const TfgNrcBuffers& b = *buffers;
+    if (!b.img || !b.infer || !b.thr || !b.regs || !b.counter || !b.tail_in || !b.tail_pred || !b.train_buf)
+        return fail(TFG_E_INVALID, "tfgNrcFrame: a required buffer is null");
+    if (cfg->train_steps < 0 || cfg->max_records == 0 || b.ring_cap < cfg->max_records)
+        return fail(TFG_E_INVALID, "tfgNrcFrame: ring capacity below max_records");
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    if (int rc = require_sm100(dev)) return rc;
+    std::lock_guard<std::mutex> lk(g_frame_mutex);
+    if (!g_frame_dev[dev & 15]) {
+        e = cudaMalloc((void**)&g_frame_dev[dev & 15], sizeof(int32_t));
+        if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame: ") + cudaGetErrorString(e));
+    }
+    FrameCall c;
+    c.mlp = reinterpret_cast<ColorMlp*>(mlp);
+    c.cfg = *cfg;
+    c.prm = *params;
+    c.prm.spp = 1;
+    c.prm.accumulate = 0;
+    c.prm.profile = 0;
+    c.cam = camara; c.prims = primitivas; c.nprims = num_primitivas; c.lights = luces; c.nlights = num_luces;
+    c.W = W; c.H = H; c.bvh = bvh; c.tris_wt = tris_wt; c.mesh = primitivas_bvh; c.nmesh = num_prims_bvh;
+    c.b = b;
+    c.frame_dev = g_frame_dev[dev & 15];
+    mlp_set_gate_threshold(c.mlp, cfg->gate_threshold);
+    k_set_frame<<<1, 32, 0, s>>>(c.frame_dev, frame);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame: ") + cudaGetErrorString(e));
+    const bool graph = cfg->use_graph && s != nullptr;
+    if (!graph) {
+        if (int rc = enqueue_frame(c, true, s)) return rc;
+        return enqueue_frame(c, false, s);
+    }
+    FrameGraph& g = g_graph[dev & 15];
+    const FrameKey key = key_of(c);
+    if (!g.valid || !(g.key == key)) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+        g.exec = nullptr; g.graph = nullptr; g.valid = false;
+        if (int rc = enqueue_frame(c, true, s)) return rc;
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame capture: ") + cudaGetErrorString(e));
+        const int rc = enqueue_frame(c, false, s);
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(s, &gr);
+        if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+        if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&g.exec, gr, 0);
+        if (e != cudaSuccess) { cudaGraphDestroy(gr); return fail((int)e, std::string("tfgNrcFrame instantiate: ") + cudaGetErrorString(e)); }
+        g.graph = gr;
+        g.key = key;
+        g.valid = true;
+    }
+    e = cudaGraphLaunch(g.exec, s);
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame launch: ") + cudaGetErrorString(e));
+    return ok();
+}
+
+extern "C" int tfgMlpGetState(TfgColorMLP* mlp, uint32_t* out8) {
+    using namespace tfg;
+    if (!mlp || !out8) return fail(TFG_E_INVALID, "tfgMlpGetState: null argument");
+    cudaError_t e = cudaMemcpy(out8, mlp_state(reinterpret_cast<ColorMlp*>(mlp)), 8 * sizeof(uint32_t),
+                               cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgMlpGetState: ") + cudaGetErrorString(e));
+    return ok();
+}

@@ -159,6 +159,67 @@ __global__ void k_default_camera(TfgCamara* c, int W, int H) {
     *c = r;
 }
 
+// Device-count forms for the frame driver: the record count lives in device
+// memory (no host read between render and training).
+__global__ void k_tail_dev(const TfgRegistroEntrenamiento* __restrict__ regs, TfgDatosMLP* __restrict__ out,
+                           const uint32_t* n_dev, uint32_t min_n) {
+    const uint32_t n = *n_dev;
+    if (n < min_n) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const TfgRegistroEntrenamiento& r = regs[i];
+        TfgDatosMLP d;
+        memset(&d, 0, sizeof(d));
+        if (r.valido) {
+            d.posicion = r.tail.posicion; d.direccion = r.tail.direccion; d.normal = r.tail.normal;
+            d.difuso = r.tail.difuso; d.especular = r.tail.especular;
+        }
+        out[i] = d;
+    }
+}
+
+__global__ void k_targets_dev(const TfgRegistroEntrenamiento* regs, const TfgColor* tail, TfgDatosMLP* out,
+                              const uint32_t* n_dev, uint32_t min_n) {
+    const uint32_t n = *n_dev;
+    if (n < min_n) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const TfgRegistroEntrenamiento r = regs[i];
+        if (!r.valido) { out[i].color = TfgColor{0.0f, 0.0f, 0.0f}; continue; }
+        const TfgColor tl = tail[i];
+        const float rr = r.luz_acumulada_sufijo.r + r.throughput_sufijo.r * tl.r;
+        const float rg = r.luz_acumulada_sufijo.g + r.throughput_sufijo.g * tl.g;
+        const float rb = r.luz_acumulada_sufijo.b + r.throughput_sufijo.b * tl.b;
+        float c[3] = {rr / fmaxf(r.factor_normalizacion.r, 1e-8f), rg / fmaxf(r.factor_normalizacion.g, 1e-8f),
+                      rb / fmaxf(r.factor_normalizacion.b, 1e-8f)};
+        for (int k = 0; k < 3; ++k) {
+            c[k] = fminf(c[k], 100000.0f);
+            if (isnan(c[k]) || isinf(c[k])) c[k] = 0.0f;
+        }
+        TfgDatosMLP d;
+        d.posicion = r.head.posicion; d.direccion = r.head.direccion; d.normal = r.head.normal;
+        d.difuso = r.head.difuso; d.especular = r.head.especular;
+        d.color = TfgColor{c[0], c[1], c[2]};
+        out[i] = d;
+    }
+}
+
+// main.cpp:1033-1039: records appended this frame, capped and rounded down
+// to a multiple of 4.
+__global__ void k_record_count(const uint32_t* counter, uint32_t* n_out, uint32_t cap) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        uint32_t n = min(*counter, cap);
+        *n_out = (n / 4u) * 4u;
+    }
+}
+
+__global__ void k_accumulate(float* __restrict__ accum, const TfgColor* __restrict__ img, uint32_t n) {
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const TfgColor c = img[i];
+        accum[3 * (size_t)i] += c.r;
+        accum[3 * (size_t)i + 1] += c.g;
+        accum[3 * (size_t)i + 2] += c.b;
+    }
+}
+
 int launch_check(const char* what) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return fail((int)e, std::string(what) + ": " + cudaGetErrorString(e));
@@ -175,6 +236,31 @@ int device_ok() {
 inline int blocks_for(long n) { return (int)std::max(1L, (n + 255) / 256); }
 
 }  // namespace
+
+int launch_nrc_frame_small(int which, const void* a, void* b, const void* c, const uint32_t* n_dev, uint32_t cap,
+                           uint32_t min_n, cudaStream_t s) {
+    const int blocks = std::max(1, std::min((int)((cap + 255) / 256), 148 * 4));
+    switch (which) {
+        case 0:
+            k_tail_dev<<<blocks, 256, 0, s>>>(static_cast<const TfgRegistroEntrenamiento*>(a),
+                                              static_cast<TfgDatosMLP*>(b), n_dev, min_n);
+            return launch_check("nrc tail queries");
+        case 1:
+            k_targets_dev<<<blocks, 256, 0, s>>>(static_cast<const TfgRegistroEntrenamiento*>(a),
+                                                 static_cast<const TfgColor*>(c), static_cast<TfgDatosMLP*>(b), n_dev,
+                                                 min_n);
+            return launch_check("nrc targets");
+        case 2:
+            k_record_count<<<1, 32, 0, s>>>(static_cast<const uint32_t*>(a), static_cast<uint32_t*>(b), cap);
+            return launch_check("nrc record count");
+        case 3:
+            k_accumulate<<<blocks, 256, 0, s>>>(static_cast<float*>(b), static_cast<const TfgColor*>(a), cap);
+            return launch_check("accumulate");
+        default:
+            return fail(TFG_E_INVALID, "unknown frame kernel");
+    }
+}
+
 }  // namespace tfg
 
 using namespace tfg;

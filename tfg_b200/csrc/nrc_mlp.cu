@@ -189,7 +189,8 @@ constexpr int kInferSmemX = 51200;
 constexpr int kInferSmemA = 51200 + 14336 + 1024;   // 1024-aligned: 66560
 constexpr int kInferSmem = kInferSmemA + 2 * kTile * 128;   // 99328
 
-__global__ void __launch_bounds__(128) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n, Bounds bounds,
+__global__ void __launch_bounds__(128) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
+                                               const uint32_t* __restrict__ n_dev, Bounds bounds,
                                                const uint8_t* __restrict__ wimg, TfgColor* __restrict__ out,
                                                TfgColor* __restrict__ img, const TfgColor* __restrict__ thr) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -200,6 +201,7 @@ __global__ void __launch_bounds__(128) k_infer(const TfgDatosMLP* __restrict__ i
     __shared__ uint64_t mb_w, mb_x, mb_mma;
     __shared__ uint32_t tslot;
     const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t n = n_dev ? min(*n_dev, n_max) : n_max;
     const uint32_t ntiles = (n + kTile - 1) / kTile;
     if (blockIdx.x >= ntiles) return;
     if (warp == 0) umma::tmem_alloc(&tslot, 128);
@@ -308,11 +310,23 @@ constexpr int kTrainSmemB = 51200 + 1024;            // 52224, 1024-aligned
 constexpr int kTrainSmemA = kTrainSmemB + 40960;      // 93184
 constexpr int kTrainSmem = kTrainSmemA + 2 * kTile * 128;   // 125952
 
+// Device-resident training state (one per model): read by the kernels so a
+// whole frame can be enqueued (and captured in a CUDA graph) without reading
+// anything back to the host.
+enum : int {
+    S_STEP = 0,      // ColorMLP::step_counter (mlp.cpp:103), seed of the sample indices
+    S_ADAM_T = 1,    // Adam time step
+    S_NAVAIL = 2,    // training records available to this step
+    S_GATE = 3,      // 1: the cache's running error is low enough to answer queries
+    S_LOSS_EMA = 4,  // running loss (float bits)
+    S_WORDS = 8
+};
+
 struct TrainArgs {
     const TfgDatosMLP* buf;      // training records (targets in .color)
-    uint32_t n_avail;            // records available
+    const uint32_t* state;       // S_NAVAIL records available, S_STEP seed
+    uint32_t min_n;              // no step below this many records
     uint32_t batch;              // samples in this step (multiple of kTile)
-    uint32_t seed;               // index stream seed (ColorMLP step counter)
     Bounds bounds;
     const uint8_t* fwd;          // FP16 forward image
     const uint8_t* bwd;          // BF16 backward image
@@ -343,7 +357,9 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     __shared__ uint32_t tslot;
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t ntiles = a.batch / kTile;
-    if (blockIdx.x >= ntiles) return;
+    const uint32_t n_avail = a.state[S_NAVAIL];
+    const uint32_t seed = a.state[S_STEP];
+    if (blockIdx.x >= ntiles || n_avail < a.min_n || n_avail == 0) return;
     if (warp == 0) umma::tmem_alloc(&tslot, 128);
     if (t == 0) {
         umma::mbar_init(&mb_w, 1);
@@ -368,8 +384,8 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const uint32_t s = tile * kTile + (uint32_t)t;
         // Sample selection as generarIndicesAleatorios (NrcKernel.cu:10-16).
-        uint32_t st = a.seed ^ s;
-        const uint32_t idx = pcg_next(st) % a.n_avail;
+        uint32_t st = seed ^ s;
+        const uint32_t idx = pcg_next(st) % n_avail;
         const TfgDatosMLP d = a.buf[idx];
         float tgt[3] = {d.color.r, d.color.g, d.color.b};
 #pragma unroll
@@ -487,6 +503,8 @@ struct WgradArgs {
     const uint8_t* zT[kLayers];
     const uint8_t* hT[kLayers];
     float* grad;
+    const uint32_t* state;
+    uint32_t min_n;
     uint32_t ntiles;
     uint32_t tiles_per_cta;
 };
@@ -500,7 +518,7 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     const int l = blockIdx.y;
     const int FZ = kZTFeat(l), FH = kHTFeat(l);
     const uint32_t t0 = blockIdx.x * a.tiles_per_cta;
-    if (t0 >= a.ntiles) return;
+    if (t0 >= a.ntiles || a.state[S_NAVAIL] < a.min_n || a.state[S_NAVAIL] == 0) return;
     const uint32_t t1 = min(a.ntiles, t0 + a.tiles_per_cta);
     if (warp == 0) umma::tmem_alloc(&tslot, 128);
     if (t == 0) {
@@ -592,7 +610,8 @@ struct AdamArgs {
     uint8_t* inf;    // FP16 image of the debiased EMA
     float lr, beta1, beta2, eps, decay;
     float grad_scale;              // 1 / (batch * 3)
-    float bc1, bc2, ema_debias;    // 1 - beta^t, 1 - decay^t
+    const uint32_t* state;         // S_ADAM_T before this step, S_NAVAIL
+    uint32_t min_n;
     int update;                    // 0: only re-pack (after loading parameters)
 };
 
@@ -613,20 +632,24 @@ __global__ void k_adam(AdamArgs a) {
     const bool live = !(l == kLayers - 1 && r >= 3) && !(l == 0 && c >= 85);
     float w = a.w[i];
     float e = a.ema[i];
-    if (a.update && live) {
+    const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
+    const float tn = (float)(a.state[S_ADAM_T] + (update ? 1u : 0u));
+    if (update && live) {
+        const float bc1 = 1.0f - powf(a.beta1, tn), bc2 = 1.0f - powf(a.beta2, tn);
         const float g = a.grad[i] * a.grad_scale;
         const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
         const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
         a.m[i] = m;
         a.v[i] = v;
-        w -= a.lr * (m / a.bc1) / (sqrtf(v / a.bc2) + a.eps);
+        w -= a.lr * (m / bc1) / (sqrtf(v / bc2) + a.eps);
         e = a.decay * e + (1.0f - a.decay) * w;
         a.w[i] = w;
         a.ema[i] = e;
     }
     if (!live) { w = 0.0f; e = 0.0f; }
     a.grad[i] = 0.0f;
-    const float ew = a.ema_debias > 0.0f ? e / a.ema_debias : w;
+    const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
+    const float ew = ema_debias > 0.0f ? e / ema_debias : w;
     // forward / inference images: row r, K index c
     const int rows = kRows(l);
     const uint32_t off = (uint32_t)kFOff(l) + (uint32_t)(c >> 6) * rows * 128 + umma::sw128_offset(r, (c & 63) >> 3) +
@@ -640,14 +663,31 @@ __global__ void k_adam(AdamArgs a) {
     }
 }
 
+// After a step: advance the step counter and Adam time, keep a running loss
+// and open the cache-query gate once it falls below `gate`.
+__global__ void k_tick(uint32_t* state, const float* loss_sum, float inv_count, uint32_t min_n, float gate) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    const uint32_t n = state[S_NAVAIL];
+    if (n < min_n || n == 0) return;
+    state[S_STEP] += 1u;
+    state[S_ADAM_T] += 1u;
+    const float loss = *loss_sum * inv_count;
+    float ema = __uint_as_float(state[S_LOSS_EMA]);
+    ema = (state[S_ADAM_T] == 1u) ? loss : 0.9f * ema + 0.1f * loss;
+    state[S_LOSS_EMA] = __float_as_uint(ema);
+    if (gate <= 0.0f || ema < gate) state[S_GATE] = 1u;
+}
+
+__global__ void k_set_word(uint32_t* state, int index, uint32_t value) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) state[index] = value;
+}
+
 }  // namespace mlp
 
 // ====================================================================== host object
 struct ColorMlp {
     int dev = 0;
     uint32_t batch = 16384;
-    uint32_t step = 0;           // ColorMLP::step_counter (mlp.cpp:103)
-    uint32_t adam_t = 0;
     float lr = 1e-2f, beta1 = 0.9f, beta2 = 0.99f, eps = 1e-15f, decay = 0.99f;
     mlp::Bounds bounds{{-1, -1, -1}, {1, 1, 1}};
     float* w = nullptr; float* m = nullptr; float* v = nullptr; float* ema = nullptr; float* grad = nullptr;
@@ -655,6 +695,8 @@ struct ColorMlp {
     uint8_t* hT[mlp::kLayers] = {nullptr};
     uint8_t* zT[mlp::kLayers] = {nullptr};
     float* loss = nullptr;
+    uint32_t* dstate = nullptr;  // mlp::S_* words
+    float gate = 0.0f;           // cache-query gate threshold on the running loss (<= 0: always open)
     uint32_t act_tiles = 0;
     int sms = 148;
 };
@@ -672,15 +714,14 @@ uint64_t splitmix(uint64_t& s) {
     return z ^ (z >> 31);
 }
 
-int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t batch_used) {
+int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
     mlp::AdamArgs a;
     a.w = n->w; a.m = n->m; a.v = n->v; a.ema = n->ema; a.grad = n->grad;
     a.fwd = n->fwd; a.bwd = n->bwd; a.inf = n->inf;
     a.lr = n->lr; a.beta1 = n->beta1; a.beta2 = n->beta2; a.eps = n->eps; a.decay = n->decay;
-    a.grad_scale = batch_used ? 1.0f / (3.0f * (float)batch_used) : 0.0f;
-    a.bc1 = 1.0f - std::pow(n->beta1, (float)std::max(1u, n->adam_t));
-    a.bc2 = 1.0f - std::pow(n->beta2, (float)std::max(1u, n->adam_t));
-    a.ema_debias = n->adam_t ? 1.0f - std::pow(n->decay, (float)n->adam_t) : 0.0f;
+    a.grad_scale = 1.0f / (3.0f * (float)n->batch);
+    a.state = n->dstate;
+    a.min_n = min_n;
     a.update = update ? 1 : 0;
     mlp::k_adam<<<(mlp::kParams + 255) / 256, 256, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
@@ -716,7 +757,72 @@ int check_error_flag() {
     return ok();
 }
 
+// Forward/backward, weight gradients (and, with `update`, Adam + tick) of one
+// step whose record count and seed are already in the device state.
+int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool update, cudaStream_t s) {
+    const uint32_t tiles = n->batch / mlp::kTile;
+    cudaError_t e = cudaMemsetAsync(n->loss, 0, sizeof(float), s);
+    if (e != cudaSuccess) return cuda_fail(e, "mlp step");
+    mlp::TrainArgs ta;
+    ta.buf = buf; ta.state = n->dstate; ta.min_n = min_n; ta.batch = n->batch;
+    ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
+    for (int l = 0; l < mlp::kLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
+    mlp::k_train<<<std::min<uint32_t>(tiles, (uint32_t)n->sms), 128, mlp::kTrainSmem + 1024, s>>>(ta);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mlp step: forward/backward");
+    mlp::WgradArgs wa;
+    for (int l = 0; l < mlp::kLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
+    wa.grad = n->grad; wa.state = n->dstate; wa.min_n = min_n;
+    wa.ntiles = tiles;
+    wa.tiles_per_cta = std::max<uint32_t>(2u, (tiles + 15u) / 16u);
+    mlp::k_wgrad<<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, mlp::kLayers), 128, mlp::kWgSmem + 1024,
+                   s>>>(wa);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mlp step: weight gradients");
+    if (!update) return ok();
+    if (int rc = repack(n, s, true, min_n)) return rc;
+    mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n, n->gate);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mlp step: tick");
+    return ok();
+}
+
+int set_word(ColorMlp* n, int index, uint32_t value, cudaStream_t s) {
+    mlp::k_set_word<<<1, 32, 0, s>>>(n->dstate, index, value);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mlp state");
+    return ok();
+}
+
+int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img, const TfgColor* thr, uint32_t count,
+               const uint32_t* n_dev, cudaStream_t s) {
+    if (count == 0) return ok();
+    if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
+        return fail(TFG_E_INVALID, "mlp inference: input buffer must be 16-byte aligned");
+    const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
+    const uint32_t grid = std::min<uint32_t>(tiles, 2u * (uint32_t)n->sms);
+    mlp::k_infer<<<grid, 128, mlp::kInferSmem + 1024, s>>>(in, count, n_dev, n->bounds, n->inf, out, img, thr);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mlp inference");
+    return ok();
+}
+
 }  // namespace
+
+// ------------------------------------------------------------------ internal API (frame driver)
+int mlp_prepare(ColorMlp* n) { return ensure_acts(n, n->batch / mlp::kTile); }
+uint32_t* mlp_state(ColorMlp* n) { return n->dstate; }
+uint32_t* mlp_gate(ColorMlp* n) { return n->dstate + mlp::S_GATE; }
+uint32_t* mlp_navail(ColorMlp* n) { return n->dstate + mlp::S_NAVAIL; }
+int mlp_enqueue_infer(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img, const TfgColor* thr,
+                      uint32_t max_count, const uint32_t* n_dev, cudaStream_t s) {
+    return infer_impl(n, in, out, img, thr, max_count, n_dev, s);
+}
+int mlp_enqueue_train(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, cudaStream_t s) {
+    return enqueue_step(n, buf, min_n, true, s);
+}
+void mlp_set_gate_threshold(ColorMlp* n, float g) { n->gate = g; }
+
 }  // namespace tfg
 
 using tfg::ColorMlp;
@@ -746,31 +852,35 @@ extern "C" int tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint6
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->bwd, M::kBwdBytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf, M::kFwdBytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->loss, sizeof(float));
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->dstate, M::S_WORDS * sizeof(uint32_t));
     if (e != cudaSuccess) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return tfg::cuda_fail(e, "tfgMlpCreate"); }
     cudaMemset(n->fwd, 0, M::kFwdBytes);
     cudaMemset(n->bwd, 0, M::kBwdBytes);
     cudaMemset(n->inf, 0, M::kFwdBytes);
+    cudaMemset(n->dstate, 0, M::S_WORDS * sizeof(uint32_t));
     // Uniform (-s, s) initialisation with s = sqrt(6 / (fan_in + fan_out)) per layer.
     std::vector<float> h(M::kParams, 0.0f);
     uint64_t st = seed ? seed : 0x5EEDull;
     const int fan_in[M::kLayers] = {85, 64, 64, 64, 64, 64};
     const int fan_out[M::kLayers] = {64, 64, 64, 64, 64, 3};
     for (int l = 0; l < M::kLayers; ++l) {
-        const float s = std::sqrt(6.0f / (float)(fan_in[l] + fan_out[l]));
+        const float sc = std::sqrt(6.0f / (float)(fan_in[l] + fan_out[l]));
         for (int r = 0; r < M::kRows(l); ++r)
             for (int c = 0; c < M::kCols(l); ++c) {
                 const bool live = !(l == M::kLayers - 1 && r >= 3) && !(l == 0 && c >= 85);
                 const double u = (double)(tfg::splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
-                h[M::kPOff(l) + r * M::kCols(l) + c] = live ? (float)((2.0 * u - 1.0) * s) : 0.0f;
+                h[M::kPOff(l) + r * M::kCols(l) + c] = live ? (float)((2.0 * u - 1.0) * sc) : 0.0f;
             }
     }
+    // The weight average starts at zero and is debiased by 1 - decay^t for
+    // inference; before the first step inference uses the weights themselves.
     e = cudaMemcpy(n->w, h.data(), pb, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(n->ema, h.data(), pb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(n->ema, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->m, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->v, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->grad, 0, pb);
     if (e != cudaSuccess) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return tfg::cuda_fail(e, "tfgMlpCreate"); }
-    if (int rc = tfg::repack(n, 0, false, 0)) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return rc; }
+    if (int rc = tfg::repack(n, 0, false, 1)) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return rc; }
     static bool attrs = false;
     if (!attrs) {
         cudaFuncSetAttribute(M::k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kInferSmem + 1024);
@@ -788,7 +898,7 @@ extern "C" void tfgMlpDestroy(TfgColorMLP* h) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n) return;
     for (void* p : {(void*)n->w, (void*)n->m, (void*)n->v, (void*)n->ema, (void*)n->grad, (void*)n->fwd, (void*)n->bwd,
-                    (void*)n->inf, (void*)n->loss})
+                    (void*)n->inf, (void*)n->loss, (void*)n->dstate})
         if (p) cudaFree(p);
     for (int l = 0; l < M::kLayers; ++l) {
         if (n->hT[l]) cudaFree(n->hT[l]);
@@ -813,23 +923,10 @@ extern "C" int tfgMlpSetHyperparams(TfgColorMLP* h, float lr, float beta1, float
     return tfg::ok();
 }
 
-static int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img, const TfgColor* thr,
-                      uint32_t count, cudaStream_t s) {
-    if (count == 0) return tfg::ok();
-    if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
-        return tfg::fail(TFG_E_INVALID, "tfgMlpInference: input buffer must be 16-byte aligned");
-    const uint32_t tiles = (count + M::kTile - 1) / M::kTile;
-    const uint32_t grid = std::min<uint32_t>(tiles, 2u * (uint32_t)n->sms);
-    M::k_infer<<<grid, 128, M::kInferSmem + 1024, s>>>(in, count, n->bounds, n->inf, out, img, thr);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpInference");
-    return tfg::ok();
-}
-
 extern "C" int tfgMlpInference(TfgColorMLP* h, const TfgDatosMLP* in, TfgColor* out, uint32_t count, void* stream) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n || (count && (!in || !out))) return tfg::fail(TFG_E_INVALID, "tfgMlpInference: null argument");
-    return infer_impl(n, in, out, nullptr, nullptr, count, (cudaStream_t)stream);
+    return tfg::infer_impl(n, in, out, nullptr, nullptr, count, nullptr, (cudaStream_t)stream);
 }
 
 extern "C" int tfgMlpInferenceComposite(TfgColorMLP* h, const TfgDatosMLP* in, const TfgColor* throughput,
@@ -837,7 +934,7 @@ extern "C" int tfgMlpInferenceComposite(TfgColorMLP* h, const TfgDatosMLP* in, c
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n || (count && (!in || !throughput || !img)))
         return tfg::fail(TFG_E_INVALID, "tfgMlpInferenceComposite: null argument");
-    return infer_impl(n, in, nullptr, img, throughput, count, (cudaStream_t)stream);
+    return tfg::infer_impl(n, in, nullptr, img, throughput, count, nullptr, (cudaStream_t)stream);
 }
 
 extern "C" int tfgMlpTrainStep(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32_t n_available, float* loss_out,
@@ -847,32 +944,12 @@ extern "C" int tfgMlpTrainStep(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32
     if (loss_out) *loss_out = 0.0f;
     if (n_available < 100) return tfg::ok();   // mlp.cpp:96: too few samples, no step
     cudaStream_t s = (cudaStream_t)stream;
-    const uint32_t tiles = n->batch / M::kTile;
-    if (int rc = tfg::ensure_acts(n, tiles)) return rc;
-    cudaError_t e = cudaMemsetAsync(n->loss, 0, sizeof(float), s);
-    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpTrainStep");
-    M::TrainArgs ta;
-    ta.buf = buffer; ta.n_avail = n_available; ta.batch = n->batch; ta.seed = n->step++;
-    ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
-    for (int l = 0; l < M::kLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
-    const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)n->sms);
-    M::k_train<<<grid, 128, M::kTrainSmem + 1024, s>>>(ta);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpTrainStep: forward/backward");
-    M::WgradArgs wa;
-    for (int l = 0; l < M::kLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
-    wa.grad = n->grad;
-    wa.ntiles = tiles;
-    wa.tiles_per_cta = std::max<uint32_t>(2u, (tiles + 15u) / 16u);
-    dim3 g((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, M::kLayers);
-    M::k_wgrad<<<g, 128, M::kWgSmem + 1024, s>>>(wa);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpTrainStep: weight gradients");
-    n->adam_t++;
-    if (int rc = tfg::repack(n, s, true, n->batch)) return rc;
+    if (int rc = tfg::mlp_prepare(n)) return rc;
+    if (int rc = tfg::set_word(n, M::S_NAVAIL, n_available, s)) return rc;
+    if (int rc = tfg::enqueue_step(n, buffer, 100, true, s)) return rc;
     if (loss_out) {
         float l = 0.0f;
-        e = cudaMemcpyAsync(&l, n->loss, sizeof(float), cudaMemcpyDeviceToHost, s);
+        cudaError_t e = cudaMemcpyAsync(&l, n->loss, sizeof(float), cudaMemcpyDeviceToHost, s);
         if (e == cudaSuccess) e = cudaStreamSynchronize(s);
         if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpTrainStep: loss");
         *loss_out = l / (3.0f * (float)n->batch);
@@ -896,56 +973,44 @@ extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count
     if (!n || !host || count != (uint32_t)M::kParams) return tfg::fail(TFG_E_INVALID, "tfgMlpSetParams: bad argument");
     const size_t pb = count * sizeof(float);
     cudaError_t e = cudaMemcpy(n->w, host, pb, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemcpy(n->ema, host, pb, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(n->ema, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->m, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->v, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->grad, 0, pb);
+    if (e == cudaSuccess) e = cudaMemset(n->dstate + M::S_ADAM_T, 0, sizeof(uint32_t));
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetParams");
-    n->adam_t = 0;
-    if (int rc = tfg::repack(n, 0, false, 0)) return rc;
+    if (int rc = tfg::repack(n, 0, false, 1)) return rc;
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetParams");
     return tfg::ok();
 }
 
-// Gradient of the last step is consumed by Adam; this runs the
-// forward/backward/weight-gradient kernels alone and returns the normalised
-// gradient (d loss / d W) without updating the parameters.
 extern "C" int tfgMlpComputeGradient(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
                                      float* host_grad, uint32_t count, float* loss_out) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n || !buffer || !host_grad || count != (uint32_t)M::kParams || n_available == 0)
         return tfg::fail(TFG_E_INVALID, "tfgMlpComputeGradient: bad argument");
-    const uint32_t tiles = n->batch / M::kTile;
-    if (int rc = tfg::ensure_acts(n, tiles)) return rc;
-    cudaError_t e = cudaMemset(n->loss, 0, sizeof(float));
+    if (int rc = tfg::mlp_prepare(n)) return rc;
+    uint32_t saved[M::S_WORDS];
+    cudaError_t e = cudaMemcpy(saved, n->dstate, sizeof(saved), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemset(n->grad, 0, M::kParams * sizeof(float));
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
-    M::TrainArgs ta;
-    ta.buf = buffer; ta.n_avail = n_available; ta.batch = n->batch; ta.seed = seed;
-    ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
-    for (int l = 0; l < M::kLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
-    M::k_train<<<std::min<uint32_t>(tiles, (uint32_t)n->sms), 128, M::kTrainSmem + 1024>>>(ta);
-    M::WgradArgs wa;
-    for (int l = 0; l < M::kLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
-    wa.grad = n->grad;
-    wa.ntiles = tiles;
-    wa.tiles_per_cta = std::max<uint32_t>(2u, (tiles + 15u) / 16u);
-    M::k_wgrad<<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, M::kLayers), 128, M::kWgSmem + 1024>>>(wa);
+    if (int rc = tfg::set_word(n, M::S_NAVAIL, n_available, 0)) return rc;
+    if (int rc = tfg::set_word(n, M::S_STEP, seed, 0)) return rc;
+    if (int rc = tfg::enqueue_step(n, buffer, 1, false, 0)) return rc;
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
     if (int rc = tfg::check_error_flag()) return rc;
     std::vector<float> g(M::kParams);
+    float l = 0.0f;
     e = cudaMemcpy(g.data(), n->grad, M::kParams * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&l, n->loss, sizeof(float), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, M::kParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(n->dstate, saved, sizeof(saved), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
     const float sc = 1.0f / (3.0f * (float)n->batch);
     for (int i = 0; i < M::kParams; ++i) host_grad[i] = g[i] * sc;
-    cudaMemset(n->grad, 0, M::kParams * sizeof(float));
-    if (loss_out) {
-        float l = 0.0f;
-        cudaMemcpy(&l, n->loss, sizeof(float), cudaMemcpyDeviceToHost);
-        *loss_out = l * sc;
-    }
+    if (loss_out) *loss_out = l * sc;
     return tfg::ok();
 }
 

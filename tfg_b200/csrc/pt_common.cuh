@@ -49,6 +49,10 @@ __device__ __forceinline__ V3 normalized(V3 a) {
     float l = sqrtf(dot(a, a));
     return l > 0.0f ? a * (1.0f / l) : a;   // vector3d.h:65-71 leaves a zero vector unchanged
 }
+// Color / float (color.h:40-46): division by zero gives black.
+__device__ __forceinline__ V3 div_or_black(V3 c, float s) {
+    return s == 0.0f ? v3(0.0f, 0.0f, 0.0f) : v3(c.x / s, c.y / s, c.z / s);
+}
 __device__ __forceinline__ float cmax(V3 c) {   // color.h:66-78 (r >= g ? r : g, then b)
     float m = c.x >= c.y ? c.x : c.y;
     return c.z > m ? c.z : m;

@@ -80,7 +80,9 @@ struct PassArgs {
     const TfgLuzPuntual* lights; int nlights;
     const float4* nodes; const float4* tris; int has_bvh;
     const TfgPrimitiva* mesh; int nmesh;
-    TfgCamara cam;
+    const TfgCamara* cam;        // device pointer, read by k_generate
+    const int32_t* frame_dev;    // optional device-side base frame number
+    const uint32_t* use_inf_dev; // optional device-side gate on cache queries
     int W, H, frame;
     TfgColor* img; float* accum;
     TfgRegistroEntrenamiento* regs; uint32_t* reg_counter; int reg_cap;
@@ -146,17 +148,24 @@ __device__ __forceinline__ int load_aprims_smem(APrim* sp, const TfgPrimitiva* g
 
 // ------------------------------------------------------------------ generate
 // render.h:424-447: seed, jitter draws, training / unbiased draws, camera ray.
+__device__ __forceinline__ int use_inf_of(const PassArgs& a) {
+    return a.use_inf && (!a.use_inf_dev || *a.use_inf_dev != 0u);
+}
+
 __global__ void k_generate(PassArgs a) {
     const uint32_t N = (uint32_t)a.W * (uint32_t)a.H;
+    const TfgCamara cam = *a.cam;
+    const int frame = a.frame + (a.frame_dev ? *a.frame_dev : 0);
+    const int use_inf = use_inf_of(a);
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
         const int x = (int)(p % (uint32_t)a.W), y = (int)(p / (uint32_t)a.W);
-        uint32_t rng = seed_pixel(x, y, a.frame);
+        uint32_t rng = seed_pixel(x, y, frame);
         const float ox = pcg_uniform(rng);
         const float oy = pcg_uniform(rng);
         V3 O, D;
-        camera_ray(a.cam, x, y, a.W, a.H, ox, oy, O, D);
+        camera_ray(cam, x, y, a.W, a.H, ox, oy, O, D);
         uint32_t flags = 0;
-        bool training = a.train ? (a.use_inf ? (pcg_uniform(rng) < 0.05f) : true) : false;
+        bool training = a.train ? (use_inf ? (pcg_uniform(rng) < 0.05f) : true) : false;
         if (training) {
             flags |= F_TRAIN;
             if (pcg_uniform(rng) < 0.0625f) flags |= F_UNBIASED;
@@ -245,6 +254,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
     uint32_t* next_count = &a.ws.counters[4 * (bounce + 1) + 0];
     uint32_t* shadow_count = &a.ws.counters[4 * bounce + 2];
     const bool nrc = a.use_inf || a.train;
+    const int use_inf = use_inf_of(a);
     const uint32_t stride = gridDim.x * blockDim.x;
     // Uniform trip count so that every lane of a warp reaches the warp-wide appends.
     const uint32_t n_round = (n + stride - 1) / stride * stride;
@@ -333,7 +343,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
                         V3 refl = m.difuso + m.especular + m.transmision;
                         refl = v3(fmaxf(refl.x, 1e-3f), fmaxf(refl.y, 1e-3f), fmaxf(refl.z, 1e-3f));
                         const bool training = (flags & F_TRAIN) != 0;
-                        if (!training && a.use_inf) {
+                        if (!training && use_inf) {
                             write_datos(&a.infer[p], P, map01(view), map01(nrm), m.difuso, m.especular);
                             const V3 tt = mul(cam, refl);
                             a.thr_out[p] = TfgColor{tt.x, tt.y, tt.z};
@@ -358,8 +368,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
                             const float pd = mkd / sum, ps = mks / sum, pt = 1.0f - pd - ps;
                             const float r = pcg_uniform(rng);
                             if (r < pd) {
-                                cam = mul(cam, m.difuso);
-                                cam = v3(cam.x / pd, cam.y / pd, cam.z / pd);
+                                cam = div_or_black(mul(cam, m.difuso), pd);
                                 const float r1 = pcg_uniform(rng);
                                 const float r2 = pcg_uniform(rng);
                                 const float phi = 2.0f * kPiF * r1;
@@ -377,15 +386,13 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
                                 }
                             } else if (r < pd + ps) {
                                 const V3 wr = reflect_dir(D, nrm);
-                                cam = mul(cam, m.especular);
-                                cam = v3(cam.x / ps, cam.y / ps, cam.z / ps);
+                                cam = div_or_black(mul(cam, m.especular), ps);
                                 O = P + wr * kEps;
                                 D = normalized(wr);
                                 pdf_last = 1e6f;
                             } else {
                                 const V3 wt = refract_dir(D, nrm, m.ior, ior);
-                                cam = mul(cam, m.transmision);
-                                cam = v3(cam.x / pt, cam.y / pt, cam.z / pt);
+                                cam = div_or_black(mul(cam, m.transmision), pt);
                                 O = P + wt * kEps;
                                 D = normalized(wt);
                                 pdf_last = 1e6f;
@@ -396,7 +403,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
                             float prob = fmaxf(cam.x, fmaxf(cam.y, cam.z));
                             if (prob > 0.95f) prob = 0.95f;
                             if (pcg_uniform(rng) > prob) end = true;
-                            else cam = v3(cam.x / prob, cam.y / prob, cam.z / prob);
+                            else cam = div_or_black(cam, prob);
                         }
                         if (!end && bounce + 1 < a.max_depth) survive = true;
                     }
@@ -665,6 +672,17 @@ int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPri
                 const float* tris_wt, const TfgPrimitiva* mesh, int nmesh, TfgColor* img, float* accum,
                 TfgRegistroEntrenamiento* regs, uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer,
                 TfgColor* thr_out, int use_inf, int train, cudaStream_t stream) {
+    return render_pass_ex(prm, d_cam, prims, nprims, lights, nlights, W, H, frame, nullptr, nullptr, bvh, tris_wt,
+                          mesh, nmesh, img, accum, regs, reg_counter, reg_cap, infer, thr_out, use_inf, train, false,
+                          stream);
+}
+
+int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
+                   const TfgLuzPuntual* lights, int nlights, int W, int H, int frame, const int32_t* frame_dev,
+                   const uint32_t* use_inf_dev, const TfgTinyBVHD_GPU* bvh, const float* tris_wt,
+                   const TfgPrimitiva* mesh, int nmesh, TfgColor* img, float* accum, TfgRegistroEntrenamiento* regs,
+                   uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer, TfgColor* thr_out, int use_inf, int train,
+                   bool prepare_only, cudaStream_t stream) {
     if (W <= 0 || H <= 0 || (size_t)W * (size_t)H > (1u << 28)) return fail(TFG_E_INVALID, "render: bad image size");
     if (!d_cam) return fail(TFG_E_INVALID, "render: camara is null");
     if (nprims < 0 || nlights < 0 || nmesh < 0) return fail(TFG_E_INVALID, "render: negative count");
@@ -687,11 +705,7 @@ int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPri
     if (int rc = ensure_workspace(dev, (size_t)W * H, nrc, ws)) return rc;
     LaunchShapes sh;
     shapes_for(dev, sh);
-
-    TfgCamara cam;
-    e = cudaMemcpyAsync(&cam, d_cam, sizeof(cam), cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return fail((int)e, std::string("render: camera read: ") + cudaGetErrorString(e));
+    if (prepare_only) return ok();
 
     PassArgs a{};
     a.prims = prims; a.nprims = nprims; a.lights = lights; a.nlights = nlights;
@@ -699,7 +713,9 @@ int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPri
     a.tris = has_bvh ? reinterpret_cast<const float4*>(prm.tri_format == TFG_TRIS_REF ? bvh->d_tris : tris_wt) : nullptr;
     a.has_bvh = has_bvh ? 1 : 0;
     a.mesh = mesh; a.nmesh = nmesh;
-    a.cam = cam;
+    a.cam = d_cam;
+    a.frame_dev = frame_dev;
+    a.use_inf_dev = use_inf_dev;
     a.W = W; a.H = H;
     a.accum = accum;
     a.regs = regs; a.reg_counter = reg_counter; a.reg_cap = reg_cap;
@@ -781,8 +797,9 @@ __global__ void __launch_bounds__(128) k_trace_rays(const float4* __restrict__ n
     }
 }
 
-__global__ void k_camera_rays(TfgCamara cam, int W, int H, int frame, float4* rays) {
+__global__ void k_camera_rays(const TfgCamara* camp, int W, int H, int frame, float4* rays) {
     const uint32_t N = (uint32_t)W * (uint32_t)H;
+    const TfgCamara cam = *camp;
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
         const int x = (int)(p % (uint32_t)W), y = (int)(p / (uint32_t)W);
         uint32_t rng = seed_pixel(x, y, frame);
@@ -845,12 +862,8 @@ int camera_rays(const TfgCamara* d_cam, int W, int H, int frame, float* rays, cu
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     if (int rc = require_sm100(dev)) return rc;
-    TfgCamara cam;
-    e = cudaMemcpyAsync(&cam, d_cam, sizeof(cam), cudaMemcpyDeviceToHost, stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(stream);
-    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     const int blocks = std::max(1, std::min((W * H + 255) / 256, 148 * 8));
-    k_camera_rays<<<blocks, 256, 0, stream>>>(cam, W, H, frame, reinterpret_cast<float4*>(rays));
+    k_camera_rays<<<blocks, 256, 0, stream>>>(d_cam, W, H, frame, reinterpret_cast<float4*>(rays));
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     return ok();

@@ -17,9 +17,37 @@ int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPri
                 TfgRegistroEntrenamiento* regs, uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer,
                 TfgColor* thr_out, int use_inf, int train, cudaStream_t stream);
 
+// render_pass with a device-side frame number / cache-query gate (both
+// optional) and a prepare-only mode that validates and allocates without
+// launching (so a later call can be captured in a CUDA graph).
+int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
+                   const TfgLuzPuntual* lights, int nlights, int W, int H, int frame, const int32_t* frame_dev,
+                   const uint32_t* use_inf_dev, const TfgTinyBVHD_GPU* bvh, const float* tris_wt,
+                   const TfgPrimitiva* mesh, int nmesh, TfgColor* img, float* accum, TfgRegistroEntrenamiento* regs,
+                   uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer, TfgColor* thr_out, int use_inf, int train,
+                   bool prepare_only, cudaStream_t stream);
+
 int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const float* rays, int n, float* hits,
                cudaStream_t stream);
 
 int camera_rays(const TfgCamara* d_cam, int W, int H, int frame, float* rays, cudaStream_t stream);
+
+// Small frame kernels with a device-side count: 0 tail queries (a = records,
+// b = DatosMLP out), 1 targets (a = records, c = tail predictions, b = out),
+// 2 record count (a = ring counter, b = count out, cap), 3 accumulate
+// (a = image, b = FP32 accumulation, cap = pixels).
+int launch_nrc_frame_small(int which, const void* a, void* b, const void* c, const uint32_t* n_dev, uint32_t cap,
+                           uint32_t min_n, cudaStream_t s);
+
+// Cache model internals used by the frame driver (nrc_mlp.cu).
+struct ColorMlp;
+int mlp_prepare(ColorMlp* n);
+uint32_t* mlp_state(ColorMlp* n);
+uint32_t* mlp_gate(ColorMlp* n);
+uint32_t* mlp_navail(ColorMlp* n);
+int mlp_enqueue_infer(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img, const TfgColor* thr,
+                      uint32_t max_count, const uint32_t* n_dev, cudaStream_t s);
+int mlp_enqueue_train(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, cudaStream_t s);
+void mlp_set_gate_threshold(ColorMlp* n, float g);
 
 }  // namespace tfg

@@ -8,7 +8,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .structs import BOUNDS
+from .structs import BOUNDS, DATOS_MLP, REGISTRO, CNrcBuffers, CNrcFrameConfig
 
 N_PARAMS = 23552
 # padded [out][in] shapes of the six weight matrices, in parameter order
@@ -93,6 +93,12 @@ class ColorMLP:
         """Weights, EMA and Adam moments as one float32 .npz archive."""
         np.savez(path, w=self.get_params(WEIGHTS), ema=self.get_params(EMA))
 
+    def state(self) -> dict:
+        st = (ctypes.c_uint32 * 8)()
+        _lib.call("tfgMlpGetState", self.h, st)
+        return {"step": st[0], "adam_t": st[1], "records": st[2], "gate": st[3],
+                "loss_ema": float(np.array([st[4]], np.uint32).view(np.float32)[0])}
+
     def load_model(self, path: str) -> bool:
         try:
             d = np.load(path)
@@ -104,3 +110,60 @@ class ColorMLP:
 
 def status() -> None:
     _lib.call("tfgMlpStatus")
+
+
+
+
+class NrcRenderer:
+    """The reference's normal-mode frame loop (main.cpp:895-1089) as GPU-only
+    frames: tfgNrcFrame renders with cache queries and training records,
+    answers and composites the queries, bootstraps targets and trains."""
+
+    def __init__(self, ds, mlp: ColorMLP, params, train_steps: int = 4, max_records: int = 65536,
+                 min_records: int = 1024, gate_threshold: float = 0.0, use_graph: bool = True, stream=None):
+        self.ds, self.mlp, self.params = ds, mlp, params
+        W, H = ds.scene.width, ds.scene.height
+        dev = ds.device
+        n = W * H
+        self.W, self.H = W, H
+        self.stream = stream or torch.cuda.Stream(device=dev)
+        self.img = torch.zeros(n * 3, dtype=torch.float32, device=dev)
+        self.accum = torch.zeros(n * 3, dtype=torch.float32, device=dev)
+        self.infer = torch.zeros(n * DATOS_MLP.itemsize, dtype=torch.uint8, device=dev)
+        self.thr = torch.zeros(n * 3, dtype=torch.float32, device=dev)
+        self.ring_cap = max(n, max_records)
+        self.regs = torch.zeros(self.ring_cap * REGISTRO.itemsize, dtype=torch.uint8, device=dev)
+        self.counter = torch.zeros(1, dtype=torch.int32, device=dev)
+        self.tail_in = torch.zeros(max_records * DATOS_MLP.itemsize, dtype=torch.uint8, device=dev)
+        self.tail_pred = torch.zeros(max_records * 3, dtype=torch.float32, device=dev)
+        self.train_buf = torch.zeros(max_records * DATOS_MLP.itemsize, dtype=torch.uint8, device=dev)
+        self.cfg = CNrcFrameConfig()
+        _lib.lib.tfgNrcFrameConfigReference(ctypes.byref(self.cfg))
+        self.cfg.train_steps, self.cfg.max_records, self.cfg.min_records = train_steps, max_records, min_records
+        self.cfg.gate_threshold, self.cfg.use_graph = gate_threshold, int(use_graph)
+        self.bufs = CNrcBuffers(self.img.data_ptr(), self.accum.data_ptr(), self.infer.data_ptr(),
+                                self.thr.data_ptr(), self.regs.data_ptr(), self.counter.data_ptr(), self.ring_cap, 0,
+                                self.tail_in.data_ptr(), self.tail_pred.data_ptr(), self.train_buf.data_ptr())
+        self.frames_accumulated = 0
+
+    def frame(self, frame: int, warmup: bool = False, accumulate: bool = True) -> None:
+        ds = self.ds
+        self.cfg.warmup = int(warmup)
+        self.bufs.accum = self.accum.data_ptr() if accumulate else None
+        _lib.call("tfgNrcFrame", self.mlp.h, ctypes.byref(self.cfg), ctypes.byref(self.params.c()),
+                  ds.camera.data_ptr(), ds.prims.data_ptr() if ds.prims is not None else None, ds.n_prims,
+                  ds.lights.data_ptr(), ds.n_lights, self.W, self.H, ctypes.byref(ds.bvh.ref), ds.bvh.d_tris_wt,
+                  ds.bvh.d_primitivas, ds.n_mesh, ctypes.byref(self.bufs), frame, self.stream.cuda_stream)
+        if accumulate:
+            self.frames_accumulated += 1
+
+    def image(self) -> torch.Tensor:
+        return self.img.view(self.H, self.W, 3)
+
+    def mean_image(self) -> torch.Tensor:
+        return (self.accum / max(1, self.frames_accumulated)).view(self.H, self.W, 3)
+
+    def reset_accumulation(self) -> None:
+        with torch.cuda.stream(self.stream):
+            self.accum.zero_()
+        self.frames_accumulated = 0

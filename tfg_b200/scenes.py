@@ -263,10 +263,11 @@ def _mesh_bounds(*arrays):
 # ---------------------------------------------------------------- workloads
 def box_icosphere(width=512, height=512, subdiv=6, seed=1) -> Scene:
     """Displaced icosphere (amplitude 0.1, 20*4**subdiv triangles) inside a
-    12-triangle box, one point light, albedo U[0.2, 0.8]."""
+    12-triangle box, one point light; the sphere's Lambertian albedo is drawn
+    from U[0.2, 0.8] per colour channel."""
     rng = np.random.default_rng(seed)
     V, F = displaced_icosphere(subdiv, (0.0, -0.8, -0.6), 1.0, 0.1, seed)
-    kd = rng.uniform(0.2, 0.8, size=(len(F), 3)).astype(np.float32)
+    kd = np.repeat(rng.uniform(0.2, 0.8, size=(1, 3)), len(F), axis=0).astype(np.float32)
     mesh = mesh_prims(V, F, kd)
     box = box_prims((-2.6, -2.0, -4.0), (2.6, 2.4, 5.5), {"left": (0.7, 0.2, 0.2), "right": (0.2, 0.7, 0.2)})
     L = lights(((0.0, 1.9, 0.8), (25.0, 25.0, 25.0)))
@@ -278,11 +279,13 @@ def box_icosphere(width=512, height=512, subdiv=6, seed=1) -> Scene:
 def spheres_terrain(width=1920, height=1080, subdiv=5, terrain_n=580, seed=7, angle_deg=0.0) -> Scene:
     """16 displaced icospheres (20*4**subdiv triangles each) on a fractal
     heightfield (2*terrain_n**2 triangles); ~1.0M triangles at the defaults.
-    Two point lights, albedo U[0.1, 0.9]."""
+    Two point lights; each object's Lambertian albedo is drawn from
+    U[0.1, 0.9] per colour channel."""
     rng = np.random.default_rng(seed)
-    Vs, Fs = [], []
+    Vs, Fs, kds = [], [], []
     Vt, Ft = terrain(terrain_n, -10.0, 10.0, -18.0, 2.0, -1.8, 0.9, seed + 1)
     Vs.append(Vt); Fs.append(Ft)
+    kds.append(np.repeat(rng.uniform(0.1, 0.9, size=(1, 3)), len(Ft), axis=0))
     off = len(Vt)
     k = 0
     for gx in (-6.0, -2.0, 2.0, 6.0):
@@ -291,11 +294,12 @@ def spheres_terrain(width=1920, height=1080, subdiv=5, terrain_n=580, seed=7, an
             c = (gx + float(rng.uniform(-0.8, 0.8)), -0.6 + r * 0.6, gz + float(rng.uniform(-0.8, 0.8)))
             V, F = displaced_icosphere(subdiv, c, r, 0.1, seed + 100 + k)
             Vs.append(V); Fs.append(F + off)
+            kds.append(np.repeat(rng.uniform(0.1, 0.9, size=(1, 3)), len(F), axis=0))
             off += len(V)
             k += 1
     V = np.concatenate(Vs)
     F = np.concatenate(Fs)
-    kd = rng.uniform(0.1, 0.9, size=(len(F), 3)).astype(np.float32)
+    kd = np.concatenate(kds).astype(np.float32)
     mesh = mesh_prims(V, F, kd)
     L = lights(((-5.0, 8.0, -4.0), (140.0, 140.0, 140.0)), ((6.0, 6.0, 1.0), (90.0, 80.0, 70.0)))
     cam = orbit_camera((0.0, -1.0, -7.0), 13.0, 2.8, angle_deg, width, height)
@@ -325,7 +329,7 @@ def reference_room(width=64, height=64, subdiv=2, seed=5) -> Scene:
         sphere_prim((1.8, 1.0, -4.0), 0.3, emission=(6.0, 5.0, 4.0)),
     ])
     V, F = displaced_icosphere(subdiv, (-0.6, -1.3, -2.2), 0.6, 0.1, seed)
-    kd = rng.uniform(0.2, 0.8, size=(len(F), 3)).astype(np.float32)
+    kd = np.repeat(rng.uniform(0.2, 0.8, size=(1, 3)), len(F), axis=0).astype(np.float32)
     mesh = mesh_prims(V, F, kd)
     L = lights(((0.0, -0.23, -2.0), (70.0, 70.0, 70.0)))
     cam = make_camera((0.0, -0.75, 4.25), (0.0, -0.75, 0.0), width=width, height=height)

@@ -101,3 +101,15 @@ class CImagenGPU(ctypes.Structure):
 
 
 assert ctypes.sizeof(CTinyBVHD_GPU) == 24 and ctypes.sizeof(CImagenGPU) == 16
+
+
+class CNrcFrameConfig(ctypes.Structure):
+    _fields_ = [("train_steps", ctypes.c_int32), ("max_records", ctypes.c_uint32), ("min_records", ctypes.c_uint32),
+                ("warmup", ctypes.c_int32), ("gate_threshold", ctypes.c_float), ("use_graph", ctypes.c_int32)]
+
+
+class CNrcBuffers(ctypes.Structure):
+    _fields_ = [("img", ctypes.c_void_p), ("accum", ctypes.c_void_p), ("infer", ctypes.c_void_p),
+                ("thr", ctypes.c_void_p), ("regs", ctypes.c_void_p), ("counter", ctypes.c_void_p),
+                ("ring_cap", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("tail_in", ctypes.c_void_p),
+                ("tail_pred", ctypes.c_void_p), ("train_buf", ctypes.c_void_p)]
