@@ -248,6 +248,29 @@ int tfgRenderPass(
     TfgDatosMLP* buffer_inference, TfgColor* buffer_throughput,
     int32_t usar_red_inferencia, int32_t entrenar_red, void* stream);
 
+/* tfgRenderPass without any device allocation -- no counterpart in the
+ * reference.  For callers that cannot allocate device memory (code running
+ * while another thread captures a CUDA graph in global mode, engines that
+ * give the library a fixed memory budget, real-time threads that must not
+ * block on the allocator).  The wavefront queues and path state live in a
+ * static device array of ~3.7 MB that the library reserves on every GPU that
+ * loads it, until the process exits; images are limited to 16384 pixels
+ * (e.g. 128 x 128) and plain path tracing (no cache queries or training
+ * records) -- larger images return TFG_E_INVALID.  The first call on a device
+ * looks up the array's device address; make that first call before any
+ * stream capture.  All calls share the one array, which keeps the last call's
+ * contents: calls that overlap on the GPU (different streams, or concurrent
+ * host threads) race and must be serialised by the caller.  `accum` is used
+ * when params->accumulate is set; params->profile must be 0. */
+int tfgRenderPassStatic(
+    const TfgRenderParams* params,
+    const TfgCamara* camara, const TfgPrimitiva* primitivas, int32_t num_primitivas,
+    const TfgLuzPuntual* luces, int32_t num_luces,
+    int32_t ancho_img, int32_t alto_img, int32_t frame_number,
+    const TfgTinyBVHD_GPU* nodos_bvh, const float* tris_wt,
+    const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh,
+    const TfgImagenGPU* imagen_directa, float* accum, void* stream);
+
 /* Closest-hit traversal of `n` rays (primary-ray mode).  rays: 8 floats per
  * ray (O.x, O.y, O.z, t_max, D.x, D.y, D.z, unused).  hits: 4 floats per ray
  * (t, u, v, prim id bits); a miss returns t = t_max and id 0xFFFFFFFF.  This

@@ -48,6 +48,9 @@ _PROTOS = {
         POINTER(CRenderParams), c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32,
         POINTER(CTinyBVHD_GPU), c_void_p, c_void_p, c_int32, POINTER(CImagenGPU), c_void_p, c_void_p, c_void_p,
         c_int32, c_void_p, c_void_p, c_int32, c_int32, c_void_p]),
+    "tfgRenderPassStatic": (c_int32, [
+        POINTER(CRenderParams), c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32,
+        POINTER(CTinyBVHD_GPU), c_void_p, c_void_p, c_int32, POINTER(CImagenGPU), c_void_p, c_void_p]),
     "tfgTraceRays": (c_int32, [POINTER(CTinyBVHD_GPU), c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_void_p]),
     "tfgGenerateCameraRays": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
     "tfgLaunchInicializarCamara": (c_int32, [c_void_p, c_int32, c_int32, c_void_p]),

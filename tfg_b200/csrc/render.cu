@@ -667,6 +667,9 @@ int profile_get(TfgRenderProfile* out) {
     return ok();
 }
 
+int enqueue_pass(PassArgs a, const TfgRenderParams& prm, int frame, TfgColor* img, const LaunchShapes& sh,
+                 cudaStream_t stream);
+
 int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
                 const TfgLuzPuntual* lights, int nlights, int W, int H, int frame, const TfgTinyBVHD_GPU* bvh,
                 const float* tris_wt, const TfgPrimitiva* mesh, int nmesh, TfgColor* img, float* accum,
@@ -722,8 +725,18 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
     a.infer = infer; a.thr_out = thr_out; a.use_inf = use_inf; a.train = train;
     a.max_depth = prm.max_depth; a.rr_min_depth = prm.rr_min_depth; a.shadow_mesh = prm.shadow_mesh;
     a.ws = ws;
+    return enqueue_pass(a, prm, frame, img, sh, stream);
+}
+
+// The launch sequence of one call: `prm.spp` samples, each generate ->
+// (trace -> shade -> shadow) x max_depth -> resolve, on the workspace in `a.ws`.
+int enqueue_pass(PassArgs a, const TfgRenderParams& prm, int frame, TfgColor* img, const LaunchShapes& sh,
+                 cudaStream_t stream) {
+    const int W = a.W, H = a.H;
     const int fmt = prm.tri_format;
-    const size_t smem = trace_smem(nprims);
+    const size_t smem = trace_smem(a.nprims);
+    const Workspace& ws = a.ws;
+    cudaError_t e = cudaSuccess;
     const int gen_blocks = std::max(1, std::min((W * H + 255) / 256, sh.sms * 8));
     const bool times = (prm.profile & TFG_PROFILE_TIMES) != 0;
     const bool counts = (prm.profile & TFG_PROFILE_COUNTS) != 0;
@@ -934,4 +947,107 @@ extern "C" int tfgTraceRays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, in
 extern "C" int tfgGenerateCameraRays(const TfgCamara* camara, int32_t ancho_img, int32_t alto_img, int32_t frame_number,
                                      float* rays, void* stream) {
     return tfg::camera_rays(camara, ancho_img, alto_img, frame_number, rays, (cudaStream_t)stream);
+}
+
+// ------------------------------------------------------------------ allocation-free render pass
+// Some callers cannot allocate device memory at all: code running while
+// another thread captures a CUDA graph in global mode (cudaMalloc is illegal
+// then), engines that hand the library a fixed memory budget and forbid
+// allocations behind their back, and real-time threads that must never block
+// on the allocator.  tfgRenderPassStatic serves them: the wavefront queues
+// and path state live in this file-scope array, which the library image
+// reserves on every GPU that loads it, for the life of the process.
+namespace tfg {
+namespace {
+
+constexpr size_t kStaticPaths = 128 * 128;
+constexpr size_t kStaticCounters = 4 * (kMaxBounces + 1) * sizeof(uint32_t);
+// Per path: 2 ray queues (32 B each), hit (16 B), shadow item (64 B),
+// throughput, state, prefix and suffix radiance, footprint (16 B each).
+constexpr size_t kStaticPathBytes = 2 * 32 + 16 + 64 + 5 * 16;
+constexpr size_t kStaticBytes = kStaticPaths * kStaticPathBytes + kStaticCounters;
+
+static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
+
+std::mutex g_static_mutex;
+unsigned char* g_static_base[16] = {nullptr};
+
+// Device address of g_static_scratch for the current device, looked up once
+// per device (the array's name is only a host-side stand-in in host code).
+int static_scratch(int dev, unsigned char** out) {
+    std::lock_guard<std::mutex> lk(g_static_mutex);
+    if (!g_static_base[dev & 15]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
+        if (e != cudaSuccess) return fail((int)e, std::string("tfgRenderPassStatic: scratch address: ") + cudaGetErrorString(e));
+        g_static_base[dev & 15] = static_cast<unsigned char*>(p);
+    }
+    *out = g_static_base[dev & 15];
+    return ok();
+}
+
+}  // namespace
+}  // namespace tfg
+
+extern "C" int tfgRenderPassStatic(const TfgRenderParams* params, const TfgCamara* camara,
+                                   const TfgPrimitiva* primitivas, int32_t num_primitivas, const TfgLuzPuntual* luces,
+                                   int32_t num_luces, int32_t ancho_img, int32_t alto_img, int32_t frame_number,
+                                   const TfgTinyBVHD_GPU* nodos_bvh, const float* tris_wt,
+                                   const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh,
+                                   const TfgImagenGPU* imagen_directa, float* accum, void* stream) {
+    using namespace tfg;
+    if (!params) return fail(TFG_E_INVALID, "tfgRenderPassStatic: params is null");
+    const TfgRenderParams& prm = *params;
+    if (ancho_img <= 0 || alto_img <= 0 || (size_t)ancho_img * (size_t)alto_img > kStaticPaths)
+        return fail(TFG_E_INVALID, "tfgRenderPassStatic: image larger than the 16384-pixel (128 x 128) static scratch");
+    if (!camara) return fail(TFG_E_INVALID, "tfgRenderPassStatic: camara is null");
+    if (num_primitivas < 0 || num_luces < 0 || num_prims_bvh < 0) return fail(TFG_E_INVALID, "tfgRenderPassStatic: negative count");
+    if ((num_primitivas > 0 && !primitivas) || (num_luces > 0 && !luces))
+        return fail(TFG_E_INVALID, "tfgRenderPassStatic: null scene array");
+    if (prm.max_depth < 1 || prm.max_depth > kMaxBounces) return fail(TFG_E_INVALID, "tfgRenderPassStatic: max_depth out of [1,64]");
+    if (prm.spp < 1) return fail(TFG_E_INVALID, "tfgRenderPassStatic: spp < 1");
+    if (prm.tri_format != TFG_TRIS_REF && prm.tri_format != TFG_TRIS_WATERTIGHT)
+        return fail(TFG_E_INVALID, "tfgRenderPassStatic: unknown tri_format");
+    if (prm.profile != 0) return fail(TFG_E_INVALID, "tfgRenderPassStatic: profiling is not available here");
+    const bool has_bvh = nodos_bvh && nodos_bvh->d_nodos && nodos_bvh->d_tris && num_prims_bvh > 0;
+    if (has_bvh && !primitivas_bvh) return fail(TFG_E_INVALID, "tfgRenderPassStatic: mesh primitives are null");
+    if (has_bvh && prm.tri_format == TFG_TRIS_WATERTIGHT && !tris_wt)
+        return fail(TFG_E_INVALID, "tfgRenderPassStatic: watertight format needs tris_wt");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    if (int rc = require_sm100(dev)) return rc;
+    unsigned char* base = nullptr;
+    if (int rc = static_scratch(dev, &base)) return rc;
+    LaunchShapes sh;
+    shapes_for(dev, sh);
+    // Carve the scratch: queues first, then per-path state, counters last.
+    const size_t P = kStaticPaths;
+    Workspace ws;
+    ws.cap = P;
+    ws.ray[0] = reinterpret_cast<float4*>(base);
+    ws.ray[1] = ws.ray[0] + 2 * P;
+    ws.hit = ws.ray[1] + 2 * P;
+    ws.shadow = ws.hit + P;
+    ws.thr = ws.shadow + 4 * P;
+    ws.st = reinterpret_cast<uint4*>(ws.thr + P);
+    ws.lpre = reinterpret_cast<float4*>(ws.st + P);
+    ws.lsuf = ws.lpre + P;
+    ws.nrc = ws.lsuf + P;
+    ws.ts = nullptr;
+    ws.counters = reinterpret_cast<uint32_t*>(ws.nrc + P);
+    PassArgs a{};
+    a.prims = primitivas; a.nprims = num_primitivas; a.lights = luces; a.nlights = num_luces;
+    a.nodes = has_bvh ? reinterpret_cast<const float4*>(nodos_bvh->d_nodos) : nullptr;
+    a.tris = has_bvh ? reinterpret_cast<const float4*>(prm.tri_format == TFG_TRIS_REF ? nodos_bvh->d_tris : tris_wt)
+                     : nullptr;
+    a.has_bvh = has_bvh ? 1 : 0;
+    a.mesh = primitivas_bvh; a.nmesh = num_prims_bvh;
+    a.cam = camara;
+    a.W = ancho_img; a.H = alto_img;
+    a.accum = prm.accumulate ? accum : nullptr;
+    a.max_depth = prm.max_depth; a.rr_min_depth = prm.rr_min_depth; a.shadow_mesh = prm.shadow_mesh;
+    a.ws = ws;
+    return enqueue_pass(a, prm, frame_number, imagen_directa ? imagen_directa->datos : nullptr, sh,
+                        (cudaStream_t)stream);
 }

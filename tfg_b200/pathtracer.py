@@ -138,6 +138,18 @@ def render_pass(ds: DeviceScene, params: RenderParams, frame: int, img: torch.Te
               int(use_inf), int(train), _stream(stream))
 
 
+def render_pass_static(ds: DeviceScene, params: RenderParams, frame: int, img: torch.Tensor | None = None,
+                       accum: torch.Tensor | None = None, stream=None) -> None:
+    """tfgRenderPassStatic: the same pass with no device allocation (plain path
+    tracing, at most 16384 pixels; calls must not overlap on the GPU)."""
+    W, H = ds.scene.width, ds.scene.height
+    im = CImagenGPU(W, H, img.data_ptr() if img is not None else None)
+    _lib.call("tfgRenderPassStatic", ctypes.byref(params.c()),
+              _ptr(ds.camera), _ptr(ds.prims), ds.n_prims, _ptr(ds.lights), ds.n_lights, W, H, frame,
+              ctypes.byref(ds.bvh.ref), ds.bvh.d_tris_wt, ds.bvh.d_primitivas, ds.n_mesh, ctypes.byref(im),
+              _ptr(accum), _stream(stream))
+
+
 def camera_rays(ds: DeviceScene, frame: int, rays: torch.Tensor, stream=None) -> None:
     W, H = ds.scene.width, ds.scene.height
     _lib.call("tfgGenerateCameraRays", _ptr(ds.camera), W, H, frame, _ptr(rays), _stream(stream))
