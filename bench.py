@@ -170,6 +170,124 @@ def reference_arm(args):
     }))
 
 
+def nrc_eval(scene, ds, dev, ref_spp: int = 1024, frames: int = 300) -> dict:
+    """Online radiance caching at 1920x1080 (1 spp per frame, camera orbiting
+    1 degree per frame, 4 x 16384 training samples per frame after the
+    reference's 48 warm-up frames) against plain path tracing at equal GPU
+    time.  Both are scored by relMSE against a `ref_spp` plain path-traced
+    image of the final camera pose, accumulated in FP64 (64-sample FP32
+    batches summed in FP64)."""
+    import numpy as np
+    import torch
+
+    from tfg_b200 import pathtracer as pt
+    from tfg_b200 import scenes as sc
+    from tfg_b200.nrc import ColorMLP, NrcRenderer
+
+    params = pt.RenderParams(max_depth=DEPTH, rr_min_depth=RR, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT)
+    mlp = ColorMLP(batch=16384, seed=2024)
+    mlp.set_bounds(*scene.bounds)
+    r = NrcRenderer(ds, mlp, params, train_steps=4, use_graph=True)
+
+    def set_pose(k):
+        cam = sc.orbit_camera((0.0, -1.0, -7.0), 13.0, 2.8, float(k), W_PX, H_PX)
+        ds.camera.copy_(torch.from_numpy(cam.view("u1").copy()).to(dev), non_blocking=False)
+
+    for f in range(48):
+        with torch.cuda.stream(r.stream):
+            set_pose(0)
+        r.frame(f, warmup=True, accumulate=False)
+    for k in range(frames):
+        with torch.cuda.stream(r.stream):
+            set_pose(k)
+        r.frame(48 + k, accumulate=False)
+    r.stream.synchronize()
+    # time cache frames and plain passes at the final pose
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(r.stream)
+    for k in range(10):
+        r.frame(10_000 + k, accumulate=False)
+    e1.record(r.stream)
+    e1.synchronize()
+    t_nrc = e0.elapsed_time(e1) / 10
+    nrc_img = r.image().cpu().numpy().astype(np.float64)
+    img = torch.zeros(W_PX * H_PX * 3, dtype=torch.float32, device=dev)
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record()
+    for k in range(10):
+        pt.render_pass(ds, params, 20_000 + k, img)
+    p1.record()
+    p1.synchronize()
+    t_pt = p0.elapsed_time(p1) / 10
+    spp_eq = max(1, int(round(t_nrc / t_pt)))
+    plain = pt.accumulate_spp(ds, params, spp_eq, 30_000).cpu().numpy().astype(np.float64)
+    ref = np.zeros_like(plain)
+    for b in range(ref_spp // 64):
+        ref += pt.accumulate_spp(ds, params, 64, 1_000_000 + 64 * b).cpu().numpy().astype(np.float64)
+    ref /= ref_spp // 64
+
+    def rel(x):
+        return float(np.mean((x - ref) ** 2 / (ref ** 2 + 1e-2)))
+
+    e_nrc, e_pt = rel(nrc_img), rel(plain)
+    # plain path tracing is unbiased: relMSE x time is its equal-time figure of merit
+    ratio_time = (e_pt * t_pt * spp_eq) / (e_nrc * t_nrc)
+    st = mlp.state()
+    # MLP inference throughput on the frame's 2.07M cache queries
+    n = W_PX * H_PX
+    out = torch.zeros(n * 3, dtype=torch.float32, device=dev)
+    for _ in range(3):
+        mlp.inference(r.infer, out, n)
+    torch.cuda.synchronize()
+    q0, q1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    q0.record()
+    for _ in range(10):
+        mlp.inference(r.infer, out, n)
+    q1.record()
+    q1.synchronize()
+    t_inf = q0.elapsed_time(q1) / 10
+    flops = 2.0 * (96 * 64 + 4 * 64 * 64 + 64 * 16) * n
+    mlp.close()
+    return {
+        "frames": 48 + frames, "warmup_frames": 48, "camera": "orbit 1 deg/frame", "train_samples_per_frame": 4 * 16384,
+        "ms_per_frame_nrc": round(t_nrc, 3), "ms_per_pass_plain_1spp": round(t_pt, 3),
+        "plain_spp_at_equal_time": spp_eq, "relmse_nrc": round(e_nrc, 5), "relmse_plain": round(e_pt, 5),
+        "relmse_ratio_plain_over_nrc": round(e_pt / e_nrc, 3), "relmse_x_time_ratio": round(ratio_time, 3),
+        "reference_spp": ref_spp, "adam_steps": int(st["adam_t"]), "loss_ema": round(st["loss_ema"], 5),
+        "mlp_inference": {"queries": n, "ms": round(t_inf, 4), "tflops": round(flops / (t_inf * 1e-3) / 1e12, 2),
+                          "flops_per_query": int(flops / n)},
+    }
+
+
+def profile_mlp():
+    """Cache inference over 2,073,600 queries (232 MB of DatosMLP, more than
+    L2) and one 16384-sample train step, untimed; used for ncu captures."""
+    import numpy as np
+    import torch
+
+    from tfg_b200.nrc import ColorMLP
+    from tfg_b200.structs import DATOS_MLP
+    n = W_PX * H_PX
+    rng = np.random.default_rng(0)
+    d = np.zeros(n, DATOS_MLP)
+    for k in "xyz":
+        d["posicion"][k] = rng.uniform(-5, 5, n)
+        d["direccion"][k] = rng.uniform(0, 1, n)
+        d["normal"][k] = rng.uniform(0, 1, n)
+    for k in "rgb":
+        d["difuso"][k] = rng.uniform(0, 1, n)
+        d["color"][k] = rng.uniform(0, 2, n)
+    dd = torch.from_numpy(d.view(np.uint8).copy()).cuda()
+    m = ColorMLP(batch=16384, seed=1)
+    m.set_bounds((-6, -6, -6), (6, 6, 6))
+    out = torch.zeros(n * 3, device="cuda")
+    m.inference(dd, out, n)
+    m.train_step(dd, n, read_loss=False)
+    torch.cuda.synchronize()
+    m.close()
+    print("profile mlp done")
+
+
 def profile_pass():
     """One 1-spp pass (8 bounces) of the benchmark frame: ~0.3 GB of scene
     data (more than L2) and ~0.5 GB of queues; used for ncu captures."""
@@ -195,14 +313,20 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache evaluation")
     ap.add_argument("--profile-pass", action="store_true",
                     help="run one untimed 1-spp pass of the workload and exit (small case for ncu)")
+    ap.add_argument("--profile-mlp", action="store_true",
+                    help="run cache inference on 1920x1080 queries and one train step, then exit (case for ncu)")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
         return
     if args.profile_pass:
         profile_pass()
+        return
+    if args.profile_mlp:
+        profile_mlp()
         return
 
     import torch
@@ -304,6 +428,13 @@ def main():
             dist.destroy_process_group()
         return
 
+    nrc = None
+    if not args.no_nrc and world == 1:
+        nrc = nrc_eval(scene, ds, dev)
+        bf16 = json.loads((ROOT / "MEASURED_PEAKS.json").read_text()).get("bf16_tflops") if (ROOT / "MEASURED_PEAKS.json").exists() else 1590.0
+        nrc["mlp_inference"]["frac_of_dense_f16_peak"] = round(nrc["mlp_inference"]["tflops"] / bf16, 4)
+        nrc["mlp_inference"]["peak_tflops"] = bf16
+
     pk = peaks()
     trace_ms = prof["ms"]["trace"]
     trace_launches = prof["launches"]["trace"]
@@ -350,6 +481,7 @@ def main():
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
+        "nrc": nrc,
     }
     print(json.dumps(out))
     ds.close()
