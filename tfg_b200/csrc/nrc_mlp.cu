@@ -47,7 +47,6 @@ namespace tfg {
 namespace mlp {
 
 constexpr int kTile = 128;
-constexpr int kIn = 96;          // encoded features
 constexpr int kHid = 64;
 constexpr int kLayers = 6;       // 96->64, 4 x 64->64, 64->16 (3 used)
 constexpr int kOutPad = 16;
@@ -183,124 +182,249 @@ __device__ __forceinline__ float scrub(float c) {
 __device__ __forceinline__ bool all_ok(bool ok) { return __syncthreads_and(ok ? 1 : 0) != 0; }
 
 // ------------------------------------------------------------------ inference
-// Shared memory: weights 51200 | input tile 14336 | A 32768 (two regions).
-constexpr int kInferSmemW = 0;
-constexpr int kInferSmemX = 51200;
-constexpr int kInferSmemA = 51200 + 14336 + 1024;   // 1024-aligned: 66560
-constexpr int kInferSmem = kInferSmemA + 2 * kTile * 128;   // 99328
+// Persistent kernel, one CTA per SM.  The CTA runs kSlots tiles of 128
+// queries at a time; each tile ("slot") has its own 128 TMEM columns (64 FP32
+// accumulator columns, then the FP16 A operand of the next layer, two features
+// per column), its own input staging buffer, MMA mbarrier and named barrier,
+// and is served by kSplit warpgroups: thread t of every warpgroup of the slot
+// owns row t (TMEM lane t).  With two warpgroups, the first encodes the x and y
+// bands and converts accumulator columns 0..31, the second encodes the z bands
+// and the other inputs and converts columns 32..63, which halves the
+// per-layer latency chain (MMA -> TMEM load -> ReLU/pack -> TMEM store ->
+// barrier -> next MMA) each tile walks through.  Only the weights (51,200 B,
+// bulk-copied once) and the staged inputs live in shared memory, so the
+// tensor pipe reads B from shared memory and A from TMEM.
+#ifndef TFG_INFER_SPLIT
+#define TFG_INFER_SPLIT 1
+#endif
+#ifndef TFG_INFER_SLOTS
+#define TFG_INFER_SLOTS 4
+#endif
+constexpr int kSplit = TFG_INFER_SPLIT;
+constexpr int kSlots = TFG_INFER_SLOTS;
+constexpr int kSlotThreads = 128 * kSplit;
+constexpr int kInferThreads = kSlotThreads * kSlots;
+constexpr int kRowBytes = (int)sizeof(TfgDatosMLP);              // 112
+constexpr int kStageBytes = kTile * kRowBytes;                   // 14336
+constexpr int kInferSmemStage = 51200 + 1024;
+constexpr int kInferSmem = kInferSmemStage + kSlots * kStageBytes;
+static_assert(kSplit == 1 || kSplit == 2, "one or two warpgroups per tile");
+static_assert(kSlots * 128 <= 512, "TMEM: 128 columns per slot");
+static_assert(kInferThreads <= 1024, "threads per CTA");
+static_assert(kInferSmem + 1024 <= 227 * 1024, "inference shared memory");
 
-__global__ void __launch_bounds__(128) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
-                                               const uint32_t* __restrict__ n_dev, Bounds bounds,
-                                               const uint8_t* __restrict__ wimg, TfgColor* __restrict__ out,
-                                               TfgColor* __restrict__ img, const TfgColor* __restrict__ thr) {
+__device__ __forceinline__ void slot_sync(int id) {
+    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(kSlotThreads) : "memory");
+}
+
+// AND of `p` over the slot's threads (all of them get the result).
+__device__ __forceinline__ bool slot_all(int id, bool p) {
+    uint32_t r;
+    asm volatile(
+        "{\n\t.reg .pred pi, po;\n\t"
+        "setp.ne.u32 pi, %1, 0;\n\t"
+        "bar.red.and.pred po, %2, %3, pi;\n\t"
+        "selp.u32 %0, 1, 0, po;\n\t}\n"
+        : "=r"(r)
+        : "r"((uint32_t)p), "r"(id), "n"(kSlotThreads)
+        : "memory");
+    return r != 0;
+}
+
+// max(x, 0) of two floats packed as FP16x2 (ReLU fused into the conversion).
+__device__ __forceinline__ uint32_t relu_h2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+
+// 12 frequency bands of one position coordinate (already mapped to [0,1]):
+// (sin, cos)(2^k pi p) as FP16 pairs, double-angle recurrence from a hardware
+// sin/cos of the base band.
+__device__ __forceinline__ void encode_axis(float p, uint32_t* w) {
+    float s, c;
+    __sincosf(kPiF * p, &s, &c);
+#pragma unroll
+    for (int k = 0; k < kBands; ++k) {
+        w[k] = pack_h2(s, c);
+        const float s2 = 2.0f * s * c;
+        const float c2 = (c - s) * (c + s);
+        s = s2;
+        c = c2;
+    }
+}
+
+// Encoded features 0..47 (FP16 pairs) of a staged row: words 0..23 are the x
+// and y bands, 24..35 the z bands, 36..42 direction, normal, albedos and the
+// constant 1, 43..47 zero.  `part` 0 writes words 0..23, part 1 words 24..47,
+// part -1 all of them, into TMEM columns of the same index.
+__device__ __forceinline__ void encode_to_tmem(const TfgDatosMLP* r, const Bounds& b, int part, uint32_t ta) {
+    if (part <= 0) {
+        uint32_t w[24];
+        encode_axis(unit_clamp((float)r->posicion.x, b.lo[0], b.hi[0]), w);
+        encode_axis(unit_clamp((float)r->posicion.y, b.lo[1], b.hi[1]), w + 12);
+        umma::tmem_st16(ta, *reinterpret_cast<const uint32_t(*)[16]>(w));
+        umma::tmem_st8(ta + 16u, w + 16);
+    }
+    if (part != 0) {
+        uint32_t w[24];
+        encode_axis(unit_clamp((float)r->posicion.z, b.lo[2], b.hi[2]), w);
+        w[12] = pack_h2((float)r->direccion.x, (float)r->direccion.y);
+        w[13] = pack_h2((float)r->direccion.z, (float)r->normal.x);
+        w[14] = pack_h2((float)r->normal.y, (float)r->normal.z);
+        w[15] = pack_h2(r->difuso.r, r->difuso.g);
+        w[16] = pack_h2(r->difuso.b, r->especular.r);
+        w[17] = pack_h2(r->especular.g, r->especular.b);
+        w[18] = pack_h2(1.0f, 0.0f);
+#pragma unroll
+        for (int k = 19; k < 24; ++k) w[k] = 0u;
+        umma::tmem_st8(ta + 24u, w);
+        umma::tmem_st16(ta + 32u, *reinterpret_cast<const uint32_t(*)[16]>(w + 8));
+    }
+}
+
+__global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
+                                                            const uint32_t* __restrict__ n_dev, Bounds bounds,
+                                                            const uint8_t* __restrict__ wimg,
+                                                            TfgColor* __restrict__ out, TfgColor* __restrict__ img,
+                                                            const TfgColor* __restrict__ thr) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* sw = smem + kInferSmemW;
-    uint8_t* sx = smem + kInferSmemX;
-    uint8_t* sa = smem + kInferSmemA;
-    __shared__ uint64_t mb_w, mb_x, mb_mma;
+    uint8_t* sw = smem;
+    __shared__ uint64_t mb_w, mb_mma[kSlots], mb_in[kSlots];
     __shared__ uint32_t tslot;
-    const int t = threadIdx.x, warp = t >> 5;
+    const int tid = threadIdx.x, warp = tid >> 5, q = warp & 3, t = tid & 127;
+    const int slot = tid / kSlotThreads;
+    const int part = kSplit == 1 ? -1 : (tid / 128) % kSplit;     // warpgroup within the slot
+    const bool leader = tid % kSlotThreads == 0;
+    const bool issuer_warp = tid % kSlotThreads < 32;             // first warp of the slot issues its MMAs
+    const int bar = 1 + slot;
+    uint8_t* stage = smem + kInferSmemStage + slot * kStageBytes;
     const uint32_t n = n_dev ? min(*n_dev, n_max) : n_max;
     const uint32_t ntiles = (n + kTile - 1) / kTile;
-    if (blockIdx.x >= ntiles) return;
-    if (warp == 0) umma::tmem_alloc(&tslot, 128);
-    if (t == 0) {
+    if (blockIdx.x * kSlots >= ntiles) return;
+    if (warp == 0) umma::tmem_alloc(&tslot, 512);
+    if (tid == 0) {
         umma::mbar_init(&mb_w, 1);
-        umma::mbar_init(&mb_x, 1);
-        umma::mbar_init(&mb_mma, 1);
+        for (int k = 0; k < kSlots; ++k) {
+            umma::mbar_init(&mb_mma[k], 1);
+            umma::mbar_init(&mb_in[k], 1);
+        }
         umma::mbar_fence_init();
-    }
-    // Region 1 chunks 4..7 (features 96..127) are never written: zero them once.
-    for (int i = t; i < kTile * 4; i += blockDim.x) {
-        const int r = i >> 2, c = 4 + (i & 3);
-        *reinterpret_cast<uint4*>(sa + kTile * 128 + umma::sw128_offset(r, c)) = make_uint4(0, 0, 0, 0);
     }
     __syncthreads();
     umma::fence_after_sync();
-    const uint32_t tmem = tslot;
-    if (t == 0) {
+    const uint32_t tlane = (uint32_t)(32 * q) << 16;
+    const uint32_t tmem = tslot + 128u * (uint32_t)slot;          // accumulator: columns 0..63 of the slot
+    const uint32_t tmem_a = tmem + 64u;                            // A operand: columns 64..111
+    const uint32_t tstride = gridDim.x * kSlots;
+    const uint64_t wdesc = umma::sdesc_sw128(umma::smem_u32(sw));
+    // Bulk copy of tile `tl`'s rows (a multiple of 16 bytes from a 16-byte
+    // aligned source) into the slot's staging buffer.
+    auto fetch = [&](uint32_t tl) {
+        const uint32_t rows = min((uint32_t)kTile, n - tl * kTile);
+        umma::mbar_expect_tx(&mb_in[slot], rows * kRowBytes);
+        umma::bulk_g2s(stage, reinterpret_cast<const uint8_t*>(in) + (size_t)tl * kStageBytes, rows * kRowBytes,
+                       &mb_in[slot]);
+    };
+    if (tid == 0) {
         umma::mbar_expect_tx(&mb_w, kFwdBytes);
         umma::bulk_g2s(sw, wimg, kFwdBytes, &mb_w);
-        const uint32_t tile = blockIdx.x;
-        const uint32_t rows = min((uint32_t)kTile, n - tile * kTile);
-        umma::mbar_expect_tx(&mb_x, rows * (uint32_t)sizeof(TfgDatosMLP));
-        umma::bulk_g2s(sx, in + (size_t)tile * kTile, rows * (uint32_t)sizeof(TfgDatosMLP), &mb_x);
     }
+    uint32_t tile = blockIdx.x * kSlots + slot;
+    bool pending = tile < ntiles;
+    if (pending && leader) fetch(tile);
     bool ok = umma::mbar_wait(&mb_w, 0, kSpinLimit);
-    uint32_t xph = 0, mph = 0;
-    for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    uint32_t mph = 0, iph = 0;
+    for (; tile < ntiles && ok; tile += tstride) {
         const uint32_t row = tile * kTile + (uint32_t)t;
         const bool valid = row < n;
-        ok = all_ok(umma::mbar_wait(&mb_x, xph, kSpinLimit));
-        xph ^= 1u;
+        ok = slot_all(bar, umma::mbar_wait(&mb_in[slot], iph, kSpinLimit));
         if (!ok) break;
-        {
-            uint32_t w[48];
-            TfgDatosMLP d;
-            if (valid) d = reinterpret_cast<const TfgDatosMLP*>(sx)[t];
-            else memset(&d, 0, sizeof(d));
-            encode(d, bounds, w);
-            store_encoded(sa, t, w);
-        }
-        umma::fence_smem_to_async();
-        __syncthreads();
-        if (t == 0) {
-            const uint32_t next = tile + gridDim.x;
-            if (next < ntiles) {
-                // The input tile is consumed; prefetch the next one during the GEMM chain.
-                const uint32_t rows = min((uint32_t)kTile, n - next * kTile);
-                umma::mbar_expect_tx(&mb_x, rows * (uint32_t)sizeof(TfgDatosMLP));
-                umma::bulk_g2s(sx, in + (size_t)next * kTile, rows * (uint32_t)sizeof(TfgDatosMLP), &mb_x);
+        pending = false;
+        iph ^= 1u;
+        // rows past the end of a partial tile encode stale staging bytes; the
+        // rows of the MLP are independent and those outputs are never stored
+        encode_to_tmem(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds, part, tmem_a + tlane);
+        umma::tmem_wait_st();
+        umma::fence_before_sync();
+        slot_sync(bar);   // staging buffer consumed, A operand of layer 0 in TMEM
+        if (tile + tstride < ntiles) {
+            if (leader) {
+                umma::fence_smem_to_async();
+                fetch(tile + tstride);
             }
+            pending = true;
         }
-        for (int l = 0; l < kLayers && ok; ++l) {
-            const int K = kCols(l), N = (l == kLayers - 1) ? kOutPad : kHid;
-            const uint32_t dcol = (l == kLayers - 1) ? 64u : 0u;
-            if (t == 0) {
+        // Fully unrolled: every descriptor is the weights' base descriptor plus
+        // an immediate (the start-address field holds address / 16), so the
+        // issuing thread runs no descriptor arithmetic between MMAs.
+#pragma unroll
+        for (int l = 0; l < kLayers; ++l) {
+            const bool last = l == kLayers - 1;
+            if (issuer_warp) {
                 umma::fence_after_sync();
-                issue_layer(tmem + dcol, sa, kTile * 128, sw + kFOff(l), kRows(l) * 128, K, N, false);
-                umma::mma_commit(&mb_mma);
+                constexpr uint32_t id_hid = umma::idesc_f16(kTile, kHid, false);
+                constexpr uint32_t id_out = umma::idesc_f16(kTile, kOutPad, false);
+                if (umma::elect_one()) {
+#pragma unroll
+                    for (int s = 0; s < kCols(l) / 16; ++s) {
+                        const uint64_t bd =
+                            wdesc + (uint64_t)((kFOff(l) + (s >> 2) * (kRows(l) * 128) + (s & 3) * 32) >> 4);
+                        umma::mma_f16_ta(tmem, tmem_a + 8u * s, bd, last ? id_out : id_hid, s > 0);
+                    }
+                    umma::mma_commit(&mb_mma[slot]);
+                }
+                __syncwarp();
             }
-            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+            ok = slot_all(bar, umma::mbar_wait(&mb_mma[slot], mph, kSpinLimit));
             mph ^= 1u;
             if (!ok) break;
             umma::fence_after_sync();
-            if (l < kLayers - 1) {
-                float v[64];
-                tmem_row64(tmem, warp, 0, v);
+            if (!last) {
 #pragma unroll
-                for (int i = 0; i < 64; ++i) v[i] = fmaxf(v[i], 0.0f);
-                store_row64<false>(sa, t, v);
+                for (int h = 0; h < 2; ++h) {
+                    if (kSplit == 2 && h != part) continue;
+                    float v[32];
+                    umma::tmem_ld32(tmem + tlane + 32u * h, v);
+                    uint32_t r[16];
+#pragma unroll
+                    for (int i = 0; i < 16; ++i) r[i] = relu_h2(v[2 * i], v[2 * i + 1]);
+                    umma::tmem_st16(tmem_a + tlane + 16u * h, r);
+                }
+                umma::tmem_wait_st();
                 umma::fence_before_sync();
-                umma::fence_smem_to_async();
-                __syncthreads();
+                slot_sync(bar);
             } else {
-                float v[16];
-                umma::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + 64u, v);
-                umma::fence_before_sync();
-                if (valid) {
-                    const float r = scrub(v[0]), g = scrub(v[1]), b = scrub(v[2]);
-                    if (img) {
-                        const TfgColor th = thr[row];
-                        if (th.r > 0 || th.g > 0 || th.b > 0) {
-                            TfgColor f = img[row];
-                            f.r = f.r + th.r * r;
-                            f.g = f.g + th.g * g;
-                            f.b = f.b + th.b * b;
-                            img[row] = f;
+                if (part <= 0) {
+                    float v[16];
+                    umma::tmem_ld16(tmem + tlane, v);
+                    if (valid) {
+                        const float cr = scrub(v[0]), cg = scrub(v[1]), cb = scrub(v[2]);
+                        if (img) {
+                            const TfgColor th = thr[row];
+                            if (th.r > 0 || th.g > 0 || th.b > 0) {
+                                TfgColor f = img[row];
+                                f.r = f.r + th.r * cr;
+                                f.g = f.g + th.g * cg;
+                                f.b = f.b + th.b * cb;
+                                img[row] = f;
+                            }
+                        } else {
+                            out[row] = TfgColor{cr, cg, cb};
                         }
-                    } else {
-                        out[row] = TfgColor{r, g, b};
                     }
                 }
-                __syncthreads();
+                umma::fence_before_sync();
+                slot_sync(bar);   // accumulator read before the next tile's first MMA
             }
         }
     }
-    if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
+    if (pending) umma::mbar_wait(&mb_in[slot], iph, kSpinLimit);   // no copy may land after exit
+    if (!ok && leader) atomicExch(&g_mlp_error, 1);
     __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(tmem, 128);
+    if (warp == 0) umma::tmem_dealloc(tslot, 512);
 }
 
 // ------------------------------------------------------------------ training forward + backward
@@ -800,8 +924,9 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
     if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
         return fail(TFG_E_INVALID, "mlp inference: input buffer must be 16-byte aligned");
     const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
-    const uint32_t grid = std::min<uint32_t>(tiles, 2u * (uint32_t)n->sms);
-    mlp::k_infer<<<grid, 128, mlp::kInferSmem + 1024, s>>>(in, count, n_dev, n->bounds, n->inf, out, img, thr);
+    const uint32_t grid = std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, (uint32_t)n->sms);
+    mlp::k_infer<<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(in, count, n_dev, n->bounds, n->inf, out,
+                                                                            img, thr);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp inference");
     return ok();

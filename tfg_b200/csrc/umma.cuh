@@ -26,6 +26,13 @@ __host__ __device__ __forceinline__ uint32_t sw128_offset(uint32_t r, uint32_t c
     return (r >> 3) * 1024u + (r & 7u) * 128u + ((c ^ (r & 7u)) << 4);
 }
 
+// Byte offset of 16-byte chunk `c` (0..3) of row `r` inside a 64-byte-swizzle
+// region (64-byte rows, 512-byte 8-row atoms): the chunk index is XORed with
+// bits 7..8 of the address, i.e. (r / 2) mod 4.
+__host__ __device__ __forceinline__ uint32_t sw64_offset(uint32_t r, uint32_t c) {
+    return (r >> 3) * 512u + (r & 7u) * 64u + ((c ^ ((r >> 1) & 3u)) << 4);
+}
+
 // ------------------------------------------------------------------ descriptors
 // Shared-memory matrix descriptor: start address, leading byte offset (unused
 // for swizzled K-major), stride byte offset between 8-row groups (1024 B),
@@ -37,6 +44,17 @@ __device__ __forceinline__ uint64_t sdesc_sw128(uint32_t saddr) {
     d |= (uint64_t)(1024u >> 4) << 32;
     d |= (uint64_t)1u << 46;
     d |= (uint64_t)2u << 61;
+    return d;
+}
+
+// The same for a 64-byte-swizzle K-major region (8-row stride 512 B, layout 4).
+__device__ __forceinline__ uint64_t sdesc_sw64(uint32_t saddr) {
+    uint64_t d = 0;
+    d |= (uint64_t)((saddr >> 4) & 0x3FFFu);
+    d |= (uint64_t)(16u >> 4) << 16;
+    d |= (uint64_t)(512u >> 4) << 32;
+    d |= (uint64_t)1u << 46;
+    d |= (uint64_t)4u << 61;
     return d;
 }
 
@@ -75,10 +93,34 @@ __device__ __forceinline__ void mma_f16(uint32_t d_tmem, uint64_t a, uint64_t b,
         "l"(a), "l"(b), "r"(idesc), "r"((uint32_t)accumulate));
 }
 
+// The same with A read from TMEM: row m of A in lane m, K elements packed two
+// per 32-bit column (element 2j in the low half of column j).
+__device__ __forceinline__ void mma_f16_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc, bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b), "r"(idesc), "r"((uint32_t)accumulate));
+}
+
 // Arrive on `mbar` once all previously issued MMAs of this thread complete.
 __device__ __forceinline__ void mma_commit(uint64_t* mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))
                  : "memory");
+}
+
+// One lane of the (converged) calling warp returns true.  MMAs are issued
+// from a warp-uniform branch through this, which keeps their descriptors in
+// uniform registers; a divergent single-thread branch costs roughly twice the
+// cycles per MMA.
+__device__ __forceinline__ bool elect_one() {
+    uint32_t pred = 0;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "elect.sync _|p, 0xffffffff;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(pred));
+    return pred != 0;
 }
 
 // ------------------------------------------------------------------ mbarrier
@@ -152,6 +194,23 @@ __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
 #pragma unroll
     for (int i = 0; i < 32; ++i) v[i] = __uint_as_float(r[i]);
 }
+
+// Each thread of a warp writes 16 consecutive 32-bit columns of its own TMEM
+// lane; wait_st blocks until this thread's TMEM stores are complete.
+__device__ __forceinline__ void tmem_st16(uint32_t taddr, const uint32_t (&r)[16]) {
+    asm volatile(
+        "tcgen05.st.sync.aligned.32x32b.x16.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,%16};" ::"r"(
+            taddr),
+        "r"(r[0]), "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7]), "r"(r[8]), "r"(r[9]),
+        "r"(r[10]), "r"(r[11]), "r"(r[12]), "r"(r[13]), "r"(r[14]), "r"(r[15])
+        : "memory");
+}
+__device__ __forceinline__ void tmem_st8(uint32_t taddr, const uint32_t* r) {
+    asm volatile("tcgen05.st.sync.aligned.32x32b.x8.b32 [%0], {%1,%2,%3,%4,%5,%6,%7,%8};" ::"r"(taddr), "r"(r[0]),
+                 "r"(r[1]), "r"(r[2]), "r"(r[3]), "r"(r[4]), "r"(r[5]), "r"(r[6]), "r"(r[7])
+                 : "memory");
+}
+__device__ __forceinline__ void tmem_wait_st() { asm volatile("tcgen05.wait::st.sync.aligned;" ::: "memory"); }
 
 }  // namespace umma
 }  // namespace tfg
