@@ -48,18 +48,8 @@ struct TravStack {
 };
 
 __device__ __forceinline__ uint32_t msb_index(uint32_t v) { return 31u - (uint32_t)__clz(v); }
-// Byte k of w as a float.  TFG_BYTE_PRMT selects a PRMT into the mantissa of
-// 2^23 followed by an exact subtraction instead of an integer conversion.
-#ifndef TFG_BYTE_PRMT
-#define TFG_BYTE_PRMT 0
-#endif
-__device__ __forceinline__ float byte_f(uint32_t w, int k) {
-#if TFG_BYTE_PRMT
-    return __int_as_float((int)__byte_perm(w, 0x4B00u, 0x5440u + (uint32_t)k)) - 8388608.0f;
-#else
-    return (float)((w >> (8 * k)) & 0xFFu);
-#endif
-}
+// Byte k of w as a float.
+__device__ __forceinline__ float byte_f(uint32_t w, int k) { return (float)((w >> (8 * k)) & 0xFFu); }
 
 // Per-ray constants of the watertight test: permutation and shear.
 struct WtRay {

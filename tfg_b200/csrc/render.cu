@@ -439,45 +439,72 @@ __global__ void __launch_bounds__(128) k_shadow(PassArgs a, int bounce) {
     TravStack stck;
     stck.smem = sstack; stck.stride = blockDim.x; stck.tid = threadIdx.x;
     const uint32_t n = a.ws.counters[4 * bounce + 2];
+    uint32_t* fetch = &a.ws.counters[4 * bounce + 3];
     TravCounts cnt;
     uint32_t nrays = 0;
-    const uint32_t stride = gridDim.x * blockDim.x;
-    const uint32_t n_round = STATS ? (n + stride - 1) / stride * stride : n;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n_round; i += stride) {
-        if (STATS && i >= n) continue;
-        const float4* s = &a.ws.shadow[4 * (size_t)i];
-        const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
-        const V3 P = xyz(s0), N = xyz(s1), kd = xyz(s2), cam = xyz(s3);
-        const uint32_t p = __float_as_uint(s0.w);
-        const bool to_suffix = __float_as_uint(s1.w) != 0u;
+    // One shadow ray per lane: the lights of an item sit on G adjacent lanes
+    // (G = light count rounded up to a power of two; more than 32 lights fall
+    // back to one lane looping over them), and warps fetch items dynamically.
+    const int nl = a.nlights;
+    const uint32_t G = nl <= 1 ? 1u : nl <= 2 ? 2u : nl <= 4 ? 4u : nl <= 8 ? 8u : nl <= 16 ? 16u : nl <= 32 ? 32u : 1u;
+    const uint32_t lane = lane_id(), lg = lane & (G - 1u), group0 = lane & ~(G - 1u);
+    const int l_begin = G == 1u ? 0 : (int)lg;
+    const int l_end = G == 1u ? nl : min(nl, (int)lg + 1);
+    while (true) {
+        uint32_t base = 0;
+        if (lane == 0) base = atomicAdd(fetch, 32u / G);
+        base = __shfl_sync(0xFFFFFFFFu, base, 0);
+        if (base >= n) break;
+        const uint32_t i = base + lane / G;
+        const bool have = i < n;
         V3 L = v3(0.0f, 0.0f, 0.0f);
-        for (int l = 0; l < a.nlights; ++l) {
-            const TfgLuzPuntual lz = a.lights[l];
-            V3 dl = ld3(lz.posicion) - P;
-            float dist = sqrtf(dot(dl, dl));
-            dl = normalized(dl);
-            const float c = dot(N, dl);
-            if (c <= 0.0f) continue;
-            const V3 so = P + dl * kEps;
-            if (STATS) ++nrays;
-            if (analytic_any(sprims, nsm, a.prims, a.nprims, so, dl, dist)) continue;
-            if (a.shadow_mesh && a.has_bvh) {
-                float tm = dist, hu, hv;
-                uint32_t hid;
-                if (cwbvh_trace<TRI_FMT, true>(a.nodes, a.tris, so, dl, kEps, tm, hid, hu, hv, stck,
-                                               STATS ? &cnt : nullptr)) continue;
+        V3 P, N, kd, cam;
+        uint32_t p = 0;
+        bool to_suffix = false;
+        if (have) {
+            const float4* s = &a.ws.shadow[4 * (size_t)i];
+            const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
+            P = xyz(s0); N = xyz(s1); kd = xyz(s2); cam = xyz(s3);
+            p = __float_as_uint(s0.w);
+            to_suffix = __float_as_uint(s1.w) != 0u;
+            for (int l = l_begin; l < l_end; ++l) {
+                const TfgLuzPuntual lz = a.lights[l];
+                V3 dl = ld3(lz.posicion) - P;
+                float dist = sqrtf(dot(dl, dl));
+                dl = normalized(dl);
+                const float c = dot(N, dl);
+                if (c <= 0.0f) continue;
+                const V3 so = P + dl * kEps;
+                if (STATS) ++nrays;
+                if (analytic_any(sprims, nsm, a.prims, a.nprims, so, dl, dist)) continue;
+                if (a.shadow_mesh && a.has_bvh) {
+                    float tm = dist, hu, hv;
+                    uint32_t hid;
+                    if (cwbvh_trace<TRI_FMT, true>(a.nodes, a.tris, so, dl, kEps, tm, hid, hu, hv, stck,
+                                                   STATS ? &cnt : nullptr)) continue;
+                }
+                const V3 kdpi = v3(kd.x / kPiF, kd.y / kPiF, kd.z / kPiF);
+                dist = fmaxf(dist, 1.0f);
+                const float d2 = dist * dist;
+                const V3 Li = v3(lz.intensidad.r / d2, lz.intensidad.g / d2, lz.intensidad.b / d2);
+                L = L + mul(Li, kdpi) * c;
             }
-            const V3 kdpi = v3(kd.x / kPiF, kd.y / kPiF, kd.z / kPiF);
-            dist = fmaxf(dist, 1.0f);
-            const float d2 = dist * dist;
-            const V3 Li = v3(lz.intensidad.r / d2, lz.intensidad.g / d2, lz.intensidad.b / d2);
-            L = L + mul(Li, kdpi) * c;
         }
-        const V3 add = mul(cam, L);
-        float4* dst = to_suffix ? &a.ws.lsuf[p] : &a.ws.lpre[p];
-        float4 v = *dst;
-        v.x += add.x; v.y += add.y; v.z += add.z;
-        *dst = v;
+        // Sum the group's lights in light order on its first lane (an occluded
+        // or back-facing light adds an exact zero), as the sequential loop does.
+        for (uint32_t j = 1; j < G; ++j) {
+            const float x = __shfl_sync(0xFFFFFFFFu, L.x, group0 + j);
+            const float y = __shfl_sync(0xFFFFFFFFu, L.y, group0 + j);
+            const float z = __shfl_sync(0xFFFFFFFFu, L.z, group0 + j);
+            if (lg == 0u && (int)j < nl) L = L + v3(x, y, z);
+        }
+        if (have && lg == 0u) {
+            const V3 add = mul(cam, L);
+            float4* dst = to_suffix ? &a.ws.lsuf[p] : &a.ws.lpre[p];
+            float4 v = *dst;
+            v.x += add.x; v.y += add.y; v.z += add.z;
+            *dst = v;
+        }
     }
     if (STATS) flush_work(3, nrays, cnt);
 }
