@@ -192,24 +192,39 @@ struct TravCounts {
     uint32_t nodes = 0, tris = 0;
 };
 
-// Closest hit (ANY_HIT = false) or first hit (ANY_HIT = true) against the
-// CWBVH.  tmax in: upper bound (exclusive); out: hit distance when found.
-// Returns true on a hit; id / u / v are written only then.  `cnt`, when not
-// null, accumulates the work done.
+// Per-ray traversal state, advanced one node at a time by step(): lets a
+// persistent kernel give an idle lane a new ray while the other lanes of its
+// warp are still traversing.  Closest hit (ANY_HIT = false) or first hit
+// (ANY_HIT = true); tmax is the current upper bound (exclusive) and becomes
+// the hit distance; id / hu / hv are valid when `found`.
 template <int TRI_FMT, bool ANY_HIT>
-__device__ __forceinline__ bool cwbvh_trace(const float4* __restrict__ nodes, const float4* __restrict__ tris,
-                                            V3 O, V3 D, float tmin, float& tmax, uint32_t& id, float& hu,
-                                            float& hv, TravStack& st, TravCounts* cnt) {
-    const V3 rD = v3(1.0f / D.x, 1.0f / D.y, 1.0f / D.z);
-    const uint32_t octinv = 7u - ((D.x < 0.0f ? 4u : 0u) | (D.y < 0.0f ? 2u : 0u) | (D.z < 0.0f ? 1u : 0u));
+struct CwbvhRay {
+    V3 O, D, rD;
+    uint32_t octinv;
     WtRay wr;
-    if (TRI_FMT == 1) wr = wt_setup(D);
-    uint2 ng = make_uint2(0u, 0x80000000u);
-    uint32_t sp = 0, nsteps = 0, ntris = 0;
-    bool found = false;
-    while (nsteps < kMaxNodeVisits) {
+    float tmin, tmax, hu, hv;
+    uint32_t id;
+    bool found;
+    uint2 ng;
+    uint32_t sp, nsteps, ntris;
+
+    __device__ __forceinline__ void init(V3 O_, V3 D_, float tmin_, float tmax_) {
+        O = O_; D = D_; tmin = tmin_; tmax = tmax_;
+        rD = v3(1.0f / D.x, 1.0f / D.y, 1.0f / D.z);
+        octinv = 7u - ((D.x < 0.0f ? 4u : 0u) | (D.y < 0.0f ? 2u : 0u) | (D.z < 0.0f ? 1u : 0u));
+        if (TRI_FMT == 1) wr = wt_setup(D);
+        ng = make_uint2(0u, 0x80000000u);
+        sp = 0; nsteps = 0; ntris = 0;
+        found = false;
+        id = 0; hu = 0.0f; hv = 0.0f;
+    }
+
+    // Decode the next inner node, test its triangles and pop the stack when
+    // its group is empty.  Returns false once the traversal is complete.
+    __device__ __forceinline__ bool step(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                                         TravStack& st) {
+        if (nsteps >= kMaxNodeVisits) return false;
         ++nsteps;
-        // Pick the next inner child from the current node group.
         const uint32_t bit = msb_index(ng.y);
         const uint32_t imask_parent = ng.y & 0xFFu;
         ng.y &= ~(1u << bit);
@@ -221,7 +236,7 @@ __device__ __forceinline__ bool cwbvh_trace(const float4* __restrict__ nodes, co
         ng = make_uint2(cbase, (hm & 0xFF000000u) | imask);
         uint32_t tbits = hm & 0x00FFFFFFu;
         while (tbits) {
-            if (cnt) ++ntris;
+            ++ntris;
             const uint32_t k = msb_index(tbits);
             tbits &= ~(1u << k);
             float t, u, v;
@@ -229,24 +244,40 @@ __device__ __forceinline__ bool cwbvh_trace(const float4* __restrict__ nodes, co
                 uint32_t tid;
                 if (ref_hit(tris, tbase + 4u * k, O, D, tmin, tmax, t, u, v, tid)) {
                     tmax = t; hu = u; hv = v; id = tid; found = true;
-                    if (ANY_HIT) { if (cnt) { cnt->nodes += nsteps; cnt->tris += ntris; } return true; }
+                    if (ANY_HIT) return false;
                 }
             } else {
                 const uint32_t tri = (tbase >> 2) + k;
                 if (wt_hit(tris, tri, O, wr, tmin, tmax, t, u, v)) {
                     tmax = t; hu = u; hv = v; id = __float_as_uint(__ldg(&tris[3 * tri]).w); found = true;
-                    if (ANY_HIT) { if (cnt) { cnt->nodes += nsteps; cnt->tris += ntris; } return true; }
+                    if (ANY_HIT) return false;
                 }
             }
         }
         if (ng.y <= 0x00FFFFFFu) {
-            if (sp == 0) break;
+            if (sp == 0) return false;
             --sp;
             ng = st.get(sp);
         }
+        return true;
     }
-    if (cnt) { cnt->nodes += nsteps; cnt->tris += ntris; }
-    return found;
+};
+
+// Whole traversal in one call.  tmax in: upper bound (exclusive); out: hit
+// distance when found.  Returns true on a hit; id / u / v are written only
+// then.  `cnt`, when not null, accumulates the work done.
+template <int TRI_FMT, bool ANY_HIT>
+__device__ __forceinline__ bool cwbvh_trace(const float4* __restrict__ nodes, const float4* __restrict__ tris,
+                                            V3 O, V3 D, float tmin, float& tmax, uint32_t& id, float& hu,
+                                            float& hv, TravStack& st, TravCounts* cnt) {
+    CwbvhRay<TRI_FMT, ANY_HIT> r;
+    r.init(O, D, tmin, tmax);
+    while (r.step(nodes, tris, st)) {
+    }
+    if (cnt) { cnt->nodes += r.nsteps; cnt->tris += r.ntris; }
+    if (!r.found) return false;
+    tmax = r.tmax; id = r.id; hu = r.hu; hv = r.hv;
+    return true;
 }
 
 }  // namespace tfg

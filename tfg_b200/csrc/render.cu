@@ -42,6 +42,7 @@ enum : uint32_t {
 };
 
 constexpr uint32_t kMissId = 0xFFFFFFFFu;
+constexpr int kRefillMin = 8;   // idle lanes that trigger a warp's refill (4..24 measured; 8 best)
 
 // Traversal work totals for TFG_PROFILE_COUNTS: rays, nodes, triangle tests
 // for closest-hit rays, then the same for shadow rays.
@@ -197,30 +198,43 @@ __global__ void __launch_bounds__(128) k_trace(PassArgs a, int bounce) {
     uint32_t* fetch = &a.ws.counters[4 * bounce + 1];
     TravCounts cnt;
     uint32_t nrays = 0;
+    // Persistent lanes: a lane whose ray is done takes a new one as soon as
+    // kRefillMin lanes of its warp are idle, instead of waiting for the
+    // slowest ray of a 32-ray batch.
+    const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
+    CwbvhRay<TRI_FMT, false> r;
+    uint32_t cur = kMissId, bid = kMissId;
+    float best = 0.0f, bu = 0.0f, bv = 0.0f;
+    bool exhausted = false;
     while (true) {
-        uint32_t base = 0;
-        if (lane_id() == 0) base = atomicAdd(fetch, 32u);
-        base = __shfl_sync(0xFFFFFFFFu, base, 0);
-        if (base >= n) break;
-        const uint32_t i = base + lane_id();
-        if (i < n) {
-            const float4 o4 = rays[2 * i], d4 = rays[2 * i + 1];
-            const V3 O = xyz(o4), D = xyz(d4);
-            float best = o4.w, bu = 0.0f, bv = 0.0f;
-            uint32_t id = kMissId;
-            const int ai = analytic_closest(sprims, nsm, a.prims, a.nprims, O, D, best, bu, bv);
-            if (ai >= 0) id = kAnalyticBit | (uint32_t)ai;
-            if (a.has_bvh) {
-                float tm = best, hu, hv;
-                uint32_t mid;
-                if (cwbvh_trace<TRI_FMT, false>(a.nodes, a.tris, O, D, 0.0f, tm, mid, hu, hv, st,
-                                                STATS ? &cnt : nullptr) &&
-                    tm < best && tm > kEps) {
-                    best = tm; bu = hu; bv = hv; id = mid;
-                }
+        const bool idle = cur == kMissId;
+        const uint32_t im = __ballot_sync(0xFFFFFFFFu, idle);
+        if (exhausted) {
+            if (im == 0xFFFFFFFFu) break;
+        } else if (__popc(im) >= kRefillMin) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(im));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            exhausted = base + (uint32_t)__popc(im) >= n;
+            const uint32_t k = base + (uint32_t)__popc(im & lt);
+            if (idle && k < n) {
+                cur = k;
+                const float4 o4 = rays[2 * k], d4 = rays[2 * k + 1];
+                const V3 O = xyz(o4), D = xyz(d4);
+                best = o4.w; bu = 0.0f; bv = 0.0f; bid = kMissId;
+                const int ai = analytic_closest(sprims, nsm, a.prims, a.nprims, O, D, best, bu, bv);
+                if (ai >= 0) bid = kAnalyticBit | (uint32_t)ai;
+                r.init(O, D, 0.0f, best);
             }
-            a.ws.hit[i] = make_float4(best, bu, bv, __uint_as_float(id));
+        }
+        if (cur != kMissId && !(a.has_bvh && r.step(a.nodes, a.tris, st))) {
+            if (a.has_bvh) {
+                if (r.found && r.tmax < best && r.tmax > kEps) { best = r.tmax; bu = r.hu; bv = r.hv; bid = r.id; }
+                if (STATS) { cnt.nodes += r.nsteps; cnt.tris += r.ntris; }
+            }
+            a.ws.hit[cur] = make_float4(best, bu, bv, __uint_as_float(bid));
             ++nrays;
+            cur = kMissId;
         }
     }
     if (STATS) flush_work(0, nrays, cnt);
