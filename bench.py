@@ -31,6 +31,10 @@ METRIC = "Mpaths/s & ms/frame @1080p"
 WORKLOAD = "plain path tracing, 1920x1080, 64 spp, depth 8, RR from depth 3, 16 displaced icospheres + fractal terrain (1,000,480 tris), 2 point lights"
 
 
+# Measured once with ncu on `bench.py --profile-pass` (see the profiles/ summary named above).
+TRACE_DRAM_BYTES_PER_LAUNCH = 41_169_312
+
+
 def peaks() -> dict:
     p = ROOT / "MEASURED_PEAKS.json"
     if p.exists():
@@ -149,7 +153,7 @@ def reference_arm(args):
     scene = scenes.spheres_terrain(W_PX, H_PX)
     hb = hbvh.build_host(hbvh.triangle_vertices(scene.mesh))
     nthreads = os.cpu_count() or 1
-    rows = 24
+    rows = H_PX
     for _ in range(args.warmup):
         cpu_oracle_sample(scene, hb, 8, nthreads)
     secs, paths = 0.0, 0
@@ -158,7 +162,8 @@ def reference_arm(args):
         secs += dt
         paths += n
     v = paths / secs / 1e6
-    sample = f"{rows} rows x 1920 px x 1 spp per step (of 1920x1080x64 spp), depth {DEPTH}, RR from {RR}"
+    sample = (f"each step: the full 1920x1080 frame at 1 spp (1/64 of a 64-spp frame), depth {DEPTH}, "
+              f"RR from {RR}; warm-up steps: 8 rows")
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": round(v, 4), "unit": "Mpaths/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * secs / args.steps, 3),
@@ -259,6 +264,136 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 1024, frames: int = 300) -> dict:
     }
 
 
+def batched_eval(dev, frames: int = 20) -> dict:
+    """Twelve independent scenes (10k to 2M triangles, 1-4 lights, 640x360 to
+    1920x1080), one cache model each, 1 spp + cache per frame, advanced by
+    one tfgNrcFrameBatch call per frame and replayed as one CUDA graph.  Also
+    times the same batch without the graph and the twelve scenes as
+    single-scene tfgNrcFrame calls one after another."""
+    import torch
+
+    from tfg_b200 import pathtracer as pt
+    from tfg_b200 import scenes as sc
+    from tfg_b200.nrc import ColorMLP, NrcBatch, NrcRenderer
+
+    params = pt.RenderParams(max_depth=DEPTH, rr_min_depth=RR, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT)
+    t0 = time.perf_counter()
+    scs = [sc.batch_scene(i) for i in range(12)]
+    dss = [pt.DeviceScene(s, dev) for s in scs]
+    t_setup = time.perf_counter() - t0
+    rs = []
+    for k, (s, ds) in enumerate(zip(scs, dss)):
+        m = ColorMLP(batch=16384, seed=500 + k)
+        m.set_bounds(*s.bounds)
+        rs.append(NrcRenderer(ds, m, params, train_steps=4, use_graph=True))
+    batch = NrcBatch(rs, use_graph=True)
+    st = batch.stream
+    for f in range(48):
+        batch.frame(f, warmup=True)
+    for f in range(8):
+        batch.frame(48 + f)
+    st.synchronize()
+
+    def timed(fn, n):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(st)
+        for k in range(n):
+            fn(k)
+        e1.record(st)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / n
+
+    ms_graph = timed(lambda k: batch.frame(1000 + k), frames)
+    eager = NrcBatch(rs, use_graph=False, stream=st)
+    ms_eager = timed(lambda k: eager.frame(2000 + k), frames)
+
+    # tfgNrcFrame keeps one captured graph per device, so twelve alternating
+    # scenes run as eager single-scene calls
+    for r in rs:
+        r.stream = st
+        r.cfg.use_graph = 0
+
+    def one_by_one(k):
+        for r in rs:
+            r.frame(3000 + k, accumulate=False)
+
+    one_by_one(0)
+    ms_single = timed(one_by_one, frames)
+    px = sum(s.width * s.height for s in scs)
+    adam = [int(r.mlp.state()["adam_t"]) for r in rs]
+    for r in rs:
+        r.mlp.close()
+    for ds in dss:
+        ds.close()
+    return {
+        "scenes": len(scs), "triangles": [int(len(s.mesh)) for s in scs],
+        "resolutions": [f"{s.width}x{s.height}" for s in scs], "lights": [int(len(s.lights)) for s in scs],
+        "paths_per_frame": px, "frames_timed": frames,
+        "ms_per_batch_frame_graph": round(ms_graph, 3), "ms_per_batch_frame_eager": round(ms_eager, 3),
+        "ms_per_frame_12_single_scene_calls": round(ms_single, 3),
+        "mpaths_per_s_graph": round(px / (ms_graph * 1e-3) / 1e6, 1),
+        "adam_steps_min": min(adam), "setup_s": round(t_setup, 1),
+        "frame": "render 1 spp with cache queries + training records, inference + composite, targets, 4 Adam steps",
+    }
+
+
+def measure_peaks():
+    """Peaks this pod's MEASURED_PEAKS.json does not hold, measured the same
+    way (best of 10, CUDA events): an L2-resident copy (2 x 24 MB buffers,
+    read + write bytes), and dense FP16 and FP8 (e4m3, per-tensor scales)
+    GEMMs of 8192^3 through torch (cuBLAS / cuBLASLt)."""
+    import torch
+    dev = torch.device("cuda", 0)
+
+    def best_ms(fn, reps=10):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        best = float("inf")
+        for _ in range(reps):
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record()
+            fn()
+            e1.record()
+            e1.synchronize()
+            best = min(best, e0.elapsed_time(e1))
+        return best
+
+    out = {}
+    n = 24 << 20
+    a = torch.empty(n, dtype=torch.uint8, device=dev).fill_(1)
+    b = torch.empty(n, dtype=torch.uint8, device=dev)
+    inner = 50
+    ms = best_ms(lambda: [b.copy_(a) for _ in range(inner)])
+    out["l2_copy_gbs"] = round(2 * n * inner / (ms * 1e-3) / 1e9, 1)
+    big = 1 << 30
+    a2 = torch.empty(big, dtype=torch.uint8, device=dev).fill_(1)
+    b2 = torch.empty(big, dtype=torch.uint8, device=dev)
+    ms = best_ms(lambda: b2.copy_(a2))
+    out["hbm_copy_gbs"] = round(2 * big / (ms * 1e-3) / 1e9, 1)
+    del a2, b2
+    N = 8192
+    x = torch.randn(N, N, device=dev, dtype=torch.float16)
+    y = torch.randn(N, N, device=dev, dtype=torch.float16)
+    ms = best_ms(lambda: torch.matmul(x, y))
+    out["fp16_tflops"] = round(2 * N ** 3 / (ms * 1e-3) / 1e12, 1)
+    xb, yb = x.bfloat16(), y.bfloat16()
+    ms = best_ms(lambda: torch.matmul(xb, yb))
+    out["bf16_tflops"] = round(2 * N ** 3 / (ms * 1e-3) / 1e12, 1)
+    try:
+        x8 = x.to(torch.float8_e4m3fn)
+        y8 = y.t().contiguous().t().to(torch.float8_e4m3fn)
+        one = torch.ones((), device=dev)
+        ms = best_ms(lambda: torch._scaled_mm(x8, y8, scale_a=one, scale_b=one, out_dtype=torch.bfloat16))
+        out["fp8_e4m3_tflops"] = round(2 * N ** 3 / (ms * 1e-3) / 1e12, 1)
+    except Exception as e:   # older torch without the scaled GEMM
+        out["fp8_e4m3_tflops"] = None
+        out["fp8_error"] = str(e).splitlines()[0][:200]
+    out["how"] = ("best of 10 CUDA-event timings after 3 warm-ups; L2: 50 back-to-back copies of a 24 MB buffer; "
+                  "HBM: one 1 GiB copy; GEMMs: torch.matmul / torch._scaled_mm, 8192^3, 2*N^3 FLOP")
+    print(json.dumps(out))
+
+
 def profile_mlp():
     """Cache inference over 2,073,600 queries (232 MB of DatosMLP, more than
     L2) and one 16384-sample train step, untimed; used for ncu captures."""
@@ -314,8 +449,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache evaluation")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 12-scene batched cache frame")
     ap.add_argument("--profile-pass", action="store_true",
                     help="run one untimed 1-spp pass of the workload and exit (small case for ncu)")
+    ap.add_argument("--measure-peaks", action="store_true",
+                    help="measure L2 copy bandwidth and FP16 / BF16 / FP8 GEMM peaks, print them and exit")
     ap.add_argument("--profile-mlp", action="store_true",
                     help="run cache inference on 1920x1080 queries and one train step, then exit (case for ncu)")
     args = ap.parse_args()
@@ -327,6 +465,9 @@ def main():
         return
     if args.profile_mlp:
         profile_mlp()
+        return
+    if args.measure_peaks:
+        measure_peaks()
         return
 
     import torch
@@ -435,6 +576,10 @@ def main():
         nrc["mlp_inference"]["frac_of_dense_f16_peak"] = round(nrc["mlp_inference"]["tflops"] / bf16, 4)
         nrc["mlp_inference"]["peak_tflops"] = bf16
 
+    batched = None
+    if not args.no_batched and world == 1:
+        batched = batched_eval(dev)
+
     pk = peaks()
     trace_ms = prof["ms"]["trace"]
     trace_launches = prof["launches"]["trace"]
@@ -448,10 +593,15 @@ def main():
         from tfg_b200 import bvh as hbvh
         hb = hbvh.build_host(hbvh.triangle_vertices(scene.mesh))
         nthreads = os.cpu_count() or 1
-        rows = 48
-        dt, n = cpu_oracle_sample(scene, hb, rows, nthreads)
+        frames = 8
+        dt, n = 0.0, 0
+        for f in range(frames):
+            d, k = cpu_oracle_sample(scene, hb, H_PX, nthreads, frame=1 + f)
+            dt += d
+            n += k
         cpu = {"value": round(n / dt / 1e6, 4), "unit": "Mpaths/s", "cores": nthreads, "kind": "port",
-               "sample": f"{rows} rows x 1920 px x 1 spp of the same frame (depth {DEPTH}, RR from {RR}), {dt:.1f} s"}
+               "sample": f"{frames} full 1920x1080 frames at 1 spp (8 of the 64 samples of the timed frame; "
+                         f"depth {DEPTH}, RR from {RR}), {dt:.1f} s"}
 
     out = {
         "metric": METRIC, "value": round(value, 3), "unit": "Mpaths/s", "n_gpus": world, "steps": args.steps,
@@ -470,7 +620,11 @@ def main():
             "achieved": round(achieved, 1) if achieved else None,
             "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,
-            "peak_source": pk["source"], "traffic": None,
+            "peak_source": pk["source"],
+            # ncu dram__bytes_read.sum + dram__bytes_write.sum of the 8 closest-hit launches of one
+            # 1-spp pass of this frame, per launch (profiles/k_trace_k_shadow_dram_1080p.md): the
+            # 64 MB CWBVH + triangles stay L2-resident, so DRAM sees ~8 % of the algorithmic bytes.
+            "traffic": TRACE_DRAM_BYTES_PER_LAUNCH, "traffic_unit": "bytes per launch",
             "algorithmic_bytes_per_ray": round(bytes_per_ray, 1),
             "nodes_per_ray": round(nodes_per_ray, 3), "tri_tests_per_ray": round(tris_per_ray, 3),
             "rays_per_launch_avg": round(rays_timed / max(1, trace_launches), 1),
@@ -482,6 +636,7 @@ def main():
         "clocks": clocks,
         "cpu_baseline": cpu,
         "nrc": nrc,
+        "batched": batched,
     }
     print(json.dumps(out))
     ds.close()

@@ -430,6 +430,36 @@ int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const TfgRenderP
                 const TfgTinyBVHD_GPU* bvh, const float* tris_wt, const TfgPrimitiva* primitivas_bvh,
                 int32_t num_prims_bvh, const TfgNrcBuffers* buffers, int32_t frame, void* stream);
 
+/* One scene of a batched cache frame: the arguments of tfgNrcFrame (104 B). */
+typedef struct TfgNrcSceneFrame {
+    TfgColorMLP*             mlp;
+    const TfgNrcFrameConfig* cfg;
+    const TfgRenderParams*   params;
+    const TfgCamara*         camara;
+    const TfgPrimitiva*      primitivas;
+    const TfgLuzPuntual*     luces;
+    const TfgTinyBVHD_GPU*   bvh;
+    const float*             tris_wt;
+    const TfgPrimitiva*      primitivas_bvh;
+    const TfgNrcBuffers*     buffers;
+    int32_t                  num_primitivas;
+    int32_t                  num_luces;
+    int32_t                  num_prims_bvh;
+    int32_t                  ancho_img;
+    int32_t                  alto_img;
+    int32_t                  reserved;
+} TfgNrcSceneFrame;
+
+/* No reference counterpart (the reference renders one scene per process).
+ * One cache frame of each of `n` independent scenes -- each with its own
+ * cache model, configuration and buffers, all distinct -- as tfgNrcFrame
+ * would run it, enqueued on `stream` as up to four concurrent branches
+ * (scenes assigned largest first, one render workspace per branch).  With
+ * `use_graph` set and a non-default `stream`, the whole batch is captured
+ * once as a single CUDA graph (re-captured when any argument changes) and
+ * replayed.  `frame` seeds every scene's RNG; cfg->use_graph is ignored. */
+int tfgNrcFrameBatch(int32_t n, const TfgNrcSceneFrame* scenes, int32_t frame, int32_t use_graph, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

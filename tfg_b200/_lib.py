@@ -10,8 +10,8 @@ import ctypes
 from ctypes import POINTER, c_char_p, c_float, c_int32, c_uint32, c_uint64, c_void_p
 from pathlib import Path
 
-from .structs import (CCWBVHHost, CImagenGPU, CNrcBuffers, CNrcFrameConfig, CRenderParams, CRenderProfile, CTinyBVH,
-                      CTinyBVHD_GPU)
+from .structs import (CCWBVHHost, CImagenGPU, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame, CRenderParams,
+                      CRenderProfile, CTinyBVH, CTinyBVHD_GPU)
 
 LIB_PATH = Path(__file__).resolve().parent / "libtfgpt.so"
 
@@ -76,6 +76,7 @@ _PROTOS = {
     "tfgMlpStatus": (c_int32, []),
     "tfgMlpGetState": (c_int32, [c_void_p, POINTER(c_uint32)]),
     "tfgNrcFrameConfigReference": (None, [POINTER(CNrcFrameConfig)]),
+    "tfgNrcFrameBatch": (c_int32, [c_int32, POINTER(CNrcSceneFrame), c_int32, c_int32, c_void_p]),
     "tfgNrcFrame": (c_int32, [c_void_p, POINTER(CNrcFrameConfig), POINTER(CRenderParams), c_void_p, c_void_p, c_int32,
                               c_void_p, c_int32, c_int32, c_int32, POINTER(CTinyBVHD_GPU), c_void_p, c_void_p, c_int32,
                               POINTER(CNrcBuffers), c_int32, c_void_p]),

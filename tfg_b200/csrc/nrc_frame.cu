@@ -12,9 +12,11 @@
 // number (RNG seed) is written before each launch.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <vector>
 
 #include "../../include/tfg_pt.h"
 #include "tfg_errors.h"
@@ -55,6 +57,7 @@ struct FrameCall {
     const TfgTinyBVHD_GPU* bvh; const float* tris_wt; const TfgPrimitiva* mesh; int nmesh;
     TfgNrcBuffers b;
     int32_t* frame_dev;
+    int ws_slot = 0;
 };
 
 int enqueue_frame(const FrameCall& c, bool prepare_only, cudaStream_t s) {
@@ -70,7 +73,8 @@ int enqueue_frame(const FrameCall& c, bool prepare_only, cudaStream_t s) {
     }
     if (int rc = render_pass_ex(c.prm, c.cam, c.prims, c.nprims, c.lights, c.nlights, c.W, c.H, 0, c.frame_dev, gate,
                                 c.bvh, c.tris_wt, c.mesh, c.nmesh, c.b.img, nullptr, c.b.regs, c.b.counter,
-                                (int)c.b.ring_cap, c.b.infer, c.b.thr, c.cfg.warmup ? 0 : 1, 1, prepare_only, s))
+                                (int)c.b.ring_cap, c.b.infer, c.b.thr, c.cfg.warmup ? 0 : 1, 1, prepare_only,
+                                c.ws_slot, s))
         return rc;
     if (prepare_only) return ok();
     if (int rc = mlp_enqueue_infer(c.mlp, c.b.infer, nullptr, c.b.img, c.b.thr, npx, nullptr, s)) return rc;
@@ -97,10 +101,89 @@ FrameKey key_of(const FrameCall& c) {
     std::memcpy(k.ptrs, p, sizeof(p));
     const int32_t v[] = {c.nprims, c.nlights, c.W, c.H, c.nmesh, (int32_t)c.b.ring_cap, c.cfg.train_steps,
                          (int32_t)c.cfg.max_records, (int32_t)c.cfg.min_records, c.cfg.warmup, c.prm.max_depth,
-                         c.prm.rr_min_depth, c.prm.shadow_mesh, c.prm.tri_format};
+                         c.prm.rr_min_depth, c.prm.shadow_mesh, c.prm.tri_format, c.ws_slot};
     std::memcpy(k.ints, v, sizeof(v));
     k.gate = c.cfg.gate_threshold;
     return k;
+}
+
+// Validated FrameCall from the public arguments (spp 1, no accumulation or
+// profiling inside a frame).
+int make_call(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const TfgRenderParams* params,
+              const TfgCamara* camara, const TfgPrimitiva* primitivas, int32_t num_primitivas,
+              const TfgLuzPuntual* luces, int32_t num_luces, int32_t W, int32_t H, const TfgTinyBVHD_GPU* bvh,
+              const float* tris_wt, const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh,
+              const TfgNrcBuffers* buffers, int32_t* frame_dev, FrameCall& c) {
+    if (!mlp || !cfg || !params || !buffers) return fail(TFG_E_INVALID, "nrc frame: null argument");
+    const TfgNrcBuffers& b = *buffers;
+    if (!b.img || !b.infer || !b.thr || !b.regs || !b.counter || !b.tail_in || !b.tail_pred || !b.train_buf)
+        return fail(TFG_E_INVALID, "nrc frame: a required buffer is null");
+    if (cfg->train_steps < 0 || cfg->max_records == 0 || b.ring_cap < cfg->max_records)
+        return fail(TFG_E_INVALID, "nrc frame: ring capacity below max_records");
+    c.mlp = reinterpret_cast<ColorMlp*>(mlp);
+    c.cfg = *cfg;
+    c.prm = *params;
+    c.prm.spp = 1;
+    c.prm.accumulate = 0;
+    c.prm.profile = 0;
+    c.cam = camara; c.prims = primitivas; c.nprims = num_primitivas; c.lights = luces; c.nlights = num_luces;
+    c.W = W; c.H = H; c.bvh = bvh; c.tris_wt = tris_wt; c.mesh = primitivas_bvh; c.nmesh = num_prims_bvh;
+    c.b = b;
+    c.frame_dev = frame_dev;
+    c.ws_slot = 0;
+    return ok();
+}
+
+int frame_word(int dev, int32_t** out) {
+    if (!g_frame_dev[dev & 15]) {
+        cudaError_t e = cudaMalloc((void**)&g_frame_dev[dev & 15], sizeof(int32_t));
+        if (e != cudaSuccess) return fail((int)e, std::string("nrc frame: ") + cudaGetErrorString(e));
+    }
+    *out = g_frame_dev[dev & 15];
+    return ok();
+}
+
+// ------------------------------------------------------------------ batched frames
+struct BatchGraph {
+    std::vector<FrameKey> keys;
+    bool valid = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+BatchGraph g_batch[16];
+cudaStream_t g_branch[16][kWorkspaceSlots] = {};
+cudaEvent_t g_fork[16] = {};
+cudaEvent_t g_join[16][kWorkspaceSlots] = {};
+
+int branch_resources(int dev, int nb) {
+    cudaError_t e = cudaSuccess;
+    if (!g_fork[dev & 15]) e = cudaEventCreateWithFlags(&g_fork[dev & 15], cudaEventDisableTiming);
+    for (int b = 1; b < nb && e == cudaSuccess; ++b) {
+        if (!g_branch[dev & 15][b]) e = cudaStreamCreateWithFlags(&g_branch[dev & 15][b], cudaStreamNonBlocking);
+        if (e == cudaSuccess && !g_join[dev & 15][b])
+            e = cudaEventCreateWithFlags(&g_join[dev & 15][b], cudaEventDisableTiming);
+    }
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch: ") + cudaGetErrorString(e));
+    return ok();
+}
+
+// Fork `nb` branches off `s`, enqueue every scene on its branch, join back.
+int enqueue_batch(const std::vector<FrameCall>& calls, int nb, int dev, cudaStream_t s) {
+    cudaError_t e = cudaEventRecord(g_fork[dev & 15], s);
+    for (int b = 1; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(g_branch[dev & 15][b], g_fork[dev & 15], 0);
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch fork: ") + cudaGetErrorString(e));
+    int rc = 0;
+    for (const FrameCall& c : calls) {
+        rc = enqueue_frame(c, false, c.ws_slot == 0 ? s : g_branch[dev & 15][c.ws_slot]);
+        if (rc) break;
+    }
+    // join every branch even after a failure, so a capture can end cleanly
+    for (int b = 1; b < nb; ++b) {
+        cudaError_t e2 = cudaEventRecord(g_join[dev & 15][b], g_branch[dev & 15][b]);
+        if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(s, g_join[dev & 15][b], 0);
+        if (e2 != cudaSuccess && !rc) rc = fail((int)e2, std::string("tfgNrcFrameBatch join: ") + cudaGetErrorString(e2));
+    }
+    return rc;
 }
 
 }  // namespace
@@ -122,33 +205,18 @@ extern "C" int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const
                            const TfgTinyBVHD_GPU* bvh, const float* tris_wt, const TfgPrimitiva* primitivas_bvh,
                            int32_t num_prims_bvh, const TfgNrcBuffers* buffers, int32_t frame, void* stream) {
     using namespace tfg;
-    if (!mlp || !cfg || !params || !buffers) return fail(TFG_E_INVALID, "tfgNrcFrame: null argument");
-    const TfgNrcBuffers& b = *buffers;
-    if (!b.img || !b.infer || !b.thr || !b.regs || !b.counter || !b.tail_in || !b.tail_pred || !b.train_buf)
-        return fail(TFG_E_INVALID, "tfgNrcFrame: a required buffer is null");
-    if (cfg->train_steps < 0 || cfg->max_records == 0 || b.ring_cap < cfg->max_records)
-        return fail(TFG_E_INVALID, "tfgNrcFrame: ring capacity below max_records");
     cudaStream_t s = (cudaStream_t)stream;
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     if (int rc = require_sm100(dev)) return rc;
     std::lock_guard<std::mutex> lk(g_frame_mutex);
-    if (!g_frame_dev[dev & 15]) {
-        e = cudaMalloc((void**)&g_frame_dev[dev & 15], sizeof(int32_t));
-        if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame: ") + cudaGetErrorString(e));
-    }
+    int32_t* frame_dev = nullptr;
+    if (int rc = frame_word(dev, &frame_dev)) return rc;
     FrameCall c;
-    c.mlp = reinterpret_cast<ColorMlp*>(mlp);
-    c.cfg = *cfg;
-    c.prm = *params;
-    c.prm.spp = 1;
-    c.prm.accumulate = 0;
-    c.prm.profile = 0;
-    c.cam = camara; c.prims = primitivas; c.nprims = num_primitivas; c.lights = luces; c.nlights = num_luces;
-    c.W = W; c.H = H; c.bvh = bvh; c.tris_wt = tris_wt; c.mesh = primitivas_bvh; c.nmesh = num_prims_bvh;
-    c.b = b;
-    c.frame_dev = g_frame_dev[dev & 15];
+    if (int rc = make_call(mlp, cfg, params, camara, primitivas, num_primitivas, luces, num_luces, W, H, bvh, tris_wt,
+                           primitivas_bvh, num_prims_bvh, buffers, frame_dev, c))
+        return rc;
     mlp_set_gate_threshold(c.mlp, cfg->gate_threshold);
     k_set_frame<<<1, 32, 0, s>>>(c.frame_dev, frame);
     e = cudaGetLastError();
@@ -180,6 +248,82 @@ extern "C" int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const
     }
     e = cudaGraphLaunch(g.exec, s);
     if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame launch: ") + cudaGetErrorString(e));
+    return ok();
+}
+
+extern "C" int tfgNrcFrameBatch(int32_t n, const TfgNrcSceneFrame* scenes, int32_t frame, int32_t use_graph,
+                                void* stream) {
+    using namespace tfg;
+    if (n < 0 || (n > 0 && !scenes)) return fail(TFG_E_INVALID, "tfgNrcFrameBatch: bad scene array");
+    if (n == 0) return ok();
+    cudaStream_t s = (cudaStream_t)stream;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    if (int rc = require_sm100(dev)) return rc;
+    std::lock_guard<std::mutex> lk(g_frame_mutex);
+    int32_t* frame_dev = nullptr;
+    if (int rc = frame_word(dev, &frame_dev)) return rc;
+    std::vector<FrameCall> calls((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        const TfgNrcSceneFrame& f = scenes[i];
+        if (int rc = make_call(f.mlp, f.cfg, f.params, f.camara, f.primitivas, f.num_primitivas, f.luces, f.num_luces,
+                               f.ancho_img, f.alto_img, f.bvh, f.tris_wt, f.primitivas_bvh, f.num_prims_bvh, f.buffers,
+                               frame_dev, calls[(size_t)i]))
+            return rc;
+        for (int j = 0; j < i; ++j)
+            if (calls[(size_t)j].mlp == calls[(size_t)i].mlp || calls[(size_t)j].b.img == calls[(size_t)i].b.img ||
+                calls[(size_t)j].b.regs == calls[(size_t)i].b.regs)
+                return fail(TFG_E_INVALID, "tfgNrcFrameBatch: scenes share a cache model or buffers");
+    }
+    // Largest scenes first, each to the branch with the fewest pixels so far.
+    const int nb = std::min(n, kWorkspaceSlots);
+    std::vector<int> order((size_t)n);
+    for (int i = 0; i < n; ++i) order[(size_t)i] = i;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        return (int64_t)calls[(size_t)x].W * calls[(size_t)x].H > (int64_t)calls[(size_t)y].W * calls[(size_t)y].H;
+    });
+    std::vector<int64_t> load((size_t)nb, 0);
+    for (int i : order) {
+        const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
+        calls[(size_t)i].ws_slot = b;
+        load[(size_t)b] += (int64_t)calls[(size_t)i].W * calls[(size_t)i].H;
+    }
+    if (int rc = branch_resources(dev, nb)) return rc;
+    for (const FrameCall& c : calls) {
+        mlp_set_gate_threshold(c.mlp, c.cfg.gate_threshold);
+        if (int rc = enqueue_frame(c, true, s)) return rc;
+    }
+    k_set_frame<<<1, 32, 0, s>>>(frame_dev, frame);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch: ") + cudaGetErrorString(e));
+    if (!(use_graph && s != nullptr)) return enqueue_batch(calls, nb, dev, s);
+    BatchGraph& g = g_batch[dev & 15];
+    std::vector<FrameKey> keys;
+    for (const FrameCall& c : calls) keys.push_back(key_of(c));
+    if (!g.valid || g.keys.size() != keys.size() ||
+        !std::equal(keys.begin(), keys.end(), g.keys.begin())) {
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        if (g.graph) cudaGraphDestroy(g.graph);
+        g.exec = nullptr; g.graph = nullptr; g.valid = false;
+        e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
+        if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch capture: ") + cudaGetErrorString(e));
+        const int rc = enqueue_batch(calls, nb, dev, s);
+        cudaGraph_t gr = nullptr;
+        e = cudaStreamEndCapture(s, &gr);
+        if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }
+        if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch capture: ") + cudaGetErrorString(e));
+        e = cudaGraphInstantiate(&g.exec, gr, 0);
+        if (e != cudaSuccess) {
+            cudaGraphDestroy(gr);
+            return fail((int)e, std::string("tfgNrcFrameBatch instantiate: ") + cudaGetErrorString(e));
+        }
+        g.graph = gr;
+        g.keys = keys;
+        g.valid = true;
+    }
+    e = cudaGraphLaunch(g.exec, s);
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch launch: ") + cudaGetErrorString(e));
     return ok();
 }
 

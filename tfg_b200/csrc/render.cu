@@ -579,12 +579,16 @@ __global__ void k_resolve(PassArgs a) {
 // ------------------------------------------------------------------ host side
 namespace {
 
+// Queues and per-path state, one set per (device, slot): passes that may run
+// concurrently (the branches of a batched multi-scene frame) use different
+// slots; everything else uses slot 0.
 std::mutex g_ws_mutex;
-Workspace g_ws[16];
+Workspace g_ws[16][kWorkspaceSlots];
 
-int ensure_workspace(int dev, size_t paths, bool nrc, Workspace& out) {
+int ensure_workspace(int dev, int slot, size_t paths, bool nrc, Workspace& out) {
+    if (slot < 0 || slot >= kWorkspaceSlots) return fail(TFG_E_INVALID, "render: workspace slot out of range");
     std::lock_guard<std::mutex> lk(g_ws_mutex);
-    Workspace& w = g_ws[dev & 15];
+    Workspace& w = g_ws[dev & 15][slot];
     auto grow = [](void** p, size_t bytes) -> cudaError_t {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -718,7 +722,7 @@ int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPri
                 TfgColor* thr_out, int use_inf, int train, cudaStream_t stream) {
     return render_pass_ex(prm, d_cam, prims, nprims, lights, nlights, W, H, frame, nullptr, nullptr, bvh, tris_wt,
                           mesh, nmesh, img, accum, regs, reg_counter, reg_cap, infer, thr_out, use_inf, train, false,
-                          stream);
+                          0, stream);
 }
 
 int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
@@ -726,7 +730,7 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
                    const uint32_t* use_inf_dev, const TfgTinyBVHD_GPU* bvh, const float* tris_wt,
                    const TfgPrimitiva* mesh, int nmesh, TfgColor* img, float* accum, TfgRegistroEntrenamiento* regs,
                    uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer, TfgColor* thr_out, int use_inf, int train,
-                   bool prepare_only, cudaStream_t stream) {
+                   bool prepare_only, int ws_slot, cudaStream_t stream) {
     if (W <= 0 || H <= 0 || (size_t)W * (size_t)H > (1u << 28)) return fail(TFG_E_INVALID, "render: bad image size");
     if (!d_cam) return fail(TFG_E_INVALID, "render: camara is null");
     if (nprims < 0 || nlights < 0 || nmesh < 0) return fail(TFG_E_INVALID, "render: negative count");
@@ -746,7 +750,7 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     if (int rc = require_sm100(dev)) return rc;
     Workspace ws;
-    if (int rc = ensure_workspace(dev, (size_t)W * H, nrc, ws)) return rc;
+    if (int rc = ensure_workspace(dev, ws_slot, (size_t)W * H, nrc, ws)) return rc;
     LaunchShapes sh;
     shapes_for(dev, sh);
     if (prepare_only) return ok();

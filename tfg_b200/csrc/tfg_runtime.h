@@ -17,15 +17,20 @@ int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPri
                 TfgRegistroEntrenamiento* regs, uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer,
                 TfgColor* thr_out, int use_inf, int train, cudaStream_t stream);
 
+// Workspace slots per device: passes in flight at the same time (branches of
+// a batched frame) must use different slots.
+constexpr int kWorkspaceSlots = 4;
+
 // render_pass with a device-side frame number / cache-query gate (both
-// optional) and a prepare-only mode that validates and allocates without
-// launching (so a later call can be captured in a CUDA graph).
+// optional), a prepare-only mode that validates and allocates without
+// launching (so a later call can be captured in a CUDA graph), and the
+// workspace slot to run on.
 int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
                    const TfgLuzPuntual* lights, int nlights, int W, int H, int frame, const int32_t* frame_dev,
                    const uint32_t* use_inf_dev, const TfgTinyBVHD_GPU* bvh, const float* tris_wt,
                    const TfgPrimitiva* mesh, int nmesh, TfgColor* img, float* accum, TfgRegistroEntrenamiento* regs,
                    uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer, TfgColor* thr_out, int use_inf, int train,
-                   bool prepare_only, cudaStream_t stream);
+                   bool prepare_only, int ws_slot, cudaStream_t stream);
 
 int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const float* rays, int n, float* hits,
                cudaStream_t stream);

@@ -8,7 +8,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .structs import BOUNDS, DATOS_MLP, REGISTRO, CNrcBuffers, CNrcFrameConfig
+from .structs import BOUNDS, DATOS_MLP, REGISTRO, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame
 
 N_PARAMS = 23552
 # padded [out][in] shapes of the six weight matrices, in parameter order
@@ -167,3 +167,44 @@ class NrcRenderer:
         with torch.cuda.stream(self.stream):
             self.accum.zero_()
         self.frames_accumulated = 0
+
+
+class NrcBatch:
+    """Several independent scenes, each with its own cache model and
+    NrcRenderer buffers, advanced one frame at a time by tfgNrcFrameBatch:
+    up to four concurrent branches, optionally captured as one CUDA graph.
+    No reference counterpart (the reference renders one scene per process)."""
+
+    def __init__(self, renderers: list[NrcRenderer], use_graph: bool = True, stream=None):
+        if not renderers:
+            raise ValueError("NrcBatch needs at least one renderer")
+        self.renderers = renderers
+        self.use_graph = use_graph
+        dev = renderers[0].ds.device
+        self.stream = stream or torch.cuda.Stream(device=dev)
+        n = len(renderers)
+        self._arr = (CNrcSceneFrame * n)()
+        self._params = [r.params.c() for r in renderers]
+
+    def frame(self, frame: int, warmup: bool = False, accumulate: bool = False) -> None:
+        for k, r in enumerate(self.renderers):
+            r.cfg.warmup = int(warmup)
+            r.bufs.accum = r.accum.data_ptr() if accumulate else None
+            ds = r.ds
+            f = self._arr[k]
+            f.mlp = r.mlp.h
+            f.cfg = ctypes.addressof(r.cfg)
+            f.params = ctypes.addressof(self._params[k])
+            f.camara = ds.camera.data_ptr()
+            f.primitivas = ds.prims.data_ptr() if ds.prims is not None else None
+            f.luces = ds.lights.data_ptr()
+            f.bvh = ctypes.addressof(ds.bvh.ref)
+            f.tris_wt = ds.bvh.d_tris_wt
+            f.primitivas_bvh = ds.bvh.d_primitivas
+            f.buffers = ctypes.addressof(r.bufs)
+            f.num_primitivas, f.num_luces, f.num_prims_bvh = ds.n_prims, ds.n_lights, ds.n_mesh
+            f.ancho_img, f.alto_img = r.W, r.H
+            if accumulate:
+                r.frames_accumulated += 1
+        _lib.call("tfgNrcFrameBatch", len(self.renderers), self._arr, frame, int(self.use_graph),
+                  self.stream.cuda_stream)

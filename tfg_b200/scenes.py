@@ -307,6 +307,39 @@ def spheres_terrain(width=1920, height=1080, subdiv=5, terrain_n=580, seed=7, an
                  name=f"spheres_terrain_{len(F)}")
 
 
+def sized_terrain_scene(target_tris: int, width: int, height: int, n_lights: int, seed: int) -> Scene:
+    """The spheres-over-terrain layout at a chosen size: 16 displaced
+    icospheres carry about a third of `target_tris` (subdivision picked to
+    fit), the heightfield the rest; 1-4 point lights on a ring above the
+    scene.  Used for the batched multi-scene workload."""
+    rng = np.random.default_rng(seed)
+    subdiv = 0
+    while subdiv < 7 and 16 * 20 * 4 ** (subdiv + 1) <= target_tris // 3:
+        subdiv += 1
+    n_sph = 16 * 20 * 4 ** subdiv
+    terrain_n = max(8, int(round(np.sqrt(max(target_tris - n_sph, 128) / 2.0))))
+    s = spheres_terrain(width, height, subdiv=subdiv, terrain_n=terrain_n, seed=seed)
+    items = []
+    for k in range(n_lights):
+        a = 2.0 * np.pi * (k + float(rng.uniform(0.0, 0.5))) / n_lights
+        pos = (7.0 * np.cos(a), float(rng.uniform(5.0, 9.0)), -6.0 + 7.0 * np.sin(a))
+        items.append((pos, tuple(float(x) for x in rng.uniform(60.0, 140.0, 3))))
+    s.lights = lights(*items)
+    s.name = f"sized_terrain_{len(s.mesh)}_{width}x{height}_L{n_lights}"
+    return s
+
+
+# The batched workload: 12 scenes from 10k to 2M triangles (log-spaced),
+# 1-4 lights, 640x360 to 1920x1080.
+BATCH_RESOLUTIONS = [(640, 360), (960, 540), (1280, 720), (1600, 900), (1920, 1080)]
+
+
+def batch_scene(i: int, n: int = 12) -> Scene:
+    tris = int(round(np.exp(np.log(1e4) + (np.log(2e6) - np.log(1e4)) * i / max(1, n - 1))))
+    w, h = BATCH_RESOLUTIONS[(i * 7) % len(BATCH_RESOLUTIONS)]
+    return sized_terrain_scene(tris, w, h, 1 + (i % 4), seed=1000 + 17 * i)
+
+
 def tiny_box(width=64, height=64, subdiv=2, seed=3) -> Scene:
     s = box_icosphere(width, height, subdiv, seed)
     s.name = f"tiny_box_s{subdiv}"

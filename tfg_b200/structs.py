@@ -113,3 +113,16 @@ class CNrcBuffers(ctypes.Structure):
                 ("thr", ctypes.c_void_p), ("regs", ctypes.c_void_p), ("counter", ctypes.c_void_p),
                 ("ring_cap", ctypes.c_uint32), ("reserved", ctypes.c_uint32), ("tail_in", ctypes.c_void_p),
                 ("tail_pred", ctypes.c_void_p), ("train_buf", ctypes.c_void_p)]
+
+
+class CNrcSceneFrame(ctypes.Structure):
+    """TfgNrcSceneFrame: one scene of tfgNrcFrameBatch (104 bytes)."""
+    _fields_ = [("mlp", ctypes.c_void_p), ("cfg", ctypes.c_void_p), ("params", ctypes.c_void_p),
+                ("camara", ctypes.c_void_p), ("primitivas", ctypes.c_void_p), ("luces", ctypes.c_void_p),
+                ("bvh", ctypes.c_void_p), ("tris_wt", ctypes.c_void_p), ("primitivas_bvh", ctypes.c_void_p),
+                ("buffers", ctypes.c_void_p), ("num_primitivas", ctypes.c_int32), ("num_luces", ctypes.c_int32),
+                ("num_prims_bvh", ctypes.c_int32), ("ancho_img", ctypes.c_int32), ("alto_img", ctypes.c_int32),
+                ("reserved", ctypes.c_int32)]
+
+
+assert ctypes.sizeof(CNrcSceneFrame) == 104
