@@ -365,6 +365,21 @@ int  tfgMlpInference(TfgColorMLP* mlp, const TfgDatosMLP* in, TfgColor* out, uin
  * img[i] += throughput[i] * prediction where throughput[i] != 0. */
 int  tfgMlpInferenceComposite(TfgColorMLP* mlp, const TfgDatosMLP* in, const TfgColor* throughput, TfgColor* img,
                               uint32_t count, void* stream);
+/* No reference counterpart (tiny-cuda-nn runs its network in FP16): operand
+ * precision of later inference calls -- TFG_MLP_FP16 (default), TFG_MLP_BF16,
+ * or TFG_MLP_FP8 (E4M3 with per-layer scales).  Accumulation is FP32 in all
+ * three and training is unchanged; the BF16 / FP8 weight images are re-packed
+ * from the weight average before every such call. */
+#define TFG_MLP_FP16 0
+#define TFG_MLP_BF16 1
+#define TFG_MLP_FP8  2
+int  tfgMlpSetPrecision(TfgColorMLP* mlp, int32_t precision);
+/* No reference counterpart: FP8 input scales from the per-layer input amax of
+ * `count` samples run through the FP16 path (scale = 448 / (2 amax)).  Needed
+ * once before FP8 inference; afterwards every FP8 call re-derives the scales
+ * from the amax it sees on the first tile of each slot (delayed scaling), so
+ * they follow the model while it trains.  `in` must be 16-byte aligned. */
+int  tfgMlpCalibrate(TfgColorMLP* mlp, const TfgDatosMLP* in, uint32_t count, void* stream);
 /* FP32 parameter arrays (count = 23552, padded [out][in] per layer):
  * which = 0 weights, 1 EMA, 2 Adam m, 3 Adam v. */
 int  tfgMlpGetParams(TfgColorMLP* mlp, int which, float* host, uint32_t count);

@@ -84,3 +84,61 @@ def scrub(c):
     c = np.where(c < 0, 0, c)
     c = np.where(np.isnan(c), 0, c)
     return np.minimum(c, 1e5)
+
+
+def round_bf16(a) -> np.ndarray:
+    """Round to the nearest BF16 value (ties to even) and back to FP64."""
+    f = np.asarray(a, np.float32)
+    u = f.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def _e4m3_grid() -> np.ndarray:
+    """Every finite non-negative E4M3 value (bias 7, 3 mantissa bits, max 448)."""
+    vals = [m / 8.0 * 2.0 ** -6 for m in range(8)]                        # subnormals
+    vals += [(1.0 + m / 8.0) * 2.0 ** (e - 7) for e in range(1, 16) for m in range(8)
+             if not (e == 15 and m == 7)]                                  # S.1111.111 is NaN
+    return np.array(sorted(set(vals)))
+
+
+_E4M3 = _e4m3_grid()
+
+
+def round_e4m3(a) -> np.ndarray:
+    """Round to the nearest E4M3 value, ties to even mantissa, saturating at
+    +-448 (the satfinite conversion)."""
+    x = np.asarray(a, np.float64)
+    s, m = np.sign(x), np.minimum(np.abs(x), 448.0)
+    i = np.clip(np.searchsorted(_E4M3, m), 1, len(_E4M3) - 1)
+    lo, hi = _E4M3[i - 1], _E4M3[i]
+    pick_hi = (m - lo > hi - m) | ((m - lo == hi - m) & ((i % 2) == 0))   # grid index parity = mantissa parity
+    r = np.where(pick_hi, hi, lo)
+    r = np.where(m >= _E4M3[-1], _E4M3[-1], r)
+    return s * r
+
+
+def forward_quantized(W, x, kind: str, amax=None):
+    """Output (first 3 columns) of the network with operands rounded as the
+    BF16 or FP8 inference kernels round them: BF16 rounds weights and every
+    layer input; FP8 scales layer l's input by q = 448 / (2 amax[l]) and its
+    weights by wq = 448 / max|W_l|, rounds both to E4M3 and rescales the
+    FP64 product by 1 / (q wq)."""
+    h = x
+    for l, w in enumerate(W):
+        if kind == "bf16":
+            z = round_bf16(h) @ round_bf16(w).T
+        else:
+            q = 448.0 / (2.0 * amax[l])
+            wq = 448.0 / np.abs(w).max()
+            z = (round_e4m3(h * q) @ round_e4m3(w * wq).T) / (q * wq)
+        h = np.maximum(z, 0.0) if l < len(W) - 1 else z
+    return h[:, :3]
+
+
+def layer_input_amax(W, x) -> list[float]:
+    """Largest |input| of each layer (the encoded features' amax is at least 1)."""
+    _, hs, _ = forward(W, x)
+    out = [max(1.0, float(np.abs(x[:, 72:85]).max()))]
+    out += [float(np.abs(h).max()) for h in hs[1:len(W)]]
+    return out

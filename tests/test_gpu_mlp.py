@@ -8,7 +8,8 @@ import torch
 
 from oracle import mlp_oracle as mo
 from oracle import oracle as orc
-from tfg_b200.nrc import ColorMLP, EMA, WEIGHTS, split_layers
+from tfg_b200 import TfgError
+from tfg_b200.nrc import BF16, EMA, FP8, FP16, WEIGHTS, ColorMLP, split_layers
 from tfg_b200.structs import DATOS_MLP
 
 pytestmark = pytest.mark.gpu
@@ -176,4 +177,68 @@ def test_online_training_learns_a_signal(built):
     # inference with the EMA weights tracks the signal on held-out samples
     after = held_out_error()
     assert after < 0.2 * before, (before, after)
+    m.close()
+
+
+def _untrained_reference(m, d):
+    W = split_layers(m.get_params(WEIGHTS))
+    x = mo.encode(mo.rows15(d, LO, HI))
+    return [np.asarray(w, np.float64) for w in W], x
+
+
+def test_bf16_inference_matches_rounded_model(built):
+    m = ColorMLP(batch=4096, seed=21)
+    m.set_bounds(LO, HI)
+    n = 3000
+    d = _datos(np.random.default_rng(21), n)
+    W, x = _untrained_reference(m, d)
+    m.set_precision(BF16)
+    out = torch.zeros(n * 3, device="cuda")
+    m.inference(_dev(d), out, n)
+    torch.cuda.synchronize()
+    got = out.view(n, 3).cpu().numpy()
+    want = mo.scrub(mo.forward_quantized(W, x, "bf16"))
+    scale = np.abs(mo.forward(W, x)[0]).mean() + 1e-3
+    err = np.abs(got - want) / scale
+    assert np.isfinite(got).all()
+    assert err.mean() < 0.01 and err.max() < 0.08, (err.mean(), err.max())
+    m.close()
+
+
+def test_fp8_inference_matches_quantized_model(built):
+    m = ColorMLP(batch=4096, seed=22)
+    m.set_bounds(LO, HI)
+    n = 4096
+    d = _datos(np.random.default_rng(22), n)
+    dd = _dev(d)
+    W, x = _untrained_reference(m, d)
+    m.set_precision(FP8)
+    out = torch.zeros(n * 3, device="cuda")
+    with pytest.raises(TfgError):          # FP8 needs calibrated scales first
+        m.inference(dd, out, n)
+    m.calibrate(dd, n)
+    m.inference(dd, out, n)
+    torch.cuda.synchronize()
+    got = out.view(n, 3).cpu().numpy()
+    want = mo.scrub(mo.forward_quantized(W, x, "fp8", mo.layer_input_amax(W, x)))
+    ref = mo.scrub(mo.forward(W, x)[0])
+    scale = np.abs(ref).mean() + 1e-3
+    err = np.abs(got - want) / scale
+    assert np.isfinite(got).all()
+    # One E4M3 step is 12.5 % of a value, and the kernel's scales (from FP16
+    # activations) and features (hardware sin/cos) differ from the FP64
+    # emulation's by ~1e-3, so individual values round to neighbouring codes:
+    # compare on average, and require the kernel to be as accurate against
+    # the FP64 network as an exact E4M3 pipeline is.
+    assert err.mean() < 0.03, err.mean()
+    e_kernel = (np.abs(got - ref) / scale).mean()
+    e_exact = (np.abs(want - ref) / scale).mean()
+    assert e_kernel < 1.3 * e_exact + 0.01, (e_kernel, e_exact)
+    assert e_kernel < 0.15
+    # a second call uses the scales re-derived from the first call's amax
+    m.inference(dd, out, n)
+    torch.cuda.synchronize()
+    got2 = out.view(n, 3).cpu().numpy()
+    assert (np.abs(got2 - ref) / scale).mean() < 0.15
+    m.set_precision(FP16)
     m.close()

@@ -68,6 +68,8 @@ _PROTOS = {
     "tfgMlpSetHyperparams": (c_int32, [c_void_p, c_float, c_float, c_float, c_float, c_float]),
     "tfgMlpTrainStep": (c_int32, [c_void_p, c_void_p, c_uint32, POINTER(c_float), c_void_p]),
     "tfgMlpInference": (c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
+    "tfgMlpSetPrecision": (c_int32, [c_void_p, c_int32]),
+    "tfgMlpCalibrate": (c_int32, [c_void_p, c_void_p, c_uint32, c_void_p]),
     "tfgMlpInferenceComposite": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
     "tfgMlpGetParams": (c_int32, [c_void_p, c_int32, POINTER(c_float), c_uint32]),
     "tfgMlpSetParams": (c_int32, [c_void_p, POINTER(c_float), c_uint32]),

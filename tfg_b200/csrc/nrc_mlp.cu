@@ -27,6 +27,7 @@
 //   k_wgrad   dW = dZ^T H per layer, reduced over the batch with tcgen05
 //   k_adam    Adam + EMA on FP32 masters, re-packs the three weight images
 #include <cuda_bf16.h>
+#include <cuda_fp8.h>
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
@@ -78,6 +79,18 @@ constexpr uint32_t kSpinLimit = 1u << 26;
 struct Bounds {
     float lo[3], hi[3];
 };
+
+// Device state words of a cache model.
+enum : int {
+    S_STEP = 0,      // ColorMLP::step_counter (mlp.cpp:103), seed of the sample indices
+    S_ADAM_T = 1,    // Adam time step
+    S_NAVAIL = 2,    // training records available to this step
+    S_GATE = 3,      // 1: the cache's running error is low enough to answer queries
+    S_LOSS_EMA = 4,  // running loss (float bits)
+    S_F8_VER = 5,    // S_ADAM_T + 1 of the weights in the FP8 image (0: not packed)
+    S_WORDS = 8
+};
+
 
 __device__ int g_mlp_error;   // set when a bounded wait gives up (TFG_E_TIMEOUT)
 
@@ -183,126 +196,193 @@ __device__ __forceinline__ bool all_ok(bool ok) { return __syncthreads_and(ok ? 
 
 // ------------------------------------------------------------------ inference
 // Persistent kernel, one CTA per SM.  The CTA runs kSlots tiles of 128
-// queries at a time; each tile ("slot") has its own 128 TMEM columns (64 FP32
-// accumulator columns, then the FP16 A operand of the next layer, two features
-// per column), its own input staging buffer, MMA mbarrier and named barrier,
-// and is served by kSplit warpgroups: thread t of every warpgroup of the slot
-// owns row t (TMEM lane t).  With two warpgroups, the first encodes the x and y
-// bands and converts accumulator columns 0..31, the second encodes the z bands
-// and the other inputs and converts columns 32..63, which halves the
-// per-layer latency chain (MMA -> TMEM load -> ReLU/pack -> TMEM store ->
-// barrier -> next MMA) each tile walks through.  Only the weights (51,200 B,
-// bulk-copied once) and the staged inputs live in shared memory, so the
-// tensor pipe reads B from shared memory and A from TMEM.
-#ifndef TFG_INFER_SPLIT
-#define TFG_INFER_SPLIT 1
-#endif
-#ifndef TFG_INFER_SLOTS
-#define TFG_INFER_SLOTS 4
-#endif
-constexpr int kSplit = TFG_INFER_SPLIT;
-constexpr int kSlots = TFG_INFER_SLOTS;
-constexpr int kSlotThreads = 128 * kSplit;
-constexpr int kInferThreads = kSlotThreads * kSlots;
+// queries at a time; each tile ("slot") is one warpgroup with its own 128
+// TMEM columns (64 FP32 accumulator columns, then the A operand of the next
+// layer), its own input staging buffer, MMA mbarrier and named barrier;
+// thread t owns row t (TMEM lane t).  Only the weights (bulk-copied once) and
+// the staged inputs live in shared memory: the tensor pipe reads B from
+// shared memory and A from TMEM.  Per layer: MMAs (issued from a converged
+// warp through elect.sync) -> commit -> TMEM load -> scale / ReLU / pack ->
+// TMEM store of the next A operand -> barrier.
+//
+// Precisions (template PREC): FP16 and BF16 operands (kind::f16, K = 16 per
+// MMA, two features per TMEM column) or FP8 E4M3 with per-layer scales
+// (kind::f8f6f4, K = 32 per MMA, four features per column): inputs of layer
+// l are quantised as x * q[l] (q = 448 / (2 * amax of the layer's input)),
+// weights as w * wq[l] (wq = 448 / amax|W_l|), and the accumulator is
+// rescaled by 1 / (q[l] * wq[l]).  All accumulate in FP32.
+enum : int { kPrecF16 = 0, kPrecBF16 = 1, kPrecF8 = 2 };
+constexpr int kSlots = 4;
+constexpr int kInferThreads = 128 * kSlots;
 constexpr int kRowBytes = (int)sizeof(TfgDatosMLP);              // 112
 constexpr int kStageBytes = kTile * kRowBytes;                   // 14336
 constexpr int kInferSmemStage = 51200 + 1024;
 constexpr int kInferSmem = kInferSmemStage + kSlots * kStageBytes;
-static_assert(kSplit == 1 || kSplit == 2, "one or two warpgroups per tile");
 static_assert(kSlots * 128 <= 512, "TMEM: 128 columns per slot");
-static_assert(kInferThreads <= 1024, "threads per CTA");
 static_assert(kInferSmem + 1024 <= 227 * 1024, "inference shared memory");
+// FP8 weight image: one SW128 region per layer (K <= 128 bytes per row).
+__host__ __device__ constexpr int kF8Off(int l) { return l < kLayers - 1 ? l * 8192 : 40960; }
+constexpr int kF8Bytes = 43008;
+// Scale words of the FP8 path (device floats): q[l], wq[l] and the running
+// amax of each layer's input observed by the last inference calls.
+constexpr int kF8Q = 0, kF8WQ = 8, kF8Amax = 16, kF8Words = 24;
+constexpr float kF8Max = 448.0f;
 
-__device__ __forceinline__ void slot_sync(int id) {
-    asm volatile("bar.sync %0, %1;" ::"r"(id), "n"(kSlotThreads) : "memory");
-}
+__device__ __forceinline__ void slot_sync(int id) { asm volatile("bar.sync %0, 128;" ::"r"(id) : "memory"); }
 
-// AND of `p` over the slot's threads (all of them get the result).
+// AND of `p` over the slot's 128 threads (all of them get the result).
 __device__ __forceinline__ bool slot_all(int id, bool p) {
     uint32_t r;
     asm volatile(
         "{\n\t.reg .pred pi, po;\n\t"
         "setp.ne.u32 pi, %1, 0;\n\t"
-        "bar.red.and.pred po, %2, %3, pi;\n\t"
+        "bar.red.and.pred po, %2, 128, pi;\n\t"
         "selp.u32 %0, 1, 0, po;\n\t}\n"
         : "=r"(r)
-        : "r"((uint32_t)p), "r"(id), "n"(kSlotThreads)
+        : "r"((uint32_t)p), "r"(id)
         : "memory");
     return r != 0;
 }
 
-// max(x, 0) of two floats packed as FP16x2 (ReLU fused into the conversion).
+// max(x, 0) of two floats packed as FP16x2 / BF16x2 (ReLU fused into the
+// conversion); lo in the low half.
 __device__ __forceinline__ uint32_t relu_h2(float lo, float hi) {
     uint32_t r;
     asm("cvt.rn.relu.f16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
     return r;
 }
-
-// 12 frequency bands of one position coordinate (already mapped to [0,1]):
-// (sin, cos)(2^k pi p) as FP16 pairs, double-angle recurrence from a hardware
-// sin/cos of the base band.
-__device__ __forceinline__ void encode_axis(float p, uint32_t* w) {
-    float s, c;
-    __sincosf(kPiF * p, &s, &c);
-#pragma unroll
-    for (int k = 0; k < kBands; ++k) {
-        w[k] = pack_h2(s, c);
-        const float s2 = 2.0f * s * c;
-        const float c2 = (c - s) * (c + s);
-        s = s2;
-        c = c2;
+__device__ __forceinline__ uint32_t relu_bf2(float lo, float hi) {
+    uint32_t r;
+    asm("cvt.rn.relu.bf16x2.f32 %0, %1, %2;" : "=r"(r) : "f"(hi), "f"(lo));
+    return r;
+}
+// Four floats as E4M3 (round to nearest, saturating), element a in the lowest
+// byte; the RELU form clamps negatives to zero.
+template <bool RELU>
+__device__ __forceinline__ uint32_t pack_e4m3x4(float a, float b, float c, float d) {
+    uint16_t lo, hi;
+    if (RELU) {
+        asm("cvt.rn.satfinite.relu.e4m3x2.f32 %0, %1, %2;" : "=h"(lo) : "f"(b), "f"(a));
+        asm("cvt.rn.satfinite.relu.e4m3x2.f32 %0, %1, %2;" : "=h"(hi) : "f"(d), "f"(c));
+    } else {
+        asm("cvt.rn.satfinite.e4m3x2.f32 %0, %1, %2;" : "=h"(lo) : "f"(b), "f"(a));
+        asm("cvt.rn.satfinite.e4m3x2.f32 %0, %1, %2;" : "=h"(hi) : "f"(d), "f"(c));
     }
+    return (uint32_t)lo | ((uint32_t)hi << 16);
 }
 
-// Encoded features 0..47 (FP16 pairs) of a staged row: words 0..23 are the x
-// and y bands, 24..35 the z bands, 36..42 direction, normal, albedos and the
-// constant 1, 43..47 zero.  `part` 0 writes words 0..23, part 1 words 24..47,
-// part -1 all of them, into TMEM columns of the same index.
-__device__ __forceinline__ void encode_to_tmem(const TfgDatosMLP* r, const Bounds& b, int part, uint32_t ta) {
-    if (part <= 0) {
+template <int PREC>
+__device__ __forceinline__ uint32_t pack2(float a, float b) {
+    return PREC == kPrecBF16 ? pack_bf2(a, b) : pack_h2(a, b);
+}
+
+// Encoded features of one staged row as 96 floats' worth of packed words:
+// features 0..71 are (sin, cos)(2^k pi p) of the x, y, z bands (double-angle
+// recurrence from a hardware sin/cos of the base band), 72..84 direction,
+// normal, albedos and the constant 1, 85..95 zero.  FP16 / BF16 write 48 TMEM
+// columns (two features each), FP8 24 columns (four each, scaled by q0).
+// Returns the largest |feature| of 72..84 (the bands are within [-1, 1]).
+template <int PREC>
+__device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Bounds& b, float q0, uint32_t ta) {
+    const float misc[13] = {(float)r->direccion.x, (float)r->direccion.y, (float)r->direccion.z,
+                            (float)r->normal.x,    (float)r->normal.y,    (float)r->normal.z,
+                            r->difuso.r,           r->difuso.g,           r->difuso.b,
+                            r->especular.r,        r->especular.g,        r->especular.b, 1.0f};
+    float amax = 1.0f;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) amax = fmaxf(amax, fabsf(misc[k]));
+    const float p[3] = {unit_clamp((float)r->posicion.x, b.lo[0], b.hi[0]),
+                        unit_clamp((float)r->posicion.y, b.lo[1], b.hi[1]),
+                        unit_clamp((float)r->posicion.z, b.lo[2], b.hi[2])};
+    if constexpr (PREC == kPrecF8) {
         uint32_t w[24];
-        encode_axis(unit_clamp((float)r->posicion.x, b.lo[0], b.hi[0]), w);
-        encode_axis(unit_clamp((float)r->posicion.y, b.lo[1], b.hi[1]), w + 12);
+#pragma unroll
+        for (int j = 0; j < 3; ++j) {
+            float s, c;
+            __sincosf(kPiF * p[j], &s, &c);
+#pragma unroll
+            for (int k = 0; k < kBands; k += 2) {
+                const float s1 = 2.0f * s * c, c1 = (c - s) * (c + s);
+                w[6 * j + k / 2] = pack_e4m3x4<false>(s * q0, c * q0, s1 * q0, c1 * q0);
+                s = 2.0f * s1 * c1;
+                c = (c1 - s1) * (c1 + s1);
+            }
+        }
+        w[18] = pack_e4m3x4<false>(misc[0] * q0, misc[1] * q0, misc[2] * q0, misc[3] * q0);
+        w[19] = pack_e4m3x4<false>(misc[4] * q0, misc[5] * q0, misc[6] * q0, misc[7] * q0);
+        w[20] = pack_e4m3x4<false>(misc[8] * q0, misc[9] * q0, misc[10] * q0, misc[11] * q0);
+        w[21] = pack_e4m3x4<false>(q0, 0.0f, 0.0f, 0.0f);
+        w[22] = 0u;
+        w[23] = 0u;
         umma::tmem_st16(ta, *reinterpret_cast<const uint32_t(*)[16]>(w));
         umma::tmem_st8(ta + 16u, w + 16);
-    }
-    if (part != 0) {
-        uint32_t w[24];
-        encode_axis(unit_clamp((float)r->posicion.z, b.lo[2], b.hi[2]), w);
-        w[12] = pack_h2((float)r->direccion.x, (float)r->direccion.y);
-        w[13] = pack_h2((float)r->direccion.z, (float)r->normal.x);
-        w[14] = pack_h2((float)r->normal.y, (float)r->normal.z);
-        w[15] = pack_h2(r->difuso.r, r->difuso.g);
-        w[16] = pack_h2(r->difuso.b, r->especular.r);
-        w[17] = pack_h2(r->especular.g, r->especular.b);
-        w[18] = pack_h2(1.0f, 0.0f);
+    } else {
+        uint32_t w[48];
 #pragma unroll
-        for (int k = 19; k < 24; ++k) w[k] = 0u;
-        umma::tmem_st8(ta + 24u, w);
-        umma::tmem_st16(ta + 32u, *reinterpret_cast<const uint32_t(*)[16]>(w + 8));
+        for (int j = 0; j < 3; ++j) {
+            float s, c;
+            __sincosf(kPiF * p[j], &s, &c);
+#pragma unroll
+            for (int k = 0; k < kBands; ++k) {
+                w[12 * j + k] = pack2<PREC>(s, c);
+                const float s2 = 2.0f * s * c;
+                const float c2 = (c - s) * (c + s);
+                s = s2;
+                c = c2;
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < 6; ++k) w[36 + k] = pack2<PREC>(misc[2 * k], misc[2 * k + 1]);
+        w[42] = pack2<PREC>(1.0f, 0.0f);
+#pragma unroll
+        for (int k = 43; k < 48; ++k) w[k] = 0u;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) umma::tmem_st16(ta + 16u * c, *reinterpret_cast<const uint32_t(*)[16]>(w + 16 * c));
     }
+    return amax;
 }
 
+// Largest value over the warp, folded into *dst (values are >= 0, so their
+// bit patterns order like the floats).
+__device__ __forceinline__ void warp_amax(float v, float* dst) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xFFFFFFFFu, v, o));
+    if ((threadIdx.x & 31) == 0 && v > 0.0f) atomicMax(reinterpret_cast<int*>(dst), __float_as_int(v));
+}
+
+// `f8` (FP8 only): scale words.  TRACK: the per-layer input amax is folded
+// into amax[0..5]; with `amax_all` every tile contributes, otherwise only the
+// first tile of each slot (the delayed-scaling estimate).
+template <int PREC, bool TRACK>
 __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
                                                             const uint32_t* __restrict__ n_dev, Bounds bounds,
                                                             const uint8_t* __restrict__ wimg,
                                                             TfgColor* __restrict__ out, TfgColor* __restrict__ img,
-                                                            const TfgColor* __restrict__ thr) {
+                                                            const TfgColor* __restrict__ thr,
+                                                            const float* __restrict__ f8, float* amax, int amax_all) {
+    constexpr bool kF8 = PREC == kPrecF8;
+    constexpr uint32_t kWBytes = kF8 ? kF8Bytes : kFwdBytes;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sw = smem;
     __shared__ uint64_t mb_w, mb_mma[kSlots], mb_in[kSlots];
     __shared__ uint32_t tslot;
     const int tid = threadIdx.x, warp = tid >> 5, q = warp & 3, t = tid & 127;
-    const int slot = tid / kSlotThreads;
-    const int part = kSplit == 1 ? -1 : (tid / 128) % kSplit;     // warpgroup within the slot
-    const bool leader = tid % kSlotThreads == 0;
-    const bool issuer_warp = tid % kSlotThreads < 32;             // first warp of the slot issues its MMAs
+    const int slot = tid / 128;
+    const bool leader = t == 0;
+    const bool issuer_warp = t < 32;                               // first warp of the slot issues its MMAs
     const int bar = 1 + slot;
     uint8_t* stage = smem + kInferSmemStage + slot * kStageBytes;
     const uint32_t n = n_dev ? min(*n_dev, n_max) : n_max;
     const uint32_t ntiles = (n + kTile - 1) / kTile;
     if (blockIdx.x * kSlots >= ntiles) return;
+    // FP8 scales: input quantisation of each layer and the accumulator rescale.
+    float qs[kLayers], deq[kLayers];
+#pragma unroll
+    for (int l = 0; l < kLayers; ++l) {
+        qs[l] = kF8 ? f8[kF8Q + l] : 1.0f;
+        deq[l] = kF8 ? 1.0f / (f8[kF8Q + l] * f8[kF8WQ + l]) : 1.0f;
+    }
     if (warp == 0) umma::tmem_alloc(&tslot, 512);
     if (tid == 0) {
         umma::mbar_init(&mb_w, 1);
@@ -328,8 +408,8 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
                        &mb_in[slot]);
     };
     if (tid == 0) {
-        umma::mbar_expect_tx(&mb_w, kFwdBytes);
-        umma::bulk_g2s(sw, wimg, kFwdBytes, &mb_w);
+        umma::mbar_expect_tx(&mb_w, kWBytes);
+        umma::bulk_g2s(sw, wimg, kWBytes, &mb_w);
     }
     uint32_t tile = blockIdx.x * kSlots + slot;
     bool pending = tile < ntiles;
@@ -337,16 +417,20 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
     bool ok = umma::mbar_wait(&mb_w, 0, kSpinLimit);
     ok = __syncthreads_and(ok ? 1 : 0) != 0;
     uint32_t mph = 0, iph = 0;
-    for (; tile < ntiles && ok; tile += tstride) {
+    bool first = true;
+    for (; tile < ntiles && ok; tile += tstride, first = false) {
         const uint32_t row = tile * kTile + (uint32_t)t;
         const bool valid = row < n;
+        const bool track = TRACK && (amax_all || first);
         ok = slot_all(bar, umma::mbar_wait(&mb_in[slot], iph, kSpinLimit));
         if (!ok) break;
         pending = false;
         iph ^= 1u;
         // rows past the end of a partial tile encode stale staging bytes; the
         // rows of the MLP are independent and those outputs are never stored
-        encode_to_tmem(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds, part, tmem_a + tlane);
+        const float a0 = encode_to_tmem<PREC>(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds,
+                                              qs[0], tmem_a + tlane);
+        if (track) warp_amax(valid ? a0 : 0.0f, &amax[0]);
         umma::tmem_wait_st();
         umma::fence_before_sync();
         slot_sync(bar);   // staging buffer consumed, A operand of layer 0 in TMEM
@@ -365,14 +449,21 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
             const bool last = l == kLayers - 1;
             if (issuer_warp) {
                 umma::fence_after_sync();
-                constexpr uint32_t id_hid = umma::idesc_f16(kTile, kHid, false);
-                constexpr uint32_t id_out = umma::idesc_f16(kTile, kOutPad, false);
+                constexpr uint32_t id_hid = umma::idesc_f16(kTile, kHid, PREC == kPrecBF16);
+                constexpr uint32_t id_out = umma::idesc_f16(kTile, kOutPad, PREC == kPrecBF16);
                 if (umma::elect_one()) {
+                    if constexpr (kF8) {
 #pragma unroll
-                    for (int s = 0; s < kCols(l) / 16; ++s) {
-                        const uint64_t bd =
-                            wdesc + (uint64_t)((kFOff(l) + (s >> 2) * (kRows(l) * 128) + (s & 3) * 32) >> 4);
-                        umma::mma_f16_ta(tmem, tmem_a + 8u * s, bd, last ? id_out : id_hid, s > 0);
+                        for (int s = 0; s < kCols(l) / 32; ++s)
+                            umma::mma_f8_ta(tmem, tmem_a + 8u * s, wdesc + (uint64_t)((kF8Off(l) + s * 32) >> 4),
+                                            last ? id_out : id_hid, s > 0);
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < kCols(l) / 16; ++s) {
+                            const uint64_t bd =
+                                wdesc + (uint64_t)((kFOff(l) + (s >> 2) * (kRows(l) * 128) + (s & 3) * 32) >> 4);
+                            umma::mma_f16_ta(tmem, tmem_a + 8u * s, bd, last ? id_out : id_hid, s > 0);
+                        }
                     }
                     umma::mma_commit(&mb_mma[slot]);
                 }
@@ -383,37 +474,56 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
             if (!ok) break;
             umma::fence_after_sync();
             if (!last) {
+                float lmax = 0.0f;
 #pragma unroll
                 for (int h = 0; h < 2; ++h) {
-                    if (kSplit == 2 && h != part) continue;
                     float v[32];
                     umma::tmem_ld32(tmem + tlane + 32u * h, v);
-                    uint32_t r[16];
+                    if constexpr (kF8) {
+                        // dequantise, ReLU, requantise for the next layer
+                        const float sc = deq[l] * qs[l + 1];
+                        uint32_t r[8];
 #pragma unroll
-                    for (int i = 0; i < 16; ++i) r[i] = relu_h2(v[2 * i], v[2 * i + 1]);
-                    umma::tmem_st16(tmem_a + tlane + 16u * h, r);
+                        for (int i = 0; i < 8; ++i)
+                            r[i] = pack_e4m3x4<true>(v[4 * i] * sc, v[4 * i + 1] * sc, v[4 * i + 2] * sc,
+                                                     v[4 * i + 3] * sc);
+                        umma::tmem_st8(tmem_a + tlane + 8u * h, r);
+                        if (track) {
+#pragma unroll
+                            for (int i = 0; i < 32; ++i) lmax = fmaxf(lmax, v[i] * deq[l]);
+                        }
+                    } else {
+                        uint32_t r[16];
+#pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                            r[i] = PREC == kPrecBF16 ? relu_bf2(v[2 * i], v[2 * i + 1]) : relu_h2(v[2 * i], v[2 * i + 1]);
+                        umma::tmem_st16(tmem_a + tlane + 16u * h, r);
+                        if (track) {
+#pragma unroll
+                            for (int i = 0; i < 32; ++i) lmax = fmaxf(lmax, v[i]);
+                        }
+                    }
                 }
+                if (track) warp_amax(valid ? lmax : 0.0f, &amax[l + 1]);
                 umma::tmem_wait_st();
                 umma::fence_before_sync();
                 slot_sync(bar);
             } else {
-                if (part <= 0) {
-                    float v[16];
-                    umma::tmem_ld16(tmem + tlane, v);
-                    if (valid) {
-                        const float cr = scrub(v[0]), cg = scrub(v[1]), cb = scrub(v[2]);
-                        if (img) {
-                            const TfgColor th = thr[row];
-                            if (th.r > 0 || th.g > 0 || th.b > 0) {
-                                TfgColor f = img[row];
-                                f.r = f.r + th.r * cr;
-                                f.g = f.g + th.g * cg;
-                                f.b = f.b + th.b * cb;
-                                img[row] = f;
-                            }
-                        } else {
-                            out[row] = TfgColor{cr, cg, cb};
+                float v[16];
+                umma::tmem_ld16(tmem + tlane, v);
+                if (valid && (out || img)) {
+                    const float cr = scrub(v[0] * deq[l]), cg = scrub(v[1] * deq[l]), cb = scrub(v[2] * deq[l]);
+                    if (img) {
+                        const TfgColor th = thr[row];
+                        if (th.r > 0 || th.g > 0 || th.b > 0) {
+                            TfgColor f = img[row];
+                            f.r = f.r + th.r * cr;
+                            f.g = f.g + th.g * cg;
+                            f.b = f.b + th.b * cb;
+                            img[row] = f;
                         }
+                    } else {
+                        out[row] = TfgColor{cr, cg, cb};
                     }
                 }
                 umma::fence_before_sync();
@@ -427,6 +537,56 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
     if (warp == 0) umma::tmem_dealloc(tslot, 512);
 }
 
+// FP8 inference image from the debiased weight average, one block per
+// layer: the layer's weight scale wq = 448 / amax|W| goes to f8[kF8WQ + l].
+// Skipped when the image already holds the weights of this Adam step.
+__global__ void __launch_bounds__(1024) k_pack_f8(const float* __restrict__ w, const float* __restrict__ ema,
+                                                  const uint32_t* __restrict__ state, float decay,
+                                                  uint8_t* __restrict__ img, float* f8) {
+    __shared__ float smax[32];
+    const uint32_t t_adam = state[S_ADAM_T];
+    if (state[S_F8_VER] == t_adam + 1u) return;
+    const int l = blockIdx.x;
+    const float debias = t_adam > 0u ? 1.0f - powf(decay, (float)t_adam) : 0.0f;
+    const int cnt = kRows(l) * kCols(l);
+    float m = 0.0f;
+    for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
+        const int i = kPOff(l) + j;
+        m = fmaxf(m, fabsf(debias > 0.0f ? ema[i] / debias : w[i]));
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xFFFFFFFFu, m, o));
+    if ((threadIdx.x & 31) == 0) smax[threadIdx.x >> 5] = m;
+    __syncthreads();
+    m = 0.0f;
+    for (int k = 0; k < (int)(blockDim.x >> 5); ++k) m = fmaxf(m, smax[k]);
+    const float wq = m > 0.0f ? kF8Max / m : 1.0f;
+    if (threadIdx.x == 0) f8[kF8WQ + l] = wq;
+    // every byte of the layer's 128-byte rows: K index c (zero past kCols)
+    for (int j = threadIdx.x; j < kRows(l) * 128; j += blockDim.x) {
+        const int r = j / 128, c = j % 128;
+        float x = 0.0f;
+        if (c < kCols(l)) {
+            const int i = kPOff(l) + r * kCols(l) + c;
+            x = (debias > 0.0f ? ema[i] / debias : w[i]) * wq;
+        }
+        __nv_fp8_e4m3 e(x);
+        img[kF8Off(l) + umma::sw128_offset(r, c >> 4) + (c & 15)] = *reinterpret_cast<uint8_t*>(&e);
+    }
+}
+
+// After an FP8 inference call: new input scales from the observed amax (with
+// a factor-2 margin; a layer that saw nothing keeps its scale), amax cleared,
+// and the FP8 image marked current for this Adam step.
+__global__ void k_f8_update(float* f8, uint32_t* state, int mark_packed) {
+    const int l = threadIdx.x;
+    if (l == 0 && mark_packed) state[S_F8_VER] = state[S_ADAM_T] + 1u;
+    if (l >= kLayers) return;
+    const float a = f8[kF8Amax + l];
+    if (a > 0.0f) f8[kF8Q + l] = kF8Max / (2.0f * a);
+    f8[kF8Amax + l] = 0.0f;
+}
+
 // ------------------------------------------------------------------ training forward + backward
 // Shared memory: fwd weights 51200 | bwd weights 40960 | A 32768.
 constexpr int kTrainSmemF = 0;
@@ -437,15 +597,6 @@ constexpr int kTrainSmem = kTrainSmemA + 2 * kTile * 128;   // 125952
 // Device-resident training state (one per model): read by the kernels so a
 // whole frame can be enqueued (and captured in a CUDA graph) without reading
 // anything back to the host.
-enum : int {
-    S_STEP = 0,      // ColorMLP::step_counter (mlp.cpp:103), seed of the sample indices
-    S_ADAM_T = 1,    // Adam time step
-    S_NAVAIL = 2,    // training records available to this step
-    S_GATE = 3,      // 1: the cache's running error is low enough to answer queries
-    S_LOSS_EMA = 4,  // running loss (float bits)
-    S_WORDS = 8
-};
-
 struct TrainArgs {
     const TfgDatosMLP* buf;      // training records (targets in .color)
     const uint32_t* state;       // S_NAVAIL records available, S_STEP seed
@@ -732,6 +883,7 @@ struct AdamArgs {
     uint8_t* fwd;    // FP16 forward image of w
     uint8_t* bwd;    // BF16 W^T image of w
     uint8_t* inf;    // FP16 image of the debiased EMA
+    uint8_t* inf_bf; // BF16 image of the debiased EMA (same layout)
     float lr, beta1, beta2, eps, decay;
     float grad_scale;              // 1 / (batch * 3)
     const uint32_t* state;         // S_ADAM_T before this step, S_NAVAIL
@@ -780,6 +932,7 @@ __global__ void k_adam(AdamArgs a) {
                          2 * (c & 7);
     *reinterpret_cast<__half*>(a.fwd + off) = __float2half_rn(w);
     *reinterpret_cast<__half*>(a.inf + off) = __float2half_rn(ew);
+    *reinterpret_cast<__nv_bfloat16*>(a.inf_bf + off) = __float2bfloat16_rn(ew);
     if (l >= 1) {
         // backward image: W^T, row = c (input unit), K index = r (output unit)
         const uint32_t boff = (uint32_t)kBOff(l) + umma::sw128_offset(c, r >> 3) + 2 * (r & 7);
@@ -821,6 +974,11 @@ struct ColorMlp {
     float* loss = nullptr;
     uint32_t* dstate = nullptr;  // mlp::S_* words
     float gate = 0.0f;           // cache-query gate threshold on the running loss (<= 0: always open)
+    int prec = mlp::kPrecF16;    // inference operand precision
+    uint8_t* inf_bf = nullptr;   // BF16 inference image (written with the FP16 one)
+    uint8_t* inf_f8 = nullptr;   // FP8 inference image (re-packed when the weights changed)
+    float* f8 = nullptr;         // FP8 scale words (mlp::kF8*)
+    bool f8_calibrated = false;
     uint32_t act_tiles = 0;
     int sms = 148;
 };
@@ -841,7 +999,7 @@ uint64_t splitmix(uint64_t& s) {
 int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
     mlp::AdamArgs a;
     a.w = n->w; a.m = n->m; a.v = n->v; a.ema = n->ema; a.grad = n->grad;
-    a.fwd = n->fwd; a.bwd = n->bwd; a.inf = n->inf;
+    a.fwd = n->fwd; a.bwd = n->bwd; a.inf = n->inf; a.inf_bf = n->inf_bf;
     a.lr = n->lr; a.beta1 = n->beta1; a.beta2 = n->beta2; a.eps = n->eps; a.decay = n->decay;
     a.grad_scale = 1.0f / (3.0f * (float)n->batch);
     a.state = n->dstate;
@@ -923,12 +1081,50 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
     if (count == 0) return ok();
     if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
         return fail(TFG_E_INVALID, "mlp inference: input buffer must be 16-byte aligned");
+    if (n->prec == mlp::kPrecF8 && !n->f8_calibrated)
+        return fail(TFG_E_INVALID, "mlp inference: FP8 needs tfgMlpCalibrate first");
     const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
     const uint32_t grid = std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, (uint32_t)n->sms);
-    mlp::k_infer<<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(in, count, n_dev, n->bounds, n->inf, out,
-                                                                            img, thr);
-    cudaError_t e = cudaGetLastError();
+    const size_t smem = mlp::kInferSmem + 1024;
+    cudaError_t e = cudaSuccess;
+    if (n->prec == mlp::kPrecF16) {
+        mlp::k_infer<mlp::kPrecF16, false><<<grid, mlp::kInferThreads, smem, s>>>(in, count, n_dev, n->bounds, n->inf,
+                                                                                out, img, thr, nullptr, nullptr, 0);
+    } else if (n->prec == mlp::kPrecBF16) {
+        mlp::k_infer<mlp::kPrecBF16, false><<<grid, mlp::kInferThreads, smem, s>>>(in, count, n_dev, n->bounds,
+                                                                                 n->inf_bf, out, img, thr, nullptr,
+                                                                                 nullptr, 0);
+    } else {
+        mlp::k_pack_f8<<<mlp::kLayers, 1024, 0, s>>>(n->w, n->ema, n->dstate, n->decay, n->inf_f8, n->f8);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "mlp inference: FP8 weight image");
+        mlp::k_infer<mlp::kPrecF8, true><<<grid, mlp::kInferThreads, smem, s>>>(
+            in, count, n_dev, n->bounds, n->inf_f8, out, img, thr, n->f8, n->f8 + mlp::kF8Amax, 0);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "mlp inference");
+        mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 1);
+    }
+    e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp inference");
+    return ok();
+}
+
+// Per-layer input amax over `count` samples through the FP16 path (every
+// tile), turned into the FP8 input scales.
+int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStream_t s) {
+    if (count == 0) return fail(TFG_E_INVALID, "tfgMlpCalibrate: no samples");
+    if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
+        return fail(TFG_E_INVALID, "tfgMlpCalibrate: input buffer must be 16-byte aligned");
+    const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
+    const uint32_t grid = std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, (uint32_t)n->sms);
+    cudaError_t e = cudaMemsetAsync(n->f8 + mlp::kF8Amax, 0, mlp::kLayers * sizeof(float), s);
+    if (e != cudaSuccess) return cuda_fail(e, "tfgMlpCalibrate");
+    mlp::k_infer<mlp::kPrecF16, true><<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(
+        in, count, nullptr, n->bounds, n->inf, nullptr, nullptr, nullptr, nullptr, n->f8 + mlp::kF8Amax, 1);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) { mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 0); e = cudaGetLastError(); }
+    if (e != cudaSuccess) return cuda_fail(e, "tfgMlpCalibrate");
+    n->f8_calibrated = true;
     return ok();
 }
 
@@ -976,12 +1172,18 @@ extern "C" int tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint6
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->fwd, M::kFwdBytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->bwd, M::kBwdBytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf, M::kFwdBytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf_bf, M::kFwdBytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf_f8, M::kF8Bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->f8, M::kF8Words * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->loss, sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->dstate, M::S_WORDS * sizeof(uint32_t));
     if (e != cudaSuccess) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return tfg::cuda_fail(e, "tfgMlpCreate"); }
     cudaMemset(n->fwd, 0, M::kFwdBytes);
     cudaMemset(n->bwd, 0, M::kBwdBytes);
     cudaMemset(n->inf, 0, M::kFwdBytes);
+    cudaMemset(n->inf_bf, 0, M::kFwdBytes);
+    cudaMemset(n->inf_f8, 0, M::kF8Bytes);
+    cudaMemset(n->f8, 0, M::kF8Words * sizeof(float));
     cudaMemset(n->dstate, 0, M::S_WORDS * sizeof(uint32_t));
     // Uniform (-s, s) initialisation with s = sqrt(6 / (fan_in + fan_out)) per layer.
     std::vector<float> h(M::kParams, 0.0f);
@@ -1008,7 +1210,11 @@ extern "C" int tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint6
     if (int rc = tfg::repack(n, 0, false, 1)) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return rc; }
     static bool attrs = false;
     if (!attrs) {
-        cudaFuncSetAttribute(M::k_infer, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kInferSmem + 1024);
+        const int ism = M::kInferSmem + 1024;
+        cudaFuncSetAttribute(M::k_infer<M::kPrecF16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+        cudaFuncSetAttribute(M::k_infer<M::kPrecF16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+        cudaFuncSetAttribute(M::k_infer<M::kPrecBF16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+        cudaFuncSetAttribute(M::k_infer<M::kPrecF8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
         cudaFuncSetAttribute(M::k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kTrainSmem + 1024);
         cudaFuncSetAttribute(M::k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
         attrs = true;
@@ -1023,7 +1229,7 @@ extern "C" void tfgMlpDestroy(TfgColorMLP* h) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n) return;
     for (void* p : {(void*)n->w, (void*)n->m, (void*)n->v, (void*)n->ema, (void*)n->grad, (void*)n->fwd, (void*)n->bwd,
-                    (void*)n->inf, (void*)n->loss, (void*)n->dstate})
+                    (void*)n->inf, (void*)n->inf_bf, (void*)n->inf_f8, (void*)n->f8, (void*)n->loss, (void*)n->dstate})
         if (p) cudaFree(p);
     for (int l = 0; l < M::kLayers; ++l) {
         if (n->hT[l]) cudaFree(n->hT[l]);
@@ -1052,6 +1258,21 @@ extern "C" int tfgMlpInference(TfgColorMLP* h, const TfgDatosMLP* in, TfgColor* 
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n || (count && (!in || !out))) return tfg::fail(TFG_E_INVALID, "tfgMlpInference: null argument");
     return tfg::infer_impl(n, in, out, nullptr, nullptr, count, nullptr, (cudaStream_t)stream);
+}
+
+extern "C" int tfgMlpSetPrecision(TfgColorMLP* h, int32_t precision) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n) return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: null model");
+    if (precision != TFG_MLP_FP16 && precision != TFG_MLP_BF16 && precision != TFG_MLP_FP8)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: unknown precision");
+    n->prec = precision;
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpCalibrate(TfgColorMLP* h, const TfgDatosMLP* in, uint32_t count, void* stream) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !in) return tfg::fail(TFG_E_INVALID, "tfgMlpCalibrate: null argument");
+    return tfg::calibrate_impl(n, in, count, (cudaStream_t)stream);
 }
 
 extern "C" int tfgMlpInferenceComposite(TfgColorMLP* h, const TfgDatosMLP* in, const TfgColor* throughput,
@@ -1103,6 +1324,7 @@ extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count
     if (e == cudaSuccess) e = cudaMemset(n->v, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->grad, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->dstate + M::S_ADAM_T, 0, sizeof(uint32_t));
+    if (e == cudaSuccess) e = cudaMemset(n->dstate + M::S_F8_VER, 0, sizeof(uint32_t));
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetParams");
     if (int rc = tfg::repack(n, 0, false, 1)) return rc;
     e = cudaDeviceSynchronize();

@@ -103,6 +103,18 @@ __device__ __forceinline__ void mma_f16_ta(uint32_t d_tmem, uint32_t a_tmem, uin
         "r"(a_tmem), "l"(b), "r"(idesc), "r"((uint32_t)accumulate));
 }
 
+// kind::f8f6f4 (E4M3 / E5M2 operands, K = 32 per instruction, FP32
+// accumulation) with A from TMEM: four 8-bit elements per 32-bit column,
+// element 4j in the lowest byte of column j.  The instruction descriptor has
+// the same fields as kind::f16 (format 0 = E4M3).
+__device__ __forceinline__ void mma_f8_ta(uint32_t d_tmem, uint32_t a_tmem, uint64_t b, uint32_t idesc, bool accumulate) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f8f6f4 [%0], [%1], %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+        "r"(a_tmem), "l"(b), "r"(idesc), "r"((uint32_t)accumulate));
+}
+
 // Arrive on `mbar` once all previously issued MMAs of this thread complete.
 __device__ __forceinline__ void mma_commit(uint64_t* mbar) {
     asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(mbar))

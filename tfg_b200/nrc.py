@@ -14,6 +14,7 @@ N_PARAMS = 23552
 # padded [out][in] shapes of the six weight matrices, in parameter order
 LAYER_SHAPES = [(64, 96), (64, 64), (64, 64), (64, 64), (64, 64), (16, 64)]
 WEIGHTS, EMA, ADAM_M, ADAM_V = 0, 1, 2, 3
+FP16, BF16, FP8 = 0, 1, 2      # inference operand precisions (TFG_MLP_*)
 
 
 def _stream(stream=None) -> int:
@@ -66,6 +67,14 @@ class ColorMLP:
 
     def inference(self, datos: torch.Tensor, out: torch.Tensor, n: int, stream=None) -> None:
         _lib.call("tfgMlpInference", self.h, datos.data_ptr(), out.data_ptr(), int(n), _stream(stream))
+
+    def set_precision(self, precision: int) -> None:
+        """Operand precision of later inference calls: FP16, BF16 or FP8."""
+        _lib.call("tfgMlpSetPrecision", self.h, precision)
+
+    def calibrate(self, datos: torch.Tensor, n: int, stream=None) -> None:
+        """FP8 input scales from the per-layer amax of n samples."""
+        _lib.call("tfgMlpCalibrate", self.h, datos.data_ptr(), n, _stream(stream))
 
     def inference_composite(self, datos: torch.Tensor, thr: torch.Tensor, img: torch.Tensor, n: int,
                             stream=None) -> None:
