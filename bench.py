@@ -252,6 +252,38 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 1024, frames: int = 300) -> dict:
     q1.synchronize()
     t_inf = q0.elapsed_time(q1) / 10
     flops = 2.0 * (96 * 64 + 4 * 64 * 64 + 64 * 16) * n
+
+    # Inference-precision sweep on the trained cache: the same frame (same
+    # paths, no further training) answered in FP16, BF16 and FP8 (E4M3 with
+    # per-layer scales calibrated on the last frame's queries).
+    from tfg_b200.nrc import BF16, FP8, FP16
+    r.cfg.train_steps = 0
+    mlp.calibrate(r.infer, n, stream=r.stream)
+    sweep = {}
+    for name, prec in (("fp16", FP16), ("bf16", BF16), ("fp8", FP8)):
+        mlp.set_precision(prec)
+        r.frame(40_000, accumulate=False)
+        r.stream.synchronize()
+        img_p = r.image().cpu().numpy().astype(np.float64)
+        f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        f0.record(r.stream)
+        for k in range(10):
+            r.frame(40_000, accumulate=False)
+        f1.record(r.stream)
+        f1.synchronize()
+        with torch.cuda.stream(r.stream):
+            for _ in range(3):
+                mlp.inference(r.infer, out, n, stream=r.stream)
+            g0, g1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            g0.record(r.stream)
+            for _ in range(10):
+                mlp.inference(r.infer, out, n, stream=r.stream)
+            g1.record(r.stream)
+        g1.synchronize()
+        ti = g0.elapsed_time(g1) / 10
+        sweep[name] = {"relmse": round(rel(img_p), 5), "ms_per_frame_no_training": round(f0.elapsed_time(f1) / 10, 3),
+                       "inference_ms": round(ti, 4), "inference_tflops_fp16_equiv": round(flops / (ti * 1e-3) / 1e12, 1)}
+    mlp.set_precision(FP16)
     mlp.close()
     return {
         "frames": 48 + frames, "warmup_frames": 48, "camera": "orbit 1 deg/frame", "train_samples_per_frame": 4 * 16384,
@@ -261,6 +293,7 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 1024, frames: int = 300) -> dict:
         "reference_spp": ref_spp, "adam_steps": int(st["adam_t"]), "loss_ema": round(st["loss_ema"], 5),
         "mlp_inference": {"queries": n, "ms": round(t_inf, 4), "tflops": round(flops / (t_inf * 1e-3) / 1e12, 2),
                           "flops_per_query": int(flops / n)},
+        "precision_sweep": sweep,
     }
 
 

@@ -10,7 +10,7 @@ import torch
 from tests.helpers import rel_mse
 from tfg_b200 import pathtracer as pt
 from tfg_b200 import scenes
-from tfg_b200.nrc import ColorMLP, NrcRenderer
+from tfg_b200.nrc import BF16, FP16, ColorMLP, NrcRenderer
 
 pytestmark = pytest.mark.gpu
 
@@ -53,6 +53,29 @@ def test_graph_replay_matches_eager(scene_ds):
         m.close()
     assert np.isfinite(imgs[0]).all()
     np.testing.assert_array_equal(imgs[0], imgs[1])
+
+
+def test_precision_change_recaptures_the_frame_graph(scene_ds):
+    # The inference precision is part of a captured frame's identity: after
+    # switching it, a replayed frame must match the same frame run eagerly.
+    s, ds = scene_ds
+    imgs = {}
+    for graph in (False, True):
+        m = _mlp(s)
+        r = NrcRenderer(ds, m, PARAMS, train_steps=0, use_graph=graph)
+        r.frame(5, accumulate=False)                 # FP16 (captured when graph)
+        m.set_precision(BF16)
+        r.frame(5, accumulate=False)
+        r.stream.synchronize()
+        imgs[graph] = r.image().cpu().numpy().copy()
+        m.set_precision(FP16)
+        r.frame(5, accumulate=False)
+        r.stream.synchronize()
+        imgs[(graph, "fp16")] = r.image().cpu().numpy().copy()
+        m.close()
+    np.testing.assert_array_equal(imgs[True], imgs[False])
+    np.testing.assert_array_equal(imgs[(True, "fp16")], imgs[(False, "fp16")])
+    assert not np.array_equal(imgs[False], imgs[(False, "fp16")])
 
 
 def test_frames_train_the_cache(scene_ds):

@@ -101,7 +101,8 @@ FrameKey key_of(const FrameCall& c) {
     std::memcpy(k.ptrs, p, sizeof(p));
     const int32_t v[] = {c.nprims, c.nlights, c.W, c.H, c.nmesh, (int32_t)c.b.ring_cap, c.cfg.train_steps,
                          (int32_t)c.cfg.max_records, (int32_t)c.cfg.min_records, c.cfg.warmup, c.prm.max_depth,
-                         c.prm.rr_min_depth, c.prm.shadow_mesh, c.prm.tri_format, c.ws_slot};
+                         c.prm.rr_min_depth, c.prm.shadow_mesh, c.prm.tri_format, c.ws_slot,
+                         mlp_precision(c.mlp)};
     std::memcpy(k.ints, v, sizeof(v));
     k.gate = c.cfg.gate_threshold;
     return k;

@@ -1143,6 +1143,7 @@ int mlp_enqueue_train(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, cudaS
     return enqueue_step(n, buf, min_n, true, s);
 }
 void mlp_set_gate_threshold(ColorMlp* n, float g) { n->gate = g; }
+int mlp_precision(const ColorMlp* n) { return n->prec; }
 
 }  // namespace tfg
 

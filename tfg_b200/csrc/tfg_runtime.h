@@ -54,5 +54,6 @@ int mlp_enqueue_infer(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColo
                       uint32_t max_count, const uint32_t* n_dev, cudaStream_t s);
 int mlp_enqueue_train(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, cudaStream_t s);
 void mlp_set_gate_threshold(ColorMlp* n, float g);
+int mlp_precision(const ColorMlp* n);   // inference precision (part of a frame graph's identity)
 
 }  // namespace tfg
