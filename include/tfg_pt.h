@@ -345,6 +345,13 @@ typedef struct TfgColorMLP TfgColorMLP;
  * multiple of 128.  Weights are drawn from `seed`.  Adam lr 1e-2,
  * beta1 0.9, beta2 0.99, eps 1e-15, EMA decay 0.99. */
 int  tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, TfgColorMLP** out);
+/* No reference counterpart (the reference's network has a fixed shape): the
+ * same model with 3, 5 (= tfgMlpCreate) or 7 hidden layers of 64 units. */
+int  tfgMlpCreateEx(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
+                    TfgColorMLP** out);
+/* Length of the model's FP32 parameter arrays: 6144 + 4096 (hidden - 1) +
+ * 1024 (23552 for 5 hidden layers). */
+int32_t tfgMlpParamCount(const TfgColorMLP* mlp);
 void tfgMlpDestroy(TfgColorMLP* mlp);
 /* ColorMLP::setBounds (mlp.cpp:89-93): position normalisation box. */
 int  tfgMlpSetBounds(TfgColorMLP* mlp, const TfgSceneBounds* bounds);
@@ -380,7 +387,7 @@ int  tfgMlpSetPrecision(TfgColorMLP* mlp, int32_t precision);
  * from the amax it sees on the first tile of each slot (delayed scaling), so
  * they follow the model while it trains.  `in` must be 16-byte aligned. */
 int  tfgMlpCalibrate(TfgColorMLP* mlp, const TfgDatosMLP* in, uint32_t count, void* stream);
-/* FP32 parameter arrays (count = 23552, padded [out][in] per layer):
+/* FP32 parameter arrays (count = tfgMlpParamCount, padded [out][in] per layer):
  * which = 0 weights, 1 EMA, 2 Adam m, 3 Adam v. */
 int  tfgMlpGetParams(TfgColorMLP* mlp, int which, float* host, uint32_t count);
 /* Set the weights and restart the optimiser (Adam moments and the weight

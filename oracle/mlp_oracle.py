@@ -11,12 +11,18 @@ from __future__ import annotations
 
 import numpy as np
 
-SHAPES = [(64, 96), (64, 64), (64, 64), (64, 64), (64, 64), (16, 64)]
+def shapes(hidden_layers: int = 5) -> list[tuple[int, int]]:
+    return [(64, 96)] + [(64, 64)] * (hidden_layers - 1) + [(16, 64)]
+
+
+SHAPES = shapes(5)
 
 
 def split(flat):
+    """Layer matrices of a flat parameter array; its length gives the depth."""
+    hidden = (len(flat) - 6144 - 1024) // 4096 + 1
     out, o = [], 0
-    for r, c in SHAPES:
+    for r, c in shapes(hidden):
         out.append(np.asarray(flat[o:o + r * c], np.float64).reshape(r, c))
         o += r * c
     return out

@@ -242,3 +242,52 @@ def test_fp8_inference_matches_quantized_model(built):
     assert (np.abs(got2 - ref) / scale).mean() < 0.15
     m.set_precision(FP16)
     m.close()
+
+
+@pytest.mark.parametrize("hidden", [3, 7])
+def test_other_depths_match_fp64_model(built, hidden):
+    """3 and 7 hidden layers: parameter layout, inference and the loss
+    gradient against the FP64 model of the same depth."""
+    m = ColorMLP(batch=2048, seed=30 + hidden, hidden_layers=hidden)
+    m.set_bounds(LO, HI)
+    assert m.n_params == 6144 + 4096 * (hidden - 1) + 1024
+    w = m.get_params(WEIGHTS)
+    W = split_layers(w)
+    assert len(W) == hidden + 1 and np.count_nonzero(W[-1][3:]) == 0 and np.count_nonzero(W[0][:, 85:]) == 0
+    n = 1500
+    d = _datos(np.random.default_rng(hidden), n)
+    out = torch.zeros(n * 3, device="cuda")
+    m.inference(_dev(d), out, n)
+    torch.cuda.synchronize()
+    x = mo.encode(mo.rows15(d, LO, HI))
+    Wf = [_f16(a) for a in W]
+    want = mo.scrub(mo.forward(Wf, x)[0])
+    scale = np.abs(mo.forward(Wf, x)[0]).mean() + 1e-3
+    err = np.abs(out.view(n, 3).cpu().numpy() - want) / scale
+    assert err.max() < 0.05 and err.mean() < 0.01, (err.max(), err.mean())
+    n_avail = 9000
+    dt = _datos(np.random.default_rng(40 + hidden), n_avail)
+    g, loss = m.compute_gradient(_dev(dt), n_avail, seed=3)
+    idx = np.zeros(m.batch, np.int32)
+    orc.cpu.orc_indices(orc.p(idx), n_avail, m.batch, 3)
+    sel = dt[idx]
+    xs = mo.encode(mo.rows15(sel, LO, HI))
+    y = np.stack([sel["color"][k] for k in "rgb"], 1).astype(np.float64)
+    ref_loss, ref = mo.loss_and_grad(Wf, xs, y)
+    assert abs(loss - ref_loss) / ref_loss < 0.02, (loss, ref_loss)
+    for l, (gg, rr) in enumerate(zip(split_layers(g), ref)):
+        rel = np.linalg.norm(gg - rr) / (np.linalg.norm(rr) + 1e-30)
+        assert rel < 0.05, f"layer {l}: relative gradient error {rel:.3e}"
+    # a few steps on a smooth signal lower the loss
+    def f(pos, kd):
+        return (0.5 + 0.3 * np.sin(0.7 * pos[:, :1])) * (0.2 + kd)
+    ds = _datos(np.random.default_rng(7), 20000, f)
+    dd = _dev(ds)
+    losses = [m.train_step(dd, 20000) for _ in range(60)]
+    assert np.isfinite(losses).all() and np.mean(losses[-5:]) < np.mean(losses[:5]) / 2, losses[::10]
+    m.close()
+
+
+def test_unsupported_depth_is_rejected(built):
+    with pytest.raises(TfgError):
+        ColorMLP(hidden_layers=4)

@@ -68,6 +68,8 @@ _PROTOS = {
     "tfgMlpSetHyperparams": (c_int32, [c_void_p, c_float, c_float, c_float, c_float, c_float]),
     "tfgMlpTrainStep": (c_int32, [c_void_p, c_void_p, c_uint32, POINTER(c_float), c_void_p]),
     "tfgMlpInference": (c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
+    "tfgMlpCreateEx": (c_int32, [c_uint32, c_uint32, c_uint32, c_uint64, c_int32, c_void_p]),
+    "tfgMlpParamCount": (c_int32, [c_void_p]),
     "tfgMlpSetPrecision": (c_int32, [c_void_p, c_int32]),
     "tfgMlpCalibrate": (c_int32, [c_void_p, c_void_p, c_uint32, c_void_p]),
     "tfgMlpInferenceComposite": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),

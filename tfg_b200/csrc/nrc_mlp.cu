@@ -49,30 +49,53 @@ namespace mlp {
 
 constexpr int kTile = 128;
 constexpr int kHid = 64;
-constexpr int kLayers = 6;       // 96->64, 4 x 64->64, 64->16 (3 used)
 constexpr int kOutPad = 16;
 constexpr int kBands = 12;
+constexpr int kMaxLayers = 8;    // up to 7 hidden layers
 
+// A network of `nl` layers: 96 -> 64, (nl - 2) x 64 -> 64, 64 -> 16 (3
+// outputs used); nl = 4, 6 (the default: 5 hidden layers of 64) or 8.  The
+// runtime forms serve the host; kernels use the template forms kRows<NL> etc.
+//
 // FP32 master parameters, row-major [out][in] per layer with padded shapes
-// 64x96, 4 x 64x64, 16x64 (rows 3..15 of the last layer stay zero).
-__host__ __device__ constexpr int kRows(int l) { return l == kLayers - 1 ? 16 : 64; }
-__host__ __device__ constexpr int kCols(int l) { return l == 0 ? 96 : 64; }
-__host__ __device__ constexpr int kPOff(int l) { return l == 0 ? 0 : (l <= 5 ? 6144 + (l - 1) * 4096 : 23552); }
-constexpr int kParams = 23552;
+// 64x96, (nl - 2) x 64x64, 16x64 (rows 3..15 of the last layer stay zero).
+__host__ __device__ constexpr int rows_of(int nl, int l) { return l == nl - 1 ? 16 : 64; }
+__host__ __device__ constexpr int cols_of(int l) { return l == 0 ? 96 : 64; }
+__host__ __device__ constexpr int poff_of(int nl, int l) {
+    return l == 0 ? 0 : (l <= nl - 1 ? 6144 + (l - 1) * 4096 : 6144 + (nl - 2) * 4096 + 1024);
+}
+__host__ __device__ constexpr int params_of(int nl) { return poff_of(nl, nl); }
+// Forward / inference weight image (FP16 or BF16, SW128 K-major): layer 0 uses
+// two K regions (64 rows x 128 B each), hidden layers one region, the last
+// layer 16 rows.
+__host__ __device__ constexpr int foff_of(int nl, int l) {
+    return l == 0 ? 0 : (l <= nl - 1 ? 16384 + (l - 1) * 8192 : 16384 + (nl - 2) * 8192 + 2048);
+}
+__host__ __device__ constexpr int fwd_bytes_of(int nl) { return foff_of(nl, nl); }
+// Backward image (BF16, W^T: [in rows][out K]) for layers 1..nl-1; the last
+// layer's K = 16 occupies the first two chunks of each row.
+__host__ __device__ constexpr int bwd_bytes_of(int nl) { return (nl - 1) * 8192; }
+// FP8 inference image: one SW128 region per layer (K <= 128 bytes per row).
+__host__ __device__ constexpr int f8_bytes_of(int nl) { return (nl - 1) * 8192 + 2048; }
 
-// Forward / inference weight image (FP16, SW128 K-major): layer 0 uses two
-// K regions (64 rows x 128 B each), layers 1-4 one region, layer 5 16 rows.
-__host__ __device__ constexpr int kFOff(int l) { return l == 0 ? 0 : (l <= 5 ? 16384 + (l - 1) * 8192 : 51200); }
-constexpr int kFwdBytes = 51200;
-// Backward image (BF16, W^T: [in rows][out K]) for layers 1..5; layer 5's
-// K = 16 occupies the first two chunks of each row.
-__host__ __device__ constexpr int kBOff(int l) { return l == 0 ? 0 : (l - 1) * 8192; }
-constexpr int kBwdBytes = 40960;
-
+template <int NL> __host__ __device__ constexpr int kRows(int l) { return rows_of(NL, l); }
+template <int NL> __host__ __device__ constexpr int kCols(int l) { return cols_of(l); }
+template <int NL> __host__ __device__ constexpr int kPOff(int l) { return poff_of(NL, l); }
+template <int NL> __host__ __device__ constexpr int kFOff(int l) { return foff_of(NL, l); }
+template <int NL> __host__ __device__ constexpr int kBOff(int l) { return (l - 1) * 8192; }
+template <int NL> __host__ __device__ constexpr int kF8Off(int l) { return l * 8192; }
 // Transposed per-tile layouts written by k_train for k_wgrad: feature rows x
 // 128 samples, two 64-sample K regions of F*128 bytes.
-__host__ __device__ constexpr int kHTFeat(int l) { return l == 0 ? 96 : 64; }   // input of layer l
-__host__ __device__ constexpr int kZTFeat(int l) { return l == kLayers - 1 ? 16 : 64; }   // output gradient of layer l
+template <int NL> __host__ __device__ constexpr int kHTFeat(int l) { return l == 0 ? 96 : 64; }        // input of layer l
+template <int NL> __host__ __device__ constexpr int kZTFeat(int l) { return l == NL - 1 ? 16 : 64; }   // output gradient
+template <int NL> constexpr int kParams = params_of(NL);
+template <int NL> constexpr int kFwdBytes = fwd_bytes_of(NL);
+template <int NL> constexpr int kBwdBytes = bwd_bytes_of(NL);
+template <int NL> constexpr int kF8Bytes = f8_bytes_of(NL);
+// Shared-memory layouts are sized for the deepest network.
+constexpr int kFwdBytesMax = fwd_bytes_of(kMaxLayers);            // 67584
+constexpr int kWeightRegion = (kFwdBytesMax + 1023) / 1024 * 1024;  // 68608
+static_assert(fwd_bytes_of(6) == 51200 && bwd_bytes_of(6) == 40960 && params_of(6) == 23552, "default layout");
 
 constexpr uint32_t kSpinLimit = 1u << 26;
 
@@ -216,13 +239,10 @@ constexpr int kSlots = 4;
 constexpr int kInferThreads = 128 * kSlots;
 constexpr int kRowBytes = (int)sizeof(TfgDatosMLP);              // 112
 constexpr int kStageBytes = kTile * kRowBytes;                   // 14336
-constexpr int kInferSmemStage = 51200 + 1024;
+constexpr int kInferSmemStage = kWeightRegion;
 constexpr int kInferSmem = kInferSmemStage + kSlots * kStageBytes;
 static_assert(kSlots * 128 <= 512, "TMEM: 128 columns per slot");
 static_assert(kInferSmem + 1024 <= 227 * 1024, "inference shared memory");
-// FP8 weight image: one SW128 region per layer (K <= 128 bytes per row).
-__host__ __device__ constexpr int kF8Off(int l) { return l < kLayers - 1 ? l * 8192 : 40960; }
-constexpr int kF8Bytes = 43008;
 // Scale words of the FP8 path (device floats): q[l], wq[l] and the running
 // amax of each layer's input observed by the last inference calls.
 constexpr int kF8Q = 0, kF8WQ = 8, kF8Amax = 16, kF8Words = 24;
@@ -353,7 +373,7 @@ __device__ __forceinline__ void warp_amax(float v, float* dst) {
 // `f8` (FP8 only): scale words.  TRACK: the per-layer input amax is folded
 // into amax[0..5]; with `amax_all` every tile contributes, otherwise only the
 // first tile of each slot (the delayed-scaling estimate).
-template <int PREC, bool TRACK>
+template <int PREC, bool TRACK, int NL>
 __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
                                                             const uint32_t* __restrict__ n_dev, Bounds bounds,
                                                             const uint8_t* __restrict__ wimg,
@@ -361,7 +381,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
                                                             const TfgColor* __restrict__ thr,
                                                             const float* __restrict__ f8, float* amax, int amax_all) {
     constexpr bool kF8 = PREC == kPrecF8;
-    constexpr uint32_t kWBytes = kF8 ? kF8Bytes : kFwdBytes;
+    constexpr uint32_t kWBytes = kF8 ? kF8Bytes<NL> : kFwdBytes<NL>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sw = smem;
@@ -377,9 +397,9 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
     const uint32_t ntiles = (n + kTile - 1) / kTile;
     if (blockIdx.x * kSlots >= ntiles) return;
     // FP8 scales: input quantisation of each layer and the accumulator rescale.
-    float qs[kLayers], deq[kLayers];
+    float qs[NL], deq[NL];
 #pragma unroll
-    for (int l = 0; l < kLayers; ++l) {
+    for (int l = 0; l < NL; ++l) {
         qs[l] = kF8 ? f8[kF8Q + l] : 1.0f;
         deq[l] = kF8 ? 1.0f / (f8[kF8Q + l] * f8[kF8WQ + l]) : 1.0f;
     }
@@ -445,8 +465,8 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
         // an immediate (the start-address field holds address / 16), so the
         // issuing thread runs no descriptor arithmetic between MMAs.
 #pragma unroll
-        for (int l = 0; l < kLayers; ++l) {
-            const bool last = l == kLayers - 1;
+        for (int l = 0; l < NL; ++l) {
+            const bool last = l == NL - 1;
             if (issuer_warp) {
                 umma::fence_after_sync();
                 constexpr uint32_t id_hid = umma::idesc_f16(kTile, kHid, PREC == kPrecBF16);
@@ -454,14 +474,14 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
                 if (umma::elect_one()) {
                     if constexpr (kF8) {
 #pragma unroll
-                        for (int s = 0; s < kCols(l) / 32; ++s)
-                            umma::mma_f8_ta(tmem, tmem_a + 8u * s, wdesc + (uint64_t)((kF8Off(l) + s * 32) >> 4),
+                        for (int s = 0; s < kCols<NL>(l) / 32; ++s)
+                            umma::mma_f8_ta(tmem, tmem_a + 8u * s, wdesc + (uint64_t)((kF8Off<NL>(l) + s * 32) >> 4),
                                             last ? id_out : id_hid, s > 0);
                     } else {
 #pragma unroll
-                        for (int s = 0; s < kCols(l) / 16; ++s) {
+                        for (int s = 0; s < kCols<NL>(l) / 16; ++s) {
                             const uint64_t bd =
-                                wdesc + (uint64_t)((kFOff(l) + (s >> 2) * (kRows(l) * 128) + (s & 3) * 32) >> 4);
+                                wdesc + (uint64_t)((kFOff<NL>(l) + (s >> 2) * (kRows<NL>(l) * 128) + (s & 3) * 32) >> 4);
                             umma::mma_f16_ta(tmem, tmem_a + 8u * s, bd, last ? id_out : id_hid, s > 0);
                         }
                     }
@@ -540,6 +560,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
 // FP8 inference image from the debiased weight average, one block per
 // layer: the layer's weight scale wq = 448 / amax|W| goes to f8[kF8WQ + l].
 // Skipped when the image already holds the weights of this Adam step.
+template <int NL>
 __global__ void __launch_bounds__(1024) k_pack_f8(const float* __restrict__ w, const float* __restrict__ ema,
                                                   const uint32_t* __restrict__ state, float decay,
                                                   uint8_t* __restrict__ img, float* f8) {
@@ -548,10 +569,10 @@ __global__ void __launch_bounds__(1024) k_pack_f8(const float* __restrict__ w, c
     if (state[S_F8_VER] == t_adam + 1u) return;
     const int l = blockIdx.x;
     const float debias = t_adam > 0u ? 1.0f - powf(decay, (float)t_adam) : 0.0f;
-    const int cnt = kRows(l) * kCols(l);
+    const int cnt = kRows<NL>(l) * kCols<NL>(l);
     float m = 0.0f;
     for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-        const int i = kPOff(l) + j;
+        const int i = kPOff<NL>(l) + j;
         m = fmaxf(m, fabsf(debias > 0.0f ? ema[i] / debias : w[i]));
     }
 #pragma unroll
@@ -563,15 +584,15 @@ __global__ void __launch_bounds__(1024) k_pack_f8(const float* __restrict__ w, c
     const float wq = m > 0.0f ? kF8Max / m : 1.0f;
     if (threadIdx.x == 0) f8[kF8WQ + l] = wq;
     // every byte of the layer's 128-byte rows: K index c (zero past kCols)
-    for (int j = threadIdx.x; j < kRows(l) * 128; j += blockDim.x) {
+    for (int j = threadIdx.x; j < kRows<NL>(l) * 128; j += blockDim.x) {
         const int r = j / 128, c = j % 128;
         float x = 0.0f;
-        if (c < kCols(l)) {
-            const int i = kPOff(l) + r * kCols(l) + c;
+        if (c < kCols<NL>(l)) {
+            const int i = kPOff<NL>(l) + r * kCols<NL>(l) + c;
             x = (debias > 0.0f ? ema[i] / debias : w[i]) * wq;
         }
         __nv_fp8_e4m3 e(x);
-        img[kF8Off(l) + umma::sw128_offset(r, c >> 4) + (c & 15)] = *reinterpret_cast<uint8_t*>(&e);
+        img[kF8Off<NL>(l) + umma::sw128_offset(r, c >> 4) + (c & 15)] = *reinterpret_cast<uint8_t*>(&e);
     }
 }
 
@@ -581,7 +602,7 @@ __global__ void __launch_bounds__(1024) k_pack_f8(const float* __restrict__ w, c
 __global__ void k_f8_update(float* f8, uint32_t* state, int mark_packed) {
     const int l = threadIdx.x;
     if (l == 0 && mark_packed) state[S_F8_VER] = state[S_ADAM_T] + 1u;
-    if (l >= kLayers) return;
+    if (l >= kMaxLayers) return;
     const float a = f8[kF8Amax + l];
     if (a > 0.0f) f8[kF8Q + l] = kF8Max / (2.0f * a);
     f8[kF8Amax + l] = 0.0f;
@@ -590,9 +611,9 @@ __global__ void k_f8_update(float* f8, uint32_t* state, int mark_packed) {
 // ------------------------------------------------------------------ training forward + backward
 // Shared memory: fwd weights 51200 | bwd weights 40960 | A 32768.
 constexpr int kTrainSmemF = 0;
-constexpr int kTrainSmemB = 51200 + 1024;            // 52224, 1024-aligned
-constexpr int kTrainSmemA = kTrainSmemB + 40960;      // 93184
-constexpr int kTrainSmem = kTrainSmemA + 2 * kTile * 128;   // 125952
+constexpr int kTrainSmemB = kWeightRegion;                          // 68608, 1024-aligned
+constexpr int kTrainSmemA = kTrainSmemB + bwd_bytes_of(kMaxLayers);   // 125952
+constexpr int kTrainSmem = kTrainSmemA + 2 * kTile * 128;           // 158720
 
 // Device-resident training state (one per model): read by the kernels so a
 // whole frame can be enqueued (and captured in a CUDA graph) without reading
@@ -605,8 +626,8 @@ struct TrainArgs {
     Bounds bounds;
     const uint8_t* fwd;          // FP16 forward image
     const uint8_t* bwd;          // BF16 backward image
-    uint8_t* hT[kLayers];        // transposed inputs of each layer, per tile
-    uint8_t* zT[kLayers];        // transposed output gradients of each layer, per tile
+    uint8_t* hT[kMaxLayers];  // transposed inputs of each layer, per tile
+    uint8_t* zT[kMaxLayers];  // transposed output gradients of each layer, per tile
     float* loss;                 // sum of per-sample losses (unnormalised)
 };
 
@@ -622,6 +643,7 @@ __device__ __forceinline__ void store_T(uint8_t* tile, int s, const float* v) {
     }
 }
 
+template <int NL>
 __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -649,9 +671,9 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     umma::fence_after_sync();
     const uint32_t tmem = tslot;
     if (t == 0) {
-        umma::mbar_expect_tx(&mb_w, kFwdBytes + kBwdBytes);
-        umma::bulk_g2s(sf, a.fwd, kFwdBytes, &mb_w);
-        umma::bulk_g2s(sb, a.bwd, kBwdBytes, &mb_w);
+        umma::mbar_expect_tx(&mb_w, kFwdBytes<NL> + kBwdBytes<NL>);
+        umma::bulk_g2s(sf, a.fwd, kFwdBytes<NL>, &mb_w);
+        umma::bulk_g2s(sb, a.bwd, kBwdBytes<NL>, &mb_w);
     }
     bool ok = umma::mbar_wait(&mb_w, 0, kSpinLimit);
     uint32_t mph = 0;
@@ -681,21 +703,21 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
         }
         umma::fence_smem_to_async();
         __syncthreads();
-        uint32_t mask[kLayers - 1][2];
+        uint32_t mask[NL - 1][2];
         // forward
-        for (int l = 0; l < kLayers && ok; ++l) {
-            const int K = kCols(l), N = (l == kLayers - 1) ? kOutPad : kHid;
-            const uint32_t dcol = (l == kLayers - 1) ? 64u : 0u;
+        for (int l = 0; l < NL && ok; ++l) {
+            const int K = kCols<NL>(l), N = (l == NL - 1) ? kOutPad : kHid;
+            const uint32_t dcol = (l == NL - 1) ? 64u : 0u;
             if (t == 0) {
                 umma::fence_after_sync();
-                issue_layer(tmem + dcol, sa, kTile * 128, sf + kFOff(l), kRows(l) * 128, K, N, false);
+                issue_layer(tmem + dcol, sa, kTile * 128, sf + kFOff<NL>(l), kRows<NL>(l) * 128, K, N, false);
                 umma::mma_commit(&mb_mma);
             }
             ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
             mph ^= 1u;
             if (!ok) break;
             umma::fence_after_sync();
-            if (l < kLayers - 1) {
+            if (l < NL - 1) {
                 float v[64];
                 tmem_row64(tmem, warp, 0, v);
                 uint32_t m0 = 0, m1 = 0;
@@ -725,18 +747,18 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
                     g[k] = 2.0f * diff / den;
                 }
                 store_row64<true>(sa, t, g);
-                store_T<16>(a.zT[kLayers - 1] + (size_t)tile * (2 * 16 * 128), t, g);
+                store_T<16>(a.zT[NL - 1] + (size_t)tile * (2 * 16 * 128), t, g);
             }
             umma::fence_before_sync();
             umma::fence_smem_to_async();
             __syncthreads();
         }
         // backward: dH_{l-1} = dZ_l * W_l, masked by the ReLU of layer l-1
-        for (int l = kLayers - 1; l >= 1 && ok; --l) {
-            const int K = (l == kLayers - 1) ? kOutPad : kHid;
+        for (int l = NL - 1; l >= 1 && ok; --l) {
+            const int K = (l == NL - 1) ? kOutPad : kHid;
             if (t == 0) {
                 umma::fence_after_sync();
-                issue_layer(tmem, sa, kTile * 128, sb + kBOff(l), 64 * 128, K, kHid, true);
+                issue_layer(tmem, sa, kTile * 128, sb + kBOff<NL>(l), 64 * 128, K, kHid, true);
                 umma::mma_commit(&mb_mma);
             }
             ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
@@ -775,8 +797,8 @@ constexpr int kWgSmemB = 65536;                      // 2 stages x 2 x 96 x 128
 constexpr int kWgSmem = kWgSmemB + 2 * 2 * 96 * 128; // 114688
 
 struct WgradArgs {
-    const uint8_t* zT[kLayers];
-    const uint8_t* hT[kLayers];
+    const uint8_t* zT[kMaxLayers];
+    const uint8_t* hT[kMaxLayers];
     float* grad;
     const uint32_t* state;
     uint32_t min_n;
@@ -784,6 +806,7 @@ struct WgradArgs {
     uint32_t tiles_per_cta;
 };
 
+template <int NL>
 __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -791,7 +814,7 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     __shared__ uint32_t tslot;
     const int t = threadIdx.x, warp = t >> 5;
     const int l = blockIdx.y;
-    const int FZ = kZTFeat(l), FH = kHTFeat(l);
+    const int FZ = kZTFeat<NL>(l), FH = kHTFeat<NL>(l);
     const uint32_t t0 = blockIdx.x * a.tiles_per_cta;
     if (t0 >= a.ntiles || a.state[S_NAVAIL] < a.min_n || a.state[S_NAVAIL] == 0) return;
     const uint32_t t1 = min(a.ntiles, t0 + a.tiles_per_cta);
@@ -861,7 +884,7 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
             float v[32];
             umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
             if (row < FZ) {
-                float* g = a.grad + kPOff(l) + row * kCols(l) + c0;
+                float* g = a.grad + kPOff<NL>(l) + row * kCols<NL>(l) + c0;
 #pragma unroll
                 for (int i = 0; i < 32; ++i) atomicAdd(&g[i], v[i]);
             }
@@ -891,21 +914,23 @@ struct AdamArgs {
     int update;                    // 0: only re-pack (after loading parameters)
 };
 
+template <int NL>
 __device__ __forceinline__ void layer_of(int i, int& l, int& r, int& c) {
     l = 0;
-    while (i >= kPOff(l + 1)) ++l;
-    const int j = i - kPOff(l);
-    r = j / kCols(l);
-    c = j % kCols(l);
+    while (i >= kPOff<NL>(l + 1)) ++l;
+    const int j = i - kPOff<NL>(l);
+    r = j / kCols<NL>(l);
+    c = j % kCols<NL>(l);
 }
 
+template <int NL>
 __global__ void k_adam(AdamArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kParams) return;
+    if (i >= kParams<NL>) return;
     int l, r, c;
-    layer_of(i, l, r, c);
+    layer_of<NL>(i, l, r, c);
     // Padded entries (output rows 3..15, input columns 85..95 of layer 0) stay zero.
-    const bool live = !(l == kLayers - 1 && r >= 3) && !(l == 0 && c >= 85);
+    const bool live = !(l == NL - 1 && r >= 3) && !(l == 0 && c >= 85);
     float w = a.w[i];
     float e = a.ema[i];
     const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
@@ -927,15 +952,15 @@ __global__ void k_adam(AdamArgs a) {
     const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
     const float ew = ema_debias > 0.0f ? e / ema_debias : w;
     // forward / inference images: row r, K index c
-    const int rows = kRows(l);
-    const uint32_t off = (uint32_t)kFOff(l) + (uint32_t)(c >> 6) * rows * 128 + umma::sw128_offset(r, (c & 63) >> 3) +
+    const int rows = kRows<NL>(l);
+    const uint32_t off = (uint32_t)kFOff<NL>(l) + (uint32_t)(c >> 6) * rows * 128 + umma::sw128_offset(r, (c & 63) >> 3) +
                          2 * (c & 7);
     *reinterpret_cast<__half*>(a.fwd + off) = __float2half_rn(w);
     *reinterpret_cast<__half*>(a.inf + off) = __float2half_rn(ew);
     *reinterpret_cast<__nv_bfloat16*>(a.inf_bf + off) = __float2bfloat16_rn(ew);
     if (l >= 1) {
         // backward image: W^T, row = c (input unit), K index = r (output unit)
-        const uint32_t boff = (uint32_t)kBOff(l) + umma::sw128_offset(c, r >> 3) + 2 * (r & 7);
+        const uint32_t boff = (uint32_t)kBOff<NL>(l) + umma::sw128_offset(c, r >> 3) + 2 * (r & 7);
         *reinterpret_cast<__nv_bfloat16*>(a.bwd + boff) = __float2bfloat16_rn(w);
     }
 }
@@ -969,8 +994,9 @@ struct ColorMlp {
     mlp::Bounds bounds{{-1, -1, -1}, {1, 1, 1}};
     float* w = nullptr; float* m = nullptr; float* v = nullptr; float* ema = nullptr; float* grad = nullptr;
     uint8_t* fwd = nullptr; uint8_t* bwd = nullptr; uint8_t* inf = nullptr;
-    uint8_t* hT[mlp::kLayers] = {nullptr};
-    uint8_t* zT[mlp::kLayers] = {nullptr};
+    int nl = 6;                  // layers (hidden layers + 1)
+    uint8_t* hT[mlp::kMaxLayers] = {nullptr};
+    uint8_t* zT[mlp::kMaxLayers] = {nullptr};
     float* loss = nullptr;
     uint32_t* dstate = nullptr;  // mlp::S_* words
     float gate = 0.0f;           // cache-query gate threshold on the running loss (<= 0: always open)
@@ -989,6 +1015,17 @@ int cuda_fail(cudaError_t e, const char* what) {
     return fail((int)e, std::string(what) + ": " + cudaGetErrorString(e));
 }
 
+// Calls f(std::integral_constant<int, NL>) for the model's layer count.
+template <typename F>
+int with_layers(int nl, F&& f) {
+    switch (nl) {
+        case 4: return f(std::integral_constant<int, 4>{});
+        case 6: return f(std::integral_constant<int, 6>{});
+        case 8: return f(std::integral_constant<int, 8>{});
+        default: return fail(TFG_E_INVALID, "mlp: unsupported number of layers");
+    }
+}
+
 uint64_t splitmix(uint64_t& s) {
     uint64_t z = (s += 0x9E3779B97F4A7C15ull);
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -1005,7 +1042,11 @@ int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
     a.state = n->dstate;
     a.min_n = min_n;
     a.update = update ? 1 : 0;
-    mlp::k_adam<<<(mlp::kParams + 255) / 256, 256, 0, s>>>(a);
+    with_layers(n->nl, [&](auto c) {
+        constexpr int NL = decltype(c)::value;
+        mlp::k_adam<NL><<<(mlp::kParams<NL> + 255) / 256, 256, 0, s>>>(a);
+        return 0;
+    });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp adam");
     return ok();
@@ -1013,14 +1054,15 @@ int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
 
 int ensure_acts(ColorMlp* n, uint32_t tiles) {
     if (n->act_tiles >= tiles) return ok();
-    for (int l = 0; l < mlp::kLayers; ++l) {
+    for (int l = 0; l < mlp::kMaxLayers; ++l) {
         if (n->hT[l]) cudaFree(n->hT[l]);
         if (n->zT[l]) cudaFree(n->zT[l]);
         n->hT[l] = n->zT[l] = nullptr;
     }
-    for (int l = 0; l < mlp::kLayers; ++l) {
-        cudaError_t e = cudaMalloc((void**)&n->hT[l], (size_t)tiles * 2 * mlp::kHTFeat(l) * 128);
-        if (e == cudaSuccess) e = cudaMalloc((void**)&n->zT[l], (size_t)tiles * 2 * mlp::kZTFeat(l) * 128);
+    for (int l = 0; l < n->nl; ++l) {
+        const int fh = l == 0 ? 96 : 64, fz = l == n->nl - 1 ? 16 : 64;   // kHTFeat / kZTFeat
+        cudaError_t e = cudaMalloc((void**)&n->hT[l], (size_t)tiles * 2 * fh * 128);
+        if (e == cudaSuccess) e = cudaMalloc((void**)&n->zT[l], (size_t)tiles * 2 * fz * 128);
         if (e != cudaSuccess) { n->act_tiles = 0; return cuda_fail(e, "mlp activations"); }
     }
     n->act_tiles = tiles;
@@ -1048,17 +1090,25 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     mlp::TrainArgs ta;
     ta.buf = buf; ta.state = n->dstate; ta.min_n = min_n; ta.batch = n->batch;
     ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
-    for (int l = 0; l < mlp::kLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
-    mlp::k_train<<<std::min<uint32_t>(tiles, (uint32_t)n->sms), 128, mlp::kTrainSmem + 1024, s>>>(ta);
+    for (int l = 0; l < mlp::kMaxLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
+    with_layers(n->nl, [&](auto c) {
+        constexpr int NL = decltype(c)::value;
+        mlp::k_train<NL><<<std::min<uint32_t>(tiles, (uint32_t)n->sms), 128, mlp::kTrainSmem + 1024, s>>>(ta);
+        return 0;
+    });
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp step: forward/backward");
     mlp::WgradArgs wa;
-    for (int l = 0; l < mlp::kLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
+    for (int l = 0; l < mlp::kMaxLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
     wa.grad = n->grad; wa.state = n->dstate; wa.min_n = min_n;
     wa.ntiles = tiles;
     wa.tiles_per_cta = std::max<uint32_t>(2u, (tiles + 15u) / 16u);
-    mlp::k_wgrad<<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, mlp::kLayers), 128, mlp::kWgSmem + 1024,
-                   s>>>(wa);
+    with_layers(n->nl, [&](auto c) {
+        constexpr int NL = decltype(c)::value;
+        mlp::k_wgrad<NL><<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, NL), 128, mlp::kWgSmem + 1024, s>>>(
+            wa);
+        return 0;
+    });
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp step: weight gradients");
     if (!update) return ok();
@@ -1087,23 +1137,27 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
     const uint32_t grid = std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, (uint32_t)n->sms);
     const size_t smem = mlp::kInferSmem + 1024;
     cudaError_t e = cudaSuccess;
-    if (n->prec == mlp::kPrecF16) {
-        mlp::k_infer<mlp::kPrecF16, false><<<grid, mlp::kInferThreads, smem, s>>>(in, count, n_dev, n->bounds, n->inf,
-                                                                                out, img, thr, nullptr, nullptr, 0);
-    } else if (n->prec == mlp::kPrecBF16) {
-        mlp::k_infer<mlp::kPrecBF16, false><<<grid, mlp::kInferThreads, smem, s>>>(in, count, n_dev, n->bounds,
-                                                                                 n->inf_bf, out, img, thr, nullptr,
-                                                                                 nullptr, 0);
-    } else {
-        mlp::k_pack_f8<<<mlp::kLayers, 1024, 0, s>>>(n->w, n->ema, n->dstate, n->decay, n->inf_f8, n->f8);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(e, "mlp inference: FP8 weight image");
-        mlp::k_infer<mlp::kPrecF8, true><<<grid, mlp::kInferThreads, smem, s>>>(
-            in, count, n_dev, n->bounds, n->inf_f8, out, img, thr, n->f8, n->f8 + mlp::kF8Amax, 0);
-        e = cudaGetLastError();
-        if (e != cudaSuccess) return cuda_fail(e, "mlp inference");
-        mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 1);
-    }
+    const int rc = with_layers(n->nl, [&](auto c) {
+        constexpr int NL = decltype(c)::value;
+        if (n->prec == mlp::kPrecF16) {
+            mlp::k_infer<mlp::kPrecF16, false, NL><<<grid, mlp::kInferThreads, smem, s>>>(
+                in, count, n_dev, n->bounds, n->inf, out, img, thr, nullptr, nullptr, 0);
+        } else if (n->prec == mlp::kPrecBF16) {
+            mlp::k_infer<mlp::kPrecBF16, false, NL><<<grid, mlp::kInferThreads, smem, s>>>(
+                in, count, n_dev, n->bounds, n->inf_bf, out, img, thr, nullptr, nullptr, 0);
+        } else {
+            mlp::k_pack_f8<NL><<<NL, 1024, 0, s>>>(n->w, n->ema, n->dstate, n->decay, n->inf_f8, n->f8);
+            cudaError_t e2 = cudaGetLastError();
+            if (e2 != cudaSuccess) return cuda_fail(e2, "mlp inference: FP8 weight image");
+            mlp::k_infer<mlp::kPrecF8, true, NL><<<grid, mlp::kInferThreads, smem, s>>>(
+                in, count, n_dev, n->bounds, n->inf_f8, out, img, thr, n->f8, n->f8 + mlp::kF8Amax, 0);
+            e2 = cudaGetLastError();
+            if (e2 != cudaSuccess) return cuda_fail(e2, "mlp inference");
+            mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 1);
+        }
+        return 0;
+    });
+    if (rc) return rc;
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp inference");
     return ok();
@@ -1117,10 +1171,14 @@ int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStrea
         return fail(TFG_E_INVALID, "tfgMlpCalibrate: input buffer must be 16-byte aligned");
     const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
     const uint32_t grid = std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, (uint32_t)n->sms);
-    cudaError_t e = cudaMemsetAsync(n->f8 + mlp::kF8Amax, 0, mlp::kLayers * sizeof(float), s);
+    cudaError_t e = cudaMemsetAsync(n->f8 + mlp::kF8Amax, 0, mlp::kMaxLayers * sizeof(float), s);
     if (e != cudaSuccess) return cuda_fail(e, "tfgMlpCalibrate");
-    mlp::k_infer<mlp::kPrecF16, true><<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(
-        in, count, nullptr, n->bounds, n->inf, nullptr, nullptr, nullptr, nullptr, n->f8 + mlp::kF8Amax, 1);
+    with_layers(n->nl, [&](auto c) {
+        constexpr int NL = decltype(c)::value;
+        mlp::k_infer<mlp::kPrecF16, true, NL><<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(
+            in, count, nullptr, n->bounds, n->inf, nullptr, nullptr, nullptr, nullptr, n->f8 + mlp::kF8Amax, 1);
+        return 0;
+    });
     e = cudaGetLastError();
     if (e == cudaSuccess) { mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 0); e = cudaGetLastError(); }
     if (e != cudaSuccess) return cuda_fail(e, "tfgMlpCalibrate");
@@ -1150,9 +1208,30 @@ int mlp_precision(const ColorMlp* n) { return n->prec; }
 using tfg::ColorMlp;
 namespace M = tfg::mlp;
 
+namespace {
+template <int NL>
+void set_kernel_attrs() {
+    const int ism = M::kInferSmem + 1024;
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF16, false, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF16, true, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecBF16, false, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF8, true, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_train<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kTrainSmem + 1024);
+    cudaFuncSetAttribute(M::k_wgrad<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
+}
+}  // namespace
+
 extern "C" int tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, TfgColorMLP** out) {
+    return tfgMlpCreateEx(n_in, n_out, batch, seed, 5, out);
+}
+
+extern "C" int tfgMlpCreateEx(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
+                              TfgColorMLP** out) {
     if (!out) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: out is null");
     *out = nullptr;
+    if (hidden_layers != 3 && hidden_layers != 5 && hidden_layers != 7)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: hidden_layers must be 3, 5 or 7");
+    const int nl = hidden_layers + 1;
     if (n_in != 15 || n_out != 3) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: the cache takes 15 inputs and 3 outputs");
     if (batch == 0 || batch % M::kTile != 0 || batch > (1u << 24))
         return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: batch must be a positive multiple of 128");
@@ -1163,41 +1242,43 @@ extern "C" int tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint6
     ColorMlp* n = new ColorMlp();
     n->dev = dev;
     n->batch = batch;
+    n->nl = nl;
     cudaDeviceGetAttribute(&n->sms, cudaDevAttrMultiProcessorCount, dev);
-    const size_t pb = M::kParams * sizeof(float);
+    const int nparams = M::params_of(nl);
+    const size_t pb = nparams * sizeof(float);
+    const size_t fwd_bytes = M::fwd_bytes_of(nl), bwd_bytes = M::bwd_bytes_of(nl), f8_bytes = M::f8_bytes_of(nl);
     e = cudaMalloc((void**)&n->w, pb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->m, pb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->v, pb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->ema, pb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->grad, pb);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&n->fwd, M::kFwdBytes);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&n->bwd, M::kBwdBytes);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf, M::kFwdBytes);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf_bf, M::kFwdBytes);
-    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf_f8, M::kF8Bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->fwd, fwd_bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->bwd, bwd_bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf, fwd_bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf_bf, fwd_bytes);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->inf_f8, f8_bytes);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->f8, M::kF8Words * sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->loss, sizeof(float));
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->dstate, M::S_WORDS * sizeof(uint32_t));
     if (e != cudaSuccess) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return tfg::cuda_fail(e, "tfgMlpCreate"); }
-    cudaMemset(n->fwd, 0, M::kFwdBytes);
-    cudaMemset(n->bwd, 0, M::kBwdBytes);
-    cudaMemset(n->inf, 0, M::kFwdBytes);
-    cudaMemset(n->inf_bf, 0, M::kFwdBytes);
-    cudaMemset(n->inf_f8, 0, M::kF8Bytes);
+    cudaMemset(n->fwd, 0, fwd_bytes);
+    cudaMemset(n->bwd, 0, bwd_bytes);
+    cudaMemset(n->inf, 0, fwd_bytes);
+    cudaMemset(n->inf_bf, 0, fwd_bytes);
+    cudaMemset(n->inf_f8, 0, f8_bytes);
     cudaMemset(n->f8, 0, M::kF8Words * sizeof(float));
     cudaMemset(n->dstate, 0, M::S_WORDS * sizeof(uint32_t));
     // Uniform (-s, s) initialisation with s = sqrt(6 / (fan_in + fan_out)) per layer.
-    std::vector<float> h(M::kParams, 0.0f);
+    std::vector<float> h(nparams, 0.0f);
     uint64_t st = seed ? seed : 0x5EEDull;
-    const int fan_in[M::kLayers] = {85, 64, 64, 64, 64, 64};
-    const int fan_out[M::kLayers] = {64, 64, 64, 64, 64, 3};
-    for (int l = 0; l < M::kLayers; ++l) {
-        const float sc = std::sqrt(6.0f / (float)(fan_in[l] + fan_out[l]));
-        for (int r = 0; r < M::kRows(l); ++r)
-            for (int c = 0; c < M::kCols(l); ++c) {
-                const bool live = !(l == M::kLayers - 1 && r >= 3) && !(l == 0 && c >= 85);
+    for (int l = 0; l < nl; ++l) {
+        const int fan_in = l == 0 ? 85 : 64, fan_out = l == nl - 1 ? 3 : 64;
+        const float sc = std::sqrt(6.0f / (float)(fan_in + fan_out));
+        for (int r = 0; r < M::rows_of(nl, l); ++r)
+            for (int c = 0; c < M::cols_of(l); ++c) {
+                const bool live = !(l == nl - 1 && r >= 3) && !(l == 0 && c >= 85);
                 const double u = (double)(tfg::splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
-                h[M::kPOff(l) + r * M::kCols(l) + c] = live ? (float)((2.0 * u - 1.0) * sc) : 0.0f;
+                h[M::poff_of(nl, l) + r * M::cols_of(l) + c] = live ? (float)((2.0 * u - 1.0) * sc) : 0.0f;
             }
     }
     // The weight average starts at zero and is debiased by 1 - decay^t for
@@ -1211,13 +1292,9 @@ extern "C" int tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint6
     if (int rc = tfg::repack(n, 0, false, 1)) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return rc; }
     static bool attrs = false;
     if (!attrs) {
-        const int ism = M::kInferSmem + 1024;
-        cudaFuncSetAttribute(M::k_infer<M::kPrecF16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
-        cudaFuncSetAttribute(M::k_infer<M::kPrecF16, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
-        cudaFuncSetAttribute(M::k_infer<M::kPrecBF16, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
-        cudaFuncSetAttribute(M::k_infer<M::kPrecF8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
-        cudaFuncSetAttribute(M::k_train, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kTrainSmem + 1024);
-        cudaFuncSetAttribute(M::k_wgrad, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
+        set_kernel_attrs<4>();
+        set_kernel_attrs<6>();
+        set_kernel_attrs<8>();
         attrs = true;
     }
     e = cudaDeviceSynchronize();
@@ -1232,7 +1309,7 @@ extern "C" void tfgMlpDestroy(TfgColorMLP* h) {
     for (void* p : {(void*)n->w, (void*)n->m, (void*)n->v, (void*)n->ema, (void*)n->grad, (void*)n->fwd, (void*)n->bwd,
                     (void*)n->inf, (void*)n->inf_bf, (void*)n->inf_f8, (void*)n->f8, (void*)n->loss, (void*)n->dstate})
         if (p) cudaFree(p);
-    for (int l = 0; l < M::kLayers; ++l) {
+    for (int l = 0; l < M::kMaxLayers; ++l) {
         if (n->hT[l]) cudaFree(n->hT[l]);
         if (n->zT[l]) cudaFree(n->zT[l]);
     }
@@ -1307,7 +1384,8 @@ extern "C" int tfgMlpTrainStep(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32
 
 extern "C" int tfgMlpGetParams(TfgColorMLP* h, int which, float* host, uint32_t count) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
-    if (!n || !host || count != (uint32_t)M::kParams) return tfg::fail(TFG_E_INVALID, "tfgMlpGetParams: bad argument");
+    if (!n || !host || count != (uint32_t)M::params_of(n->nl))
+        return tfg::fail(TFG_E_INVALID, "tfgMlpGetParams: bad argument");
     const float* src = which == 0 ? n->w : which == 1 ? n->ema : which == 2 ? n->m : which == 3 ? n->v : nullptr;
     if (!src) return tfg::fail(TFG_E_INVALID, "tfgMlpGetParams: unknown array");
     cudaError_t e = cudaMemcpy(host, src, count * sizeof(float), cudaMemcpyDeviceToHost);
@@ -1317,7 +1395,8 @@ extern "C" int tfgMlpGetParams(TfgColorMLP* h, int which, float* host, uint32_t 
 
 extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
-    if (!n || !host || count != (uint32_t)M::kParams) return tfg::fail(TFG_E_INVALID, "tfgMlpSetParams: bad argument");
+    if (!n || !host || count != (uint32_t)M::params_of(n->nl))
+        return tfg::fail(TFG_E_INVALID, "tfgMlpSetParams: bad argument");
     const size_t pb = count * sizeof(float);
     cudaError_t e = cudaMemcpy(n->w, host, pb, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(n->ema, 0, pb);
@@ -1336,12 +1415,12 @@ extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count
 extern "C" int tfgMlpComputeGradient(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
                                      float* host_grad, uint32_t count, float* loss_out) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
-    if (!n || !buffer || !host_grad || count != (uint32_t)M::kParams || n_available == 0)
+    if (!n || !buffer || !host_grad || count != (uint32_t)M::params_of(n->nl) || n_available == 0)
         return tfg::fail(TFG_E_INVALID, "tfgMlpComputeGradient: bad argument");
     if (int rc = tfg::mlp_prepare(n)) return rc;
     uint32_t saved[M::S_WORDS];
     cudaError_t e = cudaMemcpy(saved, n->dstate, sizeof(saved), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, M::kParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, count * sizeof(float));
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
     if (int rc = tfg::set_word(n, M::S_NAVAIL, n_available, 0)) return rc;
     if (int rc = tfg::set_word(n, M::S_STEP, seed, 0)) return rc;
@@ -1349,17 +1428,22 @@ extern "C" int tfgMlpComputeGradient(TfgColorMLP* h, const TfgDatosMLP* buffer, 
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
     if (int rc = tfg::check_error_flag()) return rc;
-    std::vector<float> g(M::kParams);
+    std::vector<float> g(count);
     float l = 0.0f;
-    e = cudaMemcpy(g.data(), n->grad, M::kParams * sizeof(float), cudaMemcpyDeviceToHost);
+    e = cudaMemcpy(g.data(), n->grad, count * sizeof(float), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemcpy(&l, n->loss, sizeof(float), cudaMemcpyDeviceToHost);
-    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, M::kParams * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, count * sizeof(float));
     if (e == cudaSuccess) e = cudaMemcpy(n->dstate, saved, sizeof(saved), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
     const float sc = 1.0f / (3.0f * (float)n->batch);
-    for (int i = 0; i < M::kParams; ++i) host_grad[i] = g[i] * sc;
+    for (uint32_t i = 0; i < count; ++i) host_grad[i] = g[i] * sc;
     if (loss_out) *loss_out = l * sc;
     return tfg::ok();
+}
+
+extern "C" int32_t tfgMlpParamCount(const TfgColorMLP* h) {
+    const ColorMlp* n = reinterpret_cast<const ColorMlp*>(h);
+    return n ? M::params_of(n->nl) : 0;
 }
 
 extern "C" int tfgMlpStatus(void) {

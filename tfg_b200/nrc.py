@@ -10,9 +10,18 @@ import torch
 from . import _lib
 from .structs import BOUNDS, DATOS_MLP, REGISTRO, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame
 
-N_PARAMS = 23552
-# padded [out][in] shapes of the six weight matrices, in parameter order
-LAYER_SHAPES = [(64, 96), (64, 64), (64, 64), (64, 64), (64, 64), (16, 64)]
+def layer_shapes(hidden_layers: int = 5) -> list[tuple[int, int]]:
+    """Padded [out][in] shapes of the weight matrices, in parameter order."""
+    return [(64, 96)] + [(64, 64)] * (hidden_layers - 1) + [(16, 64)]
+
+
+def param_count(hidden_layers: int = 5) -> int:
+    return sum(r * c for r, c in layer_shapes(hidden_layers))
+
+
+# the default network: 5 hidden layers of 64
+LAYER_SHAPES = layer_shapes(5)
+N_PARAMS = param_count(5)
 WEIGHTS, EMA, ADAM_M, ADAM_V = 0, 1, 2, 3
 FP16, BF16, FP8 = 0, 1, 2      # inference operand precisions (TFG_MLP_*)
 
@@ -23,21 +32,27 @@ def _stream(stream=None) -> int:
 
 
 def split_layers(flat: np.ndarray) -> list[np.ndarray]:
+    """Weight matrices of a flat parameter array (its length gives the depth)."""
+    hidden = (len(flat) - 6144 - 1024) // 4096 + 1
+    assert param_count(hidden) == len(flat), "not a parameter array of this network"
     out, o = [], 0
-    for r, c in LAYER_SHAPES:
+    for r, c in layer_shapes(hidden):
         out.append(flat[o:o + r * c].reshape(r, c))
         o += r * c
     return out
 
 
 class ColorMLP:
-    """ColorMLP(n_in=15, n_out=3, batch): train_step / inference / setBounds."""
+    """ColorMLP(n_in=15, n_out=3, batch): train_step / inference / setBounds.
+    `hidden_layers` (3, 5 or 7; the reference's network has 5) sets the depth."""
 
-    def __init__(self, n_in: int = 15, n_out: int = 3, batch: int = 16384, seed: int = 1337):
+    def __init__(self, n_in: int = 15, n_out: int = 3, batch: int = 16384, seed: int = 1337, hidden_layers: int = 5):
         self.batch = batch
+        self.hidden_layers = hidden_layers
         h = ctypes.c_void_p()
-        _lib.call("tfgMlpCreate", n_in, n_out, batch, seed, ctypes.byref(h))
+        _lib.call("tfgMlpCreateEx", n_in, n_out, batch, seed, hidden_layers, ctypes.byref(h))
         self.h = h
+        self.n_params = int(_lib.lib.tfgMlpParamCount(self.h))
 
     def close(self) -> None:
         if self.h:
@@ -82,20 +97,20 @@ class ColorMLP:
                   _stream(stream))
 
     def get_params(self, which: int = WEIGHTS) -> np.ndarray:
-        out = np.zeros(N_PARAMS, np.float32)
-        _lib.call("tfgMlpGetParams", self.h, which, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), N_PARAMS)
+        out = np.zeros(self.n_params, np.float32)
+        _lib.call("tfgMlpGetParams", self.h, which, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), self.n_params)
         return out
 
     def set_params(self, w: np.ndarray) -> None:
         w = np.ascontiguousarray(w, np.float32)
-        assert w.size == N_PARAMS
-        _lib.call("tfgMlpSetParams", self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), N_PARAMS)
+        assert w.size == self.n_params
+        _lib.call("tfgMlpSetParams", self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), self.n_params)
 
     def compute_gradient(self, buffer: torch.Tensor, n_available: int, seed: int) -> tuple[np.ndarray, float]:
-        g = np.zeros(N_PARAMS, np.float32)
+        g = np.zeros(self.n_params, np.float32)
         loss = ctypes.c_float(0.0)
         _lib.call("tfgMlpComputeGradient", self.h, buffer.data_ptr(), int(n_available), seed,
-                  g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), N_PARAMS, ctypes.byref(loss))
+                  g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), self.n_params, ctypes.byref(loss))
         return g, float(loss.value)
 
     def save_model(self, path: str) -> None:
