@@ -285,6 +285,43 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 1024, frames: int = 300) -> dict:
                        "inference_ms": round(ti, 4), "inference_tflops_fp16_equiv": round(flops / (ti * 1e-3) / 1e12, 1)}
     mlp.set_precision(FP16)
     mlp.close()
+
+    # Depth sweep: the same protocol (warm-up, orbit, final pose) with 3 and 7
+    # hidden layers of 64; 5 is the run above.
+    depth = {5: {"relmse": round(e_nrc, 5), "ms_per_frame": round(t_nrc, 3), "inference_ms": round(t_inf, 4),
+                 "adam_steps": int(st["adam_t"])}}
+    for hidden in (3, 7):
+        m2 = ColorMLP(batch=16384, seed=2024, hidden_layers=hidden)
+        m2.set_bounds(*scene.bounds)
+        r2 = NrcRenderer(ds, m2, params, train_steps=4, use_graph=True)
+        for f in range(48):
+            with torch.cuda.stream(r2.stream):
+                set_pose(0)
+            r2.frame(f, warmup=True, accumulate=False)
+        for k in range(frames):
+            with torch.cuda.stream(r2.stream):
+                set_pose(k)
+            r2.frame(48 + k, accumulate=False)
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        d0.record(r2.stream)
+        for k in range(10):
+            r2.frame(10_000 + k, accumulate=False)
+        d1.record(r2.stream)
+        d1.synchronize()
+        img2 = r2.image().cpu().numpy().astype(np.float64)
+        with torch.cuda.stream(r2.stream):
+            for _ in range(3):
+                m2.inference(r2.infer, out, n, stream=r2.stream)
+            h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            h0.record(r2.stream)
+            for _ in range(10):
+                m2.inference(r2.infer, out, n, stream=r2.stream)
+            h1.record(r2.stream)
+        h1.synchronize()
+        depth[hidden] = {"relmse": round(rel(img2), 5), "ms_per_frame": round(d0.elapsed_time(d1) / 10, 3),
+                         "inference_ms": round(h0.elapsed_time(h1) / 10, 4), "adam_steps": int(m2.state()["adam_t"])}
+        m2.close()
+        del r2
     return {
         "frames": 48 + frames, "warmup_frames": 48, "camera": "orbit 1 deg/frame", "train_samples_per_frame": 4 * 16384,
         "ms_per_frame_nrc": round(t_nrc, 3), "ms_per_pass_plain_1spp": round(t_pt, 3),
@@ -294,6 +331,7 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 1024, frames: int = 300) -> dict:
         "mlp_inference": {"queries": n, "ms": round(t_inf, 4), "tflops": round(flops / (t_inf * 1e-3) / 1e12, 2),
                           "flops_per_query": int(flops / n)},
         "precision_sweep": sweep,
+        "depth_sweep": {f"{k}x64": v for k, v in sorted(depth.items())},
     }
 
 
@@ -626,14 +664,15 @@ def main():
         from tfg_b200 import bvh as hbvh
         hb = hbvh.build_host(hbvh.triangle_vertices(scene.mesh))
         nthreads = os.cpu_count() or 1
-        frames = 8
-        dt, n = 0.0, 0
-        for f in range(frames):
-            d, k = cpu_oracle_sample(scene, hb, H_PX, nthreads, frame=1 + f)
+        # full frames at 1 spp until at least 12 s of CPU work (at most 64)
+        frames, dt, n = 0, 0.0, 0
+        while dt < 12.0 and frames < 64:
+            d, k = cpu_oracle_sample(scene, hb, H_PX, nthreads, frame=1 + frames)
             dt += d
             n += k
+            frames += 1
         cpu = {"value": round(n / dt / 1e6, 4), "unit": "Mpaths/s", "cores": nthreads, "kind": "port",
-               "sample": f"{frames} full 1920x1080 frames at 1 spp (8 of the 64 samples of the timed frame; "
+               "sample": f"{frames} full 1920x1080 frames at 1 spp ({frames} of the 64 samples of the timed frame; "
                          f"depth {DEPTH}, RR from {RR}), {dt:.1f} s"}
 
     out = {
