@@ -381,6 +381,13 @@ int  tfgMlpInferenceComposite(TfgColorMLP* mlp, const TfgDatosMLP* in, const Tfg
 #define TFG_MLP_BF16 1
 #define TFG_MLP_FP8  2
 int  tfgMlpSetPrecision(TfgColorMLP* mlp, int32_t precision);
+/* ColorMLP::save_model / load_model (mlp.cpp:173-276): a binary checkpoint of
+ * the weights, weight average, Adam moments, step counters, bounds and
+ * hyper-parameters (tiny-cuda-nn's JSON format is not reproduced).  Loading
+ * needs a model of the same depth and restores training exactly where it
+ * stopped. */
+int  tfgMlpSave(TfgColorMLP* mlp, const char* path);
+int  tfgMlpLoad(TfgColorMLP* mlp, const char* path);
 /* No reference counterpart: FP8 input scales from the per-layer input amax of
  * `count` samples run through the FP16 path (scale = 448 / (2 amax)).  Needed
  * once before FP8 inference; afterwards every FP8 call re-derives the scales
@@ -451,6 +458,31 @@ int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const TfgRenderP
                 const TfgLuzPuntual* luces, int32_t num_luces, int32_t ancho_img, int32_t alto_img,
                 const TfgTinyBVHD_GPU* bvh, const float* tris_wt, const TfgPrimitiva* primitivas_bvh,
                 int32_t num_prims_bvh, const TfgNrcBuffers* buffers, int32_t frame, void* stream);
+
+/* The reference's reconstruction mode (main.cpp:454-668): `spp` samples
+ * (frames first_frame ..) rendered with cache queries and no training, each
+ * answered by the cache, composited into `img` and summed into `accum`
+ * (W*H*3 floats, cleared first) -- all enqueued on `stream`, no host
+ * synchronisation.  `img`, `infer`, `thr`: W*H scratch buffers.  Finish with
+ * tfgToneMapFilmic(accum, spp, ...). */
+int tfgNrcReconstruct(TfgColorMLP* mlp, const TfgRenderParams* params, const TfgCamara* camara,
+                      const TfgPrimitiva* primitivas, int32_t num_primitivas, const TfgLuzPuntual* luces,
+                      int32_t num_luces, int32_t ancho_img, int32_t alto_img, const TfgTinyBVHD_GPU* bvh,
+                      const float* tris_wt, const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh, int32_t spp,
+                      int32_t first_frame, TfgColor* img, TfgDatosMLP* infer, TfgColor* thr, float* accum,
+                      void* stream);
+
+/* Final image (main.cpp:1108-1115): accum / frames into `hdr_out` (W*H*3
+ * floats, optional) and the reference's filmic curve (imagen.h:193-214) as
+ * 8-bit RGB, round(clamp(v, 0, 1) * 255) (imagen_utils.h:59-62), into
+ * `rgb8_out` (W*H*3 bytes, optional).  Device buffers. */
+int tfgToneMapFilmic(const float* accum, int32_t frames, int32_t ancho_img, int32_t alto_img, float* hdr_out,
+                     uint8_t* rgb8_out, void* stream);
+/* Headless image files from host buffers (the reference writes PNG through
+ * libpng, absent here): binary PPM (8-bit RGB, top row first) and PFM (float
+ * RGB, little-endian, bottom row first as the format requires). */
+int tfgWritePPM(const char* path, const uint8_t* rgb8, int32_t ancho_img, int32_t alto_img);
+int tfgWritePFM(const char* path, const float* rgb, int32_t ancho_img, int32_t alto_img);
 
 /* One scene of a batched cache frame: the arguments of tfgNrcFrame (104 B). */
 typedef struct TfgNrcSceneFrame {

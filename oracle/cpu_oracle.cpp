@@ -756,6 +756,25 @@ void orc_composite(TfgColor* img, const TfgColor* pred, const TfgColor* thr, int
     }
 }
 
+// Final image: sum * (1 / frames) (main.cpp:1106-1110), the filmic curve
+// (imagen.h:193-204) and the 8-bit conversion of guardarPNG
+// (imagen_utils.h:59-62); float arithmetic in the written order.
+static float orc_filmic(float x) {
+    const float a = 2.51f, b = 0.03f, c = 2.43f, d = 0.59f, e = 0.14f;
+    x = x * 0.6f;
+    const float v = (x * (a * x + b)) / (x * (c * x + d) + e);
+    return std::min(std::max(v, 0.0f), 1.0f);
+}
+
+void orc_tonemap_filmic(const float* sum, int frames, int n, float* hdr, uint8_t* rgb8) {
+    const float inv = 1.0f / (float)frames;
+    for (int i = 0; i < 3 * n; ++i) {
+        const float v = sum[i] * inv;
+        hdr[i] = v;
+        rgb8[i] = (uint8_t)std::round(std::min(std::max(orc_filmic(v), 0.0f), 1.0f) * 255.0f);
+    }
+}
+
 void orc_targets(const TfgRegistroEntrenamiento* regs, const TfgColor* tail, TfgDatosMLP* out, int n) {   // RenderKernel.cu:92-137
     for (int i = 0; i < n; ++i) {
         const TfgRegistroEntrenamiento& r = regs[i];

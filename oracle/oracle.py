@@ -34,6 +34,7 @@ def _load_cpu():
     lib.orc_infer_rows.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p]
     lib.orc_scrub.argtypes = [c_void_p, c_void_p, c_int]
     lib.orc_composite.argtypes = [c_void_p, c_void_p, c_void_p, c_int]
+    lib.orc_tonemap_filmic.argtypes = [c_void_p, c_int, c_int, c_void_p, c_void_p]
     lib.orc_targets.argtypes = [c_void_p, c_void_p, c_void_p, c_int]
     lib.orc_tail.argtypes = [c_void_p, c_void_p, c_int]
     lib.orc_default_camera.argtypes = [c_void_p, c_int, c_int]

@@ -70,6 +70,14 @@ _PROTOS = {
     "tfgMlpInference": (c_int32, [c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),
     "tfgMlpCreateEx": (c_int32, [c_uint32, c_uint32, c_uint32, c_uint64, c_int32, c_void_p]),
     "tfgMlpParamCount": (c_int32, [c_void_p]),
+    "tfgMlpSave": (c_int32, [c_void_p, c_char_p]),
+    "tfgMlpLoad": (c_int32, [c_void_p, c_char_p]),
+    "tfgNrcReconstruct": (c_int32, [c_void_p, POINTER(CRenderParams), c_void_p, c_void_p, c_int32, c_void_p, c_int32,
+                                    c_int32, c_int32, POINTER(CTinyBVHD_GPU), c_void_p, c_void_p, c_int32, c_int32,
+                                    c_int32, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p]),
+    "tfgToneMapFilmic": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
+    "tfgWritePPM": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
+    "tfgWritePFM": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
     "tfgMlpSetPrecision": (c_int32, [c_void_p, c_int32]),
     "tfgMlpCalibrate": (c_int32, [c_void_p, c_void_p, c_uint32, c_void_p]),
     "tfgMlpInferenceComposite": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),

@@ -328,6 +328,40 @@ extern "C" int tfgNrcFrameBatch(int32_t n, const TfgNrcSceneFrame* scenes, int32
     return ok();
 }
 
+// The reference's reconstruction mode (main.cpp:454-668) without its host
+// round trips: `spp` samples, each rendered with cache queries and no
+// training (main.cpp:566-575), answered by the cache and composited
+// (main.cpp:594-595), and summed into `accum` on the device (main.cpp:600-603).
+extern "C" int tfgNrcReconstruct(TfgColorMLP* mlp, const TfgRenderParams* params, const TfgCamara* camara,
+                                 const TfgPrimitiva* primitivas, int32_t num_primitivas, const TfgLuzPuntual* luces,
+                                 int32_t num_luces, int32_t W, int32_t H, const TfgTinyBVHD_GPU* bvh,
+                                 const float* tris_wt, const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh,
+                                 int32_t spp, int32_t first_frame, TfgColor* img, TfgDatosMLP* infer, TfgColor* thr,
+                                 float* accum, void* stream) {
+    using namespace tfg;
+    if (!mlp || !params || !img || !infer || !thr || !accum) return fail(TFG_E_INVALID, "tfgNrcReconstruct: null argument");
+    if (spp < 1) return fail(TFG_E_INVALID, "tfgNrcReconstruct: spp < 1");
+    if (W <= 0 || H <= 0) return fail(TFG_E_INVALID, "tfgNrcReconstruct: bad image size");
+    cudaStream_t s = (cudaStream_t)stream;
+    ColorMlp* m = reinterpret_cast<ColorMlp*>(mlp);
+    TfgRenderParams prm = *params;
+    prm.spp = 1;
+    prm.accumulate = 0;
+    prm.profile = 0;
+    const uint32_t npx = (uint32_t)W * (uint32_t)H;
+    cudaError_t e = cudaMemsetAsync(accum, 0, (size_t)npx * 3 * sizeof(float), s);
+    if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcReconstruct: ") + cudaGetErrorString(e));
+    for (int k = 0; k < spp; ++k) {
+        if (int rc = render_pass_ex(prm, camara, primitivas, num_primitivas, luces, num_luces, W, H, first_frame + k,
+                                    nullptr, nullptr, bvh, tris_wt, primitivas_bvh, num_prims_bvh, img, nullptr,
+                                    nullptr, nullptr, 0, infer, thr, 1, 0, false, 0, s))
+            return rc;
+        if (int rc = mlp_enqueue_infer(m, infer, nullptr, img, thr, npx, nullptr, s)) return rc;
+        if (int rc = launch_nrc_frame_small(3, img, accum, nullptr, nullptr, npx, 0, s)) return rc;
+    }
+    return ok();
+}
+
 extern "C" int tfgMlpGetState(TfgColorMLP* mlp, uint32_t* out8) {
     using namespace tfg;
     if (!mlp || !out8) return fail(TFG_E_INVALID, "tfgMlpGetState: null argument");

@@ -1446,6 +1446,90 @@ extern "C" int32_t tfgMlpParamCount(const TfgColorMLP* h) {
     return n ? M::params_of(n->nl) : 0;
 }
 
+// ------------------------------------------------------------------ checkpoints
+// The reference saves tiny-cuda-nn's serialised trainer (weights and
+// optimiser state, mlp.cpp:173-194) and reloads it for reconstruction
+// (mlp.cpp:196-276).  Here a checkpoint is one little-endian binary file:
+// 8-byte magic "TFGNRC01", u32 version 1, i32 hidden layers, u32 parameter
+// count, f32 bounds[6], f32 lr / beta1 / beta2 / eps / decay, u32 state[8]
+// (step, Adam t, ...), then the FP32 weights, weight average, Adam m and v.
+namespace {
+constexpr char kCkptMagic[8] = {'T', 'F', 'G', 'N', 'R', 'C', '0', '1'};
+}
+
+extern "C" int tfgMlpSave(TfgColorMLP* h, const char* path) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !path) return tfg::fail(TFG_E_INVALID, "tfgMlpSave: null argument");
+    const uint32_t np = (uint32_t)M::params_of(n->nl);
+    std::vector<float> arrays[4];
+    uint32_t st[M::S_WORDS];
+    const float* src[4] = {n->w, n->ema, n->m, n->v};
+    cudaError_t e = cudaDeviceSynchronize();
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k) {
+        arrays[k].resize(np);
+        e = cudaMemcpy(arrays[k].data(), src[k], np * sizeof(float), cudaMemcpyDeviceToHost);
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(st, n->dstate, sizeof(st), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSave");
+    FILE* f = std::fopen(path, "wb");
+    if (!f) return tfg::fail(TFG_E_INVALID, std::string("tfgMlpSave: cannot open ") + path);
+    const uint32_t version = 1;
+    const int32_t hidden = n->nl - 1;
+    const float hyper[5] = {n->lr, n->beta1, n->beta2, n->eps, n->decay};
+    bool good = std::fwrite(kCkptMagic, 1, 8, f) == 8 && std::fwrite(&version, 4, 1, f) == 1 &&
+                std::fwrite(&hidden, 4, 1, f) == 1 && std::fwrite(&np, 4, 1, f) == 1 &&
+                std::fwrite(n->bounds.lo, 4, 3, f) == 3 && std::fwrite(n->bounds.hi, 4, 3, f) == 3 &&
+                std::fwrite(hyper, 4, 5, f) == 5 && std::fwrite(st, 4, M::S_WORDS, f) == (size_t)M::S_WORDS;
+    for (int k = 0; k < 4 && good; ++k) good = std::fwrite(arrays[k].data(), 4, np, f) == np;
+    if (std::fclose(f) != 0 || !good) return tfg::fail(TFG_E_INVALID, std::string("tfgMlpSave: write failed: ") + path);
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpLoad(TfgColorMLP* h, const char* path) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !path) return tfg::fail(TFG_E_INVALID, "tfgMlpLoad: null argument");
+    FILE* f = std::fopen(path, "rb");
+    if (!f) return tfg::fail(TFG_E_INVALID, std::string("tfgMlpLoad: cannot open ") + path);
+    char magic[8];
+    uint32_t version = 0, np = 0;
+    int32_t hidden = 0;
+    float lo[3], hi[3], hyper[5];
+    uint32_t st[M::S_WORDS];
+    bool good = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kCkptMagic, 8) == 0 &&
+                std::fread(&version, 4, 1, f) == 1 && version == 1 && std::fread(&hidden, 4, 1, f) == 1 &&
+                std::fread(&np, 4, 1, f) == 1 && std::fread(lo, 4, 3, f) == 3 && std::fread(hi, 4, 3, f) == 3 &&
+                std::fread(hyper, 4, 5, f) == 5 && std::fread(st, 4, M::S_WORDS, f) == (size_t)M::S_WORDS;
+    if (!good) {
+        std::fclose(f);
+        return tfg::fail(TFG_E_INVALID, std::string("tfgMlpLoad: not a cache checkpoint: ") + path);
+    }
+    if (hidden != n->nl - 1 || np != (uint32_t)M::params_of(n->nl)) {
+        std::fclose(f);
+        return tfg::fail(TFG_E_INVALID, "tfgMlpLoad: the checkpoint's network depth differs from this model's");
+    }
+    std::vector<float> arrays[4];
+    for (int k = 0; k < 4 && good; ++k) {
+        arrays[k].resize(np);
+        good = std::fread(arrays[k].data(), 4, np, f) == np;
+    }
+    std::fclose(f);
+    if (!good) return tfg::fail(TFG_E_INVALID, std::string("tfgMlpLoad: truncated checkpoint: ") + path);
+    float* dst[4] = {n->w, n->ema, n->m, n->v};
+    cudaError_t e = cudaDeviceSynchronize();
+    for (int k = 0; k < 4 && e == cudaSuccess; ++k)
+        e = cudaMemcpy(dst[k], arrays[k].data(), np * sizeof(float), cudaMemcpyHostToDevice);
+    st[M::S_F8_VER] = 0;   // the FP8 image is re-packed on its next use
+    if (e == cudaSuccess) e = cudaMemcpy(n->dstate, st, sizeof(st), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(n->grad, 0, np * sizeof(float));
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpLoad");
+    n->bounds = M::Bounds{{lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}};
+    n->lr = hyper[0]; n->beta1 = hyper[1]; n->beta2 = hyper[2]; n->eps = hyper[3]; n->decay = hyper[4];
+    if (int rc = tfg::repack(n, 0, false, 1)) return rc;   // operand images of the loaded arrays
+    e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpLoad");
+    return tfg::ok();
+}
+
 extern "C" int tfgMlpStatus(void) {
     return tfg::check_error_flag();
 }

@@ -114,8 +114,9 @@ class ColorMLP:
         return g, float(loss.value)
 
     def save_model(self, path: str) -> None:
-        """Weights, EMA and Adam moments as one float32 .npz archive."""
-        np.savez(path, w=self.get_params(WEIGHTS), ema=self.get_params(EMA))
+        """Binary checkpoint (tfgMlpSave): weights, weight average, Adam state,
+        counters, bounds and hyper-parameters."""
+        _lib.call("tfgMlpSave", self.h, str(path).encode())
 
     def state(self) -> dict:
         st = (ctypes.c_uint32 * 8)()
@@ -124,11 +125,13 @@ class ColorMLP:
                 "loss_ema": float(np.array([st[4]], np.uint32).view(np.float32)[0])}
 
     def load_model(self, path: str) -> bool:
+        """Restore a checkpoint written by save_model (same depth); False when
+        the file is missing or not a checkpoint of this network, as the
+        reference's load_model (mlp.cpp:196-276)."""
         try:
-            d = np.load(path)
-            self.set_params(d["ema"])
+            _lib.call("tfgMlpLoad", self.h, str(path).encode())
             return True
-        except (OSError, KeyError, ValueError):
+        except _lib.TfgError:
             return False
 
 
@@ -232,3 +235,20 @@ class NrcBatch:
                 r.frames_accumulated += 1
         _lib.call("tfgNrcFrameBatch", len(self.renderers), self._arr, frame, int(self.use_graph),
                   self.stream.cuda_stream)
+
+
+def reconstruct(ds, mlp: ColorMLP, params, spp: int, first_frame: int = 0, stream=None) -> torch.Tensor:
+    """The reference's reconstruction mode (tfgNrcReconstruct): `spp` samples
+    answered by a trained cache without training; returns the (H*W*3) sum."""
+    W, H = ds.scene.width, ds.scene.height
+    n = W * H
+    dev = ds.device
+    img = torch.zeros(n * 3, dtype=torch.float32, device=dev)
+    infer = torch.zeros(n * DATOS_MLP.itemsize, dtype=torch.uint8, device=dev)
+    thr = torch.zeros(n * 3, dtype=torch.float32, device=dev)
+    accum = torch.empty(n * 3, dtype=torch.float32, device=dev)
+    _lib.call("tfgNrcReconstruct", mlp.h, ctypes.byref(params.c()), ds.camera.data_ptr(),
+              ds.prims.data_ptr() if ds.prims is not None else None, ds.n_prims, ds.lights.data_ptr(), ds.n_lights,
+              W, H, ctypes.byref(ds.bvh.ref), ds.bvh.d_tris_wt, ds.bvh.d_primitivas, ds.n_mesh, spp, first_frame,
+              img.data_ptr(), infer.data_ptr(), thr.data_ptr(), accum.data_ptr(), _stream(stream))
+    return accum

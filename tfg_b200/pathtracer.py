@@ -171,6 +171,27 @@ def accumulate_spp(ds: DeviceScene, params: RenderParams, spp: int, first_frame:
     return (acc / spp).view(H, W, 3)
 
 
+def tonemap_filmic(accum: torch.Tensor, frames: int, W: int, H: int, stream=None) -> tuple[torch.Tensor, torch.Tensor]:
+    """tfgToneMapFilmic: the averaged HDR image (H, W, 3 float32) and the
+    reference's filmic 8-bit image (H, W, 3 uint8), both on the device."""
+    hdr = torch.empty(H * W * 3, dtype=torch.float32, device=accum.device)
+    rgb8 = torch.empty(H * W * 3, dtype=torch.uint8, device=accum.device)
+    _lib.call("tfgToneMapFilmic", _ptr(accum), frames, W, H, _ptr(hdr), _ptr(rgb8), _stream(stream))
+    return hdr.view(H, W, 3), rgb8.view(H, W, 3)
+
+
+def write_ppm(path: str, rgb8) -> None:
+    """Binary PPM from an (H, W, 3) uint8 array or tensor (host copy made here)."""
+    a = np.ascontiguousarray(rgb8.cpu().numpy() if isinstance(rgb8, torch.Tensor) else rgb8, dtype=np.uint8)
+    _lib.call("tfgWritePPM", str(path).encode(), a.ctypes.data, a.shape[1], a.shape[0])
+
+
+def write_pfm(path: str, rgb) -> None:
+    """PFM (little-endian float RGB) from an (H, W, 3) float array or tensor."""
+    a = np.ascontiguousarray(rgb.cpu().numpy() if isinstance(rgb, torch.Tensor) else rgb, dtype=np.float32)
+    _lib.call("tfgWritePFM", str(path).encode(), a.ctypes.data, a.shape[1], a.shape[0])
+
+
 def profile_reset() -> None:
     _lib.call("tfgRenderProfileReset")
 
