@@ -113,13 +113,22 @@ def barrier(world):
 
 
 def max_over_ranks(x: float, world: int) -> float:
+    """Largest value over the ranks (device times: the job is as slow as its
+    slowest replica).  NCCL reduces a CUDA tensor, gloo a host one."""
     if world == 1:
         return x
     import torch
     import torch.distributed as dist
-    t = torch.tensor([x], dtype=torch.float64, device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([x], dtype=torch.float64, device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
+
+
+def replicas_value(paths_per_rank: int, ms_max: float, world: int) -> float:
+    """Whole-job Mpaths/s of `world` replicas that each trace `paths_per_rank`
+    paths, timed by the slowest rank."""
+    return world * paths_per_rank / (ms_max * 1e-3) / 1e6
 
 
 def cpu_oracle_sample(scene, hb, rows: int, nthreads: int, frame: int = 1) -> tuple[float, int]:
@@ -592,7 +601,7 @@ def main():
     prof = pt.profile_get()
     ms_max = max_over_ranks(ms, world)
     paths = n_px * SPP * args.steps
-    value = world * paths / (ms_max * 1e-3) / 1e6
+    value = replicas_value(paths, ms_max, world)
 
     # End to end through the C ABI with host buffers: per frame, camera + lights
     # from pinned host memory, 64-spp render, accumulated image back to pinned host.
