@@ -184,7 +184,7 @@ def reference_arm(args):
     }))
 
 
-def nrc_eval(scene, ds, dev, ref_spp: int = 1024, frames: int = 300) -> dict:
+def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
     """Online radiance caching at 1920x1080 (1 spp per frame, camera orbiting
     1 degree per frame, 4 x 16384 training samples per frame after the
     reference's 48 warm-up frames) against plain path tracing at equal GPU
@@ -417,6 +417,53 @@ def batched_eval(dev, frames: int = 20) -> dict:
     }
 
 
+def compare_bvh_builders():
+    """Host binned-SAH builder (tfgTinyBVHConstruir) against the device
+    Morton-order builder (tfgTinyBVHConstruirGPU) on the benchmark scene:
+    build time (including the primitive upload), primary-ray throughput and
+    8-spp path throughput with each tree."""
+    import torch
+
+    from tfg_b200 import pathtracer as pt
+    from tfg_b200 import scenes
+    s = scenes.spheres_terrain(W_PX, H_PX)
+    n = W_PX * H_PX
+    out = {}
+    for name, gpu in (("host_sah", False), ("device_morton", True)):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ds = pt.DeviceScene(s, "cuda", gpu_build=gpu)
+        torch.cuda.synchronize()
+        tb = time.perf_counter() - t0
+        rays = torch.empty(n * 8, device="cuda")
+        hits = torch.empty(n * 4, device="cuda")
+        pt.camera_rays(ds, 0, rays)
+        for _ in range(3):
+            pt.trace_rays(ds, rays, hits, pt.TRIS_WATERTIGHT)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(10):
+            pt.trace_rays(ds, rays, hits, pt.TRIS_WATERTIGHT)
+        e1.record()
+        torch.cuda.synchronize()
+        grays = n * 10 / (e0.elapsed_time(e1) * 1e-3) / 1e9
+        p = pt.RenderParams(max_depth=DEPTH, rr_min_depth=RR, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT, spp=8,
+                            accumulate=1)
+        acc = torch.zeros(n * 3, device="cuda")
+        pt.render_pass(ds, p, 0, None, acc)
+        torch.cuda.synchronize()
+        e0.record()
+        pt.render_pass(ds, p, 100, None, acc)
+        e1.record()
+        torch.cuda.synchronize()
+        out[name] = {"build_s_incl_upload": round(tb, 3), "nodes": int(ds.bvh.ref.num_nodos),
+                     "depth": int(ds.bvh.max_depth), "primary_grays_per_s": round(grays, 3),
+                     "mpaths_per_s_8spp": round(n * 8 / (e0.elapsed_time(e1) * 1e-3) / 1e6, 1)}
+        ds.close()
+    print(json.dumps(out))
+
+
 def measure_peaks():
     """Peaks this pod's MEASURED_PEAKS.json does not hold, measured the same
     way (best of 10, CUDA events): an L2-resident copy (2 x 24 MB buffers,
@@ -532,6 +579,8 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the 12-scene batched cache frame")
     ap.add_argument("--profile-pass", action="store_true",
                     help="run one untimed 1-spp pass of the workload and exit (small case for ncu)")
+    ap.add_argument("--compare-bvh-builders", action="store_true",
+                    help="host SAH vs device Morton-order CWBVH: build time and traversal speed, then exit")
     ap.add_argument("--measure-peaks", action="store_true",
                     help="measure L2 copy bandwidth and FP16 / BF16 / FP8 GEMM peaks, print them and exit")
     ap.add_argument("--profile-mlp", action="store_true",
@@ -548,6 +597,9 @@ def main():
         return
     if args.measure_peaks:
         measure_peaks()
+        return
+    if args.compare_bvh_builders:
+        compare_bvh_builders()
         return
 
     import torch

@@ -161,7 +161,15 @@ typedef struct TfgTinyBVH {
 /* TinyBVH::construirBVH: filter TRIANGULO primitives (input order kept),
  * build, upload nodes / both triangle layouts / primitives with cudaMalloc. */
 int  tfgTinyBVHConstruir(const TfgPrimitiva* primitivas_host, int32_t n, TfgTinyBVH* out);
-/* Frees what tfgTinyBVHConstruir allocated (TinyBVH::~TinyBVH). */
+/* The same hand-off built on the GPU from a DEVICE primitive array (the
+ * reference builds on the host with tinybvh, tinybvh_wrapper.cpp:30-83):
+ * TRIANGULO entries compacted in input order (their index is the prim id),
+ * Morton-ordered binary tree (Karras 2012), collapsed to 8-wide nodes and
+ * quantised on the device; same node / triangle layouts as
+ * tfgTinyBVHConstruir, a lower-quality (LBVH) tree that builds in
+ * milliseconds.  Synchronises `stream`; free with tfgTinyBVHLiberar. */
+int  tfgTinyBVHConstruirGPU(const TfgPrimitiva* primitivas_device, int32_t n, TfgTinyBVH* out, void* stream);
+/* Frees what tfgTinyBVHConstruir / tfgTinyBVHConstruirGPU allocated (TinyBVH::~TinyBVH). */
 void tfgTinyBVHLiberar(TfgTinyBVH* bvh);
 
 /* ------------------------------------------------------------------ */

@@ -36,6 +36,7 @@ _PROTOS = {
     "tfgCWBVHBuild": (c_int32, [POINTER(c_float), c_uint32, POINTER(CCWBVHHost)]),
     "tfgCWBVHFree": (None, [POINTER(CCWBVHHost)]),
     "tfgTinyBVHConstruir": (c_int32, [c_void_p, c_int32, POINTER(CTinyBVH)]),
+    "tfgTinyBVHConstruirGPU": (c_int32, [c_void_p, c_int32, POINTER(CTinyBVH), c_void_p]),
     "tfgTinyBVHLiberar": (None, [POINTER(CTinyBVH)]),
     "tfgRenderParamsReference": (None, [POINTER(CRenderParams)]),
     "tfgRenderProfileReset": (c_int32, []),

@@ -63,7 +63,9 @@ class RenderParams:
 class DeviceScene:
     """Scene resident on a GPU: analytic primitives, lights, camera, CWBVH."""
 
-    def __init__(self, scene: Scene, device="cuda"):
+    def __init__(self, scene: Scene, device="cuda", gpu_build: bool = False):
+        """`gpu_build`: build the CWBVH on the device (tfgTinyBVHConstruirGPU,
+        Morton-order tree) instead of the host binned-SAH builder."""
         self.scene = scene
         self.device = torch.device(device)
         self.prims = _dev_bytes(scene.prims, self.device)
@@ -72,8 +74,14 @@ class DeviceScene:
         self.bvh = CTinyBVH()
         mesh = np.ascontiguousarray(scene.mesh)
         with torch.cuda.device(self.device):
-            _lib.call("tfgTinyBVHConstruir", mesh.ctypes.data if len(mesh) else None, len(mesh),
-                      ctypes.byref(self.bvh))
+            if gpu_build:
+                dmesh = _dev_bytes(mesh, self.device)
+                _lib.call("tfgTinyBVHConstruirGPU", _ptr(dmesh), len(mesh), ctypes.byref(self.bvh),
+                          _stream(None))
+                del dmesh
+            else:
+                _lib.call("tfgTinyBVHConstruir", mesh.ctypes.data if len(mesh) else None, len(mesh),
+                          ctypes.byref(self.bvh))
         self.n_prims = len(scene.prims)
         self.n_lights = len(scene.lights)
         self.n_mesh = int(self.bvh.num_primitivas)
