@@ -63,6 +63,29 @@ def main() -> None:
         e1.synchronize()
         ms = e0.elapsed_time(e1) / args.frames
         out[name] = {"ms_per_frame_1spp": round(ms, 3), "mpaths_per_s": round(W * H / (ms * 1e-3) / 1e6, 1)}
+    # primary-ray traversal: traverse_cwbvh (RenderKernel.cu build) against tfgTraceRays, same rays and BVH
+    n = W * H
+    rays = torch.zeros(n * 8, dtype=torch.float32, device="cuda")
+    pt.camera_rays(ds, 0, rays)
+    hits_r = torch.zeros(n * 4, dtype=torch.float32, device="cuda")
+    hits_o = torch.zeros(n * 4, dtype=torch.float32, device="cuda")
+    steps = torch.zeros(n, dtype=torch.int32, device="cuda")
+    tr = {"reference_traverse_cwbvh": lambda: ref.ref_trace(ds.bvh.ref.d_nodos, ds.bvh.ref.d_tris, rays.data_ptr(), n,
+                                                             hits_r.data_ptr(), steps.data_ptr()),
+          "tfgTraceRays": lambda: pt.trace_rays(ds, rays, hits_o, pt.TRIS_REF, stream=torch.cuda.default_stream())}
+    for name, fn in tr.items():
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(torch.cuda.default_stream())
+        for _ in range(args.frames):
+            fn()
+        e1.record(torch.cuda.default_stream())
+        e1.synchronize()
+        out[name] = {"grays_per_s": round(n * args.frames / (e0.elapsed_time(e1) * 1e-3) / 1e9, 3)}
+    ids_r, ids_o = hits_r.view(-1, 4)[:, 3].cpu(), hits_o.view(-1, 4)[:, 3].cpu()
+    out["primary_hit_ids_equal"] = bool(torch.equal(ids_r.view(torch.int32), ids_o.view(torch.int32)))
     # same RNG streams: the last frames rendered by both are frame 100 + frames - 1
     a, b = img_ref.cpu().double(), img_ours.cpu().double()
     out["image_relmse_between_them"] = float(((a - b) ** 2 / (a ** 2 + 1e-2)).mean())
