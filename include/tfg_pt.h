@@ -413,6 +413,12 @@ int  tfgMlpSetParams(TfgColorMLP* mlp, const float* host, uint32_t count);
  * (synchronous; for gradient checks). */
 int  tfgMlpComputeGradient(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
                            float* host_grad, uint32_t count, float* loss_out);
+/* Diagnostic without a reference counterpart: runs one bounded wait that can
+ * never complete (an mbarrier nothing arrives on) with a `timeout_us` limit
+ * (at most 2 s) through the cache kernels' wait and error-flag path, and
+ * returns what a stuck cache kernel would: TFG_E_TIMEOUT (the flag is cleared
+ * and the context stays usable).  Every real wait gives up after 1 s. */
+int  tfgMlpSelfTestWait(uint32_t timeout_us);
 /* TFG_E_TIMEOUT if a bounded tensor-core wait in an MLP kernel gave up since
  * the last call (synchronous). */
 int  tfgMlpStatus(void);

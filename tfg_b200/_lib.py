@@ -79,6 +79,7 @@ _PROTOS = {
     "tfgToneMapFilmic": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p, c_void_p]),
     "tfgWritePPM": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
     "tfgWritePFM": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
+    "tfgMlpSelfTestWait": (c_int32, [c_uint32]),
     "tfgMlpSetPrecision": (c_int32, [c_void_p, c_int32]),
     "tfgMlpCalibrate": (c_int32, [c_void_p, c_void_p, c_uint32, c_void_p]),
     "tfgMlpInferenceComposite": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),

@@ -97,7 +97,10 @@ constexpr int kFwdBytesMax = fwd_bytes_of(kMaxLayers);            // 67584
 constexpr int kWeightRegion = (kFwdBytesMax + 1023) / 1024 * 1024;  // 68608
 static_assert(fwd_bytes_of(6) == 51200 && bwd_bytes_of(6) == 40960 && params_of(6) == 23552, "default layout");
 
-constexpr uint32_t kSpinLimit = 1u << 26;
+// Every wait on a bulk copy or an MMA gives up after this long (a stuck
+// wait sets g_mlp_error; the host reports TFG_E_TIMEOUT), far above any
+// legitimate wait (microseconds).
+constexpr uint64_t kSpinLimit = 1000000000ull;   // 1 s
 
 struct Bounds {
     float lo[3], hi[3];
@@ -708,10 +711,13 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
         for (int l = 0; l < NL && ok; ++l) {
             const int K = kCols<NL>(l), N = (l == NL - 1) ? kOutPad : kHid;
             const uint32_t dcol = (l == NL - 1) ? 64u : 0u;
-            if (t == 0) {
+            if (warp == 0) {   // converged warp, one elected lane issues (see k_infer)
                 umma::fence_after_sync();
-                issue_layer(tmem + dcol, sa, kTile * 128, sf + kFOff<NL>(l), kRows<NL>(l) * 128, K, N, false);
-                umma::mma_commit(&mb_mma);
+                if (umma::elect_one()) {
+                    issue_layer(tmem + dcol, sa, kTile * 128, sf + kFOff<NL>(l), kRows<NL>(l) * 128, K, N, false);
+                    umma::mma_commit(&mb_mma);
+                }
+                __syncwarp();
             }
             ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
             mph ^= 1u;
@@ -756,10 +762,13 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
         // backward: dH_{l-1} = dZ_l * W_l, masked by the ReLU of layer l-1
         for (int l = NL - 1; l >= 1 && ok; --l) {
             const int K = (l == NL - 1) ? kOutPad : kHid;
-            if (t == 0) {
+            if (warp == 0) {
                 umma::fence_after_sync();
-                issue_layer(tmem, sa, kTile * 128, sb + kBOff<NL>(l), 64 * 128, K, kHid, true);
-                umma::mma_commit(&mb_mma);
+                if (umma::elect_one()) {
+                    issue_layer(tmem, sa, kTile * 128, sb + kBOff<NL>(l), 64 * 128, K, kHid, true);
+                    umma::mma_commit(&mb_mma);
+                }
+                __syncwarp();
             }
             ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
             mph ^= 1u;
@@ -1528,6 +1537,27 @@ extern "C" int tfgMlpLoad(TfgColorMLP* h, const char* path) {
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpLoad");
     return tfg::ok();
+}
+
+// Diagnostic for the failure path: one thread waits on an mbarrier that
+// nothing arrives on, with the given limit, through the same bounded wait the
+// cache kernels use; on giving up it sets the same error flag.
+__global__ void k_selftest_wait(uint64_t limit_ns) {
+    __shared__ uint64_t mb;
+    if (threadIdx.x != 0) return;
+    tfg::umma::mbar_init(&mb, 1);
+    tfg::umma::mbar_fence_init();
+    if (!tfg::umma::mbar_wait(&mb, 0, limit_ns)) atomicExch(&M::g_mlp_error, 1);
+}
+
+extern "C" int tfgMlpSelfTestWait(uint32_t timeout_us) {
+    if (timeout_us == 0 || timeout_us > 2000000u)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpSelfTestWait: timeout must be in (0, 2 s]");
+    k_selftest_wait<<<1, 32>>>((uint64_t)timeout_us * 1000ull);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSelfTestWait");
+    return tfg::check_error_flag();
 }
 
 extern "C" int tfgMlpStatus(void) {

@@ -158,12 +158,21 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* mbar, uint32_t phase) {
     return ok != 0;
 }
 
-// Bounded wait: returns false (and leaves the barrier alone) when `limit`
-// polls pass without the phase completing.
-__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t phase, uint32_t limit = (1u << 26)) {
-    for (uint32_t i = 0; i < limit; ++i)
+__device__ __forceinline__ uint64_t globaltimer_ns() {
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Bounded wait: returns false (and leaves the barrier alone) when the phase
+// has not completed `limit_ns` nanoseconds after the call (checked every 64
+// polls; each poll may itself suspend the thread briefly).
+__device__ __forceinline__ bool mbar_wait(uint64_t* mbar, uint32_t phase, uint64_t limit_ns = 1000000000ull) {
+    const uint64_t t0 = globaltimer_ns();
+    for (uint32_t i = 1;; ++i) {
         if (mbar_try_wait(mbar, phase)) return true;
-    return false;
+        if ((i & 63u) == 0u && globaltimer_ns() - t0 > limit_ns) return false;
+    }
 }
 
 // ------------------------------------------------------------------ bulk copy (TMA, non-tensor)
