@@ -388,7 +388,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sw = smem;
-    __shared__ uint64_t mb_w, mb_mma[kSlots], mb_in[kSlots];
+    __shared__ uint64_t mb_w, mb_mma[kSlots], mb_in[kSlots], mb_drain[kSlots];
     __shared__ uint32_t tslot;
     const int tid = threadIdx.x, warp = tid >> 5, q = warp & 3, t = tid & 127;
     const int slot = tid / 128;
@@ -412,6 +412,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
         for (int k = 0; k < kSlots; ++k) {
             umma::mbar_init(&mb_mma[k], 1);
             umma::mbar_init(&mb_in[k], 1);
+            umma::mbar_init(&mb_drain[k], 1);
         }
         umma::mbar_fence_init();
     }
@@ -555,6 +556,13 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
         }
     }
     if (pending) umma::mbar_wait(&mb_in[slot], iph, kSpinLimit);   // no copy may land after exit
+    if (!ok && issuer_warp) {   // after a timeout: every MMA this slot issued must finish before TMEM is freed
+        if (umma::elect_one()) {
+            umma::mma_commit(&mb_drain[slot]);
+            umma::mbar_wait(&mb_drain[slot], 0, kSpinLimit);
+        }
+        __syncwarp();
+    }
     if (!ok && leader) atomicExch(&g_mlp_error, 1);
     __syncthreads();
     if (warp == 0) umma::tmem_dealloc(tslot, 512);
@@ -653,7 +661,7 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     uint8_t* sf = smem + kTrainSmemF;
     uint8_t* sb = smem + kTrainSmemB;
     uint8_t* sa = smem + kTrainSmemA;
-    __shared__ uint64_t mb_w, mb_mma;
+    __shared__ uint64_t mb_w, mb_mma, mb_drain;
     __shared__ uint32_t tslot;
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t ntiles = a.batch / kTile;
@@ -664,6 +672,7 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     if (t == 0) {
         umma::mbar_init(&mb_w, 1);
         umma::mbar_init(&mb_mma, 1);
+        umma::mbar_init(&mb_drain, 1);
         umma::mbar_fence_init();
     }
     for (int i = t; i < kTile * 4; i += blockDim.x) {
@@ -678,7 +687,8 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
         umma::bulk_g2s(sf, a.fwd, kFwdBytes<NL>, &mb_w);
         umma::bulk_g2s(sb, a.bwd, kBwdBytes<NL>, &mb_w);
     }
-    bool ok = umma::mbar_wait(&mb_w, 0, kSpinLimit);
+    bool ok = all_ok(umma::mbar_wait(&mb_w, 0, kSpinLimit));
+    const bool weights_in = ok;
     uint32_t mph = 0;
     float lsum = 0.0f;
     for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
@@ -791,6 +801,14 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     // loss reduction
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xFFFFFFFFu, lsum, o);
     if ((t & 31) == 0) atomicAdd(a.loss, lsum);
+    if (!ok && warp == 0) {   // after a timeout: the weight copy and every issued MMA finish first
+        if (umma::elect_one()) {
+            if (!weights_in) umma::mbar_wait(&mb_w, 0, kSpinLimit);
+            umma::mma_commit(&mb_drain);
+            umma::mbar_wait(&mb_drain, 0, kSpinLimit);
+        }
+        __syncwarp();
+    }
     if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
     __syncthreads();
     if (warp == 0) umma::tmem_dealloc(tmem, 128);
@@ -840,7 +858,9 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     umma::fence_after_sync();
     const uint32_t tmem = tslot;
     const uint32_t zbytes = (uint32_t)FZ * 128, hbytes = 2u * FH * 128;
+    bool ld_pending[2] = {false, false};
     auto load = [&](uint32_t tile, int stage) {
+        ld_pending[stage] = true;
         uint8_t* sA = smem + kWgSmemA + stage * 32768;
         uint8_t* sB = smem + kWgSmemB + stage * (2 * 96 * 128);
         const uint8_t* gz = a.zT[l] + (size_t)tile * 2 * zbytes;
@@ -859,8 +879,9 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
         for (uint32_t tile = t0; tile < t1 && ok; ++tile) {
             const int stage = (int)((tile - t0) & 1u);
             ok = umma::mbar_wait(&mb_ld[stage], ldph[stage], kSpinLimit);
-            ldph[stage] ^= 1u;
             if (!ok) break;
+            ldph[stage] ^= 1u;
+            ld_pending[stage] = false;
             umma::fence_after_sync();
             const uint8_t* sA = smem + kWgSmemA + stage * 32768;
             const uint8_t* sB = smem + kWgSmemB + stage * (2 * 96 * 128);
@@ -879,11 +900,12 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
                 load(tile + 2, stage);
             }
         }
-        // One more commit tracks every MMA issued above.
-        if (ok) {
-            umma::mma_commit(&mb_done);
-            ok = umma::mbar_wait(&mb_done, 0, kSpinLimit);
-        }
+        // One more commit tracks every MMA issued above; after a timeout the
+        // loads still in flight are waited for as well (no copy lands after exit).
+        umma::mma_commit(&mb_done);
+        ok = umma::mbar_wait(&mb_done, 0, kSpinLimit) && ok;
+        for (int k = 0; k < 2; ++k)
+            if (ld_pending[k]) umma::mbar_wait(&mb_ld[k], ldph[k], kSpinLimit);
     }
     ok = all_ok(ok);
     umma::fence_after_sync();
