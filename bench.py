@@ -344,6 +344,64 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
     }
 
 
+def c1_eval(dev, nthreads: int) -> dict:
+    """The reference's CPU-runnable case (config 1): displaced icosphere
+    (subdiv 6, 81,920 tris) in a 12-triangle box, one light, 512x512, 16 spp,
+    depth 5, roulette from depth 3, frames 1..16.  GPU time with resident
+    inputs, the CPU oracle on all host cores for the same 16 samples, and the
+    relMSE between the two images (same RNG streams)."""
+    import ctypes
+
+    import numpy as np
+    import torch
+
+    from oracle import oracle as orc
+    from tfg_b200 import bvh as hbvh
+    from tfg_b200 import pathtracer as pt
+    from tfg_b200 import scenes
+    s = scenes.box_icosphere(512, 512, subdiv=6, seed=1)
+    ds = pt.DeviceScene(s, dev)
+    W, H, spp = s.width, s.height, 16
+    p = pt.RenderParams(max_depth=5, rr_min_depth=3, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT, spp=spp,
+                        accumulate=1)
+    acc = torch.zeros(W * H * 3, device=dev)
+    for _ in range(3):
+        acc.zero_()
+        pt.render_pass(ds, p, 1, None, acc)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 10
+    e0.record()
+    for _ in range(reps):
+        acc.zero_()
+        pt.render_pass(ds, p, 1, None, acc)
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    gpu_img = (acc / spp).view(H, W, 3).cpu().numpy().astype(np.float64)
+    ds.close()
+    hb = hbvh.build_host(hbvh.triangle_vertices(s.mesh))
+    prm = pt.RenderParams(max_depth=5, rr_min_depth=3, shadow_mesh=1).c()
+    cpu = np.zeros((H, W, 3), np.float64)
+    img = np.zeros((H, W, 3), np.float32)
+    t0 = time.perf_counter()
+    for f in range(1, spp + 1):
+        orc.cpu.orc_render(orc.p(s.prims), len(s.prims), orc.p(s.lights), len(s.lights), orc.p(hb.nodes),
+                           orc.p(hb.tris_ref), orc.p(s.mesh), len(s.mesh), orc.p(s.camera), W, H, f,
+                           ctypes.addressof(prm), 0, H, orc.p(img), None, None, None, None, 0, 0, nthreads)
+        cpu += img
+    t_cpu = time.perf_counter() - t0
+    cpu /= spp
+    relmse = float(np.mean((gpu_img - cpu) ** 2 / (cpu ** 2 + 1e-2)))
+    return {"workload": "512x512, 16 spp, depth 5, RR from 3, displaced icosphere (81,920 tris) in a 12-tri box, "
+                        "1 light, frames 1..16",
+            "gpu_ms_per_frame": round(ms, 3), "gpu_mpaths_per_s": round(W * H * spp / (ms * 1e-3) / 1e6, 1),
+            "cpu_s_per_frame": round(t_cpu, 2), "cpu_mpaths_per_s": round(W * H * spp / t_cpu / 1e6, 3),
+            "cpu_cores": nthreads, "cpu_kind": "port",
+            "relmse_gpu_vs_cpu_oracle": relmse, "note": "the CPU oracle uses the reference's transform triangle "
+            "test, the GPU the watertight one"}
+
+
 def batched_eval(dev, frames: int = 20) -> dict:
     """Twelve independent scenes (10k to 2M triangles, 1-4 lights, 640x360 to
     1920x1080), one cache model each, 1 spp + cache per frame, advanced by
@@ -711,6 +769,9 @@ def main():
     batched = None
     if not args.no_batched and world == 1:
         batched = batched_eval(dev)
+    c1 = None
+    if not args.no_cpu_baseline and world == 1:
+        c1 = c1_eval(dev, os.cpu_count() or 1)
 
     pk = peaks()
     trace_ms = prof["ms"]["trace"]
@@ -770,6 +831,7 @@ def main():
         "cpu_baseline": cpu,
         "nrc": nrc,
         "batched": batched,
+        "c1_cpu_runnable_case": c1,
     }
     print(json.dumps(out))
     ds.close()
