@@ -31,8 +31,15 @@ METRIC = "Mpaths/s & ms/frame @1080p"
 WORKLOAD = "plain path tracing, 1920x1080, 64 spp, depth 8, RR from depth 3, 16 displaced icospheres + fractal terrain (1,000,480 tris), 2 point lights"
 
 
-# Measured once with ncu on `bench.py --profile-pass` (see the profiles/ summary named above).
-TRACE_DRAM_BYTES_PER_LAUNCH = 41_169_312
+# DRAM bytes (read + write) per closest-hit launch, measured with ncu on
+# `bench.py --profile-pass --wavefront-samples K`, by K = image samples per
+# wavefront (profiles/k_trace_k_shadow_dram_1080p.md).
+TRACE_DRAM_BYTES_PER_LAUNCH = {1: 41_169_312, 16: 538_379_104}
+
+
+def trace_traffic(wavefront_paths: int, n_px: int):
+    k = max(1, wavefront_paths // n_px) if wavefront_paths else 1
+    return TRACE_DRAM_BYTES_PER_LAUNCH.get(k)
 
 
 def peaks() -> dict:
@@ -365,6 +372,7 @@ def c1_eval(dev, nthreads: int) -> dict:
     p = pt.RenderParams(max_depth=5, rr_min_depth=3, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT, spp=spp,
                         accumulate=1)
     acc = torch.zeros(W * H * 3, device=dev)
+    tuning, _ = pt.autotune(ds, p, repeats=3)
     for _ in range(3):
         acc.zero_()
         pt.render_pass(ds, p, 1, None, acc)
@@ -396,6 +404,7 @@ def c1_eval(dev, nthreads: int) -> dict:
     return {"workload": "512x512, 16 spp, depth 5, RR from 3, displaced icosphere (81,920 tris) in a 12-tri box, "
                         "1 light, frames 1..16",
             "gpu_ms_per_frame": round(ms, 3), "gpu_mpaths_per_s": round(W * H * spp / (ms * 1e-3) / 1e6, 1),
+            "tuning": tuning.__dict__,
             "cpu_s_per_frame": round(t_cpu, 2), "cpu_mpaths_per_s": round(W * H * spp / t_cpu / 1e6, 3),
             "cpu_cores": nthreads, "cpu_kind": "port",
             "relmse_gpu_vs_cpu_oracle": relmse, "note": "the CPU oracle uses the reference's transform triangle "
@@ -430,6 +439,18 @@ def batched_eval(dev, frames: int = 20) -> dict:
         batch.frame(f, warmup=True)
     for f in range(8):
         batch.frame(48 + f)
+    st.synchronize()
+    # Autotuned queue and MLP tile sizes: the launch settings on the largest
+    # scene (plain 1-spp passes), the model's tiling on that scene's cache
+    # queries; every model shares the architecture and takes the same tiling.
+    big = max(range(len(scs)), key=lambda k: scs[k].width * scs[k].height)
+    render_tuning, _ = pt.autotune(dss[big], params, repeats=3, stream=st)
+    n_big = scs[big].width * scs[big].height
+    scratch = torch.zeros(n_big * 3, dtype=torch.float32, device=dev)
+    mlp_tuning = rs[big].mlp.autotune(rs[big].infer, scratch, n_big, repeats=5, stream=st)
+    for r in rs:
+        r.mlp.set_tuning(mlp_tuning["wgrad_tiles_per_cta"], mlp_tuning["infer_ctas"])
+    batch.frame(56)   # captures the graph again under the new settings
     st.synchronize()
 
     def timed(fn, n):
@@ -471,6 +492,7 @@ def batched_eval(dev, frames: int = 20) -> dict:
         "ms_per_frame_12_single_scene_calls": round(ms_single, 3),
         "mpaths_per_s_graph": round(px / (ms_graph * 1e-3) / 1e6, 1),
         "adam_steps_min": min(adam), "setup_s": round(t_setup, 1),
+        "render_tuning": render_tuning.__dict__, "mlp_tuning": mlp_tuning,
         "frame": "render 1 spp with cache queries + training records, inference + composite, targets, 4 Adam steps",
     }
 
@@ -608,17 +630,21 @@ def profile_mlp():
     print("profile mlp done")
 
 
-def profile_pass():
-    """One 1-spp pass (8 bounces) of the benchmark frame: ~0.3 GB of scene
-    data (more than L2) and ~0.5 GB of queues; used for ncu captures."""
+def profile_pass(samples: int = 1, tuning: str | None = None):
+    """One pass of `samples` spp (8 bounces) of the benchmark frame in one
+    wavefront of samples x W x H paths: ~0.3 GB of scene data (more than L2)
+    and ~0.5 GB of queues per sample; used for ncu captures.  `tuning`: JSON
+    object of further TfgRenderTuning fields (e.g. the autotuner's pick)."""
     import torch
 
     from tfg_b200 import pathtracer as pt
     from tfg_b200 import scenes
     scene = scenes.spheres_terrain(W_PX, H_PX)
     ds = pt.DeviceScene(scene, "cuda")
+    fields = {"wavefront_paths": 0 if samples == 1 else samples * W_PX * H_PX, **json.loads(tuning or "{}")}
+    pt.set_tuning(pt.RenderTuning(**fields))
     p = pt.RenderParams(max_depth=DEPTH, rr_min_depth=RR, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT,
-                        spp=1, accumulate=1)
+                        spp=samples, accumulate=1)
     accum = torch.zeros(W_PX * H_PX * 3, dtype=torch.float32, device="cuda")
     pt.render_pass(ds, p, 1, None, accum)
     torch.cuda.synchronize()
@@ -636,7 +662,11 @@ def main():
     ap.add_argument("--no-nrc", action="store_true", help="skip the radiance-cache evaluation")
     ap.add_argument("--no-batched", action="store_true", help="skip the 12-scene batched cache frame")
     ap.add_argument("--profile-pass", action="store_true",
-                    help="run one untimed 1-spp pass of the workload and exit (small case for ncu)")
+                    help="run one untimed pass of the workload and exit (small case for ncu)")
+    ap.add_argument("--wavefront-samples", type=int, default=1,
+                    help="with --profile-pass: samples per pass, all in one wavefront")
+    ap.add_argument("--tuning", default=None,
+                    help='with --profile-pass: JSON of launch tuning fields, e.g. \'{"shadow_one_lane": 1}\'')
     ap.add_argument("--compare-bvh-builders", action="store_true",
                     help="host SAH vs device Morton-order CWBVH: build time and traversal speed, then exit")
     ap.add_argument("--measure-peaks", action="store_true",
@@ -648,7 +678,7 @@ def main():
         reference_arm(args)
         return
     if args.profile_pass:
-        profile_pass()
+        profile_pass(args.wavefront_samples, args.tuning)
         return
     if args.profile_mlp:
         profile_mlp()
@@ -688,6 +718,13 @@ def main():
     # Algorithmic bytes of one closest-hit ray (watertight layout): 80 B per node
     # decoded, 48 B per triangle tested, 32 B ray read, 16 B hit written.
     bytes_per_ray = 80.0 * nodes_per_ray + 48.0 * tris_per_ray + 32.0 + 16.0
+
+    # The autotuner picks the wavefront size and launch shapes on this frame
+    # (untimed, like the warm-up); the timed frames and the e2e calls use it.
+    t_tune = time.perf_counter()
+    tuning, tune_table = pt.autotune(ds, base, repeats=2)
+    tune_s = time.perf_counter() - t_tune
+    tuned_ms = min(ms for t, ms in tune_table if t == tuning)
 
     for s in range(args.warmup):
         accum.zero_()
@@ -816,9 +853,9 @@ def main():
             "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,
             "peak_source": pk["source"],
             # ncu dram__bytes_read.sum + dram__bytes_write.sum of the 8 closest-hit launches of one
-            # 1-spp pass of this frame, per launch (profiles/k_trace_k_shadow_dram_1080p.md): the
-            # 64 MB CWBVH + triangles stay L2-resident, so DRAM sees ~8 % of the algorithmic bytes.
-            "traffic": TRACE_DRAM_BYTES_PER_LAUNCH, "traffic_unit": "bytes per launch",
+            # pass in the tuned wavefront size, per launch (profiles/k_trace_k_shadow_dram_1080p.md):
+            # the 64 MB CWBVH + triangles stay L2-resident, so DRAM sees ~6-8 % of the algorithmic bytes.
+            "traffic": trace_traffic(tuning.wavefront_paths, n_px), "traffic_unit": "bytes per launch",
             "algorithmic_bytes_per_ray": round(bytes_per_ray, 1),
             "nodes_per_ray": round(nodes_per_ray, 3), "tri_tests_per_ray": round(tris_per_ray, 3),
             "rays_per_launch_avg": round(rays_timed / max(1, trace_launches), 1),
@@ -826,6 +863,14 @@ def main():
             "stage_ms": {k: round(v, 2) for k, v in prof["ms"].items()},
         },
         "primary_rays": {"grays_per_s": round(primary_grays, 3), "rays": n_px, "tri_test": "watertight"},
+        "autotune": {
+            "tuning": tuning.__dict__, "seconds": round(tune_s, 2), "spp_per_pass": min(SPP, 16),
+            "pass_ms_start": round(tune_table[0][1], 3), "pass_ms_tuned": round(tuned_ms, 3),
+            "candidates": [[t.wavefront_paths, t.trace_threads, t.trace_warps_per_sm, t.refill_min,
+                            t.shadow_one_lane, round(ms, 3)] for t, ms in tune_table],
+            "candidate_fields": ["wavefront_paths", "trace_threads", "trace_warps_per_sm", "refill_min",
+                                 "shadow_one_lane", "ms_per_pass"],
+        },
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,

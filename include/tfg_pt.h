@@ -293,6 +293,57 @@ int tfgTraceRays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int32_t tri_f
 int tfgGenerateCameraRays(const TfgCamara* camara, int32_t ancho_img, int32_t alto_img,
                           int32_t frame_number, float* rays, void* stream);
 
+/* ------------------------------------------------------------------ */
+/* Launch tuning and the autotuner -- no reference counterpart (the    */
+/* reference launches one thread per pixel in fixed 16 x 16 blocks,    */
+/* RenderKernel.cu:16-25)                                              */
+/* ------------------------------------------------------------------ */
+
+/* How the wavefront stages of the current device are sized and launched.
+ * Every setting computes the same image from the same inputs (bit for bit);
+ * only speed and memory change. */
+typedef struct TfgRenderTuning {
+    int32_t wavefront_paths;    /* queue capacity: paths per wavefront, 0 (default) = one sample of every
+                                   pixel (W*H).  More runs several samples of the call per launch, less
+                                   splits a sample into chunks; passes that query or train the cache
+                                   stop at W*H.  0 or 1024 .. 2^26 (224 B of device memory per path) */
+    int32_t trace_threads;      /* threads per traversal and shadow-ray CTA: 64, 128 (default) or 256 */
+    int32_t trace_warps_per_sm; /* resident traversal warps per SM; 0 (default) = as many as fit */
+    int32_t refill_min;         /* idle lanes that make a traversal warp fetch new rays, 1..32 (default 8) */
+    int32_t shadow_one_lane;    /* threads per shadow query: 0 (default) = one lane per light (up to 32
+                                   lights), 1 = one lane traces all lights of a shading point */
+    int32_t reserved[3];
+} TfgRenderTuning;
+
+void tfgRenderTuningDefault(TfgRenderTuning* t);
+/* Applies to later passes on the current device, including frames captured
+ * as CUDA graphs (they are re-captured on their next call). */
+int  tfgRenderTuningSet(const TfgRenderTuning* t);
+int  tfgRenderTuningGet(TfgRenderTuning* out);
+
+/* One autotuner measurement: a candidate and its mean pass time. */
+typedef struct TfgTuneRecord {
+    TfgRenderTuning tuning;
+    float ms;
+    int32_t reserved;
+} TfgTuneRecord;
+
+/* The autotuner: times plain passes of this scene (no image written; the
+ * call's spp capped at 16) under candidate tunings with CUDA events on
+ * `stream`, one setting at a time starting from the current one (queue size,
+ * then CTA size, warps per SM, refill threshold, shadow lanes), `repeats`
+ * timed passes per candidate after one warm-up (0 = 3).  A candidate must be
+ * at least 1% faster to replace the best.  Sets the winner on the current
+ * device and returns it in `out`.  `num_records` (optional) gets the number
+ * of candidates timed, the first `max_records` of them stored in `records`
+ * (optional) in the order timed.  Synchronous; not during stream capture. */
+int  tfgRenderAutotune(const TfgRenderParams* params, const TfgCamara* camara, const TfgPrimitiva* primitivas,
+                       int32_t num_primitivas, const TfgLuzPuntual* luces, int32_t num_luces, int32_t ancho_img,
+                       int32_t alto_img, const TfgTinyBVHD_GPU* nodos_bvh, const float* tris_wt,
+                       const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh, int32_t repeats,
+                       TfgRenderTuning* out, TfgTuneRecord* records, int32_t max_records, int32_t* num_records,
+                       void* stream);
+
 /* launchInicializarCamara (RenderKernel.cu:68-90): default 45-degree camera
  * at (0,-0.75,4.25) looking down -z, written to device pointer d_camara. */
 int tfgLaunchInicializarCamara(TfgCamara* d_camara, int32_t ancho_imagen, int32_t alto_imagen,
@@ -419,6 +470,27 @@ int  tfgMlpComputeGradient(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t
  * returns what a stuck cache kernel would: TFG_E_TIMEOUT (the flag is cleared
  * and the context stays usable).  Every real wait gives up after 1 s. */
 int  tfgMlpSelfTestWait(uint32_t timeout_us);
+/* How a model's kernels tile their batches (no reference counterpart).
+ * Every setting computes the same values up to the order of FP32 gradient
+ * additions. */
+typedef struct TfgMlpTuning {
+    int32_t wgrad_tiles_per_cta;  /* 128-sample tiles one weight-gradient CTA reduces before adding to the
+                                     gradient; 0 (default) = max(2, tiles / 16) */
+    int32_t infer_ctas;           /* CTAs of an inference launch (4 tiles of 128 in flight each);
+                                     0 (default) = one per SM */
+    int32_t reserved[2];
+} TfgMlpTuning;
+int  tfgMlpTuningSet(TfgColorMLP* mlp, const TfgMlpTuning* t);
+int  tfgMlpTuningGet(TfgColorMLP* mlp, TfgMlpTuning* out);
+/* The autotuner for the model's kernels: times the weight-gradient kernel of
+ * one training batch for tiles-per-CTA in {1, 2, 4, ..., 64} and inference of
+ * `count` samples of `in` (written to `out`) for CTA counts of 1/2, 3/4 and 1
+ * per SM, `repeats` timed launches each after a warm-up (0 = 5), with CUDA
+ * events on `stream`.  The model's weights, optimiser state, pending gradient
+ * and FP8 scales are left as they were.  Sets and returns the winners;
+ * `ms_out` (optional, 2 floats) gets their times.  Synchronous. */
+int  tfgMlpAutotune(TfgColorMLP* mlp, const TfgDatosMLP* in, uint32_t count, TfgColor* out, int32_t repeats,
+                    TfgMlpTuning* result, float* ms_out, void* stream);
 /* TFG_E_TIMEOUT if a bounded tensor-core wait in an MLP kernel gave up since
  * the last call (synchronous). */
 int  tfgMlpStatus(void);

@@ -10,8 +10,8 @@ import ctypes
 from ctypes import POINTER, c_char_p, c_float, c_int32, c_uint32, c_uint64, c_void_p
 from pathlib import Path
 
-from .structs import (CCWBVHHost, CImagenGPU, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame, CRenderParams,
-                      CRenderProfile, CTinyBVH, CTinyBVHD_GPU)
+from .structs import (CCWBVHHost, CImagenGPU, CMlpTuning, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame,
+                      CRenderParams, CRenderProfile, CRenderTuning, CTinyBVH, CTinyBVHD_GPU, CTuneRecord)
 
 LIB_PATH = Path(__file__).resolve().parent / "libtfgpt.so"
 
@@ -41,6 +41,17 @@ _PROTOS = {
     "tfgRenderParamsReference": (None, [POINTER(CRenderParams)]),
     "tfgRenderProfileReset": (c_int32, []),
     "tfgRenderProfileGet": (c_int32, [POINTER(CRenderProfile)]),
+    "tfgRenderTuningDefault": (None, [POINTER(CRenderTuning)]),
+    "tfgRenderTuningSet": (c_int32, [POINTER(CRenderTuning)]),
+    "tfgRenderTuningGet": (c_int32, [POINTER(CRenderTuning)]),
+    "tfgRenderAutotune": (c_int32, [
+        POINTER(CRenderParams), c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32,
+        POINTER(CTinyBVHD_GPU), c_void_p, c_void_p, c_int32, c_int32, POINTER(CRenderTuning), POINTER(CTuneRecord),
+        c_int32, POINTER(c_int32), c_void_p]),
+    "tfgMlpTuningSet": (c_int32, [c_void_p, POINTER(CMlpTuning)]),
+    "tfgMlpTuningGet": (c_int32, [c_void_p, POINTER(CMlpTuning)]),
+    "tfgMlpAutotune": (c_int32, [c_void_p, c_void_p, c_uint32, c_void_p, c_int32, POINTER(CMlpTuning),
+                                 POINTER(c_float), c_void_p]),
     "tfgLaunchKernelRenderTiny": (c_int32, [
         c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32,
         POINTER(CTinyBVHD_GPU), c_void_p, c_int32, POINTER(CImagenGPU), c_void_p, c_void_p, c_void_p, c_int32,

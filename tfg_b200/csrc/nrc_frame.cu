@@ -31,7 +31,7 @@ __global__ void k_set_frame(int32_t* frame_dev, int32_t frame) {
 
 struct FrameKey {
     const void* ptrs[20];
-    int32_t ints[16];
+    int32_t ints[20];
     float gate;
     bool operator==(const FrameKey& o) const { return std::memcmp(this, &o, sizeof(FrameKey)) == 0; }
 };
@@ -92,6 +92,19 @@ int enqueue_frame(const FrameCall& c, bool prepare_only, cudaStream_t s) {
     return ok();
 }
 
+int current_device() {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    return dev;
+}
+
+// Launch tuning of the current device: a change re-captures the frame graph.
+uint32_t render_generation() {
+    uint32_t g = 0;
+    render_tuning_get(current_device(), nullptr, &g);
+    return g;
+}
+
 FrameKey key_of(const FrameCall& c) {
     FrameKey k;
     std::memset(&k, 0, sizeof(k));
@@ -102,7 +115,9 @@ FrameKey key_of(const FrameCall& c) {
     const int32_t v[] = {c.nprims, c.nlights, c.W, c.H, c.nmesh, (int32_t)c.b.ring_cap, c.cfg.train_steps,
                          (int32_t)c.cfg.max_records, (int32_t)c.cfg.min_records, c.cfg.warmup, c.prm.max_depth,
                          c.prm.rr_min_depth, c.prm.shadow_mesh, c.prm.tri_format, c.ws_slot,
-                         mlp_precision(c.mlp)};
+                         mlp_precision(c.mlp), (int32_t)render_generation(), (int32_t)mlp_tuning_generation(c.mlp),
+                         (int32_t)workspace_generation(current_device(), c.ws_slot)};
+    static_assert(sizeof(v) <= sizeof(k.ints), "frame key: too many ints");
     std::memcpy(k.ints, v, sizeof(v));
     k.gate = c.cfg.gate_threshold;
     return k;
@@ -228,12 +243,14 @@ extern "C" int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const
         return enqueue_frame(c, false, s);
     }
     FrameGraph& g = g_graph[dev & 15];
+    // Prepare first: a workspace that had to grow since the capture changes
+    // the key, and the frame is captured again.
+    if (int rc = enqueue_frame(c, true, s)) return rc;
     const FrameKey key = key_of(c);
     if (!g.valid || !(g.key == key)) {
         if (g.exec) cudaGraphExecDestroy(g.exec);
         if (g.graph) cudaGraphDestroy(g.graph);
         g.exec = nullptr; g.graph = nullptr; g.valid = false;
-        if (int rc = enqueue_frame(c, true, s)) return rc;
         e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame capture: ") + cudaGetErrorString(e));
         const int rc = enqueue_frame(c, false, s);

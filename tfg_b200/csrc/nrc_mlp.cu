@@ -1038,6 +1038,8 @@ struct ColorMlp {
     bool f8_calibrated = false;
     uint32_t act_tiles = 0;
     int sms = 148;
+    TfgMlpTuning tune{};         // batch tiling of the kernels (zero fields: defaults)
+    uint32_t tune_generation = 0;
 };
 
 namespace {
@@ -1112,6 +1114,39 @@ int check_error_flag() {
     return ok();
 }
 
+// Sample tiles per weight-gradient CTA: the tuned value, else enough CTAs
+// per layer (16) to spread the reduction with at least 2 tiles each.
+uint32_t wgrad_tiles_per_cta(const ColorMlp* n, uint32_t tiles) {
+    if (n->tune.wgrad_tiles_per_cta > 0) return std::min<uint32_t>((uint32_t)n->tune.wgrad_tiles_per_cta, tiles);
+    return std::max<uint32_t>(2u, (tiles + 15u) / 16u);
+}
+
+// Inference CTAs for `tiles` tiles of 128 queries: 4 tiles in flight per CTA,
+// at most one CTA per SM or the tuned count.
+uint32_t infer_grid(const ColorMlp* n, uint32_t tiles) {
+    uint32_t cap = (uint32_t)n->sms;
+    if (n->tune.infer_ctas > 0) cap = std::min<uint32_t>(cap, (uint32_t)n->tune.infer_ctas);
+    return std::max<uint32_t>(1u, std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, cap));
+}
+
+int enqueue_wgrad(ColorMlp* n, uint32_t tiles_per_cta, uint32_t min_n, cudaStream_t s) {
+    const uint32_t tiles = n->batch / mlp::kTile;
+    mlp::WgradArgs wa;
+    for (int l = 0; l < mlp::kMaxLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
+    wa.grad = n->grad; wa.state = n->dstate; wa.min_n = min_n;
+    wa.ntiles = tiles;
+    wa.tiles_per_cta = std::max<uint32_t>(1u, tiles_per_cta);
+    with_layers(n->nl, [&](auto c) {
+        constexpr int NL = decltype(c)::value;
+        mlp::k_wgrad<NL><<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, NL), 128, mlp::kWgSmem + 1024, s>>>(
+            wa);
+        return 0;
+    });
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mlp step: weight gradients");
+    return ok();
+}
+
 // Forward/backward, weight gradients (and, with `update`, Adam + tick) of one
 // step whose record count and seed are already in the device state.
 int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool update, cudaStream_t s) {
@@ -1129,19 +1164,7 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     });
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp step: forward/backward");
-    mlp::WgradArgs wa;
-    for (int l = 0; l < mlp::kMaxLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
-    wa.grad = n->grad; wa.state = n->dstate; wa.min_n = min_n;
-    wa.ntiles = tiles;
-    wa.tiles_per_cta = std::max<uint32_t>(2u, (tiles + 15u) / 16u);
-    with_layers(n->nl, [&](auto c) {
-        constexpr int NL = decltype(c)::value;
-        mlp::k_wgrad<NL><<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, NL), 128, mlp::kWgSmem + 1024, s>>>(
-            wa);
-        return 0;
-    });
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "mlp step: weight gradients");
+    if (int rc = enqueue_wgrad(n, wgrad_tiles_per_cta(n, tiles), min_n, s)) return rc;
     if (!update) return ok();
     if (int rc = repack(n, s, true, min_n)) return rc;
     mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n, n->gate);
@@ -1165,7 +1188,7 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
     if (n->prec == mlp::kPrecF8 && !n->f8_calibrated)
         return fail(TFG_E_INVALID, "mlp inference: FP8 needs tfgMlpCalibrate first");
     const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
-    const uint32_t grid = std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, (uint32_t)n->sms);
+    const uint32_t grid = infer_grid(n, tiles);
     const size_t smem = mlp::kInferSmem + 1024;
     cudaError_t e = cudaSuccess;
     const int rc = with_layers(n->nl, [&](auto c) {
@@ -1217,6 +1240,95 @@ int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStrea
     return ok();
 }
 
+// Times `launch` (one warm-up, then `repeats` launches between two events on
+// `s`); the mean in *ms.
+template <typename F>
+int time_launches(F&& launch, int repeats, cudaStream_t s, cudaEvent_t e0, cudaEvent_t e1, float* ms) {
+    if (int rc = launch()) return rc;
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < repeats; ++r)
+        if (int rc = launch()) return rc;
+    cudaEventRecord(e1, s);
+    cudaError_t e = cudaEventSynchronize(e1);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(ms, e0, e1);
+    if (e != cudaSuccess) return cuda_fail(e, "tfgMlpAutotune: timing");
+    *ms /= (float)repeats;
+    return check_error_flag();
+}
+
+// The model's autotuner: candidates in turn, the current setting first; a
+// candidate replaces the best only when at least 1% faster.  The gradient
+// buffer, FP8 scale words and device state words are saved before and put
+// back after, so the model continues exactly as before.
+int autotune_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, TfgColor* out, int repeats,
+                  TfgMlpTuning* result, float* ms_out, cudaStream_t s) {
+    if (count && (!in || !out)) return fail(TFG_E_INVALID, "tfgMlpAutotune: null inference buffer");
+    if (count && (reinterpret_cast<uintptr_t>(in) & 15u) != 0)
+        return fail(TFG_E_INVALID, "tfgMlpAutotune: input buffer must be 16-byte aligned");
+    if (count && n->prec == mlp::kPrecF8 && !n->f8_calibrated)
+        return fail(TFG_E_INVALID, "tfgMlpAutotune: FP8 needs tfgMlpCalibrate first");
+    repeats = repeats > 0 ? std::min(repeats, 1000) : 5;
+    const uint32_t tiles = n->batch / mlp::kTile;
+    if (int rc = ensure_acts(n, tiles)) return rc;
+    const size_t gbytes = (size_t)mlp::params_of(n->nl) * sizeof(float);
+    const size_t fbytes = mlp::kF8Words * sizeof(float), sbytes = mlp::S_WORDS * sizeof(uint32_t);
+    uint8_t* saved = nullptr;
+    cudaError_t e = cudaMalloc((void**)&saved, gbytes + fbytes + sbytes);
+    if (e != cudaSuccess) return cuda_fail(e, "tfgMlpAutotune");
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    e = cudaEventCreate(&e0);
+    if (e == cudaSuccess) e = cudaEventCreate(&e1);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(saved, n->grad, gbytes, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(saved + gbytes, n->f8, fbytes, cudaMemcpyDeviceToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(saved + gbytes + fbytes, n->dstate, sbytes, cudaMemcpyDeviceToDevice, s);
+    int rc = e == cudaSuccess ? 0 : cuda_fail(e, "tfgMlpAutotune: save state");
+    const TfgMlpTuning before = n->tune;
+    TfgMlpTuning best = n->tune;
+    float best_wg = 0.0f, best_inf = 0.0f;
+    // Weight gradients of one batch; the record count is set so the kernel runs.
+    if (!rc) rc = set_word(n, mlp::S_NAVAIL, n->batch, s);
+    if (!rc) {
+        std::vector<uint32_t> cands{wgrad_tiles_per_cta(n, tiles)};
+        for (uint32_t t = 1; t <= 64 && t <= tiles; t *= 2)
+            if (t != cands[0]) cands.push_back(t);
+        for (size_t i = 0; i < cands.size() && !rc; ++i) {
+            float ms = 0.0f;
+            rc = time_launches([&] { return enqueue_wgrad(n, cands[i], 0, s); }, repeats, s, e0, e1, &ms);
+            if (!rc && (i == 0 || ms < 0.99f * best_wg)) { best_wg = ms; best.wgrad_tiles_per_cta = (int32_t)cands[i]; }
+        }
+    }
+    // Inference of the caller's batch.
+    if (!rc && count) {
+        const int sms = n->sms;
+        std::vector<int> cands{n->tune.infer_ctas > 0 ? std::min(n->tune.infer_ctas, sms) : sms};
+        for (int c : {sms, 3 * sms / 4, sms / 2})
+            if (c > 0 && c != cands[0]) cands.push_back(c);
+        for (size_t i = 0; i < cands.size() && !rc; ++i) {
+            n->tune.infer_ctas = cands[i];
+            float ms = 0.0f;
+            rc = time_launches([&] { return infer_impl(n, in, out, nullptr, nullptr, count, nullptr, s); }, repeats, s,
+                               e0, e1, &ms);
+            if (!rc && (i == 0 || ms < 0.99f * best_inf)) { best_inf = ms; best.infer_ctas = cands[i]; }
+        }
+    }
+    // Put the model back as it was.
+    cudaError_t r = cudaMemcpyAsync(n->grad, saved, gbytes, cudaMemcpyDeviceToDevice, s);
+    if (r == cudaSuccess) r = cudaMemcpyAsync(n->f8, saved + gbytes, fbytes, cudaMemcpyDeviceToDevice, s);
+    if (r == cudaSuccess) r = cudaMemcpyAsync(n->dstate, saved + gbytes + fbytes, sbytes, cudaMemcpyDeviceToDevice, s);
+    if (r == cudaSuccess) r = cudaStreamSynchronize(s);
+    cudaFree(saved);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    if (rc) { n->tune = before; return rc; }
+    if (r != cudaSuccess) { n->tune = before; return cuda_fail(r, "tfgMlpAutotune: restore state"); }
+    if (best.infer_ctas == n->sms) best.infer_ctas = 0;
+    n->tune = best;
+    ++n->tune_generation;
+    if (result) *result = best;
+    if (ms_out) { ms_out[0] = best_wg; ms_out[1] = best_inf; }
+    return ok();
+}
+
 }  // namespace
 
 // ------------------------------------------------------------------ internal API (frame driver)
@@ -1233,6 +1345,7 @@ int mlp_enqueue_train(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, cudaS
 }
 void mlp_set_gate_threshold(ColorMlp* n, float g) { n->gate = g; }
 int mlp_precision(const ColorMlp* n) { return n->prec; }
+uint32_t mlp_tuning_generation(const ColorMlp* n) { return n->tune_generation; }
 
 }  // namespace tfg
 
@@ -1376,6 +1489,32 @@ extern "C" int tfgMlpSetPrecision(TfgColorMLP* h, int32_t precision) {
         return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: unknown precision");
     n->prec = precision;
     return tfg::ok();
+}
+
+extern "C" int tfgMlpTuningSet(TfgColorMLP* h, const TfgMlpTuning* t) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !t) return tfg::fail(TFG_E_INVALID, "tfgMlpTuningSet: null argument");
+    if (t->wgrad_tiles_per_cta < 0 || t->wgrad_tiles_per_cta > 4096)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpTuningSet: wgrad_tiles_per_cta must be in [0, 4096]");
+    if (t->infer_ctas < 0 || t->infer_ctas > 4096)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpTuningSet: infer_ctas must be in [0, 4096]");
+    n->tune = *t;
+    ++n->tune_generation;
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpTuningGet(TfgColorMLP* h, TfgMlpTuning* out) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !out) return tfg::fail(TFG_E_INVALID, "tfgMlpTuningGet: null argument");
+    *out = n->tune;
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpAutotune(TfgColorMLP* h, const TfgDatosMLP* in, uint32_t count, TfgColor* out, int32_t repeats,
+                              TfgMlpTuning* result, float* ms_out, void* stream) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n) return tfg::fail(TFG_E_INVALID, "tfgMlpAutotune: null model");
+    return tfg::autotune_impl(n, in, count, out, repeats, result, ms_out, (cudaStream_t)stream);
 }
 
 extern "C" int tfgMlpCalibrate(TfgColorMLP* h, const TfgDatosMLP* in, uint32_t count, void* stream) {

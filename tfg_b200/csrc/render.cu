@@ -20,6 +20,7 @@
 
 #include <algorithm>
 #include <cstdio>
+#include <cstring>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -42,7 +43,6 @@ enum : uint32_t {
 };
 
 constexpr uint32_t kMissId = 0xFFFFFFFFu;
-constexpr int kRefillMin = 8;   // idle lanes that trigger a warp's refill (4..24 measured; 8 best)
 
 // Traversal work totals for TFG_PROFILE_COUNTS: rays, nodes, triangle tests
 // for closest-hit rays, then the same for shadow rays.
@@ -74,6 +74,7 @@ struct Workspace {
     float4* nrc = nullptr;                  // a_suffix, a_prefix
     float4* ts = nullptr;                   // training scratch, 10 float4 per path
     uint32_t* counters = nullptr;           // per bounce: rays, fetch, shadows, spare
+    uint32_t generation = 0;                // changes whenever a buffer is reallocated
 };
 
 struct PassArgs {
@@ -90,11 +91,22 @@ struct PassArgs {
     TfgDatosMLP* infer; TfgColor* thr_out;
     int use_inf, train;
     int max_depth, rr_min_depth, shadow_mesh;
+    // The call's paths are `spp` samples of every pixel, numbered sample-major
+    // (path q = sample * npix + pixel).  A wavefront runs `nq` consecutive
+    // paths starting at pixel p0 of sample s0; its per-path state is indexed
+    // by the path's slot in the wavefront (0 .. nq-1).
+    uint32_t npix, nq, p0;
+    int s0, last_sample;      // samples relative to `frame`; the last one writes `img`
+    int refill_min;           // idle lanes that trigger a traversal warp's refill
+    int shadow_one_lane;      // 1: one lane traces all lights of a shading point
     Workspace ws;
 };
 
 // ------------------------------------------------------------------ helpers
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+// Pixel of the path in wavefront slot `slot`.
+__device__ __forceinline__ uint32_t pixel_of(const PassArgs& a, uint32_t slot) { return (a.p0 + slot) % a.npix; }
 
 // Warp-aggregated queue append: every lane with `want` gets a unique slot.
 __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
@@ -154,13 +166,14 @@ __device__ __forceinline__ int use_inf_of(const PassArgs& a) {
 }
 
 __global__ void k_generate(PassArgs a) {
-    const uint32_t N = (uint32_t)a.W * (uint32_t)a.H;
+    const uint32_t N = a.npix;
     const TfgCamara cam = *a.cam;
-    const int frame = a.frame + (a.frame_dev ? *a.frame_dev : 0);
+    const int frame0 = a.frame + a.s0 + (a.frame_dev ? *a.frame_dev : 0);
     const int use_inf = use_inf_of(a);
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
-        const int x = (int)(p % (uint32_t)a.W), y = (int)(p / (uint32_t)a.W);
-        uint32_t rng = seed_pixel(x, y, frame);
+    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.nq; p += gridDim.x * blockDim.x) {
+        const uint32_t q = a.p0 + p, s = q / N, pix = q - s * N;
+        const int x = (int)(pix % (uint32_t)a.W), y = (int)(pix / (uint32_t)a.W);
+        uint32_t rng = seed_pixel(x, y, frame0 + (int)s);
         const float ox = pcg_uniform(rng);
         const float oy = pcg_uniform(rng);
         V3 O, D;
@@ -181,12 +194,12 @@ __global__ void k_generate(PassArgs a) {
             a.ws.nrc[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         }
     }
-    if (blockIdx.x == 0 && threadIdx.x == 0) a.ws.counters[0] = N;
+    if (blockIdx.x == 0 && threadIdx.x == 0) a.ws.counters[0] = a.nq;
 }
 
 // ------------------------------------------------------------------ trace
 template <int TRI_FMT, bool STATS>
-__global__ void __launch_bounds__(128) k_trace(PassArgs a, int bounce) {
+__global__ void __launch_bounds__(256) k_trace(PassArgs a, int bounce) {
     extern __shared__ unsigned char smem_raw[];
     uint2* sstack = reinterpret_cast<uint2*>(smem_raw);
     APrim* sprims = reinterpret_cast<APrim*>(smem_raw + sizeof(uint2) * kSmemStack * blockDim.x);
@@ -199,7 +212,7 @@ __global__ void __launch_bounds__(128) k_trace(PassArgs a, int bounce) {
     TravCounts cnt;
     uint32_t nrays = 0;
     // Persistent lanes: a lane whose ray is done takes a new one as soon as
-    // kRefillMin lanes of its warp are idle, instead of waiting for the
+    // a.refill_min lanes of its warp are idle, instead of waiting for the
     // slowest ray of a 32-ray batch.
     const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
     CwbvhRay<TRI_FMT, false> r;
@@ -211,7 +224,7 @@ __global__ void __launch_bounds__(128) k_trace(PassArgs a, int bounce) {
         const uint32_t im = __ballot_sync(0xFFFFFFFFu, idle);
         if (exhausted) {
             if (im == 0xFFFFFFFFu) break;
-        } else if (__popc(im) >= kRefillMin) {
+        } else if (__popc(im) >= a.refill_min) {
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(im));
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
@@ -358,9 +371,10 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
                         refl = v3(fmaxf(refl.x, 1e-3f), fmaxf(refl.y, 1e-3f), fmaxf(refl.z, 1e-3f));
                         const bool training = (flags & F_TRAIN) != 0;
                         if (!training && use_inf) {
-                            write_datos(&a.infer[p], P, map01(view), map01(nrm), m.difuso, m.especular);
+                            const uint32_t px = pixel_of(a, p);
+                            write_datos(&a.infer[px], P, map01(view), map01(nrm), m.difuso, m.especular);
                             const V3 tt = mul(cam, refl);
-                            a.thr_out[p] = TfgColor{tt.x, tt.y, tt.z};
+                            a.thr_out[px] = TfgColor{tt.x, tt.y, tt.z};
                             flags |= F_INF;
                             end = true;
                         } else if (training && !captured) {
@@ -445,7 +459,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
 // falloff with the distance clamped to >= 1, summed then scaled by the path
 // throughput (render.h:128-130).
 template <int TRI_FMT, bool STATS>
-__global__ void __launch_bounds__(128) k_shadow(PassArgs a, int bounce) {
+__global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce) {
     extern __shared__ unsigned char smem_raw[];
     uint2* sstack = reinterpret_cast<uint2*>(smem_raw);
     APrim* sprims = reinterpret_cast<APrim*>(smem_raw + sizeof(uint2) * kSmemStack * blockDim.x);
@@ -457,10 +471,12 @@ __global__ void __launch_bounds__(128) k_shadow(PassArgs a, int bounce) {
     TravCounts cnt;
     uint32_t nrays = 0;
     // One shadow ray per lane: the lights of an item sit on G adjacent lanes
-    // (G = light count rounded up to a power of two; more than 32 lights fall
-    // back to one lane looping over them), and warps fetch items dynamically.
+    // (G = light count rounded up to a power of two; more than 32 lights, or
+    // a.shadow_one_lane, give one lane looping over them), and warps fetch
+    // items dynamically.
     const int nl = a.nlights;
-    const uint32_t G = nl <= 1 ? 1u : nl <= 2 ? 2u : nl <= 4 ? 4u : nl <= 8 ? 8u : nl <= 16 ? 16u : nl <= 32 ? 32u : 1u;
+    const uint32_t G = a.shadow_one_lane ? 1u
+                       : nl <= 1 ? 1u : nl <= 2 ? 2u : nl <= 4 ? 4u : nl <= 8 ? 8u : nl <= 16 ? 16u : nl <= 32 ? 32u : 1u;
     const uint32_t lane = lane_id(), lg = lane & (G - 1u), group0 = lane & ~(G - 1u);
     const int l_begin = G == 1u ? 0 : (int)lg;
     const int l_end = G == 1u ? nl : min(nl, (int)lg + 1);
@@ -501,7 +517,11 @@ __global__ void __launch_bounds__(128) k_shadow(PassArgs a, int bounce) {
                 dist = fmaxf(dist, 1.0f);
                 const float d2 = dist * dist;
                 const V3 Li = v3(lz.intensidad.r / d2, lz.intensidad.g / d2, lz.intensidad.b / d2);
-                L = L + mul(Li, kdpi) * c;
+                // Each light's term is rounded before it is added (no fused
+                // multiply-add), so one lane looping over the lights sums the
+                // same values in the same order as the lanes of a group.
+                const V3 term = mul(Li, kdpi) * c;
+                L = v3(__fadd_rn(L.x, term.x), __fadd_rn(L.y, term.y), __fadd_rn(L.z, term.z));
             }
         }
         // Sum the group's lights in light order on its first lane (an occluded
@@ -533,45 +553,55 @@ __device__ __forceinline__ void get_geo(const float4* src, TfgDatosGeometricos& 
     g.especular = TfgColor{a3.x, a3.y, a3.z};
 }
 
+// One thread per pixel of the wavefront: slots j, j + npix, j + 2 npix ...
+// hold that pixel's samples in order, so the accumulation adds them in sample
+// order whatever the wavefront size.
 __global__ void k_resolve(PassArgs a) {
-    const uint32_t N = (uint32_t)a.W * (uint32_t)a.H;
+    const uint32_t N = a.npix;
     const bool nrc = a.use_inf || a.train;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
-        const float4 lp = a.ws.lpre[p];
-        if (a.img) a.img[p] = TfgColor{lp.x, lp.y, lp.z};
-        if (a.accum) { a.accum[3 * (size_t)p] += lp.x; a.accum[3 * (size_t)p + 1] += lp.y; a.accum[3 * (size_t)p + 2] += lp.z; }
-        const uint32_t flags = a.ws.st[p].y;
-        const bool rec = nrc && (flags & F_TRAIN) && (flags & F_CAPTURED);
-        if (a.thr_out && !(flags & F_INF) && !rec) a.thr_out[p] = TfgColor{0.0f, 0.0f, 0.0f};
-        if (!rec) continue;
-        // Training path with a head vertex: its pixel keeps the prefix radiance and
-        // asks the cache at the head (render.h:243-260); the record goes to the ring
-        // (render.h:461-464).
-        const float4* ts = &a.ws.ts[10 * (size_t)p];
-        TfgDatosGeometricos head, tail;
-        get_geo(ts, head);
-        const float4 thr_train = ts[8];
-        if (a.infer) {
-            TfgDatosMLP d;
-            d.posicion = head.posicion; d.direccion = head.direccion; d.normal = head.normal;
-            d.difuso = head.difuso; d.especular = head.especular; d.color = TfgColor{0.0f, 0.0f, 0.0f};
-            a.infer[p] = d;
-        }
-        if (a.thr_out) a.thr_out[p] = TfgColor{thr_train.x, thr_train.y, thr_train.z};
-        if (a.reg_counter && a.regs && a.reg_cap > 0) {
-            TfgRegistroEntrenamiento r;
-            r.head = head;
-            float4 thr_suf = make_float4(0, 0, 0, 0);
-            if (flags & F_TAIL) { get_geo(ts + 4, tail); thr_suf = ts[9]; }
-            else { memset(&tail, 0, sizeof(tail)); }
-            r.tail = tail;
-            const float4 ls = a.ws.lsuf[p];
-            r.luz_acumulada_sufijo = TfgColor{ls.x, ls.y, ls.z};
-            r.throughput_sufijo = TfgColor{thr_suf.x, thr_suf.y, thr_suf.z};
-            r.factor_normalizacion = TfgColor{thr_train.x, thr_train.y, thr_train.z};
-            r.valido = 1;
-            const uint32_t idx = atomicAdd(a.reg_counter, 1u);
-            a.regs[idx % (uint32_t)a.reg_cap] = r;
+    const uint32_t first = min(a.nq, N);
+    for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < first; j += gridDim.x * blockDim.x) {
+        const uint32_t q = a.p0 + j, s_rel = q / N, px = q - s_rel * N;
+        int sample = a.s0 + (int)s_rel;
+        for (uint32_t p = j; p < a.nq; p += N, ++sample) {
+            const float4 lp = a.ws.lpre[p];
+            if (a.img && sample == a.last_sample) a.img[px] = TfgColor{lp.x, lp.y, lp.z};
+            if (a.accum) {
+                a.accum[3 * (size_t)px] += lp.x; a.accum[3 * (size_t)px + 1] += lp.y; a.accum[3 * (size_t)px + 2] += lp.z;
+            }
+            const uint32_t flags = a.ws.st[p].y;
+            const bool rec = nrc && (flags & F_TRAIN) && (flags & F_CAPTURED);
+            if (a.thr_out && !(flags & F_INF) && !rec) a.thr_out[px] = TfgColor{0.0f, 0.0f, 0.0f};
+            if (!rec) continue;
+            // Training path with a head vertex: its pixel keeps the prefix radiance and
+            // asks the cache at the head (render.h:243-260); the record goes to the ring
+            // (render.h:461-464).
+            const float4* ts = &a.ws.ts[10 * (size_t)p];
+            TfgDatosGeometricos head, tail;
+            get_geo(ts, head);
+            const float4 thr_train = ts[8];
+            if (a.infer) {
+                TfgDatosMLP d;
+                d.posicion = head.posicion; d.direccion = head.direccion; d.normal = head.normal;
+                d.difuso = head.difuso; d.especular = head.especular; d.color = TfgColor{0.0f, 0.0f, 0.0f};
+                a.infer[px] = d;
+            }
+            if (a.thr_out) a.thr_out[px] = TfgColor{thr_train.x, thr_train.y, thr_train.z};
+            if (a.reg_counter && a.regs && a.reg_cap > 0) {
+                TfgRegistroEntrenamiento r;
+                r.head = head;
+                float4 thr_suf = make_float4(0, 0, 0, 0);
+                if (flags & F_TAIL) { get_geo(ts + 4, tail); thr_suf = ts[9]; }
+                else { memset(&tail, 0, sizeof(tail)); }
+                r.tail = tail;
+                const float4 ls = a.ws.lsuf[p];
+                r.luz_acumulada_sufijo = TfgColor{ls.x, ls.y, ls.z};
+                r.throughput_sufijo = TfgColor{thr_suf.x, thr_suf.y, thr_suf.z};
+                r.factor_normalizacion = TfgColor{thr_train.x, thr_train.y, thr_train.z};
+                r.valido = 1;
+                const uint32_t idx = atomicAdd(a.reg_counter, 1u);
+                a.regs[idx % (uint32_t)a.reg_cap] = r;
+            }
         }
     }
 }
@@ -606,11 +636,13 @@ int ensure_workspace(int dev, int slot, size_t paths, bool nrc, Workspace& out) 
         if (e == cudaSuccess) e = grow((void**)&w.lsuf, cap * sizeof(float4));
         if (e == cudaSuccess) e = grow((void**)&w.nrc, cap * sizeof(float4));
         if (e == cudaSuccess && !w.counters) e = cudaMalloc((void**)&w.counters, 4 * (kMaxBounces + 1) * sizeof(uint32_t));
+        ++w.generation;
         if (e != cudaSuccess) { w.cap = 0; return fail((int)e, std::string("render workspace: ") + cudaGetErrorString(e)); }
         w.cap = cap;
     }
     if (nrc && w.train_cap < paths) {
         e = grow((void**)&w.ts, paths * 10 * sizeof(float4));
+        ++w.generation;
         if (e != cudaSuccess) { w.train_cap = 0; return fail((int)e, std::string("training scratch: ") + cudaGetErrorString(e)); }
         w.train_cap = paths;
     }
@@ -618,16 +650,36 @@ int ensure_workspace(int dev, int slot, size_t paths, bool nrc, Workspace& out) 
     return 0;
 }
 
+// Launch tuning of each device (tfgRenderTuningSet / tfgRenderAutotune).
+// Every setting computes the same image; the generation number changes with
+// every set, so captured frame graphs know when to re-capture.
+std::mutex g_tune_mutex;
+TfgRenderTuning g_tune[16];
+bool g_tune_valid[16] = {false};
+uint32_t g_tune_generation = 1;
+
+constexpr int kThreadChoices[3] = {64, 128, 256};
+int threads_index(int t) { return t == 64 ? 0 : t == 256 ? 2 : 1; }
+
+}  // namespace
+
+uint32_t workspace_generation(int dev, int slot) {
+    std::lock_guard<std::mutex> lk(g_ws_mutex);
+    return g_ws[dev & 15][slot & (kWorkspaceSlots - 1)].generation;
+}
+
+namespace {
+
 struct LaunchShapes {
     int sms = 0;
-    int trace_blocks[2] = {0, 0};
-    int shadow_blocks[2] = {0, 0};
+    int trace_occ[2][3] = {};    // resident CTAs per SM: [triangle format][64, 128, 256 threads]
+    int shadow_occ[2][3] = {};
     int shade_blocks = 0;
 };
 LaunchShapes g_shapes[16];
 
-size_t trace_smem(int nprims) {
-    return sizeof(uint2) * kSmemStack * 128 + sizeof(APrim) * (size_t)std::min(nprims, kSmemPrims);
+size_t trace_smem(int nprims, int threads) {
+    return sizeof(uint2) * kSmemStack * (size_t)threads + sizeof(APrim) * (size_t)std::min(nprims, kSmemPrims);
 }
 
 int shapes_for(int dev, LaunchShapes& s) {
@@ -635,16 +687,20 @@ int shapes_for(int dev, LaunchShapes& s) {
     if (g.sms == 0) {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        for (int k = 0; k < 3; ++k) {
+            const int bt = kThreadChoices[k];
+            const size_t sm = trace_smem(kSmemPrims, bt);
+            int occ = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<0, false>, bt, sm);
+            g.trace_occ[0][k] = std::max(occ, 1);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<1, false>, bt, sm);
+            g.trace_occ[1][k] = std::max(occ, 1);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<0, false>, bt, sm);
+            g.shadow_occ[0][k] = std::max(occ, 1);
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<1, false>, bt, sm);
+            g.shadow_occ[1][k] = std::max(occ, 1);
+        }
         int occ = 0;
-        size_t sm = trace_smem(kSmemPrims);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<0, false>, 128, sm);
-        g.trace_blocks[0] = sms * std::max(occ, 1);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<1, false>, 128, sm);
-        g.trace_blocks[1] = sms * std::max(occ, 1);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<0, false>, 128, sm);
-        g.shadow_blocks[0] = sms * std::max(occ, 1);
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<1, false>, 128, sm);
-        g.shadow_blocks[1] = sms * std::max(occ, 1);
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade, 256, 0);
         g.shade_blocks = sms * std::max(occ, 1);
         g.sms = sms;
@@ -652,6 +708,78 @@ int shapes_for(int dev, LaunchShapes& s) {
     s = g;
     return 0;
 }
+
+// A device's tuning resolved for one call: the wavefront in paths, capped by
+// the call's path count (and by one sample of the image for cache passes,
+// whose per-pixel outputs take one sample per pixel at a time).
+struct Tuning {
+    uint32_t wavefront = 0;
+    int threads = 128, warps_per_sm = 0, refill = 8, shadow_one_lane = 0;
+};
+
+Tuning resolve_tuning(int dev, uint32_t npix, int spp, bool nrc, uint32_t* generation) {
+    TfgRenderTuning t;
+    {
+        std::lock_guard<std::mutex> lk(g_tune_mutex);
+        if (g_tune_valid[dev & 15]) t = g_tune[dev & 15];
+        else tfgRenderTuningDefault(&t);
+        if (generation) *generation = g_tune_generation;
+    }
+    Tuning r;
+    uint64_t wf = t.wavefront_paths > 0 ? (uint64_t)t.wavefront_paths : npix;
+    if (nrc) wf = std::min<uint64_t>(wf, npix);
+    wf = std::min<uint64_t>(wf, (uint64_t)spp * npix);
+    r.wavefront = (uint32_t)std::max<uint64_t>(wf, 1);
+    r.threads = t.trace_threads;
+    r.warps_per_sm = t.trace_warps_per_sm;
+    r.refill = t.refill_min;
+    r.shadow_one_lane = t.shadow_one_lane;
+    return r;
+}
+
+// Persistent traversal grid: every SM holds as many CTAs as fit, or the
+// tuned number of warps.
+int persistent_grid(const LaunchShapes& sh, int occ, const Tuning& t) {
+    int per_sm = occ;
+    if (t.warps_per_sm > 0) per_sm = std::max(1, std::min(occ, t.warps_per_sm * 32 / t.threads));
+    return sh.sms * per_sm;
+}
+
+}  // namespace
+
+int render_tuning_check(const TfgRenderTuning& t) {
+    if (t.wavefront_paths != 0 && (t.wavefront_paths < 1024 || t.wavefront_paths > (1 << 26)))
+        return fail(TFG_E_INVALID, "render tuning: wavefront_paths must be 0 or in [1024, 2^26]");
+    if (t.trace_threads != 64 && t.trace_threads != 128 && t.trace_threads != 256)
+        return fail(TFG_E_INVALID, "render tuning: trace_threads must be 64, 128 or 256");
+    if (t.trace_warps_per_sm < 0 || t.trace_warps_per_sm > 64)
+        return fail(TFG_E_INVALID, "render tuning: trace_warps_per_sm must be in [0, 64]");
+    if (t.refill_min < 1 || t.refill_min > 32) return fail(TFG_E_INVALID, "render tuning: refill_min must be in [1, 32]");
+    if (t.shadow_one_lane != 0 && t.shadow_one_lane != 1)
+        return fail(TFG_E_INVALID, "render tuning: shadow_one_lane must be 0 or 1");
+    return ok();
+}
+
+int render_tuning_set(int dev, const TfgRenderTuning& t) {
+    if (int rc = render_tuning_check(t)) return rc;
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    g_tune[dev & 15] = t;
+    g_tune_valid[dev & 15] = true;
+    ++g_tune_generation;
+    return ok();
+}
+
+int render_tuning_get(int dev, TfgRenderTuning* out, uint32_t* generation) {
+    std::lock_guard<std::mutex> lk(g_tune_mutex);
+    if (out) {
+        if (g_tune_valid[dev & 15]) *out = g_tune[dev & 15];
+        else tfgRenderTuningDefault(out);
+    }
+    if (generation) *generation = g_tune_generation;
+    return ok();
+}
+
+namespace {
 
 // Stage timing with CUDA events (TFG_PROFILE_TIMES): one start/stop pair per
 // launch, summed by tfgRenderProfileGet.
@@ -713,7 +841,7 @@ int profile_get(TfgRenderProfile* out) {
 }
 
 int enqueue_pass(PassArgs a, const TfgRenderParams& prm, int frame, TfgColor* img, const LaunchShapes& sh,
-                 cudaStream_t stream);
+                 const Tuning& tu, cudaStream_t stream);
 
 int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
                 const TfgLuzPuntual* lights, int nlights, int W, int H, int frame, const TfgTinyBVHD_GPU* bvh,
@@ -749,8 +877,9 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     if (int rc = require_sm100(dev)) return rc;
+    const Tuning tu = resolve_tuning(dev, (uint32_t)W * (uint32_t)H, prm.spp, nrc, nullptr);
     Workspace ws;
-    if (int rc = ensure_workspace(dev, ws_slot, (size_t)W * H, nrc, ws)) return rc;
+    if (int rc = ensure_workspace(dev, ws_slot, tu.wavefront, nrc, ws)) return rc;
     LaunchShapes sh;
     shapes_for(dev, sh);
     if (prepare_only) return ok();
@@ -770,19 +899,23 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
     a.infer = infer; a.thr_out = thr_out; a.use_inf = use_inf; a.train = train;
     a.max_depth = prm.max_depth; a.rr_min_depth = prm.rr_min_depth; a.shadow_mesh = prm.shadow_mesh;
     a.ws = ws;
-    return enqueue_pass(a, prm, frame, img, sh, stream);
+    return enqueue_pass(a, prm, frame, img, sh, tu, stream);
 }
 
-// The launch sequence of one call: `prm.spp` samples, each generate ->
-// (trace -> shade -> shadow) x max_depth -> resolve, on the workspace in `a.ws`.
+// The launch sequence of one call: its spp x W x H paths in wavefronts of
+// `tu.wavefront` paths, each generate -> (trace -> shade -> shadow) x
+// max_depth -> resolve, on the workspace in `a.ws`.
 int enqueue_pass(PassArgs a, const TfgRenderParams& prm, int frame, TfgColor* img, const LaunchShapes& sh,
-                 cudaStream_t stream) {
-    const int W = a.W, H = a.H;
+                 const Tuning& tu, cudaStream_t stream) {
+    const uint32_t N = (uint32_t)a.W * (uint32_t)a.H;
     const int fmt = prm.tri_format;
-    const size_t smem = trace_smem(a.nprims);
+    const int ti = threads_index(tu.threads);
+    const int bt = kThreadChoices[ti];
+    const size_t smem = trace_smem(a.nprims, bt);
+    const int trace_grid = persistent_grid(sh, sh.trace_occ[fmt][ti], tu);
+    const int shadow_grid = persistent_grid(sh, sh.shadow_occ[fmt][ti], tu);
     const Workspace& ws = a.ws;
     cudaError_t e = cudaSuccess;
-    const int gen_blocks = std::max(1, std::min((W * H + 255) / 256, sh.sms * 8));
     const bool times = (prm.profile & TFG_PROFILE_TIMES) != 0;
     const bool counts = (prm.profile & TFG_PROFILE_COUNTS) != 0;
     auto stage = [&](int id, auto&& launch) {
@@ -795,34 +928,45 @@ int enqueue_pass(PassArgs a, const TfgRenderParams& prm, int frame, TfgColor* im
             launch();
         }
     };
-    for (int s = 0; s < prm.spp; ++s) {
-        a.frame = frame + s;
-        a.img = (s == prm.spp - 1) ? img : nullptr;
+    a.frame = frame;
+    a.img = img;
+    a.npix = N;
+    a.last_sample = prm.spp - 1;
+    a.refill_min = tu.refill;
+    a.shadow_one_lane = tu.shadow_one_lane;
+    const uint64_t total = (uint64_t)prm.spp * N;
+    for (uint64_t q0 = 0; q0 < total; q0 += tu.wavefront) {
+        a.nq = (uint32_t)std::min<uint64_t>(tu.wavefront, total - q0);
+        a.s0 = (int)(q0 / N);
+        a.p0 = (uint32_t)(q0 % N);
+        const int gen_blocks = (int)std::max<uint32_t>(1u, std::min<uint32_t>((a.nq + 255) / 256, (uint32_t)sh.sms * 8u));
+        const uint32_t resolve_n = std::min(a.nq, N);
+        const int res_blocks = (int)std::max<uint32_t>(1u, std::min<uint32_t>((resolve_n + 255) / 256, (uint32_t)sh.sms * 8u));
         e = cudaMemsetAsync(ws.counters, 0, 4 * (kMaxBounces + 1) * sizeof(uint32_t), stream);
         if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
         stage(0, [&] { k_generate<<<gen_blocks, 256, 0, stream>>>(a); });
         for (int b = 0; b < prm.max_depth; ++b) {
             stage(1, [&] {
                 if (fmt == 0) {
-                    if (counts) k_trace<0, true><<<sh.trace_blocks[0], 128, smem, stream>>>(a, b);
-                    else k_trace<0, false><<<sh.trace_blocks[0], 128, smem, stream>>>(a, b);
+                    if (counts) k_trace<0, true><<<trace_grid, bt, smem, stream>>>(a, b);
+                    else k_trace<0, false><<<trace_grid, bt, smem, stream>>>(a, b);
                 } else {
-                    if (counts) k_trace<1, true><<<sh.trace_blocks[1], 128, smem, stream>>>(a, b);
-                    else k_trace<1, false><<<sh.trace_blocks[1], 128, smem, stream>>>(a, b);
+                    if (counts) k_trace<1, true><<<trace_grid, bt, smem, stream>>>(a, b);
+                    else k_trace<1, false><<<trace_grid, bt, smem, stream>>>(a, b);
                 }
             });
             stage(2, [&] { k_shade<<<sh.shade_blocks, 256, 0, stream>>>(a, b); });
             stage(3, [&] {
                 if (fmt == 0) {
-                    if (counts) k_shadow<0, true><<<sh.shadow_blocks[0], 128, smem, stream>>>(a, b);
-                    else k_shadow<0, false><<<sh.shadow_blocks[0], 128, smem, stream>>>(a, b);
+                    if (counts) k_shadow<0, true><<<shadow_grid, bt, smem, stream>>>(a, b);
+                    else k_shadow<0, false><<<shadow_grid, bt, smem, stream>>>(a, b);
                 } else {
-                    if (counts) k_shadow<1, true><<<sh.shadow_blocks[1], 128, smem, stream>>>(a, b);
-                    else k_shadow<1, false><<<sh.shadow_blocks[1], 128, smem, stream>>>(a, b);
+                    if (counts) k_shadow<1, true><<<shadow_grid, bt, smem, stream>>>(a, b);
+                    else k_shadow<1, false><<<shadow_grid, bt, smem, stream>>>(a, b);
                 }
             });
         }
-        stage(4, [&] { k_resolve<<<gen_blocks, 256, 0, stream>>>(a); });
+        stage(4, [&] { k_resolve<<<res_blocks, 256, 0, stream>>>(a); });
         e = cudaGetLastError();
         if (e != cudaSuccess) return fail((int)e, std::string("render launch: ") + cudaGetErrorString(e));
     }
@@ -902,11 +1046,11 @@ int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const 
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     const float4* tr = reinterpret_cast<const float4*>(fmt == TFG_TRIS_REF ? bvh->d_tris : tris_wt);
     if (fmt == 0)
-        k_trace_rays<0><<<sh.trace_blocks[0], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
+        k_trace_rays<0><<<sh.sms * sh.trace_occ[0][1], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
                                                                  reinterpret_cast<const float4*>(rays), (uint32_t)n,
                                                                  reinterpret_cast<float4*>(hits), fetch);
     else
-        k_trace_rays<1><<<sh.trace_blocks[1], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
+        k_trace_rays<1><<<sh.sms * sh.trace_occ[1][1], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
                                                                  reinterpret_cast<const float4*>(rays), (uint32_t)n,
                                                                  reinterpret_cast<float4*>(hits), fetch);
     e = cudaGetLastError();
@@ -940,6 +1084,32 @@ extern "C" void tfgRenderParamsReference(TfgRenderParams* p) {
     p->accumulate = 0;
     p->profile = 0;
     p->reserved = 0;
+}
+
+extern "C" void tfgRenderTuningDefault(TfgRenderTuning* t) {
+    if (!t) return;
+    std::memset(t, 0, sizeof(*t));
+    t->wavefront_paths = 0;
+    t->trace_threads = 128;
+    t->trace_warps_per_sm = 0;
+    t->refill_min = 8;
+    t->shadow_one_lane = 0;
+}
+
+extern "C" int tfgRenderTuningSet(const TfgRenderTuning* t) {
+    if (!t) return tfg::fail(TFG_E_INVALID, "tfgRenderTuningSet: tuning is null");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return tfg::fail((int)e, cudaGetErrorString(e));
+    return tfg::render_tuning_set(dev, *t);
+}
+
+extern "C" int tfgRenderTuningGet(TfgRenderTuning* out) {
+    if (!out) return tfg::fail(TFG_E_INVALID, "tfgRenderTuningGet: out is null");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return tfg::fail((int)e, cudaGetErrorString(e));
+    return tfg::render_tuning_get(dev, out, nullptr);
 }
 
 extern "C" int tfgRenderProfileReset(void) { return tfg::profile_reset(); }
@@ -1066,6 +1236,8 @@ extern "C" int tfgRenderPassStatic(const TfgRenderParams* params, const TfgCamar
     if (int rc = static_scratch(dev, &base)) return rc;
     LaunchShapes sh;
     shapes_for(dev, sh);
+    Tuning tu = resolve_tuning(dev, (uint32_t)ancho_img * (uint32_t)alto_img, prm.spp, false, nullptr);
+    tu.wavefront = std::min<uint32_t>(tu.wavefront, (uint32_t)kStaticPaths);
     // Carve the scratch: queues first, then per-path state, counters last.
     const size_t P = kStaticPaths;
     Workspace ws;
@@ -1093,6 +1265,6 @@ extern "C" int tfgRenderPassStatic(const TfgRenderParams* params, const TfgCamar
     a.accum = prm.accumulate ? accum : nullptr;
     a.max_depth = prm.max_depth; a.rr_min_depth = prm.rr_min_depth; a.shadow_mesh = prm.shadow_mesh;
     a.ws = ws;
-    return enqueue_pass(a, prm, frame_number, imagen_directa ? imagen_directa->datos : nullptr, sh,
+    return enqueue_pass(a, prm, frame_number, imagen_directa ? imagen_directa->datos : nullptr, sh, tu,
                         (cudaStream_t)stream);
 }

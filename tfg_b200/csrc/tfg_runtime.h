@@ -32,6 +32,16 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
                    uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer, TfgColor* thr_out, int use_inf, int train,
                    bool prepare_only, int ws_slot, cudaStream_t stream);
 
+// Changes whenever the workspace of (dev, slot) is reallocated: a CUDA graph
+// captured before holds stale queue pointers then.
+uint32_t workspace_generation(int dev, int slot);
+
+// Launch tuning of device `dev` (render.cu).  The generation number changes
+// with every successful set.
+int render_tuning_check(const TfgRenderTuning& t);
+int render_tuning_set(int dev, const TfgRenderTuning& t);
+int render_tuning_get(int dev, TfgRenderTuning* out, uint32_t* generation);
+
 int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const float* rays, int n, float* hits,
                cudaStream_t stream);
 
@@ -55,5 +65,6 @@ int mlp_enqueue_infer(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColo
 int mlp_enqueue_train(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, cudaStream_t s);
 void mlp_set_gate_threshold(ColorMlp* n, float g);
 int mlp_precision(const ColorMlp* n);   // inference precision (part of a frame graph's identity)
+uint32_t mlp_tuning_generation(const ColorMlp* n);   // changes with every tuning set
 
 }  // namespace tfg

@@ -8,7 +8,7 @@ import numpy as np
 import torch
 
 from . import _lib
-from .structs import BOUNDS, DATOS_MLP, REGISTRO, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame
+from .structs import BOUNDS, DATOS_MLP, REGISTRO, CMlpTuning, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame
 
 def layer_shapes(hidden_layers: int = 5) -> list[tuple[int, int]]:
     """Padded [out][in] shapes of the weight matrices, in parameter order."""
@@ -90,6 +90,30 @@ class ColorMLP:
     def calibrate(self, datos: torch.Tensor, n: int, stream=None) -> None:
         """FP8 input scales from the per-layer amax of n samples."""
         _lib.call("tfgMlpCalibrate", self.h, datos.data_ptr(), n, _stream(stream))
+
+    def set_tuning(self, wgrad_tiles_per_cta: int = 0, infer_ctas: int = 0) -> None:
+        """Batch tiling of the model's kernels (0 = default)."""
+        t = CMlpTuning()
+        t.wgrad_tiles_per_cta, t.infer_ctas = wgrad_tiles_per_cta, infer_ctas
+        _lib.call("tfgMlpTuningSet", self.h, ctypes.byref(t))
+
+    def get_tuning(self) -> dict:
+        t = CMlpTuning()
+        _lib.call("tfgMlpTuningGet", self.h, ctypes.byref(t))
+        return {"wgrad_tiles_per_cta": int(t.wgrad_tiles_per_cta), "infer_ctas": int(t.infer_ctas)}
+
+    def autotune(self, datos: torch.Tensor | None = None, out: torch.Tensor | None = None, n: int = 0,
+                 repeats: int = 5, stream=None) -> dict:
+        """tfgMlpAutotune: weight-gradient tiles per CTA of one training batch
+        and inference CTAs over `n` samples of `datos` (skipped when n = 0).
+        The model state is left as it was; the winners are set and returned
+        with their times."""
+        t = CMlpTuning()
+        ms = (ctypes.c_float * 2)()
+        _lib.call("tfgMlpAutotune", self.h, datos.data_ptr() if datos is not None else None, int(n),
+                  out.data_ptr() if out is not None else None, repeats, ctypes.byref(t), ms, _stream(stream))
+        return {"wgrad_tiles_per_cta": int(t.wgrad_tiles_per_cta), "infer_ctas": int(t.infer_ctas),
+                "wgrad_ms": float(ms[0]), "infer_ms": float(ms[1])}
 
     def inference_composite(self, datos: torch.Tensor, thr: torch.Tensor, img: torch.Tensor, n: int,
                             stream=None) -> None:

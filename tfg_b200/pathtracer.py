@@ -16,7 +16,8 @@ import torch
 
 from . import _lib
 from .scenes import Scene
-from .structs import CImagenGPU, CRenderParams, CRenderProfile, CTinyBVH, CTinyBVHD_GPU, DATOS_MLP, REGISTRO
+from .structs import (CImagenGPU, CRenderParams, CRenderProfile, CRenderTuning, CTinyBVH, CTinyBVHD_GPU,
+                      CTuneRecord, DATOS_MLP, REGISTRO)
 
 TRIS_REF, TRIS_WATERTIGHT = 0, 1
 PROFILE_TIMES, PROFILE_COUNTS = 1, 2
@@ -215,3 +216,57 @@ def profile_get() -> dict:
         "shadow_rays": int(p.shadow_rays), "shadow_nodes": int(p.shadow_nodes),
         "shadow_tri_tests": int(p.shadow_tri_tests),
     }
+
+
+@dataclass
+class RenderTuning:
+    """TfgRenderTuning: how the wavefront stages are sized and launched on the
+    current device.  Every setting renders the same image."""
+    wavefront_paths: int = 0      # queue capacity in paths; 0 = one sample of the image (W*H)
+    trace_threads: int = 128      # threads per traversal / shadow CTA: 64, 128, 256
+    trace_warps_per_sm: int = 0   # resident traversal warps per SM; 0 = as many as fit
+    refill_min: int = 8           # idle lanes that make a traversal warp fetch new rays
+    shadow_one_lane: int = 0      # 1: one lane traces all lights of a shading point
+
+    def c(self) -> CRenderTuning:
+        t = CRenderTuning()
+        t.wavefront_paths, t.trace_threads, t.trace_warps_per_sm = (self.wavefront_paths, self.trace_threads,
+                                                                    self.trace_warps_per_sm)
+        t.refill_min, t.shadow_one_lane = self.refill_min, self.shadow_one_lane
+        return t
+
+    @staticmethod
+    def of(t: CRenderTuning) -> "RenderTuning":
+        return RenderTuning(int(t.wavefront_paths), int(t.trace_threads), int(t.trace_warps_per_sm),
+                            int(t.refill_min), int(t.shadow_one_lane))
+
+    @staticmethod
+    def default() -> "RenderTuning":
+        t = CRenderTuning()
+        _lib.lib.tfgRenderTuningDefault(ctypes.byref(t))
+        return RenderTuning.of(t)
+
+
+def set_tuning(t: RenderTuning) -> None:
+    _lib.call("tfgRenderTuningSet", ctypes.byref(t.c()))
+
+
+def get_tuning() -> RenderTuning:
+    t = CRenderTuning()
+    _lib.call("tfgRenderTuningGet", ctypes.byref(t))
+    return RenderTuning.of(t)
+
+
+def autotune(ds: DeviceScene, params: RenderParams, repeats: int = 3, max_records: int = 64,
+             stream=None) -> tuple[RenderTuning, list[tuple[RenderTuning, float]]]:
+    """tfgRenderAutotune on this scene: sets and returns the fastest tuning and
+    every candidate timed, as (tuning, ms per pass) in the order timed."""
+    W, H = ds.scene.width, ds.scene.height
+    out = CRenderTuning()
+    recs = (CTuneRecord * max_records)()
+    n = ctypes.c_int32(0)
+    _lib.call("tfgRenderAutotune", ctypes.byref(params.c()), _ptr(ds.camera), _ptr(ds.prims), ds.n_prims,
+              _ptr(ds.lights), ds.n_lights, W, H, ctypes.byref(ds.bvh.ref), ds.bvh.d_tris_wt, ds.bvh.d_primitivas,
+              ds.n_mesh, repeats, ctypes.byref(out), recs, max_records, ctypes.byref(n), _stream(stream))
+    table = [(RenderTuning.of(recs[i].tuning), float(recs[i].ms)) for i in range(min(n.value, max_records))]
+    return RenderTuning.of(out), table

@@ -96,6 +96,24 @@ class CRenderProfile(ctypes.Structure):
                 ("shadow_nodes", ctypes.c_uint64), ("shadow_tri_tests", ctypes.c_uint64)]
 
 
+class CRenderTuning(ctypes.Structure):
+    _fields_ = [("wavefront_paths", ctypes.c_int32), ("trace_threads", ctypes.c_int32),
+                ("trace_warps_per_sm", ctypes.c_int32), ("refill_min", ctypes.c_int32),
+                ("shadow_one_lane", ctypes.c_int32), ("reserved", ctypes.c_int32 * 3)]
+
+
+class CTuneRecord(ctypes.Structure):
+    _fields_ = [("tuning", CRenderTuning), ("ms", ctypes.c_float), ("reserved", ctypes.c_int32)]
+
+
+class CMlpTuning(ctypes.Structure):
+    _fields_ = [("wgrad_tiles_per_cta", ctypes.c_int32), ("infer_ctas", ctypes.c_int32),
+                ("reserved", ctypes.c_int32 * 2)]
+
+
+assert ctypes.sizeof(CRenderTuning) == 32 and ctypes.sizeof(CTuneRecord) == 40 and ctypes.sizeof(CMlpTuning) == 16
+
+
 class CImagenGPU(ctypes.Structure):
     _fields_ = [("anchura", ctypes.c_int32), ("altura", ctypes.c_int32), ("datos", ctypes.c_void_p)]
 
