@@ -279,6 +279,31 @@ int tfgRenderPassStatic(
     const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh,
     const TfgImagenGPU* imagen_directa, float* accum, void* stream);
 
+/* One scene of tfgRenderPassBatch: the scene arguments of tfgRenderPass. */
+typedef struct TfgRenderScene {
+    const TfgCamara*       camara;
+    const TfgPrimitiva*    primitivas;
+    int32_t                num_primitivas;
+    int32_t                num_luces;
+    const TfgLuzPuntual*   luces;
+    int32_t                ancho_img, alto_img;
+    const TfgTinyBVHD_GPU* nodos_bvh;
+    const float*           tris_wt;
+    const TfgPrimitiva*    primitivas_bvh;
+    int32_t                num_prims_bvh;
+    int32_t                reserved;
+    TfgColor*              imagen;   /* W*H: the last sample's radiance (may be null) */
+    float*                 accum;    /* W*H*3 sums when params->accumulate (may be null) */
+} TfgRenderScene;
+
+/* No reference counterpart (the reference renders one scene per launch):
+ * plain path tracing of `n` scenes of any sizes with the same settings, each
+ * stage launched once for all of them (groups of up to 16 scenes share one
+ * wavefront series).  Every scene's image equals what tfgRenderPass gives
+ * for it alone, bit for bit. */
+int tfgRenderPassBatch(int32_t n, const TfgRenderScene* scenes, const TfgRenderParams* params,
+                       int32_t frame_number, void* stream);
+
 /* Closest-hit traversal of `n` rays (primary-ray mode).  rays: 8 floats per
  * ray (O.x, O.y, O.z, t_max, D.x, D.y, D.z, unused).  hits: 4 floats per ray
  * (t, u, v, prim id bits); a miss returns t = t_max and id 0xFFFFFFFF.  This

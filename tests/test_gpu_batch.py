@@ -29,12 +29,18 @@ def batch_scenes(built):
         ds.close()
 
 
-def _renderers(batch_scenes, seed=11, graph=False, train_steps=2):
+# Scenes with different render settings cannot share a wavefront: the batch
+# then renders each scene on its own branch.
+MIXED = [PARAMS, pt.RenderParams(max_depth=5, rr_min_depth=3, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT)]
+
+
+def _renderers(batch_scenes, seed=11, graph=False, train_steps=2, mixed=False):
     rs = []
     for k, (s, ds) in enumerate(batch_scenes):
         m = ColorMLP(batch=16384, seed=seed + k)
         m.set_bounds(*s.bounds)
-        rs.append(NrcRenderer(ds, m, PARAMS, train_steps=train_steps, max_records=4096, min_records=256,
+        prm = MIXED[k % 2] if mixed else PARAMS
+        rs.append(NrcRenderer(ds, m, prm, train_steps=train_steps, max_records=4096, min_records=256,
                               use_graph=graph))
     return rs
 
@@ -44,21 +50,22 @@ def _close(rs):
         r.mlp.close()
 
 
+@pytest.mark.parametrize("mixed", [False, True])
 @pytest.mark.parametrize("graph", [False, True])
-def test_batch_frame_equals_single_scene_frames(batch_scenes, graph):
+def test_batch_frame_equals_single_scene_frames(batch_scenes, graph, mixed):
     # With no training steps the cache model stays fixed and a frame is a
     # function of the scene, the model and the frame number (the training
     # record ring is filled through atomics, so trained models are not
     # bit-reproducible).  Both frames query the cache; with the graph, frame 6
     # captures and frame 7 replays the capture.
-    single = _renderers(batch_scenes, train_steps=0)
+    single = _renderers(batch_scenes, train_steps=0, mixed=mixed)
     for r in single:
         r.frame(6, warmup=False, accumulate=False)
         r.frame(7, warmup=False, accumulate=False)
         r.stream.synchronize()
     want = [r.image().cpu().numpy().copy() for r in single]
     _close(single)
-    rs = _renderers(batch_scenes, train_steps=0)
+    rs = _renderers(batch_scenes, train_steps=0, mixed=mixed)
     b = NrcBatch(rs, use_graph=graph)
     b.frame(6, warmup=False)
     b.frame(7, warmup=False)

@@ -11,7 +11,8 @@ from ctypes import POINTER, c_char_p, c_float, c_int32, c_uint32, c_uint64, c_vo
 from pathlib import Path
 
 from .structs import (CCWBVHHost, CImagenGPU, CMlpTuning, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame,
-                      CRenderParams, CRenderProfile, CRenderTuning, CTinyBVH, CTinyBVHD_GPU, CTuneRecord)
+                      CRenderParams, CRenderProfile, CRenderScene, CRenderTuning, CTinyBVH, CTinyBVHD_GPU,
+                      CTuneRecord)
 
 LIB_PATH = Path(__file__).resolve().parent / "libtfgpt.so"
 
@@ -41,6 +42,7 @@ _PROTOS = {
     "tfgRenderParamsReference": (None, [POINTER(CRenderParams)]),
     "tfgRenderProfileReset": (c_int32, []),
     "tfgRenderProfileGet": (c_int32, [POINTER(CRenderProfile)]),
+    "tfgRenderPassBatch": (c_int32, [c_int32, POINTER(CRenderScene), POINTER(CRenderParams), c_int32, c_void_p]),
     "tfgRenderTuningDefault": (None, [POINTER(CRenderTuning)]),
     "tfgRenderTuningSet": (c_int32, [POINTER(CRenderTuning)]),
     "tfgRenderTuningGet": (c_int32, [POINTER(CRenderTuning)]),

@@ -57,13 +57,13 @@ struct FrameCall {
     const TfgTinyBVHD_GPU* bvh; const float* tris_wt; const TfgPrimitiva* mesh; int nmesh;
     TfgNrcBuffers b;
     int32_t* frame_dev;
-    int ws_slot = 0;
+    int ws_slot = 0;   // render workspace slot
+    int branch = 0;    // branch of a batched frame that runs this scene's cache steps
 };
 
+int enqueue_cache_steps(const FrameCall& c, cudaStream_t s);
+
 int enqueue_frame(const FrameCall& c, bool prepare_only, cudaStream_t s) {
-    const uint32_t npx = (uint32_t)c.W * (uint32_t)c.H;
-    const uint32_t min_n = std::max(c.cfg.min_records + 1u, 100u);
-    uint32_t* navail = mlp_navail(c.mlp);
     const uint32_t* gate = c.cfg.gate_threshold > 0.0f ? mlp_gate(c.mlp) : nullptr;
     if (prepare_only) {
         if (int rc = mlp_prepare(c.mlp)) return rc;
@@ -77,6 +77,29 @@ int enqueue_frame(const FrameCall& c, bool prepare_only, cudaStream_t s) {
                                 c.ws_slot, s))
         return rc;
     if (prepare_only) return ok();
+    return enqueue_cache_steps(c, s);
+}
+
+// The scene as one member of a batched render pass.
+PassScene pass_scene(const FrameCall& c) {
+    PassScene p{};
+    p.cam = c.cam; p.prims = c.prims; p.nprims = c.nprims; p.lights = c.lights; p.nlights = c.nlights;
+    p.W = c.W; p.H = c.H;
+    p.bvh = c.bvh; p.tris_wt = c.tris_wt; p.mesh = c.mesh; p.nmesh = c.nmesh;
+    p.img = c.b.img; p.accum = nullptr;
+    p.regs = c.b.regs; p.reg_counter = c.b.counter; p.reg_cap = (int)c.b.ring_cap;
+    p.infer = c.b.infer; p.thr_out = c.b.thr;
+    p.use_inf_dev = c.cfg.gate_threshold > 0.0f ? mlp_gate(c.mlp) : nullptr;
+    p.use_inf = c.cfg.warmup ? 0 : 1;
+    return p;
+}
+
+// After the render: answer and composite the cache queries, accumulate,
+// bootstrap targets from the tail queries and train (main.cpp:1016-1061).
+int enqueue_cache_steps(const FrameCall& c, cudaStream_t s) {
+    const uint32_t npx = (uint32_t)c.W * (uint32_t)c.H;
+    const uint32_t min_n = std::max(c.cfg.min_records + 1u, 100u);
+    uint32_t* navail = mlp_navail(c.mlp);
     if (int rc = mlp_enqueue_infer(c.mlp, c.b.infer, nullptr, c.b.img, c.b.thr, npx, nullptr, s)) return rc;
     if (c.b.accum)
         if (int rc = launch_nrc_frame_small(3, c.b.img, c.b.accum, nullptr, nullptr, npx, 0, s)) return rc;
@@ -116,7 +139,7 @@ FrameKey key_of(const FrameCall& c) {
                          (int32_t)c.cfg.max_records, (int32_t)c.cfg.min_records, c.cfg.warmup, c.prm.max_depth,
                          c.prm.rr_min_depth, c.prm.shadow_mesh, c.prm.tri_format, c.ws_slot,
                          mlp_precision(c.mlp), (int32_t)render_generation(), (int32_t)mlp_tuning_generation(c.mlp),
-                         (int32_t)workspace_generation(current_device(), c.ws_slot)};
+                         (int32_t)workspace_generation(current_device(), c.ws_slot), c.branch};
     static_assert(sizeof(v) <= sizeof(k.ints), "frame key: too many ints");
     std::memcpy(k.ints, v, sizeof(v));
     k.gate = c.cfg.gate_threshold;
@@ -183,14 +206,43 @@ int branch_resources(int dev, int nb) {
     return ok();
 }
 
+// Scenes that share their render settings (at most 16) render as one
+// wavefront series; otherwise each scene renders on its own branch.
+bool merged_render(const std::vector<FrameCall>& calls) {
+    if (calls.size() > 16) return false;
+    for (const FrameCall& c : calls) {
+        const TfgRenderParams& p = c.prm, & q = calls[0].prm;
+        if (p.max_depth != q.max_depth || p.rr_min_depth != q.rr_min_depth || p.shadow_mesh != q.shadow_mesh ||
+            p.tri_format != q.tri_format || p.spp != q.spp || p.profile != q.profile)
+            return false;
+    }
+    return true;
+}
+
+int render_merged(const std::vector<FrameCall>& calls, bool prepare_only, cudaStream_t s) {
+    PassScene ps[16];
+    for (size_t i = 0; i < calls.size(); ++i) ps[i] = pass_scene(calls[i]);
+    return render_pass_multi(calls[0].prm, ps, (int)calls.size(), 0, calls[0].frame_dev, 1, prepare_only, 0, s);
+}
+
 // Fork `nb` branches off `s`, enqueue every scene on its branch, join back.
-int enqueue_batch(const std::vector<FrameCall>& calls, int nb, int dev, cudaStream_t s) {
-    cudaError_t e = cudaEventRecord(g_fork[dev & 15], s);
+// With `merged`, the scenes render first as one wavefront series on `s` and
+// only their cache steps run on the branches.
+int enqueue_batch(const std::vector<FrameCall>& calls, int nb, int dev, bool merged, cudaStream_t s) {
+    cudaError_t e = cudaSuccess;
+    int rc = 0;
+    if (merged) {
+        for (const FrameCall& c : calls)
+            if (e == cudaSuccess) e = cudaMemsetAsync(c.b.counter, 0, sizeof(uint32_t), s);
+        if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch: ") + cudaGetErrorString(e));
+        if (int r = render_merged(calls, false, s)) return r;
+    }
+    e = cudaEventRecord(g_fork[dev & 15], s);
     for (int b = 1; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(g_branch[dev & 15][b], g_fork[dev & 15], 0);
     if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch fork: ") + cudaGetErrorString(e));
-    int rc = 0;
     for (const FrameCall& c : calls) {
-        rc = enqueue_frame(c, false, c.ws_slot == 0 ? s : g_branch[dev & 15][c.ws_slot]);
+        cudaStream_t bs = c.branch == 0 ? s : g_branch[dev & 15][c.branch];
+        rc = merged ? enqueue_cache_steps(c, bs) : enqueue_frame(c, false, bs);
         if (rc) break;
     }
     // join every branch even after a failure, so a capture can end cleanly
@@ -301,21 +353,29 @@ extern "C" int tfgNrcFrameBatch(int32_t n, const TfgNrcSceneFrame* scenes, int32
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
         return (int64_t)calls[(size_t)x].W * calls[(size_t)x].H > (int64_t)calls[(size_t)y].W * calls[(size_t)y].H;
     });
+    const bool merged = merged_render(calls);
     std::vector<int64_t> load((size_t)nb, 0);
     for (int i : order) {
         const int b = (int)(std::min_element(load.begin(), load.end()) - load.begin());
-        calls[(size_t)i].ws_slot = b;
+        calls[(size_t)i].branch = b;
+        calls[(size_t)i].ws_slot = merged ? 0 : b;
         load[(size_t)b] += (int64_t)calls[(size_t)i].W * calls[(size_t)i].H;
     }
     if (int rc = branch_resources(dev, nb)) return rc;
     for (const FrameCall& c : calls) {
         mlp_set_gate_threshold(c.mlp, c.cfg.gate_threshold);
-        if (int rc = enqueue_frame(c, true, s)) return rc;
+        if (merged) {
+            if (int rc = mlp_prepare(c.mlp)) return rc;
+        } else if (int rc = enqueue_frame(c, true, s)) {
+            return rc;
+        }
     }
+    if (merged)
+        if (int rc = render_merged(calls, true, s)) return rc;
     k_set_frame<<<1, 32, 0, s>>>(frame_dev, frame);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch: ") + cudaGetErrorString(e));
-    if (!(use_graph && s != nullptr)) return enqueue_batch(calls, nb, dev, s);
+    if (!(use_graph && s != nullptr)) return enqueue_batch(calls, nb, dev, merged, s);
     BatchGraph& g = g_batch[dev & 15];
     std::vector<FrameKey> keys;
     for (const FrameCall& c : calls) keys.push_back(key_of(c));
@@ -326,7 +386,7 @@ extern "C" int tfgNrcFrameBatch(int32_t n, const TfgNrcSceneFrame* scenes, int32
         g.exec = nullptr; g.graph = nullptr; g.valid = false;
         e = cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal);
         if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch capture: ") + cudaGetErrorString(e));
-        const int rc = enqueue_batch(calls, nb, dev, s);
+        const int rc = enqueue_batch(calls, nb, dev, merged, s);
         cudaGraph_t gr = nullptr;
         e = cudaStreamEndCapture(s, &gr);
         if (rc) { if (gr) cudaGraphDestroy(gr); return rc; }

@@ -23,6 +23,7 @@
 #include <cstring>
 #include <mutex>
 #include <string>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/tfg_pt.h"
@@ -102,8 +103,74 @@ struct PassArgs {
     Workspace ws;
 };
 
+// Several scenes in one wavefront (a batch): the scenes' pixels are
+// concatenated (scene i owns global pixels pix0 .. pix0 + W*H - 1) and every
+// path carries its scene index, in the ray queue entry's first w (closest-hit
+// rays always start with t_max = 1e9) and in the shadow item.  The table
+// travels by value in the kernel parameters, so a captured graph keeps the
+// table it was captured with.
+constexpr int kMaxBatchScenes = 16;
+struct SceneDesc {
+    const TfgPrimitiva* prims; const TfgLuzPuntual* lights;
+    const float4* nodes; const float4* tris; const TfgPrimitiva* mesh;
+    const TfgCamara* cam; const uint32_t* use_inf_dev;
+    TfgColor* img; float* accum;
+    TfgRegistroEntrenamiento* regs; uint32_t* reg_counter;
+    TfgDatosMLP* infer; TfgColor* thr_out;
+    int nprims, nlights, has_bvh, nmesh, W, H, reg_cap, use_inf;
+    uint32_t pix0;
+};
+struct SceneTable {
+    SceneDesc s[kMaxBatchScenes];
+    int n;
+};
+struct NoTable {};
+template <bool MS> using TableOf = typename std::conditional<MS, SceneTable, NoTable>::type;
+
+// The geometry a path sees.
+struct Geo {
+    const TfgPrimitiva* prims; const float4* nodes; const float4* tris; const TfgPrimitiva* mesh;
+    int nprims, has_bvh;
+};
+
+// Per-pixel outputs of a path's scene.
+struct Outs {
+    TfgColor* img; float* accum;
+    TfgRegistroEntrenamiento* regs; uint32_t* reg_counter; int reg_cap;
+    TfgDatosMLP* infer; TfgColor* thr_out;
+};
+
 // ------------------------------------------------------------------ helpers
 __device__ __forceinline__ uint32_t lane_id() { return threadIdx.x & 31u; }
+
+template <bool MS>
+__device__ __forceinline__ Geo geo_of(const PassArgs& a, const TableOf<MS>& tab, uint32_t sc) {
+    if constexpr (MS) {
+        const SceneDesc& d = tab.s[sc];
+        return Geo{d.prims, d.nodes, d.tris, d.mesh, d.nprims, d.has_bvh};
+    } else {
+        (void)tab; (void)sc;
+        return Geo{a.prims, a.nodes, a.tris, a.mesh, a.nprims, a.has_bvh};
+    }
+}
+
+template <bool MS>
+__device__ __forceinline__ Outs outs_of(const PassArgs& a, const TableOf<MS>& tab, uint32_t sc) {
+    if constexpr (MS) {
+        const SceneDesc& d = tab.s[sc];
+        return Outs{d.img, d.accum, d.regs, d.reg_counter, d.reg_cap, d.infer, d.thr_out};
+    } else {
+        (void)tab; (void)sc;
+        return Outs{a.img, a.accum, a.regs, a.reg_counter, a.reg_cap, a.infer, a.thr_out};
+    }
+}
+
+// Scene owning global pixel g (scenes in pixel order).
+__device__ __forceinline__ uint32_t scene_of_pixel(const SceneTable& tab, uint32_t g) {
+    uint32_t sc = 0;
+    while ((int)sc + 1 < tab.n && g >= tab.s[sc + 1].pix0) ++sc;
+    return sc;
+}
 
 // Pixel of the path in wavefront slot `slot`.
 __device__ __forceinline__ uint32_t pixel_of(const PassArgs& a, uint32_t slot) { return (a.p0 + slot) % a.npix; }
@@ -122,8 +189,8 @@ __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
 
 __device__ __forceinline__ V3 xyz(float4 a) { return v3(a.x, a.y, a.z); }
 
-__device__ __forceinline__ const TfgPrimitiva* prim_of(const PassArgs& a, uint32_t id) {
-    return (id & kAnalyticBit) ? &a.prims[id & ~kAnalyticBit] : &a.mesh[id];
+__device__ __forceinline__ const TfgPrimitiva* prim_of(const Geo& g, uint32_t id) {
+    return (id & kAnalyticBit) ? &g.prims[id & ~kAnalyticBit] : &g.mesh[id];
 }
 
 // Closest analytic hit (escenario.h:323-334): strict t < best, t > 1e-6.
@@ -165,26 +232,42 @@ __device__ __forceinline__ int use_inf_of(const PassArgs& a) {
     return a.use_inf && (!a.use_inf_dev || *a.use_inf_dev != 0u);
 }
 
-__global__ void k_generate(PassArgs a) {
+__device__ __forceinline__ int use_inf_of(const SceneDesc& d) {
+    return d.use_inf && (!d.use_inf_dev || *d.use_inf_dev != 0u);
+}
+
+template <bool MS>
+__global__ void k_generate(PassArgs a, TableOf<MS> tab) {
     const uint32_t N = a.npix;
-    const TfgCamara cam = *a.cam;
+    TfgCamara cam;
+    int use_inf = 0;
+    if constexpr (!MS) { cam = *a.cam; use_inf = use_inf_of(a); }
     const int frame0 = a.frame + a.s0 + (a.frame_dev ? *a.frame_dev : 0);
-    const int use_inf = use_inf_of(a);
     for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < a.nq; p += gridDim.x * blockDim.x) {
-        const uint32_t q = a.p0 + p, s = q / N, pix = q - s * N;
-        const int x = (int)(pix % (uint32_t)a.W), y = (int)(pix / (uint32_t)a.W);
+        const uint32_t q = a.p0 + p, s = q / N;
+        uint32_t pix = q - s * N, sc = 0;
+        int W = a.W, H = a.H;
+        if constexpr (MS) {
+            sc = scene_of_pixel(tab, pix);
+            const SceneDesc& d = tab.s[sc];
+            pix -= d.pix0;
+            W = d.W; H = d.H;
+            cam = *d.cam;
+            use_inf = use_inf_of(d);
+        }
+        const int x = (int)(pix % (uint32_t)W), y = (int)(pix / (uint32_t)W);
         uint32_t rng = seed_pixel(x, y, frame0 + (int)s);
         const float ox = pcg_uniform(rng);
         const float oy = pcg_uniform(rng);
         V3 O, D;
-        camera_ray(cam, x, y, a.W, a.H, ox, oy, O, D);
+        camera_ray(cam, x, y, W, H, ox, oy, O, D);
         uint32_t flags = 0;
         bool training = a.train ? (use_inf ? (pcg_uniform(rng) < 0.05f) : true) : false;
         if (training) {
             flags |= F_TRAIN;
             if (pcg_uniform(rng) < 0.0625f) flags |= F_UNBIASED;
         }
-        a.ws.ray[0][2 * p + 0] = make_float4(O.x, O.y, O.z, 1e9f);
+        a.ws.ray[0][2 * p + 0] = make_float4(O.x, O.y, O.z, MS ? __uint_as_float(sc) : 1e9f);
         a.ws.ray[0][2 * p + 1] = make_float4(D.x, D.y, D.z, __uint_as_float(p));
         a.ws.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
         a.ws.st[p] = make_uint4(rng, flags, __float_as_uint(1.0f), 0u);
@@ -198,12 +281,14 @@ __global__ void k_generate(PassArgs a) {
 }
 
 // ------------------------------------------------------------------ trace
-template <int TRI_FMT, bool STATS>
-__global__ void __launch_bounds__(256) k_trace(PassArgs a, int bounce) {
+template <int TRI_FMT, bool STATS, bool MS>
+__global__ void __launch_bounds__(256) k_trace(PassArgs a, int bounce, TableOf<MS> tab) {
     extern __shared__ unsigned char smem_raw[];
     uint2* sstack = reinterpret_cast<uint2*>(smem_raw);
     APrim* sprims = reinterpret_cast<APrim*>(smem_raw + sizeof(uint2) * kSmemStack * blockDim.x);
-    const int nsm = load_aprims_smem(sprims, a.prims, a.nprims);
+    // one scene: its analytic primitives are cached in shared memory
+    const int nsm = MS ? 0 : load_aprims_smem(sprims, a.prims, a.nprims);
+    Geo g = geo_of<MS>(a, tab, 0);
     TravStack st;
     st.smem = sstack; st.stride = blockDim.x; st.tid = threadIdx.x;
     const float4* rays = a.ws.ray[bounce & 1];
@@ -234,14 +319,16 @@ __global__ void __launch_bounds__(256) k_trace(PassArgs a, int bounce) {
                 cur = k;
                 const float4 o4 = rays[2 * k], d4 = rays[2 * k + 1];
                 const V3 O = xyz(o4), D = xyz(d4);
-                best = o4.w; bu = 0.0f; bv = 0.0f; bid = kMissId;
-                const int ai = analytic_closest(sprims, nsm, a.prims, a.nprims, O, D, best, bu, bv);
+                if constexpr (MS) { g = geo_of<MS>(a, tab, __float_as_uint(o4.w)); best = 1e9f; }
+                else best = o4.w;
+                bu = 0.0f; bv = 0.0f; bid = kMissId;
+                const int ai = analytic_closest(sprims, nsm, g.prims, g.nprims, O, D, best, bu, bv);
                 if (ai >= 0) bid = kAnalyticBit | (uint32_t)ai;
                 r.init(O, D, 0.0f, best);
             }
         }
-        if (cur != kMissId && !(a.has_bvh && r.step(a.nodes, a.tris, st))) {
-            if (a.has_bvh) {
+        if (cur != kMissId && !(g.has_bvh && r.step(g.nodes, g.tris, st))) {
+            if (g.has_bvh) {
                 if (r.found && r.tmax < best && r.tmax > kEps) { best = r.tmax; bu = r.hu; bv = r.hv; bid = r.id; }
                 if (STATS) { cnt.nodes += r.nsteps; cnt.tris += r.ntris; }
             }
@@ -274,14 +361,15 @@ __device__ __forceinline__ void write_datos(TfgDatosMLP* d, V3 P, V3 dir, V3 n, 
     *d = r;
 }
 
-__global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
+template <bool MS>
+__global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<MS> tab) {
     const uint32_t n = a.ws.counters[4 * bounce + 0];
     const float4* rays = a.ws.ray[bounce & 1];
     float4* next = a.ws.ray[(bounce + 1) & 1];
     uint32_t* next_count = &a.ws.counters[4 * (bounce + 1) + 0];
     uint32_t* shadow_count = &a.ws.counters[4 * bounce + 2];
     const bool nrc = a.use_inf || a.train;
-    const int use_inf = use_inf_of(a);
+    const int use_inf_single = MS ? 0 : use_inf_of(a);
     const uint32_t stride = gridDim.x * blockDim.x;
     // Uniform trip count so that every lane of a warp reaches the warp-wide appends.
     const uint32_t n_round = (n + stride - 1) / stride * stride;
@@ -292,6 +380,10 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
         if (live) {
             const float4 o4 = rays[2 * i], d4 = rays[2 * i + 1], h = a.ws.hit[i];
             p = __float_as_uint(d4.w);
+            const uint32_t sc = MS ? __float_as_uint(o4.w) : 0u;
+            const Geo g = geo_of<MS>(a, tab, sc);
+            int use_inf = use_inf_single;
+            if constexpr (MS) use_inf = use_inf_of(tab.s[sc]);
             V3 O = xyz(o4), D = xyz(d4);
             float4 thr4 = a.ws.thr[p];
             uint4 st = a.ws.st[p];
@@ -307,7 +399,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
             if (id == kMissId) {
                 end = true;   // background is black (render.h:227-239)
             } else {
-                const TfgPrimitiva* pr = prim_of(a, id);
+                const TfgPrimitiva* pr = prim_of(g, id);
                 const float t = h.x;
                 const V3 P = O + D * t;
                 const V3 nrm = surface_normal(pr, P, h.y, h.z);
@@ -350,7 +442,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
                         want_shadow = true;
                         sh0 = make_float4(ps.x, ps.y, ps.z, __uint_as_float(p));
                         sh1 = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(captured ? 1u : 0u));
-                        sh2 = make_float4(m.difuso.x, m.difuso.y, m.difuso.z, 0.0f);
+                        sh2 = make_float4(m.difuso.x, m.difuso.y, m.difuso.z, MS ? __uint_as_float(sc) : 0.0f);
                         sh3 = make_float4(cam.x, cam.y, cam.z, 0.0f);
                     }
                     if (captured) {
@@ -371,10 +463,12 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
                         refl = v3(fmaxf(refl.x, 1e-3f), fmaxf(refl.y, 1e-3f), fmaxf(refl.z, 1e-3f));
                         const bool training = (flags & F_TRAIN) != 0;
                         if (!training && use_inf) {
-                            const uint32_t px = pixel_of(a, p);
-                            write_datos(&a.infer[px], P, map01(view), map01(nrm), m.difuso, m.especular);
+                            const Outs o = outs_of<MS>(a, tab, sc);
+                            uint32_t px = pixel_of(a, p);
+                            if constexpr (MS) px -= tab.s[sc].pix0;
+                            write_datos(&o.infer[px], P, map01(view), map01(nrm), m.difuso, m.especular);
                             const V3 tt = mul(cam, refl);
-                            a.thr_out[px] = TfgColor{tt.x, tt.y, tt.z};
+                            o.thr_out[px] = TfgColor{tt.x, tt.y, tt.z};
                             flags |= F_INF;
                             end = true;
                         } else if (training && !captured) {
@@ -441,7 +535,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
             a.ws.st[p] = make_uint4(rng, flags, __float_as_uint(pdf_last), 0u);
             a.ws.lpre[p] = lpre;
             if (nrc) { a.ws.lsuf[p] = lsuf; a.ws.nrc[p] = nrc4; }
-            nr0 = make_float4(O.x, O.y, O.z, 1e9f);
+            nr0 = make_float4(O.x, O.y, O.z, MS ? __uint_as_float(sc) : 1e9f);
             nr1 = make_float4(D.x, D.y, D.z, __uint_as_float(p));
         }
         const uint32_t slot = warp_append(next_count, survive);
@@ -458,12 +552,12 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce) {
 // escenario.h:144-184: every light in order, Lambert BRDF kd/pi, inverse-square
 // falloff with the distance clamped to >= 1, summed then scaled by the path
 // throughput (render.h:128-130).
-template <int TRI_FMT, bool STATS>
-__global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce) {
+template <int TRI_FMT, bool STATS, bool MS>
+__global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<MS> tab) {
     extern __shared__ unsigned char smem_raw[];
     uint2* sstack = reinterpret_cast<uint2*>(smem_raw);
     APrim* sprims = reinterpret_cast<APrim*>(smem_raw + sizeof(uint2) * kSmemStack * blockDim.x);
-    const int nsm = load_aprims_smem(sprims, a.prims, a.nprims);
+    const int nsm = MS ? 0 : load_aprims_smem(sprims, a.prims, a.nprims);
     TravStack stck;
     stck.smem = sstack; stck.stride = blockDim.x; stck.tid = threadIdx.x;
     const uint32_t n = a.ws.counters[4 * bounce + 2];
@@ -471,11 +565,11 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce) {
     TravCounts cnt;
     uint32_t nrays = 0;
     // One shadow ray per lane: the lights of an item sit on G adjacent lanes
-    // (G = light count rounded up to a power of two; more than 32 lights, or
-    // a.shadow_one_lane, give one lane looping over them), and warps fetch
-    // items dynamically.
+    // (G = light count rounded up to a power of two; more than 32 lights,
+    // a.shadow_one_lane, or a batch of scenes with their own light counts give
+    // one lane looping over them), and warps fetch items dynamically.
     const int nl = a.nlights;
-    const uint32_t G = a.shadow_one_lane ? 1u
+    const uint32_t G = (MS || a.shadow_one_lane) ? 1u
                        : nl <= 1 ? 1u : nl <= 2 ? 2u : nl <= 4 ? 4u : nl <= 8 ? 8u : nl <= 16 ? 16u : nl <= 32 ? 32u : 1u;
     const uint32_t lane = lane_id(), lg = lane & (G - 1u), group0 = lane & ~(G - 1u);
     const int l_begin = G == 1u ? 0 : (int)lg;
@@ -497,8 +591,13 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce) {
             P = xyz(s0); N = xyz(s1); kd = xyz(s2); cam = xyz(s3);
             p = __float_as_uint(s0.w);
             to_suffix = __float_as_uint(s1.w) != 0u;
-            for (int l = l_begin; l < l_end; ++l) {
-                const TfgLuzPuntual lz = a.lights[l];
+            const uint32_t sc = MS ? __float_as_uint(s2.w) : 0u;
+            const Geo g = geo_of<MS>(a, tab, sc);
+            const TfgLuzPuntual* lights = a.lights;
+            int lend = l_end;
+            if constexpr (MS) { lights = tab.s[sc].lights; lend = tab.s[sc].nlights; }
+            for (int l = l_begin; l < lend; ++l) {
+                const TfgLuzPuntual lz = lights[l];
                 V3 dl = ld3(lz.posicion) - P;
                 float dist = sqrtf(dot(dl, dl));
                 dl = normalized(dl);
@@ -506,11 +605,11 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce) {
                 if (c <= 0.0f) continue;
                 const V3 so = P + dl * kEps;
                 if (STATS) ++nrays;
-                if (analytic_any(sprims, nsm, a.prims, a.nprims, so, dl, dist)) continue;
-                if (a.shadow_mesh && a.has_bvh) {
+                if (analytic_any(sprims, nsm, g.prims, g.nprims, so, dl, dist)) continue;
+                if (a.shadow_mesh && g.has_bvh) {
                     float tm = dist, hu, hv;
                     uint32_t hid;
-                    if (cwbvh_trace<TRI_FMT, true>(a.nodes, a.tris, so, dl, kEps, tm, hid, hu, hv, stck,
+                    if (cwbvh_trace<TRI_FMT, true>(g.nodes, g.tris, so, dl, kEps, tm, hid, hu, hv, stck,
                                                    STATS ? &cnt : nullptr)) continue;
                 }
                 const V3 kdpi = v3(kd.x / kPiF, kd.y / kPiF, kd.z / kPiF);
@@ -556,22 +655,26 @@ __device__ __forceinline__ void get_geo(const float4* src, TfgDatosGeometricos& 
 // One thread per pixel of the wavefront: slots j, j + npix, j + 2 npix ...
 // hold that pixel's samples in order, so the accumulation adds them in sample
 // order whatever the wavefront size.
-__global__ void k_resolve(PassArgs a) {
+template <bool MS>
+__global__ void k_resolve(PassArgs a, TableOf<MS> tab) {
     const uint32_t N = a.npix;
     const bool nrc = a.use_inf || a.train;
     const uint32_t first = min(a.nq, N);
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < first; j += gridDim.x * blockDim.x) {
-        const uint32_t q = a.p0 + j, s_rel = q / N, px = q - s_rel * N;
+        const uint32_t q = a.p0 + j, s_rel = q / N;
+        uint32_t px = q - s_rel * N, sc = 0;
+        if constexpr (MS) { sc = scene_of_pixel(tab, px); px -= tab.s[sc].pix0; }
+        const Outs o = outs_of<MS>(a, tab, sc);
         int sample = a.s0 + (int)s_rel;
         for (uint32_t p = j; p < a.nq; p += N, ++sample) {
             const float4 lp = a.ws.lpre[p];
-            if (a.img && sample == a.last_sample) a.img[px] = TfgColor{lp.x, lp.y, lp.z};
-            if (a.accum) {
-                a.accum[3 * (size_t)px] += lp.x; a.accum[3 * (size_t)px + 1] += lp.y; a.accum[3 * (size_t)px + 2] += lp.z;
+            if (o.img && sample == a.last_sample) o.img[px] = TfgColor{lp.x, lp.y, lp.z};
+            if (o.accum) {
+                o.accum[3 * (size_t)px] += lp.x; o.accum[3 * (size_t)px + 1] += lp.y; o.accum[3 * (size_t)px + 2] += lp.z;
             }
             const uint32_t flags = a.ws.st[p].y;
             const bool rec = nrc && (flags & F_TRAIN) && (flags & F_CAPTURED);
-            if (a.thr_out && !(flags & F_INF) && !rec) a.thr_out[px] = TfgColor{0.0f, 0.0f, 0.0f};
+            if (o.thr_out && !(flags & F_INF) && !rec) o.thr_out[px] = TfgColor{0.0f, 0.0f, 0.0f};
             if (!rec) continue;
             // Training path with a head vertex: its pixel keeps the prefix radiance and
             // asks the cache at the head (render.h:243-260); the record goes to the ring
@@ -580,14 +683,14 @@ __global__ void k_resolve(PassArgs a) {
             TfgDatosGeometricos head, tail;
             get_geo(ts, head);
             const float4 thr_train = ts[8];
-            if (a.infer) {
+            if (o.infer) {
                 TfgDatosMLP d;
                 d.posicion = head.posicion; d.direccion = head.direccion; d.normal = head.normal;
                 d.difuso = head.difuso; d.especular = head.especular; d.color = TfgColor{0.0f, 0.0f, 0.0f};
-                a.infer[px] = d;
+                o.infer[px] = d;
             }
-            if (a.thr_out) a.thr_out[px] = TfgColor{thr_train.x, thr_train.y, thr_train.z};
-            if (a.reg_counter && a.regs && a.reg_cap > 0) {
+            if (o.thr_out) o.thr_out[px] = TfgColor{thr_train.x, thr_train.y, thr_train.z};
+            if (o.reg_counter && o.regs && o.reg_cap > 0) {
                 TfgRegistroEntrenamiento r;
                 r.head = head;
                 float4 thr_suf = make_float4(0, 0, 0, 0);
@@ -599,8 +702,8 @@ __global__ void k_resolve(PassArgs a) {
                 r.throughput_sufijo = TfgColor{thr_suf.x, thr_suf.y, thr_suf.z};
                 r.factor_normalizacion = TfgColor{thr_train.x, thr_train.y, thr_train.z};
                 r.valido = 1;
-                const uint32_t idx = atomicAdd(a.reg_counter, 1u);
-                a.regs[idx % (uint32_t)a.reg_cap] = r;
+                const uint32_t idx = atomicAdd(o.reg_counter, 1u);
+                o.regs[idx % (uint32_t)o.reg_cap] = r;
             }
         }
     }
@@ -672,9 +775,10 @@ namespace {
 
 struct LaunchShapes {
     int sms = 0;
-    int trace_occ[2][3] = {};    // resident CTAs per SM: [triangle format][64, 128, 256 threads]
-    int shadow_occ[2][3] = {};
-    int shade_blocks = 0;
+    // resident CTAs per SM: [one scene / batch][triangle format][64, 128, 256 threads]
+    int trace_occ[2][2][3] = {};
+    int shadow_occ[2][2][3] = {};
+    int shade_blocks[2] = {0, 0};
 };
 LaunchShapes g_shapes[16];
 
@@ -687,22 +791,25 @@ int shapes_for(int dev, LaunchShapes& s) {
     if (g.sms == 0) {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        auto occ_of = [](auto kernel, int bt, size_t sm) {
+            int occ = 0;
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kernel, bt, sm);
+            return std::max(occ, 1);
+        };
         for (int k = 0; k < 3; ++k) {
             const int bt = kThreadChoices[k];
-            const size_t sm = trace_smem(kSmemPrims, bt);
-            int occ = 0;
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<0, false>, bt, sm);
-            g.trace_occ[0][k] = std::max(occ, 1);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_trace<1, false>, bt, sm);
-            g.trace_occ[1][k] = std::max(occ, 1);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<0, false>, bt, sm);
-            g.shadow_occ[0][k] = std::max(occ, 1);
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shadow<1, false>, bt, sm);
-            g.shadow_occ[1][k] = std::max(occ, 1);
+            const size_t sm = trace_smem(kSmemPrims, bt), sm_ms = trace_smem(0, bt);
+            g.trace_occ[0][0][k] = occ_of(k_trace<0, false, false>, bt, sm);
+            g.trace_occ[0][1][k] = occ_of(k_trace<1, false, false>, bt, sm);
+            g.shadow_occ[0][0][k] = occ_of(k_shadow<0, false, false>, bt, sm);
+            g.shadow_occ[0][1][k] = occ_of(k_shadow<1, false, false>, bt, sm);
+            g.trace_occ[1][0][k] = occ_of(k_trace<0, false, true>, bt, sm_ms);
+            g.trace_occ[1][1][k] = occ_of(k_trace<1, false, true>, bt, sm_ms);
+            g.shadow_occ[1][0][k] = occ_of(k_shadow<0, false, true>, bt, sm_ms);
+            g.shadow_occ[1][1][k] = occ_of(k_shadow<1, false, true>, bt, sm_ms);
         }
-        int occ = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_shade, 256, 0);
-        g.shade_blocks = sms * std::max(occ, 1);
+        g.shade_blocks[0] = sms * occ_of(k_shade<false>, 256, 0);
+        g.shade_blocks[1] = sms * occ_of(k_shade<true>, 256, 0);
         g.sms = sms;
     }
     s = g;
@@ -840,8 +947,9 @@ int profile_get(TfgRenderProfile* out) {
     return ok();
 }
 
-int enqueue_pass(PassArgs a, const TfgRenderParams& prm, int frame, TfgColor* img, const LaunchShapes& sh,
-                 const Tuning& tu, cudaStream_t stream);
+template <bool MS>
+int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm, int frame, TfgColor* img,
+                 const LaunchShapes& sh, const Tuning& tu, cudaStream_t stream);
 
 int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
                 const TfgLuzPuntual* lights, int nlights, int W, int H, int frame, const TfgTinyBVHD_GPU* bvh,
@@ -899,21 +1007,91 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
     a.infer = infer; a.thr_out = thr_out; a.use_inf = use_inf; a.train = train;
     a.max_depth = prm.max_depth; a.rr_min_depth = prm.rr_min_depth; a.shadow_mesh = prm.shadow_mesh;
     a.ws = ws;
-    return enqueue_pass(a, prm, frame, img, sh, tu, stream);
+    return enqueue_pass<false>(a, NoTable{}, prm, frame, img, sh, tu, stream);
+}
+
+// Several scenes with the same settings in one wavefront series: each stage
+// is one launch for all of them, so the small scenes of a batch and the deep,
+// sparse bounces of every scene share the GPU.  A path computes exactly what
+// it computes in a single-scene pass.
+int render_pass_multi(const TfgRenderParams& prm, const PassScene* scenes, int n, int frame, const int32_t* frame_dev,
+                      int train, bool prepare_only, int ws_slot, cudaStream_t stream) {
+    if (n < 1 || n > kMaxBatchScenes) return fail(TFG_E_INVALID, "render batch: 1 to 16 scenes per pass");
+    if (!scenes) return fail(TFG_E_INVALID, "render batch: scenes is null");
+    if (prm.max_depth < 1 || prm.max_depth > kMaxBounces) return fail(TFG_E_INVALID, "render: max_depth out of [1,64]");
+    if (prm.spp < 1) return fail(TFG_E_INVALID, "render: spp < 1");
+    if (prm.tri_format != TFG_TRIS_REF && prm.tri_format != TFG_TRIS_WATERTIGHT)
+        return fail(TFG_E_INVALID, "render: unknown tri_format");
+    SceneTable tab{};
+    tab.n = n;
+    uint64_t total = 0;
+    int any_inf = 0;
+    for (int i = 0; i < n; ++i) {
+        const PassScene& c = scenes[i];
+        const std::string at = "render batch: scene " + std::to_string(i) + ": ";
+        if (c.W <= 0 || c.H <= 0) return fail(TFG_E_INVALID, at + "bad image size");
+        if (!c.cam) return fail(TFG_E_INVALID, at + "camara is null");
+        if (c.nprims < 0 || c.nlights < 0 || c.nmesh < 0) return fail(TFG_E_INVALID, at + "negative count");
+        if ((c.nprims > 0 && !c.prims) || (c.nlights > 0 && !c.lights)) return fail(TFG_E_INVALID, at + "null scene array");
+        if ((c.use_inf || train) && (!c.infer || !c.thr_out))
+            return fail(TFG_E_INVALID, at + "NRC flags need inference and throughput buffers");
+        const bool has_bvh = c.bvh && c.bvh->d_nodos && c.bvh->d_tris && c.nmesh > 0;
+        if (has_bvh && !c.mesh) return fail(TFG_E_INVALID, at + "mesh primitives are null");
+        if (has_bvh && prm.tri_format == TFG_TRIS_WATERTIGHT && !c.tris_wt)
+            return fail(TFG_E_INVALID, at + "watertight format needs tris_wt");
+        SceneDesc& d = tab.s[i];
+        d.prims = c.prims; d.nprims = c.nprims; d.lights = c.lights; d.nlights = c.nlights;
+        d.nodes = has_bvh ? reinterpret_cast<const float4*>(c.bvh->d_nodos) : nullptr;
+        d.tris = has_bvh ? reinterpret_cast<const float4*>(prm.tri_format == TFG_TRIS_REF ? c.bvh->d_tris : c.tris_wt)
+                         : nullptr;
+        d.has_bvh = has_bvh ? 1 : 0;
+        d.mesh = c.mesh; d.nmesh = c.nmesh;
+        d.cam = c.cam; d.use_inf_dev = c.use_inf_dev; d.use_inf = c.use_inf;
+        d.img = c.img; d.accum = c.accum;
+        d.regs = c.regs; d.reg_counter = c.reg_counter; d.reg_cap = c.reg_cap;
+        d.infer = c.infer; d.thr_out = c.thr_out;
+        d.W = c.W; d.H = c.H;
+        d.pix0 = (uint32_t)total;
+        total += (uint64_t)c.W * (uint64_t)c.H;
+        if (total > (1u << 28)) return fail(TFG_E_INVALID, "render batch: more than 2^28 pixels in one pass");
+        any_inf |= c.use_inf ? 1 : 0;
+    }
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+    if (int rc = require_sm100(dev)) return rc;
+    const bool nrc = any_inf || train;
+    const Tuning tu = resolve_tuning(dev, (uint32_t)total, prm.spp, nrc, nullptr);
+    Workspace ws;
+    if (int rc = ensure_workspace(dev, ws_slot, tu.wavefront, nrc, ws)) return rc;
+    LaunchShapes sh;
+    shapes_for(dev, sh);
+    if (prepare_only) return ok();
+
+    PassArgs a{};
+    a.frame_dev = frame_dev;
+    a.W = (int)total; a.H = 1;
+    a.use_inf = any_inf; a.train = train;
+    a.max_depth = prm.max_depth; a.rr_min_depth = prm.rr_min_depth; a.shadow_mesh = prm.shadow_mesh;
+    a.ws = ws;
+    return enqueue_pass<true>(a, tab, prm, frame, nullptr, sh, tu, stream);
 }
 
 // The launch sequence of one call: its spp x W x H paths in wavefronts of
 // `tu.wavefront` paths, each generate -> (trace -> shade -> shadow) x
 // max_depth -> resolve, on the workspace in `a.ws`.
-int enqueue_pass(PassArgs a, const TfgRenderParams& prm, int frame, TfgColor* img, const LaunchShapes& sh,
-                 const Tuning& tu, cudaStream_t stream) {
+template <bool MS>
+int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm, int frame, TfgColor* img,
+                 const LaunchShapes& sh, const Tuning& tu, cudaStream_t stream) {
+    // one scene: W x H pixels; a batch: the scenes' pixels concatenated (a.W = total, a.H = 1)
     const uint32_t N = (uint32_t)a.W * (uint32_t)a.H;
     const int fmt = prm.tri_format;
     const int ti = threads_index(tu.threads);
     const int bt = kThreadChoices[ti];
-    const size_t smem = trace_smem(a.nprims, bt);
-    const int trace_grid = persistent_grid(sh, sh.trace_occ[fmt][ti], tu);
-    const int shadow_grid = persistent_grid(sh, sh.shadow_occ[fmt][ti], tu);
+    const size_t smem = trace_smem(MS ? 0 : a.nprims, bt);
+    const int trace_grid = persistent_grid(sh, sh.trace_occ[MS][fmt][ti], tu);
+    const int shadow_grid = persistent_grid(sh, sh.shadow_occ[MS][fmt][ti], tu);
+    const int shade_grid = sh.shade_blocks[MS];
     const Workspace& ws = a.ws;
     cudaError_t e = cudaSuccess;
     const bool times = (prm.profile & TFG_PROFILE_TIMES) != 0;
@@ -944,29 +1122,29 @@ int enqueue_pass(PassArgs a, const TfgRenderParams& prm, int frame, TfgColor* im
         const int res_blocks = (int)std::max<uint32_t>(1u, std::min<uint32_t>((resolve_n + 255) / 256, (uint32_t)sh.sms * 8u));
         e = cudaMemsetAsync(ws.counters, 0, 4 * (kMaxBounces + 1) * sizeof(uint32_t), stream);
         if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
-        stage(0, [&] { k_generate<<<gen_blocks, 256, 0, stream>>>(a); });
+        stage(0, [&] { k_generate<MS><<<gen_blocks, 256, 0, stream>>>(a, tab); });
         for (int b = 0; b < prm.max_depth; ++b) {
             stage(1, [&] {
                 if (fmt == 0) {
-                    if (counts) k_trace<0, true><<<trace_grid, bt, smem, stream>>>(a, b);
-                    else k_trace<0, false><<<trace_grid, bt, smem, stream>>>(a, b);
+                    if (counts) k_trace<0, true, MS><<<trace_grid, bt, smem, stream>>>(a, b, tab);
+                    else k_trace<0, false, MS><<<trace_grid, bt, smem, stream>>>(a, b, tab);
                 } else {
-                    if (counts) k_trace<1, true><<<trace_grid, bt, smem, stream>>>(a, b);
-                    else k_trace<1, false><<<trace_grid, bt, smem, stream>>>(a, b);
+                    if (counts) k_trace<1, true, MS><<<trace_grid, bt, smem, stream>>>(a, b, tab);
+                    else k_trace<1, false, MS><<<trace_grid, bt, smem, stream>>>(a, b, tab);
                 }
             });
-            stage(2, [&] { k_shade<<<sh.shade_blocks, 256, 0, stream>>>(a, b); });
+            stage(2, [&] { k_shade<MS><<<shade_grid, 256, 0, stream>>>(a, b, tab); });
             stage(3, [&] {
                 if (fmt == 0) {
-                    if (counts) k_shadow<0, true><<<shadow_grid, bt, smem, stream>>>(a, b);
-                    else k_shadow<0, false><<<shadow_grid, bt, smem, stream>>>(a, b);
+                    if (counts) k_shadow<0, true, MS><<<shadow_grid, bt, smem, stream>>>(a, b, tab);
+                    else k_shadow<0, false, MS><<<shadow_grid, bt, smem, stream>>>(a, b, tab);
                 } else {
-                    if (counts) k_shadow<1, true><<<shadow_grid, bt, smem, stream>>>(a, b);
-                    else k_shadow<1, false><<<shadow_grid, bt, smem, stream>>>(a, b);
+                    if (counts) k_shadow<1, true, MS><<<shadow_grid, bt, smem, stream>>>(a, b, tab);
+                    else k_shadow<1, false, MS><<<shadow_grid, bt, smem, stream>>>(a, b, tab);
                 }
             });
         }
-        stage(4, [&] { k_resolve<<<res_blocks, 256, 0, stream>>>(a); });
+        stage(4, [&] { k_resolve<MS><<<res_blocks, 256, 0, stream>>>(a, tab); });
         e = cudaGetLastError();
         if (e != cudaSuccess) return fail((int)e, std::string("render launch: ") + cudaGetErrorString(e));
     }
@@ -1046,11 +1224,11 @@ int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const 
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     const float4* tr = reinterpret_cast<const float4*>(fmt == TFG_TRIS_REF ? bvh->d_tris : tris_wt);
     if (fmt == 0)
-        k_trace_rays<0><<<sh.sms * sh.trace_occ[0][1], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
+        k_trace_rays<0><<<sh.sms * sh.trace_occ[0][0][1], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
                                                                  reinterpret_cast<const float4*>(rays), (uint32_t)n,
                                                                  reinterpret_cast<float4*>(hits), fetch);
     else
-        k_trace_rays<1><<<sh.sms * sh.trace_occ[1][1], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
+        k_trace_rays<1><<<sh.sms * sh.trace_occ[0][1][1], 128, 0, stream>>>(reinterpret_cast<const float4*>(bvh->d_nodos), tr,
                                                                  reinterpret_cast<const float4*>(rays), (uint32_t)n,
                                                                  reinterpret_cast<float4*>(hits), fetch);
     e = cudaGetLastError();
@@ -1152,6 +1330,31 @@ extern "C" int tfgRenderPass(const TfgRenderParams* params, const TfgCamara* cam
                             params->accumulate ? accum : nullptr, buffer_registros, counter_train, max_cap_train,
                             buffer_inference, buffer_throughput, usar_red_inferencia, entrenar_red,
                             (cudaStream_t)stream);
+}
+
+static_assert(sizeof(TfgRenderScene) == 88, "TfgRenderScene layout");
+
+extern "C" int tfgRenderPassBatch(int32_t n, const TfgRenderScene* scenes, const TfgRenderParams* params,
+                                  int32_t frame_number, void* stream) {
+    using namespace tfg;
+    if (!params) return fail(TFG_E_INVALID, "tfgRenderPassBatch: params is null");
+    if (n < 0 || (n > 0 && !scenes)) return fail(TFG_E_INVALID, "tfgRenderPassBatch: bad scene array");
+    // groups of up to 16 scenes, each one wavefront series
+    for (int g0 = 0; g0 < n; g0 += kMaxBatchScenes) {
+        const int m = std::min(n - g0, kMaxBatchScenes);
+        PassScene ps[kMaxBatchScenes] = {};
+        for (int i = 0; i < m; ++i) {
+            const TfgRenderScene& r = scenes[g0 + i];
+            PassScene& c = ps[i];
+            c.cam = r.camara; c.prims = r.primitivas; c.nprims = r.num_primitivas;
+            c.lights = r.luces; c.nlights = r.num_luces; c.W = r.ancho_img; c.H = r.alto_img;
+            c.bvh = r.nodos_bvh; c.tris_wt = r.tris_wt; c.mesh = r.primitivas_bvh; c.nmesh = r.num_prims_bvh;
+            c.img = r.imagen; c.accum = params->accumulate ? r.accum : nullptr;
+        }
+        if (int rc = render_pass_multi(*params, ps, m, frame_number, nullptr, 0, false, 0, (cudaStream_t)stream))
+            return rc;
+    }
+    return ok();
 }
 
 extern "C" int tfgTraceRays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int32_t tri_format, const float* rays,
@@ -1265,6 +1468,6 @@ extern "C" int tfgRenderPassStatic(const TfgRenderParams* params, const TfgCamar
     a.accum = prm.accumulate ? accum : nullptr;
     a.max_depth = prm.max_depth; a.rr_min_depth = prm.rr_min_depth; a.shadow_mesh = prm.shadow_mesh;
     a.ws = ws;
-    return enqueue_pass(a, prm, frame_number, imagen_directa ? imagen_directa->datos : nullptr, sh, tu,
-                        (cudaStream_t)stream);
+    return enqueue_pass<false>(a, NoTable{}, prm, frame_number, imagen_directa ? imagen_directa->datos : nullptr, sh,
+                               tu, (cudaStream_t)stream);
 }

@@ -36,6 +36,22 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
 // captured before holds stale queue pointers then.
 uint32_t workspace_generation(int dev, int slot);
 
+// One scene of a batched pass.
+struct PassScene {
+    const TfgCamara* cam; const TfgPrimitiva* prims; int nprims;
+    const TfgLuzPuntual* lights; int nlights; int W, H;
+    const TfgTinyBVHD_GPU* bvh; const float* tris_wt; const TfgPrimitiva* mesh; int nmesh;
+    TfgColor* img; float* accum;
+    TfgRegistroEntrenamiento* regs; uint32_t* reg_counter; int reg_cap;
+    TfgDatosMLP* infer; TfgColor* thr_out;
+    const uint32_t* use_inf_dev; int use_inf;
+};
+
+// 1 to 16 scenes with the same settings rendered as one wavefront series
+// (one launch per stage for all of them), on workspace slot `ws_slot`.
+int render_pass_multi(const TfgRenderParams& prm, const PassScene* scenes, int n, int frame, const int32_t* frame_dev,
+                      int train, bool prepare_only, int ws_slot, cudaStream_t stream);
+
 // Launch tuning of device `dev` (render.cu).  The generation number changes
 // with every successful set.
 int render_tuning_check(const TfgRenderTuning& t);

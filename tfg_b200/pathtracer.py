@@ -16,8 +16,8 @@ import torch
 
 from . import _lib
 from .scenes import Scene
-from .structs import (CImagenGPU, CRenderParams, CRenderProfile, CRenderTuning, CTinyBVH, CTinyBVHD_GPU,
-                      CTuneRecord, DATOS_MLP, REGISTRO)
+from .structs import (CImagenGPU, CRenderParams, CRenderProfile, CRenderScene, CRenderTuning, CTinyBVH,
+                      CTinyBVHD_GPU, CTuneRecord, DATOS_MLP, REGISTRO)
 
 TRIS_REF, TRIS_WATERTIGHT = 0, 1
 PROFILE_TIMES, PROFILE_COUNTS = 1, 2
@@ -145,6 +145,24 @@ def render_pass(ds: DeviceScene, params: RenderParams, frame: int, img: torch.Te
               _ptr(accum), _ptr(nrc.regs) if nrc else None, _ptr(nrc.counter) if nrc else None,
               nrc.cap if nrc else 0, _ptr(nrc.infer) if nrc else None, _ptr(nrc.thr) if nrc else None,
               int(use_inf), int(train), _stream(stream))
+
+
+def render_pass_batch(dss: list, params: RenderParams, frame: int, imgs: list | None = None,
+                      accums: list | None = None, stream=None) -> None:
+    """tfgRenderPassBatch: plain path tracing of several scenes, each stage
+    launched once for all of them; imgs / accums: per scene (or None)."""
+    n = len(dss)
+    arr = (CRenderScene * n)()
+    for k, ds in enumerate(dss):
+        f = arr[k]
+        f.camara, f.primitivas, f.num_primitivas = _ptr(ds.camera), _ptr(ds.prims), ds.n_prims
+        f.luces, f.num_luces = _ptr(ds.lights), ds.n_lights
+        f.ancho_img, f.alto_img = ds.scene.width, ds.scene.height
+        f.nodos_bvh = ctypes.addressof(ds.bvh.ref)
+        f.tris_wt, f.primitivas_bvh, f.num_prims_bvh = ds.bvh.d_tris_wt, ds.bvh.d_primitivas, ds.n_mesh
+        f.imagen = _ptr(imgs[k]) if imgs is not None else None
+        f.accum = _ptr(accums[k]) if accums is not None else None
+    _lib.call("tfgRenderPassBatch", n, arr, ctypes.byref(params.c()), frame, _stream(stream))
 
 
 def render_pass_static(ds: DeviceScene, params: RenderParams, frame: int, img: torch.Tensor | None = None,

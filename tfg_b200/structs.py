@@ -96,6 +96,17 @@ class CRenderProfile(ctypes.Structure):
                 ("shadow_nodes", ctypes.c_uint64), ("shadow_tri_tests", ctypes.c_uint64)]
 
 
+class CRenderScene(ctypes.Structure):
+    _fields_ = [("camara", ctypes.c_void_p), ("primitivas", ctypes.c_void_p), ("num_primitivas", ctypes.c_int32),
+                ("num_luces", ctypes.c_int32), ("luces", ctypes.c_void_p), ("ancho_img", ctypes.c_int32),
+                ("alto_img", ctypes.c_int32), ("nodos_bvh", ctypes.c_void_p), ("tris_wt", ctypes.c_void_p),
+                ("primitivas_bvh", ctypes.c_void_p), ("num_prims_bvh", ctypes.c_int32), ("reserved", ctypes.c_int32),
+                ("imagen", ctypes.c_void_p), ("accum", ctypes.c_void_p)]
+
+
+assert ctypes.sizeof(CRenderScene) == 88
+
+
 class CRenderTuning(ctypes.Structure):
     _fields_ = [("wavefront_paths", ctypes.c_int32), ("trace_threads", ctypes.c_int32),
                 ("trace_warps_per_sm", ctypes.c_int32), ("refill_min", ctypes.c_int32),
