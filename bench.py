@@ -773,21 +773,29 @@ def main():
     wall_ms = (time.perf_counter() - t0) * 1e3
     e2e_value = world * n_px * SPP * e2e_steps / (e2e_ms * 1e-3) / 1e6
 
-    # Primary-ray traversal throughput (rays resident in HBM): the traversal-only entry.
-    rays = torch.empty(n_px * 8, dtype=torch.float32, device=dev)
-    hits = torch.empty(n_px * 4, dtype=torch.float32, device=dev)
-    pt.camera_rays(ds, 0, rays)
-    for _ in range(3):
-        pt.trace_rays(ds, rays, hits, pt.TRIS_WATERTIGHT)
-    torch.cuda.synchronize()
-    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    reps = 10
-    p0.record(stream)
-    for _ in range(reps):
-        pt.trace_rays(ds, rays, hits, pt.TRIS_WATERTIGHT)
-    p1.record(stream)
-    torch.cuda.synchronize()
-    primary_grays = n_px * reps / (p0.elapsed_time(p1) * 1e-3) / 1e9
+    # Primary-ray traversal throughput (rays resident in HBM) through the
+    # traversal-only entry: the primary rays of as many samples per call as
+    # the tuned wavefront holds, in the path tracer's 8 x 4 tile order, and
+    # one sample per call (scanline and tile order) for comparison.
+    def primary(samples: int, order: int, reps: int = 10) -> float:
+        rays = torch.empty(samples * n_px * 8, dtype=torch.float32, device=dev)
+        hits = torch.empty(samples * n_px * 4, dtype=torch.float32, device=dev)
+        pt.camera_rays_ex(ds, 0, samples, order, rays)
+        for _ in range(3):
+            pt.trace_rays(ds, rays, hits, pt.TRIS_WATERTIGHT)
+        torch.cuda.synchronize()
+        p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        p0.record(stream)
+        for _ in range(reps):
+            pt.trace_rays(ds, rays, hits, pt.TRIS_WATERTIGHT)
+        p1.record(stream)
+        torch.cuda.synchronize()
+        del rays, hits
+        return samples * n_px * reps / (p0.elapsed_time(p1) * 1e-3) / 1e9
+
+    primary_samples = max(1, min(16, tuning.wavefront_paths // n_px)) if tuning.wavefront_paths else 1
+    primary_grays = primary(primary_samples, pt.RAYS_TILES)
+    primary_one = {"scanline": round(primary(1, pt.RAYS_SCANLINE), 3), "tiles": round(primary(1, pt.RAYS_TILES), 3)}
 
     if rank != 0:
         ds.close()
@@ -862,14 +870,18 @@ def main():
             "ms_per_launch_avg": round(trace_ms / max(1, trace_launches), 4),
             "stage_ms": {k: round(v, 2) for k, v in prof["ms"].items()},
         },
-        "primary_rays": {"grays_per_s": round(primary_grays, 3), "rays": n_px, "tri_test": "watertight"},
+        "primary_rays": {"grays_per_s": round(primary_grays, 3), "rays_per_call": primary_samples * n_px,
+                         "samples_per_call": primary_samples, "order": "8x4 tiles", "tri_test": "watertight",
+                         "grays_per_s_one_sample_per_call": primary_one,
+                         "note": "a call of one sample (2,073,600 rays) waits on its few longest grazing rays; "
+                                 "more samples per call amortise that tail"},
         "autotune": {
             "tuning": tuning.__dict__, "seconds": round(tune_s, 2), "spp_per_pass": min(SPP, 16),
             "pass_ms_start": round(tune_table[0][1], 3), "pass_ms_tuned": round(tuned_ms, 3),
             "candidates": [[t.wavefront_paths, t.trace_threads, t.trace_warps_per_sm, t.refill_min,
-                            t.shadow_one_lane, round(ms, 3)] for t, ms in tune_table],
+                            t.shadow_one_lane, t.refill_min_primary, round(ms, 3)] for t, ms in tune_table],
             "candidate_fields": ["wavefront_paths", "trace_threads", "trace_warps_per_sm", "refill_min",
-                                 "shadow_one_lane", "ms_per_pass"],
+                                 "shadow_one_lane", "refill_min_primary", "ms_per_pass"],
         },
         "gpu_launches": launches,
         "clocks": clocks,

@@ -337,7 +337,9 @@ typedef struct TfgRenderTuning {
     int32_t refill_min;         /* idle lanes that make a traversal warp fetch new rays, 1..32 (default 8) */
     int32_t shadow_one_lane;    /* threads per shadow query: 0 (default) = one lane per light (up to 32
                                    lights), 1 = one lane traces all lights of a shading point */
-    int32_t reserved[3];
+    int32_t refill_min_primary; /* refill threshold of the first bounce's traversal (camera rays, coherent
+                                   in 8 x 4 pixel tiles; 32 = whole-warp batches), 0 (default) = refill_min */
+    int32_t reserved[2];
 } TfgRenderTuning;
 
 void tfgRenderTuningDefault(TfgRenderTuning* t);
@@ -356,7 +358,8 @@ typedef struct TfgTuneRecord {
 /* The autotuner: times plain passes of this scene (no image written; the
  * call's spp capped at 16) under candidate tunings with CUDA events on
  * `stream`, one setting at a time starting from the current one (queue size,
- * then CTA size, warps per SM, refill threshold, shadow lanes), `repeats`
+ * then CTA size, warps per SM, refill threshold, shadow lanes, first-bounce
+ * refill threshold), `repeats`
  * timed passes per candidate after one warm-up (0 = 3).  A candidate must be
  * at least 1% faster to replace the best.  Sets the winner on the current
  * device and returns it in `out`.  `num_records` (optional) gets the number
@@ -368,6 +371,20 @@ int  tfgRenderAutotune(const TfgRenderParams* params, const TfgCamara* camara, c
                        const TfgPrimitiva* primitivas_bvh, int32_t num_prims_bvh, int32_t repeats,
                        TfgRenderTuning* out, TfgTuneRecord* records, int32_t max_records, int32_t* num_records,
                        void* stream);
+
+/* No reference counterpart: camera rays of `samples` consecutive samples
+ * (frames frame_number .. frame_number + samples - 1), sample-major, each
+ * sample's W*H rays in `order`: TFG_RAYS_SCANLINE (ray l starts at pixel l,
+ * as tfgGenerateCameraRays) or TFG_RAYS_TILES, the path tracer's order (ray l
+ * starts at pixel tfgTiledPixel(l, W, H): 8 x 4 pixel tiles, so a warp's 32
+ * rays are coherent).  At most 2^31 rays. */
+enum { TFG_RAYS_SCANLINE = 0, TFG_RAYS_TILES = 1 };
+int tfgGenerateCameraRaysEx(const TfgCamara* camara, int32_t ancho_img, int32_t alto_img, int32_t frame_number,
+                            int32_t samples, int32_t order, float* rays, void* stream);
+/* Pixel index (y * W + x) of the l-th path or ray of a sample in tile
+ * order: bands of 4 rows cut into 8 x 4 tiles left to right; 0xFFFFFFFF when
+ * l >= W*H. */
+uint32_t tfgTiledPixel(uint32_t l, uint32_t ancho_img, uint32_t alto_img);
 
 /* launchInicializarCamara (RenderKernel.cu:68-90): default 45-degree camera
  * at (0,-0.75,4.25) looking down -z, written to device pointer d_camara. */

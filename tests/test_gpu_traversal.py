@@ -157,3 +157,27 @@ def test_empty_batch_and_all_miss(setup):
     h = _trace(ds, r.reshape(-1), pt.TRIS_WATERTIGHT)
     assert (h[:, 3].view(np.uint32) == MISS).all() and (h[:, 0] == 1e9).all()
     pt.trace_rays(ds, torch.zeros(0, device="cuda"), torch.zeros(0, device="cuda"))
+
+
+def test_camera_rays_in_samples_and_tile_order(setup):
+    scene, ds, _, _ = setup
+    W, H = scene.width, scene.height
+    n = W * H
+    single = []
+    for f in range(5, 8):
+        r = torch.zeros(n * 8, device="cuda")
+        pt.camera_rays(ds, f, r)
+        single.append(r.view(-1, 8))
+    lin = torch.zeros(3 * n * 8, device="cuda")
+    pt.camera_rays_ex(ds, 5, 3, pt.RAYS_SCANLINE, lin)
+    til = torch.zeros(3 * n * 8, device="cuda")
+    pt.camera_rays_ex(ds, 5, 3, pt.RAYS_TILES, til)
+    torch.cuda.synchronize()
+    perm = torch.from_numpy(pt.tiled_pixels(W, H)).cuda()
+    for s in range(3):
+        assert torch.equal(lin.view(-1, 8)[s * n:(s + 1) * n], single[s])
+        assert torch.equal(til.view(-1, 8)[s * n:(s + 1) * n], single[s][perm])
+    # tile order hits the same primitives as scanline order, ray for ray
+    hl, ht = _trace(ds, lin, pt.TRIS_WATERTIGHT), _trace(ds, til, pt.TRIS_WATERTIGHT)
+    p3 = np.concatenate([perm.cpu().numpy() + s * n for s in range(3)])
+    assert np.array_equal(ht[:, 3].view(np.uint32), hl[p3, 3].view(np.uint32))

@@ -58,6 +58,8 @@ TUNINGS = [
     pt.RenderTuning(refill_min=1),
     pt.RenderTuning(refill_min=32),
     pt.RenderTuning(shadow_one_lane=1),
+    pt.RenderTuning(refill_min_primary=32),
+    pt.RenderTuning(refill_min_primary=2, refill_min=29),
     pt.RenderTuning(wavefront_paths=2 * N + 1000, trace_threads=256, trace_warps_per_sm=16, refill_min=12,
                     shadow_one_lane=1),
 ]
@@ -141,7 +143,8 @@ def test_cache_frames_under_tuning(scene, graph):
 def test_bad_tunings_are_rejected(built):
     for bad in (pt.RenderTuning(wavefront_paths=100), pt.RenderTuning(wavefront_paths=(1 << 26) + 1),
                 pt.RenderTuning(trace_threads=96), pt.RenderTuning(refill_min=0), pt.RenderTuning(refill_min=33),
-                pt.RenderTuning(trace_warps_per_sm=-1), pt.RenderTuning(shadow_one_lane=2)):
+                pt.RenderTuning(trace_warps_per_sm=-1), pt.RenderTuning(shadow_one_lane=2),
+                pt.RenderTuning(refill_min_primary=33)):
         with pytest.raises(TfgError):
             pt.set_tuning(bad)
     assert pt.get_tuning() == pt.RenderTuning.default()
@@ -152,7 +155,7 @@ def test_autotune_picks_a_measured_tuning(scene):
     want_img, want_acc = _render(ds)
     best, table = pt.autotune(ds, PARAMS, repeats=2)
     assert pt.get_tuning() == best
-    assert len(table) >= 12
+    assert len(table) >= 15
     assert all(ms > 0 for _, ms in table)
     tried = [t for t, _ in table]
     assert best in tried

@@ -67,6 +67,8 @@ _PROTOS = {
         POINTER(CTinyBVHD_GPU), c_void_p, c_void_p, c_int32, POINTER(CImagenGPU), c_void_p, c_void_p]),
     "tfgTraceRays": (c_int32, [POINTER(CTinyBVHD_GPU), c_void_p, c_int32, c_void_p, c_int32, c_void_p, c_void_p]),
     "tfgGenerateCameraRays": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
+    "tfgGenerateCameraRaysEx": (c_int32, [c_void_p, c_int32, c_int32, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
+    "tfgTiledPixel": (c_uint32, [c_uint32, c_uint32, c_uint32]),
     "tfgLaunchInicializarCamara": (c_int32, [c_void_p, c_int32, c_int32, c_void_p]),
     "tfgLaunchKernelComposite": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_int32, c_void_p]),
     "tfgLaunchKernelCalcularTargets": (c_int32, [c_void_p, c_void_p, c_void_p, c_int32, c_void_p]),

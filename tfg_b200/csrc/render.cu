@@ -99,6 +99,7 @@ struct PassArgs {
     uint32_t npix, nq, p0;
     int s0, last_sample;      // samples relative to `frame`; the last one writes `img`
     int refill_min;           // idle lanes that trigger a traversal warp's refill
+    int refill_primary;       // the same for the first bounce
     int shadow_one_lane;      // 1: one lane traces all lights of a shading point
     Workspace ws;
 };
@@ -172,8 +173,29 @@ __device__ __forceinline__ uint32_t scene_of_pixel(const SceneTable& tab, uint32
     return sc;
 }
 
-// Pixel of the path in wavefront slot `slot`.
-__device__ __forceinline__ uint32_t pixel_of(const PassArgs& a, uint32_t slot) { return (a.p0 + slot) % a.npix; }
+// Pixel (y * W + x) of the l-th path of a sample of a W x H image: bands of
+// 4 rows cut into 8 x 4 tiles left to right (the band's last tile narrower
+// when W is not a multiple of 8, the last band lower when H is not a
+// multiple of 4), so the 32 paths of a warp start from one 8 x 4 block of
+// pixels and their primary and first shadow rays stay coherent.  A
+// bijection on [0, W*H).
+__host__ __device__ __forceinline__ uint32_t tiled_pixel(uint32_t l, uint32_t W, uint32_t H) {
+    const uint32_t band = l / (4u * W), y0 = 4u * band;
+    const uint32_t h = H - y0 < 4u ? H - y0 : 4u;
+    const uint32_t o = l - band * 4u * W;
+    const uint32_t full = W / 8u;
+    uint32_t x, y;
+    if (o < full * 8u * h) {
+        const uint32_t tc = o / (8u * h), i = o - tc * 8u * h;
+        x = 8u * tc + (i & 7u);
+        y = y0 + (i >> 3);
+    } else {
+        const uint32_t wr = W - 8u * full, i = o - full * 8u * h;
+        x = 8u * full + i % wr;
+        y = y0 + i / wr;
+    }
+    return y * W + x;
+}
 
 // Warp-aggregated queue append: every lane with `want` gets a unique slot.
 __device__ __forceinline__ uint32_t warp_append(uint32_t* counter, bool want) {
@@ -255,6 +277,7 @@ __global__ void k_generate(PassArgs a, TableOf<MS> tab) {
             cam = *d.cam;
             use_inf = use_inf_of(d);
         }
+        pix = tiled_pixel(pix, (uint32_t)W, (uint32_t)H);
         const int x = (int)(pix % (uint32_t)W), y = (int)(pix / (uint32_t)W);
         uint32_t rng = seed_pixel(x, y, frame0 + (int)s);
         const float ox = pcg_uniform(rng);
@@ -270,7 +293,7 @@ __global__ void k_generate(PassArgs a, TableOf<MS> tab) {
         a.ws.ray[0][2 * p + 0] = make_float4(O.x, O.y, O.z, MS ? __uint_as_float(sc) : 1e9f);
         a.ws.ray[0][2 * p + 1] = make_float4(D.x, D.y, D.z, __uint_as_float(p));
         a.ws.thr[p] = make_float4(1.0f, 1.0f, 1.0f, 1.0f);
-        a.ws.st[p] = make_uint4(rng, flags, __float_as_uint(1.0f), 0u);
+        a.ws.st[p] = make_uint4(rng, flags, __float_as_uint(1.0f), pix);   // w: the path's pixel in its image
         a.ws.lpre[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
         if (a.use_inf || a.train) {
             a.ws.lsuf[p] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -300,6 +323,7 @@ __global__ void __launch_bounds__(256) k_trace(PassArgs a, int bounce, TableOf<M
     // a.refill_min lanes of its warp are idle, instead of waiting for the
     // slowest ray of a 32-ray batch.
     const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
+    const int refill = bounce == 0 ? a.refill_primary : a.refill_min;
     CwbvhRay<TRI_FMT, false> r;
     uint32_t cur = kMissId, bid = kMissId;
     float best = 0.0f, bu = 0.0f, bv = 0.0f;
@@ -309,7 +333,7 @@ __global__ void __launch_bounds__(256) k_trace(PassArgs a, int bounce, TableOf<M
         const uint32_t im = __ballot_sync(0xFFFFFFFFu, idle);
         if (exhausted) {
             if (im == 0xFFFFFFFFu) break;
-        } else if (__popc(im) >= a.refill_min) {
+        } else if (__popc(im) >= refill) {
             uint32_t base = 0;
             if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(im));
             base = __shfl_sync(0xFFFFFFFFu, base, 0);
@@ -464,8 +488,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<M
                         const bool training = (flags & F_TRAIN) != 0;
                         if (!training && use_inf) {
                             const Outs o = outs_of<MS>(a, tab, sc);
-                            uint32_t px = pixel_of(a, p);
-                            if constexpr (MS) px -= tab.s[sc].pix0;
+                            const uint32_t px = st.w;
                             write_datos(&o.infer[px], P, map01(view), map01(nrm), m.difuso, m.especular);
                             const V3 tt = mul(cam, refl);
                             o.thr_out[px] = TfgColor{tt.x, tt.y, tt.z};
@@ -532,7 +555,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<M
                 }
             }
             a.ws.thr[p] = make_float4(cam.x, cam.y, cam.z, ior);
-            a.ws.st[p] = make_uint4(rng, flags, __float_as_uint(pdf_last), 0u);
+            a.ws.st[p] = make_uint4(rng, flags, __float_as_uint(pdf_last), st.w);
             a.ws.lpre[p] = lpre;
             if (nrc) { a.ws.lsuf[p] = lsuf; a.ws.nrc[p] = nrc4; }
             nr0 = make_float4(O.x, O.y, O.z, MS ? __uint_as_float(sc) : 1e9f);
@@ -663,7 +686,9 @@ __global__ void k_resolve(PassArgs a, TableOf<MS> tab) {
     for (uint32_t j = blockIdx.x * blockDim.x + threadIdx.x; j < first; j += gridDim.x * blockDim.x) {
         const uint32_t q = a.p0 + j, s_rel = q / N;
         uint32_t px = q - s_rel * N, sc = 0;
-        if constexpr (MS) { sc = scene_of_pixel(tab, px); px -= tab.s[sc].pix0; }
+        uint32_t W = (uint32_t)a.W, H = (uint32_t)a.H;
+        if constexpr (MS) { sc = scene_of_pixel(tab, px); px -= tab.s[sc].pix0; W = tab.s[sc].W; H = tab.s[sc].H; }
+        px = tiled_pixel(px, W, H);
         const Outs o = outs_of<MS>(a, tab, sc);
         int sample = a.s0 + (int)s_rel;
         for (uint32_t p = j; p < a.nq; p += N, ++sample) {
@@ -821,7 +846,7 @@ int shapes_for(int dev, LaunchShapes& s) {
 // whose per-pixel outputs take one sample per pixel at a time).
 struct Tuning {
     uint32_t wavefront = 0;
-    int threads = 128, warps_per_sm = 0, refill = 8, shadow_one_lane = 0;
+    int threads = 128, warps_per_sm = 0, refill = 8, refill_primary = 8, shadow_one_lane = 0;
 };
 
 Tuning resolve_tuning(int dev, uint32_t npix, int spp, bool nrc, uint32_t* generation) {
@@ -840,6 +865,7 @@ Tuning resolve_tuning(int dev, uint32_t npix, int spp, bool nrc, uint32_t* gener
     r.threads = t.trace_threads;
     r.warps_per_sm = t.trace_warps_per_sm;
     r.refill = t.refill_min;
+    r.refill_primary = t.refill_min_primary > 0 ? t.refill_min_primary : t.refill_min;
     r.shadow_one_lane = t.shadow_one_lane;
     return r;
 }
@@ -864,6 +890,8 @@ int render_tuning_check(const TfgRenderTuning& t) {
     if (t.refill_min < 1 || t.refill_min > 32) return fail(TFG_E_INVALID, "render tuning: refill_min must be in [1, 32]");
     if (t.shadow_one_lane != 0 && t.shadow_one_lane != 1)
         return fail(TFG_E_INVALID, "render tuning: shadow_one_lane must be 0 or 1");
+    if (t.refill_min_primary < 0 || t.refill_min_primary > 32)
+        return fail(TFG_E_INVALID, "render tuning: refill_min_primary must be in [0, 32]");
     return ok();
 }
 
@@ -1111,6 +1139,7 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
     a.npix = N;
     a.last_sample = prm.spp - 1;
     a.refill_min = tu.refill;
+    a.refill_primary = tu.refill_primary;
     a.shadow_one_lane = tu.shadow_one_lane;
     const uint64_t total = (uint64_t)prm.spp * N;
     for (uint64_t q0 = 0; q0 < total; q0 += tu.wavefront) {
@@ -1152,6 +1181,8 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
 }
 
 // ------------------------------------------------------------------ traversal-only entries
+// tfgTraceRays: closest hit of a batch of rays, 32 consecutive rays per warp
+// (coherent when the rays come in tile order).
 template <int TRI_FMT>
 __global__ void __launch_bounds__(128) k_trace_rays(const float4* __restrict__ nodes, const float4* __restrict__ tris,
                                                     const float4* __restrict__ rays, uint32_t n, float4* __restrict__ hits,
@@ -1177,12 +1208,17 @@ __global__ void __launch_bounds__(128) k_trace_rays(const float4* __restrict__ n
     }
 }
 
-__global__ void k_camera_rays(const TfgCamara* camp, int W, int H, int frame, float4* rays) {
+// Camera rays of `samples` samples, sample-major; within a sample in
+// scanline order or in the path tracer's 8 x 4 tile order.
+__global__ void k_camera_rays(const TfgCamara* camp, int W, int H, int frame, int samples, int tiles, float4* rays) {
     const uint32_t N = (uint32_t)W * (uint32_t)H;
+    const uint64_t total = (uint64_t)N * (uint32_t)samples;
     const TfgCamara cam = *camp;
-    for (uint32_t p = blockIdx.x * blockDim.x + threadIdx.x; p < N; p += gridDim.x * blockDim.x) {
-        const int x = (int)(p % (uint32_t)W), y = (int)(p / (uint32_t)W);
-        uint32_t rng = seed_pixel(x, y, frame);
+    for (uint64_t p = blockIdx.x * blockDim.x + threadIdx.x; p < total; p += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t s = (uint32_t)(p / N), l = (uint32_t)(p - (uint64_t)s * N);
+        const uint32_t pix = tiles ? tiled_pixel(l, (uint32_t)W, (uint32_t)H) : l;
+        const int x = (int)(pix % (uint32_t)W), y = (int)(pix / (uint32_t)W);
+        uint32_t rng = seed_pixel(x, y, frame + (int)s);
         const float ox = pcg_uniform(rng);
         const float oy = pcg_uniform(rng);
         V3 O, D;
@@ -1236,14 +1272,21 @@ int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const 
     return ok();
 }
 
-int camera_rays(const TfgCamara* d_cam, int W, int H, int frame, float* rays, cudaStream_t stream) {
+int camera_rays(const TfgCamara* d_cam, int W, int H, int frame, int samples, int order, float* rays,
+                cudaStream_t stream) {
     if (!d_cam || !rays || W <= 0 || H <= 0) return fail(TFG_E_INVALID, "tfgGenerateCameraRays: bad argument");
+    if (samples < 1 || (uint64_t)W * (uint64_t)H * (uint64_t)samples > (1ull << 31))
+        return fail(TFG_E_INVALID, "tfgGenerateCameraRays: samples out of range");
+    if (order != TFG_RAYS_SCANLINE && order != TFG_RAYS_TILES)
+        return fail(TFG_E_INVALID, "tfgGenerateCameraRays: unknown ray order");
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     if (int rc = require_sm100(dev)) return rc;
-    const int blocks = std::max(1, std::min((W * H + 255) / 256, 148 * 8));
-    k_camera_rays<<<blocks, 256, 0, stream>>>(d_cam, W, H, frame, reinterpret_cast<float4*>(rays));
+    const int blocks = (int)std::max<uint64_t>(
+        1, std::min<uint64_t>(((uint64_t)W * (uint64_t)H * (uint64_t)samples + 255) / 256, 148 * 8));
+    k_camera_rays<<<blocks, 256, 0, stream>>>(d_cam, W, H, frame, samples, order == TFG_RAYS_TILES ? 1 : 0,
+                                              reinterpret_cast<float4*>(rays));
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
     return ok();
@@ -1272,6 +1315,7 @@ extern "C" void tfgRenderTuningDefault(TfgRenderTuning* t) {
     t->trace_warps_per_sm = 0;
     t->refill_min = 8;
     t->shadow_one_lane = 0;
+    t->refill_min_primary = 0;
 }
 
 extern "C" int tfgRenderTuningSet(const TfgRenderTuning* t) {
@@ -1364,7 +1408,18 @@ extern "C" int tfgTraceRays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, in
 
 extern "C" int tfgGenerateCameraRays(const TfgCamara* camara, int32_t ancho_img, int32_t alto_img, int32_t frame_number,
                                      float* rays, void* stream) {
-    return tfg::camera_rays(camara, ancho_img, alto_img, frame_number, rays, (cudaStream_t)stream);
+    return tfg::camera_rays(camara, ancho_img, alto_img, frame_number, 1, TFG_RAYS_SCANLINE, rays, (cudaStream_t)stream);
+}
+
+extern "C" int tfgGenerateCameraRaysEx(const TfgCamara* camara, int32_t ancho_img, int32_t alto_img,
+                                       int32_t frame_number, int32_t samples, int32_t order, float* rays,
+                                       void* stream) {
+    return tfg::camera_rays(camara, ancho_img, alto_img, frame_number, samples, order, rays, (cudaStream_t)stream);
+}
+
+extern "C" uint32_t tfgTiledPixel(uint32_t l, uint32_t ancho_img, uint32_t alto_img) {
+    if (ancho_img == 0 || alto_img == 0 || l >= ancho_img * alto_img) return 0xFFFFFFFFu;
+    return tfg::tiled_pixel(l, ancho_img, alto_img);
 }
 
 // ------------------------------------------------------------------ allocation-free render pass

@@ -61,7 +61,8 @@ int render_tuning_get(int dev, TfgRenderTuning* out, uint32_t* generation);
 int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const float* rays, int n, float* hits,
                cudaStream_t stream);
 
-int camera_rays(const TfgCamara* d_cam, int W, int H, int frame, float* rays, cudaStream_t stream);
+int camera_rays(const TfgCamara* d_cam, int W, int H, int frame, int samples, int order, float* rays,
+                cudaStream_t stream);
 
 // Small frame kernels with a device-side count: 0 tail queries (a = records,
 // b = DatosMLP out), 1 targets (a = records, c = tail predictions, b = out),

@@ -182,6 +182,21 @@ def camera_rays(ds: DeviceScene, frame: int, rays: torch.Tensor, stream=None) ->
     _lib.call("tfgGenerateCameraRays", _ptr(ds.camera), W, H, frame, _ptr(rays), _stream(stream))
 
 
+RAYS_SCANLINE, RAYS_TILES = 0, 1
+
+
+def camera_rays_ex(ds: DeviceScene, frame: int, samples: int, order: int, rays: torch.Tensor, stream=None) -> None:
+    """tfgGenerateCameraRaysEx: `samples` samples of camera rays, sample-major,
+    scanline or 8 x 4 tile order (rays: samples*W*H*8 floats)."""
+    W, H = ds.scene.width, ds.scene.height
+    _lib.call("tfgGenerateCameraRaysEx", _ptr(ds.camera), W, H, frame, samples, order, _ptr(rays), _stream(stream))
+
+
+def tiled_pixels(W: int, H: int) -> np.ndarray:
+    """Pixel index of every position of a sample in tile order (tfgTiledPixel)."""
+    return np.array([_lib.lib.tfgTiledPixel(i, W, H) for i in range(W * H)], dtype=np.int64)
+
+
 def trace_rays(ds: DeviceScene, rays: torch.Tensor, hits: torch.Tensor, tri_format: int = TRIS_WATERTIGHT,
                stream=None) -> None:
     n = rays.numel() // 8
@@ -245,18 +260,20 @@ class RenderTuning:
     trace_warps_per_sm: int = 0   # resident traversal warps per SM; 0 = as many as fit
     refill_min: int = 8           # idle lanes that make a traversal warp fetch new rays
     shadow_one_lane: int = 0      # 1: one lane traces all lights of a shading point
+    refill_min_primary: int = 0   # first-bounce refill threshold; 0 = refill_min
 
     def c(self) -> CRenderTuning:
         t = CRenderTuning()
         t.wavefront_paths, t.trace_threads, t.trace_warps_per_sm = (self.wavefront_paths, self.trace_threads,
                                                                     self.trace_warps_per_sm)
         t.refill_min, t.shadow_one_lane = self.refill_min, self.shadow_one_lane
+        t.refill_min_primary = self.refill_min_primary
         return t
 
     @staticmethod
     def of(t: CRenderTuning) -> "RenderTuning":
         return RenderTuning(int(t.wavefront_paths), int(t.trace_threads), int(t.trace_warps_per_sm),
-                            int(t.refill_min), int(t.shadow_one_lane))
+                            int(t.refill_min), int(t.shadow_one_lane), int(t.refill_min_primary))
 
     @staticmethod
     def default() -> "RenderTuning":
