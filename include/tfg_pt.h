@@ -450,6 +450,38 @@ int  tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, 
  * same model with 3, 5 (= tfgMlpCreate) or 7 hidden layers of 64 units. */
 int  tfgMlpCreateEx(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
                     TfgColorMLP** out);
+/* The reference's own cache input (mlp.cpp:22-49): a multiresolution hash
+ * grid on the position, one-blob on direction and normal, identity on the
+ * albedos.  Reference settings (tfgHashGridConfigReference): 16 levels of 2
+ * features, 2^19 entries per level, base resolution 16, per-level scale 1.5,
+ * 4 one-blob bins. */
+typedef struct TfgHashGridConfig {
+    int32_t n_levels;            /* 1..16 */
+    int32_t log2_hashmap_size;   /* 10..24: entries per level */
+    float   base_resolution;     /* cells per axis at level 0 (>= 2) */
+    float   per_level_scale;     /* >= 1 */
+    int32_t reserved[4];
+} TfgHashGridConfig;
+void tfgHashGridConfigReference(TfgHashGridConfig* c);
+/* tfgMlpCreateEx with the composite encoding instead of the frequency
+ * encoding; the tables (2 features x n_levels x 2^log2_hashmap_size FP32
+ * values, uniform in +-1e-4 from `seed`) train with the same Adam and weight
+ * average as the layers.  Inference in FP16, BF16 or FP8 reads an FP16 image
+ * of the tables' debiased average. */
+int  tfgMlpCreateHashGrid(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
+                          const TfgHashGridConfig* config, TfgColorMLP** out);
+/* Length of the FP32 table arrays (0 for the frequency encoding). */
+int64_t tfgMlpHashParamCount(const TfgColorMLP* mlp);
+/* Table arrays [level][entry][feature]: which = 0 values, 1 average, 2 Adam m, 3 Adam v. */
+int  tfgMlpGetHashParams(TfgColorMLP* mlp, int which, float* host, int64_t count);
+/* Set the table values and restart the optimiser as tfgMlpSetParams does
+ * (moments and averages of layers and tables cleared, step 0). */
+int  tfgMlpSetHashParams(TfgColorMLP* mlp, const float* host, int64_t count);
+/* tfgMlpComputeGradient that also returns the tables' gradient
+ * (`host_table_grad`, tfgMlpHashParamCount floats; may be null). */
+int  tfgMlpComputeGradientEx(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
+                             float* host_grad, uint32_t count, float* host_table_grad, int64_t table_count,
+                             float* loss_out);
 /* Length of the model's FP32 parameter arrays: 6144 + 4096 (hidden - 1) +
  * 1024 (23552 for 5 hidden layers). */
 int32_t tfgMlpParamCount(const TfgColorMLP* mlp);

@@ -6,10 +6,22 @@ time Neural Radiance Caching for Path Tracing"; Kingma & Ba 2015) for the
 network the product kernels implement: 12-band frequency encoding of the
 normalised position + 12 raw inputs + constant 1 -> 5 x 64 ReLU -> 3.
 Input rows follow the reference's 15-float layout (NrcKernel.cu:18-97).
+
+The reference's own input (mlp.cpp:22-49: tiny-cuda-nn's Composite of
+HashGrid, OneBlob and Identity; tiny-cuda-nn is not in the reference tree
+and its version is not pinned) is restated from the published methods: the
+multiresolution hash encoding of Mueller, Evans, Schied and Keller 2022
+("Instant Neural Graphics Primitives", Sec. 3: N_l = floor(N_min b^l),
+trilinear interpolation of the 2^d corner features, the spatial hash
+x * 1 ^ y * 2654435761 ^ z * 805459861 mod T, dense indexing where the
+level's corners fit in T) and the one-blob encoding of Mueller et al. 2019
+("Neural Importance Sampling", Sec. 4.3: k bins, a Gaussian of sigma 1/k
+centred on the input, integrated over each bin).
 """
 from __future__ import annotations
 
 import numpy as np
+from scipy.special import ndtr
 
 def shapes(hidden_layers: int = 5) -> list[tuple[int, int]]:
     return [(64, 96)] + [(64, 64)] * (hidden_layers - 1) + [(16, 64)]
@@ -69,7 +81,7 @@ def forward(W, x):
     return zs[-1][:, :3], hs, zs
 
 
-def loss_and_grad(W, x, y):
+def loss_and_grad(W, x, y, want_dx: bool = False):
     pred, hs, zs = forward(W, x)
     lum = 0.299 * pred[:, 0] + 0.587 * pred[:, 1] + 0.114 * pred[:, 2]
     den = lum * lum + 0.01
@@ -83,7 +95,75 @@ def loss_and_grad(W, x, y):
         if l > 0:
             dh = dz @ W[l]
             dz = dh * (zs[l - 1] > 0)
+    if want_dx:
+        return loss, grads, dz @ W[0]     # gradient of the layer-0 input features
     return loss, grads
+
+
+# ---------------------------------------------------------------- composite encoding
+def hashgrid_levels(cfg: dict):
+    """(N_l, dense) per level and the entries per level T."""
+    T = 2 ** int(cfg["log2_hashmap_size"])
+    out = []
+    for l in range(int(cfg["n_levels"])):
+        N = int(np.floor(float(np.float32(cfg["base_resolution"])) * float(np.float32(cfg["per_level_scale"])) ** l))
+        out.append((N, (N + 1) ** 3 <= T))
+    return out, T
+
+
+def hash_index(x, y, z, N: int, dense: bool, T: int):
+    x, y, z = (np.asarray(a, np.uint64) for a in (x, y, z))
+    if dense:
+        return x + np.uint64(N + 1) * (y + np.uint64(N + 1) * z)
+    m = np.uint64(0xFFFFFFFF)
+    return (x ^ ((y * np.uint64(2654435761)) & m) ^ ((z * np.uint64(805459861)) & m)) & np.uint64(T - 1)
+
+
+def composite_encode(r15: np.ndarray, table: np.ndarray, cfg: dict):
+    """Layer-0 input (n x 96) of the composite encoding -- 2L hash-grid
+    features, 6 x 4 one-blob bins, 6 albedos, the constant 1 -- and, per
+    level, the (flat table entry, trilinear weight) of the 8 corners of every
+    sample's cell, for the table gradient.  The cell arithmetic is FP32, as in
+    the kernels, so both pick the same cells."""
+    levels, T = hashgrid_levels(cfg)
+    n = len(r15)
+    x = np.zeros((n, 96))
+    tab = np.asarray(table, np.float64).reshape(len(levels), T, 2)
+    p32 = r15[:, 0:3].astype(np.float32)
+    corners = []
+    for l, (N, dense) in enumerate(levels):
+        pos = p32 * np.float32(N)
+        c = np.minimum(np.floor(pos), np.float32(N - 1))
+        i = c.astype(np.uint64)
+        f = (pos - c).astype(np.float64)
+        lst = []
+        for k in range(8):
+            ox, oy, oz = k & 1, (k >> 1) & 1, k >> 2
+            q = hash_index(i[:, 0] + ox, i[:, 1] + oy, i[:, 2] + oz, N, dense, T).astype(np.int64)
+            w = (f[:, 0] if ox else 1 - f[:, 0]) * (f[:, 1] if oy else 1 - f[:, 1]) * (f[:, 2] if oz else 1 - f[:, 2])
+            x[:, 2 * l:2 * l + 2] += w[:, None] * tab[l, q]
+            lst.append((l * T + q, w))
+        corners.append(lst)
+    k = 4
+    for j in range(6):
+        s = r15[:, 3 + j].astype(np.float64)
+        cdf = [ndtr((b / k - s) * k) for b in range(k + 1)]
+        for b in range(k):
+            x[:, 32 + k * j + b] = cdf[b + 1] - cdf[b]
+    x[:, 56:62] = r15[:, 9:15]
+    x[:, 62] = 1.0
+    return x, corners
+
+
+def table_grad(dx: np.ndarray, corners, size: int) -> np.ndarray:
+    """Gradient of the flat [level][entry][feature] table from the gradient
+    of the hash-grid features (dx[:, 2l], dx[:, 2l + 1] of level l)."""
+    g = np.zeros(size)
+    for l, lst in enumerate(corners):
+        for q, w in lst:
+            np.add.at(g, 2 * q, w * dx[:, 2 * l])
+            np.add.at(g, 2 * q + 1, w * dx[:, 2 * l + 1])
+    return g
 
 
 def scrub(c):

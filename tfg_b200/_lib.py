@@ -10,7 +10,7 @@ import ctypes
 from ctypes import POINTER, c_char_p, c_float, c_int32, c_uint32, c_uint64, c_void_p
 from pathlib import Path
 
-from .structs import (CCWBVHHost, CImagenGPU, CMlpTuning, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame,
+from .structs import (CCWBVHHost, CHashGridConfig, CImagenGPU, CMlpTuning, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame,
                       CRenderParams, CRenderProfile, CRenderScene, CRenderTuning, CTinyBVH, CTinyBVHD_GPU,
                       CTuneRecord)
 
@@ -50,6 +50,14 @@ _PROTOS = {
         POINTER(CRenderParams), c_void_p, c_void_p, c_int32, c_void_p, c_int32, c_int32, c_int32,
         POINTER(CTinyBVHD_GPU), c_void_p, c_void_p, c_int32, c_int32, POINTER(CRenderTuning), POINTER(CTuneRecord),
         c_int32, POINTER(c_int32), c_void_p]),
+    "tfgHashGridConfigReference": (None, [POINTER(CHashGridConfig)]),
+    "tfgMlpCreateHashGrid": (c_int32, [c_uint32, c_uint32, c_uint32, c_uint64, c_int32, POINTER(CHashGridConfig),
+                                       c_void_p]),
+    "tfgMlpHashParamCount": (ctypes.c_int64, [c_void_p]),
+    "tfgMlpGetHashParams": (c_int32, [c_void_p, c_int32, POINTER(c_float), ctypes.c_int64]),
+    "tfgMlpSetHashParams": (c_int32, [c_void_p, POINTER(c_float), ctypes.c_int64]),
+    "tfgMlpComputeGradientEx": (c_int32, [c_void_p, c_void_p, c_uint32, c_uint32, POINTER(c_float), c_uint32,
+                                          POINTER(c_float), ctypes.c_int64, POINTER(c_float)]),
     "tfgMlpTuningSet": (c_int32, [c_void_p, POINTER(CMlpTuning)]),
     "tfgMlpTuningGet": (c_int32, [c_void_p, POINTER(CMlpTuning)]),
     "tfgMlpAutotune": (c_int32, [c_void_p, c_void_p, c_uint32, c_void_p, c_int32, POINTER(CMlpTuning),

@@ -135,8 +135,131 @@ __device__ __forceinline__ float unit_clamp(float v, float lo, float hi) {   // 
     return fminf(fmaxf(n, 0.0f), 1.0f);
 }
 
+// ------------------------------------------------------------------ composite encoding
+// The reference's own cache input (mlp.cpp:22-49, tiny-cuda-nn "Composite"):
+// a multiresolution hash grid on the normalised position (Mueller, Evans,
+// Schied, Keller 2022: level l has N_l = floor(N_min * b^l) cells per axis,
+// trilinear interpolation of 2 features stored at the 8 cell corners; a
+// level whose (N_l + 1)^3 corners fit in the table is indexed densely, the
+// others by the spatial hash x * 1 ^ y * 2654435761 ^ z * 805459861 mod T),
+// one-blob encoding of the view direction and the normal (Mueller et al.
+// 2019: k bins per input, each the mass of a Gaussian of sigma 1/k centred at
+// the input that falls in the bin) and the albedos as they are.  Feature
+// layout of layer 0: 0..2L-1 hash grid (level-major), 32..55 one-blob (6
+// inputs x 4 bins), 56..61 albedos, 62 the constant 1, the rest zero.
+constexpr int kHashMaxLevels = 16;
+constexpr int kBlobBins = 4;
+constexpr int kHashLive = 63;     // live input columns of layer 0 with the composite encoding
+constexpr int kFreqLive = 85;     // ... with the frequency encoding
+
+struct HashGrid {
+    const float2* master;    // FP32 tables [level][T] (training forward); null: use `infer`
+    const __half2* infer;    // FP16 tables of the debiased weight average (inference)
+    uint32_t T;              // entries per level (a power of two)
+    int levels;              // 0: frequency encoding
+    uint32_t dense;          // bit l: level l indexed densely
+    float res[kHashMaxLevels];
+};
+
+// Index of corner (x, y, z) of level l in its table.
+__host__ __device__ __forceinline__ uint32_t hash_index(uint32_t x, uint32_t y, uint32_t z, uint32_t n_cells,
+                                                        bool dense, uint32_t T) {
+    if (dense) {
+        const uint32_t st = n_cells + 1u;
+        return x + st * (y + st * z);
+    }
+    return (x ^ (y * 2654435761u) ^ (z * 805459861u)) & (T - 1u);
+}
+
+// Cell of position p (in [0, 1]) at level l: integer corner and weights.
+__device__ __forceinline__ void hash_cell(const float (&p)[3], float n, uint32_t (&i)[3], float (&f)[3]) {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const float x = p[k] * n;
+        const float c = fminf(floorf(x), n - 1.0f);
+        i[k] = (uint32_t)c;
+        f[k] = x - c;
+    }
+}
+
+// The 2L hash-grid features of position p.
+__device__ __forceinline__ void hash_features(const float (&p)[3], const HashGrid& g, float (&h)[2 * kHashMaxLevels]) {
+#pragma unroll
+    for (int l = 0; l < kHashMaxLevels; ++l) {
+        h[2 * l] = 0.0f;
+        h[2 * l + 1] = 0.0f;
+        if (l >= g.levels) continue;
+        const float n = g.res[l];
+        uint32_t i[3];
+        float f[3];
+        hash_cell(p, n, i, f);
+        const bool dense = (g.dense >> l) & 1u;
+        const size_t base = (size_t)l * g.T;
+        float a0 = 0.0f, a1 = 0.0f;
+#pragma unroll
+        for (int c = 0; c < 8; ++c) {
+            const uint32_t cx = i[0] + (c & 1), cy = i[1] + ((c >> 1) & 1), cz = i[2] + (c >> 2);
+            const float w = ((c & 1) ? f[0] : 1.0f - f[0]) * ((c & 2) ? f[1] : 1.0f - f[1]) *
+                            ((c & 4) ? f[2] : 1.0f - f[2]);
+            const uint32_t k = hash_index(cx, cy, cz, (uint32_t)n, dense, g.T);
+            float2 v;
+            if (g.master) v = __ldg(&g.master[base + k]);
+            else v = __half22float2(__ldg(&g.infer[base + k]));
+            a0 = fmaf(w, v.x, a0);
+            a1 = fmaf(w, v.y, a1);
+        }
+        h[2 * l] = a0;
+        h[2 * l + 1] = a1;
+    }
+}
+
+// One-blob bins of an input in [0, 1]: Phi((b+1)/k - s; 1/k) - Phi(b/k - s; 1/k).
+__device__ __forceinline__ void one_blob(float s, float (&o)[kBlobBins]) {
+    float prev = normcdff((0.0f - s) * (float)kBlobBins);
+#pragma unroll
+    for (int b = 0; b < kBlobBins; ++b) {
+        const float next = normcdff(((float)(b + 1) / (float)kBlobBins - s) * (float)kBlobBins);
+        o[b] = next - prev;
+        prev = next;
+    }
+}
+
+// The 64 features of layer 0 with the composite encoding (63 live + one zero).
+__device__ __forceinline__ void composite_features(const TfgDatosMLP& d, const Bounds& b, const HashGrid& g,
+                                                   float (&x)[64]) {
+    const float p[3] = {unit_clamp((float)d.posicion.x, b.lo[0], b.hi[0]),
+                        unit_clamp((float)d.posicion.y, b.lo[1], b.hi[1]),
+                        unit_clamp((float)d.posicion.z, b.lo[2], b.hi[2])};
+    float h[2 * kHashMaxLevels];
+    hash_features(p, g, h);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) x[k] = h[k];
+    const float dirn[6] = {(float)d.direccion.x, (float)d.direccion.y, (float)d.direccion.z,
+                           (float)d.normal.x,    (float)d.normal.y,    (float)d.normal.z};
+#pragma unroll
+    for (int j = 0; j < 6; ++j) {
+        float o[kBlobBins];
+        one_blob(dirn[j], o);
+#pragma unroll
+        for (int k = 0; k < kBlobBins; ++k) x[32 + kBlobBins * j + k] = o[k];
+    }
+    x[56] = d.difuso.r; x[57] = d.difuso.g; x[58] = d.difuso.b;
+    x[59] = d.especular.r; x[60] = d.especular.g; x[61] = d.especular.b;
+    x[62] = 1.0f;
+    x[63] = 0.0f;
+}
+
 // Encoded features of one sample, packed as 48 FP16 pairs (96 features).
-__device__ __forceinline__ void encode(const TfgDatosMLP& d, const Bounds& b, uint32_t (&w)[48]) {
+__device__ __forceinline__ void encode(const TfgDatosMLP& d, const Bounds& b, const HashGrid& g, uint32_t (&w)[48]) {
+    if (g.levels > 0) {
+        float x[64];
+        composite_features(d, b, g, x);
+#pragma unroll
+        for (int k = 0; k < 32; ++k) w[k] = pack_h2(x[2 * k], x[2 * k + 1]);
+#pragma unroll
+        for (int k = 32; k < 48; ++k) w[k] = 0u;
+        return;
+    }
     const float p[3] = {unit_clamp((float)d.posicion.x, b.lo[0], b.hi[0]),
                         unit_clamp((float)d.posicion.y, b.lo[1], b.hi[1]),
                         unit_clamp((float)d.posicion.z, b.lo[2], b.hi[2])};
@@ -306,7 +429,36 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
 // columns (two features each), FP8 24 columns (four each, scaled by q0).
 // Returns the largest |feature| of 72..84 (the bands are within [-1, 1]).
 template <int PREC>
-__device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Bounds& b, float q0, uint32_t ta) {
+__device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Bounds& b, const HashGrid& g, float q0,
+                                                uint32_t ta) {
+    if (g.levels > 0) {
+        // composite encoding: 64 features, the largest |feature| for the FP8 scale
+        float x[64];
+        composite_features(*r, b, g, x);
+        float amax = 1.0f;
+#pragma unroll
+        for (int k = 0; k < 62; ++k) amax = fmaxf(amax, fabsf(x[k]));
+        if constexpr (PREC == kPrecF8) {
+            uint32_t w[24];
+#pragma unroll
+            for (int k = 0; k < 16; ++k)
+                w[k] = pack_e4m3x4<false>(x[4 * k] * q0, x[4 * k + 1] * q0, x[4 * k + 2] * q0, x[4 * k + 3] * q0);
+#pragma unroll
+            for (int k = 16; k < 24; ++k) w[k] = 0u;
+            umma::tmem_st16(ta, *reinterpret_cast<const uint32_t(*)[16]>(w));
+            umma::tmem_st8(ta + 16u, w + 16);
+        } else {
+            uint32_t w[48];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) w[k] = pack2<PREC>(x[2 * k], x[2 * k + 1]);
+#pragma unroll
+            for (int k = 32; k < 48; ++k) w[k] = 0u;
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+                umma::tmem_st16(ta + 16u * c, *reinterpret_cast<const uint32_t(*)[16]>(w + 16 * c));
+        }
+        return amax;
+    }
     const float misc[13] = {(float)r->direccion.x, (float)r->direccion.y, (float)r->direccion.z,
                             (float)r->normal.x,    (float)r->normal.y,    (float)r->normal.z,
                             r->difuso.r,           r->difuso.g,           r->difuso.b,
@@ -379,6 +531,7 @@ __device__ __forceinline__ void warp_amax(float v, float* dst) {
 template <int PREC, bool TRACK, int NL>
 __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
                                                             const uint32_t* __restrict__ n_dev, Bounds bounds,
+                                                            HashGrid hg,
                                                             const uint8_t* __restrict__ wimg,
                                                             TfgColor* __restrict__ out, TfgColor* __restrict__ img,
                                                             const TfgColor* __restrict__ thr,
@@ -452,7 +605,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
         iph ^= 1u;
         // rows past the end of a partial tile encode stale staging bytes; the
         // rows of the MLP are independent and those outputs are never stored
-        const float a0 = encode_to_tmem<PREC>(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds,
+        const float a0 = encode_to_tmem<PREC>(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds, hg,
                                               qs[0], tmem_a + tlane);
         if (track) warp_amax(valid ? a0 : 0.0f, &amax[0]);
         umma::tmem_wait_st();
@@ -640,6 +793,7 @@ struct TrainArgs {
     uint8_t* hT[kMaxLayers];  // transposed inputs of each layer, per tile
     uint8_t* zT[kMaxLayers];  // transposed output gradients of each layer, per tile
     float* loss;                 // sum of per-sample losses (unnormalised)
+    HashGrid hg;                 // composite encoding (levels 0: frequency encoding)
 };
 
 // Write 64 (or 16) values of sample s into the transposed BF16 tile layout.
@@ -702,7 +856,7 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
         for (int k = 0; k < 3; ++k) if (tgt[k] > 100000.0f) tgt[k] = 100000.0f;   // NrcKernel.cu:52-57
         {
             uint32_t w[48];
-            encode(d, a.bounds, w);
+            encode(d, a.bounds, a.hg, w);
             store_encoded(sa, t, w);
             // transposed copy of the layer-0 input for dW0
             float f[96];
@@ -943,6 +1097,7 @@ struct AdamArgs {
     const uint32_t* state;         // S_ADAM_T before this step, S_NAVAIL
     uint32_t min_n;
     int update;                    // 0: only re-pack (after loading parameters)
+    int live0;                     // live input columns of layer 0 (the rest stay zero)
 };
 
 template <int NL>
@@ -960,8 +1115,8 @@ __global__ void k_adam(AdamArgs a) {
     if (i >= kParams<NL>) return;
     int l, r, c;
     layer_of<NL>(i, l, r, c);
-    // Padded entries (output rows 3..15, input columns 85..95 of layer 0) stay zero.
-    const bool live = !(l == NL - 1 && r >= 3) && !(l == 0 && c >= 85);
+    // Padded entries (output rows 3..15, input columns past the encoding of layer 0) stay zero.
+    const bool live = !(l == NL - 1 && r >= 3) && !(l == 0 && c >= a.live0);
     float w = a.w[i];
     float e = a.ema[i];
     const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
@@ -993,6 +1148,123 @@ __global__ void k_adam(AdamArgs a) {
         // backward image: W^T, row = c (input unit), K index = r (output unit)
         const uint32_t boff = (uint32_t)kBOff<NL>(l) + umma::sw128_offset(c, r >> 3) + 2 * (r & 7);
         *reinterpret_cast<__nv_bfloat16*>(a.bwd + boff) = __float2bfloat16_rn(w);
+    }
+}
+
+// ------------------------------------------------------------------ hash-grid tables
+// Gradient of the hash-grid tables for one training batch.  dZ_0 (the
+// gradient at layer 0's pre-activation, written by k_train as transposed BF16
+// tiles) times the FP16-rounded layer-0 weights gives the gradient of the 2L
+// hash features; each is spread over its cell's 8 corners with the
+// trilinear weights (float2 atomics into the FP32 table gradient).
+struct HashGradArgs {
+    const TfgDatosMLP* buf;
+    const uint32_t* state;
+    uint32_t min_n, batch;
+    Bounds bounds;
+    const uint8_t* zT0;          // dZ_0 tiles
+    const float* w0;             // FP32 master weights of layer 0, [64][96]
+    float2* grad;                // table gradient [level][T]
+    HashGrid hg;
+};
+
+__global__ void __launch_bounds__(128) k_hash_grad(HashGradArgs a) {
+    __shared__ float sw[64][2 * kHashMaxLevels];
+    const int L2 = 2 * a.hg.levels;
+    for (int i = threadIdx.x; i < 64 * 2 * kHashMaxLevels; i += blockDim.x) {
+        const int o = i / (2 * kHashMaxLevels), j = i % (2 * kHashMaxLevels);
+        sw[o][j] = j < L2 ? __half2float(__float2half_rn(a.w0[o * 96 + j])) : 0.0f;
+    }
+    __syncthreads();
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t n_avail = a.state[S_NAVAIL];
+    if (s >= a.batch || n_avail < a.min_n || n_avail == 0) return;
+    // the sample k_train drew for row s (NrcKernel.cu:10-16)
+    uint32_t st = a.state[S_STEP] ^ s;
+    const uint32_t idx = pcg_next(st) % n_avail;
+    const TfgDatosMLP d = a.buf[idx];
+    const uint32_t tile = s / kTile, t = s % kTile;
+    const uint8_t* region = a.zT0 + (size_t)tile * (2 * 64 * 128) + (t >> 6) * (64 * 128);
+    const uint32_t c = (t & 63u) >> 3, e = t & 7u;
+    float dx[2 * kHashMaxLevels];
+#pragma unroll
+    for (int j = 0; j < 2 * kHashMaxLevels; ++j) dx[j] = 0.0f;
+    for (int o = 0; o < 64; ++o) {
+        const float dz = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(region + umma::sw128_offset(o, c) + 2 * e));
+        if (dz == 0.0f) continue;
+#pragma unroll
+        for (int j = 0; j < 2 * kHashMaxLevels; ++j) dx[j] = fmaf(dz, sw[o][j], dx[j]);
+    }
+    const float p[3] = {unit_clamp((float)d.posicion.x, a.bounds.lo[0], a.bounds.hi[0]),
+                        unit_clamp((float)d.posicion.y, a.bounds.lo[1], a.bounds.hi[1]),
+                        unit_clamp((float)d.posicion.z, a.bounds.lo[2], a.bounds.hi[2])};
+#pragma unroll
+    for (int l = 0; l < kHashMaxLevels; ++l) {
+        if (l >= a.hg.levels) break;
+        if (dx[2 * l] == 0.0f && dx[2 * l + 1] == 0.0f) continue;
+        const float n = a.hg.res[l];
+        uint32_t i[3];
+        float f[3];
+        hash_cell(p, n, i, f);
+        const bool dense = (a.hg.dense >> l) & 1u;
+        const size_t base = (size_t)l * a.hg.T;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t cx = i[0] + (k & 1), cy = i[1] + ((k >> 1) & 1), cz = i[2] + (k >> 2);
+            const float w = ((k & 1) ? f[0] : 1.0f - f[0]) * ((k & 2) ? f[1] : 1.0f - f[1]) *
+                            ((k & 4) ? f[2] : 1.0f - f[2]);
+            const uint32_t q = hash_index(cx, cy, cz, (uint32_t)n, dense, a.hg.T);
+            atomicAdd(&a.grad[base + q], make_float2(w * dx[2 * l], w * dx[2 * l + 1]));
+        }
+    }
+}
+
+// Adam + weight average over the tables (the same optimiser and step as the
+// layer weights, updated in the same step), the FP16 image of the debiased
+// average for inference, and the gradient reset.
+struct HashAdamArgs {
+    float* w; float* m; float* v; float* ema; float* grad;
+    __half* infer;
+    size_t count;
+    float lr, beta1, beta2, eps, decay, grad_scale;
+    const uint32_t* state;
+    uint32_t min_n;
+    int update;
+};
+
+__global__ void k_adam_hash(HashAdamArgs a) {
+    const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
+    const float tn = (float)(a.state[S_ADAM_T] + (update ? 1u : 0u));
+    const float bc1 = 1.0f - powf(a.beta1, tn), bc2 = 1.0f - powf(a.beta2, tn);
+    const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < a.count; i += (size_t)gridDim.x * blockDim.x) {
+        float w = a.w[i], e = a.ema[i];
+        if (update) {
+            const float g = a.grad[i] * a.grad_scale;
+            const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
+            const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
+            a.m[i] = m;
+            a.v[i] = v;
+            w -= a.lr * (m / bc1) / (sqrtf(v / bc2) + a.eps);
+            e = a.decay * e + (1.0f - a.decay) * w;
+            a.w[i] = w;
+            a.ema[i] = e;
+        }
+        a.grad[i] = 0.0f;
+        a.infer[i] = __float2half_rn(ema_debias > 0.0f ? e / ema_debias : w);
+    }
+}
+
+// Initial table values: uniform in (-1e-4, 1e-4) (Mueller et al. 2022),
+// from a counter-based hash of (seed, index).
+__global__ void k_hash_init(float* w, size_t count, uint64_t seed) {
+    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < count; i += (size_t)gridDim.x * blockDim.x) {
+        uint64_t z = seed + 0x9E3779B97F4A7C15ull * (uint64_t)(i + 1);
+        z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+        z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+        z ^= z >> 31;
+        const float u = (float)(z >> 40) * (1.0f / 16777216.0f);
+        w[i] = (2.0f * u - 1.0f) * 1e-4f;
     }
 }
 
@@ -1040,9 +1312,31 @@ struct ColorMlp {
     int sms = 148;
     TfgMlpTuning tune{};         // batch tiling of the kernels (zero fields: defaults)
     uint32_t tune_generation = 0;
+    // composite encoding: hash-grid tables (hlevels 0: frequency encoding)
+    int hlevels = 0;
+    uint32_t hT_entries = 0;     // entries per level
+    uint32_t hdense = 0;
+    float hres[mlp::kHashMaxLevels] = {};
+    size_t hcount = 0;           // floats per table array (levels x entries x 2)
+    float* hw = nullptr; float* hm = nullptr; float* hv = nullptr; float* hema = nullptr; float* hgrad = nullptr;
+    __half* hinf = nullptr;      // FP16 image of the debiased average (inference)
 };
 
 namespace {
+
+// The encoding view the kernels take: training reads the FP32 tables,
+// inference the FP16 image of their average.
+mlp::HashGrid hash_view(const ColorMlp* n, bool train) {
+    mlp::HashGrid g{};
+    g.levels = n->hlevels;
+    if (!n->hlevels) return g;
+    g.master = train ? reinterpret_cast<const float2*>(n->hw) : nullptr;
+    g.infer = reinterpret_cast<const __half2*>(n->hinf);
+    g.T = n->hT_entries;
+    g.dense = n->hdense;
+    for (int l = 0; l < mlp::kHashMaxLevels; ++l) g.res[l] = n->hres[l];
+    return g;
+}
 
 int cuda_fail(cudaError_t e, const char* what) {
     return fail((int)e, std::string(what) + ": " + cudaGetErrorString(e));
@@ -1075,6 +1369,7 @@ int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
     a.state = n->dstate;
     a.min_n = min_n;
     a.update = update ? 1 : 0;
+    a.live0 = n->hlevels ? mlp::kHashLive : mlp::kFreqLive;
     with_layers(n->nl, [&](auto c) {
         constexpr int NL = decltype(c)::value;
         mlp::k_adam<NL><<<(mlp::kParams<NL> + 255) / 256, 256, 0, s>>>(a);
@@ -1082,6 +1377,17 @@ int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
     });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp adam");
+    if (n->hlevels) {
+        mlp::HashAdamArgs h;
+        h.w = n->hw; h.m = n->hm; h.v = n->hv; h.ema = n->hema; h.grad = n->hgrad; h.infer = n->hinf;
+        h.count = n->hcount;
+        h.lr = n->lr; h.beta1 = n->beta1; h.beta2 = n->beta2; h.eps = n->eps; h.decay = n->decay;
+        h.grad_scale = a.grad_scale;
+        h.state = n->dstate; h.min_n = min_n; h.update = a.update;
+        mlp::k_adam_hash<<<(unsigned)std::min<size_t>((n->hcount + 255) / 256, (size_t)n->sms * 16), 256, 0, s>>>(h);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "mlp adam (tables)");
+    }
     return ok();
 }
 
@@ -1156,6 +1462,7 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     mlp::TrainArgs ta;
     ta.buf = buf; ta.state = n->dstate; ta.min_n = min_n; ta.batch = n->batch;
     ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
+    ta.hg = hash_view(n, true);
     for (int l = 0; l < mlp::kMaxLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
     with_layers(n->nl, [&](auto c) {
         constexpr int NL = decltype(c)::value;
@@ -1165,6 +1472,14 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp step: forward/backward");
     if (int rc = enqueue_wgrad(n, wgrad_tiles_per_cta(n, tiles), min_n, s)) return rc;
+    if (n->hlevels) {
+        mlp::HashGradArgs ha;
+        ha.buf = buf; ha.state = n->dstate; ha.min_n = min_n; ha.batch = n->batch; ha.bounds = n->bounds;
+        ha.zT0 = n->zT[0]; ha.w0 = n->w; ha.grad = reinterpret_cast<float2*>(n->hgrad); ha.hg = hash_view(n, true);
+        mlp::k_hash_grad<<<tiles, mlp::kTile, 0, s>>>(ha);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "mlp step: table gradient");
+    }
     if (!update) return ok();
     if (int rc = repack(n, s, true, min_n)) return rc;
     mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n, n->gate);
@@ -1195,16 +1510,17 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
         constexpr int NL = decltype(c)::value;
         if (n->prec == mlp::kPrecF16) {
             mlp::k_infer<mlp::kPrecF16, false, NL><<<grid, mlp::kInferThreads, smem, s>>>(
-                in, count, n_dev, n->bounds, n->inf, out, img, thr, nullptr, nullptr, 0);
+                in, count, n_dev, n->bounds, hash_view(n, false), n->inf, out, img, thr, nullptr, nullptr, 0);
         } else if (n->prec == mlp::kPrecBF16) {
             mlp::k_infer<mlp::kPrecBF16, false, NL><<<grid, mlp::kInferThreads, smem, s>>>(
-                in, count, n_dev, n->bounds, n->inf_bf, out, img, thr, nullptr, nullptr, 0);
+                in, count, n_dev, n->bounds, hash_view(n, false), n->inf_bf, out, img, thr, nullptr, nullptr, 0);
         } else {
             mlp::k_pack_f8<NL><<<NL, 1024, 0, s>>>(n->w, n->ema, n->dstate, n->decay, n->inf_f8, n->f8);
             cudaError_t e2 = cudaGetLastError();
             if (e2 != cudaSuccess) return cuda_fail(e2, "mlp inference: FP8 weight image");
             mlp::k_infer<mlp::kPrecF8, true, NL><<<grid, mlp::kInferThreads, smem, s>>>(
-                in, count, n_dev, n->bounds, n->inf_f8, out, img, thr, n->f8, n->f8 + mlp::kF8Amax, 0);
+                in, count, n_dev, n->bounds, hash_view(n, false), n->inf_f8, out, img, thr, n->f8, n->f8 + mlp::kF8Amax,
+                0);
             e2 = cudaGetLastError();
             if (e2 != cudaSuccess) return cuda_fail(e2, "mlp inference");
             mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 1);
@@ -1230,7 +1546,8 @@ int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStrea
     with_layers(n->nl, [&](auto c) {
         constexpr int NL = decltype(c)::value;
         mlp::k_infer<mlp::kPrecF16, true, NL><<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(
-            in, count, nullptr, n->bounds, n->inf, nullptr, nullptr, nullptr, nullptr, n->f8 + mlp::kF8Amax, 1);
+            in, count, nullptr, n->bounds, hash_view(n, false), n->inf, nullptr, nullptr, nullptr, nullptr,
+            n->f8 + mlp::kF8Amax, 1);
         return 0;
     });
     e = cudaGetLastError();
@@ -1369,8 +1686,61 @@ extern "C" int tfgMlpCreate(uint32_t n_in, uint32_t n_out, uint32_t batch, uint6
     return tfgMlpCreateEx(n_in, n_out, batch, seed, 5, out);
 }
 
-extern "C" int tfgMlpCreateEx(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
-                              TfgColorMLP** out) {
+extern "C" void tfgHashGridConfigReference(TfgHashGridConfig* c) {
+    if (!c) return;
+    std::memset(c, 0, sizeof(*c));
+    c->n_levels = 16;              // mlp.cpp:33-39
+    c->log2_hashmap_size = 19;
+    c->base_resolution = 16.0f;
+    c->per_level_scale = 1.5f;
+}
+
+namespace tfg {
+namespace {
+
+// Tables of the composite encoding: sizes, level resolutions, FP32 arrays and
+// the FP16 inference image (written by the first re-pack).
+int create_tables(ColorMlp* n, const TfgHashGridConfig& c, uint64_t seed) {
+    if (c.n_levels < 1 || c.n_levels > M::kHashMaxLevels)
+        return fail(TFG_E_INVALID, "tfgMlpCreateHashGrid: n_levels must be in [1, 16]");
+    if (c.log2_hashmap_size < 10 || c.log2_hashmap_size > 24)
+        return fail(TFG_E_INVALID, "tfgMlpCreateHashGrid: log2_hashmap_size must be in [10, 24]");
+    if (!(c.base_resolution >= 2.0f) || !(c.per_level_scale >= 1.0f))
+        return fail(TFG_E_INVALID, "tfgMlpCreateHashGrid: base_resolution >= 2 and per_level_scale >= 1");
+    const uint32_t T = 1u << c.log2_hashmap_size;
+    n->hlevels = c.n_levels;
+    n->hT_entries = T;
+    n->hdense = 0;
+    for (int l = 0; l < c.n_levels; ++l) {
+        const double N = std::floor((double)c.base_resolution * std::pow((double)c.per_level_scale, (double)l));
+        if (N < 1.0 || N > (double)(1u << 20))
+            return fail(TFG_E_INVALID, "tfgMlpCreateHashGrid: a level resolution leaves [1, 2^20]");
+        n->hres[l] = (float)N;
+        const uint64_t st = (uint64_t)N + 1u;
+        if (st * st * st <= (uint64_t)T) n->hdense |= 1u << l;
+    }
+    n->hcount = (size_t)c.n_levels * T * 2u;
+    const size_t hb = n->hcount * sizeof(float);
+    cudaError_t e = cudaMalloc((void**)&n->hw, hb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->hm, hb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->hv, hb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->hema, hb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->hgrad, hb);
+    if (e == cudaSuccess) e = cudaMalloc((void**)&n->hinf, n->hcount * sizeof(__half));
+    if (e == cudaSuccess) e = cudaMemset(n->hm, 0, hb);
+    if (e == cudaSuccess) e = cudaMemset(n->hv, 0, hb);
+    if (e == cudaSuccess) e = cudaMemset(n->hema, 0, hb);
+    if (e == cudaSuccess) e = cudaMemset(n->hgrad, 0, hb);
+    if (e != cudaSuccess) return cuda_fail(e, "tfgMlpCreateHashGrid");
+    M::k_hash_init<<<(unsigned)std::min<size_t>((n->hcount + 255) / 256, (size_t)n->sms * 16), 256>>>(
+        n->hw, n->hcount, seed ^ 0x7AB1E5ull);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "tfgMlpCreateHashGrid");
+    return ok();
+}
+
+int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
+                 const TfgHashGridConfig* hc, TfgColorMLP** out) {
     if (!out) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: out is null");
     *out = nullptr;
     if (hidden_layers != 3 && hidden_layers != 5 && hidden_layers != 7)
@@ -1412,15 +1782,19 @@ extern "C" int tfgMlpCreateEx(uint32_t n_in, uint32_t n_out, uint32_t batch, uin
     cudaMemset(n->inf_f8, 0, f8_bytes);
     cudaMemset(n->f8, 0, M::kF8Words * sizeof(float));
     cudaMemset(n->dstate, 0, M::S_WORDS * sizeof(uint32_t));
+    if (hc) {
+        if (int rc = create_tables(n, *hc, seed)) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return rc; }
+    }
+    const int live0 = hc ? M::kHashLive : M::kFreqLive;
     // Uniform (-s, s) initialisation with s = sqrt(6 / (fan_in + fan_out)) per layer.
     std::vector<float> h(nparams, 0.0f);
     uint64_t st = seed ? seed : 0x5EEDull;
     for (int l = 0; l < nl; ++l) {
-        const int fan_in = l == 0 ? 85 : 64, fan_out = l == nl - 1 ? 3 : 64;
+        const int fan_in = l == 0 ? live0 : 64, fan_out = l == nl - 1 ? 3 : 64;
         const float sc = std::sqrt(6.0f / (float)(fan_in + fan_out));
         for (int r = 0; r < M::rows_of(nl, l); ++r)
             for (int c = 0; c < M::cols_of(l); ++c) {
-                const bool live = !(l == nl - 1 && r >= 3) && !(l == 0 && c >= 85);
+                const bool live = !(l == nl - 1 && r >= 3) && !(l == 0 && c >= live0);
                 const double u = (double)(tfg::splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
                 h[M::poff_of(nl, l) + r * M::cols_of(l) + c] = live ? (float)((2.0 * u - 1.0) * sc) : 0.0f;
             }
@@ -1447,11 +1821,55 @@ extern "C" int tfgMlpCreateEx(uint32_t n_in, uint32_t n_out, uint32_t batch, uin
     return tfg::ok();
 }
 
+}  // namespace
+}  // namespace tfg
+
+extern "C" int tfgMlpCreateEx(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
+                              TfgColorMLP** out) {
+    return tfg::create_model(n_in, n_out, batch, seed, hidden_layers, nullptr, out);
+}
+
+extern "C" int tfgMlpCreateHashGrid(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed,
+                                    int32_t hidden_layers, const TfgHashGridConfig* config, TfgColorMLP** out) {
+    if (!config) return tfg::fail(TFG_E_INVALID, "tfgMlpCreateHashGrid: config is null");
+    return tfg::create_model(n_in, n_out, batch, seed, hidden_layers, config, out);
+}
+
+extern "C" int64_t tfgMlpHashParamCount(const TfgColorMLP* h) {
+    const ColorMlp* n = reinterpret_cast<const ColorMlp*>(h);
+    return n ? (int64_t)n->hcount : 0;
+}
+
+extern "C" int tfgMlpGetHashParams(TfgColorMLP* h, int which, float* host, int64_t count) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !host || !n->hlevels || count != (int64_t)n->hcount)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpGetHashParams: bad argument");
+    const float* src = which == 0 ? n->hw : which == 1 ? n->hema : which == 2 ? n->hm : which == 3 ? n->hv : nullptr;
+    if (!src) return tfg::fail(TFG_E_INVALID, "tfgMlpGetHashParams: unknown array");
+    cudaError_t e = cudaMemcpy(host, src, n->hcount * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpGetHashParams");
+    return tfg::ok();
+}
+
+extern "C" int tfgMlpSetHashParams(TfgColorMLP* h, const float* host, int64_t count) {
+    ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
+    if (!n || !host || !n->hlevels || count != (int64_t)n->hcount)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpSetHashParams: bad argument");
+    cudaError_t e = cudaMemcpy(n->hw, host, n->hcount * sizeof(float), cudaMemcpyHostToDevice);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetHashParams");
+    // restart the optimiser of the whole model (tfgMlpSetParams clears the tables' state too)
+    std::vector<float> w((size_t)M::params_of(n->nl));
+    e = cudaMemcpy(w.data(), n->w, w.size() * sizeof(float), cudaMemcpyDeviceToHost);
+    if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetHashParams");
+    return tfgMlpSetParams(h, w.data(), (uint32_t)w.size());
+}
+
 extern "C" void tfgMlpDestroy(TfgColorMLP* h) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n) return;
     for (void* p : {(void*)n->w, (void*)n->m, (void*)n->v, (void*)n->ema, (void*)n->grad, (void*)n->fwd, (void*)n->bwd,
-                    (void*)n->inf, (void*)n->inf_bf, (void*)n->inf_f8, (void*)n->f8, (void*)n->loss, (void*)n->dstate})
+                    (void*)n->inf, (void*)n->inf_bf, (void*)n->inf_f8, (void*)n->f8, (void*)n->loss, (void*)n->dstate,
+                    (void*)n->hw, (void*)n->hm, (void*)n->hv, (void*)n->hema, (void*)n->hgrad, (void*)n->hinf})
         if (p) cudaFree(p);
     for (int l = 0; l < M::kMaxLayers; ++l) {
         if (n->hT[l]) cudaFree(n->hT[l]);
@@ -1575,6 +1993,13 @@ extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count
     if (e == cudaSuccess) e = cudaMemset(n->grad, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->dstate + M::S_ADAM_T, 0, sizeof(uint32_t));
     if (e == cudaSuccess) e = cudaMemset(n->dstate + M::S_F8_VER, 0, sizeof(uint32_t));
+    if (n->hlevels) {
+        const size_t hb = n->hcount * sizeof(float);
+        if (e == cudaSuccess) e = cudaMemset(n->hema, 0, hb);
+        if (e == cudaSuccess) e = cudaMemset(n->hm, 0, hb);
+        if (e == cudaSuccess) e = cudaMemset(n->hv, 0, hb);
+        if (e == cudaSuccess) e = cudaMemset(n->hgrad, 0, hb);
+    }
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetParams");
     if (int rc = tfg::repack(n, 0, false, 1)) return rc;
     e = cudaDeviceSynchronize();
@@ -1584,13 +2009,22 @@ extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count
 
 extern "C" int tfgMlpComputeGradient(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
                                      float* host_grad, uint32_t count, float* loss_out) {
+    return tfgMlpComputeGradientEx(h, buffer, n_available, seed, host_grad, count, nullptr, 0, loss_out);
+}
+
+extern "C" int tfgMlpComputeGradientEx(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
+                                       float* host_grad, uint32_t count, float* host_table_grad, int64_t table_count,
+                                       float* loss_out) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n || !buffer || !host_grad || count != (uint32_t)M::params_of(n->nl) || n_available == 0)
         return tfg::fail(TFG_E_INVALID, "tfgMlpComputeGradient: bad argument");
+    if (host_table_grad && table_count != (int64_t)n->hcount)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpComputeGradientEx: table_count differs from tfgMlpHashParamCount");
     if (int rc = tfg::mlp_prepare(n)) return rc;
     uint32_t saved[M::S_WORDS];
     cudaError_t e = cudaMemcpy(saved, n->dstate, sizeof(saved), cudaMemcpyDeviceToHost);
     if (e == cudaSuccess) e = cudaMemset(n->grad, 0, count * sizeof(float));
+    if (e == cudaSuccess && n->hlevels) e = cudaMemset(n->hgrad, 0, n->hcount * sizeof(float));
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
     if (int rc = tfg::set_word(n, M::S_NAVAIL, n_available, 0)) return rc;
     if (int rc = tfg::set_word(n, M::S_STEP, seed, 0)) return rc;
@@ -1607,6 +2041,14 @@ extern "C" int tfgMlpComputeGradient(TfgColorMLP* h, const TfgDatosMLP* buffer, 
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradient");
     const float sc = 1.0f / (3.0f * (float)n->batch);
     for (uint32_t i = 0; i < count; ++i) host_grad[i] = g[i] * sc;
+    if (n->hlevels) {
+        if (host_table_grad) {
+            e = cudaMemcpy(host_table_grad, n->hgrad, n->hcount * sizeof(float), cudaMemcpyDeviceToHost);
+            for (size_t i = 0; e == cudaSuccess && i < n->hcount; ++i) host_table_grad[i] *= sc;
+        }
+        if (e == cudaSuccess) e = cudaMemset(n->hgrad, 0, n->hcount * sizeof(float));
+        if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpComputeGradientEx");
+    }
     if (loss_out) *loss_out = l * sc;
     return tfg::ok();
 }
@@ -1643,7 +2085,9 @@ extern "C" int tfgMlpSave(TfgColorMLP* h, const char* path) {
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSave");
     FILE* f = std::fopen(path, "wb");
     if (!f) return tfg::fail(TFG_E_INVALID, std::string("tfgMlpSave: cannot open ") + path);
-    const uint32_t version = 1;
+    // version 1: frequency encoding; version 2 adds the composite encoding's
+    // table description and its four table arrays
+    const uint32_t version = n->hlevels ? 2 : 1;
     const int32_t hidden = n->nl - 1;
     const float hyper[5] = {n->lr, n->beta1, n->beta2, n->eps, n->decay};
     bool good = std::fwrite(kCkptMagic, 1, 8, f) == 8 && std::fwrite(&version, 4, 1, f) == 1 &&
@@ -1651,6 +2095,18 @@ extern "C" int tfgMlpSave(TfgColorMLP* h, const char* path) {
                 std::fwrite(n->bounds.lo, 4, 3, f) == 3 && std::fwrite(n->bounds.hi, 4, 3, f) == 3 &&
                 std::fwrite(hyper, 4, 5, f) == 5 && std::fwrite(st, 4, M::S_WORDS, f) == (size_t)M::S_WORDS;
     for (int k = 0; k < 4 && good; ++k) good = std::fwrite(arrays[k].data(), 4, np, f) == np;
+    if (good && n->hlevels) {
+        const int32_t lv = n->hlevels;
+        const uint64_t cnt = n->hcount;
+        good = std::fwrite(&lv, 4, 1, f) == 1 && std::fwrite(&n->hT_entries, 4, 1, f) == 1 &&
+               std::fwrite(n->hres, 4, M::kHashMaxLevels, f) == (size_t)M::kHashMaxLevels && std::fwrite(&cnt, 8, 1, f) == 1;
+        const float* tsrc[4] = {n->hw, n->hema, n->hm, n->hv};
+        std::vector<float> buf(n->hcount);
+        for (int k = 0; k < 4 && good; ++k) {
+            good = cudaMemcpy(buf.data(), tsrc[k], n->hcount * sizeof(float), cudaMemcpyDeviceToHost) == cudaSuccess &&
+                   std::fwrite(buf.data(), 4, n->hcount, f) == n->hcount;
+        }
+    }
     if (std::fclose(f) != 0 || !good) return tfg::fail(TFG_E_INVALID, std::string("tfgMlpSave: write failed: ") + path);
     return tfg::ok();
 }
@@ -1665,8 +2121,9 @@ extern "C" int tfgMlpLoad(TfgColorMLP* h, const char* path) {
     int32_t hidden = 0;
     float lo[3], hi[3], hyper[5];
     uint32_t st[M::S_WORDS];
+    const uint32_t want_version = n->hlevels ? 2 : 1;
     bool good = std::fread(magic, 1, 8, f) == 8 && std::memcmp(magic, kCkptMagic, 8) == 0 &&
-                std::fread(&version, 4, 1, f) == 1 && version == 1 && std::fread(&hidden, 4, 1, f) == 1 &&
+                std::fread(&version, 4, 1, f) == 1 && version == want_version && std::fread(&hidden, 4, 1, f) == 1 &&
                 std::fread(&np, 4, 1, f) == 1 && std::fread(lo, 4, 3, f) == 3 && std::fread(hi, 4, 3, f) == 3 &&
                 std::fread(hyper, 4, 5, f) == 5 && std::fread(st, 4, M::S_WORDS, f) == (size_t)M::S_WORDS;
     if (!good) {
@@ -1682,6 +2139,24 @@ extern "C" int tfgMlpLoad(TfgColorMLP* h, const char* path) {
         arrays[k].resize(np);
         good = std::fread(arrays[k].data(), 4, np, f) == np;
     }
+    std::vector<float> tables[4];
+    if (good && n->hlevels) {
+        int32_t lv = 0;
+        uint32_t T = 0;
+        float res[M::kHashMaxLevels];
+        uint64_t cnt = 0;
+        good = std::fread(&lv, 4, 1, f) == 1 && std::fread(&T, 4, 1, f) == 1 &&
+               std::fread(res, 4, M::kHashMaxLevels, f) == (size_t)M::kHashMaxLevels && std::fread(&cnt, 8, 1, f) == 1;
+        if (good && (lv != n->hlevels || T != n->hT_entries || cnt != n->hcount ||
+                     std::memcmp(res, n->hres, sizeof(res)) != 0)) {
+            std::fclose(f);
+            return tfg::fail(TFG_E_INVALID, "tfgMlpLoad: the checkpoint's hash-grid tables differ from this model's");
+        }
+        for (int k = 0; k < 4 && good; ++k) {
+            tables[k].resize(n->hcount);
+            good = std::fread(tables[k].data(), 4, n->hcount, f) == n->hcount;
+        }
+    }
     std::fclose(f);
     if (!good) return tfg::fail(TFG_E_INVALID, std::string("tfgMlpLoad: truncated checkpoint: ") + path);
     float* dst[4] = {n->w, n->ema, n->m, n->v};
@@ -1691,6 +2166,12 @@ extern "C" int tfgMlpLoad(TfgColorMLP* h, const char* path) {
     st[M::S_F8_VER] = 0;   // the FP8 image is re-packed on its next use
     if (e == cudaSuccess) e = cudaMemcpy(n->dstate, st, sizeof(st), cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(n->grad, 0, np * sizeof(float));
+    if (n->hlevels) {
+        float* tdst[4] = {n->hw, n->hema, n->hm, n->hv};
+        for (int k = 0; k < 4 && e == cudaSuccess; ++k)
+            e = cudaMemcpy(tdst[k], tables[k].data(), n->hcount * sizeof(float), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemset(n->hgrad, 0, n->hcount * sizeof(float));
+    }
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpLoad");
     n->bounds = M::Bounds{{lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}};
     n->lr = hyper[0]; n->beta1 = hyper[1]; n->beta2 = hyper[2]; n->eps = hyper[3]; n->decay = hyper[4];

@@ -8,7 +8,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from .structs import BOUNDS, DATOS_MLP, REGISTRO, CMlpTuning, CNrcBuffers, CNrcFrameConfig, CNrcSceneFrame
+from .structs import (BOUNDS, DATOS_MLP, REGISTRO, CHashGridConfig, CMlpTuning, CNrcBuffers, CNrcFrameConfig,
+                      CNrcSceneFrame)
 
 def layer_shapes(hidden_layers: int = 5) -> list[tuple[int, int]]:
     """Padded [out][in] shapes of the weight matrices, in parameter order."""
@@ -24,6 +25,15 @@ LAYER_SHAPES = layer_shapes(5)
 N_PARAMS = param_count(5)
 WEIGHTS, EMA, ADAM_M, ADAM_V = 0, 1, 2, 3
 FP16, BF16, FP8 = 0, 1, 2      # inference operand precisions (TFG_MLP_*)
+FREQUENCY, HASHGRID = "frequency", "hashgrid"   # input encodings
+
+
+def hashgrid_reference() -> dict:
+    """The reference's hash-grid settings (mlp.cpp:33-39)."""
+    c = CHashGridConfig()
+    _lib.lib.tfgHashGridConfigReference(ctypes.byref(c))
+    return {"n_levels": c.n_levels, "log2_hashmap_size": c.log2_hashmap_size,
+            "base_resolution": c.base_resolution, "per_level_scale": c.per_level_scale}
 
 
 def _stream(stream=None) -> int:
@@ -44,15 +54,32 @@ def split_layers(flat: np.ndarray) -> list[np.ndarray]:
 
 class ColorMLP:
     """ColorMLP(n_in=15, n_out=3, batch): train_step / inference / setBounds.
-    `hidden_layers` (3, 5 or 7; the reference's network has 5) sets the depth."""
+    `hidden_layers` (3, 5 or 7; the reference's network has 5) sets the depth;
+    `encoding` the input encoding: FREQUENCY, or HASHGRID, the reference's own
+    composite (hash grid + one-blob + identity; `hashgrid` overrides fields of
+    hashgrid_reference())."""
 
-    def __init__(self, n_in: int = 15, n_out: int = 3, batch: int = 16384, seed: int = 1337, hidden_layers: int = 5):
+    def __init__(self, n_in: int = 15, n_out: int = 3, batch: int = 16384, seed: int = 1337, hidden_layers: int = 5,
+                 encoding: str = FREQUENCY, hashgrid: dict | None = None):
         self.batch = batch
         self.hidden_layers = hidden_layers
+        self.encoding = encoding
         h = ctypes.c_void_p()
-        _lib.call("tfgMlpCreateEx", n_in, n_out, batch, seed, hidden_layers, ctypes.byref(h))
+        if encoding == HASHGRID:
+            cfg = {**hashgrid_reference(), **(hashgrid or {})}
+            c = CHashGridConfig()
+            c.n_levels, c.log2_hashmap_size = cfg["n_levels"], cfg["log2_hashmap_size"]
+            c.base_resolution, c.per_level_scale = cfg["base_resolution"], cfg["per_level_scale"]
+            self.hashgrid = cfg
+            _lib.call("tfgMlpCreateHashGrid", n_in, n_out, batch, seed, hidden_layers, ctypes.byref(c), ctypes.byref(h))
+        elif encoding == FREQUENCY:
+            self.hashgrid = None
+            _lib.call("tfgMlpCreateEx", n_in, n_out, batch, seed, hidden_layers, ctypes.byref(h))
+        else:
+            raise ValueError(f"unknown encoding {encoding!r}")
         self.h = h
         self.n_params = int(_lib.lib.tfgMlpParamCount(self.h))
+        self.n_table = int(_lib.lib.tfgMlpHashParamCount(self.h))
 
     def close(self) -> None:
         if self.h:
@@ -129,6 +156,30 @@ class ColorMLP:
         w = np.ascontiguousarray(w, np.float32)
         assert w.size == self.n_params
         _lib.call("tfgMlpSetParams", self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), self.n_params)
+
+    def get_table(self, which: int = WEIGHTS) -> np.ndarray:
+        """Hash-grid table array [level][entry][feature] (flat)."""
+        out = np.zeros(self.n_table, np.float32)
+        _lib.call("tfgMlpGetHashParams", self.h, which, out.ctypes.data_as(ctypes.POINTER(ctypes.c_float)),
+                  self.n_table)
+        return out
+
+    def set_table(self, t: np.ndarray) -> None:
+        t = np.ascontiguousarray(t, np.float32)
+        assert t.size == self.n_table
+        _lib.call("tfgMlpSetHashParams", self.h, t.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), self.n_table)
+
+    def compute_gradient_ex(self, buffer: torch.Tensor, n_available: int,
+                            seed: int) -> tuple[np.ndarray, np.ndarray, float]:
+        """Gradients of the layer weights and of the hash-grid tables, and the loss."""
+        g = np.zeros(self.n_params, np.float32)
+        gt = np.zeros(self.n_table, np.float32)
+        loss = ctypes.c_float(0.0)
+        _lib.call("tfgMlpComputeGradientEx", self.h, buffer.data_ptr(), int(n_available), seed,
+                  g.ctypes.data_as(ctypes.POINTER(ctypes.c_float)), self.n_params,
+                  gt.ctypes.data_as(ctypes.POINTER(ctypes.c_float)) if self.n_table else None, self.n_table,
+                  ctypes.byref(loss))
+        return g, gt, float(loss.value)
 
     def compute_gradient(self, buffer: torch.Tensor, n_available: int, seed: int) -> tuple[np.ndarray, float]:
         g = np.zeros(self.n_params, np.float32)

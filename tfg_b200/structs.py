@@ -96,6 +96,12 @@ class CRenderProfile(ctypes.Structure):
                 ("shadow_nodes", ctypes.c_uint64), ("shadow_tri_tests", ctypes.c_uint64)]
 
 
+class CHashGridConfig(ctypes.Structure):
+    _fields_ = [("n_levels", ctypes.c_int32), ("log2_hashmap_size", ctypes.c_int32),
+                ("base_resolution", ctypes.c_float), ("per_level_scale", ctypes.c_float),
+                ("reserved", ctypes.c_int32 * 4)]
+
+
 class CRenderScene(ctypes.Structure):
     _fields_ = [("camara", ctypes.c_void_p), ("primitivas", ctypes.c_void_p), ("num_primitivas", ctypes.c_int32),
                 ("num_luces", ctypes.c_int32), ("luces", ctypes.c_void_p), ("ancho_img", ctypes.c_int32),
