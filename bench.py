@@ -302,12 +302,11 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
     mlp.set_precision(FP16)
     mlp.close()
 
-    # Depth sweep: the same protocol (warm-up, orbit, final pose) with 3 and 7
-    # hidden layers of 64; 5 is the run above.
-    depth = {5: {"relmse": round(e_nrc, 5), "ms_per_frame": round(t_nrc, 3), "inference_ms": round(t_inf, 4),
-                 "adam_steps": int(st["adam_t"])}}
-    for hidden in (3, 7):
-        m2 = ColorMLP(batch=16384, seed=2024, hidden_layers=hidden)
+    # Depth and encoding sweeps: the same protocol (warm-up, orbit, final
+    # pose) with 3 and 7 hidden layers of 64 (5 is the run above), and with
+    # the reference's own input encoding (hash grid + one-blob + identity).
+    def variant(**kw) -> dict:
+        m2 = ColorMLP(batch=16384, seed=2024, **kw)
         m2.set_bounds(*scene.bounds)
         r2 = NrcRenderer(ds, m2, params, train_steps=4, use_graph=True)
         for f in range(48):
@@ -334,10 +333,20 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
                 m2.inference(r2.infer, out, n, stream=r2.stream)
             h1.record(r2.stream)
         h1.synchronize()
-        depth[hidden] = {"relmse": round(rel(img2), 5), "ms_per_frame": round(d0.elapsed_time(d1) / 10, 3),
-                         "inference_ms": round(h0.elapsed_time(h1) / 10, 4), "adam_steps": int(m2.state()["adam_t"])}
+        res = {"relmse": round(rel(img2), 5), "ms_per_frame": round(d0.elapsed_time(d1) / 10, 3),
+               "inference_ms": round(h0.elapsed_time(h1) / 10, 4), "adam_steps": int(m2.state()["adam_t"]),
+               "loss_ema": round(m2.state()["loss_ema"], 5)}
         m2.close()
-        del r2
+        return res
+
+    depth = {5: {"relmse": round(e_nrc, 5), "ms_per_frame": round(t_nrc, 3), "inference_ms": round(t_inf, 4),
+                 "adam_steps": int(st["adam_t"])}}
+    for hidden in (3, 7):
+        depth[hidden] = variant(hidden_layers=hidden)
+    from tfg_b200.nrc import HASHGRID, hashgrid_reference
+    encoding = {"frequency_12_bands": depth[5],
+                "hashgrid_reference": {**variant(encoding=HASHGRID), "config": hashgrid_reference(),
+                                       "one_blob_bins": 4}}
     return {
         "frames": 48 + frames, "warmup_frames": 48, "camera": "orbit 1 deg/frame", "train_samples_per_frame": 4 * 16384,
         "ms_per_frame_nrc": round(t_nrc, 3), "ms_per_pass_plain_1spp": round(t_pt, 3),
@@ -348,6 +357,7 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
                           "flops_per_query": int(flops / n)},
         "precision_sweep": sweep,
         "depth_sweep": {f"{k}x64": v for k, v in sorted(depth.items())},
+        "encoding_sweep": encoding,
     }
 
 

@@ -428,10 +428,10 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
 // normal, albedos and the constant 1, 85..95 zero.  FP16 / BF16 write 48 TMEM
 // columns (two features each), FP8 24 columns (four each, scaled by q0).
 // Returns the largest |feature| of 72..84 (the bands are within [-1, 1]).
-template <int PREC>
+template <int PREC, bool HASH>
 __device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Bounds& b, const HashGrid& g, float q0,
                                                 uint32_t ta) {
-    if (g.levels > 0) {
+    if constexpr (HASH) {
         // composite encoding: 64 features, the largest |feature| for the FP8 scale
         float x[64];
         composite_features(*r, b, g, x);
@@ -458,7 +458,7 @@ __device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Boun
                 umma::tmem_st16(ta + 16u * c, *reinterpret_cast<const uint32_t(*)[16]>(w + 16 * c));
         }
         return amax;
-    }
+    } else {
     const float misc[13] = {(float)r->direccion.x, (float)r->direccion.y, (float)r->direccion.z,
                             (float)r->normal.x,    (float)r->normal.y,    (float)r->normal.z,
                             r->difuso.r,           r->difuso.g,           r->difuso.b,
@@ -515,6 +515,7 @@ __device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Boun
         for (int c = 0; c < 3; ++c) umma::tmem_st16(ta + 16u * c, *reinterpret_cast<const uint32_t(*)[16]>(w + 16 * c));
     }
     return amax;
+    }
 }
 
 // Largest value over the warp, folded into *dst (values are >= 0, so their
@@ -528,7 +529,7 @@ __device__ __forceinline__ void warp_amax(float v, float* dst) {
 // `f8` (FP8 only): scale words.  TRACK: the per-layer input amax is folded
 // into amax[0..5]; with `amax_all` every tile contributes, otherwise only the
 // first tile of each slot (the delayed-scaling estimate).
-template <int PREC, bool TRACK, int NL>
+template <int PREC, bool TRACK, int NL, bool HASH>
 __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
                                                             const uint32_t* __restrict__ n_dev, Bounds bounds,
                                                             HashGrid hg,
@@ -605,7 +606,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
         iph ^= 1u;
         // rows past the end of a partial tile encode stale staging bytes; the
         // rows of the MLP are independent and those outputs are never stored
-        const float a0 = encode_to_tmem<PREC>(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds, hg,
+        const float a0 = encode_to_tmem<PREC, HASH>(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds, hg,
                                               qs[0], tmem_a + tlane);
         if (track) warp_amax(valid ? a0 : 0.0f, &amax[0]);
         umma::tmem_wait_st();
@@ -1353,6 +1354,16 @@ int with_layers(int nl, F&& f) {
     }
 }
 
+// Calls f(integral_constant<int, NL>, integral_constant<bool, HASH>) for the
+// model's layer count and encoding.
+template <typename F>
+int with_model(const ColorMlp* n, F&& f) {
+    return with_layers(n->nl, [&](auto c) {
+        if (n->hlevels) return f(c, std::integral_constant<bool, true>{});
+        return f(c, std::integral_constant<bool, false>{});
+    });
+}
+
 uint64_t splitmix(uint64_t& s) {
     uint64_t z = (s += 0x9E3779B97F4A7C15ull);
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -1506,19 +1517,20 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
     const uint32_t grid = infer_grid(n, tiles);
     const size_t smem = mlp::kInferSmem + 1024;
     cudaError_t e = cudaSuccess;
-    const int rc = with_layers(n->nl, [&](auto c) {
+    const int rc = with_model(n, [&](auto c, auto h) {
         constexpr int NL = decltype(c)::value;
+        constexpr bool HASH = decltype(h)::value;
         if (n->prec == mlp::kPrecF16) {
-            mlp::k_infer<mlp::kPrecF16, false, NL><<<grid, mlp::kInferThreads, smem, s>>>(
+            mlp::k_infer<mlp::kPrecF16, false, NL, HASH><<<grid, mlp::kInferThreads, smem, s>>>(
                 in, count, n_dev, n->bounds, hash_view(n, false), n->inf, out, img, thr, nullptr, nullptr, 0);
         } else if (n->prec == mlp::kPrecBF16) {
-            mlp::k_infer<mlp::kPrecBF16, false, NL><<<grid, mlp::kInferThreads, smem, s>>>(
+            mlp::k_infer<mlp::kPrecBF16, false, NL, HASH><<<grid, mlp::kInferThreads, smem, s>>>(
                 in, count, n_dev, n->bounds, hash_view(n, false), n->inf_bf, out, img, thr, nullptr, nullptr, 0);
         } else {
             mlp::k_pack_f8<NL><<<NL, 1024, 0, s>>>(n->w, n->ema, n->dstate, n->decay, n->inf_f8, n->f8);
             cudaError_t e2 = cudaGetLastError();
             if (e2 != cudaSuccess) return cuda_fail(e2, "mlp inference: FP8 weight image");
-            mlp::k_infer<mlp::kPrecF8, true, NL><<<grid, mlp::kInferThreads, smem, s>>>(
+            mlp::k_infer<mlp::kPrecF8, true, NL, HASH><<<grid, mlp::kInferThreads, smem, s>>>(
                 in, count, n_dev, n->bounds, hash_view(n, false), n->inf_f8, out, img, thr, n->f8, n->f8 + mlp::kF8Amax,
                 0);
             e2 = cudaGetLastError();
@@ -1543,9 +1555,10 @@ int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStrea
     const uint32_t grid = std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, (uint32_t)n->sms);
     cudaError_t e = cudaMemsetAsync(n->f8 + mlp::kF8Amax, 0, mlp::kMaxLayers * sizeof(float), s);
     if (e != cudaSuccess) return cuda_fail(e, "tfgMlpCalibrate");
-    with_layers(n->nl, [&](auto c) {
+    with_model(n, [&](auto c, auto h) {
         constexpr int NL = decltype(c)::value;
-        mlp::k_infer<mlp::kPrecF16, true, NL><<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(
+        constexpr bool HASH = decltype(h)::value;
+        mlp::k_infer<mlp::kPrecF16, true, NL, HASH><<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(
             in, count, nullptr, n->bounds, hash_view(n, false), n->inf, nullptr, nullptr, nullptr, nullptr,
             n->f8 + mlp::kF8Amax, 1);
         return 0;
@@ -1673,10 +1686,14 @@ namespace {
 template <int NL>
 void set_kernel_attrs() {
     const int ism = M::kInferSmem + 1024;
-    cudaFuncSetAttribute(M::k_infer<M::kPrecF16, false, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
-    cudaFuncSetAttribute(M::k_infer<M::kPrecF16, true, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
-    cudaFuncSetAttribute(M::k_infer<M::kPrecBF16, false, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
-    cudaFuncSetAttribute(M::k_infer<M::kPrecF8, true, NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF16, false, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF16, true, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecBF16, false, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF8, true, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF16, false, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF16, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecBF16, false, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
+    cudaFuncSetAttribute(M::k_infer<M::kPrecF8, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
     cudaFuncSetAttribute(M::k_train<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kTrainSmem + 1024);
     cudaFuncSetAttribute(M::k_wgrad<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
 }
