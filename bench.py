@@ -206,6 +206,9 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
     from tfg_b200.nrc import ColorMLP, NrcRenderer
 
     params = pt.RenderParams(max_depth=DEPTH, rr_min_depth=RR, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT)
+    # launch settings tuned for single-sample passes; cache frames and the
+    # plain passes they are compared with both use them
+    tuning_1spp, _ = pt.autotune(ds, params, repeats=3)
     mlp = ColorMLP(batch=16384, seed=2024)
     mlp.set_bounds(*scene.bounds)
     r = NrcRenderer(ds, mlp, params, train_steps=4, use_graph=True)
@@ -351,6 +354,7 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
         "frames": 48 + frames, "warmup_frames": 48, "camera": "orbit 1 deg/frame", "train_samples_per_frame": 4 * 16384,
         "ms_per_frame_nrc": round(t_nrc, 3), "ms_per_pass_plain_1spp": round(t_pt, 3),
         "plain_spp_at_equal_time": spp_eq, "relmse_nrc": round(e_nrc, 5), "relmse_plain": round(e_pt, 5),
+        "tuning": tuning_1spp.__dict__,
         "relmse_ratio_plain_over_nrc": round(e_pt / e_nrc, 3), "relmse_x_time_ratio": round(ratio_time, 3),
         "reference_spp": ref_spp, "adam_steps": int(st["adam_t"]), "loss_ema": round(st["loss_ema"], 5),
         "mlp_inference": {"queries": n, "ms": round(t_inf, 4), "tflops": round(flops / (t_inf * 1e-3) / 1e12, 2),
@@ -889,9 +893,10 @@ def main():
             "tuning": tuning.__dict__, "seconds": round(tune_s, 2), "spp_per_pass": min(SPP, 16),
             "pass_ms_start": round(tune_table[0][1], 3), "pass_ms_tuned": round(tuned_ms, 3),
             "candidates": [[t.wavefront_paths, t.trace_threads, t.trace_warps_per_sm, t.refill_min,
-                            t.shadow_one_lane, t.refill_min_primary, round(ms, 3)] for t, ms in tune_table],
+                            t.shadow_one_lane, t.refill_min_primary, t.overlap_shadow, round(ms, 3)]
+                           for t, ms in tune_table],
             "candidate_fields": ["wavefront_paths", "trace_threads", "trace_warps_per_sm", "refill_min",
-                                 "shadow_one_lane", "refill_min_primary", "ms_per_pass"],
+                                 "shadow_one_lane", "refill_min_primary", "overlap_shadow", "ms_per_pass"],
         },
         "gpu_launches": launches,
         "clocks": clocks,

@@ -60,6 +60,9 @@ TUNINGS = [
     pt.RenderTuning(shadow_one_lane=1),
     pt.RenderTuning(refill_min_primary=32),
     pt.RenderTuning(refill_min_primary=2, refill_min=29),
+    pt.RenderTuning(overlap_shadow=0),
+    pt.RenderTuning(overlap_shadow=0, wavefront_paths=2 * N),
+    pt.RenderTuning(overlap_shadow=1, wavefront_paths=3 * N + 7, trace_threads=64, shadow_one_lane=1),
     pt.RenderTuning(wavefront_paths=2 * N + 1000, trace_threads=256, trace_warps_per_sm=16, refill_min=12,
                     shadow_one_lane=1),
 ]
@@ -133,8 +136,9 @@ def test_cache_frames_under_tuning(scene, graph):
 
     d = pt.RenderTuning.default()
     want = frames([d, d, d])
-    got = frames([pt.RenderTuning(wavefront_paths=4000), pt.RenderTuning(wavefront_paths=4 * N, trace_threads=64),
-                  pt.RenderTuning(wavefront_paths=N // 3, shadow_one_lane=1, refill_min=3)])
+    got = frames([pt.RenderTuning(wavefront_paths=4000, overlap_shadow=1),
+                  pt.RenderTuning(wavefront_paths=4 * N, trace_threads=64),
+                  pt.RenderTuning(wavefront_paths=N // 3, shadow_one_lane=1, refill_min=3, overlap_shadow=1)])
     for g, w in zip(got, want):
         assert np.isfinite(g).all()
         np.testing.assert_array_equal(g, w)
@@ -144,7 +148,7 @@ def test_bad_tunings_are_rejected(built):
     for bad in (pt.RenderTuning(wavefront_paths=100), pt.RenderTuning(wavefront_paths=(1 << 26) + 1),
                 pt.RenderTuning(trace_threads=96), pt.RenderTuning(refill_min=0), pt.RenderTuning(refill_min=33),
                 pt.RenderTuning(trace_warps_per_sm=-1), pt.RenderTuning(shadow_one_lane=2),
-                pt.RenderTuning(refill_min_primary=33)):
+                pt.RenderTuning(refill_min_primary=33), pt.RenderTuning(overlap_shadow=2)):
         with pytest.raises(TfgError):
             pt.set_tuning(bad)
     assert pt.get_tuning() == pt.RenderTuning.default()

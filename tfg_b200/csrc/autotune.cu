@@ -4,8 +4,9 @@
 // The settings (TfgRenderTuning) change only how the same paths are
 // scheduled -- the wavefront (queue) size, the traversal CTA size and
 // residency, the refill threshold of the persistent traversal lanes, how
-// many lanes share a shading point's shadow rays, and the first bounce's
-// refill threshold -- never what a path
+// many lanes share a shading point's shadow rays, the first bounce's refill
+// threshold, and whether the shadow stage overlaps the next trace -- never
+// what a path
 // computes, so every candidate renders the same image.  The search is one
 // pass of coordinate descent in that order, starting from the device's
 // current setting; a candidate replaces the best only when it is at least 1%
@@ -73,6 +74,7 @@ std::vector<int32_t> candidates(int k, uint32_t npix, uint64_t paths) {
         case 3: v = {4, 8, 12, 16, 24, 32}; break;
         case 4: v = {0, 1}; break;
         case 5: v = {0, 16, 24, 32}; break;
+        case 6: v = {0, 1}; break;
     }
     return v;
 }
@@ -84,7 +86,8 @@ int32_t& field(TfgRenderTuning& t, int k) {
         case 2: return t.trace_warps_per_sm;
         case 3: return t.refill_min;
         case 4: return t.shadow_one_lane;
-        default: return t.refill_min_primary;
+        case 5: return t.refill_min_primary;
+        default: return t.overlap_shadow;
     }
 }
 
@@ -136,7 +139,7 @@ extern "C" int tfgRenderAutotune(const TfgRenderParams* params, const TfgCamara*
     float best_ms = 0.0f;
     if (!rc) rc = time_tuning(dev, sc, best, repeats, s, e0, e1, &best_ms);
     if (!rc) record(best, best_ms);
-    for (int k = 0; k < 6 && !rc; ++k) {
+    for (int k = 0; k < 7 && !rc; ++k) {
         for (int32_t v : candidates(k, npix, paths)) {
             TfgRenderTuning cand = best;
             if (field(cand, k) == v) continue;

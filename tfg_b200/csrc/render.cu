@@ -76,6 +76,11 @@ struct Workspace {
     float4* ts = nullptr;                   // training scratch, 10 float4 per path
     uint32_t* counters = nullptr;           // per bounce: rays, fetch, shadows, spare
     uint32_t generation = 0;                // changes whenever a buffer is reallocated
+    // A second stream for the shadow stage, which then runs beside the next
+    // bounce's closest-hit trace: fork / join events per bounce.
+    cudaStream_t side = nullptr;
+    cudaEvent_t fork[kMaxBounces] = {};
+    cudaEvent_t join[kMaxBounces] = {};
 };
 
 struct PassArgs {
@@ -768,6 +773,14 @@ int ensure_workspace(int dev, int slot, size_t paths, bool nrc, Workspace& out) 
         if (e != cudaSuccess) { w.cap = 0; return fail((int)e, std::string("render workspace: ") + cudaGetErrorString(e)); }
         w.cap = cap;
     }
+    if (!w.side) {
+        e = cudaStreamCreateWithFlags(&w.side, cudaStreamNonBlocking);
+        for (int b = 0; b < kMaxBounces && e == cudaSuccess; ++b) {
+            e = cudaEventCreateWithFlags(&w.fork[b], cudaEventDisableTiming);
+            if (e == cudaSuccess) e = cudaEventCreateWithFlags(&w.join[b], cudaEventDisableTiming);
+        }
+        if (e != cudaSuccess) { w.side = nullptr; return fail((int)e, std::string("render streams: ") + cudaGetErrorString(e)); }
+    }
     if (nrc && w.train_cap < paths) {
         e = grow((void**)&w.ts, paths * 10 * sizeof(float4));
         ++w.generation;
@@ -846,7 +859,7 @@ int shapes_for(int dev, LaunchShapes& s) {
 // whose per-pixel outputs take one sample per pixel at a time).
 struct Tuning {
     uint32_t wavefront = 0;
-    int threads = 128, warps_per_sm = 0, refill = 8, refill_primary = 8, shadow_one_lane = 0;
+    int threads = 128, warps_per_sm = 0, refill = 8, refill_primary = 8, shadow_one_lane = 0, overlap_shadow = 0;
 };
 
 Tuning resolve_tuning(int dev, uint32_t npix, int spp, bool nrc, uint32_t* generation) {
@@ -867,6 +880,7 @@ Tuning resolve_tuning(int dev, uint32_t npix, int spp, bool nrc, uint32_t* gener
     r.refill = t.refill_min;
     r.refill_primary = t.refill_min_primary > 0 ? t.refill_min_primary : t.refill_min;
     r.shadow_one_lane = t.shadow_one_lane;
+    r.overlap_shadow = t.overlap_shadow;
     return r;
 }
 
@@ -892,6 +906,8 @@ int render_tuning_check(const TfgRenderTuning& t) {
         return fail(TFG_E_INVALID, "render tuning: shadow_one_lane must be 0 or 1");
     if (t.refill_min_primary < 0 || t.refill_min_primary > 32)
         return fail(TFG_E_INVALID, "render tuning: refill_min_primary must be in [0, 32]");
+    if (t.overlap_shadow != 0 && t.overlap_shadow != 1)
+        return fail(TFG_E_INVALID, "render tuning: overlap_shadow must be 0 or 1");
     return ok();
 }
 
@@ -1124,16 +1140,23 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
     cudaError_t e = cudaSuccess;
     const bool times = (prm.profile & TFG_PROFILE_TIMES) != 0;
     const bool counts = (prm.profile & TFG_PROFILE_COUNTS) != 0;
-    auto stage = [&](int id, auto&& launch) {
+    auto stage_on = [&](int id, cudaStream_t st, auto&& launch) {
         if (times) {
             StageEvents ev = profiler_pair(id);
-            cudaEventRecord(ev.start, stream);
+            cudaEventRecord(ev.start, st);
             launch();
-            cudaEventRecord(ev.stop, stream);
+            cudaEventRecord(ev.stop, st);
         } else {
             launch();
         }
     };
+    auto stage = [&](int id, auto&& launch) { stage_on(id, stream, launch); };
+    // Shadow stage on the side stream: bounce b's shadow rays run beside
+    // bounce b+1's closest-hit trace (which reads only rays and writes only
+    // hits); the next shade, which rewrites the shadow items and adds to the
+    // same radiance sums, waits for them, so every sum keeps its order.
+    const bool overlap = tu.overlap_shadow && ws.side;
+    cudaStream_t sstream = overlap ? ws.side : stream;
     a.frame = frame;
     a.img = img;
     a.npix = N;
@@ -1162,16 +1185,33 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
                     else k_trace<1, false, MS><<<trace_grid, bt, smem, stream>>>(a, b, tab);
                 }
             });
+            if (overlap && b > 0) {   // the previous bounce's shadow stage ends before this shade
+                e = cudaStreamWaitEvent(stream, ws.join[b - 1], 0);
+                if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+            }
             stage(2, [&] { k_shade<MS><<<shade_grid, 256, 0, stream>>>(a, b, tab); });
-            stage(3, [&] {
+            if (overlap) {
+                e = cudaEventRecord(ws.fork[b], stream);
+                if (e == cudaSuccess) e = cudaStreamWaitEvent(sstream, ws.fork[b], 0);
+                if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+            }
+            stage_on(3, sstream, [&] {
                 if (fmt == 0) {
-                    if (counts) k_shadow<0, true, MS><<<shadow_grid, bt, smem, stream>>>(a, b, tab);
-                    else k_shadow<0, false, MS><<<shadow_grid, bt, smem, stream>>>(a, b, tab);
+                    if (counts) k_shadow<0, true, MS><<<shadow_grid, bt, smem, sstream>>>(a, b, tab);
+                    else k_shadow<0, false, MS><<<shadow_grid, bt, smem, sstream>>>(a, b, tab);
                 } else {
-                    if (counts) k_shadow<1, true, MS><<<shadow_grid, bt, smem, stream>>>(a, b, tab);
-                    else k_shadow<1, false, MS><<<shadow_grid, bt, smem, stream>>>(a, b, tab);
+                    if (counts) k_shadow<1, true, MS><<<shadow_grid, bt, smem, sstream>>>(a, b, tab);
+                    else k_shadow<1, false, MS><<<shadow_grid, bt, smem, sstream>>>(a, b, tab);
                 }
             });
+            if (overlap) {
+                e = cudaEventRecord(ws.join[b], sstream);
+                if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
+            }
+        }
+        if (overlap) {   // join the side stream before the pixels are resolved
+            e = cudaStreamWaitEvent(stream, ws.join[prm.max_depth - 1], 0);
+            if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
         }
         stage(4, [&] { k_resolve<MS><<<res_blocks, 256, 0, stream>>>(a, tab); });
         e = cudaGetLastError();
@@ -1316,6 +1356,7 @@ extern "C" void tfgRenderTuningDefault(TfgRenderTuning* t) {
     t->refill_min = 8;
     t->shadow_one_lane = 0;
     t->refill_min_primary = 0;
+    t->overlap_shadow = 1;
 }
 
 extern "C" int tfgRenderTuningSet(const TfgRenderTuning* t) {

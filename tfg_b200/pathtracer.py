@@ -261,19 +261,21 @@ class RenderTuning:
     refill_min: int = 8           # idle lanes that make a traversal warp fetch new rays
     shadow_one_lane: int = 0      # 1: one lane traces all lights of a shading point
     refill_min_primary: int = 0   # first-bounce refill threshold; 0 = refill_min
+    overlap_shadow: int = 1       # 1: shadow stage on a second stream beside the next trace
 
     def c(self) -> CRenderTuning:
         t = CRenderTuning()
         t.wavefront_paths, t.trace_threads, t.trace_warps_per_sm = (self.wavefront_paths, self.trace_threads,
                                                                     self.trace_warps_per_sm)
         t.refill_min, t.shadow_one_lane = self.refill_min, self.shadow_one_lane
-        t.refill_min_primary = self.refill_min_primary
+        t.refill_min_primary, t.overlap_shadow = self.refill_min_primary, self.overlap_shadow
         return t
 
     @staticmethod
     def of(t: CRenderTuning) -> "RenderTuning":
         return RenderTuning(int(t.wavefront_paths), int(t.trace_threads), int(t.trace_warps_per_sm),
-                            int(t.refill_min), int(t.shadow_one_lane), int(t.refill_min_primary))
+                            int(t.refill_min), int(t.shadow_one_lane), int(t.refill_min_primary),
+                            int(t.overlap_shadow))
 
     @staticmethod
     def default() -> "RenderTuning":
