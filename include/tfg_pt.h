@@ -472,6 +472,11 @@ void tfgHashGridConfigReference(TfgHashGridConfig* c);
  * of the tables' debiased average. */
 int  tfgMlpCreateHashGrid(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
                           const TfgHashGridConfig* config, TfgColorMLP** out);
+/* The cache model with `width` = 64 or 128 units per hidden layer (128: 3 or
+ * 5 hidden layers, FP16 / BF16 inference; FP8 is built for width 64) and
+ * the frequency encoding (`config` null) or the composite encoding. */
+int  tfgMlpCreateWide(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
+                      int32_t width, const TfgHashGridConfig* config, TfgColorMLP** out);
 /* Length of the FP32 table arrays (0 for the frequency encoding). */
 int64_t tfgMlpHashParamCount(const TfgColorMLP* mlp);
 /* Table arrays [level][entry][feature]: which = 0 values, 1 average, 2 Adam m, 3 Adam v. */
@@ -484,8 +489,8 @@ int  tfgMlpSetHashParams(TfgColorMLP* mlp, const float* host, int64_t count);
 int  tfgMlpComputeGradientEx(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
                              float* host_grad, uint32_t count, float* host_table_grad, int64_t table_count,
                              float* loss_out);
-/* Length of the model's FP32 parameter arrays: 6144 + 4096 (hidden - 1) +
- * 1024 (23552 for 5 hidden layers). */
+/* Length of the model's FP32 parameter arrays: 96 W + W^2 (hidden - 1) + 16 W
+ * for width W (23552 for 5 hidden layers of 64, 79872 for 5 of 128). */
 int32_t tfgMlpParamCount(const TfgColorMLP* mlp);
 void tfgMlpDestroy(TfgColorMLP* mlp);
 /* ColorMLP::setBounds (mlp.cpp:89-93): position normalisation box. */

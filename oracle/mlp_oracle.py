@@ -23,18 +23,22 @@ from __future__ import annotations
 import numpy as np
 from scipy.special import ndtr
 
-def shapes(hidden_layers: int = 5) -> list[tuple[int, int]]:
-    return [(64, 96)] + [(64, 64)] * (hidden_layers - 1) + [(16, 64)]
+def shapes(hidden_layers: int = 5, width: int = 64) -> list[tuple[int, int]]:
+    return [(width, 96)] + [(width, width)] * (hidden_layers - 1) + [(16, width)]
 
 
 SHAPES = shapes(5)
 
 
 def split(flat):
-    """Layer matrices of a flat parameter array; its length gives the depth."""
-    hidden = (len(flat) - 6144 - 1024) // 4096 + 1
+    """Layer matrices of a flat parameter array; its length gives the depth
+    and the width (64 or 128)."""
+    for width in (64, 128):
+        hidden = (len(flat) - 112 * width) // (width * width) + 1
+        if hidden >= 1 and sum(r * c for r, c in shapes(hidden, width)) == len(flat):
+            break
     out, o = [], 0
-    for r, c in shapes(hidden):
+    for r, c in shapes(hidden, width):
         out.append(np.asarray(flat[o:o + r * c], np.float64).reshape(r, c))
         o += r * c
     return out

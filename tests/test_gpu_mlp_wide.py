@@ -1,0 +1,172 @@
+"""The cache network with 128 units per hidden layer (3 or 5 hidden layers)
+against the FP64 oracle: inference in FP16 and BF16, the gradients of the
+layers (and of the hash-grid tables with the composite encoding), online
+training, and a whole cache frame.  FP8 is built for width 64 only and must
+be refused."""
+import numpy as np
+import pytest
+import torch
+
+from oracle import mlp_oracle as mo
+from oracle import oracle as orc
+from tfg_b200 import TfgError
+from tfg_b200 import pathtracer as pt
+from tfg_b200 import scenes
+from tfg_b200.nrc import BF16, FP8, HASHGRID, WEIGHTS, ColorMLP, NrcRenderer, split_layers
+from tfg_b200.structs import DATOS_MLP
+
+pytestmark = pytest.mark.gpu
+
+LO, HI = (-6.0, -4.0, -10.0), (6.0, 6.0, 2.0)
+SMALL = {"n_levels": 8, "log2_hashmap_size": 12, "base_resolution": 4.0, "per_level_scale": 2.0}
+
+
+def _datos(rng, n, target_fn=None):
+    d = np.zeros(n, DATOS_MLP)
+    pos = rng.uniform(LO, HI, (n, 3))
+    for j, k in enumerate("xyz"):
+        d["posicion"][k] = pos[:, j]
+        d["direccion"][k] = rng.uniform(0, 1, n)
+        d["normal"][k] = rng.uniform(0, 1, n)
+    kd = rng.uniform(0, 1, (n, 3)).astype(np.float32)
+    for j, k in enumerate("rgb"):
+        d["difuso"][k] = kd[:, j]
+        d["especular"][k] = 0.0
+    y = target_fn(pos, kd) if target_fn else rng.uniform(0, 2, (n, 3))
+    for j, k in enumerate("rgb"):
+        d["color"][k] = y[:, j]
+    return d
+
+
+def _dev(a):
+    return torch.from_numpy(np.ascontiguousarray(a).view(np.uint8).copy()).cuda()
+
+
+def _f16(w):
+    return np.asarray(w, np.float32).astype(np.float16).astype(np.float64)
+
+
+@pytest.mark.parametrize("hidden", [5, 3])
+def test_inference_matches_fp64_model(built, hidden):
+    m = ColorMLP(batch=4096, seed=31 + hidden, hidden_layers=hidden, width=128)
+    m.set_bounds(LO, HI)
+    assert m.n_params == 96 * 128 + (hidden - 1) * 128 * 128 + 16 * 128
+    rng = np.random.default_rng(hidden)
+    n = 2000
+    d = _datos(rng, n)
+    out = torch.zeros(n * 3, device="cuda")
+    m.inference(_dev(d), out, n)
+    torch.cuda.synchronize()
+    got = out.view(n, 3).cpu().numpy()
+    W = [_f16(w) for w in split_layers(m.get_params(WEIGHTS))]
+    assert W[1].shape == (128, 128)
+    x = mo.encode(mo.rows15(d, LO, HI))
+    raw = mo.forward(W, x)[0]
+    scale = np.abs(raw).mean() + 1e-3
+    err = np.abs(got - mo.scrub(raw)) / scale
+    assert np.isfinite(got).all()
+    assert err.max() < 0.05, f"max scaled error {err.max():.3e}"
+    assert err.mean() < 0.01
+    # BF16 against the BF16-rounded model
+    m.set_precision(BF16)
+    b = torch.zeros(n * 3, device="cuda")
+    m.inference(_dev(d), b, n)
+    torch.cuda.synchronize()
+    ref_b = mo.scrub(mo.forward_quantized(W, x, "bf16"))
+    eb = np.abs(b.view(n, 3).cpu().numpy() - ref_b).mean() / scale
+    assert eb < 0.01, eb
+    with pytest.raises(TfgError):
+        m.set_precision(FP8)
+    m.close()
+
+
+def test_gradient_matches_fp64_model(built):
+    m = ColorMLP(batch=4096, seed=7, width=128)
+    m.set_bounds(LO, HI)
+    rng = np.random.default_rng(11)
+    n_avail = 20000
+    d = _datos(rng, n_avail)
+    w = m.get_params(WEIGHTS)
+    g, loss = m.compute_gradient(_dev(d), n_avail, seed=5)
+    idx = np.zeros(m.batch, np.int32)
+    orc.cpu.orc_indices(orc.p(idx), n_avail, m.batch, 5)
+    sel = d[idx]
+    x = mo.encode(mo.rows15(sel, LO, HI))
+    y = np.stack([sel["color"][k] for k in "rgb"], 1).astype(np.float64)
+    ref_loss, ref = mo.loss_and_grad([_f16(a) for a in split_layers(w)], x, y)
+    assert abs(loss - ref_loss) / ref_loss < 0.02, (loss, ref_loss)
+    for l, (gg, rr) in enumerate(zip(split_layers(g), ref)):
+        rel = np.linalg.norm(gg - rr) / (np.linalg.norm(rr) + 1e-30)
+        assert rel < 0.05, f"layer {l}: relative gradient error {rel:.3e}"
+    m.close()
+
+
+def test_composite_encoding_gradients(built):
+    m = ColorMLP(batch=4096, seed=9, width=128, encoding=HASHGRID, hashgrid=SMALL)
+    m.set_bounds(LO, HI)
+    rng = np.random.default_rng(2)
+    m.set_table(rng.uniform(-0.5, 0.5, m.n_table).astype(np.float32))
+    n_avail = 20000
+    d = _datos(rng, n_avail)
+    w = m.get_params(WEIGHTS)
+    tab = m.get_table(WEIGHTS).astype(np.float64)
+    g, gt, loss = m.compute_gradient_ex(_dev(d), n_avail, seed=3)
+    idx = np.zeros(m.batch, np.int32)
+    orc.cpu.orc_indices(orc.p(idx), n_avail, m.batch, 3)
+    sel = d[idx]
+    x, corners = mo.composite_encode(mo.rows15(sel, LO, HI), tab, SMALL)
+    y = np.stack([sel["color"][k] for k in "rgb"], 1).astype(np.float64)
+    ref_loss, ref, dx = mo.loss_and_grad([_f16(a) for a in split_layers(w)], x, y, want_dx=True)
+    assert abs(loss - ref_loss) / ref_loss < 0.02, (loss, ref_loss)
+    for l, (gg, rr) in enumerate(zip(split_layers(g), ref)):
+        rel = np.linalg.norm(gg - rr) / (np.linalg.norm(rr) + 1e-30)
+        assert rel < 0.05, f"layer {l}: relative gradient error {rel:.3e}"
+    ref_t = mo.table_grad(dx[:, :2 * SMALL["n_levels"]], corners, m.n_table)
+    rel = np.linalg.norm(gt - ref_t) / np.linalg.norm(ref_t)
+    assert rel < 0.05, f"table gradient: relative error {rel:.3e}"
+    m.close()
+
+
+def test_online_training_learns_a_signal(built):
+    def f(pos, kd):
+        s = 0.5 + 0.4 * np.sin(1.3 * pos[:, 0]) * np.cos(0.9 * pos[:, 2])
+        return np.stack([s * kd[:, 0], s * kd[:, 1], s * kd[:, 2]], 1) + 0.05
+
+    m = ColorMLP(batch=16384, seed=8, width=128)
+    m.set_bounds(LO, HI)
+    rng = np.random.default_rng(5)
+    n = 65536
+    dd = _dev(_datos(rng, n, f))
+    first = m.train_step(dd, n)
+    for _ in range(200):
+        m.train_step(dd, n, read_loss=False)
+    last = m.train_step(dd, n)
+    assert np.isfinite(last) and last < 0.2 * first, (first, last)
+    assert m.state()["adam_t"] == 202
+    m.close()
+
+
+def test_cache_frames_with_width_128(built):
+    s = scenes.sized_terrain_scene(20000, 160, 96, 2, seed=45)
+    ds = pt.DeviceScene(s, "cuda")
+    params = pt.RenderParams(max_depth=6, rr_min_depth=3, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT)
+    m = ColorMLP(batch=16384, seed=5, width=128)
+    m.set_bounds(*s.bounds)
+    r = NrcRenderer(ds, m, params, train_steps=2, max_records=8192, min_records=256, use_graph=True)
+    for f in range(8):
+        r.frame(f, warmup=True)
+    for f in range(8, 16):
+        r.frame(f, warmup=False, accumulate=True)
+    r.stream.synchronize()
+    img = r.mean_image().cpu().numpy()
+    assert np.isfinite(img).all() and img.mean() > 0
+    assert m.state()["adam_t"] >= 16
+    m.close()
+    ds.close()
+
+
+def test_width_128_limits(built):
+    with pytest.raises(TfgError):
+        ColorMLP(batch=4096, hidden_layers=7, width=128)
+    with pytest.raises(TfgError):
+        ColorMLP(batch=4096, width=96)

@@ -97,6 +97,39 @@ constexpr int kFwdBytesMax = fwd_bytes_of(kMaxLayers);            // 67584
 constexpr int kWeightRegion = (kFwdBytesMax + 1023) / 1024 * 1024;  // 68608
 static_assert(fwd_bytes_of(6) == 51200 && bwd_bytes_of(6) == 40960 && params_of(6) == 23552, "default layout");
 
+// The same layouts for hidden width HID (64 or 128; 128 for 3 or 5 hidden
+// layers): 96 -> HID, (nl - 2) x HID -> HID, HID -> 16.  Weight images keep
+// 64-feature (128-byte) SW128 K regions: layer 0 two regions of HID rows,
+// hidden layers HID/64 regions of HID rows, the last layer HID/64 regions of
+// 16 rows; the backward image W^T of layer l >= 1 has HID rows (input units)
+// and HID/64 regions of K (one for the last layer's K = 16).
+template <int HID> __host__ __device__ constexpr int rows_h(int nl, int l) { return l == nl - 1 ? 16 : HID; }
+template <int HID> __host__ __device__ constexpr int cols_h(int l) { return l == 0 ? 96 : HID; }
+template <int HID> __host__ __device__ constexpr int poff_h(int nl, int l) {
+    return l == 0 ? 0 : (l <= nl - 1 ? 96 * HID + (l - 1) * HID * HID : 96 * HID + (nl - 2) * HID * HID + 16 * HID);
+}
+template <int HID> __host__ __device__ constexpr int params_h(int nl) { return poff_h<HID>(nl, nl); }
+template <int HID> __host__ __device__ constexpr int foff_h(int nl, int l) {
+    return l == 0 ? 0
+                  : (l <= nl - 1 ? 2 * HID * 128 + (l - 1) * (HID / 64) * HID * 128
+                                 : 2 * HID * 128 + (nl - 2) * (HID / 64) * HID * 128 + (HID / 64) * 16 * 128);
+}
+template <int HID> __host__ __device__ constexpr int fwd_bytes_h(int nl) { return foff_h<HID>(nl, nl); }
+template <int HID> __host__ __device__ constexpr int boff_h(int, int l) { return (l - 1) * (HID / 64) * HID * 128; }
+template <int HID> __host__ __device__ constexpr int bwd_bytes_h(int nl) { return (nl - 2) * (HID / 64) * HID * 128 + HID * 128; }
+static_assert(params_h<64>(6) == params_of(6) && fwd_bytes_h<64>(6) == fwd_bytes_of(6) &&
+              bwd_bytes_h<64>(6) == bwd_bytes_of(6) && foff_h<64>(6, 5) == foff_of(6, 5) &&
+              poff_h<64>(8, 7) == poff_of(8, 7) && boff_h<64>(6, 3) == 2 * 8192, "width 64 keeps its layout");
+static_assert(params_h<128>(6) == 79872 && fwd_bytes_h<128>(6) == 167936 && bwd_bytes_h<128>(6) == 147456,
+              "width 128 layout");
+// Runtime forms for the host.
+constexpr int params_rt(int nl, int hid) { return hid == 128 ? params_h<128>(nl) : params_h<64>(nl); }
+constexpr int rows_rt(int nl, int l, int hid) { return hid == 128 ? rows_h<128>(nl, l) : rows_h<64>(nl, l); }
+constexpr int cols_rt(int l, int hid) { return hid == 128 ? cols_h<128>(l) : cols_h<64>(l); }
+constexpr int poff_rt(int nl, int l, int hid) { return hid == 128 ? poff_h<128>(nl, l) : poff_h<64>(nl, l); }
+constexpr int fwd_bytes_rt(int nl, int hid) { return hid == 128 ? fwd_bytes_h<128>(nl) : fwd_bytes_h<64>(nl); }
+constexpr int bwd_bytes_rt(int nl, int hid) { return hid == 128 ? bwd_bytes_h<128>(nl) : bwd_bytes_h<64>(nl); }
+
 // Every wait on a bulk copy or an MMA gives up after this long (a stuck
 // wait sets g_mlp_error; the host reports TFG_E_TIMEOUT), far above any
 // legitimate wait (microseconds).
@@ -722,6 +755,161 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
     if (warp == 0) umma::tmem_dealloc(tslot, 512);
 }
 
+// Width-128 inference (3 or 5 hidden layers; FP16 or BF16): the same
+// pipeline as k_infer with two 128-query slots per SM, each with 256 TMEM
+// columns (128 FP32 accumulator columns, then up to 64 columns of the next
+// layer's A operand), and the 164 KB weight image in shared memory.
+constexpr int kSlots128 = 2;
+constexpr int kInfer128Threads = 128 * kSlots128;
+constexpr int kInfer128Stage = fwd_bytes_h<128>(6);                       // 167936, 1024-aligned
+constexpr int kInfer128Smem = kInfer128Stage + kSlots128 * kStageBytes;   // 196608
+static_assert(kInfer128Stage % 1024 == 0 && kInfer128Smem + 1024 <= 227 * 1024, "width-128 inference shared memory");
+
+template <int PREC, int NL, bool HASH>
+__global__ void __launch_bounds__(kInfer128Threads, 1)
+    k_infer128(const TfgDatosMLP* __restrict__ in, uint32_t n_max, const uint32_t* __restrict__ n_dev, Bounds bounds,
+               HashGrid hg, const uint8_t* __restrict__ wimg, TfgColor* __restrict__ out, TfgColor* __restrict__ img,
+               const TfgColor* __restrict__ thr) {
+    static_assert(PREC != kPrecF8 && (NL == 4 || NL == 6), "width 128: FP16 / BF16, 3 or 5 hidden layers");
+    constexpr uint32_t kWBytes = fwd_bytes_h<128>(NL);
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sw = smem;
+    __shared__ uint64_t mb_w, mb_mma[kSlots128], mb_in[kSlots128], mb_drain[kSlots128];
+    __shared__ uint32_t tslot;
+    const int tid = threadIdx.x, warp = tid >> 5, q = warp & 3, t = tid & 127;
+    const int slot = tid / 128;
+    const bool leader = t == 0;
+    const bool issuer_warp = t < 32;
+    const int bar = 1 + slot;
+    uint8_t* stage = smem + kInfer128Stage + slot * kStageBytes;
+    const uint32_t n = n_dev ? min(*n_dev, n_max) : n_max;
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    if (blockIdx.x * kSlots128 >= ntiles) return;
+    if (warp == 0) umma::tmem_alloc(&tslot, 512);
+    if (tid == 0) {
+        umma::mbar_init(&mb_w, 1);
+        for (int k = 0; k < kSlots128; ++k) {
+            umma::mbar_init(&mb_mma[k], 1);
+            umma::mbar_init(&mb_in[k], 1);
+            umma::mbar_init(&mb_drain[k], 1);
+        }
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tlane = (uint32_t)(32 * q) << 16;
+    const uint32_t tmem = tslot + 256u * (uint32_t)slot;          // accumulator: columns 0..127 of the slot
+    const uint32_t tmem_a = tmem + 128u;                           // A operand: columns 128..191
+    const uint32_t tstride = gridDim.x * kSlots128;
+    const uint64_t wdesc = umma::sdesc_sw128(umma::smem_u32(sw));
+    auto fetch = [&](uint32_t tl) {
+        const uint32_t rows = min((uint32_t)kTile, n - tl * kTile);
+        umma::mbar_expect_tx(&mb_in[slot], rows * kRowBytes);
+        umma::bulk_g2s(stage, reinterpret_cast<const uint8_t*>(in) + (size_t)tl * kStageBytes, rows * kRowBytes,
+                       &mb_in[slot]);
+    };
+    if (tid == 0) {
+        umma::mbar_expect_tx(&mb_w, kWBytes);
+        umma::bulk_g2s(sw, wimg, kWBytes, &mb_w);
+    }
+    uint32_t tile = blockIdx.x * kSlots128 + slot;
+    bool pending = tile < ntiles;
+    if (pending && leader) fetch(tile);
+    bool ok = umma::mbar_wait(&mb_w, 0, kSpinLimit);
+    ok = __syncthreads_and(ok ? 1 : 0) != 0;
+    uint32_t mph = 0, iph = 0;
+    for (; tile < ntiles && ok; tile += tstride) {
+        const uint32_t row = tile * kTile + (uint32_t)t;
+        const bool valid = row < n;
+        ok = slot_all(bar, umma::mbar_wait(&mb_in[slot], iph, kSpinLimit));
+        if (!ok) break;
+        pending = false;
+        iph ^= 1u;
+        encode_to_tmem<PREC, HASH>(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds, hg, 1.0f,
+                                   tmem_a + tlane);
+        umma::tmem_wait_st();
+        umma::fence_before_sync();
+        slot_sync(bar);
+        if (tile + tstride < ntiles) {
+            if (leader) {
+                umma::fence_smem_to_async();
+                fetch(tile + tstride);
+            }
+            pending = true;
+        }
+#pragma unroll
+        for (int l = 0; l < NL; ++l) {
+            const bool last = l == NL - 1;
+            if (issuer_warp) {
+                umma::fence_after_sync();
+                constexpr uint32_t id_hid = umma::idesc_f16(kTile, 128, PREC == kPrecBF16);
+                constexpr uint32_t id_out = umma::idesc_f16(kTile, kOutPad, PREC == kPrecBF16);
+                if (umma::elect_one()) {
+#pragma unroll
+                    for (int s = 0; s < cols_h<128>(l) / 16; ++s) {
+                        const uint64_t bd = wdesc + (uint64_t)((foff_h<128>(NL, l) + (s >> 2) * (rows_h<128>(NL, l) * 128) +
+                                                                (s & 3) * 32) >> 4);
+                        umma::mma_f16_ta(tmem, tmem_a + 8u * s, bd, last ? id_out : id_hid, s > 0);
+                    }
+                    umma::mma_commit(&mb_mma[slot]);
+                }
+                __syncwarp();
+            }
+            ok = slot_all(bar, umma::mbar_wait(&mb_mma[slot], mph, kSpinLimit));
+            mph ^= 1u;
+            if (!ok) break;
+            umma::fence_after_sync();
+            if (!last) {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    float v[32];
+                    umma::tmem_ld32(tmem + tlane + 32u * h, v);
+                    uint32_t r[16];
+#pragma unroll
+                    for (int i = 0; i < 16; ++i)
+                        r[i] = PREC == kPrecBF16 ? relu_bf2(v[2 * i], v[2 * i + 1]) : relu_h2(v[2 * i], v[2 * i + 1]);
+                    umma::tmem_st16(tmem_a + tlane + 16u * h, r);
+                }
+                umma::tmem_wait_st();
+                umma::fence_before_sync();
+                slot_sync(bar);
+            } else {
+                float v[16];
+                umma::tmem_ld16(tmem + tlane, v);
+                if (valid && (out || img)) {
+                    const float cr = scrub(v[0]), cg = scrub(v[1]), cb = scrub(v[2]);
+                    if (img) {
+                        const TfgColor th = thr[row];
+                        if (th.r > 0 || th.g > 0 || th.b > 0) {
+                            TfgColor f = img[row];
+                            f.r = f.r + th.r * cr;
+                            f.g = f.g + th.g * cg;
+                            f.b = f.b + th.b * cb;
+                            img[row] = f;
+                        }
+                    } else {
+                        out[row] = TfgColor{cr, cg, cb};
+                    }
+                }
+                umma::fence_before_sync();
+                slot_sync(bar);
+            }
+        }
+    }
+    if (pending) umma::mbar_wait(&mb_in[slot], iph, kSpinLimit);
+    if (!ok && issuer_warp) {
+        if (umma::elect_one()) {
+            umma::mma_commit(&mb_drain[slot]);
+            umma::mbar_wait(&mb_drain[slot], 0, kSpinLimit);
+        }
+        __syncwarp();
+    }
+    if (!ok && leader) atomicExch(&g_mlp_error, 1);
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tslot, 512);
+}
+
 // FP8 inference image from the debiased weight average, one block per
 // layer: the layer's weight scale wq = 448 / amax|W| goes to f8[kF8WQ + l].
 // Skipped when the image already holds the weights of this Adam step.
@@ -969,14 +1157,224 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     if (warp == 0) umma::tmem_dealloc(tmem, 128);
 }
 
+// ------------------------------------------------------------------ width-128 training
+// k_train for 128-wide layers.  The whole network's forward and backward
+// images (308 KB) do not fit in shared memory, so they are streamed: the
+// NL forward images and then the NL - 1 backward images of each tile pass
+// through two 32 KB buffers, each bulk-copied as soon as the MMAs that read
+// the buffer's previous image have completed (one layer ahead).
+constexpr int kT128Buf = 32768;
+constexpr int kT128SmemA = 2 * kT128Buf;                    // activations: 2 regions x 16 KB
+constexpr int kT128Smem = kT128SmemA + 2 * kTile * 128;    // 98304
+
+// 32 values of row r, features f0 .. f0 + 31 (f0 a multiple of 32), into the
+// two-region A buffer as FP16 or BF16.
+template <bool BF16>
+__device__ __forceinline__ void store_row32(uint8_t* a, int r, int f0, const float* v) {
+    uint8_t* region = a + (f0 >> 6) * (kTile * 128);
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        uint32_t q[4];
+#pragma unroll
+        for (int e = 0; e < 4; ++e)
+            q[e] = BF16 ? pack_bf2(v[8 * j + 2 * e], v[8 * j + 2 * e + 1]) : pack_h2(v[8 * j + 2 * e], v[8 * j + 2 * e + 1]);
+        *reinterpret_cast<uint4*>(region + umma::sw128_offset(r, ((f0 & 63) >> 3) + j)) = make_uint4(q[0], q[1], q[2], q[3]);
+    }
+}
+
+// 32 features f0 .. f0 + 31 of sample s into a transposed tile of F features.
+template <int F>
+__device__ __forceinline__ void store_T32(uint8_t* tile, int s, int f0, const float* v) {
+    uint8_t* region = tile + (s >> 6) * (F * 128);
+    const int c = (s & 63) >> 3, e = s & 7;
+#pragma unroll
+    for (int i = 0; i < 32; ++i)
+        *reinterpret_cast<__nv_bfloat16*>(region + umma::sw128_offset(f0 + i, c) + 2 * e) = __float2bfloat16_rn(v[i]);
+}
+
+template <int NL>
+__global__ void __launch_bounds__(128) k_train128(TrainArgs a) {
+    static_assert(NL == 4 || NL == 6, "width 128: 3 or 5 hidden layers");
+    constexpr int kItems = 2 * NL - 1;   // weight images per tile: NL forward, then NL - 1 backward
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sa = smem + kT128SmemA;
+    __shared__ uint64_t mb_w[2], mb_mma, mb_drain;
+    __shared__ uint32_t tslot;
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t ntiles = a.batch / kTile;
+    const uint32_t n_avail = a.state[S_NAVAIL];
+    const uint32_t seed = a.state[S_STEP];
+    if (blockIdx.x >= ntiles || n_avail < a.min_n || n_avail == 0) return;
+    const uint32_t total = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x * kItems;   // images this CTA loads
+    if (warp == 0) umma::tmem_alloc(&tslot, 256);
+    if (t == 0) {
+        umma::mbar_init(&mb_w[0], 1);
+        umma::mbar_init(&mb_w[1], 1);
+        umma::mbar_init(&mb_mma, 1);
+        umma::mbar_init(&mb_drain, 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t tlane = (uint32_t)(32 * warp) << 16;
+    // image g % kItems of the per-tile sequence, into buffer g & 1
+    bool wpend[2] = {false, false};
+    auto load = [&](uint32_t g) {
+        const int k = (int)(g % (uint32_t)kItems), b = (int)(g & 1u);
+        wpend[b] = true;   // every thread tracks it; thread 0 issues the copy
+        if (t != 0) return;
+        uint32_t bytes;
+        const uint8_t* src;
+        if (k < NL) {
+            bytes = k == NL - 1 ? 2 * 16 * 128 : 2 * 128 * 128;
+            src = a.fwd + foff_h<128>(NL, k);
+        } else {
+            const int l = NL - 1 - (k - NL);   // backward layers NL - 1 down to 1
+            bytes = l == NL - 1 ? 128 * 128 : 2 * 128 * 128;
+            src = a.bwd + boff_h<128>(NL, l);
+        }
+        umma::mbar_expect_tx(&mb_w[b], bytes);
+        umma::bulk_g2s(smem + b * kT128Buf, src, bytes, &mb_w[b]);
+    };
+    load(0);
+    if (total > 1) load(1);
+    uint32_t wph[2] = {0, 0}, g = 0, mph = 0;
+    bool ok = true;
+    float lsum = 0.0f;
+    // Wait for image g, issue one layer's MMAs from it, wait for them, then
+    // reuse its buffer for image g + 2.
+    auto run_layer = [&](uint32_t dcol, int K, int N, int w_region_bytes, bool bf16) {
+        const int b = (int)(g & 1u);
+        ok = all_ok(umma::mbar_wait(&mb_w[b], wph[b], kSpinLimit));
+        if (!ok) return;   // the copy stays pending: the exit path waits for it
+        wph[b] ^= 1u;
+        wpend[b] = false;
+        umma::fence_after_sync();
+        if (warp == 0) {
+            if (umma::elect_one()) {
+                issue_layer(tmem + dcol, sa, kTile * 128, smem + b * kT128Buf, w_region_bytes, K, N, bf16);
+                umma::mma_commit(&mb_mma);
+            }
+            __syncwarp();
+        }
+        ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+        mph ^= 1u;
+        if (ok && g + 2 < total) load(g + 2);
+        ++g;
+        umma::fence_after_sync();
+    };
+    for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const uint32_t s = tile * kTile + (uint32_t)t;
+        uint32_t st = seed ^ s;
+        const uint32_t idx = pcg_next(st) % n_avail;
+        const TfgDatosMLP d = a.buf[idx];
+        float tgt[3] = {d.color.r, d.color.g, d.color.b};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) if (tgt[k] > 100000.0f) tgt[k] = 100000.0f;
+        {
+            uint32_t w[48];
+            encode(d, a.bounds, a.hg, w);
+            store_encoded(sa, t, w);
+            float f[96];
+#pragma unroll
+            for (int k = 0; k < 48; ++k) {
+                const float2 ff = __half22float2(*reinterpret_cast<__half2*>(&w[k]));
+                f[2 * k] = ff.x; f[2 * k + 1] = ff.y;
+            }
+            store_T<96>(a.hT[0] + (size_t)tile * (2 * 96 * 128), t, f);
+        }
+        umma::fence_smem_to_async();
+        __syncthreads();
+        uint32_t mask[NL - 1][4];
+        // forward
+        for (int l = 0; l < NL && ok; ++l) {
+            const bool last = l == NL - 1;
+            run_layer(last ? 128u : 0u, cols_h<128>(l), last ? kOutPad : 128, rows_h<128>(NL, l) * 128, false);
+            if (!ok) break;
+            if (!last) {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    float v[32];
+                    umma::tmem_ld32(tmem + tlane + 32u * h, v);
+                    uint32_t m = 0;
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) {
+                        const bool on = v[i] > 0.0f;
+                        v[i] = on ? v[i] : 0.0f;
+                        m |= (on ? 1u : 0u) << i;
+                    }
+                    mask[l][h] = m;
+                    store_row32<false>(sa, t, 32 * h, v);
+                    store_T32<128>(a.hT[l + 1] + (size_t)tile * (2 * 128 * 128), t, 32 * h, v);
+                }
+            } else {
+                float v[16];
+                umma::tmem_ld16(tmem + tlane + 128u, v);
+                const float lum = 0.299f * v[0] + 0.587f * v[1] + 0.114f * v[2];
+                const float den = lum * lum + 0.01f;
+                float gr[32];
+#pragma unroll
+                for (int k = 0; k < 32; ++k) gr[k] = 0.0f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float diff = v[k] - tgt[k];
+                    lsum += diff * diff / den;
+                    gr[k] = 2.0f * diff / den;
+                }
+                store_row32<true>(sa, t, 0, gr);    // K = 16: the backward reads the first two chunks
+                store_T<16>(a.zT[NL - 1] + (size_t)tile * (2 * 16 * 128), t, gr);
+            }
+            umma::fence_before_sync();
+            umma::fence_smem_to_async();
+            __syncthreads();
+        }
+        // backward: dH_{l-1} = dZ_l * W_l, masked by the ReLU of layer l-1
+        for (int l = NL - 1; l >= 1 && ok; --l) {
+            run_layer(0u, l == NL - 1 ? kOutPad : 128, 128, 128 * 128, true);
+            if (!ok) break;
+#pragma unroll
+            for (int h = 0; h < 4; ++h) {
+                float v[32];
+                umma::tmem_ld32(tmem + tlane + 32u * h, v);
+                const uint32_t m = mask[l - 1][h];
+#pragma unroll
+                for (int i = 0; i < 32; ++i) v[i] = ((m >> i) & 1u) ? v[i] : 0.0f;
+                if (l > 1) store_row32<true>(sa, t, 32 * h, v);
+                store_T32<128>(a.zT[l - 1] + (size_t)tile * (2 * 128 * 128), t, 32 * h, v);
+            }
+            umma::fence_before_sync();
+            umma::fence_smem_to_async();
+            __syncthreads();
+        }
+    }
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xFFFFFFFFu, lsum, o);
+    if ((t & 31) == 0) atomicAdd(a.loss, lsum);
+    if (!ok && warp == 0) {   // after a timeout: pending copies and issued MMAs finish first
+        if (umma::elect_one()) {
+            for (int b = 0; b < 2; ++b)
+                if (wpend[b]) umma::mbar_wait(&mb_w[b], wph[b], kSpinLimit);
+            umma::mma_commit(&mb_drain);
+            umma::mbar_wait(&mb_drain, 0, kSpinLimit);
+        }
+        __syncwarp();
+    }
+    if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, 256);
+}
+
 // ------------------------------------------------------------------ weight gradients
 // dW_l[out][in] = sum_s dZ_l[s][out] * H_l[s][in].  A = dZ^T (out rows padded
 // to 128 with zeros), B = H^T (in rows), K = samples.  One CTA reduces
 // `tiles_per_cta` sample tiles of one layer into TMEM, then adds its partial
 // sums to the FP32 gradient with atomics.
 constexpr int kWgSmemA = 0;                          // 2 stages x 2 regions x 16 KB
-constexpr int kWgSmemB = 65536;                      // 2 stages x 2 x 96 x 128
-constexpr int kWgSmem = kWgSmemB + 2 * 2 * 96 * 128; // 114688
+constexpr int kWgSmemB = 65536;                      // 2 stages x 2 x FH x 128 (FH <= max(96, HID))
+template <int HID> constexpr int kWgStageB = 2 * (HID > 96 ? HID : 96) * 128;
+template <int HID> constexpr int kWgSmemH = kWgSmemB + 2 * kWgStageB<HID>;
+constexpr int kWgSmem = kWgSmemH<64>;                // 114688
 
 struct WgradArgs {
     const uint8_t* zT[kMaxLayers];
@@ -988,7 +1386,7 @@ struct WgradArgs {
     uint32_t tiles_per_cta;
 };
 
-template <int NL>
+template <int NL, int HID>
 __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -996,7 +1394,7 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     __shared__ uint32_t tslot;
     const int t = threadIdx.x, warp = t >> 5;
     const int l = blockIdx.y;
-    const int FZ = kZTFeat<NL>(l), FH = kHTFeat<NL>(l);
+    const int FZ = l == NL - 1 ? 16 : HID, FH = l == 0 ? 96 : HID;
     const uint32_t t0 = blockIdx.x * a.tiles_per_cta;
     if (t0 >= a.ntiles || a.state[S_NAVAIL] < a.min_n || a.state[S_NAVAIL] == 0) return;
     const uint32_t t1 = min(a.ntiles, t0 + a.tiles_per_cta);
@@ -1017,7 +1415,7 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     auto load = [&](uint32_t tile, int stage) {
         ld_pending[stage] = true;
         uint8_t* sA = smem + kWgSmemA + stage * 32768;
-        uint8_t* sB = smem + kWgSmemB + stage * (2 * 96 * 128);
+        uint8_t* sB = smem + kWgSmemB + stage * kWgStageB<HID>;
         const uint8_t* gz = a.zT[l] + (size_t)tile * 2 * zbytes;
         const uint8_t* gh = a.hT[l] + (size_t)tile * hbytes;
         umma::mbar_expect_tx(&mb_ld[stage], 2 * zbytes + hbytes);
@@ -1039,7 +1437,7 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
             ld_pending[stage] = false;
             umma::fence_after_sync();
             const uint8_t* sA = smem + kWgSmemA + stage * 32768;
-            const uint8_t* sB = smem + kWgSmemB + stage * (2 * 96 * 128);
+            const uint8_t* sB = smem + kWgSmemB + stage * kWgStageB<HID>;
             for (int s = 0; s < 8; ++s) {
                 const int reg = s >> 2, kk = s & 3;
                 const uint64_t ad = umma::sdesc_sw128(umma::smem_u32(sA + reg * 16384 + kk * 32));
@@ -1070,7 +1468,7 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
             float v[32];
             umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
             if (row < FZ) {
-                float* g = a.grad + kPOff<NL>(l) + row * kCols<NL>(l) + c0;
+                float* g = a.grad + poff_h<HID>(NL, l) + row * cols_h<HID>(l) + c0;
 #pragma unroll
                 for (int i = 0; i < 32; ++i) atomicAdd(&g[i], v[i]);
             }
@@ -1101,21 +1499,21 @@ struct AdamArgs {
     int live0;                     // live input columns of layer 0 (the rest stay zero)
 };
 
-template <int NL>
+template <int NL, int HID>
 __device__ __forceinline__ void layer_of(int i, int& l, int& r, int& c) {
     l = 0;
-    while (i >= kPOff<NL>(l + 1)) ++l;
-    const int j = i - kPOff<NL>(l);
-    r = j / kCols<NL>(l);
-    c = j % kCols<NL>(l);
+    while (i >= poff_h<HID>(NL, l + 1)) ++l;
+    const int j = i - poff_h<HID>(NL, l);
+    r = j / cols_h<HID>(l);
+    c = j % cols_h<HID>(l);
 }
 
-template <int NL>
+template <int NL, int HID>
 __global__ void k_adam(AdamArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= kParams<NL>) return;
+    if (i >= params_h<HID>(NL)) return;
     int l, r, c;
-    layer_of<NL>(i, l, r, c);
+    layer_of<NL, HID>(i, l, r, c);
     // Padded entries (output rows 3..15, input columns past the encoding of layer 0) stay zero.
     const bool live = !(l == NL - 1 && r >= 3) && !(l == 0 && c >= a.live0);
     float w = a.w[i];
@@ -1139,15 +1537,16 @@ __global__ void k_adam(AdamArgs a) {
     const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
     const float ew = ema_debias > 0.0f ? e / ema_debias : w;
     // forward / inference images: row r, K index c
-    const int rows = kRows<NL>(l);
-    const uint32_t off = (uint32_t)kFOff<NL>(l) + (uint32_t)(c >> 6) * rows * 128 + umma::sw128_offset(r, (c & 63) >> 3) +
-                         2 * (c & 7);
+    const int rows = rows_h<HID>(NL, l);
+    const uint32_t off = (uint32_t)foff_h<HID>(NL, l) + (uint32_t)(c >> 6) * rows * 128 +
+                         umma::sw128_offset(r, (c & 63) >> 3) + 2 * (c & 7);
     *reinterpret_cast<__half*>(a.fwd + off) = __float2half_rn(w);
     *reinterpret_cast<__half*>(a.inf + off) = __float2half_rn(ew);
     *reinterpret_cast<__nv_bfloat16*>(a.inf_bf + off) = __float2bfloat16_rn(ew);
     if (l >= 1) {
         // backward image: W^T, row = c (input unit), K index = r (output unit)
-        const uint32_t boff = (uint32_t)kBOff<NL>(l) + umma::sw128_offset(c, r >> 3) + 2 * (r & 7);
+        const uint32_t boff = (uint32_t)boff_h<HID>(NL, l) + (uint32_t)(r >> 6) * (HID * 128) +
+                              umma::sw128_offset(c, (r & 63) >> 3) + 2 * (r & 7);
         *reinterpret_cast<__nv_bfloat16*>(a.bwd + boff) = __float2bfloat16_rn(w);
     }
 }
@@ -1163,16 +1562,17 @@ struct HashGradArgs {
     const uint32_t* state;
     uint32_t min_n, batch;
     Bounds bounds;
-    const uint8_t* zT0;          // dZ_0 tiles
-    const float* w0;             // FP32 master weights of layer 0, [64][96]
+    const uint8_t* zT0;          // dZ_0 tiles (hid features)
+    const float* w0;             // FP32 master weights of layer 0, [hid][96]
     float2* grad;                // table gradient [level][T]
     HashGrid hg;
+    int hid;                     // hidden width: 64 or 128
 };
 
 __global__ void __launch_bounds__(128) k_hash_grad(HashGradArgs a) {
-    __shared__ float sw[64][2 * kHashMaxLevels];
+    __shared__ float sw[128][2 * kHashMaxLevels];
     const int L2 = 2 * a.hg.levels;
-    for (int i = threadIdx.x; i < 64 * 2 * kHashMaxLevels; i += blockDim.x) {
+    for (int i = threadIdx.x; i < a.hid * 2 * kHashMaxLevels; i += blockDim.x) {
         const int o = i / (2 * kHashMaxLevels), j = i % (2 * kHashMaxLevels);
         sw[o][j] = j < L2 ? __half2float(__float2half_rn(a.w0[o * 96 + j])) : 0.0f;
     }
@@ -1185,12 +1585,12 @@ __global__ void __launch_bounds__(128) k_hash_grad(HashGradArgs a) {
     const uint32_t idx = pcg_next(st) % n_avail;
     const TfgDatosMLP d = a.buf[idx];
     const uint32_t tile = s / kTile, t = s % kTile;
-    const uint8_t* region = a.zT0 + (size_t)tile * (2 * 64 * 128) + (t >> 6) * (64 * 128);
+    const uint8_t* region = a.zT0 + (size_t)tile * (2 * a.hid * 128) + (t >> 6) * (a.hid * 128);
     const uint32_t c = (t & 63u) >> 3, e = t & 7u;
     float dx[2 * kHashMaxLevels];
 #pragma unroll
     for (int j = 0; j < 2 * kHashMaxLevels; ++j) dx[j] = 0.0f;
-    for (int o = 0; o < 64; ++o) {
+    for (int o = 0; o < a.hid; ++o) {
         const float dz = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(region + umma::sw128_offset(o, c) + 2 * e));
         if (dz == 0.0f) continue;
 #pragma unroll
@@ -1299,6 +1699,7 @@ struct ColorMlp {
     float* w = nullptr; float* m = nullptr; float* v = nullptr; float* ema = nullptr; float* grad = nullptr;
     uint8_t* fwd = nullptr; uint8_t* bwd = nullptr; uint8_t* inf = nullptr;
     int nl = 6;                  // layers (hidden layers + 1)
+    int hid = 64;                // hidden width (64, or 128 for 3 or 5 hidden layers)
     uint8_t* hT[mlp::kMaxLayers] = {nullptr};
     uint8_t* zT[mlp::kMaxLayers] = {nullptr};
     float* loss = nullptr;
@@ -1364,6 +1765,19 @@ int with_model(const ColorMlp* n, F&& f) {
     });
 }
 
+// Calls f(integral_constant<int, NL>, integral_constant<int, HID>) for the
+// model's layer count and width (width 128 only with 3 or 5 hidden layers).
+template <typename F>
+int with_width(const ColorMlp* n, F&& f) {
+    return with_layers(n->nl, [&](auto c) {
+        constexpr int NL = decltype(c)::value;
+        if constexpr (NL == 4 || NL == 6) {
+            if (n->hid == 128) return f(c, std::integral_constant<int, 128>{});
+        }
+        return f(c, std::integral_constant<int, 64>{});
+    });
+}
+
 uint64_t splitmix(uint64_t& s) {
     uint64_t z = (s += 0x9E3779B97F4A7C15ull);
     z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
@@ -1381,9 +1795,9 @@ int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
     a.min_n = min_n;
     a.update = update ? 1 : 0;
     a.live0 = n->hlevels ? mlp::kHashLive : mlp::kFreqLive;
-    with_layers(n->nl, [&](auto c) {
-        constexpr int NL = decltype(c)::value;
-        mlp::k_adam<NL><<<(mlp::kParams<NL> + 255) / 256, 256, 0, s>>>(a);
+    with_width(n, [&](auto c, auto w) {
+        constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
+        mlp::k_adam<NL, HID><<<(mlp::params_h<HID>(NL) + 255) / 256, 256, 0, s>>>(a);
         return 0;
     });
     cudaError_t e = cudaGetLastError();
@@ -1410,7 +1824,7 @@ int ensure_acts(ColorMlp* n, uint32_t tiles) {
         n->hT[l] = n->zT[l] = nullptr;
     }
     for (int l = 0; l < n->nl; ++l) {
-        const int fh = l == 0 ? 96 : 64, fz = l == n->nl - 1 ? 16 : 64;   // kHTFeat / kZTFeat
+        const int fh = l == 0 ? 96 : n->hid, fz = l == n->nl - 1 ? 16 : n->hid;   // features of the tiles
         cudaError_t e = cudaMalloc((void**)&n->hT[l], (size_t)tiles * 2 * fh * 128);
         if (e == cudaSuccess) e = cudaMalloc((void**)&n->zT[l], (size_t)tiles * 2 * fz * 128);
         if (e != cudaSuccess) { n->act_tiles = 0; return cuda_fail(e, "mlp activations"); }
@@ -1453,10 +1867,10 @@ int enqueue_wgrad(ColorMlp* n, uint32_t tiles_per_cta, uint32_t min_n, cudaStrea
     wa.grad = n->grad; wa.state = n->dstate; wa.min_n = min_n;
     wa.ntiles = tiles;
     wa.tiles_per_cta = std::max<uint32_t>(1u, tiles_per_cta);
-    with_layers(n->nl, [&](auto c) {
-        constexpr int NL = decltype(c)::value;
-        mlp::k_wgrad<NL><<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, NL), 128, mlp::kWgSmem + 1024, s>>>(
-            wa);
+    with_width(n, [&](auto c, auto w) {
+        constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
+        mlp::k_wgrad<NL, HID><<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, NL), 128,
+                                mlp::kWgSmemH<HID> + 1024, s>>>(wa);
         return 0;
     });
     cudaError_t e = cudaGetLastError();
@@ -1475,9 +1889,11 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
     ta.hg = hash_view(n, true);
     for (int l = 0; l < mlp::kMaxLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
-    with_layers(n->nl, [&](auto c) {
-        constexpr int NL = decltype(c)::value;
-        mlp::k_train<NL><<<std::min<uint32_t>(tiles, (uint32_t)n->sms), 128, mlp::kTrainSmem + 1024, s>>>(ta);
+    with_width(n, [&](auto c, auto w) {
+        constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
+        const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)n->sms);
+        if constexpr (HID == 128) mlp::k_train128<NL><<<grid, 128, mlp::kT128Smem + 1024, s>>>(ta);
+        else mlp::k_train<NL><<<grid, 128, mlp::kTrainSmem + 1024, s>>>(ta);
         return 0;
     });
     e = cudaGetLastError();
@@ -1487,6 +1903,7 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
         mlp::HashGradArgs ha;
         ha.buf = buf; ha.state = n->dstate; ha.min_n = min_n; ha.batch = n->batch; ha.bounds = n->bounds;
         ha.zT0 = n->zT[0]; ha.w0 = n->w; ha.grad = reinterpret_cast<float2*>(n->hgrad); ha.hg = hash_view(n, true);
+        ha.hid = n->hid;
         mlp::k_hash_grad<<<tiles, mlp::kTile, 0, s>>>(ha);
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "mlp step: table gradient");
@@ -1514,6 +1931,31 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
     if (n->prec == mlp::kPrecF8 && !n->f8_calibrated)
         return fail(TFG_E_INVALID, "mlp inference: FP8 needs tfgMlpCalibrate first");
     const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
+    if (n->hid == 128) {
+        if (n->prec == mlp::kPrecF8) return fail(TFG_E_UNSUPPORTED, "mlp inference: FP8 is built for width 64");
+        uint32_t cap = (uint32_t)n->sms;
+        if (n->tune.infer_ctas > 0) cap = std::min<uint32_t>(cap, (uint32_t)n->tune.infer_ctas);
+        const uint32_t grid128 =
+            std::max<uint32_t>(1u, std::min<uint32_t>((tiles + mlp::kSlots128 - 1) / mlp::kSlots128, cap));
+        const uint8_t* wimg = n->prec == mlp::kPrecBF16 ? n->inf_bf : n->inf;
+        with_model(n, [&](auto c, auto h) {
+            constexpr int NL = decltype(c)::value;
+            constexpr bool HASH = decltype(h)::value;
+            if constexpr (NL == 4 || NL == 6) {
+                const size_t sm = mlp::kInfer128Smem + 1024;
+                if (n->prec == mlp::kPrecF16)
+                    mlp::k_infer128<mlp::kPrecF16, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
+                else
+                    mlp::k_infer128<mlp::kPrecBF16, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
+            }
+            return 0;
+        });
+        cudaError_t e1 = cudaGetLastError();
+        if (e1 != cudaSuccess) return cuda_fail(e1, "mlp inference");
+        return ok();
+    }
     const uint32_t grid = infer_grid(n, tiles);
     const size_t smem = mlp::kInferSmem + 1024;
     cudaError_t e = cudaSuccess;
@@ -1548,6 +1990,7 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
 // Per-layer input amax over `count` samples through the FP16 path (every
 // tile), turned into the FP8 input scales.
 int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStream_t s) {
+    if (n->hid == 128) return fail(TFG_E_UNSUPPORTED, "tfgMlpCalibrate: FP8 is built for width 64");
     if (count == 0) return fail(TFG_E_INVALID, "tfgMlpCalibrate: no samples");
     if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
         return fail(TFG_E_INVALID, "tfgMlpCalibrate: input buffer must be 16-byte aligned");
@@ -1600,7 +2043,7 @@ int autotune_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, TfgColor* 
     repeats = repeats > 0 ? std::min(repeats, 1000) : 5;
     const uint32_t tiles = n->batch / mlp::kTile;
     if (int rc = ensure_acts(n, tiles)) return rc;
-    const size_t gbytes = (size_t)mlp::params_of(n->nl) * sizeof(float);
+    const size_t gbytes = (size_t)mlp::params_rt(n->nl, n->hid) * sizeof(float);
     const size_t fbytes = mlp::kF8Words * sizeof(float), sbytes = mlp::S_WORDS * sizeof(uint32_t);
     uint8_t* saved = nullptr;
     cudaError_t e = cudaMalloc((void**)&saved, gbytes + fbytes + sbytes);
@@ -1695,7 +2138,16 @@ void set_kernel_attrs() {
     cudaFuncSetAttribute(M::k_infer<M::kPrecBF16, false, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
     cudaFuncSetAttribute(M::k_infer<M::kPrecF8, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
     cudaFuncSetAttribute(M::k_train<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kTrainSmem + 1024);
-    cudaFuncSetAttribute(M::k_wgrad<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
+    cudaFuncSetAttribute(M::k_wgrad<NL, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
+    if constexpr (NL == 4 || NL == 6) {
+        const int i128 = M::kInfer128Smem + 1024;
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF16, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecBF16, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF16, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecBF16, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_train128<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kT128Smem + 1024);
+        cudaFuncSetAttribute(M::k_wgrad<NL, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmemH<128> + 1024);
+    }
 }
 }  // namespace
 
@@ -1756,12 +2208,15 @@ int create_tables(ColorMlp* n, const TfgHashGridConfig& c, uint64_t seed) {
     return ok();
 }
 
-int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
+int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers, int32_t width,
                  const TfgHashGridConfig* hc, TfgColorMLP** out) {
     if (!out) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: out is null");
     *out = nullptr;
     if (hidden_layers != 3 && hidden_layers != 5 && hidden_layers != 7)
         return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: hidden_layers must be 3, 5 or 7");
+    if (width != 64 && width != 128) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: width must be 64 or 128");
+    if (width == 128 && hidden_layers == 7)
+        return tfg::fail(TFG_E_UNSUPPORTED, "tfgMlpCreate: width 128 is built for 3 or 5 hidden layers");
     const int nl = hidden_layers + 1;
     if (n_in != 15 || n_out != 3) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: the cache takes 15 inputs and 3 outputs");
     if (batch == 0 || batch % M::kTile != 0 || batch > (1u << 24))
@@ -1774,10 +2229,12 @@ int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, i
     n->dev = dev;
     n->batch = batch;
     n->nl = nl;
+    n->hid = width;
     cudaDeviceGetAttribute(&n->sms, cudaDevAttrMultiProcessorCount, dev);
-    const int nparams = M::params_of(nl);
+    const int nparams = M::params_rt(nl, width);
     const size_t pb = nparams * sizeof(float);
-    const size_t fwd_bytes = M::fwd_bytes_of(nl), bwd_bytes = M::bwd_bytes_of(nl), f8_bytes = M::f8_bytes_of(nl);
+    const size_t fwd_bytes = M::fwd_bytes_rt(nl, width), bwd_bytes = M::bwd_bytes_rt(nl, width),
+                 f8_bytes = M::f8_bytes_of(nl);
     e = cudaMalloc((void**)&n->w, pb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->m, pb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->v, pb);
@@ -1807,13 +2264,13 @@ int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, i
     std::vector<float> h(nparams, 0.0f);
     uint64_t st = seed ? seed : 0x5EEDull;
     for (int l = 0; l < nl; ++l) {
-        const int fan_in = l == 0 ? live0 : 64, fan_out = l == nl - 1 ? 3 : 64;
+        const int fan_in = l == 0 ? live0 : width, fan_out = l == nl - 1 ? 3 : width;
         const float sc = std::sqrt(6.0f / (float)(fan_in + fan_out));
-        for (int r = 0; r < M::rows_of(nl, l); ++r)
-            for (int c = 0; c < M::cols_of(l); ++c) {
+        for (int r = 0; r < M::rows_rt(nl, l, width); ++r)
+            for (int c = 0; c < M::cols_rt(l, width); ++c) {
                 const bool live = !(l == nl - 1 && r >= 3) && !(l == 0 && c >= live0);
                 const double u = (double)(tfg::splitmix(st) >> 11) * (1.0 / 9007199254740992.0);
-                h[M::poff_of(nl, l) + r * M::cols_of(l) + c] = live ? (float)((2.0 * u - 1.0) * sc) : 0.0f;
+                h[M::poff_rt(nl, l, width) + r * M::cols_rt(l, width) + c] = live ? (float)((2.0 * u - 1.0) * sc) : 0.0f;
             }
     }
     // The weight average starts at zero and is debiased by 1 - decay^t for
@@ -1843,13 +2300,18 @@ int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, i
 
 extern "C" int tfgMlpCreateEx(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
                               TfgColorMLP** out) {
-    return tfg::create_model(n_in, n_out, batch, seed, hidden_layers, nullptr, out);
+    return tfg::create_model(n_in, n_out, batch, seed, hidden_layers, 64, nullptr, out);
 }
 
 extern "C" int tfgMlpCreateHashGrid(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed,
                                     int32_t hidden_layers, const TfgHashGridConfig* config, TfgColorMLP** out) {
     if (!config) return tfg::fail(TFG_E_INVALID, "tfgMlpCreateHashGrid: config is null");
-    return tfg::create_model(n_in, n_out, batch, seed, hidden_layers, config, out);
+    return tfg::create_model(n_in, n_out, batch, seed, hidden_layers, 64, config, out);
+}
+
+extern "C" int tfgMlpCreateWide(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
+                                int32_t width, const TfgHashGridConfig* config, TfgColorMLP** out) {
+    return tfg::create_model(n_in, n_out, batch, seed, hidden_layers, width, config, out);
 }
 
 extern "C" int64_t tfgMlpHashParamCount(const TfgColorMLP* h) {
@@ -1875,7 +2337,7 @@ extern "C" int tfgMlpSetHashParams(TfgColorMLP* h, const float* host, int64_t co
     cudaError_t e = cudaMemcpy(n->hw, host, n->hcount * sizeof(float), cudaMemcpyHostToDevice);
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetHashParams");
     // restart the optimiser of the whole model (tfgMlpSetParams clears the tables' state too)
-    std::vector<float> w((size_t)M::params_of(n->nl));
+    std::vector<float> w((size_t)M::params_rt(n->nl, n->hid));
     e = cudaMemcpy(w.data(), n->w, w.size() * sizeof(float), cudaMemcpyDeviceToHost);
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetHashParams");
     return tfgMlpSetParams(h, w.data(), (uint32_t)w.size());
@@ -1922,6 +2384,8 @@ extern "C" int tfgMlpSetPrecision(TfgColorMLP* h, int32_t precision) {
     if (!n) return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: null model");
     if (precision != TFG_MLP_FP16 && precision != TFG_MLP_BF16 && precision != TFG_MLP_FP8)
         return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: unknown precision");
+    if (precision == TFG_MLP_FP8 && n->hid == 128)
+        return tfg::fail(TFG_E_UNSUPPORTED, "tfgMlpSetPrecision: FP8 is built for width 64");
     n->prec = precision;
     return tfg::ok();
 }
@@ -1989,7 +2453,7 @@ extern "C" int tfgMlpTrainStep(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32
 
 extern "C" int tfgMlpGetParams(TfgColorMLP* h, int which, float* host, uint32_t count) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
-    if (!n || !host || count != (uint32_t)M::params_of(n->nl))
+    if (!n || !host || count != (uint32_t)M::params_rt(n->nl, n->hid))
         return tfg::fail(TFG_E_INVALID, "tfgMlpGetParams: bad argument");
     const float* src = which == 0 ? n->w : which == 1 ? n->ema : which == 2 ? n->m : which == 3 ? n->v : nullptr;
     if (!src) return tfg::fail(TFG_E_INVALID, "tfgMlpGetParams: unknown array");
@@ -2000,7 +2464,7 @@ extern "C" int tfgMlpGetParams(TfgColorMLP* h, int which, float* host, uint32_t 
 
 extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
-    if (!n || !host || count != (uint32_t)M::params_of(n->nl))
+    if (!n || !host || count != (uint32_t)M::params_rt(n->nl, n->hid))
         return tfg::fail(TFG_E_INVALID, "tfgMlpSetParams: bad argument");
     const size_t pb = count * sizeof(float);
     cudaError_t e = cudaMemcpy(n->w, host, pb, cudaMemcpyHostToDevice);
@@ -2033,7 +2497,7 @@ extern "C" int tfgMlpComputeGradientEx(TfgColorMLP* h, const TfgDatosMLP* buffer
                                        float* host_grad, uint32_t count, float* host_table_grad, int64_t table_count,
                                        float* loss_out) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
-    if (!n || !buffer || !host_grad || count != (uint32_t)M::params_of(n->nl) || n_available == 0)
+    if (!n || !buffer || !host_grad || count != (uint32_t)M::params_rt(n->nl, n->hid) || n_available == 0)
         return tfg::fail(TFG_E_INVALID, "tfgMlpComputeGradient: bad argument");
     if (host_table_grad && table_count != (int64_t)n->hcount)
         return tfg::fail(TFG_E_INVALID, "tfgMlpComputeGradientEx: table_count differs from tfgMlpHashParamCount");
@@ -2072,7 +2536,7 @@ extern "C" int tfgMlpComputeGradientEx(TfgColorMLP* h, const TfgDatosMLP* buffer
 
 extern "C" int32_t tfgMlpParamCount(const TfgColorMLP* h) {
     const ColorMlp* n = reinterpret_cast<const ColorMlp*>(h);
-    return n ? M::params_of(n->nl) : 0;
+    return n ? M::params_rt(n->nl, n->hid) : 0;
 }
 
 // ------------------------------------------------------------------ checkpoints
@@ -2089,7 +2553,7 @@ constexpr char kCkptMagic[8] = {'T', 'F', 'G', 'N', 'R', 'C', '0', '1'};
 extern "C" int tfgMlpSave(TfgColorMLP* h, const char* path) {
     ColorMlp* n = reinterpret_cast<ColorMlp*>(h);
     if (!n || !path) return tfg::fail(TFG_E_INVALID, "tfgMlpSave: null argument");
-    const uint32_t np = (uint32_t)M::params_of(n->nl);
+    const uint32_t np = (uint32_t)M::params_rt(n->nl, n->hid);
     std::vector<float> arrays[4];
     uint32_t st[M::S_WORDS];
     const float* src[4] = {n->w, n->ema, n->m, n->v};
@@ -2147,7 +2611,7 @@ extern "C" int tfgMlpLoad(TfgColorMLP* h, const char* path) {
         std::fclose(f);
         return tfg::fail(TFG_E_INVALID, std::string("tfgMlpLoad: not a cache checkpoint: ") + path);
     }
-    if (hidden != n->nl - 1 || np != (uint32_t)M::params_of(n->nl)) {
+    if (hidden != n->nl - 1 || np != (uint32_t)M::params_rt(n->nl, n->hid)) {
         std::fclose(f);
         return tfg::fail(TFG_E_INVALID, "tfgMlpLoad: the checkpoint's network depth differs from this model's");
     }

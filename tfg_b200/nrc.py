@@ -11,13 +11,13 @@ from . import _lib
 from .structs import (BOUNDS, DATOS_MLP, REGISTRO, CHashGridConfig, CMlpTuning, CNrcBuffers, CNrcFrameConfig,
                       CNrcSceneFrame)
 
-def layer_shapes(hidden_layers: int = 5) -> list[tuple[int, int]]:
+def layer_shapes(hidden_layers: int = 5, width: int = 64) -> list[tuple[int, int]]:
     """Padded [out][in] shapes of the weight matrices, in parameter order."""
-    return [(64, 96)] + [(64, 64)] * (hidden_layers - 1) + [(16, 64)]
+    return [(width, 96)] + [(width, width)] * (hidden_layers - 1) + [(16, width)]
 
 
-def param_count(hidden_layers: int = 5) -> int:
-    return sum(r * c for r, c in layer_shapes(hidden_layers))
+def param_count(hidden_layers: int = 5, width: int = 64) -> int:
+    return sum(r * c for r, c in layer_shapes(hidden_layers, width))
 
 
 # the default network: 5 hidden layers of 64
@@ -42,11 +42,16 @@ def _stream(stream=None) -> int:
 
 
 def split_layers(flat: np.ndarray) -> list[np.ndarray]:
-    """Weight matrices of a flat parameter array (its length gives the depth)."""
-    hidden = (len(flat) - 6144 - 1024) // 4096 + 1
-    assert param_count(hidden) == len(flat), "not a parameter array of this network"
+    """Weight matrices of a flat parameter array (its length gives the depth
+    and the width)."""
+    for width in (64, 128):
+        hidden = (len(flat) - 112 * width) // (width * width) + 1
+        if hidden >= 1 and param_count(hidden, width) == len(flat):
+            break
+    else:
+        raise AssertionError("not a parameter array of this network")
     out, o = [], 0
-    for r, c in layer_shapes(hidden):
+    for r, c in layer_shapes(hidden, width):
         out.append(flat[o:o + r * c].reshape(r, c))
         o += r * c
     return out
@@ -60,10 +65,11 @@ class ColorMLP:
     hashgrid_reference())."""
 
     def __init__(self, n_in: int = 15, n_out: int = 3, batch: int = 16384, seed: int = 1337, hidden_layers: int = 5,
-                 encoding: str = FREQUENCY, hashgrid: dict | None = None):
+                 encoding: str = FREQUENCY, hashgrid: dict | None = None, width: int = 64):
         self.batch = batch
         self.hidden_layers = hidden_layers
         self.encoding = encoding
+        self.width = width
         h = ctypes.c_void_p()
         if encoding == HASHGRID:
             cfg = {**hashgrid_reference(), **(hashgrid or {})}
@@ -71,10 +77,11 @@ class ColorMLP:
             c.n_levels, c.log2_hashmap_size = cfg["n_levels"], cfg["log2_hashmap_size"]
             c.base_resolution, c.per_level_scale = cfg["base_resolution"], cfg["per_level_scale"]
             self.hashgrid = cfg
-            _lib.call("tfgMlpCreateHashGrid", n_in, n_out, batch, seed, hidden_layers, ctypes.byref(c), ctypes.byref(h))
+            _lib.call("tfgMlpCreateWide", n_in, n_out, batch, seed, hidden_layers, width, ctypes.byref(c),
+                      ctypes.byref(h))
         elif encoding == FREQUENCY:
             self.hashgrid = None
-            _lib.call("tfgMlpCreateEx", n_in, n_out, batch, seed, hidden_layers, ctypes.byref(h))
+            _lib.call("tfgMlpCreateWide", n_in, n_out, batch, seed, hidden_layers, width, None, ctypes.byref(h))
         else:
             raise ValueError(f"unknown encoding {encoding!r}")
         self.h = h
