@@ -350,6 +350,7 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
     encoding = {"frequency_12_bands": depth[5],
                 "hashgrid_reference": {**variant(encoding=HASHGRID), "config": hashgrid_reference(),
                                        "one_blob_bins": 4}}
+    width = {"5x64": depth[5], "5x128": variant(width=128), "3x128": variant(hidden_layers=3, width=128)}
     return {
         "frames": 48 + frames, "warmup_frames": 48, "camera": "orbit 1 deg/frame", "train_samples_per_frame": 4 * 16384,
         "ms_per_frame_nrc": round(t_nrc, 3), "ms_per_pass_plain_1spp": round(t_pt, 3),
@@ -362,6 +363,7 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
         "precision_sweep": sweep,
         "depth_sweep": {f"{k}x64": v for k, v in sorted(depth.items())},
         "encoding_sweep": encoding,
+        "width_sweep": width,
     }
 
 
