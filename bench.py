@@ -617,9 +617,10 @@ def measure_peaks():
     print(json.dumps(out))
 
 
-def profile_mlp():
+def profile_mlp(width: int = 64):
     """Cache inference over 2,073,600 queries (232 MB of DatosMLP, more than
-    L2) and one 16384-sample train step, untimed; used for ncu captures."""
+    L2) and one 16384-sample train step of a network of 5 hidden layers of
+    `width` units, untimed; used for ncu captures."""
     import numpy as np
     import torch
 
@@ -636,7 +637,7 @@ def profile_mlp():
         d["difuso"][k] = rng.uniform(0, 1, n)
         d["color"][k] = rng.uniform(0, 2, n)
     dd = torch.from_numpy(d.view(np.uint8).copy()).cuda()
-    m = ColorMLP(batch=16384, seed=1)
+    m = ColorMLP(batch=16384, seed=1, width=width)
     m.set_bounds((-6, -6, -6), (6, 6, 6))
     out = torch.zeros(n * 3, device="cuda")
     m.inference(dd, out, n)
@@ -689,6 +690,7 @@ def main():
                     help="measure L2 copy bandwidth and FP16 / BF16 / FP8 GEMM peaks, print them and exit")
     ap.add_argument("--profile-mlp", action="store_true",
                     help="run cache inference on 1920x1080 queries and one train step, then exit (case for ncu)")
+    ap.add_argument("--mlp-width", type=int, default=64, help="with --profile-mlp: 64 or 128 units per hidden layer")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
@@ -697,7 +699,7 @@ def main():
         profile_pass(args.wavefront_samples, args.tuning)
         return
     if args.profile_mlp:
-        profile_mlp()
+        profile_mlp(args.mlp_width)
         return
     if args.measure_peaks:
         measure_peaks()
