@@ -70,6 +70,14 @@ class Clocks:
                                          stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
         except FileNotFoundError:
             self.proc = None
+        # Start timing only once the sampler has written its first sample:
+        # its start-up (driver initialisation) then falls outside the timed
+        # region, and the region is sampled from its first 200 ms on.
+        t_end = time.perf_counter() + 10.0
+        while self.proc is not None and self.proc.poll() is None and time.perf_counter() < t_end:
+            if os.path.getsize(self.path) > 0:
+                break
+            time.sleep(0.02)
         return self
 
     def __exit__(self, *exc):
@@ -647,6 +655,37 @@ def profile_mlp(width: int = 64):
     print("profile mlp done")
 
 
+def profile_frame(encoding: str = "frequency", width: int = 64, frames: int = 6):
+    """`frames` cache frames of the 1920x1080 benchmark scene (the first
+    four as warm-up frames, 4 x 16384 training samples each, launched
+    eagerly) and then one more inference over the last frame's 2,073,600
+    queries, untimed; used for ncu launch lists and captures.  Every frame
+    launches `k_infer` twice (the frame's queries and the tail queries), so
+    the last inference is launch 2 * frames of that kernel."""
+    import torch
+
+    from tfg_b200 import pathtracer as pt
+    from tfg_b200 import scenes
+    from tfg_b200.nrc import HASHGRID, ColorMLP, NrcRenderer
+    scene = scenes.spheres_terrain(W_PX, H_PX)
+    ds = pt.DeviceScene(scene, "cuda")
+    params = pt.RenderParams(max_depth=DEPTH, rr_min_depth=RR, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT)
+    kw = {"encoding": HASHGRID} if encoding == "hashgrid" else {}
+    m = ColorMLP(batch=16384, seed=2024, width=width, **kw)
+    m.set_bounds(*scene.bounds)
+    r = NrcRenderer(ds, m, params, train_steps=4, use_graph=False)
+    for f in range(frames):
+        r.frame(f, warmup=f < 4, accumulate=False)
+    n = W_PX * H_PX
+    out = torch.zeros(n * 3, dtype=torch.float32, device="cuda")
+    with torch.cuda.stream(r.stream):
+        m.inference(r.infer, out, n, stream=r.stream)
+    r.stream.synchronize()
+    m.close()
+    ds.close()
+    print("profile frame done")
+
+
 def profile_pass(samples: int = 1, tuning: str | None = None):
     """One pass of `samples` spp (8 bounces) of the benchmark frame in one
     wavefront of samples x W x H paths: ~0.3 GB of scene data (more than L2)
@@ -690,13 +729,21 @@ def main():
                     help="measure L2 copy bandwidth and FP16 / BF16 / FP8 GEMM peaks, print them and exit")
     ap.add_argument("--profile-mlp", action="store_true",
                     help="run cache inference on 1920x1080 queries and one train step, then exit (case for ncu)")
-    ap.add_argument("--mlp-width", type=int, default=64, help="with --profile-mlp: 64 or 128 units per hidden layer")
+    ap.add_argument("--mlp-width", type=int, default=64,
+                    help="with --profile-mlp / --profile-frame: 64 or 128 units per hidden layer")
+    ap.add_argument("--profile-frame", action="store_true",
+                    help="run six eager cache frames of the workload and one more inference, then exit (case for ncu)")
+    ap.add_argument("--mlp-encoding", default="frequency", choices=["frequency", "hashgrid"],
+                    help="with --profile-frame: the cache's input encoding")
     args = ap.parse_args()
     if args.impl == "reference":
         reference_arm(args)
         return
     if args.profile_pass:
         profile_pass(args.wavefront_samples, args.tuning)
+        return
+    if args.profile_frame:
+        profile_frame(args.mlp_encoding, args.mlp_width)
         return
     if args.profile_mlp:
         profile_mlp(args.mlp_width)

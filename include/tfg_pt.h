@@ -489,6 +489,10 @@ int  tfgMlpSetHashParams(TfgColorMLP* mlp, const float* host, int64_t count);
 int  tfgMlpComputeGradientEx(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t n_available, uint32_t seed,
                              float* host_grad, uint32_t count, float* host_table_grad, int64_t table_count,
                              float* loss_out);
+/* One-blob encoding (the composite encoding's direction and normal input) of
+ * `n` values in [0, 1] (device array): 4 bins each into `bins` (device, 4 n
+ * floats), exactly as the cache kernels compute them. */
+int  tfgOneBlobBins(const float* values, float* bins, int32_t n, void* stream);
 /* Length of the model's FP32 parameter arrays: 96 W + W^2 (hidden - 1) + 16 W
  * for width W (23552 for 5 hidden layers of 64, 79872 for 5 of 128). */
 int32_t tfgMlpParamCount(const TfgColorMLP* mlp);

@@ -123,6 +123,15 @@ def hash_index(x, y, z, N: int, dense: bool, T: int):
     return (x ^ ((y * np.uint64(2654435761)) & m) ^ ((z * np.uint64(805459861)) & m)) & np.uint64(T - 1)
 
 
+def one_blob(s: np.ndarray, k: int = 4) -> np.ndarray:
+    """One-blob bins (Mueller et al. 2019) of inputs s in [0, 1]: bin b holds
+    the mass of a Gaussian of sigma 1/k centred at s that falls in
+    [b/k, (b+1)/k), in FP64 (n x k)."""
+    s = np.asarray(s, np.float64)
+    cdf = [ndtr((b / k - s) * k) for b in range(k + 1)]
+    return np.stack([cdf[b + 1] - cdf[b] for b in range(k)], 1)
+
+
 def composite_encode(r15: np.ndarray, table: np.ndarray, cfg: dict):
     """Layer-0 input (n x 96) of the composite encoding -- 2L hash-grid
     features, 6 x 4 one-blob bins, 6 albedos, the constant 1 -- and, per
@@ -148,12 +157,8 @@ def composite_encode(r15: np.ndarray, table: np.ndarray, cfg: dict):
             x[:, 2 * l:2 * l + 2] += w[:, None] * tab[l, q]
             lst.append((l * T + q, w))
         corners.append(lst)
-    k = 4
     for j in range(6):
-        s = r15[:, 3 + j].astype(np.float64)
-        cdf = [ndtr((b / k - s) * k) for b in range(k + 1)]
-        for b in range(k):
-            x[:, 32 + k * j + b] = cdf[b + 1] - cdf[b]
+        x[:, 32 + 4 * j:36 + 4 * j] = one_blob(r15[:, 3 + j])
     x[:, 56:62] = r15[:, 9:15]
     x[:, 62] = 1.0
     return x, corners

@@ -11,7 +11,8 @@ from oracle import mlp_oracle as mo
 from oracle import oracle as orc
 from tfg_b200 import pathtracer as pt
 from tfg_b200 import scenes
-from tfg_b200.nrc import BF16, EMA, FP8, HASHGRID, WEIGHTS, ColorMLP, NrcRenderer, hashgrid_reference, split_layers
+from tfg_b200.nrc import (BF16, EMA, FP8, HASHGRID, WEIGHTS, ColorMLP, NrcRenderer, hashgrid_reference,
+                          one_blob_bins, split_layers)
 from tfg_b200.structs import DATOS_MLP
 
 pytestmark = pytest.mark.gpu
@@ -82,6 +83,29 @@ def test_inference_matches_fp64_model(built, cfg):
     x0[:, :2 * full["n_levels"]] = 0.0
     assert np.abs(mo.forward(W, x0)[0] - raw).mean() > 10 * np.abs(got - want).mean()
     m.close()
+
+
+def test_one_blob_bins_match_the_normal_cdf(built):
+    # The kernels' normal CDF (Abramowitz & Stegun 26.2.17, |error| < 7.5e-8)
+    # against the FP64 bins of the oracle and against CUDA's own normal CDF
+    # (torch.special.ndtr in FP32) on the same FP32 inputs.
+    rng = np.random.default_rng(21)
+    s = np.concatenate([np.linspace(0.0, 1.0, 4097), rng.uniform(0.0, 1.0, 20000),
+                        [0.0, 1.0, 1e-7, 1.0 - 6e-8, 0.125, 0.375, 0.625, 0.875]]).astype(np.float32)
+    st = torch.from_numpy(s).cuda()
+    got = one_blob_bins(st)
+    torch.cuda.synchronize()
+    g = got.cpu().numpy().astype(np.float64)
+    ref = mo.one_blob(s.astype(np.float64))
+    err = np.abs(g - ref).max()
+    assert err < 4e-7, f"one-blob bins differ from FP64 by {err:.3e}"
+    edges = torch.arange(5, device="cuda", dtype=torch.float32) / 4.0
+    cdf = torch.special.ndtr((edges[None, :] - st[:, None]) * 4.0)
+    cuda_bins = (cdf[:, 1:] - cdf[:, :-1]).cpu().numpy().astype(np.float64)
+    assert np.abs(g - cuda_bins).max() < 5e-7
+    assert (g >= -1e-7).all() and np.isfinite(g).all()
+    # an empty call is a no-op
+    assert one_blob_bins(torch.zeros(0, device="cuda")).shape == (0, 4)
 
 
 def test_gradients_match_fp64_model(built):

@@ -186,8 +186,8 @@ constexpr int kHashLive = 63;     // live input columns of layer 0 with the comp
 constexpr int kFreqLive = 85;     // ... with the frequency encoding
 
 struct HashGrid {
-    const float2* master;    // FP32 tables [level][T] (training forward); null: use `infer`
-    const __half2* infer;    // FP16 tables of the debiased weight average (inference)
+    const float2* master;    // FP32 tables [level][T], read by the training forward pass
+    const __half2* infer;    // FP16 tables of the debiased weight average, read by inference
     uint32_t T;              // entries per level (a power of two)
     int levels;              // 0: frequency encoding
     uint32_t dense;          // bit l: level l indexed densely
@@ -215,7 +215,38 @@ __device__ __forceinline__ void hash_cell(const float (&p)[3], float n, uint32_t
     }
 }
 
-// The 2L hash-grid features of position p.
+// Byte offsets, within its level's table, of the x pair (cx, cx + 1) of each
+// of a cell's four (y, z) corner rows (row r: y + (r & 1), z + (r >> 1)),
+// for entries of E bytes (a power of two).  Scaling by E distributes over the
+// hash's XOR and mask (both primes and the mask are pre-scaled, the mask stays
+// below 2^32 for T <= 2^24), so each corner costs one logic op.
+template <uint32_t E>
+__device__ __forceinline__ void level_rows(const uint32_t (&i)[3], uint32_t n_cells, bool dense, uint32_t T,
+                                           uint32_t (&o0)[4], uint32_t (&o1)[4]) {
+    if (dense) {
+        const uint32_t st = n_cells + 1u;
+        const uint32_t b = (i[0] + st * (i[1] + st * i[2])) * E, sy = st * E, sz = st * st * E;
+        o0[0] = b; o0[1] = b + sy; o0[2] = b + sz; o0[3] = b + sz + sy;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) o1[r] = o0[r] + E;
+    } else {
+        constexpr uint32_t P1 = 2654435761u * E, P2 = 805459861u * E;
+        const uint32_t m = (T - 1u) * E;
+        const uint32_t y0 = i[1] * P1, y1 = y0 + P1, z0 = i[2] * P2, z1 = z0 + P2;
+        const uint32_t x0 = i[0] * E, x1 = x0 + E;
+        const uint32_t yz[4] = {y0 ^ z0, y1 ^ z0, y0 ^ z1, y1 ^ z1};
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            o0[r] = (x0 ^ yz[r]) & m;
+            o1[r] = (x1 ^ yz[r]) & m;
+        }
+    }
+}
+
+// The 2L hash-grid features of position p from the FP32 tables (the training
+// forward pass).  A level's trilinear sum runs over its four (y, z) corner
+// rows: each row's x pair is blended with the x weights, then the row with
+// its (y, z) weight.
 __device__ __forceinline__ void hash_features(const float (&p)[3], const HashGrid& g, float (&h)[2 * kHashMaxLevels]) {
 #pragma unroll
     for (int l = 0; l < kHashMaxLevels; ++l) {
@@ -223,50 +254,86 @@ __device__ __forceinline__ void hash_features(const float (&p)[3], const HashGri
         h[2 * l + 1] = 0.0f;
         if (l >= g.levels) continue;
         const float n = g.res[l];
-        uint32_t i[3];
+        uint32_t i[3], o0[4], o1[4];
         float f[3];
         hash_cell(p, n, i, f);
-        const bool dense = (g.dense >> l) & 1u;
-        const size_t base = (size_t)l * g.T;
+        level_rows<8>(i, (uint32_t)n, (g.dense >> l) & 1u, g.T, o0, o1);
+        const char* lvl = reinterpret_cast<const char*>(g.master + (size_t)l * g.T);
+        const float wx0 = 1.0f - f[0], wy0 = 1.0f - f[1], wz0 = 1.0f - f[2];
         float a0 = 0.0f, a1 = 0.0f;
 #pragma unroll
-        for (int c = 0; c < 8; ++c) {
-            const uint32_t cx = i[0] + (c & 1), cy = i[1] + ((c >> 1) & 1), cz = i[2] + (c >> 2);
-            const float w = ((c & 1) ? f[0] : 1.0f - f[0]) * ((c & 2) ? f[1] : 1.0f - f[1]) *
-                            ((c & 4) ? f[2] : 1.0f - f[2]);
-            const uint32_t k = hash_index(cx, cy, cz, (uint32_t)n, dense, g.T);
-            float2 v;
-            if (g.master) v = __ldg(&g.master[base + k]);
-            else v = __half22float2(__ldg(&g.infer[base + k]));
-            a0 = fmaf(w, v.x, a0);
-            a1 = fmaf(w, v.y, a1);
+        for (int r = 0; r < 4; ++r) {
+            const float2 v0 = __ldg(reinterpret_cast<const float2*>(lvl + o0[r]));
+            const float2 v1 = __ldg(reinterpret_cast<const float2*>(lvl + o1[r]));
+            const float wyz = ((r & 1) ? f[1] : wy0) * ((r & 2) ? f[2] : wz0);
+            a0 = fmaf(wyz, fmaf(f[0], v1.x, wx0 * v0.x), a0);
+            a1 = fmaf(wyz, fmaf(f[0], v1.y, wx0 * v0.y), a1);
         }
         h[2 * l] = a0;
         h[2 * l + 1] = a1;
     }
 }
 
+// The same features from the FP16 image of the averaged tables (inference),
+// interpolated in FP16 pair arithmetic: word l holds level l's two features,
+// in the FP16 operand format layer 0 reads.
+__device__ __forceinline__ void hash_words_f16(const float (&p)[3], const HashGrid& g, __half2 (&h)[kHashMaxLevels]) {
+#pragma unroll
+    for (int l = 0; l < kHashMaxLevels; ++l) {
+        h[l] = __float2half2_rn(0.0f);
+        if (l >= g.levels) continue;
+        const float n = g.res[l];
+        uint32_t i[3], o0[4], o1[4];
+        float f[3];
+        hash_cell(p, n, i, f);
+        level_rows<4>(i, (uint32_t)n, (g.dense >> l) & 1u, g.T, o0, o1);
+        const char* lvl = reinterpret_cast<const char*>(g.infer + (size_t)l * g.T);
+        const __half2 hx0 = __float2half2_rn(1.0f - f[0]), hx1 = __float2half2_rn(f[0]);
+        const float wy0 = 1.0f - f[1], wz0 = 1.0f - f[2];
+        __half2 acc = __float2half2_rn(0.0f);
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const __half2 v0 = __ldg(reinterpret_cast<const __half2*>(lvl + o0[r]));
+            const __half2 v1 = __ldg(reinterpret_cast<const __half2*>(lvl + o1[r]));
+            const __half2 wyz = __float2half2_rn(((r & 1) ? f[1] : wy0) * ((r & 2) ? f[2] : wz0));
+            acc = __hfma2(wyz, __hfma2(hx1, v1, __hmul2(hx0, v0)), acc);
+        }
+        h[l] = acc;
+    }
+}
+
+// Standard normal CDF by Abramowitz & Stegun, Handbook of Mathematical
+// Functions, formula 26.2.17 (Hastings' rational approximation, absolute
+// error below 7.5e-8): Phi(x) = 1 - phi(x) (b1 t + ... + b5 t^5) with
+// t = 1 / (1 + p |x|) for x >= 0, and Phi(x) = 1 - Phi(-x).  About half
+// the instructions of the library's normcdff; the one-blob bins are its only
+// user.
+__device__ __forceinline__ float std_normal_cdf(float x) {
+    const float ax = fabsf(x);
+    const float t = __fdividef(1.0f, fmaf(0.2316419f, ax, 1.0f));
+    float poly = fmaf(t, 1.330274429f, -1.821255978f);
+    poly = fmaf(t, poly, 1.781477937f);
+    poly = fmaf(t, poly, -0.356563782f);
+    poly = fmaf(t, poly, 0.319381530f);
+    poly *= t;
+    const float tail = 0.3989422804f * __expf(-0.5f * ax * ax) * poly;   // phi(|x|) * poly
+    return x >= 0.0f ? 1.0f - tail : tail;
+}
+
 // One-blob bins of an input in [0, 1]: Phi((b+1)/k - s; 1/k) - Phi(b/k - s; 1/k).
 __device__ __forceinline__ void one_blob(float s, float (&o)[kBlobBins]) {
-    float prev = normcdff((0.0f - s) * (float)kBlobBins);
+    float prev = std_normal_cdf((0.0f - s) * (float)kBlobBins);
 #pragma unroll
     for (int b = 0; b < kBlobBins; ++b) {
-        const float next = normcdff(((float)(b + 1) / (float)kBlobBins - s) * (float)kBlobBins);
+        const float next = std_normal_cdf(((float)(b + 1) / (float)kBlobBins - s) * (float)kBlobBins);
         o[b] = next - prev;
         prev = next;
     }
 }
 
-// The 64 features of layer 0 with the composite encoding (63 live + one zero).
-__device__ __forceinline__ void composite_features(const TfgDatosMLP& d, const Bounds& b, const HashGrid& g,
-                                                   float (&x)[64]) {
-    const float p[3] = {unit_clamp((float)d.posicion.x, b.lo[0], b.hi[0]),
-                        unit_clamp((float)d.posicion.y, b.lo[1], b.hi[1]),
-                        unit_clamp((float)d.posicion.z, b.lo[2], b.hi[2])};
-    float h[2 * kHashMaxLevels];
-    hash_features(p, g, h);
-#pragma unroll
-    for (int k = 0; k < 32; ++k) x[k] = h[k];
+// Features 32..63 of layer 0 with the composite encoding: one-blob bins of
+// direction and normal, the albedos, the constant 1 and a zero.
+__device__ __forceinline__ void composite_tail(const TfgDatosMLP& d, float (&x)[32]) {
     const float dirn[6] = {(float)d.direccion.x, (float)d.direccion.y, (float)d.direccion.z,
                            (float)d.normal.x,    (float)d.normal.y,    (float)d.normal.z};
 #pragma unroll
@@ -274,15 +341,38 @@ __device__ __forceinline__ void composite_features(const TfgDatosMLP& d, const B
         float o[kBlobBins];
         one_blob(dirn[j], o);
 #pragma unroll
-        for (int k = 0; k < kBlobBins; ++k) x[32 + kBlobBins * j + k] = o[k];
+        for (int k = 0; k < kBlobBins; ++k) x[kBlobBins * j + k] = o[k];
     }
-    x[56] = d.difuso.r; x[57] = d.difuso.g; x[58] = d.difuso.b;
-    x[59] = d.especular.r; x[60] = d.especular.g; x[61] = d.especular.b;
-    x[62] = 1.0f;
-    x[63] = 0.0f;
+    x[24] = d.difuso.r; x[25] = d.difuso.g; x[26] = d.difuso.b;
+    x[27] = d.especular.r; x[28] = d.especular.g; x[29] = d.especular.b;
+    x[30] = 1.0f;
+    x[31] = 0.0f;
 }
 
-// Encoded features of one sample, packed as 48 FP16 pairs (96 features).
+__device__ __forceinline__ void unit_position(const TfgDatosMLP& d, const Bounds& b, float (&p)[3]) {
+    p[0] = unit_clamp((float)d.posicion.x, b.lo[0], b.hi[0]);
+    p[1] = unit_clamp((float)d.posicion.y, b.lo[1], b.hi[1]);
+    p[2] = unit_clamp((float)d.posicion.z, b.lo[2], b.hi[2]);
+}
+
+// The 64 features of layer 0 with the composite encoding (63 live + one zero)
+// from the FP32 tables (training forward pass).
+__device__ __forceinline__ void composite_features(const TfgDatosMLP& d, const Bounds& b, const HashGrid& g,
+                                                   float (&x)[64]) {
+    float p[3];
+    unit_position(d, b, p);
+    float h[2 * kHashMaxLevels], t[32];
+    hash_features(p, g, h);
+    composite_tail(d, t);
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        x[k] = h[k];
+        x[32 + k] = t[k];
+    }
+}
+
+// Encoded features of one training sample, packed as 48 FP16 pairs (96
+// features); the composite encoding reads the FP32 tables.
 __device__ __forceinline__ void encode(const TfgDatosMLP& d, const Bounds& b, const HashGrid& g, uint32_t (&w)[48]) {
     if (g.levels > 0) {
         float x[64];
@@ -465,17 +555,35 @@ template <int PREC, bool HASH>
 __device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Bounds& b, const HashGrid& g, float q0,
                                                 uint32_t ta) {
     if constexpr (HASH) {
-        // composite encoding: 64 features, the largest |feature| for the FP8 scale
-        float x[64];
-        composite_features(*r, b, g, x);
+        // composite encoding: the hash-grid pairs straight from the FP16
+        // interpolation, then the one-blob / albedo features; the largest
+        // |feature| for the FP8 scale
+        float p[3];
+        unit_position(*r, b, p);
+        __half2 hw[kHashMaxLevels];
+        hash_words_f16(p, g, hw);
+        float t[32];
+        composite_tail(*r, t);
+        float x[32];
+#pragma unroll
+        for (int k = 0; k < kHashMaxLevels; ++k) {
+            const float2 v = __half22float2(hw[k]);
+            x[2 * k] = v.x;
+            x[2 * k + 1] = v.y;
+        }
         float amax = 1.0f;
 #pragma unroll
-        for (int k = 0; k < 62; ++k) amax = fmaxf(amax, fabsf(x[k]));
+        for (int k = 0; k < 32; ++k) amax = fmaxf(amax, fabsf(x[k]));
+#pragma unroll
+        for (int k = 0; k < 30; ++k) amax = fmaxf(amax, fabsf(t[k]));
         if constexpr (PREC == kPrecF8) {
             uint32_t w[24];
 #pragma unroll
-            for (int k = 0; k < 16; ++k)
+            for (int k = 0; k < 8; ++k)
                 w[k] = pack_e4m3x4<false>(x[4 * k] * q0, x[4 * k + 1] * q0, x[4 * k + 2] * q0, x[4 * k + 3] * q0);
+#pragma unroll
+            for (int k = 0; k < 8; ++k)
+                w[8 + k] = pack_e4m3x4<false>(t[4 * k] * q0, t[4 * k + 1] * q0, t[4 * k + 2] * q0, t[4 * k + 3] * q0);
 #pragma unroll
             for (int k = 16; k < 24; ++k) w[k] = 0u;
             umma::tmem_st16(ta, *reinterpret_cast<const uint32_t(*)[16]>(w));
@@ -483,7 +591,12 @@ __device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Boun
         } else {
             uint32_t w[48];
 #pragma unroll
-            for (int k = 0; k < 32; ++k) w[k] = pack2<PREC>(x[2 * k], x[2 * k + 1]);
+            for (int k = 0; k < kHashMaxLevels; ++k) {
+                if constexpr (PREC == kPrecBF16) w[k] = pack_bf2(x[2 * k], x[2 * k + 1]);
+                else w[k] = *reinterpret_cast<const uint32_t*>(&hw[k]);
+            }
+#pragma unroll
+            for (int k = 0; k < 16; ++k) w[16 + k] = pack2<PREC>(t[2 * k], t[2 * k + 1]);
 #pragma unroll
             for (int k = 32; k < 48; ++k) w[k] = 0u;
 #pragma unroll
@@ -1569,7 +1682,14 @@ struct HashGradArgs {
     int hid;                     // hidden width: 64 or 128
 };
 
-__global__ void __launch_bounds__(128) k_hash_grad(HashGradArgs a) {
+// One thread per (sample, level): 16 samples x 16 levels per 256-thread
+// block.  The thread forms its level's two feature gradients from the
+// sample's layer-0 output gradient and the FP16-rounded layer-0 weights the
+// forward pass used, then scatters them to the level's 8 corners.
+constexpr int kHashGradThreads = 256;
+constexpr int kHashGradSamples = kHashGradThreads / kHashMaxLevels;
+
+__global__ void __launch_bounds__(kHashGradThreads) k_hash_grad(HashGradArgs a) {
     __shared__ float sw[128][2 * kHashMaxLevels];
     const int L2 = 2 * a.hg.levels;
     for (int i = threadIdx.x; i < a.hid * 2 * kHashMaxLevels; i += blockDim.x) {
@@ -1577,46 +1697,41 @@ __global__ void __launch_bounds__(128) k_hash_grad(HashGradArgs a) {
         sw[o][j] = j < L2 ? __half2float(__float2half_rn(a.w0[o * 96 + j])) : 0.0f;
     }
     __syncthreads();
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = blockIdx.x * kHashGradSamples + threadIdx.x / kHashMaxLevels;
+    const int l = (int)(threadIdx.x % kHashMaxLevels);
     const uint32_t n_avail = a.state[S_NAVAIL];
-    if (s >= a.batch || n_avail < a.min_n || n_avail == 0) return;
+    if (s >= a.batch || l >= a.hg.levels || n_avail < a.min_n || n_avail == 0) return;
     // the sample k_train drew for row s (NrcKernel.cu:10-16)
     uint32_t st = a.state[S_STEP] ^ s;
     const uint32_t idx = pcg_next(st) % n_avail;
-    const TfgDatosMLP d = a.buf[idx];
+    const TfgDatosMLP* d = a.buf + idx;
     const uint32_t tile = s / kTile, t = s % kTile;
     const uint8_t* region = a.zT0 + (size_t)tile * (2 * a.hid * 128) + (t >> 6) * (a.hid * 128);
     const uint32_t c = (t & 63u) >> 3, e = t & 7u;
-    float dx[2 * kHashMaxLevels];
-#pragma unroll
-    for (int j = 0; j < 2 * kHashMaxLevels; ++j) dx[j] = 0.0f;
+    float dx0 = 0.0f, dx1 = 0.0f;
     for (int o = 0; o < a.hid; ++o) {
         const float dz = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(region + umma::sw128_offset(o, c) + 2 * e));
         if (dz == 0.0f) continue;
-#pragma unroll
-        for (int j = 0; j < 2 * kHashMaxLevels; ++j) dx[j] = fmaf(dz, sw[o][j], dx[j]);
+        dx0 = fmaf(dz, sw[o][2 * l], dx0);
+        dx1 = fmaf(dz, sw[o][2 * l + 1], dx1);
     }
-    const float p[3] = {unit_clamp((float)d.posicion.x, a.bounds.lo[0], a.bounds.hi[0]),
-                        unit_clamp((float)d.posicion.y, a.bounds.lo[1], a.bounds.hi[1]),
-                        unit_clamp((float)d.posicion.z, a.bounds.lo[2], a.bounds.hi[2])};
+    if (dx0 == 0.0f && dx1 == 0.0f) return;
+    const float p[3] = {unit_clamp((float)d->posicion.x, a.bounds.lo[0], a.bounds.hi[0]),
+                        unit_clamp((float)d->posicion.y, a.bounds.lo[1], a.bounds.hi[1]),
+                        unit_clamp((float)d->posicion.z, a.bounds.lo[2], a.bounds.hi[2])};
+    const float n = a.hg.res[l];
+    uint32_t i[3];
+    float f[3];
+    hash_cell(p, n, i, f);
+    const bool dense = (a.hg.dense >> l) & 1u;
+    float2* grad = a.grad + (size_t)l * a.hg.T;
 #pragma unroll
-    for (int l = 0; l < kHashMaxLevels; ++l) {
-        if (l >= a.hg.levels) break;
-        if (dx[2 * l] == 0.0f && dx[2 * l + 1] == 0.0f) continue;
-        const float n = a.hg.res[l];
-        uint32_t i[3];
-        float f[3];
-        hash_cell(p, n, i, f);
-        const bool dense = (a.hg.dense >> l) & 1u;
-        const size_t base = (size_t)l * a.hg.T;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const uint32_t cx = i[0] + (k & 1), cy = i[1] + ((k >> 1) & 1), cz = i[2] + (k >> 2);
-            const float w = ((k & 1) ? f[0] : 1.0f - f[0]) * ((k & 2) ? f[1] : 1.0f - f[1]) *
-                            ((k & 4) ? f[2] : 1.0f - f[2]);
-            const uint32_t q = hash_index(cx, cy, cz, (uint32_t)n, dense, a.hg.T);
-            atomicAdd(&a.grad[base + q], make_float2(w * dx[2 * l], w * dx[2 * l + 1]));
-        }
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t cx = i[0] + (k & 1), cy = i[1] + ((k >> 1) & 1), cz = i[2] + (k >> 2);
+        const float w = ((k & 1) ? f[0] : 1.0f - f[0]) * ((k & 2) ? f[1] : 1.0f - f[1]) *
+                        ((k & 4) ? f[2] : 1.0f - f[2]);
+        const uint32_t q = hash_index(cx, cy, cz, (uint32_t)n, dense, a.hg.T);
+        atomicAdd(&grad[q], make_float2(w * dx0, w * dx1));
     }
 }
 
@@ -1633,26 +1748,59 @@ struct HashAdamArgs {
     int update;
 };
 
+// Adam step of one table value: updates w, m, v, e in place and returns the
+// inference value (the debiased average, or w before the first step).
+struct HashAdamStep {
+    float lr, beta1, beta2, eps, decay, grad_scale, bc1, bc2, ema_debias;
+    bool update;
+    __device__ __forceinline__ float operator()(float& w, float& m, float& v, float& e, float g) const {
+        if (update) {
+            g *= grad_scale;
+            m = beta1 * m + (1.0f - beta1) * g;
+            v = beta2 * v + (1.0f - beta2) * g * g;
+            w -= lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+            e = decay * e + (1.0f - decay) * w;
+        }
+        return ema_debias > 0.0f ? e / ema_debias : w;
+    }
+};
+
+// Four values per thread and iteration (16-byte loads and stores of every
+// array; the arrays are separate allocations, so 16-byte aligned), then a
+// scalar tail.  Gradient, moments, masters and average are read once and
+// written once: 38 bytes per value.
 __global__ void k_adam_hash(HashAdamArgs a) {
     const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
     const float tn = (float)(a.state[S_ADAM_T] + (update ? 1u : 0u));
-    const float bc1 = 1.0f - powf(a.beta1, tn), bc2 = 1.0f - powf(a.beta2, tn);
-    const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
-    for (size_t i = blockIdx.x * (size_t)blockDim.x + threadIdx.x; i < a.count; i += (size_t)gridDim.x * blockDim.x) {
-        float w = a.w[i], e = a.ema[i];
-        if (update) {
-            const float g = a.grad[i] * a.grad_scale;
-            const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
-            const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
-            a.m[i] = m;
-            a.v[i] = v;
-            w -= a.lr * (m / bc1) / (sqrtf(v / bc2) + a.eps);
-            e = a.decay * e + (1.0f - a.decay) * w;
-            a.w[i] = w;
-            a.ema[i] = e;
-        }
+    HashAdamStep st{a.lr, a.beta1, a.beta2, a.eps, a.decay, a.grad_scale,
+                    1.0f - powf(a.beta1, tn), 1.0f - powf(a.beta2, tn),
+                    tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f, update};
+    const size_t n4 = a.count / 4, stride = (size_t)gridDim.x * blockDim.x;
+    const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
+    float4* w4 = reinterpret_cast<float4*>(a.w);
+    float4* m4 = reinterpret_cast<float4*>(a.m);
+    float4* v4 = reinterpret_cast<float4*>(a.v);
+    float4* e4 = reinterpret_cast<float4*>(a.ema);
+    float4* g4 = reinterpret_cast<float4*>(a.grad);
+    uint2* i4 = reinterpret_cast<uint2*>(a.infer);
+    for (size_t i = t0; i < n4; i += stride) {
+        float4 w = w4[i], e = e4[i];
+        const float4 g = g4[i];
+        float4 m = make_float4(0.f, 0.f, 0.f, 0.f), v = m;
+        if (update) { m = m4[i]; v = v4[i]; }
+        const float r0 = st(w.x, m.x, v.x, e.x, g.x), r1 = st(w.y, m.y, v.y, e.y, g.y);
+        const float r2 = st(w.z, m.z, v.z, e.z, g.z), r3 = st(w.w, m.w, v.w, e.w, g.w);
+        if (update) { m4[i] = m; v4[i] = v; w4[i] = w; e4[i] = e; }
+        g4[i] = make_float4(0.f, 0.f, 0.f, 0.f);
+        __half2 h01 = __floats2half2_rn(r0, r1), h23 = __floats2half2_rn(r2, r3);
+        i4[i] = make_uint2(*reinterpret_cast<uint32_t*>(&h01), *reinterpret_cast<uint32_t*>(&h23));
+    }
+    for (size_t i = 4 * n4 + t0; i < a.count; i += stride) {
+        float w = a.w[i], m = update ? a.m[i] : 0.0f, v = update ? a.v[i] : 0.0f, e = a.ema[i];
+        const float r = st(w, m, v, e, a.grad[i]);
+        if (update) { a.m[i] = m; a.v[i] = v; a.w[i] = w; a.ema[i] = e; }
         a.grad[i] = 0.0f;
-        a.infer[i] = __float2half_rn(ema_debias > 0.0f ? e / ema_debias : w);
+        a.infer[i] = __float2half_rn(r);
     }
 }
 
@@ -1904,7 +2052,7 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
         ha.buf = buf; ha.state = n->dstate; ha.min_n = min_n; ha.batch = n->batch; ha.bounds = n->bounds;
         ha.zT0 = n->zT[0]; ha.w0 = n->w; ha.grad = reinterpret_cast<float2*>(n->hgrad); ha.hg = hash_view(n, true);
         ha.hid = n->hid;
-        mlp::k_hash_grad<<<tiles, mlp::kTile, 0, s>>>(ha);
+        mlp::k_hash_grad<<<(n->batch + mlp::kHashGradSamples - 1) / mlp::kHashGradSamples, mlp::kHashGradThreads, 0, s>>>(ha);
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "mlp step: table gradient");
     }
@@ -2312,6 +2460,33 @@ extern "C" int tfgMlpCreateHashGrid(uint32_t n_in, uint32_t n_out, uint32_t batc
 extern "C" int tfgMlpCreateWide(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
                                 int32_t width, const TfgHashGridConfig* config, TfgColorMLP** out) {
     return tfg::create_model(n_in, n_out, batch, seed, hidden_layers, width, config, out);
+}
+
+namespace tfg {
+namespace mlp {
+__global__ void k_one_blob(const float* __restrict__ in, float* __restrict__ out, int32_t n) {
+    const int32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float o[kBlobBins];
+    one_blob(in[i], o);
+#pragma unroll
+    for (int b = 0; b < kBlobBins; ++b) out[kBlobBins * i + b] = o[b];
+}
+}  // namespace mlp
+}  // namespace tfg
+
+extern "C" int tfgOneBlobBins(const float* values, float* bins, int32_t n, void* stream) {
+    if (n < 0) return tfg::fail(TFG_E_INVALID, "tfgOneBlobBins: negative n");
+    if (n == 0) return tfg::ok();
+    if (!values || !bins) return tfg::fail(TFG_E_INVALID, "tfgOneBlobBins: null pointer");
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return tfg::fail((int)e, cudaGetErrorString(e));
+    if (int rc = tfg::require_sm100(dev)) return rc;
+    tfg::mlp::k_one_blob<<<(unsigned)((n + 255) / 256), 256, 0, (cudaStream_t)stream>>>(values, bins, n);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return tfg::fail((int)e, std::string("tfgOneBlobBins: ") + cudaGetErrorString(e));
+    return tfg::ok();
 }
 
 extern "C" int64_t tfgMlpHashParamCount(const TfgColorMLP* h) {

@@ -36,6 +36,16 @@ def hashgrid_reference() -> dict:
             "base_resolution": c.base_resolution, "per_level_scale": c.per_level_scale}
 
 
+def one_blob_bins(values: torch.Tensor, stream=None) -> torch.Tensor:
+    """One-blob bins (4 per value) of a CUDA float32 tensor of values in
+    [0, 1], as the composite encoding computes them (tfgOneBlobBins)."""
+    if values.dtype != torch.float32 or not values.is_cuda or not values.is_contiguous():
+        raise ValueError("one_blob_bins wants a contiguous float32 CUDA tensor")
+    out = torch.empty(values.numel() * 4, dtype=torch.float32, device=values.device)
+    _lib.call("tfgOneBlobBins", values.data_ptr(), out.data_ptr(), values.numel(), _stream(stream))
+    return out.view(-1, 4)
+
+
 def _stream(stream=None) -> int:
     s = stream if stream is not None else torch.cuda.current_stream()
     return s.cuda_stream
