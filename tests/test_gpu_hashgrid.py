@@ -134,6 +134,40 @@ def test_gradients_match_fp64_model(built):
     m.close()
 
 
+def test_table_adam_steps_follow_the_recurrence(built):
+    # Two training steps: each step's table moments, values and average against
+    # the Adam / weight-average recurrence in FP64, from the tables before the
+    # step and that step's gradient (same sample draw, from the step word).
+    b1, b2, lr, eps, decay = 0.9, 0.99, 1e-3, 1e-15, 0.99
+    m = _model(SMALL, seed=13)
+    m.set_hyperparams(lr=lr, beta1=b1, beta2=b2, eps=eps, ema_decay=decay)
+    rng = np.random.default_rng(17)
+    n = 20000
+    dd = _dev(_datos(rng, n))
+    prev = [np.zeros(m.n_table) if k else m.get_table(WEIGHTS).astype(np.float64) for k in range(4)]
+    for t in (1, 2):
+        _, g, _ = m.compute_gradient_ex(dd, n, seed=m.state()["step"])
+        g = g.astype(np.float64)
+        m.train_step(dd, n, read_loss=False)
+        w, e, mm, vv = [m.get_table(k).astype(np.float64) for k in range(4)]
+        w0, e0, m0, v0 = prev
+        m_ref = b1 * m0 + (1 - b1) * g
+        v_ref = b2 * v0 + (1 - b2) * g * g
+        np.testing.assert_allclose(mm, m_ref, rtol=1e-4, atol=1e-4 * np.abs(m_ref).max())
+        np.testing.assert_allclose(vv, v_ref, rtol=1e-4, atol=1e-4 * np.abs(v_ref).max())
+        # the value update from the device's own moments (its FP32 rounding of them)
+        step = lr * (mm / (1 - b1 ** t)) / (np.sqrt(vv / (1 - b2 ** t)) + eps)
+        moved = np.abs(g) > 1e-3 * np.abs(g).max()
+        # the values are FP32: w0 - w carries their rounding (a few ulps of |w|)
+        ulp = float(np.spacing(np.float32(np.abs(w0).max())))
+        np.testing.assert_allclose((w0 - w)[moved], step[moved], rtol=1e-3, atol=4 * ulp)
+        assert np.abs(w - (w0 - step)).max() < 1e-6
+        np.testing.assert_allclose(e, decay * e0 + (1 - decay) * w, rtol=1e-5, atol=1e-9)
+        prev = [w, e, mm, vv]
+    assert m.state()["adam_t"] == 2
+    m.close()
+
+
 def test_online_training_fits_a_spatial_signal(built):
     def f(pos, kd):
         s = 0.5 + 0.4 * np.sin(1.3 * pos[:, 0]) * np.cos(0.9 * pos[:, 2]) + 0.2 * np.sin(2.1 * pos[:, 1])

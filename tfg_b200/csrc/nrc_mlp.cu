@@ -276,29 +276,46 @@ __device__ __forceinline__ void hash_features(const float (&p)[3], const HashGri
 
 // The same features from the FP16 image of the averaged tables (inference),
 // interpolated in FP16 pair arithmetic: word l holds level l's two features,
-// in the FP16 operand format layer 0 reads.
+// in the FP16 operand format layer 0 reads.  Levels go in pairs whose 16
+// corner loads are all issued before either level is combined, so a thread
+// keeps twice the gathers in flight.
+constexpr int kHashLevelBatch = 2;
+
 __device__ __forceinline__ void hash_words_f16(const float (&p)[3], const HashGrid& g, __half2 (&h)[kHashMaxLevels]) {
 #pragma unroll
-    for (int l = 0; l < kHashMaxLevels; ++l) {
-        h[l] = __float2half2_rn(0.0f);
-        if (l >= g.levels) continue;
-        const float n = g.res[l];
-        uint32_t i[3], o0[4], o1[4];
-        float f[3];
-        hash_cell(p, n, i, f);
-        level_rows<4>(i, (uint32_t)n, (g.dense >> l) & 1u, g.T, o0, o1);
-        const char* lvl = reinterpret_cast<const char*>(g.infer + (size_t)l * g.T);
-        const __half2 hx0 = __float2half2_rn(1.0f - f[0]), hx1 = __float2half2_rn(f[0]);
-        const float wy0 = 1.0f - f[1], wz0 = 1.0f - f[2];
-        __half2 acc = __float2half2_rn(0.0f);
+    for (int l0 = 0; l0 < kHashMaxLevels; l0 += kHashLevelBatch) {
+        __half2 v[kHashLevelBatch][8];
+        float f[kHashLevelBatch][3];
 #pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const __half2 v0 = __ldg(reinterpret_cast<const __half2*>(lvl + o0[r]));
-            const __half2 v1 = __ldg(reinterpret_cast<const __half2*>(lvl + o1[r]));
-            const __half2 wyz = __float2half2_rn(((r & 1) ? f[1] : wy0) * ((r & 2) ? f[2] : wz0));
-            acc = __hfma2(wyz, __hfma2(hx1, v1, __hmul2(hx0, v0)), acc);
+        for (int b = 0; b < kHashLevelBatch; ++b) {
+            const int l = l0 + b;
+            if (l >= g.levels) continue;
+            const float n = g.res[l];
+            uint32_t i[3], o0[4], o1[4];
+            hash_cell(p, n, i, f[b]);
+            level_rows<4>(i, (uint32_t)n, (g.dense >> l) & 1u, g.T, o0, o1);
+            const char* lvl = reinterpret_cast<const char*>(g.infer + (size_t)l * g.T);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                v[b][2 * r] = __ldg(reinterpret_cast<const __half2*>(lvl + o0[r]));
+                v[b][2 * r + 1] = __ldg(reinterpret_cast<const __half2*>(lvl + o1[r]));
+            }
         }
-        h[l] = acc;
+#pragma unroll
+        for (int b = 0; b < kHashLevelBatch; ++b) {
+            const int l = l0 + b;
+            h[l] = __float2half2_rn(0.0f);
+            if (l >= g.levels) continue;
+            const __half2 hx0 = __float2half2_rn(1.0f - f[b][0]), hx1 = __float2half2_rn(f[b][0]);
+            const float wy0 = 1.0f - f[b][1], wz0 = 1.0f - f[b][2];
+            __half2 acc = __float2half2_rn(0.0f);
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const __half2 wyz = __float2half2_rn(((r & 1) ? f[b][1] : wy0) * ((r & 2) ? f[b][2] : wz0));
+                acc = __hfma2(wyz, __hfma2(hx1, v[b][2 * r + 1], __hmul2(hx0, v[b][2 * r])), acc);
+            }
+            h[l] = acc;
+        }
     }
 }
 
@@ -1691,13 +1708,28 @@ constexpr int kHashGradSamples = kHashGradThreads / kHashMaxLevels;
 
 __global__ void __launch_bounds__(kHashGradThreads) k_hash_grad(HashGradArgs a) {
     __shared__ float sw[128][2 * kHashMaxLevels];
+    __shared__ float sdz[kHashGradSamples][128 + 1];
     const int L2 = 2 * a.hg.levels;
     for (int i = threadIdx.x; i < a.hid * 2 * kHashMaxLevels; i += blockDim.x) {
         const int o = i / (2 * kHashMaxLevels), j = i % (2 * kHashMaxLevels);
         sw[o][j] = j < L2 ? __half2float(__float2half_rn(a.w0[o * 96 + j])) : 0.0f;
     }
+    // dZ_0 of the block's samples (rows of the transposed BF16 tiles), all
+    // loads in flight at once
+    const uint32_t s0 = blockIdx.x * kHashGradSamples;
+    for (int i = threadIdx.x; i < kHashGradSamples * a.hid; i += blockDim.x) {
+        const uint32_t j = (uint32_t)i % kHashGradSamples, o = (uint32_t)i / kHashGradSamples, s = s0 + j;
+        float v = 0.0f;
+        if (s < a.batch) {
+            const uint32_t tile = s / kTile, t = s % kTile;
+            const uint8_t* region = a.zT0 + (size_t)tile * (2 * a.hid * 128) + (t >> 6) * (a.hid * 128);
+            v = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(
+                region + umma::sw128_offset(o, (t & 63u) >> 3) + 2 * (t & 7u)));
+        }
+        sdz[j][o] = v;
+    }
     __syncthreads();
-    const uint32_t s = blockIdx.x * kHashGradSamples + threadIdx.x / kHashMaxLevels;
+    const uint32_t js = threadIdx.x / kHashMaxLevels, s = s0 + js;
     const int l = (int)(threadIdx.x % kHashMaxLevels);
     const uint32_t n_avail = a.state[S_NAVAIL];
     if (s >= a.batch || l >= a.hg.levels || n_avail < a.min_n || n_avail == 0) return;
@@ -1705,13 +1737,9 @@ __global__ void __launch_bounds__(kHashGradThreads) k_hash_grad(HashGradArgs a) 
     uint32_t st = a.state[S_STEP] ^ s;
     const uint32_t idx = pcg_next(st) % n_avail;
     const TfgDatosMLP* d = a.buf + idx;
-    const uint32_t tile = s / kTile, t = s % kTile;
-    const uint8_t* region = a.zT0 + (size_t)tile * (2 * a.hid * 128) + (t >> 6) * (a.hid * 128);
-    const uint32_t c = (t & 63u) >> 3, e = t & 7u;
     float dx0 = 0.0f, dx1 = 0.0f;
     for (int o = 0; o < a.hid; ++o) {
-        const float dz = __bfloat162float(*reinterpret_cast<const __nv_bfloat16*>(region + umma::sw128_offset(o, c) + 2 * e));
-        if (dz == 0.0f) continue;
+        const float dz = sdz[js][o];
         dx0 = fmaf(dz, sw[o][2 * l], dx0);
         dx1 = fmaf(dz, sw[o][2 * l + 1], dx1);
     }
@@ -1750,18 +1778,19 @@ struct HashAdamArgs {
 
 // Adam step of one table value: updates w, m, v, e in place and returns the
 // inference value (the debiased average, or w before the first step).
+// The bias corrections enter as reciprocals (one division per value left).
 struct HashAdamStep {
-    float lr, beta1, beta2, eps, decay, grad_scale, bc1, bc2, ema_debias;
+    float lr, beta1, beta2, eps, decay, grad_scale, inv_bc1, inv_bc2, inv_debias;
     bool update;
     __device__ __forceinline__ float operator()(float& w, float& m, float& v, float& e, float g) const {
         if (update) {
             g *= grad_scale;
             m = beta1 * m + (1.0f - beta1) * g;
             v = beta2 * v + (1.0f - beta2) * g * g;
-            w -= lr * (m / bc1) / (sqrtf(v / bc2) + eps);
+            w -= lr * (m * inv_bc1) / (sqrtf(v * inv_bc2) + eps);
             e = decay * e + (1.0f - decay) * w;
         }
-        return ema_debias > 0.0f ? e / ema_debias : w;
+        return inv_debias > 0.0f ? e * inv_debias : w;
     }
 };
 
@@ -1773,8 +1802,8 @@ __global__ void k_adam_hash(HashAdamArgs a) {
     const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
     const float tn = (float)(a.state[S_ADAM_T] + (update ? 1u : 0u));
     HashAdamStep st{a.lr, a.beta1, a.beta2, a.eps, a.decay, a.grad_scale,
-                    1.0f - powf(a.beta1, tn), 1.0f - powf(a.beta2, tn),
-                    tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f, update};
+                    1.0f / (1.0f - powf(a.beta1, tn)), 1.0f / (1.0f - powf(a.beta2, tn)),
+                    tn > 0.0f ? 1.0f / (1.0f - powf(a.decay, tn)) : 0.0f, update};
     const size_t n4 = a.count / 4, stride = (size_t)gridDim.x * blockDim.x;
     const size_t t0 = blockIdx.x * (size_t)blockDim.x + threadIdx.x;
     float4* w4 = reinterpret_cast<float4*>(a.w);
