@@ -79,6 +79,48 @@ def test_ref_layout_ids_bit_exact_vs_reference_traversal(setup):
     np.testing.assert_allclose(mine[hit, 1:3], ref[hit, 1:3], rtol=1e-5, atol=1e-6)
 
 
+def test_axis_plane_rays_keep_the_reference_hits(setup):
+    # Directions with exactly zero components (either sign of zero) take a
+    # finite reciprocal of that zero's sign in the slab tests (the reference's
+    # 1/0 = infinity gives 0 * infinity = NaN, which switches that axis' box
+    # culling off and made one bench camera ray decode 382 nodes instead of
+    # 7).  A ray with a signed-zero component is thereby treated as moving
+    # infinitesimally to that side.  The ids must equal the reference's except
+    # for rays lying exactly in a plane through mesh edges (here: origin x = 0,
+    # the icosphere's symmetry plane), and there only on the reference's edge
+    # hits, where the side the reference found depended on its disabled culling.
+    scene, ds, _, _ = setup
+    rng = np.random.default_rng(3)
+    n = 40000
+    r = np.zeros((n, 8), np.float32)
+    r[:, :3] = rng.uniform([-2.5, -1.9, -3.9], [2.5, 2.3, 5.4], (n, 3))
+    d = rng.normal(size=(n, 3))
+    k = rng.integers(0, 3, n)
+    d[np.arange(n), k] = 0.0
+    d[rng.random(n) < 0.25] *= np.array([0.0, 1.0, 0.0])[None, :]   # some rays along y only
+    d[(d == 0).all(1)] = [0.0, -1.0, 0.0]
+    d = d / np.linalg.norm(d, axis=1, keepdims=True)
+    d[rng.random((n, 3)) < 0.5] *= -1.0                                # -0.0 as well as +0.0
+    r[:, 4:7] = d
+    r[:, 3] = 1e9
+    r[: n // 4, 0] = 0.0                                                # in the symmetry plane x = 0
+    assert ((r[:, 4:7] == 0) & np.signbit(r[:, 4:7])).any() and ((r[:, 4:7] == 0) & ~np.signbit(r[:, 4:7])).any()
+    rays = torch.from_numpy(r.reshape(-1)).cuda()
+    mine = _trace(ds, rays, pt.TRIS_REF)
+    ref, _ = _ref_trace(ds, rays)
+    a, b = mine[:, 3].view(np.uint32), ref[:, 3].view(np.uint32)
+    assert (a != MISS).sum() > 1000          # the icosphere mesh (the box walls are analytic)
+    bad = a != b
+    in_plane = (r[:, 0] == 0.0) & (r[:, 4] == 0.0)
+    assert not (bad & ~in_plane).any(), f"{(bad & ~in_plane).sum()} mismatches off the symmetry plane"
+    u, v = ref[:, 1], ref[:, 2]
+    ref_on_edge = (b != MISS) & (np.minimum(np.minimum(u, v), 1.0 - u - v) < 1e-6)
+    assert (ref_on_edge | ~bad).all()
+    assert bad.mean() < 1e-3
+    same = ~bad & (a != MISS)
+    np.testing.assert_allclose(mine[same, 0], ref[same, 0], rtol=1e-6)
+
+
 def test_watertight_ids_vs_reference_traversal(setup):
     scene, ds, _, rays = setup
     mine = _trace(ds, rays, pt.TRIS_WATERTIGHT)
