@@ -1,4 +1,4 @@
-// CWBVH builder: binned-SAH binary BVH -> 8-wide collapse -> 8-bit
+// CWBVH builder: binned-SAH binary BVH -> cost-optimal 8-wide collapse -> 8-bit
 // quantisation, emitted in the compressed-wide-BVH node layout that the
 // reference traversal decodes (traverse_cwbvh.cuh:77-181; Ylitie, Karras,
 // Laine 2017, "Efficient Incoherent Ray Traversal on GPUs Through Compressed
@@ -63,6 +63,18 @@ struct Node2 {
 constexpr int kBins = 32;
 constexpr int kMaxLeaf = 3;   // the 3-bit unary meta count limits a leaf to 3 triangles
 constexpr double kCostTrav = 1.0, kCostTri = 1.0;
+// Wide-node collapse costs: one 8-wide node decode against one triangle test
+// (about 200 against 60 instructions in the traversal kernels).
+constexpr double kCostWideNode = 1.0, kCostWideTri = 0.3;
+
+// Collapse plan of one binary node: for a budget of i = 1..8 slots of the
+// wide parent, the least cost of its subtree and how it is reached.
+struct Plan {
+    double cost[8];
+    uint8_t how[8];     // kLeaf / kInternal (i = 1), kSame (as with i - 1 slots), or kSplit + k
+    uint8_t split8;     // as a wide node of its own: slots given to the left child
+};
+constexpr uint8_t kLeaf = 0, kInternal = 1, kSame = 2, kSplit = 16;
 
 class Builder {
 public:
@@ -85,6 +97,9 @@ private:
     std::vector<float> out_nodes_;
     std::vector<uint32_t> out_tri_order_;
     uint32_t max_depth_ = 0;
+    std::vector<Plan> plan_;
+    void plan_collapse();
+    void gather_slots(int node2, int budget, std::vector<Child>& kids) const;
     void collapse(int node2, std::vector<Child>& kids);
     void gather_tris(int node2, std::vector<uint32_t>& dst);
 };
@@ -168,37 +183,65 @@ int Builder::build2(int first, int count, int depth) {
     return idx;
 }
 
-// Gather up to 8 children for the wide node that replaces binary node `node2`:
-// repeatedly open the interior child with the largest surface area.  A child
-// whose subtree has <= 3 triangles becomes a leaf slot.
+// Cost-optimal collapse of the binary tree into 8-wide nodes (Ylitie,
+// Karras, Laine 2017, section 3.1).  With A(n) the surface area of binary node
+// n and p(n) its triangle count, the cost of n's subtree given at most i
+// slots of the wide parent is
+//   C(n, 1) = min(leaf: A(n) p(n) c_tri if p(n) <= 3, wide node: A(n) c_node + D(n, 8))
+//   C(n, i) = min(C(n, i - 1), D(n, i))                        for i = 2..8
+//   D(n, j) = min over k = 1..j-1 of C(left, k) + C(right, j - k)
+// computed children first (a child's index is always above its parent's).
+void Builder::plan_collapse() {
+    const double inf = std::numeric_limits<double>::infinity();
+    plan_.assign(nodes2_.size(), Plan{});
+    for (int n = (int)nodes2_.size() - 1; n >= 0; --n) {
+        const Node2& m = nodes2_[n];
+        Plan& P = plan_[n];
+        const double area = m.box.area();
+        const double leaf = m.tris_below <= kMaxLeaf ? area * (double)m.tris_below * kCostWideTri : inf;
+        double dist[9];
+        uint8_t split[9] = {0};
+        for (int j = 0; j <= 8; ++j) dist[j] = inf;
+        if (m.count == 0) {
+            const Plan& L = plan_[m.left];
+            const Plan& R = plan_[m.right];
+            for (int j = 2; j <= 8; ++j)
+                for (int k = 1; k < j; ++k) {
+                    const double c = L.cost[k - 1] + R.cost[j - k - 1];
+                    if (c < dist[j]) { dist[j] = c; split[j] = (uint8_t)k; }
+                }
+        }
+        const double internal = dist[8] + area * kCostWideNode;
+        P.split8 = split[8];
+        if (leaf <= internal) { P.cost[0] = leaf; P.how[0] = kLeaf; }
+        else { P.cost[0] = internal; P.how[0] = kInternal; }
+        for (int i = 2; i <= 8; ++i) {
+            if (dist[i] < P.cost[i - 2]) { P.cost[i - 1] = dist[i]; P.how[i - 1] = (uint8_t)(kSplit + split[i]); }
+            else { P.cost[i - 1] = P.cost[i - 2]; P.how[i - 1] = kSame; }
+        }
+    }
+}
+
+// The slots that binary node `node2` fills with a budget of `budget` slots.
+void Builder::gather_slots(int node2, int budget, std::vector<Child>& kids) const {
+    const Plan& P = plan_[node2];
+    while (budget > 1 && P.how[budget - 1] == kSame) --budget;
+    const uint8_t h = P.how[budget - 1];
+    if (h == kLeaf) { kids.push_back({node2, true}); return; }
+    if (h == kInternal) { kids.push_back({node2, false}); return; }
+    const int k = h - kSplit;
+    gather_slots(nodes2_[node2].left, k, kids);
+    gather_slots(nodes2_[node2].right, budget - k, kids);
+}
+
+// The children (2..8) of the wide node that replaces binary node `node2`.
 void Builder::collapse(int node2, std::vector<Child>& kids) {
     kids.clear();
     const Node2& n = nodes2_[node2];
     if (n.count > 0) { kids.push_back({node2, true}); return; }
-    auto classify = [&](int c) -> Child {
-        const Node2& m = nodes2_[c];
-        return {c, m.count > 0 || m.tris_below <= kMaxLeaf};
-    };
-    kids.push_back(classify(n.left));
-    kids.push_back(classify(n.right));
-    while (kids.size() < 8) {
-        // Open interior children that would otherwise need a wide node of
-        // their own first; with slots to spare, split small leaves too.
-        int best = -1; double best_area = -1.0;
-        for (int pass = 0; pass < 2 && best < 0; ++pass) {
-            for (size_t i = 0; i < kids.size(); ++i) {
-                const Node2& m = nodes2_[kids[i].node2];
-                if (m.count > 0) continue;   // binary leaf: cannot open
-                if (kids[i].leaf != (pass == 1)) continue;
-                double a = m.box.area();
-                if (a > best_area) { best_area = a; best = (int)i; }
-            }
-        }
-        if (best < 0) break;
-        int c = kids[best].node2;
-        kids[best] = classify(nodes2_[c].left);
-        kids.push_back(classify(nodes2_[c].right));
-    }
+    const int k = plan_[node2].split8;
+    gather_slots(n.left, k, kids);
+    gather_slots(n.right, 8 - k, kids);
 }
 
 void Builder::gather_tris(int node2, std::vector<uint32_t>& dst) {
@@ -227,6 +270,7 @@ bool Builder::build(TfgCWBVHHost* out) {
     }
     nodes2_.reserve(2 * (size_t)n_);
     int root2 = build2(0, (int)n_, 0);
+    plan_collapse();
 
     // Breadth-first emission: node i's inner children get consecutive indices.
     struct Pending { int node2; uint32_t index; uint32_t depth; };
