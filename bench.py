@@ -34,7 +34,7 @@ WORKLOAD = "plain path tracing, 1920x1080, 64 spp, depth 8, RR from depth 3, 16 
 # DRAM bytes (read + write) per closest-hit launch, measured with ncu on
 # `bench.py --profile-pass --wavefront-samples K`, by K = image samples per
 # wavefront (profiles/k_trace_k_shadow_dram_1080p.md).
-TRACE_DRAM_BYTES_PER_LAUNCH = {1: 41_169_312, 16: 533_807_328}
+TRACE_DRAM_BYTES_PER_LAUNCH = {1: 38_063_296, 16: 505_144_128}
 
 
 def trace_traffic(wavefront_paths: int, n_px: int):
