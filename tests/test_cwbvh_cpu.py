@@ -60,6 +60,28 @@ def test_tree_covers_every_triangle_once(subdiv):
     assert (hb.tris_ref[:, 15].view(np.uint32) == hb.tris_wt[:, 3].view(np.uint32)).all()
 
 
+@pytest.mark.parametrize("n", [2, 3, 4, 5, 7, 9, 10, 24, 25, 64])
+def test_small_and_coincident_triangle_sets(n):
+    # the 8-wide collapse on tiny trees (leaves of up to 3 triangles, nodes of
+    # 2..8 slots) and on triangles that all share one centroid (split by index)
+    from oracle import oracle as orc
+    rng = np.random.default_rng(n)
+    c = rng.uniform(-1.0, 1.0, (n, 1, 3))
+    v = (c + rng.uniform(-0.3, 0.3, (n, 3, 3))).astype(np.float32)
+    same = np.repeat(rng.uniform(-0.3, 0.3, (1, 3, 3)), n, axis=0)
+    same[:, 0] += np.linspace(-1e-3, 1e-3, n)[:, None]
+    same[:, 1] -= np.linspace(-1e-3, 1e-3, n)[:, None]           # the centroids stay equal
+    for verts in (v, same.astype(np.float32)):
+        hb = hbvh.build_host(verts.reshape(-1, 9))
+        n_nodes, refs = _decode(hb)
+        assert n_nodes == hb.num_nodes and sorted(refs) == list(range(n))
+        rays = _random_rays(rng, 3000, -1.5, 1.5)
+        got, _ = orc.trace_batch(hb.nodes, hb.tris_ref, rays)
+        want = orc.brute_batch(hb.tris_ref, rays)
+        a, b = got[:, 3].view(np.uint32), want[:, 3].view(np.uint32)
+        assert (a == b).all()
+
+
 @pytest.mark.parametrize("subdiv,n_rays", [(2, 4000), (4, 6000)])
 def test_traversal_matches_brute_force(subdiv, n_rays):
     from oracle import oracle as orc
