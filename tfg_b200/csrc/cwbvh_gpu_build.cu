@@ -43,6 +43,19 @@ struct Box6 {
     float lo[3], hi[3];
 };
 
+// Collapse plan of a binary node, as in the host builder (cwbvh_build.cpp):
+// for a budget of i = 1..8 slots of the wide parent, the least SAH cost of
+// the node's subtree and how it is reached (leaf of <= 3 triangles, a wide
+// node of its own, as with one slot less, or split with k slots to the left).
+struct Plan2 {
+    float cost[8];
+    uint8_t how[8];
+    uint8_t split8;       // as a wide node: slots given to the left child
+    uint8_t pad[7];
+};
+constexpr uint8_t kLeaf = 0, kInternal = 1, kSame = 2, kSplit = 16;
+constexpr float kCostWideNode = 1.0f, kCostWideTri = 0.3f;
+
 __device__ __forceinline__ float box_area(const Box6& b) {
     const float dx = fmaxf(b.hi[0] - b.lo[0], 0.0f), dy = fmaxf(b.hi[1] - b.lo[1], 0.0f),
                 dz = fmaxf(b.hi[2] - b.lo[2], 0.0f);
@@ -171,13 +184,41 @@ __global__ void k_radix_tree(const uint32_t* __restrict__ code, int n, int* __re
 
 // Boxes and triangle counts bottom-up.  A thread stops at the first node whose
 // other child is not finished yet; the second thread to arrive continues.
+// The plan of binary node p from its area, triangle count and its children's
+// plans (C(n, 1) = min(leaf, wide node); C(n, i) = min(C(n, i - 1), D(n, i));
+// D(n, j) = min over k of C(left, k) + C(right, j - k)).
+__device__ void plan_node(Plan2& P, float area, int count, const Plan2* L, const Plan2* R) {
+    float dist[9];
+    uint8_t split[9];
+    for (int j = 0; j <= 8; ++j) { dist[j] = INFINITY; split[j] = 0; }
+    if (L && R) {
+        float lc[8], rc[8];
+        for (int k = 0; k < 8; ++k) { lc[k] = __ldcg(&L->cost[k]); rc[k] = __ldcg(&R->cost[k]); }
+        for (int j = 2; j <= 8; ++j)
+            for (int k = 1; k < j; ++k) {
+                const float c = lc[k - 1] + rc[j - k - 1];
+                if (c < dist[j]) { dist[j] = c; split[j] = (uint8_t)k; }
+            }
+    }
+    const float leaf = count <= kMaxLeaf ? area * (float)count * kCostWideTri : INFINITY;
+    const float internal = dist[8] + area * kCostWideNode;
+    P.split8 = split[8];
+    if (leaf <= internal) { P.cost[0] = leaf; P.how[0] = kLeaf; }
+    else { P.cost[0] = internal; P.how[0] = kInternal; }
+    for (int i = 2; i <= 8; ++i) {
+        if (dist[i] < P.cost[i - 2]) { P.cost[i - 1] = dist[i]; P.how[i - 1] = (uint8_t)(kSplit + split[i]); }
+        else { P.cost[i - 1] = P.cost[i - 2]; P.how[i - 1] = kSame; }
+    }
+}
+
 __global__ void k_refit(const Box6* __restrict__ tbox, const uint32_t* __restrict__ sorted, int n,
                         const int* __restrict__ child, const int* __restrict__ parent, Box6* box, int* count,
-                        uint32_t* arrivals) {
+                        Plan2* plan, uint32_t* arrivals) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         int node = n - 1 + i;
         box[node] = tbox[sorted[i]];
         count[node] = 1;
+        plan_node(plan[node], box_area(tbox[sorted[i]]), 1, nullptr, nullptr);
         __threadfence();
         while (node != 0) {
             const int p = parent[node];
@@ -192,7 +233,9 @@ __global__ void k_refit(const Box6* __restrict__ tbox, const uint32_t* __restric
                 r.hi[k] = fmaxf(ba.hi[k], bb.hi[k]);
             }
             box[p] = r;
-            count[p] = __ldcg(&count[a]) + __ldcg(&count[b]);
+            const int cnt = __ldcg(&count[a]) + __ldcg(&count[b]);
+            count[p] = cnt;
+            plan_node(plan[p], box_area(r), cnt, &plan[a], &plan[b]);
             __threadfence();
             node = p;
         }
@@ -203,6 +246,7 @@ struct WideArgs {
     const int* child;
     const Box6* box;
     const int* count;
+    const Plan2* plan;
     const uint32_t* sorted;   // sorted position -> compacted triangle index
     int n;                    // triangles
     const int2* q_in;         // (binary node, wide index)
@@ -232,8 +276,9 @@ __device__ int gather_leaf_tris(const WideArgs& a, int node, uint32_t* out) {
     return cnt;
 }
 
-// One wide node per thread: the host builder's collapse, slot assignment and
-// quantisation (cwbvh_build.cpp) on this level's queue.
+// One wide node per thread: the host builder's cost-optimal collapse (read
+// from the plans), slot assignment and quantisation (cwbvh_build.cpp) on this
+// level's queue.
 __global__ void k_wide_level(WideArgs a) {
     const uint32_t qi = blockIdx.x * blockDim.x + threadIdx.x;
     if (qi >= a.q_n) return;
@@ -242,27 +287,29 @@ __global__ void k_wide_level(WideArgs a) {
     int kid[8];
     bool leaf[8];
     int nk = 0;
-    auto classify = [&](int c) { return is_leaf2(c, a.n) || a.count[c] <= kMaxLeaf; };
     if (is_leaf2(node2, a.n)) {
         kid[0] = node2; leaf[0] = true; nk = 1;
     } else {
-        kid[0] = a.child[2 * node2]; leaf[0] = classify(kid[0]);
-        kid[1] = a.child[2 * node2 + 1]; leaf[1] = classify(kid[1]);
-        nk = 2;
-        while (nk < 8) {
-            int best = -1;
-            float best_area = -1.0f;
-            for (int pass = 0; pass < 2 && best < 0; ++pass)
-                for (int i = 0; i < nk; ++i) {
-                    if (is_leaf2(kid[i], a.n) || leaf[i] != (pass == 1)) continue;
-                    const float ar = box_area(a.box[kid[i]]);
-                    if (ar > best_area) { best_area = ar; best = i; }
-                }
-            if (best < 0) break;
-            const int c = kid[best];
-            kid[best] = a.child[2 * c]; leaf[best] = classify(kid[best]);
-            kid[nk] = a.child[2 * c + 1]; leaf[nk] = classify(kid[nk]);
-            ++nk;
+        // (binary node, slot budget) pairs, the left child on top; a split
+        // pushes two entries and pops one, and the budgets sum to 8, so the
+        // stack never holds more than 8
+        int sn[8], sb[8], sp = 0;
+        const int k8 = a.plan[node2].split8;
+        sn[sp] = a.child[2 * node2 + 1]; sb[sp++] = 8 - k8;
+        sn[sp] = a.child[2 * node2]; sb[sp++] = k8;
+        while (sp > 0 && nk < 8) {
+            const int m = sn[--sp];
+            int b = sb[sp];
+            const Plan2& P = a.plan[m];
+            while (b > 1 && P.how[b - 1] == kSame) --b;
+            const uint8_t h = P.how[b - 1];
+            if (h == kLeaf || h == kInternal) {
+                kid[nk] = m; leaf[nk] = h == kLeaf; ++nk;
+            } else if (sp + 2 <= 8) {
+                const int k = h - kSplit;
+                sn[sp] = a.child[2 * m + 1]; sb[sp++] = b - k;
+                sn[sp] = a.child[2 * m]; sb[sp++] = k;
+            }
         }
     }
     const Box6 pb = a.box[node2];
@@ -476,6 +523,7 @@ extern "C" int tfgTinyBVHConstruirGPU(const TfgPrimitiva* d_prims, int32_t n, Tf
     int* parent = sc.get<int>(nn);
     Box6* box = sc.get<Box6>(nn);
     int* count = sc.get<int>(nn);
+    Plan2* plan = sc.get<Plan2>(nn);
     uint32_t* arrivals = sc.get<uint32_t>(nt);
     int2* q[2] = {sc.get<int2>(nt + 1), sc.get<int2>(nt + 1)};
     uint32_t* ctr = sc.get<uint32_t>(3);   // next_node, next_tri, queue length
@@ -502,7 +550,7 @@ extern "C" int tfgTinyBVHConstruirGPU(const TfgPrimitiva* d_prims, int32_t n, Tf
         e = cudaMemsetAsync(arrivals, 0, (size_t)nt * sizeof(uint32_t), s);
         if (e != cudaSuccess) return bail(e);
     }
-    k_refit<<<tb, 256, 0, s>>>(tbox, idx_s, (int)nt, child, parent, box, count, arrivals);
+    k_refit<<<tb, 256, 0, s>>>(tbox, idx_s, (int)nt, child, parent, box, count, plan, arrivals);
     // Level-by-level collapse; the root is binary node 0 (or the single leaf).
     const int2 r0 = make_int2(0, 0);   // binary node 0: the root (with one triangle, its leaf)
     const uint32_t init_ctr[3] = {1u, 0u, 0u};
@@ -517,7 +565,7 @@ extern "C" int tfgTinyBVHConstruirGPU(const TfgPrimitiva* d_prims, int32_t n, Tf
             return fail(TFG_E_BUILD, "tfgTinyBVHConstruirGPU: tree deeper than 64 levels");
         }
         WideArgs wa;
-        wa.child = child; wa.box = box; wa.count = count; wa.sorted = idx_s; wa.n = (int)nt;
+        wa.child = child; wa.box = box; wa.count = count; wa.plan = plan; wa.sorted = idx_s; wa.n = (int)nt;
         wa.q_in = q[(depth - 1) & 1]; wa.q_n = qn; wa.q_out = q[depth & 1]; wa.q_out_n = ctr + 2;
         wa.next_node = ctr; wa.next_tri = ctr + 1; wa.nodes = nodes; wa.tri_order = tri_order;
         e = cudaMemsetAsync(ctr + 2, 0, 4, s);
