@@ -62,6 +62,11 @@ def test_entry_points_reject_bad_arguments(built):
                   None, None, None, 0, None, None, 0, 0, None)
     with pytest.raises(_lib.TfgError):
         _lib.call("tfgLaunchKernelComposite", None, None, None, 4, 4, None)
+    # one-blob bins: a negative count is refused, an empty call does nothing
+    with pytest.raises(_lib.TfgError) as e:
+        _lib.call("tfgOneBlobBins", None, None, -1, None)
+    assert e.value.code == 10001
+    _lib.call("tfgOneBlobBins", None, None, 0, None)
 
 
 def test_cwbvh_build_rejects_empty(built):
