@@ -358,7 +358,8 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
     encoding = {"frequency_12_bands": depth[5],
                 "hashgrid_reference": {**variant(encoding=HASHGRID), "config": hashgrid_reference(),
                                        "one_blob_bins": 4}}
-    width = {"5x64": depth[5], "5x128": variant(width=128), "3x128": variant(hidden_layers=3, width=128)}
+    width = {"5x64": depth[5], "5x128": variant(width=128), "3x128": variant(hidden_layers=3, width=128),
+             "7x128": variant(hidden_layers=7, width=128)}
     return {
         "frames": 48 + frames, "warmup_frames": 48, "camera": "orbit 1 deg/frame", "train_samples_per_frame": 4 * 16384,
         "ms_per_frame_nrc": round(t_nrc, 3), "ms_per_pass_plain_1spp": round(t_pt, 3),

@@ -1,8 +1,8 @@
-"""The cache network with 128 units per hidden layer (3 or 5 hidden layers)
-against the FP64 oracle: inference in FP16 and BF16, the gradients of the
-layers (and of the hash-grid tables with the composite encoding), online
-training, and a whole cache frame.  FP8 is built for width 64 only and must
-be refused."""
+"""The cache network with 128 units per hidden layer (3, 5 or 7 hidden
+layers; 7 streams its weights through shared memory) against the FP64
+oracle: inference in FP16 and BF16, the gradients of the layers (and of the
+hash-grid tables with the composite encoding), online training, and whole
+cache frames.  FP8 is built for width 64 only and must be refused."""
 import numpy as np
 import pytest
 import torch
@@ -46,7 +46,7 @@ def _f16(w):
     return np.asarray(w, np.float32).astype(np.float16).astype(np.float64)
 
 
-@pytest.mark.parametrize("hidden", [5, 3])
+@pytest.mark.parametrize("hidden", [5, 3, 7])
 def test_inference_matches_fp64_model(built, hidden):
     m = ColorMLP(batch=4096, seed=31 + hidden, hidden_layers=hidden, width=128)
     m.set_bounds(LO, HI)
@@ -80,8 +80,9 @@ def test_inference_matches_fp64_model(built, hidden):
     m.close()
 
 
-def test_gradient_matches_fp64_model(built):
-    m = ColorMLP(batch=4096, seed=7, width=128)
+@pytest.mark.parametrize("hidden", [5, 7])
+def test_gradient_matches_fp64_model(built, hidden):
+    m = ColorMLP(batch=4096, seed=7, width=128, hidden_layers=hidden)
     m.set_bounds(LO, HI)
     rng = np.random.default_rng(11)
     n_avail = 20000
@@ -146,11 +147,12 @@ def test_online_training_learns_a_signal(built):
     m.close()
 
 
-def test_cache_frames_with_width_128(built):
+@pytest.mark.parametrize("hidden,encoding", [(5, "frequency"), (7, "frequency"), (7, "hashgrid")])
+def test_cache_frames_with_width_128(built, hidden, encoding):
     s = scenes.sized_terrain_scene(20000, 160, 96, 2, seed=45)
     ds = pt.DeviceScene(s, "cuda")
     params = pt.RenderParams(max_depth=6, rr_min_depth=3, shadow_mesh=1, tri_format=pt.TRIS_WATERTIGHT)
-    m = ColorMLP(batch=16384, seed=5, width=128)
+    m = ColorMLP(batch=16384, seed=5, width=128, hidden_layers=hidden, encoding=encoding)
     m.set_bounds(*s.bounds)
     r = NrcRenderer(ds, m, params, train_steps=2, max_records=8192, min_records=256, use_graph=True)
     for f in range(8):
@@ -165,8 +167,37 @@ def test_cache_frames_with_width_128(built):
     ds.close()
 
 
-def test_width_128_limits(built):
-    with pytest.raises(TfgError):
-        ColorMLP(batch=4096, hidden_layers=7, width=128)
+def test_width_limits(built):
     with pytest.raises(TfgError):
         ColorMLP(batch=4096, width=96)
+    with pytest.raises(TfgError):
+        ColorMLP(batch=4096, hidden_layers=4, width=128)
+    m = ColorMLP(batch=4096, hidden_layers=7, width=128)
+    assert m.n_params == 96 * 128 + 6 * 128 * 128 + 16 * 128
+    with pytest.raises(TfgError):
+        m.set_precision(FP8)
+    m.close()
+
+
+def test_seven_layer_hash_grid_inference_matches_fp64_model(built):
+    # the streamed kernel with the composite encoding (FP16 table image)
+    m = ColorMLP(batch=4096, seed=33, width=128, hidden_layers=7, encoding=HASHGRID, hashgrid=SMALL)
+    m.set_bounds(LO, HI)
+    rng = np.random.default_rng(9)
+    m.set_table(rng.uniform(-0.5, 0.5, m.n_table).astype(np.float32))
+    n = 1500
+    d = _datos(rng, n)
+    out = torch.zeros(n * 3, device="cuda")
+    m.inference(_dev(d), out, n)
+    torch.cuda.synchronize()
+    got = out.view(n, 3).cpu().numpy()
+    W = [_f16(w) for w in split_layers(m.get_params(WEIGHTS))]
+    tab = m.get_table(WEIGHTS).astype(np.float16).astype(np.float64)
+    from tfg_b200.nrc import hashgrid_reference
+    x, _ = mo.composite_encode(mo.rows15(d, LO, HI), tab, {**hashgrid_reference(), **SMALL})
+    raw = mo.forward(W, x)[0]
+    scale = np.abs(raw).mean() + 1e-3
+    err = np.abs(got - mo.scrub(raw)) / scale
+    assert np.isfinite(got).all()
+    assert err.max() < 0.05 and err.mean() < 0.01, (err.max(), err.mean())
+    m.close()

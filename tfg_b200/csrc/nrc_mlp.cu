@@ -562,6 +562,50 @@ __device__ __forceinline__ uint32_t pack2(float a, float b) {
     return PREC == kPrecBF16 ? pack_bf2(a, b) : pack_h2(a, b);
 }
 
+// Packed words of the composite encoding: the hash-grid pairs (FP16 from
+// the interpolation, or re-rounded to BF16), then the one-blob / albedo tail.
+template <int PREC>
+__device__ __forceinline__ void composite_words(const __half2 (&hw)[kHashMaxLevels], const float (&t)[32],
+                                                uint32_t (&w)[48]) {
+#pragma unroll
+    for (int k = 0; k < kHashMaxLevels; ++k) {
+        if constexpr (PREC == kPrecBF16) {
+            const float2 v = __half22float2(hw[k]);
+            w[k] = pack_bf2(v.x, v.y);
+        } else {
+            w[k] = *reinterpret_cast<const uint32_t*>(&hw[k]);
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 16; ++k) w[16 + k] = pack2<PREC>(t[2 * k], t[2 * k + 1]);
+#pragma unroll
+    for (int k = 32; k < 48; ++k) w[k] = 0u;
+}
+
+// Packed words of the frequency encoding of the unit position p and the 13
+// other inputs (direction, normal, albedos, the constant 1).
+template <int PREC>
+__device__ __forceinline__ void frequency_words(const float (&p)[3], const float (&misc)[13], uint32_t (&w)[48]) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        float s, c;
+        __sincosf(kPiF * p[j], &s, &c);
+#pragma unroll
+        for (int k = 0; k < kBands; ++k) {
+            w[12 * j + k] = pack2<PREC>(s, c);
+            const float s2 = 2.0f * s * c;
+            const float c2 = (c - s) * (c + s);
+            s = s2;
+            c = c2;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < 6; ++k) w[36 + k] = pack2<PREC>(misc[2 * k], misc[2 * k + 1]);
+    w[42] = pack2<PREC>(1.0f, 0.0f);
+#pragma unroll
+    for (int k = 43; k < 48; ++k) w[k] = 0u;
+}
+
 // Encoded features of one staged row as 96 floats' worth of packed words:
 // features 0..71 are (sin, cos)(2^k pi p) of the x, y, z bands (double-angle
 // recurrence from a hardware sin/cos of the base band), 72..84 direction,
@@ -607,15 +651,7 @@ __device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Boun
             umma::tmem_st8(ta + 16u, w + 16);
         } else {
             uint32_t w[48];
-#pragma unroll
-            for (int k = 0; k < kHashMaxLevels; ++k) {
-                if constexpr (PREC == kPrecBF16) w[k] = pack_bf2(x[2 * k], x[2 * k + 1]);
-                else w[k] = *reinterpret_cast<const uint32_t*>(&hw[k]);
-            }
-#pragma unroll
-            for (int k = 0; k < 16; ++k) w[16 + k] = pack2<PREC>(t[2 * k], t[2 * k + 1]);
-#pragma unroll
-            for (int k = 32; k < 48; ++k) w[k] = 0u;
+            composite_words<PREC>(hw, t, w);
 #pragma unroll
             for (int c = 0; c < 3; ++c)
                 umma::tmem_st16(ta + 16u * c, *reinterpret_cast<const uint32_t(*)[16]>(w + 16 * c));
@@ -656,28 +692,33 @@ __device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Boun
         umma::tmem_st8(ta + 16u, w + 16);
     } else {
         uint32_t w[48];
-#pragma unroll
-        for (int j = 0; j < 3; ++j) {
-            float s, c;
-            __sincosf(kPiF * p[j], &s, &c);
-#pragma unroll
-            for (int k = 0; k < kBands; ++k) {
-                w[12 * j + k] = pack2<PREC>(s, c);
-                const float s2 = 2.0f * s * c;
-                const float c2 = (c - s) * (c + s);
-                s = s2;
-                c = c2;
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < 6; ++k) w[36 + k] = pack2<PREC>(misc[2 * k], misc[2 * k + 1]);
-        w[42] = pack2<PREC>(1.0f, 0.0f);
-#pragma unroll
-        for (int k = 43; k < 48; ++k) w[k] = 0u;
+        frequency_words<PREC>(p, misc, w);
 #pragma unroll
         for (int c = 0; c < 3; ++c) umma::tmem_st16(ta + 16u * c, *reinterpret_cast<const uint32_t(*)[16]>(w + 16 * c));
     }
     return amax;
+    }
+}
+
+// The 48 packed FP16 / BF16 words of one query row (both encodings), for
+// kernels whose layer-0 operand lives in shared memory.
+template <int PREC, bool HASH>
+__device__ __forceinline__ void encode_words(const TfgDatosMLP& d, const Bounds& b, const HashGrid& g,
+                                             uint32_t (&w)[48]) {
+    float p[3];
+    unit_position(d, b, p);
+    if constexpr (HASH) {
+        __half2 hw[kHashMaxLevels];
+        hash_words_f16(p, g, hw);
+        float t[32];
+        composite_tail(d, t);
+        composite_words<PREC>(hw, t, w);
+    } else {
+        const float misc[13] = {(float)d.direccion.x, (float)d.direccion.y, (float)d.direccion.z,
+                                (float)d.normal.x,    (float)d.normal.y,    (float)d.normal.z,
+                                d.difuso.r,           d.difuso.g,           d.difuso.b,
+                                d.especular.r,        d.especular.g,        d.especular.b, 1.0f};
+        frequency_words<PREC>(p, misc, w);
     }
 }
 
@@ -1324,7 +1365,7 @@ __device__ __forceinline__ void store_T32(uint8_t* tile, int s, int f0, const fl
 
 template <int NL>
 __global__ void __launch_bounds__(128) k_train128(TrainArgs a) {
-    static_assert(NL == 4 || NL == 6, "width 128: 3 or 5 hidden layers");
+    static_assert(NL == 4 || NL == 6 || NL == 8, "width 128: 3, 5 or 7 hidden layers");
     constexpr int kItems = 2 * NL - 1;   // weight images per tile: NL forward, then NL - 1 backward
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
@@ -1481,6 +1522,136 @@ __global__ void __launch_bounds__(128) k_train128(TrainArgs a) {
     }
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xFFFFFFFFu, lsum, o);
     if ((t & 31) == 0) atomicAdd(a.loss, lsum);
+    if (!ok && warp == 0) {   // after a timeout: pending copies and issued MMAs finish first
+        if (umma::elect_one()) {
+            for (int b = 0; b < 2; ++b)
+                if (wpend[b]) umma::mbar_wait(&mb_w[b], wph[b], kSpinLimit);
+            umma::mma_commit(&mb_drain);
+            umma::mbar_wait(&mb_drain, 0, kSpinLimit);
+        }
+        __syncwarp();
+    }
+    if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, 256);
+}
+
+// ------------------------------------------------------------------ width-128 streamed inference
+// Inference for width-128 networks whose forward image does not fit in shared
+// memory (7 hidden layers: 233,472 B).  One 128-query tile per CTA at a time;
+// the NL layer images of each tile pass through two 32 KB buffers, each
+// bulk-copied as soon as the MMAs that read the buffer's previous image have
+// completed (one layer ahead), as in k_train128's forward pass; the
+// activations are the A operand in shared memory.  Same output rule as
+// k_infer / k_infer128 (NrcKernel.cu:99-126; RenderKernel.cu:49-66).
+template <int PREC, int NL, bool HASH>
+__global__ void __launch_bounds__(128) k_infer128s(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
+                                                   const uint32_t* __restrict__ n_dev, Bounds bounds, HashGrid hg,
+                                                   const uint8_t* __restrict__ wimg, TfgColor* __restrict__ out,
+                                                   TfgColor* __restrict__ img, const TfgColor* __restrict__ thr) {
+    static_assert(PREC != kPrecF8 && NL >= 2 && NL <= kMaxLayers, "width 128 streamed: FP16 / BF16");
+    constexpr bool kBF = PREC == kPrecBF16;
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sa = smem + kT128SmemA;
+    __shared__ uint64_t mb_w[2], mb_mma, mb_drain;
+    __shared__ uint32_t tslot;
+    const int t = threadIdx.x, warp = t >> 5;
+    const uint32_t n = n_dev ? min(*n_dev, n_max) : n_max;
+    const uint32_t ntiles = (n + kTile - 1) / kTile;
+    if (blockIdx.x >= ntiles) return;
+    const uint32_t total = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x * NL;   // images this CTA loads
+    if (warp == 0) umma::tmem_alloc(&tslot, 256);
+    if (t == 0) {
+        umma::mbar_init(&mb_w[0], 1);
+        umma::mbar_init(&mb_w[1], 1);
+        umma::mbar_init(&mb_mma, 1);
+        umma::mbar_init(&mb_drain, 1);
+        umma::mbar_fence_init();
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tslot;
+    const uint32_t tlane = (uint32_t)(32 * warp) << 16;
+    bool wpend[2] = {false, false};
+    auto load = [&](uint32_t g) {   // layer image g % NL into buffer g & 1
+        const int k = (int)(g % (uint32_t)NL), b = (int)(g & 1u);
+        wpend[b] = true;
+        if (t != 0) return;
+        const uint32_t bytes = k == NL - 1 ? 2 * 16 * 128 : 2 * 128 * 128;
+        umma::mbar_expect_tx(&mb_w[b], bytes);
+        umma::bulk_g2s(smem + b * kT128Buf, wimg + foff_h<128>(NL, k), bytes, &mb_w[b]);
+    };
+    load(0);
+    if (total > 1) load(1);
+    uint32_t wph[2] = {0, 0}, g = 0, mph = 0;
+    bool ok = true;
+    for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        const uint32_t row = tile * kTile + (uint32_t)t;
+        const bool valid = row < n;
+        {
+            // rows past the end encode the last row again; their outputs are never stored
+            uint32_t w[48];
+            encode_words<PREC, HASH>(in[valid ? row : n - 1], bounds, hg, w);
+            store_encoded(sa, t, w);
+        }
+        umma::fence_smem_to_async();
+        __syncthreads();
+        for (int l = 0; l < NL && ok; ++l) {
+            const bool last = l == NL - 1;
+            const int b = (int)(g & 1u);
+            ok = all_ok(umma::mbar_wait(&mb_w[b], wph[b], kSpinLimit));
+            if (!ok) break;   // the copy stays pending: the exit path waits for it
+            wph[b] ^= 1u;
+            wpend[b] = false;
+            umma::fence_after_sync();
+            if (warp == 0) {
+                if (umma::elect_one()) {
+                    issue_layer(tmem + (last ? 128u : 0u), sa, kTile * 128, smem + b * kT128Buf,
+                                rows_h<128>(NL, l) * 128, cols_h<128>(l), last ? kOutPad : 128, kBF);
+                    umma::mma_commit(&mb_mma);
+                }
+                __syncwarp();
+            }
+            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+            mph ^= 1u;
+            if (ok && g + 2 < total) load(g + 2);
+            ++g;
+            umma::fence_after_sync();
+            if (!ok) break;
+            if (!last) {
+#pragma unroll
+                for (int h = 0; h < 4; ++h) {
+                    float v[32];
+                    umma::tmem_ld32(tmem + tlane + 32u * h, v);
+#pragma unroll
+                    for (int i = 0; i < 32; ++i) v[i] = fmaxf(v[i], 0.0f);
+                    store_row32<kBF>(sa, t, 32 * h, v);
+                }
+            } else {
+                float v[16];
+                umma::tmem_ld16(tmem + tlane + 128u, v);
+                if (valid && (out || img)) {
+                    const float cr = scrub(v[0]), cg = scrub(v[1]), cb = scrub(v[2]);
+                    if (img) {
+                        const TfgColor th = thr[row];
+                        if (th.r > 0 || th.g > 0 || th.b > 0) {
+                            TfgColor f = img[row];
+                            f.r = f.r + th.r * cr;
+                            f.g = f.g + th.g * cg;
+                            f.b = f.b + th.b * cb;
+                            img[row] = f;
+                        }
+                    } else {
+                        out[row] = TfgColor{cr, cg, cb};
+                    }
+                }
+            }
+            umma::fence_before_sync();
+            umma::fence_smem_to_async();
+            __syncthreads();
+        }
+    }
     if (!ok && warp == 0) {   // after a timeout: pending copies and issued MMAs finish first
         if (umma::elect_one()) {
             for (int b = 0; b < 2; ++b)
@@ -1943,12 +2114,12 @@ int with_model(const ColorMlp* n, F&& f) {
 }
 
 // Calls f(integral_constant<int, NL>, integral_constant<int, HID>) for the
-// model's layer count and width (width 128 only with 3 or 5 hidden layers).
+// model's layer count and width (width 128 with 3, 5 or 7 hidden layers).
 template <typename F>
 int with_width(const ColorMlp* n, F&& f) {
     return with_layers(n->nl, [&](auto c) {
         constexpr int NL = decltype(c)::value;
-        if constexpr (NL == 4 || NL == 6) {
+        if constexpr (NL == 4 || NL == 6 || NL == 8) {
             if (n->hid == 128) return f(c, std::integral_constant<int, 128>{});
         }
         return f(c, std::integral_constant<int, 64>{});
@@ -2125,6 +2296,16 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
                         in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
                 else
                     mlp::k_infer128<mlp::kPrecBF16, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
+            } else if constexpr (NL == 8) {
+                // streamed weights: one tile per CTA at a time, two CTAs per SM
+                const size_t sm = mlp::kT128Smem + 1024;
+                const uint32_t grid_s = std::max<uint32_t>(1u, std::min<uint32_t>(tiles, 2u * cap));
+                if (n->prec == mlp::kPrecF16)
+                    mlp::k_infer128s<mlp::kPrecF16, NL, HASH><<<grid_s, 128, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
+                else
+                    mlp::k_infer128s<mlp::kPrecBF16, NL, HASH><<<grid_s, 128, sm, s>>>(
                         in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
             }
             return 0;
@@ -2325,6 +2506,15 @@ void set_kernel_attrs() {
         cudaFuncSetAttribute(M::k_train128<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kT128Smem + 1024);
         cudaFuncSetAttribute(M::k_wgrad<NL, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmemH<128> + 1024);
     }
+    if constexpr (NL == 8) {   // width 128 with 7 hidden layers: streamed weights
+        const int s128 = M::kT128Smem + 1024;
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecF16, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecBF16, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecF16, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecBF16, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_train128<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_wgrad<NL, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmemH<128> + 1024);
+    }
 }
 }  // namespace
 
@@ -2392,8 +2582,6 @@ int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, i
     if (hidden_layers != 3 && hidden_layers != 5 && hidden_layers != 7)
         return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: hidden_layers must be 3, 5 or 7");
     if (width != 64 && width != 128) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: width must be 64 or 128");
-    if (width == 128 && hidden_layers == 7)
-        return tfg::fail(TFG_E_UNSUPPORTED, "tfgMlpCreate: width 128 is built for 3 or 5 hidden layers");
     const int nl = hidden_layers + 1;
     if (n_in != 15 || n_out != 3) return tfg::fail(TFG_E_INVALID, "tfgMlpCreate: the cache takes 15 inputs and 3 outputs");
     if (batch == 0 || batch % M::kTile != 0 || batch > (1u << 24))
