@@ -97,7 +97,7 @@ constexpr int kFwdBytesMax = fwd_bytes_of(kMaxLayers);            // 67584
 constexpr int kWeightRegion = (kFwdBytesMax + 1023) / 1024 * 1024;  // 68608
 static_assert(fwd_bytes_of(6) == 51200 && bwd_bytes_of(6) == 40960 && params_of(6) == 23552, "default layout");
 
-// The same layouts for hidden width HID (64 or 128; 128 for 3 or 5 hidden
+// The same layouts for hidden width HID (64 or 128; 3, 5 or 7 hidden
 // layers): 96 -> HID, (nl - 2) x HID -> HID, HID -> 16.  Weight images keep
 // 64-feature (128-byte) SW128 K regions: layer 0 two regions of HID rows,
 // hidden layers HID/64 regions of HID rows, the last layer HID/64 regions of
@@ -926,7 +926,8 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
     if (warp == 0) umma::tmem_dealloc(tslot, 512);
 }
 
-// Width-128 inference (3 or 5 hidden layers; FP16 or BF16): the same
+// Width-128 inference (3 or 5 hidden layers, whose weights stay resident in
+// shared memory; 7 layers use k_infer128s; FP16 or BF16): the same
 // pipeline as k_infer with two 128-query slots per SM, each with 256 TMEM
 // columns (128 FP32 accumulator columns, then up to 64 columns of the next
 // layer's A operand), and the 164 KB weight image in shared memory.
@@ -2047,7 +2048,7 @@ struct ColorMlp {
     float* w = nullptr; float* m = nullptr; float* v = nullptr; float* ema = nullptr; float* grad = nullptr;
     uint8_t* fwd = nullptr; uint8_t* bwd = nullptr; uint8_t* inf = nullptr;
     int nl = 6;                  // layers (hidden layers + 1)
-    int hid = 64;                // hidden width (64, or 128 for 3 or 5 hidden layers)
+    int hid = 64;                // hidden width (64 or 128)
     uint8_t* hT[mlp::kMaxLayers] = {nullptr};
     uint8_t* zT[mlp::kMaxLayers] = {nullptr};
     float* loss = nullptr;
