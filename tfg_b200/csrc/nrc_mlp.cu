@@ -105,6 +105,9 @@ static_assert(fwd_bytes_of(6) == 51200 && bwd_bytes_of(6) == 40960 && params_of(
 // and HID/64 regions of K (one for the last layer's K = 16).
 template <int HID> __host__ __device__ constexpr int rows_h(int nl, int l) { return l == nl - 1 ? 16 : HID; }
 template <int HID> __host__ __device__ constexpr int cols_h(int l) { return l == 0 ? 96 : HID; }
+// FP8 images: one 128-byte K row per output (K <= 128 features of one byte).
+template <int HID> __host__ __device__ constexpr int f8_off_h(int l) { return l * HID * 128; }
+template <int HID> __host__ __device__ constexpr int f8_bytes_h(int nl) { return (nl - 1) * HID * 128 + 16 * 128; }
 template <int HID> __host__ __device__ constexpr int poff_h(int nl, int l) {
     return l == 0 ? 0 : (l <= nl - 1 ? 96 * HID + (l - 1) * HID * HID : 96 * HID + (nl - 2) * HID * HID + 16 * HID);
 }
@@ -120,6 +123,9 @@ template <int HID> __host__ __device__ constexpr int bwd_bytes_h(int nl) { retur
 static_assert(params_h<64>(6) == params_of(6) && fwd_bytes_h<64>(6) == fwd_bytes_of(6) &&
               bwd_bytes_h<64>(6) == bwd_bytes_of(6) && foff_h<64>(6, 5) == foff_of(6, 5) &&
               poff_h<64>(8, 7) == poff_of(8, 7) && boff_h<64>(6, 3) == 2 * 8192, "width 64 keeps its layout");
+static_assert(rows_h<64>(6, 2) == rows_of(6, 2) && rows_h<64>(6, 5) == rows_of(6, 5) && cols_h<64>(0) == cols_of(0) &&
+                  cols_h<64>(3) == cols_of(3) && f8_off_h<64>(3) == 3 * 8192 && f8_bytes_h<64>(6) == f8_bytes_of(6),
+              "width 64 keeps its FP8 layout");
 static_assert(params_h<128>(6) == 79872 && fwd_bytes_h<128>(6) == 167936 && bwd_bytes_h<128>(6) == 147456,
               "width 128 layout");
 // Runtime forms for the host.
@@ -937,13 +943,19 @@ constexpr int kInfer128Stage = fwd_bytes_h<128>(6);                       // 167
 constexpr int kInfer128Smem = kInfer128Stage + kSlots128 * kStageBytes;   // 196608
 static_assert(kInfer128Stage % 1024 == 0 && kInfer128Smem + 1024 <= 227 * 1024, "width-128 inference shared memory");
 
-template <int PREC, int NL, bool HASH>
+// FP8 (E4M3, kind::f8f6f4, four features per TMEM column) and amax tracking
+// follow k_infer: `f8` holds the per-layer input and weight scales, TRACK
+// folds each layer's input amax into amax[] (every tile with `amax_all`,
+// otherwise the first tile of each slot).
+template <int PREC, bool TRACK, int NL, bool HASH>
 __global__ void __launch_bounds__(kInfer128Threads, 1)
     k_infer128(const TfgDatosMLP* __restrict__ in, uint32_t n_max, const uint32_t* __restrict__ n_dev, Bounds bounds,
                HashGrid hg, const uint8_t* __restrict__ wimg, TfgColor* __restrict__ out, TfgColor* __restrict__ img,
-               const TfgColor* __restrict__ thr) {
-    static_assert(PREC != kPrecF8 && (NL == 4 || NL == 6), "width 128: FP16 / BF16, 3 or 5 hidden layers");
-    constexpr uint32_t kWBytes = fwd_bytes_h<128>(NL);
+               const TfgColor* __restrict__ thr, const float* __restrict__ f8, float* amax, int amax_all) {
+    static_assert(NL == 4 || NL == 6, "width 128 with resident weights: 3 or 5 hidden layers");
+    constexpr bool kF8 = PREC == kPrecF8;
+    constexpr uint32_t kWBytes = kF8 ? f8_bytes_h<128>(NL) : fwd_bytes_h<128>(NL);
+    static_assert(kWBytes <= kInfer128Stage, "weights fit before the staging buffers");
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
     uint8_t* sw = smem;
@@ -958,6 +970,12 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
     const uint32_t n = n_dev ? min(*n_dev, n_max) : n_max;
     const uint32_t ntiles = (n + kTile - 1) / kTile;
     if (blockIdx.x * kSlots128 >= ntiles) return;
+    float qs[NL], deq[NL];
+#pragma unroll
+    for (int l = 0; l < NL; ++l) {
+        qs[l] = kF8 ? f8[kF8Q + l] : 1.0f;
+        deq[l] = kF8 ? 1.0f / (f8[kF8Q + l] * f8[kF8WQ + l]) : 1.0f;
+    }
     if (warp == 0) umma::tmem_alloc(&tslot, 512);
     if (tid == 0) {
         umma::mbar_init(&mb_w, 1);
@@ -991,15 +1009,18 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
     bool ok = umma::mbar_wait(&mb_w, 0, kSpinLimit);
     ok = __syncthreads_and(ok ? 1 : 0) != 0;
     uint32_t mph = 0, iph = 0;
-    for (; tile < ntiles && ok; tile += tstride) {
+    bool first = true;
+    for (; tile < ntiles && ok; tile += tstride, first = false) {
         const uint32_t row = tile * kTile + (uint32_t)t;
         const bool valid = row < n;
+        const bool track = TRACK && (amax_all || first);
         ok = slot_all(bar, umma::mbar_wait(&mb_in[slot], iph, kSpinLimit));
         if (!ok) break;
         pending = false;
         iph ^= 1u;
-        encode_to_tmem<PREC, HASH>(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds, hg, 1.0f,
-                                   tmem_a + tlane);
+        const float a0 = encode_to_tmem<PREC, HASH>(reinterpret_cast<const TfgDatosMLP*>(stage + t * kRowBytes), bounds,
+                                                    hg, qs[0], tmem_a + tlane);
+        if (track) warp_amax(valid ? a0 : 0.0f, &amax[0]);
         umma::tmem_wait_st();
         umma::fence_before_sync();
         slot_sync(bar);
@@ -1018,11 +1039,19 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
                 constexpr uint32_t id_hid = umma::idesc_f16(kTile, 128, PREC == kPrecBF16);
                 constexpr uint32_t id_out = umma::idesc_f16(kTile, kOutPad, PREC == kPrecBF16);
                 if (umma::elect_one()) {
+                    if constexpr (kF8) {
+                        // K = 32 one-byte features per MMA: one 128-byte row holds a layer's K
 #pragma unroll
-                    for (int s = 0; s < cols_h<128>(l) / 16; ++s) {
-                        const uint64_t bd = wdesc + (uint64_t)((foff_h<128>(NL, l) + (s >> 2) * (rows_h<128>(NL, l) * 128) +
-                                                                (s & 3) * 32) >> 4);
-                        umma::mma_f16_ta(tmem, tmem_a + 8u * s, bd, last ? id_out : id_hid, s > 0);
+                        for (int s = 0; s < cols_h<128>(l) / 32; ++s)
+                            umma::mma_f8_ta(tmem, tmem_a + 8u * s, wdesc + (uint64_t)((f8_off_h<128>(l) + s * 32) >> 4),
+                                            last ? id_out : id_hid, s > 0);
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < cols_h<128>(l) / 16; ++s) {
+                            const uint64_t bd = wdesc + (uint64_t)((foff_h<128>(NL, l) + (s >> 2) * (rows_h<128>(NL, l) * 128) +
+                                                                    (s & 3) * 32) >> 4);
+                            umma::mma_f16_ta(tmem, tmem_a + 8u * s, bd, last ? id_out : id_hid, s > 0);
+                        }
                     }
                     umma::mma_commit(&mb_mma[slot]);
                 }
@@ -1033,16 +1062,37 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
             if (!ok) break;
             umma::fence_after_sync();
             if (!last) {
+                float lmax = 0.0f;
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
                     float v[32];
                     umma::tmem_ld32(tmem + tlane + 32u * h, v);
-                    uint32_t r[16];
+                    if constexpr (kF8) {
+                        // dequantise, ReLU, requantise for the next layer
+                        const float sc = deq[l] * qs[l + 1];
+                        uint32_t r[8];
 #pragma unroll
-                    for (int i = 0; i < 16; ++i)
-                        r[i] = PREC == kPrecBF16 ? relu_bf2(v[2 * i], v[2 * i + 1]) : relu_h2(v[2 * i], v[2 * i + 1]);
-                    umma::tmem_st16(tmem_a + tlane + 16u * h, r);
+                        for (int i = 0; i < 8; ++i)
+                            r[i] = pack_e4m3x4<true>(v[4 * i] * sc, v[4 * i + 1] * sc, v[4 * i + 2] * sc,
+                                                     v[4 * i + 3] * sc);
+                        umma::tmem_st8(tmem_a + tlane + 8u * h, r);
+                        if (track) {
+#pragma unroll
+                            for (int i = 0; i < 32; ++i) lmax = fmaxf(lmax, v[i] * deq[l]);
+                        }
+                    } else {
+                        uint32_t r[16];
+#pragma unroll
+                        for (int i = 0; i < 16; ++i)
+                            r[i] = PREC == kPrecBF16 ? relu_bf2(v[2 * i], v[2 * i + 1]) : relu_h2(v[2 * i], v[2 * i + 1]);
+                        umma::tmem_st16(tmem_a + tlane + 16u * h, r);
+                        if (track) {
+#pragma unroll
+                            for (int i = 0; i < 32; ++i) lmax = fmaxf(lmax, v[i]);
+                        }
+                    }
                 }
+                if (track) warp_amax(valid ? lmax : 0.0f, &amax[l + 1]);
                 umma::tmem_wait_st();
                 umma::fence_before_sync();
                 slot_sync(bar);
@@ -1050,7 +1100,7 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
                 float v[16];
                 umma::tmem_ld16(tmem + tlane, v);
                 if (valid && (out || img)) {
-                    const float cr = scrub(v[0]), cg = scrub(v[1]), cb = scrub(v[2]);
+                    const float cr = scrub(v[0] * deq[l]), cg = scrub(v[1] * deq[l]), cb = scrub(v[2] * deq[l]);
                     if (img) {
                         const TfgColor th = thr[row];
                         if (th.r > 0 || th.g > 0 || th.b > 0) {
@@ -1085,7 +1135,7 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
 // FP8 inference image from the debiased weight average, one block per
 // layer: the layer's weight scale wq = 448 / amax|W| goes to f8[kF8WQ + l].
 // Skipped when the image already holds the weights of this Adam step.
-template <int NL>
+template <int NL, int HID = 64>
 __global__ void __launch_bounds__(1024) k_pack_f8(const float* __restrict__ w, const float* __restrict__ ema,
                                                   const uint32_t* __restrict__ state, float decay,
                                                   uint8_t* __restrict__ img, float* f8) {
@@ -1094,10 +1144,11 @@ __global__ void __launch_bounds__(1024) k_pack_f8(const float* __restrict__ w, c
     if (state[S_F8_VER] == t_adam + 1u) return;
     const int l = blockIdx.x;
     const float debias = t_adam > 0u ? 1.0f - powf(decay, (float)t_adam) : 0.0f;
-    const int cnt = kRows<NL>(l) * kCols<NL>(l);
+    const int rows = rows_h<HID>(NL, l), cols = cols_h<HID>(l), poff = poff_h<HID>(NL, l);
+    const int cnt = rows * cols;
     float m = 0.0f;
     for (int j = threadIdx.x; j < cnt; j += blockDim.x) {
-        const int i = kPOff<NL>(l) + j;
+        const int i = poff + j;
         m = fmaxf(m, fabsf(debias > 0.0f ? ema[i] / debias : w[i]));
     }
 #pragma unroll
@@ -1109,15 +1160,15 @@ __global__ void __launch_bounds__(1024) k_pack_f8(const float* __restrict__ w, c
     const float wq = m > 0.0f ? kF8Max / m : 1.0f;
     if (threadIdx.x == 0) f8[kF8WQ + l] = wq;
     // every byte of the layer's 128-byte rows: K index c (zero past kCols)
-    for (int j = threadIdx.x; j < kRows<NL>(l) * 128; j += blockDim.x) {
+    for (int j = threadIdx.x; j < rows * 128; j += blockDim.x) {
         const int r = j / 128, c = j % 128;
         float x = 0.0f;
-        if (c < kCols<NL>(l)) {
-            const int i = kPOff<NL>(l) + r * kCols<NL>(l) + c;
+        if (c < cols) {
+            const int i = poff + r * cols + c;
             x = (debias > 0.0f ? ema[i] / debias : w[i]) * wq;
         }
         __nv_fp8_e4m3 e(x);
-        img[kF8Off<NL>(l) + umma::sw128_offset(r, c >> 4) + (c & 15)] = *reinterpret_cast<uint8_t*>(&e);
+        img[f8_off_h<HID>(l) + umma::sw128_offset(r, c >> 4) + (c & 15)] = *reinterpret_cast<uint8_t*>(&e);
     }
 }
 
@@ -2281,7 +2332,8 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
         return fail(TFG_E_INVALID, "mlp inference: FP8 needs tfgMlpCalibrate first");
     const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
     if (n->hid == 128) {
-        if (n->prec == mlp::kPrecF8) return fail(TFG_E_UNSUPPORTED, "mlp inference: FP8 is built for width 64");
+        if (n->prec == mlp::kPrecF8 && n->nl == 8)
+            return fail(TFG_E_UNSUPPORTED, "mlp inference: FP8 at width 128 is built for 3 or 5 hidden layers");
         uint32_t cap = (uint32_t)n->sms;
         if (n->tune.infer_ctas > 0) cap = std::min<uint32_t>(cap, (uint32_t)n->tune.infer_ctas);
         const uint32_t grid128 =
@@ -2292,12 +2344,19 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
             constexpr bool HASH = decltype(h)::value;
             if constexpr (NL == 4 || NL == 6) {
                 const size_t sm = mlp::kInfer128Smem + 1024;
-                if (n->prec == mlp::kPrecF16)
-                    mlp::k_infer128<mlp::kPrecF16, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
-                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
-                else
-                    mlp::k_infer128<mlp::kPrecBF16, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
-                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
+                if (n->prec == mlp::kPrecF16) {
+                    mlp::k_infer128<mlp::kPrecF16, false, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr, nullptr, nullptr, 0);
+                } else if (n->prec == mlp::kPrecBF16) {
+                    mlp::k_infer128<mlp::kPrecBF16, false, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr, nullptr, nullptr, 0);
+                } else {
+                    mlp::k_pack_f8<NL, 128><<<NL, 1024, 0, s>>>(n->w, n->ema, n->dstate, n->decay, n->inf_f8, n->f8);
+                    mlp::k_infer128<mlp::kPrecF8, true, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), n->inf_f8, out, img, thr, n->f8,
+                        n->f8 + mlp::kF8Amax, 0);
+                    mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 1);
+                }
             } else if constexpr (NL == 8) {
                 // streamed weights: one tile per CTA at a time, two CTAs per SM
                 const size_t sm = mlp::kT128Smem + 1024;
@@ -2349,7 +2408,8 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
 // Per-layer input amax over `count` samples through the FP16 path (every
 // tile), turned into the FP8 input scales.
 int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStream_t s) {
-    if (n->hid == 128) return fail(TFG_E_UNSUPPORTED, "tfgMlpCalibrate: FP8 is built for width 64");
+    if (n->hid == 128 && n->nl == 8)
+        return fail(TFG_E_UNSUPPORTED, "tfgMlpCalibrate: FP8 at width 128 is built for 3 or 5 hidden layers");
     if (count == 0) return fail(TFG_E_INVALID, "tfgMlpCalibrate: no samples");
     if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
         return fail(TFG_E_INVALID, "tfgMlpCalibrate: input buffer must be 16-byte aligned");
@@ -2360,6 +2420,15 @@ int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStrea
     with_model(n, [&](auto c, auto h) {
         constexpr int NL = decltype(c)::value;
         constexpr bool HASH = decltype(h)::value;
+        if (n->hid == 128) {
+            if constexpr (NL == 4 || NL == 6) {
+                const uint32_t g128 = std::min<uint32_t>((tiles + mlp::kSlots128 - 1) / mlp::kSlots128, (uint32_t)n->sms);
+                mlp::k_infer128<mlp::kPrecF16, true, NL, HASH><<<g128, mlp::kInfer128Threads, mlp::kInfer128Smem + 1024, s>>>(
+                    in, count, nullptr, n->bounds, hash_view(n, false), n->inf, nullptr, nullptr, nullptr, nullptr,
+                    n->f8 + mlp::kF8Amax, 1);
+            }
+            return 0;
+        }
         mlp::k_infer<mlp::kPrecF16, true, NL, HASH><<<grid, mlp::kInferThreads, mlp::kInferSmem + 1024, s>>>(
             in, count, nullptr, n->bounds, hash_view(n, false), n->inf, nullptr, nullptr, nullptr, nullptr,
             n->f8 + mlp::kF8Amax, 1);
@@ -2500,10 +2569,14 @@ void set_kernel_attrs() {
     cudaFuncSetAttribute(M::k_wgrad<NL, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
     if constexpr (NL == 4 || NL == 6) {
         const int i128 = M::kInfer128Smem + 1024;
-        cudaFuncSetAttribute(M::k_infer128<M::kPrecF16, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
-        cudaFuncSetAttribute(M::k_infer128<M::kPrecBF16, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
-        cudaFuncSetAttribute(M::k_infer128<M::kPrecF16, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
-        cudaFuncSetAttribute(M::k_infer128<M::kPrecBF16, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF16, false, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecBF16, false, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF16, true, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF8, true, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF16, false, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecBF16, false, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF16, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF8, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
         cudaFuncSetAttribute(M::k_train128<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kT128Smem + 1024);
         cudaFuncSetAttribute(M::k_wgrad<NL, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmemH<128> + 1024);
     }
@@ -2600,7 +2673,7 @@ int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, i
     const int nparams = M::params_rt(nl, width);
     const size_t pb = nparams * sizeof(float);
     const size_t fwd_bytes = M::fwd_bytes_rt(nl, width), bwd_bytes = M::bwd_bytes_rt(nl, width),
-                 f8_bytes = M::f8_bytes_of(nl);
+                 f8_bytes = width == 128 ? M::f8_bytes_h<128>(nl) : M::f8_bytes_of(nl);
     e = cudaMalloc((void**)&n->w, pb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->m, pb);
     if (e == cudaSuccess) e = cudaMalloc((void**)&n->v, pb);
@@ -2777,8 +2850,8 @@ extern "C" int tfgMlpSetPrecision(TfgColorMLP* h, int32_t precision) {
     if (!n) return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: null model");
     if (precision != TFG_MLP_FP16 && precision != TFG_MLP_BF16 && precision != TFG_MLP_FP8)
         return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: unknown precision");
-    if (precision == TFG_MLP_FP8 && n->hid == 128)
-        return tfg::fail(TFG_E_UNSUPPORTED, "tfgMlpSetPrecision: FP8 is built for width 64");
+    if (precision == TFG_MLP_FP8 && n->hid == 128 && n->nl == 8)
+        return tfg::fail(TFG_E_UNSUPPORTED, "tfgMlpSetPrecision: FP8 at width 128 is built for 3 or 5 hidden layers");
     n->prec = precision;
     return tfg::ok();
 }
