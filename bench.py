@@ -316,7 +316,7 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
     # Depth and encoding sweeps: the same protocol (warm-up, orbit, final
     # pose) with 3 and 7 hidden layers of 64 (5 is the run above), and with
     # the reference's own input encoding (hash grid + one-blob + identity).
-    def variant(**kw) -> dict:
+    def variant(fp8: bool = False, **kw) -> dict:
         m2 = ColorMLP(batch=16384, seed=2024, **kw)
         m2.set_bounds(*scene.bounds)
         r2 = NrcRenderer(ds, m2, params, train_steps=4, use_graph=True)
@@ -344,9 +344,30 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
                 m2.inference(r2.infer, out, n, stream=r2.stream)
             h1.record(r2.stream)
         h1.synchronize()
+        if fp8:
+            # the trained cache answered in FP8 (scales calibrated on the last frame's queries)
+            m2.calibrate(r2.infer, n, stream=r2.stream)
+            m2.set_precision(FP8)
+            r2.cfg.train_steps = 0
+            r2.frame(40_000, accumulate=False)
+            r2.stream.synchronize()
+            img8 = r2.image().cpu().numpy().astype(np.float64)
+            with torch.cuda.stream(r2.stream):
+                for _ in range(3):
+                    m2.inference(r2.infer, out, n, stream=r2.stream)
+                k0, k1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                k0.record(r2.stream)
+                for _ in range(10):
+                    m2.inference(r2.infer, out, n, stream=r2.stream)
+                k1.record(r2.stream)
+            k1.synchronize()
+            fp8_res = {"relmse": round(rel(img8), 5), "inference_ms": round(k0.elapsed_time(k1) / 10, 4)}
+            m2.set_precision(FP16)
         res = {"relmse": round(rel(img2), 5), "ms_per_frame": round(d0.elapsed_time(d1) / 10, 3),
                "inference_ms": round(h0.elapsed_time(h1) / 10, 4), "adam_steps": int(m2.state()["adam_t"]),
                "loss_ema": round(m2.state()["loss_ema"], 5)}
+        if fp8:
+            res["fp8"] = fp8_res
         m2.close()
         return res
 
@@ -358,7 +379,7 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
     encoding = {"frequency_12_bands": depth[5],
                 "hashgrid_reference": {**variant(encoding=HASHGRID), "config": hashgrid_reference(),
                                        "one_blob_bins": 4}}
-    width = {"5x64": depth[5], "5x128": variant(width=128), "3x128": variant(hidden_layers=3, width=128),
+    width = {"5x64": depth[5], "5x128": variant(fp8=True, width=128), "3x128": variant(hidden_layers=3, width=128),
              "7x128": variant(hidden_layers=7, width=128)}
     return {
         "frames": 48 + frames, "warmup_frames": 48, "camera": "orbit 1 deg/frame", "train_samples_per_frame": 4 * 16384,
