@@ -473,8 +473,8 @@ void tfgHashGridConfigReference(TfgHashGridConfig* c);
 int  tfgMlpCreateHashGrid(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
                           const TfgHashGridConfig* config, TfgColorMLP** out);
 /* The cache model with `width` = 64 or 128 units per hidden layer (3, 5 or 7
- * hidden layers; width 128 has FP16 / BF16 inference, FP8 is built for width
- * 64) and the frequency encoding (`config` null) or the composite encoding. */
+ * hidden layers; FP8 inference at width 128 with 3 or 5 of them) and the
+ * frequency encoding (`config` null) or the composite encoding. */
 int  tfgMlpCreateWide(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
                       int32_t width, const TfgHashGridConfig* config, TfgColorMLP** out);
 /* Length of the FP32 table arrays (0 for the frequency encoding). */
