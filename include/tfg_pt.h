@@ -473,7 +473,7 @@ void tfgHashGridConfigReference(TfgHashGridConfig* c);
 int  tfgMlpCreateHashGrid(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
                           const TfgHashGridConfig* config, TfgColorMLP** out);
 /* The cache model with `width` = 64 or 128 units per hidden layer (3, 5 or 7
- * hidden layers; FP8 inference at width 128 with 3 or 5 of them) and the
+ * hidden layers; FP16, BF16 or FP8 inference at both widths) and the
  * frequency encoding (`config` null) or the composite encoding. */
 int  tfgMlpCreateWide(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, int32_t hidden_layers,
                       int32_t width, const TfgHashGridConfig* config, TfgColorMLP** out);

@@ -1,7 +1,6 @@
 """The cache network with 128 units per hidden layer (3, 5 or 7 hidden
 layers; 7 streams its weights through shared memory) against the FP64
-oracle: inference in FP16, BF16 and FP8 (3 or 5 hidden layers), the
-gradients of the layers (and of the hash-grid tables with the composite
+oracle: inference in FP16, BF16 and FP8, the gradients of the layers (and of the hash-grid tables with the composite
 encoding), online training, and whole cache frames."""
 import numpy as np
 import pytest
@@ -75,14 +74,9 @@ def test_inference_matches_fp64_model(built, hidden):
     ref_b = mo.scrub(mo.forward_quantized(W, x, "bf16"))
     eb = np.abs(b.view(n, 3).cpu().numpy() - ref_b).mean() / scale
     assert eb < 0.01, eb
-    if hidden == 7:
-        # FP8 is built for the resident-weight kernel (3 or 5 hidden layers)
-        with pytest.raises(TfgError):
-            m.set_precision(FP8)
-        m.close()
-        return
     # FP8 (E4M3, per-layer scales from a calibration pass) against the exact
-    # E4M3 pipeline of the oracle, as for width 64
+    # E4M3 pipeline of the oracle, as for width 64; with 7 hidden layers the
+    # E4M3 image stays resident while the FP16 calibration pass streams
     dd = _dev(d)
     m.set_precision(FP8)
     f8 = torch.zeros(n * 3, device="cuda")
@@ -95,14 +89,15 @@ def test_inference_matches_fp64_model(built, hidden):
     ref = mo.scrub(raw)
     want8 = mo.scrub(mo.forward_quantized(W, x, "fp8", mo.layer_input_amax(W, x)))
     assert np.isfinite(g8).all()
-    # 128-term dot products over 3-5 layers: values next to an E4M3 code
+    # 128-term dot products over 3-7 layers: values next to an E4M3 code
     # boundary round to the neighbouring code more often than at width 64
-    # (bound 0.03 there), so the per-value agreement is looser; the accuracy
-    # against the FP64 network must still match an exact E4M3 pipeline
+    # (bound 0.03 there), and more so with depth, so the two pipelines'
+    # per-value disagreement stays below their common error against the FP64
+    # network; that error itself must match an exact E4M3 pipeline's
     dev = (np.abs(g8 - want8) / scale).mean()
     e_kernel = (np.abs(g8 - ref) / scale).mean()
     e_exact = (np.abs(want8 - ref) / scale).mean()
-    assert dev < 0.05, (dev, e_kernel, e_exact)
+    assert dev < max(0.05, e_exact), (dev, e_kernel, e_exact)
     assert e_kernel < 1.3 * e_exact + 0.01, (e_kernel, e_exact)
     m.close()
 
@@ -201,8 +196,6 @@ def test_width_limits(built):
         ColorMLP(batch=4096, hidden_layers=4, width=128)
     m = ColorMLP(batch=4096, hidden_layers=7, width=128)
     assert m.n_params == 96 * 128 + 6 * 128 * 128 + 16 * 128
-    with pytest.raises(TfgError):          # FP8 stays with the resident-weight kernel
-        m.set_precision(FP8)
     m.close()
 
 

@@ -707,25 +707,37 @@ __device__ __forceinline__ float encode_to_tmem(const TfgDatosMLP* r, const Boun
 }
 
 // The 48 packed FP16 / BF16 words of one query row (both encodings), for
-// kernels whose layer-0 operand lives in shared memory.
+// kernels whose layer-0 operand lives in shared memory; returns the largest
+// |feature| as encode_to_tmem does.
 template <int PREC, bool HASH>
-__device__ __forceinline__ void encode_words(const TfgDatosMLP& d, const Bounds& b, const HashGrid& g,
-                                             uint32_t (&w)[48]) {
+__device__ __forceinline__ float encode_words(const TfgDatosMLP& d, const Bounds& b, const HashGrid& g,
+                                              uint32_t (&w)[48]) {
     float p[3];
     unit_position(d, b, p);
+    float amax = 1.0f;
     if constexpr (HASH) {
         __half2 hw[kHashMaxLevels];
         hash_words_f16(p, g, hw);
         float t[32];
         composite_tail(d, t);
         composite_words<PREC>(hw, t, w);
+#pragma unroll
+        for (int k = 0; k < kHashMaxLevels; ++k) {
+            const float2 v = __half22float2(hw[k]);
+            amax = fmaxf(amax, fmaxf(fabsf(v.x), fabsf(v.y)));
+        }
+#pragma unroll
+        for (int k = 0; k < 30; ++k) amax = fmaxf(amax, fabsf(t[k]));
     } else {
         const float misc[13] = {(float)d.direccion.x, (float)d.direccion.y, (float)d.direccion.z,
                                 (float)d.normal.x,    (float)d.normal.y,    (float)d.normal.z,
                                 d.difuso.r,           d.difuso.g,           d.difuso.b,
                                 d.especular.r,        d.especular.g,        d.especular.b, 1.0f};
         frequency_words<PREC>(p, misc, w);
+#pragma unroll
+        for (int k = 0; k < 12; ++k) amax = fmaxf(amax, fabsf(misc[k]));
     }
+    return amax;
 }
 
 // Largest value over the warp, folded into *dst (values are >= 0, so their
@@ -952,8 +964,9 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
     k_infer128(const TfgDatosMLP* __restrict__ in, uint32_t n_max, const uint32_t* __restrict__ n_dev, Bounds bounds,
                HashGrid hg, const uint8_t* __restrict__ wimg, TfgColor* __restrict__ out, TfgColor* __restrict__ img,
                const TfgColor* __restrict__ thr, const float* __restrict__ f8, float* amax, int amax_all) {
-    static_assert(NL == 4 || NL == 6, "width 128 with resident weights: 3 or 5 hidden layers");
     constexpr bool kF8 = PREC == kPrecF8;
+    static_assert(NL == 4 || NL == 6 || (kF8 && NL == 8),
+                  "width 128 with resident weights: 3 or 5 hidden layers (7 in FP8, whose image fits)");
     constexpr uint32_t kWBytes = kF8 ? f8_bytes_h<128>(NL) : fwd_bytes_h<128>(NL);
     static_assert(kWBytes <= kInfer128Stage, "weights fit before the staging buffers");
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -1596,11 +1609,12 @@ __global__ void __launch_bounds__(128) k_train128(TrainArgs a) {
 // completed (one layer ahead), as in k_train128's forward pass; the
 // activations are the A operand in shared memory.  Same output rule as
 // k_infer / k_infer128 (NrcKernel.cu:99-126; RenderKernel.cu:49-66).
-template <int PREC, int NL, bool HASH>
+template <int PREC, bool TRACK, int NL, bool HASH>
 __global__ void __launch_bounds__(128) k_infer128s(const TfgDatosMLP* __restrict__ in, uint32_t n_max,
                                                    const uint32_t* __restrict__ n_dev, Bounds bounds, HashGrid hg,
                                                    const uint8_t* __restrict__ wimg, TfgColor* __restrict__ out,
-                                                   TfgColor* __restrict__ img, const TfgColor* __restrict__ thr) {
+                                                   TfgColor* __restrict__ img, const TfgColor* __restrict__ thr,
+                                                   float* amax) {
     static_assert(PREC != kPrecF8 && NL >= 2 && NL <= kMaxLayers, "width 128 streamed: FP16 / BF16");
     constexpr bool kBF = PREC == kPrecBF16;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -1644,7 +1658,8 @@ __global__ void __launch_bounds__(128) k_infer128s(const TfgDatosMLP* __restrict
         {
             // rows past the end encode the last row again; their outputs are never stored
             uint32_t w[48];
-            encode_words<PREC, HASH>(in[valid ? row : n - 1], bounds, hg, w);
+            const float a0 = encode_words<PREC, HASH>(in[valid ? row : n - 1], bounds, hg, w);
+            if (TRACK) warp_amax(valid ? a0 : 0.0f, &amax[0]);   // every tile: the calibration pass
             store_encoded(sa, t, w);
         }
         umma::fence_smem_to_async();
@@ -1672,14 +1687,19 @@ __global__ void __launch_bounds__(128) k_infer128s(const TfgDatosMLP* __restrict
             umma::fence_after_sync();
             if (!ok) break;
             if (!last) {
+                float lmax = 0.0f;
 #pragma unroll
                 for (int h = 0; h < 4; ++h) {
                     float v[32];
                     umma::tmem_ld32(tmem + tlane + 32u * h, v);
 #pragma unroll
-                    for (int i = 0; i < 32; ++i) v[i] = fmaxf(v[i], 0.0f);
+                    for (int i = 0; i < 32; ++i) {
+                        v[i] = fmaxf(v[i], 0.0f);
+                        if (TRACK) lmax = fmaxf(lmax, v[i]);
+                    }
                     store_row32<kBF>(sa, t, 32 * h, v);
                 }
+                if (TRACK) warp_amax(valid ? lmax : 0.0f, &amax[l + 1]);
             } else {
                 float v[16];
                 umma::tmem_ld16(tmem + tlane + 128u, v);
@@ -2332,8 +2352,6 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
         return fail(TFG_E_INVALID, "mlp inference: FP8 needs tfgMlpCalibrate first");
     const uint32_t tiles = (count + mlp::kTile - 1) / mlp::kTile;
     if (n->hid == 128) {
-        if (n->prec == mlp::kPrecF8 && n->nl == 8)
-            return fail(TFG_E_UNSUPPORTED, "mlp inference: FP8 at width 128 is built for 3 or 5 hidden layers");
         uint32_t cap = (uint32_t)n->sms;
         if (n->tune.infer_ctas > 0) cap = std::min<uint32_t>(cap, (uint32_t)n->tune.infer_ctas);
         const uint32_t grid128 =
@@ -2358,15 +2376,25 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
                     mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 1);
                 }
             } else if constexpr (NL == 8) {
-                // streamed weights: one tile per CTA at a time, two CTAs per SM
+                if (n->prec == mlp::kPrecF8) {
+                    // the E4M3 image of 7 hidden layers (116,736 B) stays resident
+                    const size_t sm = mlp::kInfer128Smem + 1024;
+                    mlp::k_pack_f8<NL, 128><<<NL, 1024, 0, s>>>(n->w, n->ema, n->dstate, n->decay, n->inf_f8, n->f8);
+                    mlp::k_infer128<mlp::kPrecF8, true, NL, HASH><<<grid128, mlp::kInfer128Threads, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), n->inf_f8, out, img, thr, n->f8,
+                        n->f8 + mlp::kF8Amax, 0);
+                    mlp::k_f8_update<<<1, 32, 0, s>>>(n->f8, n->dstate, 1);
+                    return 0;
+                }
+                // FP16 / BF16 weights stream: one tile per CTA at a time, two CTAs per SM
                 const size_t sm = mlp::kT128Smem + 1024;
                 const uint32_t grid_s = std::max<uint32_t>(1u, std::min<uint32_t>(tiles, 2u * cap));
                 if (n->prec == mlp::kPrecF16)
-                    mlp::k_infer128s<mlp::kPrecF16, NL, HASH><<<grid_s, 128, sm, s>>>(
-                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
+                    mlp::k_infer128s<mlp::kPrecF16, false, NL, HASH><<<grid_s, 128, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr, nullptr);
                 else
-                    mlp::k_infer128s<mlp::kPrecBF16, NL, HASH><<<grid_s, 128, sm, s>>>(
-                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr);
+                    mlp::k_infer128s<mlp::kPrecBF16, false, NL, HASH><<<grid_s, 128, sm, s>>>(
+                        in, count, n_dev, n->bounds, hash_view(n, false), wimg, out, img, thr, nullptr);
             }
             return 0;
         });
@@ -2408,8 +2436,6 @@ int infer_impl(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img,
 // Per-layer input amax over `count` samples through the FP16 path (every
 // tile), turned into the FP8 input scales.
 int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStream_t s) {
-    if (n->hid == 128 && n->nl == 8)
-        return fail(TFG_E_UNSUPPORTED, "tfgMlpCalibrate: FP8 at width 128 is built for 3 or 5 hidden layers");
     if (count == 0) return fail(TFG_E_INVALID, "tfgMlpCalibrate: no samples");
     if ((reinterpret_cast<uintptr_t>(in) & 15u) != 0)
         return fail(TFG_E_INVALID, "tfgMlpCalibrate: input buffer must be 16-byte aligned");
@@ -2426,6 +2452,11 @@ int calibrate_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, cudaStrea
                 mlp::k_infer128<mlp::kPrecF16, true, NL, HASH><<<g128, mlp::kInfer128Threads, mlp::kInfer128Smem + 1024, s>>>(
                     in, count, nullptr, n->bounds, hash_view(n, false), n->inf, nullptr, nullptr, nullptr, nullptr,
                     n->f8 + mlp::kF8Amax, 1);
+            } else if constexpr (NL == 8) {   // the FP16 pass streams its weights
+                const uint32_t gs = std::min<uint32_t>(tiles, 2u * (uint32_t)n->sms);
+                mlp::k_infer128s<mlp::kPrecF16, true, NL, HASH><<<gs, 128, mlp::kT128Smem + 1024, s>>>(
+                    in, count, nullptr, n->bounds, hash_view(n, false), n->inf, nullptr, nullptr, nullptr,
+                    n->f8 + mlp::kF8Amax);
             }
             return 0;
         }
@@ -2582,10 +2613,15 @@ void set_kernel_attrs() {
     }
     if constexpr (NL == 8) {   // width 128 with 7 hidden layers: streamed weights
         const int s128 = M::kT128Smem + 1024;
-        cudaFuncSetAttribute(M::k_infer128s<M::kPrecF16, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
-        cudaFuncSetAttribute(M::k_infer128s<M::kPrecBF16, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
-        cudaFuncSetAttribute(M::k_infer128s<M::kPrecF16, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
-        cudaFuncSetAttribute(M::k_infer128s<M::kPrecBF16, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        const int i128 = M::kInfer128Smem + 1024;
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecF16, false, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecBF16, false, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecF16, true, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecF16, false, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecBF16, false, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128s<M::kPrecF16, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF8, true, NL, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
+        cudaFuncSetAttribute(M::k_infer128<M::kPrecF8, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, i128);
         cudaFuncSetAttribute(M::k_train128<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, s128);
         cudaFuncSetAttribute(M::k_wgrad<NL, 128>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmemH<128> + 1024);
     }
@@ -2850,8 +2886,6 @@ extern "C" int tfgMlpSetPrecision(TfgColorMLP* h, int32_t precision) {
     if (!n) return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: null model");
     if (precision != TFG_MLP_FP16 && precision != TFG_MLP_BF16 && precision != TFG_MLP_FP8)
         return tfg::fail(TFG_E_INVALID, "tfgMlpSetPrecision: unknown precision");
-    if (precision == TFG_MLP_FP8 && n->hid == 128 && n->nl == 8)
-        return tfg::fail(TFG_E_UNSUPPORTED, "tfgMlpSetPrecision: FP8 at width 128 is built for 3 or 5 hidden layers");
     n->prec = precision;
     return tfg::ok();
 }
