@@ -1,6 +1,6 @@
 """CPU checks of the oracle's number-format helpers: its BF16 and E4M3
 rounding must agree with torch's own conversions (an independent
-implementation) before they are used to judge the BF16 / FP8 kernels."""
+implementation) before they are used to check the BF16 / FP8 kernels."""
 import numpy as np
 import torch
 
