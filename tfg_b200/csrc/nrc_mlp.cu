@@ -562,6 +562,21 @@ __device__ __forceinline__ uint32_t pack_e4m3x4(float a, float b, float c, float
     }
     return (uint32_t)lo | ((uint32_t)hi << 16);
 }
+// Two lanes of an IEEE round-to-nearest multiply in one packed instruction
+// (sm_100 f32x2): each lane equals the scalar product exactly.
+__device__ __forceinline__ void mul2(float& a, float& b, float s) {
+    uint64_t x, y;
+    asm("mov.b64 %0, {%1, %2};" : "=l"(x) : "f"(a), "f"(b));
+    asm("mov.b64 %0, {%1, %1};" : "=l"(y) : "f"(s));
+    asm("mul.rn.f32x2 %0, %0, %1;" : "+l"(x) : "l"(y));
+    asm("mov.b64 {%0, %1}, %2;" : "=f"(a), "=f"(b) : "l"(x));
+}
+// Four accumulator values scaled by s, then ReLU and E4M3 as pack_e4m3x4.
+__device__ __forceinline__ uint32_t scale_relu_e4m3x4(float a, float b, float c, float d, float s) {
+    mul2(a, b, s);
+    mul2(c, d, s);
+    return pack_e4m3x4<true>(a, b, c, d);
+}
 
 template <int PREC>
 __device__ __forceinline__ uint32_t pack2(float a, float b) {
@@ -874,8 +889,10 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
             if (!ok) break;
             umma::fence_after_sync();
             if (!last) {
-                float lmax = 0.0f;
-#pragma unroll
+                float lmax = 0.0f;   // max of the raw accumulator; x deq[l] > 0 keeps the order
+                // FP8 keeps the column chunks rolled: unrolled, with the amax
+                // tracking, the kernel outgrows the instruction cache
+#pragma unroll(kF8 ? 1 : 2)
                 for (int h = 0; h < 2; ++h) {
                     float v[32];
                     umma::tmem_ld32(tmem + tlane + 32u * h, v);
@@ -885,12 +902,11 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
                         uint32_t r[8];
 #pragma unroll
                         for (int i = 0; i < 8; ++i)
-                            r[i] = pack_e4m3x4<true>(v[4 * i] * sc, v[4 * i + 1] * sc, v[4 * i + 2] * sc,
-                                                     v[4 * i + 3] * sc);
+                            r[i] = scale_relu_e4m3x4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3], sc);
                         umma::tmem_st8(tmem_a + tlane + 8u * h, r);
                         if (track) {
 #pragma unroll
-                            for (int i = 0; i < 32; ++i) lmax = fmaxf(lmax, v[i] * deq[l]);
+                            for (int i = 0; i < 32; ++i) lmax = fmaxf(lmax, v[i]);
                         }
                     } else {
                         uint32_t r[16];
@@ -904,7 +920,7 @@ __global__ void __launch_bounds__(kInferThreads, 1) k_infer(const TfgDatosMLP* _
                         }
                     }
                 }
-                if (track) warp_amax(valid ? lmax : 0.0f, &amax[l + 1]);
+                if (track) warp_amax(valid ? lmax * deq[l] : 0.0f, &amax[l + 1]);
                 umma::tmem_wait_st();
                 umma::fence_before_sync();
                 slot_sync(bar);
@@ -1075,8 +1091,10 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
             if (!ok) break;
             umma::fence_after_sync();
             if (!last) {
-                float lmax = 0.0f;
-#pragma unroll
+                float lmax = 0.0f;   // max of the raw accumulator; x deq[l] > 0 keeps the order
+                // FP8 keeps the column chunks rolled: unrolled, with the amax
+                // tracking, the kernel outgrows the instruction cache
+#pragma unroll(kF8 ? 1 : 4)
                 for (int h = 0; h < 4; ++h) {
                     float v[32];
                     umma::tmem_ld32(tmem + tlane + 32u * h, v);
@@ -1086,12 +1104,11 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
                         uint32_t r[8];
 #pragma unroll
                         for (int i = 0; i < 8; ++i)
-                            r[i] = pack_e4m3x4<true>(v[4 * i] * sc, v[4 * i + 1] * sc, v[4 * i + 2] * sc,
-                                                     v[4 * i + 3] * sc);
+                            r[i] = scale_relu_e4m3x4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3], sc);
                         umma::tmem_st8(tmem_a + tlane + 8u * h, r);
                         if (track) {
 #pragma unroll
-                            for (int i = 0; i < 32; ++i) lmax = fmaxf(lmax, v[i] * deq[l]);
+                            for (int i = 0; i < 32; ++i) lmax = fmaxf(lmax, v[i]);
                         }
                     } else {
                         uint32_t r[16];
@@ -1105,7 +1122,7 @@ __global__ void __launch_bounds__(kInfer128Threads, 1)
                         }
                     }
                 }
-                if (track) warp_amax(valid ? lmax : 0.0f, &amax[l + 1]);
+                if (track) warp_amax(valid ? lmax * deq[l] : 0.0f, &amax[l + 1]);
                 umma::tmem_wait_st();
                 umma::fence_before_sync();
                 slot_sync(bar);
