@@ -649,14 +649,15 @@ def measure_peaks():
     print(json.dumps(out))
 
 
-def profile_mlp(width: int = 64):
+def profile_mlp(width: int = 64, precision: str = "fp16"):
     """Cache inference over 2,073,600 queries (232 MB of DatosMLP, more than
     L2) and one 16384-sample train step of a network of 5 hidden layers of
-    `width` units, untimed; used for ncu captures."""
+    `width` units, untimed; used for ncu captures.  With precision "fp8" the
+    FP16 inference is preceded by a calibration pass and two FP8 inferences."""
     import numpy as np
     import torch
 
-    from tfg_b200.nrc import ColorMLP
+    from tfg_b200.nrc import FP8, FP16, ColorMLP
     from tfg_b200.structs import DATOS_MLP
     n = W_PX * H_PX
     rng = np.random.default_rng(0)
@@ -672,6 +673,12 @@ def profile_mlp(width: int = 64):
     m = ColorMLP(batch=16384, seed=1, width=width)
     m.set_bounds((-6, -6, -6), (6, 6, 6))
     out = torch.zeros(n * 3, device="cuda")
+    if precision == "fp8":
+        m.set_precision(FP8)
+        m.calibrate(dd, n)
+        for _ in range(2):
+            m.inference(dd, out, n)
+        m.set_precision(FP16)
     m.inference(dd, out, n)
     m.train_step(dd, n, read_loss=False)
     torch.cuda.synchronize()
@@ -755,6 +762,8 @@ def main():
                     help="run cache inference on 1920x1080 queries and one train step, then exit (case for ncu)")
     ap.add_argument("--mlp-width", type=int, default=64,
                     help="with --profile-mlp / --profile-frame: 64 or 128 units per hidden layer")
+    ap.add_argument("--mlp-precision", default="fp16", choices=["fp16", "fp8"],
+                    help="with --profile-mlp: fp8 adds a calibration pass and two FP8 inferences")
     ap.add_argument("--profile-frame", action="store_true",
                     help="run six eager cache frames of the workload and one more inference, then exit (case for ncu)")
     ap.add_argument("--mlp-encoding", default="frequency", choices=["frequency", "hashgrid"],
@@ -770,7 +779,7 @@ def main():
         profile_frame(args.mlp_encoding, args.mlp_width)
         return
     if args.profile_mlp:
-        profile_mlp(args.mlp_width)
+        profile_mlp(args.mlp_width, args.mlp_precision)
         return
     if args.measure_peaks:
         measure_peaks()
