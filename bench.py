@@ -371,6 +371,72 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
         m2.close()
         return res
 
+    # Cache-policy sweep: the reference's termination policy (footprint 0.01
+    # of render.h:102, 5 % training paths of render.h:443, the first diffuse
+    # vertex past the footprint) against variants, each from a fresh model
+    # through the same protocol, scored at equal GPU time against the same
+    # 4096-spp reference.
+    plain_rel = {spp_eq: e_pt}
+
+    def plain_at(spp: int) -> float:
+        if spp not in plain_rel:
+            img_p = pt.accumulate_spp(ds, params, spp, 30_000).cpu().numpy().astype(np.float64)
+            plain_rel[spp] = rel(img_p)
+        return plain_rel[spp]
+
+    def policy(footprint=0.01, train_fraction=0.05, train_steps=4, hidden_layers=5, gate=0.0) -> dict:
+        m3 = ColorMLP(batch=16384, seed=2024, hidden_layers=hidden_layers)
+        m3.set_bounds(*scene.bounds)
+        r3 = NrcRenderer(ds, m3, params, train_steps=train_steps, use_graph=True, footprint=footprint,
+                         train_fraction=train_fraction, gate_threshold=gate)
+        for f in range(48):
+            with torch.cuda.stream(r3.stream):
+                set_pose(0)
+            r3.frame(f, warmup=True, accumulate=False)
+        for k in range(frames):
+            with torch.cuda.stream(r3.stream):
+                set_pose(k)
+            r3.frame(48 + k, accumulate=False)
+        d0, d1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        d0.record(r3.stream)
+        for k in range(10):
+            r3.frame(10_000 + k, accumulate=False)
+        d1.record(r3.stream)
+        d1.synchronize()
+        t3 = d0.elapsed_time(d1) / 10
+        e3 = rel(r3.image().cpu().numpy().astype(np.float64))
+        answered = float((r3.thr.view(-1, 3) != 0).any(dim=1).float().mean())
+        sp = max(1, int(round(t3 / t_pt)))
+        ep = plain_at(sp)
+        out3 = {"footprint": footprint, "train_fraction": round(train_fraction, 5), "train_steps": train_steps,
+                "hidden_layers": hidden_layers, "gate_threshold": gate, "relmse": round(e3, 5),
+                "ms_per_frame": round(t3, 3), "plain_spp_at_equal_time": sp, "relmse_plain": round(ep, 5),
+                "relmse_ratio_plain_over_nrc": round(ep / e3, 3),
+                "relmse_x_time_ratio": round((ep * t_pt * sp) / (e3 * t3), 3),
+                "pixels_answered_by_cache": round(answered, 4)}
+        if gate > 0:
+            out3["open_gate_cells"] = int(m3.state()["gate"])
+        m3.close()
+        return out3
+
+    one_per_record = 65536 / n   # about as many training paths as records a frame uses
+    sweep_defs = {
+        "reference": {},
+        "footprint_0.001": {"footprint": 0.001},
+        "footprint_0.1": {"footprint": 0.1},
+        "primary_vertex": {"footprint": 0.0},
+        "train_fraction_3.2pct": {"train_fraction": one_per_record},
+        "train_steps_1": {"train_steps": 1},
+        "train_steps_2": {"train_steps": 2},
+        "3x64": {"hidden_layers": 3},
+        "primary_vertex_train_3.2pct": {"footprint": 0.0, "train_fraction": one_per_record},
+        "primary_vertex_train_3.2pct_steps_2": {"footprint": 0.0, "train_fraction": one_per_record, "train_steps": 2},
+        "gated_0.5": {"gate": 0.5},
+        "primary_vertex_gated_0.5": {"footprint": 0.0, "train_fraction": one_per_record, "gate": 0.5},
+    }
+    policy_sweep = {name: policy(**kw) for name, kw in sweep_defs.items()}
+    best = max(policy_sweep, key=lambda k: policy_sweep[k]["relmse_x_time_ratio"])
+
     depth = {5: {"relmse": round(e_nrc, 5), "ms_per_frame": round(t_nrc, 3), "inference_ms": round(t_inf, 4),
                  "adam_steps": int(st["adam_t"])}}
     for hidden in (3, 7):
@@ -390,6 +456,8 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
         "reference_spp": ref_spp, "adam_steps": int(st["adam_t"]), "loss_ema": round(st["loss_ema"], 5),
         "mlp_inference": {"queries": n, "ms": round(t_inf, 4), "tflops": round(flops / (t_inf * 1e-3) / 1e12, 2),
                           "flops_per_query": int(flops / n)},
+        "policy_sweep": policy_sweep,
+        "best_policy": {"name": best, **policy_sweep[best]},
         "precision_sweep": sweep,
         "depth_sweep": {f"{k}x64": v for k, v in sorted(depth.items())},
         "encoding_sweep": encoding,
@@ -768,7 +836,19 @@ def main():
                     help="run six eager cache frames of the workload and one more inference, then exit (case for ncu)")
     ap.add_argument("--mlp-encoding", default="frequency", choices=["frequency", "hashgrid"],
                     help="with --profile-frame: the cache's input encoding")
+    ap.add_argument("--nrc-only", action="store_true",
+                    help="run only the radiance-cache evaluation (config 3 and its sweeps), print it and exit")
     args = ap.parse_args()
+    if args.nrc_only:
+        import torch
+
+        from tfg_b200 import pathtracer as pt
+        from tfg_b200 import scenes
+        scene = scenes.spheres_terrain(W_PX, H_PX)
+        ds = pt.DeviceScene(scene, "cuda")
+        print(json.dumps(nrc_eval(scene, ds, torch.device("cuda", 0))))
+        ds.close()
+        return
     if args.impl == "reference":
         reference_arm(args)
         return

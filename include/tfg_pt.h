@@ -493,6 +493,20 @@ int  tfgMlpComputeGradientEx(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32
  * `n` values in [0, 1] (device array): 4 bins each into `bins` (device, 4 n
  * floats), exactly as the cache kernels compute them. */
 int  tfgOneBlobBins(const float* values, float* bins, int32_t n, void* stream);
+/* The cache kernels' layer-0 input of `n` queries (device `DatosMLP`s): 96
+ * floats per query (device `out`), each the exact FP16 / BF16 operand the
+ * first GEMM reads -- frequency bands, direction, normal, albedos and the
+ * constant 1, or the hash-grid, one-blob and albedo features of a composite
+ * model.  `pass` TFG_ENCODE_TRAINING gives the training forward pass's FP16
+ * features (FP32 tables), TFG_ENCODE_INFERENCE those of inference at the
+ * model's precision (FP16 or BF16; FP8 is refused: its features are scaled
+ * per call).  A test hook beside tfgOneBlobBins: it pins the GEMM chain of
+ * the cache kernels against a model fed with these features.  No reference
+ * counterpart (tiny-cuda-nn encodes inside its own kernels). */
+#define TFG_ENCODE_TRAINING  0
+#define TFG_ENCODE_INFERENCE 1
+int  tfgMlpEncodeFeatures(TfgColorMLP* mlp, const TfgDatosMLP* in, uint32_t n, int32_t pass, float* out,
+                          void* stream);
 /* Length of the model's FP32 parameter arrays: 96 W + W^2 (hidden - 1) + 16 W
  * for width W (23552 for 5 hidden layers of 64, 79872 for 5 of 128). */
 int32_t tfgMlpParamCount(const TfgColorMLP* mlp);
@@ -580,7 +594,7 @@ int  tfgMlpAutotune(TfgColorMLP* mlp, const TfgDatosMLP* in, uint32_t count, Tfg
  * the last call (synchronous). */
 int  tfgMlpStatus(void);
 /* Device training state (synchronous): [0] step counter, [1] Adam step,
- * [2] records used by the last step, [3] cache-query gate (1 = open),
+ * [2] records used by the last step, [3] open cells of the gate grid after the last gated frame,
  * [4] running loss (float bits), [5..7] reserved. */
 int  tfgMlpGetState(TfgColorMLP* mlp, uint32_t* out8);
 
@@ -593,13 +607,30 @@ typedef struct TfgNrcFrameConfig {
     uint32_t max_records;     /* records used per frame; reference 65536 (main.cpp:1036) */
     uint32_t min_records;     /* train only above this count; reference 1024 (main.cpp:1043) */
     int32_t  warmup;          /* 1: no cache queries, every path is a training path (main.cpp:997) */
-    float    gate_threshold;  /* > 0: answer cache queries only once the running training loss is
-                                 below this value (0: always, as the reference) */
+    float    gate_threshold;  /* > 0: per-cell gate judged by the path tracer.  Training records whose
+                                 suffix ran to its end (unbiased estimates of the radiance at their head)
+                                 are compared with the cache's answer there, per cell of a 32^3 grid over
+                                 the model's scene bounds, in running sums decayed by 0.8 per frame; a
+                                 cell opens once it holds 8 samples' weight and the cache's running
+                                 relative error there (|mean error| over sqrt(mean target^2 + 0.01)) is
+                                 below this value, and closes again when it rises.  Paths query the
+                                 cache, training paths record bootstrapped heads and cut their suffixes
+                                 into it only in open cells; elsewhere they go on as plain paths, so with
+                                 every cell closed a frame renders plain path tracing.  The training and
+                                 unbiased draws then come from a per-pixel stream of their own, which
+                                 leaves each path the random numbers of a plain pass.
+                                 0: no gate, the reference's behaviour (render.h:182) */
     int32_t  use_graph;       /* 1: capture the frame as a CUDA graph on first use and replay it
                                  (needs a non-default stream) */
+    float    footprint;       /* a path queries (or records a training head) once its footprint
+                                 a_suffix >= footprint * a_0; reference 0.01 (render.h:86-102).  0: at
+                                 the first diffuse, non-specular vertex, the primary hit included */
+    float    train_fraction;  /* share of paths traced for training while queries are on; reference
+                                 0.05 (render.h:443) */
 } TfgNrcFrameConfig;
 
-/* Reference frame settings: 1 step, 65536 records, train above 1024, no gate, no graph. */
+/* Reference frame settings: 1 step, 65536 records, train above 1024, footprint 0.01,
+ * 5 % training paths, no gate, no graph. */
 void tfgNrcFrameConfigReference(TfgNrcFrameConfig* cfg);
 
 /* Caller-owned device buffers of a cache frame (main.cpp:908-930). */

@@ -19,7 +19,18 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-REF_DIR = Path(os.environ.get("TFG_REFERENCE_DIR", "/root/reference"))
+
+
+def reference_dir() -> Path | None:
+    """The reference checkout: ``TFG_REFERENCE_DIR``, else a checkout named
+    ``reference`` beside the repository; None when neither holds the kernel
+    sources (the prebuilt library is used then)."""
+    for d in (os.environ.get("TFG_REFERENCE_DIR"), str(ROOT.parent / "reference")):
+        if d and (Path(d) / "RenderKernel.cu").exists():
+            return Path(d)
+    return None
+
+
 ORACLE_LIB = HERE / "liboracle.so"
 REF_LIB = HERE / "_ref" / "libtfgref.so"
 
@@ -43,18 +54,20 @@ def build_cpu(force: bool = False) -> Path:
 
 
 def build_ref(force: bool = False) -> Path | None:
-    """Compile the reference kernels; returns None when the checkout is absent."""
-    srcs = [REF_DIR / "RenderKernel.cu", REF_DIR / "NrcKernel.cu"]
-    if not all(s.exists() for s in srcs):
+    """Compile the reference kernels; without the checkout the prebuilt
+    library is returned (None when there is none)."""
+    ref_dir = reference_dir()
+    if ref_dir is None:
         return REF_LIB if REF_LIB.exists() else None
+    srcs = [ref_dir / "RenderKernel.cu", ref_dir / "NrcKernel.cu"]
     shim = HERE / "ref_shim.cu"
-    headers = sorted(REF_DIR.glob("*.h")) + sorted(REF_DIR.glob("*.cuh"))
+    headers = sorted(ref_dir.glob("*.h")) + sorted(ref_dir.glob("*.cuh"))
     if not force and _newer(REF_LIB, [shim, *srcs, *headers]):
         return REF_LIB
     nvcc = os.environ.get("NVCC") or shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
     REF_LIB.parent.mkdir(exist_ok=True)
     cmd = [nvcc, "-O3", "-std=c++17", "-gencode", "arch=compute_100a,code=sm_100a", "-Xcompiler", "-fPIC",
-           "-shared", "-w", "-I", str(REF_DIR), *map(str, srcs), str(shim), "-o", str(REF_LIB)]
+           "-shared", "-w", "-I", str(ref_dir), *map(str, srcs), str(shim), "-o", str(REF_LIB)]
     res = subprocess.run(cmd, capture_output=True, text=True)
     if res.returncode != 0:
         raise RuntimeError(f"reference kernel build failed:\n{res.stderr}")

@@ -189,6 +189,67 @@ def round_bf16(a) -> np.ndarray:
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+def round_f16(a) -> np.ndarray:
+    """Round to the nearest FP16 value (ties to even) and back to FP64; the
+    value is first rounded to FP32, the kernels' accumulator type."""
+    return np.asarray(a, np.float64).astype(np.float32).astype(np.float16).astype(np.float64)
+
+
+def forward_operands(W, x, kind: str = "f16"):
+    """Output (first 3 columns) of the network as the FP16 / BF16 inference
+    kernels compute it from their own layer-0 operands `x` (the features
+    tfgMlpEncodeFeatures returns, already rounded): weights rounded to the
+    operand type, every hidden layer's ReLU output rounded to it before the
+    next GEMM, products summed in FP64 (the kernels accumulate in FP32)."""
+    rnd = round_f16 if kind == "f16" else round_bf16
+    h = np.asarray(x, np.float64)
+    for l, w in enumerate(W):
+        z = h @ rnd(w).T
+        if l < len(W) - 1:
+            h = rnd(np.maximum(z, 0.0))
+    return z[:, :3]
+
+
+def loss_and_grad_operands(W, x, y):
+    """Loss, layer gradients and the gradient of the layer-0 operands as the
+    training kernels compute them from their own FP16 layer-0 operands `x`:
+    FP16 forward pass (FP16 weights, every hidden ReLU output rounded to FP16
+    for the next GEMM); the loss gradient and every layer-output gradient
+    rounded to BF16; the backward GEMMs with BF16 weights; the weight
+    gradients from the BF16-rounded layer inputs (the ReLU outputs rounded
+    from their FP32 values) and output gradients; the layer-0 operand
+    gradient (for the hash-grid tables) with FP16 layer-0 weights.  Sums in
+    FP64."""
+    W16 = [round_f16(w) for w in W]
+    Wbf = [round_bf16(w) for w in W]
+    L = len(W)
+    h = np.asarray(x, np.float64)
+    h_bf = [round_bf16(h)]
+    zs = []
+    for l in range(L):
+        z = h @ W16[l].T
+        zs.append(z)
+        if l < L - 1:
+            a = np.maximum(z, 0.0)
+            h = round_f16(a)
+            h_bf.append(round_bf16(a))
+    pred = zs[-1][:, :3]
+    lum = 0.299 * pred[:, 0] + 0.587 * pred[:, 1] + 0.114 * pred[:, 2]
+    den = lum * lum + 0.01
+    n = len(x)
+    loss = float(np.sum((pred - y) ** 2 / den[:, None]) / (3 * n))
+    g = np.zeros_like(zs[-1])
+    g[:, :3] = 2.0 * (pred - y) / den[:, None]
+    dz = round_bf16(g)
+    grads = [None] * L
+    for l in range(L - 1, -1, -1):
+        grads[l] = dz.T @ h_bf[l] / (3 * n)
+        if l > 0:
+            dz = round_bf16((dz @ Wbf[l]) * (zs[l - 1] > 0))
+    dx = dz @ W16[0] / (3 * n)
+    return loss, grads, dx
+
+
 def _e4m3_grid() -> np.ndarray:
     """Every finite non-negative E4M3 value (bias 7, 3 mantissa bits, max 448)."""
     vals = [m / 8.0 * 2.0 ** -6 for m in range(8)]                        # subnormals

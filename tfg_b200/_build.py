@@ -63,7 +63,8 @@ def build(force: bool = False, verbose: bool = False, ptxas_info: bool = False) 
         if ptxas_info and res.stderr:
             print(res.stderr, file=sys.stderr)
     if force or not LIB.exists() or LIB.stat().st_mtime < max(o.stat().st_mtime for o in objs):
-        cmd = [cc, *ARCH, "-shared", "-o", str(LIB), *map(str, objs), "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
+        cmd = [cc, *ARCH, "-shared", "-Xlinker", "-soname=libtfgpt.so", "-o", str(LIB), *map(str, objs),
+               "-lcudart_static", "-lrt", "-lpthread", "-ldl"]
         res = subprocess.run(cmd, capture_output=True, text=True)
         if res.returncode != 0:
             raise RuntimeError(f"link failed:\n{res.stdout}\n{res.stderr}")

@@ -55,6 +55,7 @@ _PROTOS = {
                                        c_void_p]),
     "tfgMlpHashParamCount": (ctypes.c_int64, [c_void_p]),
     "tfgOneBlobBins": (c_int32, [c_void_p, c_void_p, c_int32, c_void_p]),
+    "tfgMlpEncodeFeatures": (c_int32, [c_void_p, c_void_p, c_uint32, c_int32, c_void_p, c_void_p]),
     "tfgMlpCreateWide": (c_int32, [c_uint32, c_uint32, c_uint32, c_uint64, c_int32, c_int32, POINTER(CHashGridConfig),
                                    c_void_p]),
     "tfgMlpGetHashParams": (c_int32, [c_void_p, c_int32, POINTER(c_float), ctypes.c_int64]),

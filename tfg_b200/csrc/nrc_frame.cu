@@ -32,7 +32,7 @@ __global__ void k_set_frame(int32_t* frame_dev, int32_t frame) {
 struct FrameKey {
     const void* ptrs[20];
     int32_t ints[20];
-    float gate;
+    float gate, footprint, train_fraction;
     bool operator==(const FrameKey& o) const { return std::memcmp(this, &o, sizeof(FrameKey)) == 0; }
 };
 
@@ -44,8 +44,8 @@ struct FrameGraph {
 };
 
 std::mutex g_frame_mutex;
-int32_t* g_frame_dev[16] = {nullptr};
-FrameGraph g_graph[16];
+int32_t* g_frame_dev[kMaxDevices] = {nullptr};
+FrameGraph g_graph[kMaxDevices];
 
 struct FrameCall {
     ColorMlp* mlp;
@@ -63,15 +63,25 @@ struct FrameCall {
 
 int enqueue_cache_steps(const FrameCall& c, cudaStream_t s);
 
+// The frame's cache policy: footprint and training share from the frame
+// settings, the model's gate grid when the gate is on.
+CachePolicy policy_of(const FrameCall& c) {
+    CachePolicy p;
+    p.footprint = c.cfg.footprint;
+    p.train_fraction = c.cfg.train_fraction;
+    mlp_gate_view(c.mlp, p);
+    return p;
+}
+
 int enqueue_frame(const FrameCall& c, bool prepare_only, cudaStream_t s) {
-    const uint32_t* gate = c.cfg.gate_threshold > 0.0f ? mlp_gate(c.mlp) : nullptr;
+    const CachePolicy pol = policy_of(c);
     if (prepare_only) {
         if (int rc = mlp_prepare(c.mlp)) return rc;
     } else {
         cudaError_t e = cudaMemsetAsync(c.b.counter, 0, sizeof(uint32_t), s);
         if (e != cudaSuccess) return fail((int)e, std::string("nrc frame: ") + cudaGetErrorString(e));
     }
-    if (int rc = render_pass_ex(c.prm, c.cam, c.prims, c.nprims, c.lights, c.nlights, c.W, c.H, 0, c.frame_dev, gate,
+    if (int rc = render_pass_ex(c.prm, c.cam, c.prims, c.nprims, c.lights, c.nlights, c.W, c.H, 0, c.frame_dev, &pol,
                                 c.bvh, c.tris_wt, c.mesh, c.nmesh, c.b.img, nullptr, c.b.regs, c.b.counter,
                                 (int)c.b.ring_cap, c.b.infer, c.b.thr, c.cfg.warmup ? 0 : 1, 1, prepare_only,
                                 c.ws_slot, s))
@@ -89,7 +99,7 @@ PassScene pass_scene(const FrameCall& c) {
     p.img = c.b.img; p.accum = nullptr;
     p.regs = c.b.regs; p.reg_counter = c.b.counter; p.reg_cap = (int)c.b.ring_cap;
     p.infer = c.b.infer; p.thr_out = c.b.thr;
-    p.use_inf_dev = c.cfg.gate_threshold > 0.0f ? mlp_gate(c.mlp) : nullptr;
+    p.policy = policy_of(c);
     p.use_inf = c.cfg.warmup ? 0 : 1;
     return p;
 }
@@ -104,12 +114,17 @@ int enqueue_cache_steps(const FrameCall& c, cudaStream_t s) {
     if (c.b.accum)
         if (int rc = launch_nrc_frame_small(3, c.b.img, c.b.accum, nullptr, nullptr, npx, 0, s)) return rc;
     if (int rc = launch_nrc_frame_small(2, c.b.counter, navail, nullptr, nullptr, c.cfg.max_records, 0, s)) return rc;
-    if (int rc = launch_nrc_frame_small(0, c.b.regs, c.b.tail_in, nullptr, navail, c.cfg.max_records, min_n, s))
+    const bool gated = c.cfg.gate_threshold > 0.0f;
+    if (int rc = launch_nrc_frame_small(gated ? 4 : 0, c.b.regs, c.b.tail_in, nullptr, navail, c.cfg.max_records,
+                                        min_n, s))
         return rc;
     if (int rc = mlp_enqueue_infer(c.mlp, c.b.tail_in, c.b.tail_pred, nullptr, nullptr, c.cfg.max_records, navail, s))
         return rc;
     if (int rc = launch_nrc_frame_small(1, c.b.regs, c.b.train_buf, c.b.tail_pred, navail, c.cfg.max_records, min_n, s))
         return rc;
+    if (gated)
+        if (int rc = mlp_enqueue_gate_update(c.mlp, c.b.regs, c.b.tail_pred, navail, c.cfg.max_records, min_n, s))
+            return rc;
     for (int k = 0; k < c.cfg.train_steps; ++k)
         if (int rc = mlp_enqueue_train(c.mlp, c.b.train_buf, min_n, s)) return rc;
     return ok();
@@ -143,6 +158,8 @@ FrameKey key_of(const FrameCall& c) {
     static_assert(sizeof(v) <= sizeof(k.ints), "frame key: too many ints");
     std::memcpy(k.ints, v, sizeof(v));
     k.gate = c.cfg.gate_threshold;
+    k.footprint = c.cfg.footprint;
+    k.train_fraction = c.cfg.train_fraction;
     return k;
 }
 
@@ -159,6 +176,9 @@ int make_call(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const TfgRenderPar
         return fail(TFG_E_INVALID, "nrc frame: a required buffer is null");
     if (cfg->train_steps < 0 || cfg->max_records == 0 || b.ring_cap < cfg->max_records)
         return fail(TFG_E_INVALID, "nrc frame: ring capacity below max_records");
+    if (!(cfg->footprint >= 0.0f) || !(cfg->train_fraction >= 0.0f && cfg->train_fraction <= 1.0f) ||
+        !(cfg->gate_threshold >= 0.0f))
+        return fail(TFG_E_INVALID, "nrc frame: footprint, gate_threshold >= 0 and train_fraction in [0, 1]");
     c.mlp = reinterpret_cast<ColorMlp*>(mlp);
     c.cfg = *cfg;
     c.prm = *params;
@@ -174,11 +194,11 @@ int make_call(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const TfgRenderPar
 }
 
 int frame_word(int dev, int32_t** out) {
-    if (!g_frame_dev[dev & 15]) {
-        cudaError_t e = cudaMalloc((void**)&g_frame_dev[dev & 15], sizeof(int32_t));
+    if (!g_frame_dev[dev]) {
+        cudaError_t e = cudaMalloc((void**)&g_frame_dev[dev], sizeof(int32_t));
         if (e != cudaSuccess) return fail((int)e, std::string("nrc frame: ") + cudaGetErrorString(e));
     }
-    *out = g_frame_dev[dev & 15];
+    *out = g_frame_dev[dev];
     return ok();
 }
 
@@ -189,18 +209,18 @@ struct BatchGraph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
 };
-BatchGraph g_batch[16];
-cudaStream_t g_branch[16][kWorkspaceSlots] = {};
-cudaEvent_t g_fork[16] = {};
-cudaEvent_t g_join[16][kWorkspaceSlots] = {};
+BatchGraph g_batch[kMaxDevices];
+cudaStream_t g_branch[kMaxDevices][kWorkspaceSlots] = {};
+cudaEvent_t g_fork[kMaxDevices] = {};
+cudaEvent_t g_join[kMaxDevices][kWorkspaceSlots] = {};
 
 int branch_resources(int dev, int nb) {
     cudaError_t e = cudaSuccess;
-    if (!g_fork[dev & 15]) e = cudaEventCreateWithFlags(&g_fork[dev & 15], cudaEventDisableTiming);
+    if (!g_fork[dev]) e = cudaEventCreateWithFlags(&g_fork[dev], cudaEventDisableTiming);
     for (int b = 1; b < nb && e == cudaSuccess; ++b) {
-        if (!g_branch[dev & 15][b]) e = cudaStreamCreateWithFlags(&g_branch[dev & 15][b], cudaStreamNonBlocking);
-        if (e == cudaSuccess && !g_join[dev & 15][b])
-            e = cudaEventCreateWithFlags(&g_join[dev & 15][b], cudaEventDisableTiming);
+        if (!g_branch[dev][b]) e = cudaStreamCreateWithFlags(&g_branch[dev][b], cudaStreamNonBlocking);
+        if (e == cudaSuccess && !g_join[dev][b])
+            e = cudaEventCreateWithFlags(&g_join[dev][b], cudaEventDisableTiming);
     }
     if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch: ") + cudaGetErrorString(e));
     return ok();
@@ -237,18 +257,18 @@ int enqueue_batch(const std::vector<FrameCall>& calls, int nb, int dev, bool mer
         if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch: ") + cudaGetErrorString(e));
         if (int r = render_merged(calls, false, s)) return r;
     }
-    e = cudaEventRecord(g_fork[dev & 15], s);
-    for (int b = 1; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(g_branch[dev & 15][b], g_fork[dev & 15], 0);
+    e = cudaEventRecord(g_fork[dev], s);
+    for (int b = 1; b < nb && e == cudaSuccess; ++b) e = cudaStreamWaitEvent(g_branch[dev][b], g_fork[dev], 0);
     if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch fork: ") + cudaGetErrorString(e));
     for (const FrameCall& c : calls) {
-        cudaStream_t bs = c.branch == 0 ? s : g_branch[dev & 15][c.branch];
+        cudaStream_t bs = c.branch == 0 ? s : g_branch[dev][c.branch];
         rc = merged ? enqueue_cache_steps(c, bs) : enqueue_frame(c, false, bs);
         if (rc) break;
     }
     // join every branch even after a failure, so a capture can end cleanly
     for (int b = 1; b < nb; ++b) {
-        cudaError_t e2 = cudaEventRecord(g_join[dev & 15][b], g_branch[dev & 15][b]);
-        if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(s, g_join[dev & 15][b], 0);
+        cudaError_t e2 = cudaEventRecord(g_join[dev][b], g_branch[dev][b]);
+        if (e2 == cudaSuccess) e2 = cudaStreamWaitEvent(s, g_join[dev][b], 0);
         if (e2 != cudaSuccess && !rc) rc = fail((int)e2, std::string("tfgNrcFrameBatch join: ") + cudaGetErrorString(e2));
     }
     return rc;
@@ -265,6 +285,8 @@ extern "C" void tfgNrcFrameConfigReference(TfgNrcFrameConfig* c) {
     c->warmup = 0;
     c->gate_threshold = 0.0f;
     c->use_graph = 0;
+    c->footprint = 0.01f;
+    c->train_fraction = 0.05f;
 }
 
 extern "C" int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const TfgRenderParams* params,
@@ -285,7 +307,7 @@ extern "C" int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const
     if (int rc = make_call(mlp, cfg, params, camara, primitivas, num_primitivas, luces, num_luces, W, H, bvh, tris_wt,
                            primitivas_bvh, num_prims_bvh, buffers, frame_dev, c))
         return rc;
-    mlp_set_gate_threshold(c.mlp, cfg->gate_threshold);
+    if (int rc = mlp_set_gate_threshold(c.mlp, cfg->gate_threshold)) return rc;
     k_set_frame<<<1, 32, 0, s>>>(c.frame_dev, frame);
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrame: ") + cudaGetErrorString(e));
@@ -294,7 +316,7 @@ extern "C" int tfgNrcFrame(TfgColorMLP* mlp, const TfgNrcFrameConfig* cfg, const
         if (int rc = enqueue_frame(c, true, s)) return rc;
         return enqueue_frame(c, false, s);
     }
-    FrameGraph& g = g_graph[dev & 15];
+    FrameGraph& g = g_graph[dev];
     // Prepare first: a workspace that had to grow since the capture changes
     // the key, and the frame is captured again.
     if (int rc = enqueue_frame(c, true, s)) return rc;
@@ -363,7 +385,7 @@ extern "C" int tfgNrcFrameBatch(int32_t n, const TfgNrcSceneFrame* scenes, int32
     }
     if (int rc = branch_resources(dev, nb)) return rc;
     for (const FrameCall& c : calls) {
-        mlp_set_gate_threshold(c.mlp, c.cfg.gate_threshold);
+        if (int rc = mlp_set_gate_threshold(c.mlp, c.cfg.gate_threshold)) return rc;
         if (merged) {
             if (int rc = mlp_prepare(c.mlp)) return rc;
         } else if (int rc = enqueue_frame(c, true, s)) {
@@ -376,7 +398,7 @@ extern "C" int tfgNrcFrameBatch(int32_t n, const TfgNrcSceneFrame* scenes, int32
     e = cudaGetLastError();
     if (e != cudaSuccess) return fail((int)e, std::string("tfgNrcFrameBatch: ") + cudaGetErrorString(e));
     if (!(use_graph && s != nullptr)) return enqueue_batch(calls, nb, dev, merged, s);
-    BatchGraph& g = g_batch[dev & 15];
+    BatchGraph& g = g_batch[dev];
     std::vector<FrameKey> keys;
     for (const FrameCall& c : calls) keys.push_back(key_of(c));
     if (!g.valid || g.keys.size() != keys.size() ||

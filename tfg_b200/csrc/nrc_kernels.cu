@@ -161,6 +161,10 @@ __global__ void k_default_camera(TfgCamara* c, int W, int H) {
 
 // Device-count forms for the frame driver: the record count lives in device
 // memory (no host read between render and training).
+// GATED: a complete record (its suffix ran to the end: zero suffix
+// throughput, so the targets ignore its tail prediction) queries its head
+// instead, which gives the gate update the cache's prediction there.
+template <bool GATED>
 __global__ void k_tail_dev(const TfgRegistroEntrenamiento* __restrict__ regs, TfgDatosMLP* __restrict__ out,
                            const uint32_t* n_dev, uint32_t min_n) {
     const uint32_t n = *n_dev;
@@ -170,8 +174,11 @@ __global__ void k_tail_dev(const TfgRegistroEntrenamiento* __restrict__ regs, Tf
         TfgDatosMLP d;
         memset(&d, 0, sizeof(d));
         if (r.valido) {
-            d.posicion = r.tail.posicion; d.direccion = r.tail.direccion; d.normal = r.tail.normal;
-            d.difuso = r.tail.difuso; d.especular = r.tail.especular;
+            const TfgColor ts = r.throughput_sufijo;
+            const bool complete = GATED && ts.r == 0.0f && ts.g == 0.0f && ts.b == 0.0f;
+            const TfgDatosGeometricos& v = complete ? r.head : r.tail;
+            d.posicion = v.posicion; d.direccion = v.direccion; d.normal = v.normal;
+            d.difuso = v.difuso; d.especular = v.especular;
         }
         out[i] = d;
     }
@@ -242,9 +249,13 @@ int launch_nrc_frame_small(int which, const void* a, void* b, const void* c, con
     const int blocks = std::max(1, std::min((int)((cap + 255) / 256), 148 * 4));
     switch (which) {
         case 0:
-            k_tail_dev<<<blocks, 256, 0, s>>>(static_cast<const TfgRegistroEntrenamiento*>(a),
-                                              static_cast<TfgDatosMLP*>(b), n_dev, min_n);
+            k_tail_dev<false><<<blocks, 256, 0, s>>>(static_cast<const TfgRegistroEntrenamiento*>(a),
+                                                     static_cast<TfgDatosMLP*>(b), n_dev, min_n);
             return launch_check("nrc tail queries");
+        case 4:
+            k_tail_dev<true><<<blocks, 256, 0, s>>>(static_cast<const TfgRegistroEntrenamiento*>(a),
+                                                    static_cast<TfgDatosMLP*>(b), n_dev, min_n);
+            return launch_check("nrc gated tail queries");
         case 1:
             k_targets_dev<<<blocks, 256, 0, s>>>(static_cast<const TfgRegistroEntrenamiento*>(a),
                                                  static_cast<const TfgColor*>(c), static_cast<TfgDatosMLP*>(b), n_dev,

@@ -31,6 +31,7 @@
 #include <cuda_fp16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -150,7 +151,7 @@ enum : int {
     S_STEP = 0,      // ColorMLP::step_counter (mlp.cpp:103), seed of the sample indices
     S_ADAM_T = 1,    // Adam time step
     S_NAVAIL = 2,    // training records available to this step
-    S_GATE = 3,      // 1: the cache's running error is low enough to answer queries
+    S_GATE = 3,      // open cells of the gate grid after the last gated frame
     S_LOSS_EMA = 4,  // running loss (float bits)
     S_F8_VER = 5,    // S_ADAM_T + 1 of the weights in the FP8 image (0: not packed)
     S_WORDS = 8
@@ -2106,9 +2107,8 @@ __global__ void k_hash_init(float* w, size_t count, uint64_t seed) {
     }
 }
 
-// After a step: advance the step counter and Adam time, keep a running loss
-// and open the cache-query gate once it falls below `gate`.
-__global__ void k_tick(uint32_t* state, const float* loss_sum, float inv_count, uint32_t min_n, float gate) {
+// After a step: advance the step counter and Adam time, keep a running loss.
+__global__ void k_tick(uint32_t* state, const float* loss_sum, float inv_count, uint32_t min_n) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     const uint32_t n = state[S_NAVAIL];
     if (n < min_n || n == 0) return;
@@ -2118,7 +2118,78 @@ __global__ void k_tick(uint32_t* state, const float* loss_sum, float inv_count, 
     float ema = __uint_as_float(state[S_LOSS_EMA]);
     ema = (state[S_ADAM_T] == 1u) ? loss : 0.9f * ema + 0.1f * loss;
     state[S_LOSS_EMA] = __float_as_uint(ema);
-    if (gate <= 0.0f || ema < gate) state[S_GATE] = 1u;
+}
+
+// ------------------------------------------------------------------ cache gate
+// The gate judges the cache with the path tracer's own unbiased estimates: a
+// training record whose suffix ran to its end (no bootstrapped tail) carries
+// L_suffix / factor, an unbiased one-sample estimate of what the cache should
+// answer at its head (the target of RenderKernel.cu:92-166 without a tail
+// term).  Per cell of a kGateRes^3 grid over the scene bounds the gate keeps
+// running sums (decayed by kGateDecay once per frame) of the sample weight n,
+// of d = lum(cache at the head) - lum(target) and of lum(target).  The cell's
+// running relative error is |mean d| / sqrt(mean target^2 + 0.01) (the
+// offset of the loss and of relMSE); the mean of d carries the path
+// tracer's noise too (its expected square is the squared bias plus the
+// variance of d over n), so a cell needs both a small bias and enough
+// samples to open.  A cell is open when it has kGateMinWeight of evidence
+// and its error is below the threshold: cells without evidence stay closed,
+// and a cell whose error grows (the lighting changed, the cache drifted)
+// closes again.
+constexpr float kGateDecay = 0.8f;
+constexpr float kGateMinWeight = 8.0f;
+
+struct GateGeo {
+    float lo[3], inv[3];
+};
+
+__global__ void k_gate_accumulate(const TfgRegistroEntrenamiento* __restrict__ regs, const TfgColor* __restrict__ pred,
+                                  const uint32_t* n_dev, uint32_t cap, uint32_t min_n, GateGeo g, float4* cells,
+                                  uint32_t* state) {
+    const uint32_t n = min(*n_dev, cap);
+    if (n < min_n) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) state[S_GATE] = 0u;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const TfgRegistroEntrenamiento& r = regs[i];
+        if (!r.valido) continue;
+        const TfgColor ts = r.throughput_sufijo;
+        if (ts.r != 0.0f || ts.g != 0.0f || ts.b != 0.0f) continue;   // bootstrapped: not an unbiased estimate
+        const TfgColor L = r.luz_acumulada_sufijo, f = r.factor_normalizacion;
+        float t[3] = {L.r / fmaxf(f.r, 1e-8f), L.g / fmaxf(f.g, 1e-8f), L.b / fmaxf(f.b, 1e-8f)};
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            t[k] = fminf(t[k], 100000.0f);
+            if (isnan(t[k]) || isinf(t[k])) t[k] = 0.0f;
+        }
+        const TfgColor q = pred[i];
+        const float lt = 0.299f * t[0] + 0.587f * t[1] + 0.114f * t[2];
+        const float d = (0.299f * q.r + 0.587f * q.g + 0.114f * q.b) - lt;
+        const uint32_t c = gate_cell(g.lo, g.inv, (float)r.head.posicion.x, (float)r.head.posicion.y,
+                                     (float)r.head.posicion.z);
+        float* cell = reinterpret_cast<float*>(&cells[c]);
+        atomicAdd(cell + 0, 1.0f);
+        atomicAdd(cell + 1, d);
+        atomicAdd(cell + 2, lt);
+    }
+}
+
+__global__ void k_gate_finish(float4* __restrict__ cells, uint32_t* __restrict__ bits, uint32_t* state, float thr2,
+                              const uint32_t* n_dev, uint32_t cap, uint32_t min_n) {
+    if (min(*n_dev, cap) < min_n) return;   // no records this frame: sums and bits stay
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;   // the grid covers kGateCells exactly
+    const float4 v = cells[c];
+    bool open = false;
+    if (v.x >= kGateMinWeight) {
+        const float inv_n = 1.0f / v.x;
+        const float err = v.y * inv_n, mean = v.z * inv_n;
+        open = err * err < thr2 * (mean * mean + 0.01f);
+    }
+    const uint32_t word = __ballot_sync(0xFFFFFFFFu, open);
+    if ((threadIdx.x & 31u) == 0u) {
+        bits[c >> 5] = word;
+        if (word) atomicAdd(&state[S_GATE], (uint32_t)__popc(word));
+    }
+    cells[c] = make_float4(v.x * kGateDecay, v.y * kGateDecay, v.z * kGateDecay, v.w * kGateDecay);
 }
 
 __global__ void k_set_word(uint32_t* state, int index, uint32_t value) {
@@ -2141,7 +2212,9 @@ struct ColorMlp {
     uint8_t* zT[mlp::kMaxLayers] = {nullptr};
     float* loss = nullptr;
     uint32_t* dstate = nullptr;  // mlp::S_* words
-    float gate = 0.0f;           // cache-query gate threshold on the running loss (<= 0: always open)
+    float gate = 0.0f;           // gate threshold on a cell's relative bias (<= 0: no gate)
+    float4* gate_cells = nullptr;   // running sums per gate cell (allocated with the first threshold > 0)
+    uint32_t* gate_bits = nullptr;  // open cells, one bit each
     int prec = mlp::kPrecF16;    // inference operand precision
     uint8_t* inf_bf = nullptr;   // BF16 inference image (written with the FP16 one)
     uint8_t* inf_f8 = nullptr;   // FP8 inference image (re-packed when the weights changed)
@@ -2347,7 +2420,7 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     }
     if (!update) return ok();
     if (int rc = repack(n, s, true, min_n)) return rc;
-    mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n, n->gate);
+    mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n);
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp step: tick");
     return ok();
@@ -2583,7 +2656,6 @@ int autotune_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, TfgColor* 
 // ------------------------------------------------------------------ internal API (frame driver)
 int mlp_prepare(ColorMlp* n) { return ensure_acts(n, n->batch / mlp::kTile); }
 uint32_t* mlp_state(ColorMlp* n) { return n->dstate; }
-uint32_t* mlp_gate(ColorMlp* n) { return n->dstate + mlp::S_GATE; }
 uint32_t* mlp_navail(ColorMlp* n) { return n->dstate + mlp::S_NAVAIL; }
 int mlp_enqueue_infer(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColor* img, const TfgColor* thr,
                       uint32_t max_count, const uint32_t* n_dev, cudaStream_t s) {
@@ -2592,7 +2664,49 @@ int mlp_enqueue_infer(ColorMlp* n, const TfgDatosMLP* in, TfgColor* out, TfgColo
 int mlp_enqueue_train(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, cudaStream_t s) {
     return enqueue_step(n, buf, min_n, true, s);
 }
-void mlp_set_gate_threshold(ColorMlp* n, float g) { n->gate = g; }
+int mlp_set_gate_threshold(ColorMlp* n, float g) {
+    if (!(g >= 0.0f)) return fail(TFG_E_INVALID, "nrc frame: gate_threshold must be >= 0");
+    if (g > 0.0f && !n->gate_cells) {
+        cudaError_t e = cudaMalloc((void**)&n->gate_cells, (size_t)kGateCells * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMalloc((void**)&n->gate_bits, (size_t)kGateCells / 8);
+        if (e == cudaSuccess) e = cudaMemset(n->gate_cells, 0, (size_t)kGateCells * sizeof(float4));
+        if (e == cudaSuccess) e = cudaMemset(n->gate_bits, 0, (size_t)kGateCells / 8);
+        if (e != cudaSuccess) {
+            if (n->gate_cells) cudaFree(n->gate_cells);
+            if (n->gate_bits) cudaFree(n->gate_bits);
+            n->gate_cells = nullptr; n->gate_bits = nullptr;
+            return cuda_fail(e, "nrc frame: gate grid");
+        }
+    }
+    n->gate = g;
+    return ok();
+}
+
+void mlp_gate_view(ColorMlp* n, CachePolicy& p) {
+    p.gate_bits = n->gate > 0.0f ? n->gate_bits : nullptr;
+    for (int k = 0; k < 3; ++k) {
+        p.gate_lo[k] = n->bounds.lo[k];
+        const float ext = n->bounds.hi[k] - n->bounds.lo[k];
+        p.gate_inv[k] = ext > 0.0f ? (float)kGateRes / ext : 0.0f;
+    }
+}
+
+int mlp_enqueue_gate_update(ColorMlp* n, const TfgRegistroEntrenamiento* regs, const TfgColor* tail_pred,
+                            const uint32_t* n_dev, uint32_t cap, uint32_t min_n, cudaStream_t s) {
+    if (!(n->gate > 0.0f) || !n->gate_cells) return ok();
+    CachePolicy p;
+    mlp_gate_view(n, p);
+    mlp::GateGeo g;
+    for (int k = 0; k < 3; ++k) { g.lo[k] = p.gate_lo[k]; g.inv[k] = p.gate_inv[k]; }
+    const unsigned blocks = (unsigned)std::max(1u, std::min((cap + 255u) / 256u, 148u * 4u));
+    mlp::k_gate_accumulate<<<blocks, 256, 0, s>>>(regs, tail_pred, n_dev, cap, min_n, g, n->gate_cells, n->dstate);
+    static_assert(kGateCells % 256 == 0, "gate grid: whole blocks");
+    mlp::k_gate_finish<<<kGateCells / 256, 256, 0, s>>>(n->gate_cells, n->gate_bits, n->dstate, n->gate * n->gate,
+                                                          n_dev, cap, min_n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "nrc frame: gate update");
+    return ok();
+}
 int mlp_precision(const ColorMlp* n) { return n->prec; }
 uint32_t mlp_tuning_generation(const ColorMlp* n) { return n->tune_generation; }
 
@@ -2819,6 +2933,73 @@ __global__ void k_one_blob(const float* __restrict__ in, float* __restrict__ out
 }  // namespace mlp
 }  // namespace tfg
 
+namespace tfg {
+namespace mlp {
+// Layer-0 input of the cache kernels, unpacked to floats: 96 features per
+// query, each exactly the FP16 / BF16 operand the first GEMM reads.
+template <int PREC>
+__device__ __forceinline__ void unpack_words(const uint32_t (&w)[48], float* __restrict__ o) {
+#pragma unroll
+    for (int k = 0; k < 48; ++k) {
+        float2 v;
+        if constexpr (PREC == kPrecBF16) v = __bfloat1622float2(*reinterpret_cast<const __nv_bfloat162*>(&w[k]));
+        else v = __half22float2(*reinterpret_cast<const __half2*>(&w[k]));
+        o[2 * k] = v.x;
+        o[2 * k + 1] = v.y;
+    }
+}
+
+template <int PREC, bool HASH>
+__global__ void k_encode_infer(const TfgDatosMLP* __restrict__ in, uint32_t n, Bounds b, HashGrid g,
+                               float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t w[48];
+    encode_words<PREC, HASH>(in[i], b, g, w);
+    unpack_words<PREC>(w, out + 96 * (size_t)i);
+}
+
+__global__ void k_encode_train(const TfgDatosMLP* __restrict__ in, uint32_t n, Bounds b, HashGrid g,
+                               float* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    uint32_t w[48];
+    encode(in[i], b, g, w);
+    unpack_words<kPrecF16>(w, out + 96 * (size_t)i);
+}
+}  // namespace mlp
+}  // namespace tfg
+
+extern "C" int tfgMlpEncodeFeatures(TfgColorMLP* h, const TfgDatosMLP* in, uint32_t n, int32_t pass, float* out,
+                                    void* stream) {
+    ColorMlp* m = reinterpret_cast<ColorMlp*>(h);
+    if (!m) return tfg::fail(TFG_E_INVALID, "tfgMlpEncodeFeatures: model is null");
+    if (pass != TFG_ENCODE_TRAINING && pass != TFG_ENCODE_INFERENCE)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpEncodeFeatures: pass must be TFG_ENCODE_TRAINING or TFG_ENCODE_INFERENCE");
+    if (pass == TFG_ENCODE_INFERENCE && m->prec == tfg::mlp::kPrecF8)
+        return tfg::fail(TFG_E_INVALID, "tfgMlpEncodeFeatures: FP8 inference scales its features per call; "
+                                        "select FP16 or BF16 first");
+    if (n == 0) return tfg::ok();
+    if (!in || !out) return tfg::fail(TFG_E_INVALID, "tfgMlpEncodeFeatures: null pointer");
+    if (int rc = tfg::require_sm100(m->dev)) return rc;
+    cudaStream_t s = (cudaStream_t)stream;
+    const unsigned blocks = (n + 127) / 128;
+    namespace M = tfg::mlp;
+    const M::HashGrid g = tfg::hash_view(m, pass == TFG_ENCODE_TRAINING);
+    if (pass == TFG_ENCODE_TRAINING) {
+        M::k_encode_train<<<blocks, 128, 0, s>>>(in, n, m->bounds, g, out);
+    } else if (m->prec == M::kPrecBF16) {
+        if (m->hlevels) M::k_encode_infer<M::kPrecBF16, true><<<blocks, 128, 0, s>>>(in, n, m->bounds, g, out);
+        else M::k_encode_infer<M::kPrecBF16, false><<<blocks, 128, 0, s>>>(in, n, m->bounds, g, out);
+    } else {
+        if (m->hlevels) M::k_encode_infer<M::kPrecF16, true><<<blocks, 128, 0, s>>>(in, n, m->bounds, g, out);
+        else M::k_encode_infer<M::kPrecF16, false><<<blocks, 128, 0, s>>>(in, n, m->bounds, g, out);
+    }
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return tfg::fail((int)e, std::string("tfgMlpEncodeFeatures: ") + cudaGetErrorString(e));
+    return tfg::ok();
+}
+
 extern "C" int tfgOneBlobBins(const float* values, float* bins, int32_t n, void* stream) {
     if (n < 0) return tfg::fail(TFG_E_INVALID, "tfgOneBlobBins: negative n");
     if (n == 0) return tfg::ok();
@@ -2867,7 +3048,8 @@ extern "C" void tfgMlpDestroy(TfgColorMLP* h) {
     if (!n) return;
     for (void* p : {(void*)n->w, (void*)n->m, (void*)n->v, (void*)n->ema, (void*)n->grad, (void*)n->fwd, (void*)n->bwd,
                     (void*)n->inf, (void*)n->inf_bf, (void*)n->inf_f8, (void*)n->f8, (void*)n->loss, (void*)n->dstate,
-                    (void*)n->hw, (void*)n->hm, (void*)n->hv, (void*)n->hema, (void*)n->hgrad, (void*)n->hinf})
+                    (void*)n->hw, (void*)n->hm, (void*)n->hv, (void*)n->hema, (void*)n->hgrad, (void*)n->hinf,
+                    (void*)n->gate_cells, (void*)n->gate_bits})
         if (p) cudaFree(p);
     for (int l = 0; l < M::kMaxLayers; ++l) {
         if (n->hT[l]) cudaFree(n->hT[l]);

@@ -9,6 +9,7 @@
 #include <stdint.h>
 
 #include "../../include/tfg_pt.h"
+#include "tfg_runtime.h"
 
 namespace tfg {
 
@@ -29,6 +30,19 @@ static_assert(sizeof(TfgTinyBVHD_GPU) == 24, "TinyBVHD_GPU is 24 B");
 
 constexpr float kEps = 1e-3f;                       // render.h:27, escenario.h:40
 constexpr float kPiF = 3.14159265358979323846f;     // render.h:20
+
+// Cell of the radiance cache's gate grid (kGateRes per axis over the scene
+// bounds: cell = floor((x - lo) * inv)) holding a point; points outside the
+// bounds fall into the border cells.  The render pass reads the cell's gate
+// bit with it and the gate update adds a record's error to it.
+__device__ __forceinline__ uint32_t gate_cell(const float (&lo)[3], const float (&inv)[3], float x, float y,
+                                              float z) {
+    const int r = kGateRes - 1;
+    const int ix = min(max(__float2int_rd((x - lo[0]) * inv[0]), 0), r);
+    const int iy = min(max(__float2int_rd((y - lo[1]) * inv[1]), 0), r);
+    const int iz = min(max(__float2int_rd((z - lo[2]) * inv[2]), 0), r);
+    return ((uint32_t)iz * kGateRes + (uint32_t)iy) * kGateRes + (uint32_t)ix;
+}
 
 // ---------------------------------------------------------------- float3
 struct V3 {

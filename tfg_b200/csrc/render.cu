@@ -41,6 +41,8 @@ enum : uint32_t {
     F_CAPTURED = 4u,    // punto_entrenamiento_encontrado
     F_INF = 8u,         // inference query written by shade
     F_TAIL = 16u,       // tail vertex recorded
+    F_FULL = 32u,       // training path whose head lies in a closed gate cell: its suffix runs to the end
+                        // and its radiance counts in the pixel as well (a plain path with a record)
 };
 
 constexpr uint32_t kMissId = 0xFFFFFFFFu;
@@ -90,7 +92,7 @@ struct PassArgs {
     const TfgPrimitiva* mesh; int nmesh;
     const TfgCamara* cam;        // device pointer, read by k_generate
     const int32_t* frame_dev;    // optional device-side base frame number
-    const uint32_t* use_inf_dev; // optional device-side gate on cache queries
+    CachePolicy pol;             // footprint, training share, gate grid
     int W, H, frame;
     TfgColor* img; float* accum;
     TfgRegistroEntrenamiento* regs; uint32_t* reg_counter; int reg_cap;
@@ -119,7 +121,7 @@ constexpr int kMaxBatchScenes = 16;
 struct SceneDesc {
     const TfgPrimitiva* prims; const TfgLuzPuntual* lights;
     const float4* nodes; const float4* tris; const TfgPrimitiva* mesh;
-    const TfgCamara* cam; const uint32_t* use_inf_dev;
+    const TfgCamara* cam; CachePolicy pol;
     TfgColor* img; float* accum;
     TfgRegistroEntrenamiento* regs; uint32_t* reg_counter;
     TfgDatosMLP* infer; TfgColor* thr_out;
@@ -255,12 +257,20 @@ __device__ __forceinline__ int load_aprims_smem(APrim* sp, const TfgPrimitiva* g
 
 // ------------------------------------------------------------------ generate
 // render.h:424-447: seed, jitter draws, training / unbiased draws, camera ray.
-__device__ __forceinline__ int use_inf_of(const PassArgs& a) {
-    return a.use_inf && (!a.use_inf_dev || *a.use_inf_dev != 0u);
+__device__ __forceinline__ int use_inf_of(const PassArgs& a) { return a.use_inf; }
+__device__ __forceinline__ int use_inf_of(const SceneDesc& d) { return d.use_inf; }
+
+template <bool MS>
+__device__ __forceinline__ const CachePolicy& policy_of(const PassArgs& a, const TableOf<MS>& tab, uint32_t sc) {
+    if constexpr (MS) return tab.s[sc].pol;
+    else { (void)tab; (void)sc; return a.pol; }
 }
 
-__device__ __forceinline__ int use_inf_of(const SceneDesc& d) {
-    return d.use_inf && (!d.use_inf_dev || *d.use_inf_dev != 0u);
+// Whether the gate lets a path use the cache at P (always without a gate).
+__device__ __forceinline__ bool gate_open(const CachePolicy& c, V3 P) {
+    if (!c.gate_bits) return true;
+    const uint32_t cell = gate_cell(c.gate_lo, c.gate_inv, P.x, P.y, P.z);
+    return (__ldg(&c.gate_bits[cell >> 5]) >> (cell & 31u)) & 1u;
 }
 
 template <bool MS>
@@ -290,10 +300,17 @@ __global__ void k_generate(PassArgs a, TableOf<MS> tab) {
         V3 O, D;
         camera_ray(cam, x, y, W, H, ox, oy, O, D);
         uint32_t flags = 0;
-        bool training = a.train ? (use_inf ? (pcg_uniform(rng) < 0.05f) : true) : false;
-        if (training) {
-            flags |= F_TRAIN;
-            if (pcg_uniform(rng) < 0.0625f) flags |= F_UNBIASED;
+        if (a.train) {
+            const CachePolicy& pol = policy_of<MS>(a, tab, sc);
+            // Gated passes draw the training decisions from a stream of their
+            // own, so the path's stream stays that of a plain pass.
+            uint32_t side = seed_pixel(x, y, frame0 + (int)s) ^ 0x9E3779B9u;
+            uint32_t& r = pol.gate_bits ? side : rng;
+            const bool training = use_inf ? (pcg_uniform(r) < pol.train_fraction) : true;
+            if (training) {
+                flags |= F_TRAIN;
+                if (pcg_uniform(r) < 0.0625f) flags |= F_UNBIASED;
+            }
         }
         a.ws.ray[0][2 * p + 0] = make_float4(O.x, O.y, O.z, MS ? __uint_as_float(sc) : 1e9f);
         a.ws.ray[0][2 * p + 1] = make_float4(D.x, D.y, D.z, __uint_as_float(p));
@@ -413,6 +430,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<M
             const Geo g = geo_of<MS>(a, tab, sc);
             int use_inf = use_inf_single;
             if constexpr (MS) use_inf = use_inf_of(tab.s[sc]);
+            const CachePolicy& pol = policy_of<MS>(a, tab, sc);
             V3 O = xyz(o4), D = xyz(d4);
             float4 thr4 = a.ws.thr[p];
             uint4 st = a.ws.st[p];
@@ -450,13 +468,14 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<M
                         if (!captured) lsuf.w += spread;
                         else nrc4.x += spread;
                     }
-                    foot_ok = lsuf.w >= lpre.w * 0.01f;
+                    foot_ok = lsuf.w >= lpre.w * pol.footprint;
                 }
                 if (cmax(m.emision) > 0.0f) {
                     // Emission ends the path (render.h:104-123).
                     const V3 c = mul(cam, m.emision);
                     if (captured) {
                         lsuf.x += c.x; lsuf.y += c.y; lsuf.z += c.z;
+                        if (flags & F_FULL) { lpre.x += c.x; lpre.y += c.y; lpre.z += c.z; }
                         put_geo(&a.ws.ts[10 * (size_t)p + 4], P, normalized(-D), nrm, v3(0, 0, 0), v3(0, 0, 0));
                         a.ws.ts[10 * (size_t)p + 9] = make_float4(0, 0, 0, 0);
                         flags |= F_TAIL;
@@ -470,13 +489,15 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<M
                         const V3 ps = P + nrm * kEps;
                         want_shadow = true;
                         sh0 = make_float4(ps.x, ps.y, ps.z, __uint_as_float(p));
-                        sh1 = make_float4(nrm.x, nrm.y, nrm.z, __uint_as_float(captured ? 1u : 0u));
+                        // bit 0: the suffix's radiance; bit 1: the pixel's as well (F_FULL)
+                        sh1 = make_float4(nrm.x, nrm.y, nrm.z,
+                                          __uint_as_float(captured ? ((flags & F_FULL) ? 3u : 1u) : 0u));
                         sh2 = make_float4(m.difuso.x, m.difuso.y, m.difuso.z, MS ? __uint_as_float(sc) : 0.0f);
                         sh3 = make_float4(cam.x, cam.y, cam.z, 0.0f);
                     }
                     if (captured) {
                         // Suffix bootstrap termination (render.h:134-163).
-                        const bool stop = !(flags & F_UNBIASED) && (nrc4.x >= nrc4.y);
+                        const bool stop = !(flags & (F_UNBIASED | F_FULL)) && (nrc4.x >= nrc4.y) && gate_open(pol, P);
                         if (stop) {
                             put_geo(&a.ws.ts[10 * (size_t)p + 4], P, map01(view), map01(nrm), m.difuso, m.especular);
                             const V3 refl = m.difuso + m.especular + m.transmision;
@@ -491,7 +512,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<M
                         V3 refl = m.difuso + m.especular + m.transmision;
                         refl = v3(fmaxf(refl.x, 1e-3f), fmaxf(refl.y, 1e-3f), fmaxf(refl.z, 1e-3f));
                         const bool training = (flags & F_TRAIN) != 0;
-                        if (!training && use_inf) {
+                        if (!training && use_inf && gate_open(pol, P)) {
                             const Outs o = outs_of<MS>(a, tab, sc);
                             const uint32_t px = st.w;
                             write_datos(&o.infer[px], P, map01(view), map01(nrm), m.difuso, m.especular);
@@ -505,6 +526,7 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<M
                             a.ws.ts[10 * (size_t)p + 8] = make_float4(tt.x, tt.y, tt.z, 0.0f);
                             nrc4.y = lsuf.w;   // a_prefix = a_current
                             flags |= F_CAPTURED;
+                            if (!gate_open(pol, P)) flags |= F_FULL;
                             // This bounce's NEE still belongs to the prefix: sh1.w stays 0.
                         }
                     }
@@ -612,13 +634,13 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
         V3 L = v3(0.0f, 0.0f, 0.0f);
         V3 P, N, kd, cam;
         uint32_t p = 0;
-        bool to_suffix = false;
+        uint32_t dest = 0;   // bit 0: suffix radiance, bit 1: also the pixel's
         if (have) {
             const float4* s = &a.ws.shadow[4 * (size_t)i];
             const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
             P = xyz(s0); N = xyz(s1); kd = xyz(s2); cam = xyz(s3);
             p = __float_as_uint(s0.w);
-            to_suffix = __float_as_uint(s1.w) != 0u;
+            dest = __float_as_uint(s1.w);
             const uint32_t sc = MS ? __float_as_uint(s2.w) : 0u;
             const Geo g = geo_of<MS>(a, tab, sc);
             const TfgLuzPuntual* lights = a.lights;
@@ -661,10 +683,16 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
         }
         if (have && lg == 0u) {
             const V3 add = mul(cam, L);
-            float4* dst = to_suffix ? &a.ws.lsuf[p] : &a.ws.lpre[p];
-            float4 v = *dst;
-            v.x += add.x; v.y += add.y; v.z += add.z;
-            *dst = v;
+            if (dest & 1u) {
+                float4 v = a.ws.lsuf[p];
+                v.x += add.x; v.y += add.y; v.z += add.z;
+                a.ws.lsuf[p] = v;
+            }
+            if (dest != 1u) {
+                float4 v = a.ws.lpre[p];
+                v.x += add.x; v.y += add.y; v.z += add.z;
+                a.ws.lpre[p] = v;
+            }
         }
     }
     if (STATS) flush_work(3, nrays, cnt);
@@ -704,7 +732,8 @@ __global__ void k_resolve(PassArgs a, TableOf<MS> tab) {
             }
             const uint32_t flags = a.ws.st[p].y;
             const bool rec = nrc && (flags & F_TRAIN) && (flags & F_CAPTURED);
-            if (o.thr_out && !(flags & F_INF) && !rec) o.thr_out[px] = TfgColor{0.0f, 0.0f, 0.0f};
+            const bool head_query = rec && !(flags & F_FULL);
+            if (o.thr_out && !(flags & F_INF) && !head_query) o.thr_out[px] = TfgColor{0.0f, 0.0f, 0.0f};
             if (!rec) continue;
             // Training path with a head vertex: its pixel keeps the prefix radiance and
             // asks the cache at the head (render.h:243-260); the record goes to the ring
@@ -713,13 +742,13 @@ __global__ void k_resolve(PassArgs a, TableOf<MS> tab) {
             TfgDatosGeometricos head, tail;
             get_geo(ts, head);
             const float4 thr_train = ts[8];
-            if (o.infer) {
+            if (o.infer && head_query) {
                 TfgDatosMLP d;
                 d.posicion = head.posicion; d.direccion = head.direccion; d.normal = head.normal;
                 d.difuso = head.difuso; d.especular = head.especular; d.color = TfgColor{0.0f, 0.0f, 0.0f};
                 o.infer[px] = d;
             }
-            if (o.thr_out) o.thr_out[px] = TfgColor{thr_train.x, thr_train.y, thr_train.z};
+            if (o.thr_out && head_query) o.thr_out[px] = TfgColor{thr_train.x, thr_train.y, thr_train.z};
             if (o.reg_counter && o.regs && o.reg_cap > 0) {
                 TfgRegistroEntrenamiento r;
                 r.head = head;
@@ -746,12 +775,12 @@ namespace {
 // concurrently (the branches of a batched multi-scene frame) use different
 // slots; everything else uses slot 0.
 std::mutex g_ws_mutex;
-Workspace g_ws[16][kWorkspaceSlots];
+Workspace g_ws[kMaxDevices][kWorkspaceSlots];
 
 int ensure_workspace(int dev, int slot, size_t paths, bool nrc, Workspace& out) {
     if (slot < 0 || slot >= kWorkspaceSlots) return fail(TFG_E_INVALID, "render: workspace slot out of range");
     std::lock_guard<std::mutex> lk(g_ws_mutex);
-    Workspace& w = g_ws[dev & 15][slot];
+    Workspace& w = g_ws[dev][slot];
     auto grow = [](void** p, size_t bytes) -> cudaError_t {
         if (*p) cudaFree(*p);
         *p = nullptr;
@@ -795,8 +824,8 @@ int ensure_workspace(int dev, int slot, size_t paths, bool nrc, Workspace& out) 
 // Every setting computes the same image; the generation number changes with
 // every set, so captured frame graphs know when to re-capture.
 std::mutex g_tune_mutex;
-TfgRenderTuning g_tune[16];
-bool g_tune_valid[16] = {false};
+TfgRenderTuning g_tune[kMaxDevices];
+bool g_tune_valid[kMaxDevices] = {false};
 uint32_t g_tune_generation = 1;
 
 constexpr int kThreadChoices[3] = {64, 128, 256};
@@ -806,7 +835,7 @@ int threads_index(int t) { return t == 64 ? 0 : t == 256 ? 2 : 1; }
 
 uint32_t workspace_generation(int dev, int slot) {
     std::lock_guard<std::mutex> lk(g_ws_mutex);
-    return g_ws[dev & 15][slot & (kWorkspaceSlots - 1)].generation;
+    return g_ws[dev][slot & (kWorkspaceSlots - 1)].generation;
 }
 
 namespace {
@@ -818,14 +847,16 @@ struct LaunchShapes {
     int shadow_occ[2][2][3] = {};
     int shade_blocks[2] = {0, 0};
 };
-LaunchShapes g_shapes[16];
+LaunchShapes g_shapes[kMaxDevices];
+std::mutex g_shapes_mutex;   // first calls on several host threads fill a device's entry once
 
 size_t trace_smem(int nprims, int threads) {
     return sizeof(uint2) * kSmemStack * (size_t)threads + sizeof(APrim) * (size_t)std::min(nprims, kSmemPrims);
 }
 
 int shapes_for(int dev, LaunchShapes& s) {
-    LaunchShapes& g = g_shapes[dev & 15];
+    std::lock_guard<std::mutex> lk(g_shapes_mutex);
+    LaunchShapes& g = g_shapes[dev];
     if (g.sms == 0) {
         int sms = 0;
         cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
@@ -866,7 +897,7 @@ Tuning resolve_tuning(int dev, uint32_t npix, int spp, bool nrc, uint32_t* gener
     TfgRenderTuning t;
     {
         std::lock_guard<std::mutex> lk(g_tune_mutex);
-        if (g_tune_valid[dev & 15]) t = g_tune[dev & 15];
+        if (g_tune_valid[dev]) t = g_tune[dev];
         else tfgRenderTuningDefault(&t);
         if (generation) *generation = g_tune_generation;
     }
@@ -914,8 +945,8 @@ int render_tuning_check(const TfgRenderTuning& t) {
 int render_tuning_set(int dev, const TfgRenderTuning& t) {
     if (int rc = render_tuning_check(t)) return rc;
     std::lock_guard<std::mutex> lk(g_tune_mutex);
-    g_tune[dev & 15] = t;
-    g_tune_valid[dev & 15] = true;
+    g_tune[dev] = t;
+    g_tune_valid[dev] = true;
     ++g_tune_generation;
     return ok();
 }
@@ -923,7 +954,7 @@ int render_tuning_set(int dev, const TfgRenderTuning& t) {
 int render_tuning_get(int dev, TfgRenderTuning* out, uint32_t* generation) {
     std::lock_guard<std::mutex> lk(g_tune_mutex);
     if (out) {
-        if (g_tune_valid[dev & 15]) *out = g_tune[dev & 15];
+        if (g_tune_valid[dev]) *out = g_tune[dev];
         else tfgRenderTuningDefault(out);
     }
     if (generation) *generation = g_tune_generation;
@@ -1007,7 +1038,7 @@ int render_pass(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPri
 
 int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const TfgPrimitiva* prims, int nprims,
                    const TfgLuzPuntual* lights, int nlights, int W, int H, int frame, const int32_t* frame_dev,
-                   const uint32_t* use_inf_dev, const TfgTinyBVHD_GPU* bvh, const float* tris_wt,
+                   const CachePolicy* policy, const TfgTinyBVHD_GPU* bvh, const float* tris_wt,
                    const TfgPrimitiva* mesh, int nmesh, TfgColor* img, float* accum, TfgRegistroEntrenamiento* regs,
                    uint32_t* reg_counter, int reg_cap, TfgDatosMLP* infer, TfgColor* thr_out, int use_inf, int train,
                    bool prepare_only, int ws_slot, cudaStream_t stream) {
@@ -1044,7 +1075,7 @@ int render_pass_ex(const TfgRenderParams& prm, const TfgCamara* d_cam, const Tfg
     a.mesh = mesh; a.nmesh = nmesh;
     a.cam = d_cam;
     a.frame_dev = frame_dev;
-    a.use_inf_dev = use_inf_dev;
+    if (policy) a.pol = *policy;
     a.W = W; a.H = H;
     a.accum = accum;
     a.regs = regs; a.reg_counter = reg_counter; a.reg_cap = reg_cap;
@@ -1090,7 +1121,7 @@ int render_pass_multi(const TfgRenderParams& prm, const PassScene* scenes, int n
                          : nullptr;
         d.has_bvh = has_bvh ? 1 : 0;
         d.mesh = c.mesh; d.nmesh = c.nmesh;
-        d.cam = c.cam; d.use_inf_dev = c.use_inf_dev; d.use_inf = c.use_inf;
+        d.cam = c.cam; d.pol = c.policy; d.use_inf = c.use_inf;
         d.img = c.img; d.accum = c.accum;
         d.regs = c.regs; d.reg_counter = c.reg_counter; d.reg_cap = c.reg_cap;
         d.infer = c.infer; d.thr_out = c.thr_out;
@@ -1270,7 +1301,7 @@ __global__ void k_camera_rays(const TfgCamara* camp, int W, int H, int frame, in
 
 namespace {
 std::mutex g_fetch_mutex;
-uint32_t* g_fetch[16] = {nullptr};
+uint32_t* g_fetch[kMaxDevices] = {nullptr};
 }
 
 int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const float* rays, int n, float* hits,
@@ -1288,11 +1319,11 @@ int trace_rays(const TfgTinyBVHD_GPU* bvh, const float* tris_wt, int fmt, const 
     uint32_t* fetch;
     {
         std::lock_guard<std::mutex> lk(g_fetch_mutex);
-        if (!g_fetch[dev & 15]) {
-            e = cudaMalloc((void**)&g_fetch[dev & 15], sizeof(uint32_t));
+        if (!g_fetch[dev]) {
+            e = cudaMalloc((void**)&g_fetch[dev], sizeof(uint32_t));
             if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
         }
-        fetch = g_fetch[dev & 15];
+        fetch = g_fetch[dev];
     }
     LaunchShapes sh;
     shapes_for(dev, sh);
@@ -1364,6 +1395,7 @@ extern "C" int tfgRenderTuningSet(const TfgRenderTuning* t) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return tfg::fail((int)e, cudaGetErrorString(e));
+    if (int rc = tfg::require_sm100(dev)) return rc;
     return tfg::render_tuning_set(dev, *t);
 }
 
@@ -1372,6 +1404,7 @@ extern "C" int tfgRenderTuningGet(TfgRenderTuning* out) {
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return tfg::fail((int)e, cudaGetErrorString(e));
+    if (int rc = tfg::require_sm100(dev)) return rc;
     return tfg::render_tuning_get(dev, out, nullptr);
 }
 
@@ -1484,19 +1517,19 @@ constexpr size_t kStaticBytes = kStaticPaths * kStaticPathBytes + kStaticCounter
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 
 std::mutex g_static_mutex;
-unsigned char* g_static_base[16] = {nullptr};
+unsigned char* g_static_base[kMaxDevices] = {nullptr};
 
 // Device address of g_static_scratch for the current device, looked up once
 // per device (the array's name is only a host-side stand-in in host code).
 int static_scratch(int dev, unsigned char** out) {
     std::lock_guard<std::mutex> lk(g_static_mutex);
-    if (!g_static_base[dev & 15]) {
+    if (!g_static_base[dev]) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_static_scratch);
         if (e != cudaSuccess) return fail((int)e, std::string("tfgRenderPassStatic: scratch address: ") + cudaGetErrorString(e));
-        g_static_base[dev & 15] = static_cast<unsigned char*>(p);
+        g_static_base[dev] = static_cast<unsigned char*>(p);
     }
-    *out = g_static_base[dev & 15];
+    *out = g_static_base[dev];
     return ok();
 }
 

@@ -28,8 +28,11 @@ int fail(int code, const std::string& msg) {
 int ok() { return 0; }
 
 int require_sm100(int dev) {
-    static int checked[16] = {0};   // 0 unknown, 1 ok, 2 bad
-    int& c = checked[dev & 15];
+    if (dev < 0 || dev >= kMaxDevices)
+        return fail(TFG_E_INVALID, "device ordinal " + std::to_string(dev) + " is out of range: the library keeps "
+                                   "per-device state for ordinals 0-" + std::to_string(kMaxDevices - 1));
+    static int checked[kMaxDevices] = {0};   // 0 unknown, 1 ok, 2 bad
+    int& c = checked[dev];
     if (c == 0) {
         int major = 0;
         cudaError_t e = cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);

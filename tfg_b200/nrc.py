@@ -159,6 +159,15 @@ class ColorMLP:
         return {"wgrad_tiles_per_cta": int(t.wgrad_tiles_per_cta), "infer_ctas": int(t.infer_ctas),
                 "wgrad_ms": float(ms[0]), "infer_ms": float(ms[1])}
 
+    def encode_features(self, datos: torch.Tensor, n: int, training: bool = False, stream=None) -> torch.Tensor:
+        """tfgMlpEncodeFeatures: the (n, 96) layer-0 operands the cache kernels
+        compute for n queries -- the training forward pass's FP16 features, or
+        inference's at the model's precision (FP16 / BF16)."""
+        out = torch.empty(max(n, 1) * 96, dtype=torch.float32, device=datos.device)
+        _lib.call("tfgMlpEncodeFeatures", self.h, datos.data_ptr(), int(n), 0 if training else 1, out.data_ptr(),
+                  _stream(stream))
+        return out[:n * 96].view(n, 96)
+
     def inference_composite(self, datos: torch.Tensor, thr: torch.Tensor, img: torch.Tensor, n: int,
                             stream=None) -> None:
         _lib.call("tfgMlpInferenceComposite", self.h, datos.data_ptr(), thr.data_ptr(), img.data_ptr(), int(n),
@@ -239,7 +248,11 @@ class NrcRenderer:
     answers and composites the queries, bootstraps targets and trains."""
 
     def __init__(self, ds, mlp: ColorMLP, params, train_steps: int = 4, max_records: int = 65536,
-                 min_records: int = 1024, gate_threshold: float = 0.0, use_graph: bool = True, stream=None):
+                 min_records: int = 1024, gate_threshold: float = 0.0, use_graph: bool = True, stream=None,
+                 footprint: float | None = None, train_fraction: float | None = None):
+        """`footprint` / `train_fraction` override the reference's cache
+        policy (0.01 and 0.05, render.h:102 and :443); `gate_threshold` > 0
+        turns on the per-cell gate judged by the path tracer."""
         self.ds, self.mlp, self.params = ds, mlp, params
         W, H = ds.scene.width, ds.scene.height
         dev = ds.device
@@ -260,6 +273,10 @@ class NrcRenderer:
         _lib.lib.tfgNrcFrameConfigReference(ctypes.byref(self.cfg))
         self.cfg.train_steps, self.cfg.max_records, self.cfg.min_records = train_steps, max_records, min_records
         self.cfg.gate_threshold, self.cfg.use_graph = gate_threshold, int(use_graph)
+        if footprint is not None:
+            self.cfg.footprint = footprint
+        if train_fraction is not None:
+            self.cfg.train_fraction = train_fraction
         self.bufs = CNrcBuffers(self.img.data_ptr(), self.accum.data_ptr(), self.infer.data_ptr(),
                                 self.thr.data_ptr(), self.regs.data_ptr(), self.counter.data_ptr(), self.ring_cap, 0,
                                 self.tail_in.data_ptr(), self.tail_pred.data_ptr(), self.train_buf.data_ptr())

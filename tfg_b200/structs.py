@@ -141,7 +141,8 @@ assert ctypes.sizeof(CTinyBVHD_GPU) == 24 and ctypes.sizeof(CImagenGPU) == 16
 
 class CNrcFrameConfig(ctypes.Structure):
     _fields_ = [("train_steps", ctypes.c_int32), ("max_records", ctypes.c_uint32), ("min_records", ctypes.c_uint32),
-                ("warmup", ctypes.c_int32), ("gate_threshold", ctypes.c_float), ("use_graph", ctypes.c_int32)]
+                ("warmup", ctypes.c_int32), ("gate_threshold", ctypes.c_float), ("use_graph", ctypes.c_int32),
+                ("footprint", ctypes.c_float), ("train_fraction", ctypes.c_float)]
 
 
 class CNrcBuffers(ctypes.Structure):
