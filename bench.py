@@ -37,6 +37,52 @@ WORKLOAD = "plain path tracing, 1920x1080, 64 spp, depth 8, RR from depth 3, 16 
 TRACE_DRAM_BYTES_PER_LAUNCH = {1: 38_063_296, 16: 505_144_128}
 
 
+# ncu counters of the closest-hit kernel on the bench frame (one-sample pass,
+# launches of bounce 0 and 1; profiles/k_trace_l2_issue_1080p.md): L2 bytes
+# (lts__t_bytes.sum) per closest-hit ray traced, the share of issue slots
+# used (sm__inst_issued.avg.per_cycle_active / 4) and the SIMT efficiency
+# (smsp__thread_inst_executed_per_inst_executed.ratio / 32), weighted by the
+# launches' durations.
+TRACE_L2_BYTES_PER_RAY = None
+TRACE_ISSUE_FRAC = None
+TRACE_SIMT_EFFICIENCY = None
+
+
+def l2_gather_peak(dev) -> dict:
+    """Random-gather bandwidth of L2 (tfgL2GatherPass): 80-byte records at
+    hashed indices of a 64 MiB table (L2-resident, as the benchmark scene's
+    CWBVH is), 1184 x 256 threads x 256 reads per pass, best of 10 passes
+    timed with CUDA events after 3 warm-ups."""
+    import torch
+
+    from tfg_b200 import _lib
+    records = (64 << 20) // 80
+    table = torch.randint(0, 1 << 30, (records * 20,), dtype=torch.int32, device=dev)
+    sink = torch.zeros(1, dtype=torch.int32, device=dev)
+    blocks, reads = 148 * 8, 256
+    stream = torch.cuda.current_stream()
+
+    def one(seed):
+        _lib.call("tfgL2GatherPass", table.data_ptr(), records, reads, seed, sink.data_ptr(), blocks,
+                  stream.cuda_stream)
+
+    for k in range(3):
+        one(k)
+    torch.cuda.synchronize()
+    best = float("inf")
+    for k in range(10):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        one(100 + k)
+        e1.record(stream)
+        e1.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    nbytes = 80.0 * blocks * 256 * reads
+    del table
+    return {"gbs": round(nbytes / (best * 1e-3) / 1e9, 1), "ms": round(best, 4), "bytes": int(nbytes),
+            "how": "80 B records at hashed indices of a 64 MiB table, 1184 x 256 threads x 256 reads, best of 10"}
+
+
 def trace_traffic(wavefront_paths: int, n_px: int):
     k = max(1, wavefront_paths // n_px) if wavefront_paths else 1
     return TRACE_DRAM_BYTES_PER_LAUNCH.get(k)
@@ -1001,6 +1047,9 @@ def main():
     trace_launches = prof["launches"]["trace"]
     rays_timed = rays_per_spp * SPP * args.steps
     achieved = rays_timed * bytes_per_ray / (trace_ms * 1e-3) / 1e9 if trace_ms > 0 else None
+    l2_achieved = (rays_timed * TRACE_L2_BYTES_PER_RAY / (trace_ms * 1e-3) / 1e9
+                   if trace_ms > 0 and TRACE_L2_BYTES_PER_RAY else None)
+    l2_peak = l2_gather_peak(dev)
     launches = sum(prof["launches"].values())
     clocks = clk.summary()
 
@@ -1034,6 +1083,15 @@ def main():
                 "wall_ms_per_step": round(wall_ms / e2e_steps, 3), "call": "tfgRenderPass"},
         "roofline": {
             "kernel": "k_trace (CWBVH closest hit)", "bound": "hbm",
+            # What limits k_trace: its scene is L2-resident and it is issue-bound with half of each
+            # warp's lanes active (divergent node counts per ray); the HBM fraction above is the
+            # contract's figure, the L2 and issue fractions below say how far the kernel is from a roof.
+            "limiter": "instruction issue with divergent lanes (L2-resident scene)",
+            "l2_gbs": round(l2_achieved, 1) if l2_achieved else None,
+            "l2_peak_gbs": l2_peak["gbs"], "l2_peak_how": l2_peak["how"],
+            "l2_frac": round(l2_achieved / l2_peak["gbs"], 4) if l2_achieved else None,
+            "l2_bytes_per_ray": TRACE_L2_BYTES_PER_RAY,
+            "issue_frac": TRACE_ISSUE_FRAC, "simt_efficiency": TRACE_SIMT_EFFICIENCY,
             "achieved": round(achieved, 1) if achieved else None,
             "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,

@@ -336,7 +336,10 @@ typedef struct TfgRenderTuning {
     int32_t trace_warps_per_sm; /* resident traversal warps per SM; 0 (default) = as many as fit */
     int32_t refill_min;         /* idle lanes that make a traversal warp fetch new rays, 1..32 (default 8) */
     int32_t shadow_one_lane;    /* threads per shadow query: 0 (default) = one lane per light (up to 32
-                                   lights), 1 = one lane traces all lights of a shading point */
+                                   lights), 1 = one lane traces all lights of a shading point, 2 = as 1 on
+                                   persistent lanes: a lane's traversal advances one node per iteration
+                                   and the lane takes a new shading point once refill_min lanes of its
+                                   warp are idle.  Every form adds the same terms in light order */
     int32_t refill_min_primary; /* refill threshold of the first bounce's traversal (camera rays, coherent
                                    in 8 x 4 pixel tiles; 32 = whole-warp batches), 0 (default) = refill_min */
     int32_t overlap_shadow;     /* 1 (default): each bounce's shadow rays run on a second stream beside the
@@ -569,6 +572,14 @@ int  tfgMlpComputeGradient(TfgColorMLP* mlp, const TfgDatosMLP* buffer, uint32_t
  * returns what a stuck cache kernel would: TFG_E_TIMEOUT (the flag is cleared
  * and the context stays usable).  Every real wait gives up after 1 s. */
 int  tfgMlpSelfTestWait(uint32_t timeout_us);
+/* Roofline probe for the traversal stages (no reference counterpart): every
+ * thread of `blocks` x 256 reads `reads_per_thread` records of 80 bytes (five
+ * 16-byte loads, a CWBVH node's size) at hashed, independent indices of the
+ * device `table` of `records` records (16-byte aligned), so that an
+ * L2-resident table gives the random-gather bandwidth of L2.  `sink` is a
+ * device word the kernel may write; time the call with events. */
+int  tfgL2GatherPass(const void* table, uint32_t records, uint32_t reads_per_thread, uint32_t seed, uint32_t* sink,
+                     int32_t blocks, void* stream);
 /* How a model's kernels tile their batches (no reference counterpart).
  * Every setting computes the same values up to the order of FP32 gradient
  * additions. */

@@ -43,3 +43,81 @@ def oracle_image(orc, scene, hb, frame, prm=None, nthreads=8, use_inf=0, train=0
     if want_nrc:
         return img, infer, thr, regs, flags
     return img
+
+
+# ---------------------------------------------------------------- cache-network parity
+# The cache kernels are checked against an FP64 model that applies their own
+# roundings to their own layer-0 operands (tfgMlpEncodeFeatures): FP16 / BF16
+# weights and hidden activations in inference; in training an FP16 forward
+# pass, BF16 loss and layer-output gradients, BF16 backward weights and
+# BF16-rounded layer inputs for the weight gradients.  What is left is the
+# order of the FP32 sums, and an activation that lands on the other side of a
+# rounding boundary than in the model.
+INFER_MAX = 2e-3      # largest |kernel - model| / mean |model output|
+INFER_MEAN = 2e-4
+GRAD_REL = 1e-2       # per layer: |g - model|_2 / |model|_2
+LOSS_REL = 1e-3
+
+
+def cache_inference_error(mlp, datos_dev, n, got, kind="f16"):
+    """(max, mean) of |got - model| / mean|model| for inference of n queries."""
+    import numpy as np
+
+    from oracle import mlp_oracle as mo
+    from tfg_b200.nrc import EMA, WEIGHTS, split_layers
+    x = mlp.encode_features(datos_dev, n).cpu().numpy().astype(np.float64)
+    st = mlp.state()
+    if st["adam_t"] > 0:
+        # inference reads the weight average debiased by 1 - decay^t, rounded to FP32
+        w = (mlp.get_params(EMA) / np.float32(1.0 - 0.99 ** st["adam_t"])).astype(np.float32)
+    else:
+        w = mlp.get_params(WEIGHTS)
+    raw = mo.forward_operands(split_layers(w), x, kind)
+    want = mo.scrub(raw)
+    scale = np.abs(raw).mean() + 1e-3
+    err = np.abs(np.asarray(got, np.float64) - want) / scale
+    return float(err.max()), float(err.mean())
+
+
+def kchunk_columns(cols: int) -> list[int]:
+    """Columns on either side of every 16-feature boundary of a K dimension
+    (one tcgen05 MMA of 16-bit operands covers 16 features)."""
+    out = []
+    for b in range(16, cols, 16):
+        out += [b - 1, b]
+    return out
+
+
+def check_cache_gradients(mlp, sel_dev, y, g, loss, bias_col: int, g_table=None, corners=None,
+                          table_cols: int = 0, tol_rel=GRAD_REL):
+    """Layer gradients (and the hash-grid table gradient) of one training
+    batch against the operand model; `sel_dev` holds the batch's samples in
+    the order the kernel drew them.  Element-wise on the bias column of layer
+    0 and on every K-chunk boundary column: |g - model| <= 0.05 |model| +
+    0.01 rms(layer)."""
+    import numpy as np
+
+    from oracle import mlp_oracle as mo
+    from tfg_b200.nrc import WEIGHTS, split_layers
+    n = len(y)
+    x = mlp.encode_features(sel_dev, n, training=True).cpu().numpy().astype(np.float64)
+    W = split_layers(mlp.get_params(WEIGHTS))
+    ref_loss, ref, dx = mo.loss_and_grad_operands(W, x, y)
+    assert abs(loss - ref_loss) / ref_loss < LOSS_REL, (loss, ref_loss)
+    report = []
+    for l, (gg, rr) in enumerate(zip(split_layers(g), ref)):
+        rel = float(np.linalg.norm(gg - rr) / (np.linalg.norm(rr) + 1e-30))
+        report.append(rel)
+        assert rel < tol_rel, f"layer {l}: relative gradient error {rel:.3e} (all: {report})"
+        rms = float(np.sqrt(np.mean(rr ** 2)))
+        cols = kchunk_columns(rr.shape[1]) + ([bias_col] if l == 0 else [])
+        d = np.abs(gg[:, cols] - rr[:, cols])
+        bound = 0.05 * np.abs(rr[:, cols]) + 0.01 * rms
+        assert (d <= bound).all(), f"layer {l}: column check, worst {float((d - bound).max()):.3e} over rms {rms:.3e}"
+    if g_table is not None:
+        ref_t = mo.table_grad(dx[:, :table_cols], corners, len(g_table))
+        rel = float(np.linalg.norm(g_table - ref_t) / np.linalg.norm(ref_t))
+        report.append(rel)
+        assert rel < tol_rel, f"table gradient: relative error {rel:.3e}"
+        assert (g_table[ref_t == 0] == 0).all()
+    return report

@@ -8,6 +8,7 @@ import torch
 
 from oracle import mlp_oracle as mo
 from oracle import oracle as orc
+from tests.helpers import INFER_MAX, INFER_MEAN, cache_inference_error, check_cache_gradients
 from tfg_b200 import TfgError
 from tfg_b200 import pathtracer as pt
 from tfg_b200 import scenes
@@ -62,18 +63,16 @@ def test_inference_matches_fp64_model(built, hidden):
     x = mo.encode(mo.rows15(d, LO, HI))
     raw = mo.forward(W, x)[0]
     scale = np.abs(raw).mean() + 1e-3
-    err = np.abs(got - mo.scrub(raw)) / scale
     assert np.isfinite(got).all()
-    assert err.max() < 0.05, f"max scaled error {err.max():.3e}"
-    assert err.mean() < 0.01
-    # BF16 against the BF16-rounded model
+    emax, emean = cache_inference_error(m, _dev(d), n, got)
+    assert emax < INFER_MAX and emean < INFER_MEAN, (emax, emean)
+    # BF16 against the model with BF16 weights and activations on the kernel's BF16 operands
     m.set_precision(BF16)
     b = torch.zeros(n * 3, device="cuda")
     m.inference(_dev(d), b, n)
     torch.cuda.synchronize()
-    ref_b = mo.scrub(mo.forward_quantized(W, x, "bf16"))
-    eb = np.abs(b.view(n, 3).cpu().numpy() - ref_b).mean() / scale
-    assert eb < 0.01, eb
+    emax, emean = cache_inference_error(m, _dev(d), n, b.view(n, 3).cpu().numpy(), kind="bf16")
+    assert emax < 4 * INFER_MAX and emean < 4 * INFER_MEAN, (emax, emean)
     # FP8 (E4M3, per-layer scales from a calibration pass) against the exact
     # E4M3 pipeline of the oracle, as for width 64; with 7 hidden layers the
     # E4M3 image stays resident while the FP16 calibration pass streams
@@ -102,25 +101,19 @@ def test_inference_matches_fp64_model(built, hidden):
     m.close()
 
 
-@pytest.mark.parametrize("hidden", [5, 7])
+@pytest.mark.parametrize("hidden", [3, 5, 7])
 def test_gradient_matches_fp64_model(built, hidden):
     m = ColorMLP(batch=4096, seed=7, width=128, hidden_layers=hidden)
     m.set_bounds(LO, HI)
     rng = np.random.default_rng(11)
     n_avail = 20000
     d = _datos(rng, n_avail)
-    w = m.get_params(WEIGHTS)
     g, loss = m.compute_gradient(_dev(d), n_avail, seed=5)
     idx = np.zeros(m.batch, np.int32)
     orc.cpu.orc_indices(orc.p(idx), n_avail, m.batch, 5)
     sel = d[idx]
-    x = mo.encode(mo.rows15(sel, LO, HI))
     y = np.stack([sel["color"][k] for k in "rgb"], 1).astype(np.float64)
-    ref_loss, ref = mo.loss_and_grad([_f16(a) for a in split_layers(w)], x, y)
-    assert abs(loss - ref_loss) / ref_loss < 0.02, (loss, ref_loss)
-    for l, (gg, rr) in enumerate(zip(split_layers(g), ref)):
-        rel = np.linalg.norm(gg - rr) / (np.linalg.norm(rr) + 1e-30)
-        assert rel < 0.05, f"layer {l}: relative gradient error {rel:.3e}"
+    check_cache_gradients(m, _dev(sel), y, g, loss, bias_col=84)
     m.close()
 
 
@@ -131,22 +124,15 @@ def test_composite_encoding_gradients(built):
     m.set_table(rng.uniform(-0.5, 0.5, m.n_table).astype(np.float32))
     n_avail = 20000
     d = _datos(rng, n_avail)
-    w = m.get_params(WEIGHTS)
     tab = m.get_table(WEIGHTS).astype(np.float64)
     g, gt, loss = m.compute_gradient_ex(_dev(d), n_avail, seed=3)
     idx = np.zeros(m.batch, np.int32)
     orc.cpu.orc_indices(orc.p(idx), n_avail, m.batch, 3)
     sel = d[idx]
-    x, corners = mo.composite_encode(mo.rows15(sel, LO, HI), tab, SMALL)
+    _, corners = mo.composite_encode(mo.rows15(sel, LO, HI), tab, SMALL)
     y = np.stack([sel["color"][k] for k in "rgb"], 1).astype(np.float64)
-    ref_loss, ref, dx = mo.loss_and_grad([_f16(a) for a in split_layers(w)], x, y, want_dx=True)
-    assert abs(loss - ref_loss) / ref_loss < 0.02, (loss, ref_loss)
-    for l, (gg, rr) in enumerate(zip(split_layers(g), ref)):
-        rel = np.linalg.norm(gg - rr) / (np.linalg.norm(rr) + 1e-30)
-        assert rel < 0.05, f"layer {l}: relative gradient error {rel:.3e}"
-    ref_t = mo.table_grad(dx[:, :2 * SMALL["n_levels"]], corners, m.n_table)
-    rel = np.linalg.norm(gt - ref_t) / np.linalg.norm(ref_t)
-    assert rel < 0.05, f"table gradient: relative error {rel:.3e}"
+    check_cache_gradients(m, _dev(sel), y, g, loss, bias_col=62, g_table=gt, corners=corners,
+                          table_cols=2 * SMALL["n_levels"])
     m.close()
 
 
@@ -219,5 +205,7 @@ def test_seven_layer_hash_grid_inference_matches_fp64_model(built):
     scale = np.abs(raw).mean() + 1e-3
     err = np.abs(got - mo.scrub(raw)) / scale
     assert np.isfinite(got).all()
-    assert err.max() < 0.05 and err.mean() < 0.01, (err.max(), err.mean())
+    assert err.max() < 0.02 and err.mean() < 2e-3, (err.max(), err.mean())
+    emax, emean = cache_inference_error(m, _dev(d), n, got)
+    assert emax < INFER_MAX and emean < INFER_MEAN, (emax, emean)
     m.close()

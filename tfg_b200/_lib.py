@@ -107,6 +107,7 @@ _PROTOS = {
     "tfgWritePPM": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
     "tfgWritePFM": (c_int32, [c_char_p, c_void_p, c_int32, c_int32]),
     "tfgMlpSelfTestWait": (c_int32, [c_uint32]),
+    "tfgL2GatherPass": (c_int32, [c_void_p, c_uint32, c_uint32, c_uint32, c_void_p, c_int32, c_void_p]),
     "tfgMlpSetPrecision": (c_int32, [c_void_p, c_int32]),
     "tfgMlpCalibrate": (c_int32, [c_void_p, c_void_p, c_uint32, c_void_p]),
     "tfgMlpInferenceComposite": (c_int32, [c_void_p, c_void_p, c_void_p, c_void_p, c_uint32, c_void_p]),

@@ -602,6 +602,58 @@ __global__ void __launch_bounds__(256) k_shade(PassArgs a, int bounce, TableOf<M
 // escenario.h:144-184: every light in order, Lambert BRDF kd/pi, inverse-square
 // falloff with the distance clamped to >= 1, summed then scaled by the path
 // throughput (render.h:128-130).
+
+__device__ __forceinline__ float dot_rn(V3 a, V3 b) {
+    return __fadd_rn(__fadd_rn(__fmul_rn(a.x, b.x), __fmul_rn(a.y, b.y)), __fmul_rn(a.z, b.z));
+}
+
+// One light of a shading point: the shadow ray (origin nudged off the
+// surface, unit direction, length) and the term the light adds when nothing
+// occludes it, I / max(d, 1)^2 * kd / pi * cos.  False when the light is
+// behind the surface.  Every operation is rounded on its own, so all shadow
+// kernels compute the same rays and terms whatever the compiler fuses around
+// them.
+struct LightRay {
+    V3 so, dl, term;
+    float dist;
+};
+__device__ __forceinline__ bool light_ray(const TfgLuzPuntual& lz, V3 P, V3 N, V3 kd, LightRay& s) {
+    const V3 lp = ld3(lz.posicion);
+    V3 dl = v3(__fsub_rn(lp.x, P.x), __fsub_rn(lp.y, P.y), __fsub_rn(lp.z, P.z));
+    const float dist = __fsqrt_rn(dot_rn(dl, dl));
+    if (dist > 0.0f) {
+        const float inv = __fdiv_rn(1.0f, dist);
+        dl = v3(__fmul_rn(dl.x, inv), __fmul_rn(dl.y, inv), __fmul_rn(dl.z, inv));
+    }
+    const float c = dot_rn(N, dl);
+    if (!(c > 0.0f)) return false;
+    s.so = v3(__fadd_rn(P.x, __fmul_rn(dl.x, kEps)), __fadd_rn(P.y, __fmul_rn(dl.y, kEps)),
+              __fadd_rn(P.z, __fmul_rn(dl.z, kEps)));
+    s.dl = dl;
+    s.dist = dist;
+    const float dd = fmaxf(dist, 1.0f), d2 = __fmul_rn(dd, dd);
+    s.term = v3(__fmul_rn(__fmul_rn(__fdiv_rn(lz.intensidad.r, d2), __fdiv_rn(kd.x, kPiF)), c),
+                __fmul_rn(__fmul_rn(__fdiv_rn(lz.intensidad.g, d2), __fdiv_rn(kd.y, kPiF)), c),
+                __fmul_rn(__fmul_rn(__fdiv_rn(lz.intensidad.b, d2), __fdiv_rn(kd.z, kPiF)), c));
+    return true;
+}
+
+// The shading point's radiance (throughput x light sum) into the path's
+// prefix and / or suffix radiance (dest bit 0: suffix; not 1: prefix too).
+__device__ __forceinline__ void add_direct(const PassArgs& a, uint32_t p, uint32_t dest, V3 cam, V3 L) {
+    const V3 add = mul(cam, L);
+    if (dest & 1u) {
+        float4 v = a.ws.lsuf[p];
+        v.x += add.x; v.y += add.y; v.z += add.z;
+        a.ws.lsuf[p] = v;
+    }
+    if (dest != 1u) {
+        float4 v = a.ws.lpre[p];
+        v.x += add.x; v.y += add.y; v.z += add.z;
+        a.ws.lpre[p] = v;
+    }
+}
+
 template <int TRI_FMT, bool STATS, bool MS>
 __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<MS> tab) {
     extern __shared__ unsigned char smem_raw[];
@@ -647,30 +699,20 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
             int lend = l_end;
             if constexpr (MS) { lights = tab.s[sc].lights; lend = tab.s[sc].nlights; }
             for (int l = l_begin; l < lend; ++l) {
-                const TfgLuzPuntual lz = lights[l];
-                V3 dl = ld3(lz.posicion) - P;
-                float dist = sqrtf(dot(dl, dl));
-                dl = normalized(dl);
-                const float c = dot(N, dl);
-                if (c <= 0.0f) continue;
-                const V3 so = P + dl * kEps;
+                LightRay lr;
+                if (!light_ray(lights[l], P, N, kd, lr)) continue;
                 if (STATS) ++nrays;
-                if (analytic_any(sprims, nsm, g.prims, g.nprims, so, dl, dist)) continue;
+                if (analytic_any(sprims, nsm, g.prims, g.nprims, lr.so, lr.dl, lr.dist)) continue;
                 if (a.shadow_mesh && g.has_bvh) {
-                    float tm = dist, hu, hv;
+                    float tm = lr.dist, hu, hv;
                     uint32_t hid;
-                    if (cwbvh_trace<TRI_FMT, true>(g.nodes, g.tris, so, dl, kEps, tm, hid, hu, hv, stck,
+                    if (cwbvh_trace<TRI_FMT, true>(g.nodes, g.tris, lr.so, lr.dl, kEps, tm, hid, hu, hv, stck,
                                                    STATS ? &cnt : nullptr)) continue;
                 }
-                const V3 kdpi = v3(kd.x / kPiF, kd.y / kPiF, kd.z / kPiF);
-                dist = fmaxf(dist, 1.0f);
-                const float d2 = dist * dist;
-                const V3 Li = v3(lz.intensidad.r / d2, lz.intensidad.g / d2, lz.intensidad.b / d2);
-                // Each light's term is rounded before it is added (no fused
-                // multiply-add), so one lane looping over the lights sums the
-                // same values in the same order as the lanes of a group.
-                const V3 term = mul(Li, kdpi) * c;
-                L = v3(__fadd_rn(L.x, term.x), __fadd_rn(L.y, term.y), __fadd_rn(L.z, term.z));
+                // Each light's term is rounded before it is added, so one lane
+                // looping over the lights sums the same values in the same
+                // order as the lanes of a group.
+                L = v3(__fadd_rn(L.x, lr.term.x), __fadd_rn(L.y, lr.term.y), __fadd_rn(L.z, lr.term.z));
             }
         }
         // Sum the group's lights in light order on its first lane (an occluded
@@ -681,18 +723,93 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
             const float z = __shfl_sync(0xFFFFFFFFu, L.z, group0 + j);
             if (lg == 0u && (int)j < nl) L = L + v3(x, y, z);
         }
-        if (have && lg == 0u) {
-            const V3 add = mul(cam, L);
-            if (dest & 1u) {
-                float4 v = a.ws.lsuf[p];
-                v.x += add.x; v.y += add.y; v.z += add.z;
-                a.ws.lsuf[p] = v;
+        if (have && lg == 0u) add_direct(a, p, dest, cam, L);
+    }
+    if (STATS) flush_work(3, nrays, cnt);
+}
+
+// Shadow rays on persistent lanes (shadow_one_lane 2): a lane owns one
+// shading point and traces its lights one after another, exactly as the
+// one-lane form does (same rays, same terms added in light order), but its
+// traversal advances one node per iteration and the lane takes a new shading
+// point as soon as `refill_min` lanes of its warp are idle, instead of
+// waiting for the warp's slowest shadow ray.
+template <int TRI_FMT, bool STATS, bool MS>
+__global__ void __launch_bounds__(256) k_shadow_pl(PassArgs a, int bounce, TableOf<MS> tab) {
+    extern __shared__ unsigned char smem_raw[];
+    uint2* sstack = reinterpret_cast<uint2*>(smem_raw);
+    APrim* sprims = reinterpret_cast<APrim*>(smem_raw + sizeof(uint2) * kSmemStack * blockDim.x);
+    const int nsm = MS ? 0 : load_aprims_smem(sprims, a.prims, a.nprims);
+    TravStack stck;
+    stck.smem = sstack; stck.stride = blockDim.x; stck.tid = threadIdx.x;
+    const uint32_t n = a.ws.counters[4 * bounce + 2];
+    uint32_t* fetch = &a.ws.counters[4 * bounce + 3];
+    TravCounts cnt;
+    uint32_t nrays = 0;
+    const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
+    CwbvhRay<TRI_FMT, true> r;
+    uint32_t cur = kMissId, p = 0, dest = 0;
+    int l = 0, lend = 0;
+    bool tracing = false, exhausted = false;
+    V3 P = v3(0, 0, 0), N = P, kd = P, cam = P, L = P, pending = P;
+    Geo g = geo_of<MS>(a, tab, 0);
+    const TfgLuzPuntual* lights = a.lights;
+    while (true) {
+        const bool idle = cur == kMissId;
+        const uint32_t im = __ballot_sync(0xFFFFFFFFu, idle);
+        if (exhausted) {
+            if (im == 0xFFFFFFFFu) break;
+        } else if (__popc(im) >= a.refill_min) {
+            uint32_t base = 0;
+            if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(im));
+            base = __shfl_sync(0xFFFFFFFFu, base, 0);
+            exhausted = base + (uint32_t)__popc(im) >= n;
+            const uint32_t k = base + (uint32_t)__popc(im & lt);
+            if (idle && k < n) {
+                cur = k;
+                const float4* s = &a.ws.shadow[4 * (size_t)k];
+                const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
+                P = xyz(s0); N = xyz(s1); kd = xyz(s2); cam = xyz(s3);
+                p = __float_as_uint(s0.w);
+                dest = __float_as_uint(s1.w);
+                lights = a.lights;
+                lend = a.nlights;
+                if constexpr (MS) {
+                    const uint32_t sc = __float_as_uint(s2.w);
+                    g = geo_of<MS>(a, tab, sc);
+                    lights = tab.s[sc].lights;
+                    lend = tab.s[sc].nlights;
+                }
+                l = 0;
+                L = v3(0.0f, 0.0f, 0.0f);
             }
-            if (dest != 1u) {
-                float4 v = a.ws.lpre[p];
-                v.x += add.x; v.y += add.y; v.z += add.z;
-                a.ws.lpre[p] = v;
+        }
+        if (cur == kMissId) continue;
+        if (tracing) {
+            if (r.step(g.nodes, g.tris, stck)) continue;   // one node per iteration
+            tracing = false;
+            if (STATS) { cnt.nodes += r.nsteps; cnt.tris += r.ntris; }
+            if (!r.found) L = v3(__fadd_rn(L.x, pending.x), __fadd_rn(L.y, pending.y), __fadd_rn(L.z, pending.z));
+            ++l;
+        }
+        // The next light that needs a mesh test; lights behind the surface or
+        // blocked by an analytic primitive settle here.
+        for (; l < lend; ++l) {
+            LightRay lr;
+            if (!light_ray(lights[l], P, N, kd, lr)) continue;
+            if (STATS) ++nrays;
+            if (analytic_any(sprims, nsm, g.prims, g.nprims, lr.so, lr.dl, lr.dist)) continue;
+            if (a.shadow_mesh && g.has_bvh) {
+                r.init(lr.so, lr.dl, kEps, lr.dist);
+                pending = lr.term;
+                tracing = true;
+                break;
             }
+            L = v3(__fadd_rn(L.x, lr.term.x), __fadd_rn(L.y, lr.term.y), __fadd_rn(L.z, lr.term.z));
+        }
+        if (!tracing) {
+            add_direct(a, p, dest, cam, L);
+            cur = kMissId;
         }
     }
     if (STATS) flush_work(3, nrays, cnt);
@@ -845,6 +962,7 @@ struct LaunchShapes {
     // resident CTAs per SM: [one scene / batch][triangle format][64, 128, 256 threads]
     int trace_occ[2][2][3] = {};
     int shadow_occ[2][2][3] = {};
+    int shadow_pl_occ[2][2][3] = {};
     int shade_blocks[2] = {0, 0};
 };
 LaunchShapes g_shapes[kMaxDevices];
@@ -876,6 +994,10 @@ int shapes_for(int dev, LaunchShapes& s) {
             g.trace_occ[1][1][k] = occ_of(k_trace<1, false, true>, bt, sm_ms);
             g.shadow_occ[1][0][k] = occ_of(k_shadow<0, false, true>, bt, sm_ms);
             g.shadow_occ[1][1][k] = occ_of(k_shadow<1, false, true>, bt, sm_ms);
+            g.shadow_pl_occ[0][0][k] = occ_of(k_shadow_pl<0, false, false>, bt, sm);
+            g.shadow_pl_occ[0][1][k] = occ_of(k_shadow_pl<1, false, false>, bt, sm);
+            g.shadow_pl_occ[1][0][k] = occ_of(k_shadow_pl<0, false, true>, bt, sm_ms);
+            g.shadow_pl_occ[1][1][k] = occ_of(k_shadow_pl<1, false, true>, bt, sm_ms);
         }
         g.shade_blocks[0] = sms * occ_of(k_shade<false>, 256, 0);
         g.shade_blocks[1] = sms * occ_of(k_shade<true>, 256, 0);
@@ -933,8 +1055,8 @@ int render_tuning_check(const TfgRenderTuning& t) {
     if (t.trace_warps_per_sm < 0 || t.trace_warps_per_sm > 64)
         return fail(TFG_E_INVALID, "render tuning: trace_warps_per_sm must be in [0, 64]");
     if (t.refill_min < 1 || t.refill_min > 32) return fail(TFG_E_INVALID, "render tuning: refill_min must be in [1, 32]");
-    if (t.shadow_one_lane != 0 && t.shadow_one_lane != 1)
-        return fail(TFG_E_INVALID, "render tuning: shadow_one_lane must be 0 or 1");
+    if (t.shadow_one_lane < 0 || t.shadow_one_lane > 2)
+        return fail(TFG_E_INVALID, "render tuning: shadow_one_lane must be 0, 1 or 2");
     if (t.refill_min_primary < 0 || t.refill_min_primary > 32)
         return fail(TFG_E_INVALID, "render tuning: refill_min_primary must be in [0, 32]");
     if (t.overlap_shadow != 0 && t.overlap_shadow != 1)
@@ -1166,6 +1288,7 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
     const size_t smem = trace_smem(MS ? 0 : a.nprims, bt);
     const int trace_grid = persistent_grid(sh, sh.trace_occ[MS][fmt][ti], tu);
     const int shadow_grid = persistent_grid(sh, sh.shadow_occ[MS][fmt][ti], tu);
+    const int shadow_pl_grid = persistent_grid(sh, sh.shadow_pl_occ[MS][fmt][ti], tu);
     const int shade_grid = sh.shade_blocks[MS];
     const Workspace& ws = a.ws;
     cudaError_t e = cudaSuccess;
@@ -1227,7 +1350,15 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
                 if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
             }
             stage_on(3, sstream, [&] {
-                if (fmt == 0) {
+                if (tu.shadow_one_lane == 2) {
+                    if (fmt == 0) {
+                        if (counts) k_shadow_pl<0, true, MS><<<shadow_pl_grid, bt, smem, sstream>>>(a, b, tab);
+                        else k_shadow_pl<0, false, MS><<<shadow_pl_grid, bt, smem, sstream>>>(a, b, tab);
+                    } else {
+                        if (counts) k_shadow_pl<1, true, MS><<<shadow_pl_grid, bt, smem, sstream>>>(a, b, tab);
+                        else k_shadow_pl<1, false, MS><<<shadow_pl_grid, bt, smem, sstream>>>(a, b, tab);
+                    }
+                } else if (fmt == 0) {
                     if (counts) k_shadow<0, true, MS><<<shadow_grid, bt, smem, sstream>>>(a, b, tab);
                     else k_shadow<0, false, MS><<<shadow_grid, bt, smem, sstream>>>(a, b, tab);
                 } else {
