@@ -504,6 +504,11 @@ def nrc_eval(scene, ds, dev, ref_spp: int = 4096, frames: int = 300) -> dict:
                           "flops_per_query": int(flops / n)},
         "policy_sweep": policy_sweep,
         "best_policy": {"name": best, **policy_sweep[best]},
+        # the target: at least 2x lower relMSE than plain path tracing given the same GPU time
+        "target_2x_lower_relmse_at_equal_time": {
+            "met": policy_sweep[best]["relmse_ratio_plain_over_nrc"] >= 2.0, "policy": best,
+            "relmse_ratio_plain_over_nrc": policy_sweep[best]["relmse_ratio_plain_over_nrc"],
+            "relmse_x_time_ratio": policy_sweep[best]["relmse_x_time_ratio"]},
         "precision_sweep": sweep,
         "depth_sweep": {f"{k}x64": v for k, v in sorted(depth.items())},
         "encoding_sweep": encoding,

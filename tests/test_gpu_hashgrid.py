@@ -84,7 +84,8 @@ def test_inference_matches_fp64_model(built, cfg):
     feat = m.encode_features(_dev(d), n).cpu().numpy().astype(np.float64)
     L2 = 2 * full["n_levels"]
     np.testing.assert_allclose(feat[:, :L2], x[:, :L2], rtol=0, atol=4e-3 * max(1.0, np.abs(x[:, :L2]).max()))
-    np.testing.assert_allclose(feat[:, 32:62], mo.round_f16(x[:, 32:62]), rtol=0, atol=1e-6)
+    # one-blob bins (FP32 normal CDF, then FP16) and albedos: within one FP16 step of the FP64 values
+    np.testing.assert_allclose(feat[:, 32:62], mo.round_f16(x[:, 32:62]), rtol=0, atol=2.5e-4)
     # the hash-grid features matter: zero tables change the prediction
     x0 = x.copy()
     x0[:, :2 * full["n_levels"]] = 0.0

@@ -93,11 +93,21 @@ def test_frames_train_the_cache(scene_ds):
     m.close()
 
 
-def test_cache_beats_plain_path_tracing_at_equal_time(scene_ds):
+@pytest.fixture(scope="module")
+def reference_1024(scene_ds):
+    return reference_image(scene_ds[1], 1024)
+
+
+# footprint 0.01: the reference's policy (render.h:86-102), which answers only
+# the paths whose footprint has grown; 0: every path ends into the cache at its
+# first diffuse vertex, the primary hit included, which removes the noise of
+# every later bounce and is the policy the 2x target is measured with.
+@pytest.mark.parametrize("footprint,min_ratio", [(0.01, 1.0), (0.0, 2.0)])
+def test_cache_beats_plain_path_tracing_at_equal_time(scene_ds, reference_1024, footprint, min_ratio):
     s, ds = scene_ds
-    ref = reference_image(ds, 1024)
+    ref = reference_1024
     m = _mlp(s)
-    r = NrcRenderer(ds, m, PARAMS, train_steps=4)
+    r = NrcRenderer(ds, m, PARAMS, train_steps=4, footprint=footprint)
     frame = 0
     for _ in range(48):                   # reference warm-up (main.cpp:946)
         r.frame(frame, warmup=True, accumulate=False)
@@ -135,5 +145,5 @@ def test_cache_beats_plain_path_tracing_at_equal_time(scene_ds):
     print(f"nrc frame {t_nrc:.3f} ms, plain pass {t_pt:.3f} ms -> {spp_equal} spp; relMSE nrc {e_nrc:.4f} "
           f"plain {e_pt:.4f} ratio {e_pt / e_nrc:.2f}, relMSE x time ratio {eff:.2f}")
     assert np.isfinite(nrc_img).all()
-    assert e_nrc < e_pt and eff > 1.0
+    assert e_pt / e_nrc > min_ratio and eff > min_ratio, (e_nrc, e_pt, eff)
     m.close()

@@ -58,8 +58,6 @@ TUNINGS = [
     pt.RenderTuning(refill_min=1),
     pt.RenderTuning(refill_min=32),
     pt.RenderTuning(shadow_one_lane=1),
-    pt.RenderTuning(shadow_one_lane=2),                  # persistent shadow lanes
-    pt.RenderTuning(shadow_one_lane=2, refill_min=1, trace_threads=256),
     pt.RenderTuning(refill_min_primary=32),
     pt.RenderTuning(refill_min_primary=2, refill_min=29),
     pt.RenderTuning(overlap_shadow=0),
@@ -67,7 +65,6 @@ TUNINGS = [
     pt.RenderTuning(overlap_shadow=1, wavefront_paths=3 * N + 7, trace_threads=64, shadow_one_lane=1),
     pt.RenderTuning(wavefront_paths=2 * N + 1000, trace_threads=256, trace_warps_per_sm=16, refill_min=12,
                     shadow_one_lane=1),
-    pt.RenderTuning(wavefront_paths=3 * N + 7, trace_threads=64, shadow_one_lane=2, refill_min=32),
 ]
 
 
@@ -150,7 +147,7 @@ def test_cache_frames_under_tuning(scene, graph):
 def test_bad_tunings_are_rejected(built):
     for bad in (pt.RenderTuning(wavefront_paths=100), pt.RenderTuning(wavefront_paths=(1 << 26) + 1),
                 pt.RenderTuning(trace_threads=96), pt.RenderTuning(refill_min=0), pt.RenderTuning(refill_min=33),
-                pt.RenderTuning(trace_warps_per_sm=-1), pt.RenderTuning(shadow_one_lane=3),
+                pt.RenderTuning(trace_warps_per_sm=-1), pt.RenderTuning(shadow_one_lane=2),
                 pt.RenderTuning(refill_min_primary=33), pt.RenderTuning(overlap_shadow=2)):
         with pytest.raises(TfgError):
             pt.set_tuning(bad)

@@ -72,7 +72,7 @@ std::vector<int32_t> candidates(int k, uint32_t npix, uint64_t paths) {
         case 1: v = {64, 128, 256}; break;
         case 2: v = {0, 8, 16, 24}; break;
         case 3: v = {4, 8, 12, 16, 24, 32}; break;
-        case 4: v = {0, 1, 2}; break;
+        case 4: v = {0, 1}; break;
         case 5: v = {0, 16, 24, 32}; break;
         case 6: v = {0, 1}; break;
     }

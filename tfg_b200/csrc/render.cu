@@ -728,93 +728,6 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
     if (STATS) flush_work(3, nrays, cnt);
 }
 
-// Shadow rays on persistent lanes (shadow_one_lane 2): a lane owns one
-// shading point and traces its lights one after another, exactly as the
-// one-lane form does (same rays, same terms added in light order), but its
-// traversal advances one node per iteration and the lane takes a new shading
-// point as soon as `refill_min` lanes of its warp are idle, instead of
-// waiting for the warp's slowest shadow ray.
-template <int TRI_FMT, bool STATS, bool MS>
-__global__ void __launch_bounds__(256) k_shadow_pl(PassArgs a, int bounce, TableOf<MS> tab) {
-    extern __shared__ unsigned char smem_raw[];
-    uint2* sstack = reinterpret_cast<uint2*>(smem_raw);
-    APrim* sprims = reinterpret_cast<APrim*>(smem_raw + sizeof(uint2) * kSmemStack * blockDim.x);
-    const int nsm = MS ? 0 : load_aprims_smem(sprims, a.prims, a.nprims);
-    TravStack stck;
-    stck.smem = sstack; stck.stride = blockDim.x; stck.tid = threadIdx.x;
-    const uint32_t n = a.ws.counters[4 * bounce + 2];
-    uint32_t* fetch = &a.ws.counters[4 * bounce + 3];
-    TravCounts cnt;
-    uint32_t nrays = 0;
-    const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
-    CwbvhRay<TRI_FMT, true> r;
-    uint32_t cur = kMissId, p = 0, dest = 0;
-    int l = 0, lend = 0;
-    bool tracing = false, exhausted = false;
-    V3 P = v3(0, 0, 0), N = P, kd = P, cam = P, L = P, pending = P;
-    Geo g = geo_of<MS>(a, tab, 0);
-    const TfgLuzPuntual* lights = a.lights;
-    while (true) {
-        const bool idle = cur == kMissId;
-        const uint32_t im = __ballot_sync(0xFFFFFFFFu, idle);
-        if (exhausted) {
-            if (im == 0xFFFFFFFFu) break;
-        } else if (__popc(im) >= a.refill_min) {
-            uint32_t base = 0;
-            if (lane == 0) base = atomicAdd(fetch, (uint32_t)__popc(im));
-            base = __shfl_sync(0xFFFFFFFFu, base, 0);
-            exhausted = base + (uint32_t)__popc(im) >= n;
-            const uint32_t k = base + (uint32_t)__popc(im & lt);
-            if (idle && k < n) {
-                cur = k;
-                const float4* s = &a.ws.shadow[4 * (size_t)k];
-                const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
-                P = xyz(s0); N = xyz(s1); kd = xyz(s2); cam = xyz(s3);
-                p = __float_as_uint(s0.w);
-                dest = __float_as_uint(s1.w);
-                lights = a.lights;
-                lend = a.nlights;
-                if constexpr (MS) {
-                    const uint32_t sc = __float_as_uint(s2.w);
-                    g = geo_of<MS>(a, tab, sc);
-                    lights = tab.s[sc].lights;
-                    lend = tab.s[sc].nlights;
-                }
-                l = 0;
-                L = v3(0.0f, 0.0f, 0.0f);
-            }
-        }
-        if (cur == kMissId) continue;
-        if (tracing) {
-            if (r.step(g.nodes, g.tris, stck)) continue;   // one node per iteration
-            tracing = false;
-            if (STATS) { cnt.nodes += r.nsteps; cnt.tris += r.ntris; }
-            if (!r.found) L = v3(__fadd_rn(L.x, pending.x), __fadd_rn(L.y, pending.y), __fadd_rn(L.z, pending.z));
-            ++l;
-        }
-        // The next light that needs a mesh test; lights behind the surface or
-        // blocked by an analytic primitive settle here.
-        for (; l < lend; ++l) {
-            LightRay lr;
-            if (!light_ray(lights[l], P, N, kd, lr)) continue;
-            if (STATS) ++nrays;
-            if (analytic_any(sprims, nsm, g.prims, g.nprims, lr.so, lr.dl, lr.dist)) continue;
-            if (a.shadow_mesh && g.has_bvh) {
-                r.init(lr.so, lr.dl, kEps, lr.dist);
-                pending = lr.term;
-                tracing = true;
-                break;
-            }
-            L = v3(__fadd_rn(L.x, lr.term.x), __fadd_rn(L.y, lr.term.y), __fadd_rn(L.z, lr.term.z));
-        }
-        if (!tracing) {
-            add_direct(a, p, dest, cam, L);
-            cur = kMissId;
-        }
-    }
-    if (STATS) flush_work(3, nrays, cnt);
-}
-
 // ------------------------------------------------------------------ resolve
 __device__ __forceinline__ void get_geo(const float4* src, TfgDatosGeometricos& g) {
     const float4 a0 = src[0], a1 = src[1], a2 = src[2], a3 = src[3];
@@ -962,7 +875,6 @@ struct LaunchShapes {
     // resident CTAs per SM: [one scene / batch][triangle format][64, 128, 256 threads]
     int trace_occ[2][2][3] = {};
     int shadow_occ[2][2][3] = {};
-    int shadow_pl_occ[2][2][3] = {};
     int shade_blocks[2] = {0, 0};
 };
 LaunchShapes g_shapes[kMaxDevices];
@@ -994,10 +906,6 @@ int shapes_for(int dev, LaunchShapes& s) {
             g.trace_occ[1][1][k] = occ_of(k_trace<1, false, true>, bt, sm_ms);
             g.shadow_occ[1][0][k] = occ_of(k_shadow<0, false, true>, bt, sm_ms);
             g.shadow_occ[1][1][k] = occ_of(k_shadow<1, false, true>, bt, sm_ms);
-            g.shadow_pl_occ[0][0][k] = occ_of(k_shadow_pl<0, false, false>, bt, sm);
-            g.shadow_pl_occ[0][1][k] = occ_of(k_shadow_pl<1, false, false>, bt, sm);
-            g.shadow_pl_occ[1][0][k] = occ_of(k_shadow_pl<0, false, true>, bt, sm_ms);
-            g.shadow_pl_occ[1][1][k] = occ_of(k_shadow_pl<1, false, true>, bt, sm_ms);
         }
         g.shade_blocks[0] = sms * occ_of(k_shade<false>, 256, 0);
         g.shade_blocks[1] = sms * occ_of(k_shade<true>, 256, 0);
@@ -1055,8 +963,8 @@ int render_tuning_check(const TfgRenderTuning& t) {
     if (t.trace_warps_per_sm < 0 || t.trace_warps_per_sm > 64)
         return fail(TFG_E_INVALID, "render tuning: trace_warps_per_sm must be in [0, 64]");
     if (t.refill_min < 1 || t.refill_min > 32) return fail(TFG_E_INVALID, "render tuning: refill_min must be in [1, 32]");
-    if (t.shadow_one_lane < 0 || t.shadow_one_lane > 2)
-        return fail(TFG_E_INVALID, "render tuning: shadow_one_lane must be 0, 1 or 2");
+    if (t.shadow_one_lane != 0 && t.shadow_one_lane != 1)
+        return fail(TFG_E_INVALID, "render tuning: shadow_one_lane must be 0 or 1");
     if (t.refill_min_primary < 0 || t.refill_min_primary > 32)
         return fail(TFG_E_INVALID, "render tuning: refill_min_primary must be in [0, 32]");
     if (t.overlap_shadow != 0 && t.overlap_shadow != 1)
@@ -1288,7 +1196,6 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
     const size_t smem = trace_smem(MS ? 0 : a.nprims, bt);
     const int trace_grid = persistent_grid(sh, sh.trace_occ[MS][fmt][ti], tu);
     const int shadow_grid = persistent_grid(sh, sh.shadow_occ[MS][fmt][ti], tu);
-    const int shadow_pl_grid = persistent_grid(sh, sh.shadow_pl_occ[MS][fmt][ti], tu);
     const int shade_grid = sh.shade_blocks[MS];
     const Workspace& ws = a.ws;
     cudaError_t e = cudaSuccess;
@@ -1350,15 +1257,7 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
                 if (e != cudaSuccess) return fail((int)e, cudaGetErrorString(e));
             }
             stage_on(3, sstream, [&] {
-                if (tu.shadow_one_lane == 2) {
-                    if (fmt == 0) {
-                        if (counts) k_shadow_pl<0, true, MS><<<shadow_pl_grid, bt, smem, sstream>>>(a, b, tab);
-                        else k_shadow_pl<0, false, MS><<<shadow_pl_grid, bt, smem, sstream>>>(a, b, tab);
-                    } else {
-                        if (counts) k_shadow_pl<1, true, MS><<<shadow_pl_grid, bt, smem, sstream>>>(a, b, tab);
-                        else k_shadow_pl<1, false, MS><<<shadow_pl_grid, bt, smem, sstream>>>(a, b, tab);
-                    }
-                } else if (fmt == 0) {
+                if (fmt == 0) {
                     if (counts) k_shadow<0, true, MS><<<shadow_grid, bt, smem, sstream>>>(a, b, tab);
                     else k_shadow<0, false, MS><<<shadow_grid, bt, smem, sstream>>>(a, b, tab);
                 } else {

@@ -215,7 +215,7 @@ extern "C" {
 
 int dropin_render_tiny(const void* camara, const void* prims, int nprims, const void* luces, int nluces, int W, int H,
                        int frame, void* d_nodos, void* d_tris, unsigned num_nodos, unsigned num_tris,
-                       const void* bvh_prims, int n_bvh_prims, void* img) {
+                       const void* bvh_prims, int n_bvh_prims, void* img, void* thr) {
     TinyBVHD_GPU bvh;
     bvh.d_nodos = static_cast<float4*>(d_nodos);
     bvh.d_tris = static_cast<float4*>(d_tris);
@@ -225,7 +225,8 @@ int dropin_render_tiny(const void* camara, const void* prims, int nprims, const 
     launchKernelRenderTiny(dim3((W + 15) / 16, (H + 15) / 16), dim3(16, 16), static_cast<const Camara*>(camara),
                            static_cast<const Primitiva*>(prims), nprims, static_cast<const LuzPuntual*>(luces),
                            nluces, nullptr, 0, W, H, 1, frame, bvh, static_cast<const Primitiva*>(bvh_prims),
-                           n_bvh_prims, im, nullptr, nullptr, nullptr, 0, nullptr, nullptr, false, false);
+                           n_bvh_prims, im, nullptr, nullptr, nullptr, 0, nullptr, static_cast<Color*>(thr), false,
+                           false);
     return (int)cudaDeviceSynchronize();
 }
 
@@ -244,14 +245,14 @@ void* dropin_bvh_build(const void* prims_host, int n, unsigned* num_nodos, unsig
 }
 
 int dropin_bvh_render(void* bvh, const void* camara, const void* prims, int nprims, const void* luces, int nluces,
-                      int W, int H, int frame, void* img) {
+                      int W, int H, int frame, void* img, void* thr) {
     TinyBVH* b = static_cast<TinyBVH*>(bvh);
     ImagenGPU im(W, H, static_cast<Color*>(img));
     launchKernelRenderTiny(dim3((W + 15) / 16, (H + 15) / 16), dim3(16, 16), static_cast<const Camara*>(camara),
                            static_cast<const Primitiva*>(prims), nprims, static_cast<const LuzPuntual*>(luces),
                            nluces, nullptr, 0, W, H, 1, frame, b->obtenerDatosGPU(), b->getPrimitivasGPU(),
-                           (int)b->getNumPrimitivas(), im, nullptr, nullptr, nullptr, 0, nullptr, nullptr, false,
-                           false);
+                           (int)b->getNumPrimitivas(), im, nullptr, nullptr, nullptr, 0, nullptr,
+                           static_cast<Color*>(thr), false, false);
     return (int)cudaDeviceSynchronize();
 }
 

@@ -259,7 +259,7 @@ class RenderTuning:
     trace_threads: int = 128      # threads per traversal / shadow CTA: 64, 128, 256
     trace_warps_per_sm: int = 0   # resident traversal warps per SM; 0 = as many as fit
     refill_min: int = 8           # idle lanes that make a traversal warp fetch new rays
-    shadow_one_lane: int = 0      # 1: one lane traces all lights of a shading point; 2: the same on persistent lanes
+    shadow_one_lane: int = 0      # 1: one lane traces all lights of a shading point
     refill_min_primary: int = 0   # first-bounce refill threshold; 0 = refill_min
     overlap_shadow: int = 1       # 1: shadow stage on a second stream beside the next trace
 
