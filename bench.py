@@ -38,14 +38,14 @@ TRACE_DRAM_BYTES_PER_LAUNCH = {1: 38_063_296, 16: 505_144_128}
 
 
 # ncu counters of the closest-hit kernel on the bench frame (one-sample pass,
-# launches of bounce 0 and 1; profiles/k_trace_l2_issue_1080p.md): L2 bytes
+# all eight bounces; profiles/k_trace_l2_issue_1080p.md): L2 bytes
 # (lts__t_bytes.sum) per closest-hit ray traced, the share of issue slots
 # used (sm__inst_issued.avg.per_cycle_active / 4) and the SIMT efficiency
-# (smsp__thread_inst_executed_per_inst_executed.ratio / 32), weighted by the
-# launches' durations.
-TRACE_L2_BYTES_PER_RAY = None
-TRACE_ISSUE_FRAC = None
-TRACE_SIMT_EFFICIENCY = None
+# (smsp__thread_inst_executed_per_inst_executed.ratio / 32), over the pass's
+# 4,001,265 rays, weighted by duration and by instructions respectively.
+TRACE_L2_BYTES_PER_RAY = 508.0
+TRACE_ISSUE_FRAC = 0.565
+TRACE_SIMT_EFFICIENCY = 0.406
 
 
 def l2_gather_peak(dev) -> dict:

@@ -51,6 +51,11 @@ def _frame_image(r, f):
     return r.image().cpu().numpy().copy()
 
 
+# The gate learns from the frame's training records, and neither it nor the
+# training runs below `min_records` records: these small frames trace a
+# quarter of their paths for training so that every frame has enough.
+
+
 def _answered(r):
     """Pixels whose value includes a cache answer (non-zero query throughput)."""
     return float((r.thr.view(-1, 3) != 0).any(dim=1).float().mean())
@@ -129,7 +134,8 @@ def test_gate_stays_closed_in_an_unseen_region_until_judged(built):
     s = two_rooms()
     ds = pt.DeviceScene(s, "cuda")
     m = _mlp(s, seed=3)
-    r = NrcRenderer(ds, m, PARAMS, train_steps=4, gate_threshold=0.5, use_graph=True)
+    r = NrcRenderer(ds, m, PARAMS, train_steps=4, gate_threshold=0.5, use_graph=True, min_records=64,
+                    train_fraction=0.25)
     f = 0
     for _ in range(8):
         r.frame(f, warmup=True, accumulate=False)
@@ -163,7 +169,8 @@ def test_gate_stays_closed_in_an_unseen_region_until_judged(built):
 def test_gate_closes_when_the_lighting_changes(terrain):
     s, ds = terrain
     m = _mlp(s, seed=9)
-    r = NrcRenderer(ds, m, PARAMS, train_steps=4, gate_threshold=0.5, use_graph=True)
+    r = NrcRenderer(ds, m, PARAMS, train_steps=4, gate_threshold=0.5, use_graph=True, min_records=64,
+                    train_fraction=0.25)
     f = 0
     for _ in range(8):
         r.frame(f, warmup=True, accumulate=False)
