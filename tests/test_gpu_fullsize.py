@@ -171,3 +171,57 @@ def test_cpu_runnable_case_configured_pass_matches_cpu_oracle_512(c1):
         mine += img.view(H, W, 3).cpu().numpy()
         cpu += oracle_image(orc, s, hb, f, prm)
     assert rel_mse(mine / 4, cpu / 4) <= 1e-4
+
+
+def test_benchmark_scene_at_256_spp_matches_the_reference_kernel(terrain):
+    """The 1,000,480-triangle 1080p frame at 256 samples, under the reference
+    kernel's own settings (depth 20, roulette past 10, shadow rays blind to the
+    mesh): tfgLaunchKernelRenderTiny's mean against kernelRender_tiny's on the
+    same RNG streams, so that a bias shared by the product's renderer would
+    show here before it could cancel out of a relMSE against the product's own
+    high-spp reference."""
+    s, ds = terrain
+    ref = _ref_lib()
+    W, H = s.width, s.height
+    n = W * H
+    spp = 256
+    mine = torch.zeros(n * 3, dtype=torch.float64, device="cuda")
+    want = torch.zeros(n * 3, dtype=torch.float64, device="cuda")
+    img = torch.zeros(n * 3, dtype=torch.float32, device="cuda")
+    rimg = torch.zeros(n * 3, dtype=torch.float32, device="cuda")
+    nrc = pt.NrcBuffers(n + 16 * W, "cuda")   # the reference kernel writes whole 16 x 16 blocks
+    for f in range(spp):
+        pt.render_reference_call(ds, f, img)
+        assert ref.ref_render_tiny(ds.camera.data_ptr(), None, 0, ds.lights.data_ptr(), ds.n_lights, W, H, f,
+                                   ds.bvh.ref.d_nodos, ds.bvh.ref.d_tris, ds.bvh.ref.num_nodos, ds.bvh.ref.num_tris,
+                                   ds.bvh.d_primitivas, ds.n_mesh, rimg.data_ptr(), nrc.regs.data_ptr(),
+                                   nrc.counter.data_ptr(), nrc.cap, nrc.infer.data_ptr(), nrc.thr.data_ptr(), 0,
+                                   0) == 0
+        mine += img.double()
+        want += rimg.double()
+    torch.cuda.synchronize()
+    a = (mine / spp).view(H, W, 3).cpu().numpy()
+    b = (want / spp).view(H, W, 3).cpu().numpy()
+    assert np.isfinite(a).all() and a.mean() > 0
+    assert rel_mse(a, b) <= 1e-4, rel_mse(a, b)
+
+
+def test_benchmark_settings_match_the_cpu_oracle_at_64_spp(built):
+    """The benchmark's own settings (depth 8, roulette from 3, mesh-occluded
+    shadow rays) on the benchmark scene at 480x270, 64 samples, against the CPU
+    oracle on the same RNG streams (the oracle with the reference triangle
+    test, the product with both)."""
+    s = scenes.spheres_terrain(480, 270)
+    ds = pt.DeviceScene(s, "cuda")
+    hb = hbvh.build_host(hbvh.triangle_vertices(s.mesh))
+    W, H = s.width, s.height
+    prm = reference_params(max_depth=8, rr_min_depth=3, shadow_mesh=1)
+    cpu = np.zeros((H, W, 3))
+    for f in range(64):
+        cpu += oracle_image(orc, s, hb, 500 + f, prm, nthreads=16)
+    cpu /= 64
+    for fmt, tol in ((pt.TRIS_REF, 1e-4), (pt.TRIS_WATERTIGHT, 3e-4)):
+        params = pt.RenderParams(max_depth=8, rr_min_depth=3, shadow_mesh=1, tri_format=fmt)
+        acc = pt.accumulate_spp(ds, params, 64, first_frame=500).cpu().numpy().astype(np.float64)
+        assert rel_mse(acc, cpu) <= tol, (fmt, rel_mse(acc, cpu))
+    ds.close()

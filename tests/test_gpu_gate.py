@@ -160,7 +160,9 @@ def test_gate_stays_closed_in_an_unseen_region_until_judged(built):
         f += 1
         r.stream.synchronize()
         answered.append(_answered(r))
-    assert max(answered[-4:]) > max(2.0 * first, 0.02) and m.state()["gate"] > open_a, (
+    # the new room's cells open once judged; the old room's close as their
+    # evidence decays away (no new samples there)
+    assert max(answered[-4:]) > max(5.0 * first, 0.05) and m.state()["gate"] > 0, (
         answered[::4], open_a, m.state()["gate"])
     m.close()
     ds.close()
