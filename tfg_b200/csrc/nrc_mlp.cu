@@ -1770,7 +1770,7 @@ constexpr int kWgSmem = kWgSmemH<64>;                // 114688
 struct WgradArgs {
     const uint8_t* zT[kMaxLayers];
     const uint8_t* hT[kMaxLayers];
-    float* grad;
+    float* part;                 // per-CTA partial sums, [gridDim.x][params]
     const uint32_t* state;
     uint32_t min_n;
     uint32_t ntiles;
@@ -1854,14 +1854,17 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     ok = all_ok(ok);
     umma::fence_after_sync();
     if (ok && 32 * warp < FZ) {
+        // This CTA's sum over its tiles, stored (no atomics) in its own slice;
+        // the Adam step adds the slices in a fixed order.
         const int row = 32 * warp + (t & 31);
         for (int c0 = 0; c0 < FH; c0 += 32) {
             float v[32];
             umma::tmem_ld32(tmem + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
             if (row < FZ) {
-                float* g = a.grad + poff_h<HID>(NL, l) + row * cols_h<HID>(l) + c0;
+                float4* g = reinterpret_cast<float4*>(a.part + (size_t)blockIdx.x * params_h<HID>(NL) +
+                                                      poff_h<HID>(NL, l) + row * cols_h<HID>(l) + c0);
 #pragma unroll
-                for (int i = 0; i < 32; ++i) atomicAdd(&g[i], v[i]);
+                for (int i = 0; i < 8; ++i) g[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
             }
         }
     }
@@ -1871,13 +1874,30 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     if (warp == 0) umma::tmem_dealloc(tmem, 128);
 }
 
+// The gradient of a step that does not update (tfgMlpComputeGradient): the
+// weight-gradient CTAs' partial sums added in the order the Adam step adds
+// them, so both see the same gradient bit for bit.
+template <int NL, int HID>
+__global__ void k_wgrad_sum(const float* __restrict__ part, uint32_t groups, float* __restrict__ grad,
+                            const uint32_t* __restrict__ state, uint32_t min_n) {
+    if (state[S_NAVAIL] < min_n || state[S_NAVAIL] == 0) return;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < (uint32_t)params_h<HID>(NL);
+         i += gridDim.x * blockDim.x) {
+        float gs = 0.0f;
+        for (uint32_t k = 0; k < groups; ++k) gs += part[(size_t)k * params_h<HID>(NL) + i];
+        grad[i] = gs;
+    }
+}
+
 // ------------------------------------------------------------------ Adam + EMA + packing
 struct AdamArgs {
     float* w;        // FP32 master
     float* m;
     float* v;
     float* ema;      // running EMA (not debiased)
-    float* grad;     // summed gradient; reset to 0 here
+    float* grad;     // summed gradient (written here when `part` is set)
+    const float* part;   // weight-gradient partial sums [groups][params], or null
+    uint32_t groups;
     uint8_t* fwd;    // FP16 forward image of w
     uint8_t* bwd;    // BF16 W^T image of w
     uint8_t* inf;    // FP16 image of the debiased EMA
@@ -1913,7 +1933,9 @@ __global__ void k_adam(AdamArgs a) {
     const float tn = (float)(a.state[S_ADAM_T] + (update ? 1u : 0u));
     if (update && live) {
         const float bc1 = 1.0f - powf(a.beta1, tn), bc2 = 1.0f - powf(a.beta2, tn);
-        const float g = a.grad[i] * a.grad_scale;
+        float gs = 0.0f;
+        for (uint32_t k = 0; k < a.groups; ++k) gs += a.part[(size_t)k * params_h<HID>(NL) + i];
+        const float g = gs * a.grad_scale;
         const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
         const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
         a.m[i] = m;
@@ -1924,7 +1946,6 @@ __global__ void k_adam(AdamArgs a) {
         a.ema[i] = e;
     }
     if (!live) { w = 0.0f; e = 0.0f; }
-    a.grad[i] = 0.0f;
     const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
     const float ew = ema_debias > 0.0f ? e / ema_debias : w;
     // forward / inference images: row r, K index c
@@ -2205,6 +2226,8 @@ struct ColorMlp {
     float lr = 1e-2f, beta1 = 0.9f, beta2 = 0.99f, eps = 1e-15f, decay = 0.99f;
     mlp::Bounds bounds{{-1, -1, -1}, {1, 1, 1}};
     float* w = nullptr; float* m = nullptr; float* v = nullptr; float* ema = nullptr; float* grad = nullptr;
+    float* wpart = nullptr;      // weight-gradient partial sums, one slice per gradient CTA (act_tiles slices)
+    uint32_t wgroups = 0;        // slices written by the last weight-gradient launch
     uint8_t* fwd = nullptr; uint8_t* bwd = nullptr; uint8_t* inf = nullptr;
     int nl = 6;                  // layers (hidden layers + 1)
     int hid = 64;                // hidden width (64 or 128)
@@ -2298,6 +2321,8 @@ uint64_t splitmix(uint64_t& s) {
 int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
     mlp::AdamArgs a;
     a.w = n->w; a.m = n->m; a.v = n->v; a.ema = n->ema; a.grad = n->grad;
+    a.part = update ? n->wpart : nullptr;
+    a.groups = update ? n->wgroups : 0u;
     a.fwd = n->fwd; a.bwd = n->bwd; a.inf = n->inf; a.inf_bf = n->inf_bf;
     a.lr = n->lr; a.beta1 = n->beta1; a.beta2 = n->beta2; a.eps = n->eps; a.decay = n->decay;
     a.grad_scale = 1.0f / (3.0f * (float)n->batch);
@@ -2333,12 +2358,17 @@ int ensure_acts(ColorMlp* n, uint32_t tiles) {
         if (n->zT[l]) cudaFree(n->zT[l]);
         n->hT[l] = n->zT[l] = nullptr;
     }
+    if (n->wpart) cudaFree(n->wpart);
+    n->wpart = nullptr;
     for (int l = 0; l < n->nl; ++l) {
         const int fh = l == 0 ? 96 : n->hid, fz = l == n->nl - 1 ? 16 : n->hid;   // features of the tiles
         cudaError_t e = cudaMalloc((void**)&n->hT[l], (size_t)tiles * 2 * fh * 128);
         if (e == cudaSuccess) e = cudaMalloc((void**)&n->zT[l], (size_t)tiles * 2 * fz * 128);
         if (e != cudaSuccess) { n->act_tiles = 0; return cuda_fail(e, "mlp activations"); }
     }
+    // one slice per gradient CTA: at most one CTA per tile
+    cudaError_t e = cudaMalloc((void**)&n->wpart, (size_t)tiles * mlp::params_rt(n->nl, n->hid) * sizeof(float));
+    if (e != cudaSuccess) { n->act_tiles = 0; return cuda_fail(e, "mlp gradient slices"); }
     n->act_tiles = tiles;
     return ok();
 }
@@ -2374,17 +2404,31 @@ int enqueue_wgrad(ColorMlp* n, uint32_t tiles_per_cta, uint32_t min_n, cudaStrea
     const uint32_t tiles = n->batch / mlp::kTile;
     mlp::WgradArgs wa;
     for (int l = 0; l < mlp::kMaxLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
-    wa.grad = n->grad; wa.state = n->dstate; wa.min_n = min_n;
+    wa.part = n->wpart; wa.state = n->dstate; wa.min_n = min_n;
     wa.ntiles = tiles;
     wa.tiles_per_cta = std::max<uint32_t>(1u, tiles_per_cta);
+    const uint32_t groups = (tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta;
     with_width(n, [&](auto c, auto w) {
         constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
-        mlp::k_wgrad<NL, HID><<<dim3((tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta, NL), 128,
-                                mlp::kWgSmemH<HID> + 1024, s>>>(wa);
+        mlp::k_wgrad<NL, HID><<<dim3(groups, NL), 128, mlp::kWgSmemH<HID> + 1024, s>>>(wa);
         return 0;
     });
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp step: weight gradients");
+    n->wgroups = groups;
+    return ok();
+}
+
+// The summed gradient in n->grad (steps that do not update).
+int enqueue_wgrad_sum(ColorMlp* n, uint32_t min_n, cudaStream_t s) {
+    with_width(n, [&](auto c, auto w) {
+        constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
+        mlp::k_wgrad_sum<NL, HID><<<(mlp::params_h<HID>(NL) + 255) / 256, 256, 0, s>>>(n->wpart, n->wgroups, n->grad,
+                                                                                          n->dstate, min_n);
+        return 0;
+    });
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return cuda_fail(e, "mlp step: gradient sum");
     return ok();
 }
 
@@ -2418,7 +2462,7 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
         e = cudaGetLastError();
         if (e != cudaSuccess) return cuda_fail(e, "mlp step: table gradient");
     }
-    if (!update) return ok();
+    if (!update) return enqueue_wgrad_sum(n, min_n, s);
     if (int rc = repack(n, s, true, min_n)) return rc;
     mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n);
     e = cudaGetLastError();
@@ -2615,7 +2659,11 @@ int autotune_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, TfgColor* 
             if (t != cands[0]) cands.push_back(t);
         for (size_t i = 0; i < cands.size() && !rc; ++i) {
             float ms = 0.0f;
-            rc = time_launches([&] { return enqueue_wgrad(n, cands[i], 0, s); }, repeats, s, e0, e1, &ms);
+            // the gradient CTAs and the sum of their slices (which the Adam step does in a frame)
+            rc = time_launches([&] {
+                const int r = enqueue_wgrad(n, cands[i], 0, s);
+                return r ? r : enqueue_wgrad_sum(n, 0, s);
+            }, repeats, s, e0, e1, &ms);
             if (!rc && (i == 0 || ms < 0.99f * best_wg)) { best_wg = ms; best.wgrad_tiles_per_cta = (int32_t)cands[i]; }
         }
     }
@@ -3049,7 +3097,7 @@ extern "C" void tfgMlpDestroy(TfgColorMLP* h) {
     for (void* p : {(void*)n->w, (void*)n->m, (void*)n->v, (void*)n->ema, (void*)n->grad, (void*)n->fwd, (void*)n->bwd,
                     (void*)n->inf, (void*)n->inf_bf, (void*)n->inf_f8, (void*)n->f8, (void*)n->loss, (void*)n->dstate,
                     (void*)n->hw, (void*)n->hm, (void*)n->hv, (void*)n->hema, (void*)n->hgrad, (void*)n->hinf,
-                    (void*)n->gate_cells, (void*)n->gate_bits})
+                    (void*)n->gate_cells, (void*)n->gate_bits, (void*)n->wpart})
         if (p) cudaFree(p);
     for (int l = 0; l < M::kMaxLayers; ++l) {
         if (n->hT[l]) cudaFree(n->hT[l]);
