@@ -1237,7 +1237,6 @@ struct TrainArgs {
     uint8_t* zT[kMaxLayers];  // transposed output gradients of each layer, per tile
     float* loss;                 // sum of per-sample losses (unnormalised)
     HashGrid hg;                 // composite encoding (levels 0: frequency encoding)
-    float* part;                 // width 64: each tile's weight gradients, [tiles][params]
 };
 
 // Write 64 (or 16) values of sample s into the transposed BF16 tile layout.
@@ -1252,36 +1251,6 @@ __device__ __forceinline__ void store_T(uint8_t* tile, int s, const float* v) {
     }
 }
 
-// Shared memory of k_train beyond the weights and the A buffer: the
-// transposed output gradient of the layer whose weight gradient is formed
-// (A operand: 128 rows, rows past the layer's outputs zero; two 64-sample K
-// regions of 16 KB) and the layer's transposed input tile (B operand, two
-// regions of up to 96 rows).
-constexpr int kTrainSmemZ = kTrainSmem;                           // 158720
-constexpr int kTrainSmemH = kTrainSmemZ + 2 * kTile * 128;         // 191488
-constexpr int kTrainSmemFused = kTrainSmemH + 2 * 96 * 128;        // 216064
-static_assert(kTrainSmemZ % 1024 == 0 && kTrainSmemH % 1024 == 0, "SW128 regions are 1024-byte aligned");
-
-// The same transposed layout with 128-row regions (the weight-gradient A
-// operand in shared memory).
-template <int F>
-__device__ __forceinline__ void store_T128(uint8_t* stage, int s, const float* v) {
-    uint8_t* region = stage + (s >> 6) * (kTile * 128);
-    const int c = (s & 63) >> 3, e = s & 7;
-#pragma unroll
-    for (int f = 0; f < F; ++f) {
-        __nv_bfloat16 h = __float2bfloat16_rn(v[f]);
-        *reinterpret_cast<__nv_bfloat16*>(region + umma::sw128_offset(f, c) + 2 * e) = h;
-    }
-}
-
-// One training tile per CTA pass: forward (FP16), loss gradient, backward
-// (BF16) and the tile's weight gradients, all layers in one kernel.  The
-// weight gradient of layer l, dW_l = dZ_l^T H_l over the tile's 128 samples,
-// is issued as soon as dZ_l is known, beside the backward GEMM of layer l
-// (TMEM columns 128.. hold it), with H_l bulk-copied back from the tile's
-// transposed input written in the forward pass; each tile's dW goes to its
-// own slice of the partial sums, which the Adam step adds in a fixed order.
 template <int NL>
 __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     extern __shared__ __align__(1024) uint8_t smem_raw[];
@@ -1289,21 +1258,17 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     uint8_t* sf = smem + kTrainSmemF;
     uint8_t* sb = smem + kTrainSmemB;
     uint8_t* sa = smem + kTrainSmemA;
-    uint8_t* sz = smem + kTrainSmemZ;
-    uint8_t* sh = smem + kTrainSmemH;
-    __shared__ uint64_t mb_w, mb_mma, mb_wg, mb_h, mb_drain;
+    __shared__ uint64_t mb_w, mb_mma, mb_drain;
     __shared__ uint32_t tslot;
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t ntiles = a.batch / kTile;
     const uint32_t n_avail = a.state[S_NAVAIL];
     const uint32_t seed = a.state[S_STEP];
     if (blockIdx.x >= ntiles || n_avail < a.min_n || n_avail == 0) return;
-    if (warp == 0) umma::tmem_alloc(&tslot, 256);
+    if (warp == 0) umma::tmem_alloc(&tslot, 128);
     if (t == 0) {
         umma::mbar_init(&mb_w, 1);
         umma::mbar_init(&mb_mma, 1);
-        umma::mbar_init(&mb_wg, 1);
-        umma::mbar_init(&mb_h, 1);
         umma::mbar_init(&mb_drain, 1);
         umma::mbar_fence_init();
     }
@@ -1311,12 +1276,9 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
         const int r = i >> 2, c = 4 + (i & 3);
         *reinterpret_cast<uint4*>(sa + kTile * 128 + umma::sw128_offset(r, c)) = make_uint4(0, 0, 0, 0);
     }
-    // rows 64..127 of the gradient stage stay zero (M is padded to 128)
-    for (int i = t; i < 2 * kTile * 128 / 16; i += blockDim.x) reinterpret_cast<uint4*>(sz)[i] = make_uint4(0, 0, 0, 0);
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = tslot;
-    const uint32_t tmem_wg = tmem + 128u;
     if (t == 0) {
         umma::mbar_expect_tx(&mb_w, kFwdBytes<NL> + kBwdBytes<NL>);
         umma::bulk_g2s(sf, a.fwd, kFwdBytes<NL>, &mb_w);
@@ -1324,32 +1286,8 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     }
     bool ok = all_ok(umma::mbar_wait(&mb_w, 0, kSpinLimit));
     const bool weights_in = ok;
-    uint32_t mph = 0, wph = 0, hph = 0;
-    bool h_pending = false;   // a transposed-input copy is in flight
+    uint32_t mph = 0;
     float lsum = 0.0f;
-    // H_l of this tile into the B stage (thread 0).
-    auto fetch_h = [&](uint32_t tile, int l) {
-        const uint32_t bytes = 2u * (uint32_t)kHTFeat<NL>(l) * 128u;
-        umma::mbar_expect_tx(&mb_h, bytes);
-        umma::bulk_g2s(sh, a.hT[l] + (size_t)tile * bytes, bytes, &mb_h);
-    };
-    // dW_l of this tile, once its MMAs have completed: rows of the layer's
-    // outputs, FH columns, into the tile's slice.
-    auto store_dw = [&](uint32_t tile, int l) {
-        const int FZ = kZTFeat<NL>(l), FH = kHTFeat<NL>(l);
-        if (32 * warp >= FZ) return;
-        const int row = 32 * warp + (t & 31);
-        for (int c0 = 0; c0 < FH; c0 += 32) {
-            float v[32];
-            umma::tmem_ld32(tmem_wg + ((uint32_t)(32 * warp) << 16) + (uint32_t)c0, v);
-            if (row < FZ) {
-                float4* g = reinterpret_cast<float4*>(a.part + (size_t)tile * kParams<NL> + kPOff<NL>(l) +
-                                                      row * kCols<NL>(l) + c0);
-#pragma unroll
-                for (int i = 0; i < 8; ++i) g[i] = make_float4(v[4 * i], v[4 * i + 1], v[4 * i + 2], v[4 * i + 3]);
-            }
-        }
-    };
     for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
         const uint32_t s = tile * kTile + (uint32_t)t;
         // Sample selection as generarIndicesAleatorios (NrcKernel.cu:10-16).
@@ -1422,76 +1360,36 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
                     g[k] = 2.0f * diff / den;
                 }
                 store_row64<true>(sa, t, g);
-                store_T128<64>(sz, t, g);   // rows 3..63 of the gradient stage zero
-                // the transposed inputs written above reach the bulk copies that read them back
-                asm volatile("fence.proxy.async.global;" ::: "memory");
+                store_T<16>(a.zT[NL - 1] + (size_t)tile * (2 * 16 * 128), t, g);
             }
             umma::fence_before_sync();
             umma::fence_smem_to_async();
             __syncthreads();
         }
-        if (ok && t == 0) { fetch_h(tile, NL - 1); h_pending = true; }
-        // backward: dH_{l-1} = dZ_l * W_l, masked by the ReLU of layer l-1,
-        // beside dW_l = dZ_l^T H_l
-        for (int l = NL - 1; l >= 0 && ok; --l) {
+        // backward: dH_{l-1} = dZ_l * W_l, masked by the ReLU of layer l-1
+        for (int l = NL - 1; l >= 1 && ok; --l) {
             const int K = (l == NL - 1) ? kOutPad : kHid;
             if (warp == 0) {
                 umma::fence_after_sync();
                 if (umma::elect_one()) {
-                    if (l >= 1) {
-                        issue_layer(tmem, sa, kTile * 128, sb + kBOff<NL>(l), 64 * 128, K, kHid, true);
-                        umma::mma_commit(&mb_mma);
-                    }
+                    issue_layer(tmem, sa, kTile * 128, sb + kBOff<NL>(l), 64 * 128, K, kHid, true);
+                    umma::mma_commit(&mb_mma);
                 }
                 __syncwarp();
-                // H_l arrived (every lane observes the copy before one of them issues)
-                const bool hok = __all_sync(0xFFFFFFFFu, umma::mbar_wait(&mb_h, hph, kSpinLimit) ? 1 : 0) != 0;
-                if (hok) {
-                    if (t == 0) h_pending = false;
-                    umma::fence_after_sync();
-                    if (umma::elect_one()) {
-                        const int FH = kHTFeat<NL>(l);
-                        const uint32_t id = umma::idesc_f16(kTile, FH, true);
-                        for (int q = 0; q < 8; ++q) {
-                            const int reg = q >> 2, kk = q & 3;
-                            const uint64_t ad = umma::sdesc_sw128(umma::smem_u32(sz + reg * (kTile * 128) + kk * 32));
-                            const uint64_t bd = umma::sdesc_sw128(umma::smem_u32(sh + reg * (FH * 128) + kk * 32));
-                            umma::mma_f16(tmem_wg, ad, bd, id, q > 0);
-                        }
-                        umma::mma_commit(&mb_wg);
-                    }
-                    __syncwarp();
-                }
-                ok = ok && hok;
             }
-            ok = all_ok(ok);
-            if (!ok) break;
-            hph ^= 1u;
-            float v[64];
-            if (l >= 1) {
-                ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
-                mph ^= 1u;
-                if (!ok) break;
-                umma::fence_after_sync();
-                tmem_row64(tmem, warp, 0, v);
-#pragma unroll
-                for (int i = 0; i < 64; ++i) {
-                    const uint32_t bit = (i < 32) ? (mask[l - 1][0] >> i) & 1u : (mask[l - 1][1] >> (i - 32)) & 1u;
-                    v[i] = bit ? v[i] : 0.0f;
-                }
-            }
-            // dW_l done: the gradient and input stages are free again
-            ok = all_ok(umma::mbar_wait(&mb_wg, wph, kSpinLimit));
-            wph ^= 1u;
+            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+            mph ^= 1u;
             if (!ok) break;
             umma::fence_after_sync();
-            store_dw(tile, l);
-            if (l >= 1) {
-                if (t == 0) { fetch_h(tile, l - 1); h_pending = true; }
-                if (l > 1) store_row64<true>(sa, t, v);
-                store_T128<64>(sz, t, v);
-                if (l == 1 && a.hg.levels > 0) store_T<64>(a.zT[0] + (size_t)tile * (2 * 64 * 128), t, v);
+            float v[64];
+            tmem_row64(tmem, warp, 0, v);
+#pragma unroll
+            for (int i = 0; i < 64; ++i) {
+                const uint32_t bit = (i < 32) ? (mask[l - 1][0] >> i) & 1u : (mask[l - 1][1] >> (i - 32)) & 1u;
+                v[i] = bit ? v[i] : 0.0f;
             }
+            if (l > 1) store_row64<true>(sa, t, v);
+            store_T<64>(a.zT[l - 1] + (size_t)tile * (2 * 64 * 128), t, v);
             umma::fence_before_sync();
             umma::fence_smem_to_async();
             __syncthreads();
@@ -1500,18 +1398,17 @@ __global__ void __launch_bounds__(128) k_train(TrainArgs a) {
     // loss reduction
     for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xFFFFFFFFu, lsum, o);
     if ((t & 31) == 0) atomicAdd(a.loss, lsum);
-    if (!ok && warp == 0) {   // after a timeout: the copies and every issued MMA finish first
+    if (!ok && warp == 0) {   // after a timeout: the weight copy and every issued MMA finish first
         if (umma::elect_one()) {
             if (!weights_in) umma::mbar_wait(&mb_w, 0, kSpinLimit);
             umma::mma_commit(&mb_drain);
             umma::mbar_wait(&mb_drain, 0, kSpinLimit);
         }
         __syncwarp();
-        if (t == 0 && h_pending) umma::mbar_wait(&mb_h, hph, kSpinLimit);
     }
     if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
     __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(tmem, 256);
+    if (warp == 0) umma::tmem_dealloc(tmem, 128);
 }
 
 // ------------------------------------------------------------------ width-128 training
@@ -2546,21 +2443,16 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
     ta.hg = hash_view(n, true);
     for (int l = 0; l < mlp::kMaxLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
-    ta.part = n->wpart;
     with_width(n, [&](auto c, auto w) {
         constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)n->sms);
         if constexpr (HID == 128) mlp::k_train128<NL><<<grid, 128, mlp::kT128Smem + 1024, s>>>(ta);
-        else mlp::k_train<NL><<<grid, 128, mlp::kTrainSmemFused + 1024, s>>>(ta);
+        else mlp::k_train<NL><<<grid, 128, mlp::kTrainSmem + 1024, s>>>(ta);
         return 0;
     });
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp step: forward/backward");
-    if (n->hid == 128) {
-        if (int rc = enqueue_wgrad(n, wgrad_tiles_per_cta(n, tiles), min_n, s)) return rc;
-    } else {
-        n->wgroups = tiles;   // k_train wrote one slice of weight gradients per tile
-    }
+    if (int rc = enqueue_wgrad(n, wgrad_tiles_per_cta(n, tiles), min_n, s)) return rc;
     if (n->hlevels) {
         mlp::HashGradArgs ha;
         ha.buf = buf; ha.state = n->dstate; ha.min_n = min_n; ha.batch = n->batch; ha.bounds = n->bounds;
@@ -2761,7 +2653,7 @@ int autotune_impl(ColorMlp* n, const TfgDatosMLP* in, uint32_t count, TfgColor* 
     float best_wg = 0.0f, best_inf = 0.0f;
     // Weight gradients of one batch; the record count is set so the kernel runs.
     if (!rc) rc = set_word(n, mlp::S_NAVAIL, n->batch, s);
-    if (!rc && n->hid == 128) {   // width 64 forms its weight gradients inside k_train
+    if (!rc) {
         std::vector<uint32_t> cands{wgrad_tiles_per_cta(n, tiles)};
         for (uint32_t t = 1; t <= 64 && t <= tiles; t *= 2)
             if (t != cands[0]) cands.push_back(t);
@@ -2883,7 +2775,7 @@ void set_kernel_attrs() {
     cudaFuncSetAttribute(M::k_infer<M::kPrecF16, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
     cudaFuncSetAttribute(M::k_infer<M::kPrecBF16, false, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
     cudaFuncSetAttribute(M::k_infer<M::kPrecF8, true, NL, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ism);
-    cudaFuncSetAttribute(M::k_train<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kTrainSmemFused + 1024);
+    cudaFuncSetAttribute(M::k_train<NL>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kTrainSmem + 1024);
     cudaFuncSetAttribute(M::k_wgrad<NL, 64>, cudaFuncAttributeMaxDynamicSharedMemorySize, M::kWgSmem + 1024);
     if constexpr (NL == 4 || NL == 6) {
         const int i128 = M::kInfer128Smem + 1024;
