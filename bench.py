@@ -805,7 +805,7 @@ def profile_mlp(width: int = 64, precision: str = "fp16"):
     print("profile mlp done")
 
 
-def profile_frame(encoding: str = "frequency", width: int = 64, frames: int = 6):
+def profile_frame(encoding: str = "frequency", width: int = 64, frames: int = 6, footprint: float = 0.01):
     """`frames` cache frames of the 1920x1080 benchmark scene (the first
     four as warm-up frames, 4 x 16384 training samples each, launched
     eagerly) and then one more inference over the last frame's 2,073,600
@@ -823,7 +823,7 @@ def profile_frame(encoding: str = "frequency", width: int = 64, frames: int = 6)
     kw = {"encoding": HASHGRID} if encoding == "hashgrid" else {}
     m = ColorMLP(batch=16384, seed=2024, width=width, **kw)
     m.set_bounds(*scene.bounds)
-    r = NrcRenderer(ds, m, params, train_steps=4, use_graph=False)
+    r = NrcRenderer(ds, m, params, train_steps=4, use_graph=False, footprint=footprint)
     for f in range(frames):
         r.frame(f, warmup=f < 4, accumulate=False)
     n = W_PX * H_PX
@@ -887,6 +887,8 @@ def main():
                     help="run six eager cache frames of the workload and one more inference, then exit (case for ncu)")
     ap.add_argument("--mlp-encoding", default="frequency", choices=["frequency", "hashgrid"],
                     help="with --profile-frame: the cache's input encoding")
+    ap.add_argument("--nrc-footprint", type=float, default=0.01,
+                    help="with --profile-frame: the cache policy's footprint threshold (0: query at the primary hit)")
     ap.add_argument("--nrc-only", action="store_true",
                     help="run only the radiance-cache evaluation (config 3 and its sweeps), print it and exit")
     args = ap.parse_args()
@@ -907,7 +909,7 @@ def main():
         profile_pass(args.wavefront_samples, args.tuning)
         return
     if args.profile_frame:
-        profile_frame(args.mlp_encoding, args.mlp_width)
+        profile_frame(args.mlp_encoding, args.mlp_width, footprint=args.nrc_footprint)
         return
     if args.profile_mlp:
         profile_mlp(args.mlp_width, args.mlp_precision)
