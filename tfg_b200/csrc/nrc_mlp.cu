@@ -154,6 +154,7 @@ enum : int {
     S_GATE = 3,      // open cells of the gate grid after the last gated frame
     S_LOSS_EMA = 4,  // running loss (float bits)
     S_F8_VER = 5,    // S_ADAM_T + 1 of the weights in the FP8 image (0: not packed)
+    S_DONE = 6,      // blocks of an Adam step finished so far (the last one resets it)
     S_WORDS = 8
 };
 
@@ -1236,8 +1237,18 @@ struct TrainArgs {
     uint8_t* hT[kMaxLayers];  // transposed inputs of each layer, per tile
     uint8_t* zT[kMaxLayers];  // transposed output gradients of each layer, per tile
     float* loss;                 // sum of per-sample losses (unnormalised)
+    uint32_t navail;             // records available when given by the host (written to S_NAVAIL by
+                                 // CTA 0 for the later kernels of the step); 0: read S_NAVAIL
     HashGrid hg;                 // composite encoding (levels 0: frequency encoding)
 };
+
+// Records available to a training step: given by the host (CTA 0 publishes the
+// count in S_NAVAIL for the step's later kernels) or left there by the frame.
+__device__ __forceinline__ uint32_t train_navail(const TrainArgs& a) {
+    if (a.navail == 0u) return a.state[S_NAVAIL];
+    if (blockIdx.x == 0 && threadIdx.x == 0) const_cast<uint32_t*>(a.state)[S_NAVAIL] = a.navail;
+    return a.navail;
+}
 
 // Write 64 (or 16) values of sample s into the transposed BF16 tile layout.
 template <int F>
@@ -1250,176 +1261,6 @@ __device__ __forceinline__ void store_T(uint8_t* tile, int s, const float* v) {
         *reinterpret_cast<__nv_bfloat16*>(region + umma::sw128_offset(f, c) + 2 * e) = h;
     }
 }
-
-template <int NL>
-__global__ void __launch_bounds__(128) k_train(TrainArgs a) {
-    extern __shared__ __align__(1024) uint8_t smem_raw[];
-    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    uint8_t* sf = smem + kTrainSmemF;
-    uint8_t* sb = smem + kTrainSmemB;
-    uint8_t* sa = smem + kTrainSmemA;
-    __shared__ uint64_t mb_w, mb_mma, mb_drain;
-    __shared__ uint32_t tslot;
-    const int t = threadIdx.x, warp = t >> 5;
-    const uint32_t ntiles = a.batch / kTile;
-    const uint32_t n_avail = a.state[S_NAVAIL];
-    const uint32_t seed = a.state[S_STEP];
-    if (blockIdx.x >= ntiles || n_avail < a.min_n || n_avail == 0) return;
-    if (warp == 0) umma::tmem_alloc(&tslot, 128);
-    if (t == 0) {
-        umma::mbar_init(&mb_w, 1);
-        umma::mbar_init(&mb_mma, 1);
-        umma::mbar_init(&mb_drain, 1);
-        umma::mbar_fence_init();
-    }
-    for (int i = t; i < kTile * 4; i += blockDim.x) {
-        const int r = i >> 2, c = 4 + (i & 3);
-        *reinterpret_cast<uint4*>(sa + kTile * 128 + umma::sw128_offset(r, c)) = make_uint4(0, 0, 0, 0);
-    }
-    __syncthreads();
-    umma::fence_after_sync();
-    const uint32_t tmem = tslot;
-    if (t == 0) {
-        umma::mbar_expect_tx(&mb_w, kFwdBytes<NL> + kBwdBytes<NL>);
-        umma::bulk_g2s(sf, a.fwd, kFwdBytes<NL>, &mb_w);
-        umma::bulk_g2s(sb, a.bwd, kBwdBytes<NL>, &mb_w);
-    }
-    bool ok = all_ok(umma::mbar_wait(&mb_w, 0, kSpinLimit));
-    const bool weights_in = ok;
-    uint32_t mph = 0;
-    float lsum = 0.0f;
-    for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        const uint32_t s = tile * kTile + (uint32_t)t;
-        // Sample selection as generarIndicesAleatorios (NrcKernel.cu:10-16).
-        uint32_t st = seed ^ s;
-        const uint32_t idx = pcg_next(st) % n_avail;
-        const TfgDatosMLP d = a.buf[idx];
-        float tgt[3] = {d.color.r, d.color.g, d.color.b};
-#pragma unroll
-        for (int k = 0; k < 3; ++k) if (tgt[k] > 100000.0f) tgt[k] = 100000.0f;   // NrcKernel.cu:52-57
-        {
-            uint32_t w[48];
-            encode(d, a.bounds, a.hg, w);
-            store_encoded(sa, t, w);
-            // transposed copy of the layer-0 input for dW0
-            float f[96];
-#pragma unroll
-            for (int k = 0; k < 48; ++k) {
-                __half2 h = *reinterpret_cast<__half2*>(&w[k]);
-                const float2 ff = __half22float2(h);
-                f[2 * k] = ff.x; f[2 * k + 1] = ff.y;
-            }
-            store_T<96>(a.hT[0] + (size_t)tile * (2 * 96 * 128), t, f);
-        }
-        umma::fence_smem_to_async();
-        __syncthreads();
-        uint32_t mask[NL - 1][2];
-        // forward
-        for (int l = 0; l < NL && ok; ++l) {
-            const int K = kCols<NL>(l), N = (l == NL - 1) ? kOutPad : kHid;
-            const uint32_t dcol = (l == NL - 1) ? 64u : 0u;
-            if (warp == 0) {   // converged warp, one elected lane issues (see k_infer)
-                umma::fence_after_sync();
-                if (umma::elect_one()) {
-                    issue_layer(tmem + dcol, sa, kTile * 128, sf + kFOff<NL>(l), kRows<NL>(l) * 128, K, N, false);
-                    umma::mma_commit(&mb_mma);
-                }
-                __syncwarp();
-            }
-            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
-            mph ^= 1u;
-            if (!ok) break;
-            umma::fence_after_sync();
-            if (l < NL - 1) {
-                float v[64];
-                tmem_row64(tmem, warp, 0, v);
-                uint32_t m0 = 0, m1 = 0;
-#pragma unroll
-                for (int i = 0; i < 64; ++i) {
-                    const bool on = v[i] > 0.0f;
-                    v[i] = on ? v[i] : 0.0f;
-                    if (i < 32) m0 |= (on ? 1u : 0u) << i;
-                    else m1 |= (on ? 1u : 0u) << (i - 32);
-                }
-                mask[l][0] = m0; mask[l][1] = m1;
-                store_row64<false>(sa, t, v);
-                store_T<64>(a.hT[l + 1] + (size_t)tile * (2 * 64 * 128), t, v);
-            } else {
-                float v[16];
-                umma::tmem_ld16(tmem + ((uint32_t)(32 * warp) << 16) + 64u, v);
-                // Relative L2 on luminance: the denominator is held constant.
-                const float lum = 0.299f * v[0] + 0.587f * v[1] + 0.114f * v[2];
-                const float den = lum * lum + 0.01f;
-                float g[64];
-#pragma unroll
-                for (int k = 0; k < 64; ++k) g[k] = 0.0f;
-#pragma unroll
-                for (int k = 0; k < 3; ++k) {
-                    const float diff = v[k] - tgt[k];
-                    lsum += diff * diff / den;
-                    g[k] = 2.0f * diff / den;
-                }
-                store_row64<true>(sa, t, g);
-                store_T<16>(a.zT[NL - 1] + (size_t)tile * (2 * 16 * 128), t, g);
-            }
-            umma::fence_before_sync();
-            umma::fence_smem_to_async();
-            __syncthreads();
-        }
-        // backward: dH_{l-1} = dZ_l * W_l, masked by the ReLU of layer l-1
-        for (int l = NL - 1; l >= 1 && ok; --l) {
-            const int K = (l == NL - 1) ? kOutPad : kHid;
-            if (warp == 0) {
-                umma::fence_after_sync();
-                if (umma::elect_one()) {
-                    issue_layer(tmem, sa, kTile * 128, sb + kBOff<NL>(l), 64 * 128, K, kHid, true);
-                    umma::mma_commit(&mb_mma);
-                }
-                __syncwarp();
-            }
-            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
-            mph ^= 1u;
-            if (!ok) break;
-            umma::fence_after_sync();
-            float v[64];
-            tmem_row64(tmem, warp, 0, v);
-#pragma unroll
-            for (int i = 0; i < 64; ++i) {
-                const uint32_t bit = (i < 32) ? (mask[l - 1][0] >> i) & 1u : (mask[l - 1][1] >> (i - 32)) & 1u;
-                v[i] = bit ? v[i] : 0.0f;
-            }
-            if (l > 1) store_row64<true>(sa, t, v);
-            store_T<64>(a.zT[l - 1] + (size_t)tile * (2 * 64 * 128), t, v);
-            umma::fence_before_sync();
-            umma::fence_smem_to_async();
-            __syncthreads();
-        }
-    }
-    // loss reduction
-    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xFFFFFFFFu, lsum, o);
-    if ((t & 31) == 0) atomicAdd(a.loss, lsum);
-    if (!ok && warp == 0) {   // after a timeout: the weight copy and every issued MMA finish first
-        if (umma::elect_one()) {
-            if (!weights_in) umma::mbar_wait(&mb_w, 0, kSpinLimit);
-            umma::mma_commit(&mb_drain);
-            umma::mbar_wait(&mb_drain, 0, kSpinLimit);
-        }
-        __syncwarp();
-    }
-    if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
-    __syncthreads();
-    if (warp == 0) umma::tmem_dealloc(tmem, 128);
-}
-
-// ------------------------------------------------------------------ width-128 training
-// k_train for 128-wide layers.  The whole network's forward and backward
-// images (308 KB) do not fit in shared memory, so they are streamed: the
-// NL forward images and then the NL - 1 backward images of each tile pass
-// through two 32 KB buffers, each bulk-copied as soon as the MMAs that read
-// the buffer's previous image have completed (one layer ahead).
-constexpr int kT128Buf = 32768;
-constexpr int kT128SmemA = 2 * kT128Buf;                    // activations: 2 regions x 16 KB
-constexpr int kT128Smem = kT128SmemA + 2 * kTile * 128;    // 98304
 
 // 32 values of row r, features f0 .. f0 + 31 (f0 a multiple of 32), into the
 // two-region A buffer as FP16 or BF16.
@@ -1446,6 +1287,208 @@ __device__ __forceinline__ void store_T32(uint8_t* tile, int s, int f0, const fl
         *reinterpret_cast<__nv_bfloat16*>(region + umma::sw128_offset(f0 + i, c) + 2 * e) = __float2bfloat16_rn(v[i]);
 }
 
+// Two warpgroups share a tile: thread t serves row (sample) t % 128, and
+// warpgroup t / 128 handles 32 of each layer's 64 columns (TMEM lane quarter
+// warp % 4, columns 32 * half ..), so every layer's epilogue -- TMEM load,
+// ReLU and mask, the FP16 / BF16 row for the next MMA, the transposed BF16
+// copy for the weight gradients -- is split over twice the warps, which the
+// chain of dependent layer rounds is bound by.  The weight images are copied
+// while the first tile is gathered and encoded.
+constexpr int kTrainThreads = 256;
+
+template <int NL>
+__global__ void __launch_bounds__(kTrainThreads) k_train(TrainArgs a) {
+    extern __shared__ __align__(1024) uint8_t smem_raw[];
+    uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
+    uint8_t* sf = smem + kTrainSmemF;
+    uint8_t* sb = smem + kTrainSmemB;
+    uint8_t* sa = smem + kTrainSmemA;
+    __shared__ uint64_t mb_w, mb_mma, mb_drain;
+    __shared__ uint32_t tslot;
+    const int t = threadIdx.x, warp = t >> 5;
+    const int r = t & (kTile - 1);              // the row (sample) of the tile
+    const int half = t >> 7;                    // columns 32 * half .. 32 * half + 31 of a layer
+    const uint32_t lanes = (uint32_t)(32 * (warp & 3)) << 16;
+    const uint32_t ntiles = a.batch / kTile;
+    const uint32_t n_avail = train_navail(a);
+    const uint32_t seed = a.state[S_STEP];
+    if (blockIdx.x >= ntiles || n_avail < a.min_n || n_avail == 0) return;
+    if (warp == 0) umma::tmem_alloc(&tslot, 128);
+    if (t == 0) {
+        umma::mbar_init(&mb_w, 1);
+        umma::mbar_init(&mb_mma, 1);
+        umma::mbar_init(&mb_drain, 1);
+        umma::mbar_fence_init();
+    }
+    for (int i = t; i < kTile * 4; i += blockDim.x) {
+        const int rr = i >> 2, c = 4 + (i & 3);
+        *reinterpret_cast<uint4*>(sa + kTile * 128 + umma::sw128_offset(rr, c)) = make_uint4(0, 0, 0, 0);
+    }
+    __syncthreads();
+    umma::fence_after_sync();
+    const uint32_t tmem = tslot;
+    if (t == 0) {
+        umma::mbar_expect_tx(&mb_w, kFwdBytes<NL> + kBwdBytes<NL>);
+        umma::bulk_g2s(sf, a.fwd, kFwdBytes<NL>, &mb_w);
+        umma::bulk_g2s(sb, a.bwd, kBwdBytes<NL>, &mb_w);
+    }
+    bool ok = true, weights_in = false;
+    uint32_t mph = 0;
+    float lsum = 0.0f;
+    for (uint32_t tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        uint8_t* h0 = a.hT[0] + (size_t)tile * (2 * 96 * 128);
+        float tgt[3] = {0.0f, 0.0f, 0.0f};
+        if (half == 0) {
+            const uint32_t s = tile * kTile + (uint32_t)r;
+            // Sample selection as generarIndicesAleatorios (NrcKernel.cu:10-16).
+            uint32_t st = seed ^ s;
+            const uint32_t idx = pcg_next(st) % n_avail;
+            const TfgDatosMLP d = a.buf[idx];
+            tgt[0] = d.color.r; tgt[1] = d.color.g; tgt[2] = d.color.b;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) if (tgt[k] > 100000.0f) tgt[k] = 100000.0f;   // NrcKernel.cu:52-57
+            uint32_t w[48];
+            encode(d, a.bounds, a.hg, w);
+            store_encoded(sa, r, w);
+            // transposed copy of the layer-0 input for dW0: features 0..63 here,
+            // 64..95 by the other warpgroup once the row is in shared memory
+            float f[64];
+#pragma unroll
+            for (int k = 0; k < 32; ++k) {
+                const float2 ff = __half22float2(*reinterpret_cast<__half2*>(&w[k]));
+                f[2 * k] = ff.x; f[2 * k + 1] = ff.y;
+            }
+            store_T32<96>(h0, r, 0, f);
+            store_T32<96>(h0, r, 32, f + 32);
+        }
+        umma::fence_smem_to_async();
+        if (!weights_in) {
+            ok = all_ok(umma::mbar_wait(&mb_w, 0, kSpinLimit));
+            weights_in = ok;
+            if (!ok) break;
+        } else {
+            __syncthreads();
+        }
+        if (half == 1) {
+            const uint8_t* reg1 = sa + kTile * 128;
+            float f[32];
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                const uint4 q = *reinterpret_cast<const uint4*>(reg1 + umma::sw128_offset(r, c));
+                const uint32_t qq[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const float2 ff = __half22float2(*reinterpret_cast<const __half2*>(&qq[e]));
+                    f[8 * c + 2 * e] = ff.x; f[8 * c + 2 * e + 1] = ff.y;
+                }
+            }
+            store_T32<96>(h0, r, 64, f);
+        }
+        uint32_t mask[NL - 1];
+        // forward
+        for (int l = 0; l < NL && ok; ++l) {
+            const int K = kCols<NL>(l), N = (l == NL - 1) ? kOutPad : kHid;
+            const uint32_t dcol = (l == NL - 1) ? 64u : 0u;
+            if (warp == 0) {   // converged warp, one elected lane issues (see k_infer)
+                umma::fence_after_sync();
+                if (umma::elect_one()) {
+                    issue_layer(tmem + dcol, sa, kTile * 128, sf + kFOff<NL>(l), kRows<NL>(l) * 128, K, N, false);
+                    umma::mma_commit(&mb_mma);
+                }
+                __syncwarp();
+            }
+            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+            mph ^= 1u;
+            if (!ok) break;
+            umma::fence_after_sync();
+            if (l < NL - 1) {
+                float v[32];
+                umma::tmem_ld32(tmem + lanes + (uint32_t)(32 * half), v);
+                uint32_t m = 0;
+#pragma unroll
+                for (int i = 0; i < 32; ++i) {
+                    const bool on = v[i] > 0.0f;
+                    v[i] = on ? v[i] : 0.0f;
+                    m |= (on ? 1u : 0u) << i;
+                }
+                mask[l] = m;
+                store_row32<false>(sa, r, 32 * half, v);
+                store_T32<64>(a.hT[l + 1] + (size_t)tile * (2 * 64 * 128), r, 32 * half, v);
+            } else if (half == 0) {
+                float v[16];
+                umma::tmem_ld16(tmem + lanes + 64u, v);
+                // Relative L2 on luminance: the denominator is held constant.
+                const float lum = 0.299f * v[0] + 0.587f * v[1] + 0.114f * v[2];
+                const float den = lum * lum + 0.01f;
+                float g[64];
+#pragma unroll
+                for (int k = 0; k < 64; ++k) g[k] = 0.0f;
+#pragma unroll
+                for (int k = 0; k < 3; ++k) {
+                    const float diff = v[k] - tgt[k];
+                    lsum += diff * diff / den;
+                    g[k] = 2.0f * diff / den;
+                }
+                store_row64<true>(sa, r, g);
+                store_T<16>(a.zT[NL - 1] + (size_t)tile * (2 * 16 * 128), r, g);
+            }
+            umma::fence_before_sync();
+            umma::fence_smem_to_async();
+            __syncthreads();
+        }
+        // backward: dH_{l-1} = dZ_l * W_l, masked by the ReLU of layer l-1
+        for (int l = NL - 1; l >= 1 && ok; --l) {
+            const int K = (l == NL - 1) ? kOutPad : kHid;
+            if (warp == 0) {
+                umma::fence_after_sync();
+                if (umma::elect_one()) {
+                    issue_layer(tmem, sa, kTile * 128, sb + kBOff<NL>(l), 64 * 128, K, kHid, true);
+                    umma::mma_commit(&mb_mma);
+                }
+                __syncwarp();
+            }
+            ok = all_ok(umma::mbar_wait(&mb_mma, mph, kSpinLimit));
+            mph ^= 1u;
+            if (!ok) break;
+            umma::fence_after_sync();
+            float v[32];
+            umma::tmem_ld32(tmem + lanes + (uint32_t)(32 * half), v);
+            const uint32_t m = mask[l - 1];
+#pragma unroll
+            for (int i = 0; i < 32; ++i) v[i] = ((m >> i) & 1u) ? v[i] : 0.0f;
+            if (l > 1) store_row32<true>(sa, r, 32 * half, v);
+            store_T32<64>(a.zT[l - 1] + (size_t)tile * (2 * 64 * 128), r, 32 * half, v);
+            umma::fence_before_sync();
+            umma::fence_smem_to_async();
+            __syncthreads();
+        }
+    }
+    // loss reduction (the loss lives in the first warpgroup)
+    for (int o = 16; o > 0; o >>= 1) lsum += __shfl_down_sync(0xFFFFFFFFu, lsum, o);
+    if ((t & 31) == 0 && half == 0) atomicAdd(a.loss, lsum);
+    if (!ok && warp == 0) {   // after a timeout: the weight copy and every issued MMA finish first
+        if (umma::elect_one()) {
+            if (!weights_in) umma::mbar_wait(&mb_w, 0, kSpinLimit);
+            umma::mma_commit(&mb_drain);
+            umma::mbar_wait(&mb_drain, 0, kSpinLimit);
+        }
+        __syncwarp();
+    }
+    if (!ok && t == 0) atomicExch(&g_mlp_error, 1);
+    __syncthreads();
+    if (warp == 0) umma::tmem_dealloc(tmem, 128);
+}
+
+// ------------------------------------------------------------------ width-128 training
+// k_train for 128-wide layers.  The whole network's forward and backward
+// images (308 KB) do not fit in shared memory, so they are streamed: the
+// NL forward images and then the NL - 1 backward images of each tile pass
+// through two 32 KB buffers, each bulk-copied as soon as the MMAs that read
+// the buffer's previous image have completed (one layer ahead).
+constexpr int kT128Buf = 32768;
+constexpr int kT128SmemA = 2 * kT128Buf;                    // activations: 2 regions x 16 KB
+constexpr int kT128Smem = kT128SmemA + 2 * kTile * 128;    // 98304
+
 template <int NL>
 __global__ void __launch_bounds__(128) k_train128(TrainArgs a) {
     static_assert(NL == 4 || NL == 6 || NL == 8, "width 128: 3, 5 or 7 hidden layers");
@@ -1457,7 +1500,7 @@ __global__ void __launch_bounds__(128) k_train128(TrainArgs a) {
     __shared__ uint32_t tslot;
     const int t = threadIdx.x, warp = t >> 5;
     const uint32_t ntiles = a.batch / kTile;
-    const uint32_t n_avail = a.state[S_NAVAIL];
+    const uint32_t n_avail = train_navail(a);
     const uint32_t seed = a.state[S_STEP];
     if (blockIdx.x >= ntiles || n_avail < a.min_n || n_avail == 0) return;
     const uint32_t total = (ntiles - blockIdx.x + gridDim.x - 1) / gridDim.x * kItems;   // images this CTA loads
@@ -1759,13 +1802,19 @@ __global__ void __launch_bounds__(128) k_infer128s(const TfgDatosMLP* __restrict
 // ------------------------------------------------------------------ weight gradients
 // dW_l[out][in] = sum_s dZ_l[s][out] * H_l[s][in].  A = dZ^T (out rows padded
 // to 128 with zeros), B = H^T (in rows), K = samples.  One CTA reduces
-// `tiles_per_cta` sample tiles of one layer into TMEM, then adds its partial
-// sums to the FP32 gradient with atomics.
-constexpr int kWgSmemA = 0;                          // 2 stages x 2 regions x 16 KB
-constexpr int kWgSmemB = 65536;                      // 2 stages x 2 x FH x 128 (FH <= max(96, HID))
+// `tiles_per_cta` sample tiles of one layer into TMEM and stores its partial
+// sums in its own slice of `part` (the Adam step adds the slices in order).
+//
+// Tiles stream through kWgStages shared-memory stages.  (Four stages at
+// width 64, as many as fit, measured no faster than two: 11.0 against
+// 10.8 us per 16,384-sample step.)
+template <int HID> constexpr int kWgStages = 2;
+constexpr int kWgSmemA = 0;                                             // stages x 2 regions x 16 KB
+template <int HID> constexpr int kWgSmemB = kWgStages<HID> * 32768;    // stages x 2 x FH x 128
 template <int HID> constexpr int kWgStageB = 2 * (HID > 96 ? HID : 96) * 128;
-template <int HID> constexpr int kWgSmemH = kWgSmemB + 2 * kWgStageB<HID>;
-constexpr int kWgSmem = kWgSmemH<64>;                // 114688
+template <int HID> constexpr int kWgSmemH = kWgSmemB<HID> + kWgStages<HID> * kWgStageB<HID>;
+constexpr int kWgSmem = kWgSmemH<64>;                                   // 114688
+static_assert(kWgSmemH<64> + 1024 <= 232448 && kWgSmemH<128> + 1024 <= 232448, "k_wgrad shared memory");
 
 struct WgradArgs {
     const uint8_t* zT[kMaxLayers];
@@ -1779,9 +1828,10 @@ struct WgradArgs {
 
 template <int NL, int HID>
 __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
+    constexpr int S = kWgStages<HID>;
     extern __shared__ __align__(1024) uint8_t smem_raw[];
     uint8_t* smem = reinterpret_cast<uint8_t*>((reinterpret_cast<uintptr_t>(smem_raw) + 1023) & ~uintptr_t(1023));
-    __shared__ uint64_t mb_ld[2], mb_mma[2], mb_done;
+    __shared__ uint64_t mb_ld[S], mb_mma[S], mb_done;
     __shared__ uint32_t tslot;
     const int t = threadIdx.x, warp = t >> 5;
     const int l = blockIdx.y;
@@ -1791,22 +1841,26 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     const uint32_t t1 = min(a.ntiles, t0 + a.tiles_per_cta);
     if (warp == 0) umma::tmem_alloc(&tslot, 128);
     if (t == 0) {
-        for (int k = 0; k < 2; ++k) { umma::mbar_init(&mb_ld[k], 1); umma::mbar_init(&mb_mma[k], 1); }
+        for (int k = 0; k < S; ++k) { umma::mbar_init(&mb_ld[k], 1); umma::mbar_init(&mb_mma[k], 1); }
         umma::mbar_init(&mb_done, 1);
         umma::mbar_fence_init();
     }
-    // Zero both A stages: rows >= FZ stay zero (padding of M to 128).
-    for (int i = t; i < 65536 / 16; i += blockDim.x) reinterpret_cast<uint4*>(smem + kWgSmemA)[i] = make_uint4(0, 0, 0, 0);
+    // Zero every A stage: rows >= FZ stay zero (padding of M to 128).
+    for (int i = t; i < S * 32768 / 16; i += blockDim.x)
+        reinterpret_cast<uint4*>(smem + kWgSmemA)[i] = make_uint4(0, 0, 0, 0);
     umma::fence_smem_to_async();
     __syncthreads();
     umma::fence_after_sync();
     const uint32_t tmem = tslot;
     const uint32_t zbytes = (uint32_t)FZ * 128, hbytes = 2u * FH * 128;
-    bool ld_pending[2] = {false, false};
+    bool ld_pending[S];
+    uint32_t ldph[S], mmph[S];
+#pragma unroll
+    for (int k = 0; k < S; ++k) { ld_pending[k] = false; ldph[k] = 0; mmph[k] = 0; }
     auto load = [&](uint32_t tile, int stage) {
         ld_pending[stage] = true;
         uint8_t* sA = smem + kWgSmemA + stage * 32768;
-        uint8_t* sB = smem + kWgSmemB + stage * kWgStageB<HID>;
+        uint8_t* sB = smem + kWgSmemB<HID> + stage * kWgStageB<HID>;
         const uint8_t* gz = a.zT[l] + (size_t)tile * 2 * zbytes;
         const uint8_t* gh = a.hT[l] + (size_t)tile * hbytes;
         umma::mbar_expect_tx(&mb_ld[stage], 2 * zbytes + hbytes);
@@ -1815,20 +1869,18 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
         umma::bulk_g2s(sB, gh, hbytes, &mb_ld[stage]);
     };
     bool ok = true;
-    uint32_t ldph[2] = {0, 0}, mmph[2] = {0, 0};
     if (t == 0) {
-        load(t0, 0);
-        if (t0 + 1 < t1) load(t0 + 1, 1);
+        for (int k = 0; k < S && t0 + (uint32_t)k < t1; ++k) load(t0 + (uint32_t)k, k);
         const uint32_t id = umma::idesc_f16(kTile, FH, true);
         for (uint32_t tile = t0; tile < t1 && ok; ++tile) {
-            const int stage = (int)((tile - t0) & 1u);
+            const int stage = (int)((tile - t0) % (uint32_t)S);
             ok = umma::mbar_wait(&mb_ld[stage], ldph[stage], kSpinLimit);
             if (!ok) break;
             ldph[stage] ^= 1u;
             ld_pending[stage] = false;
             umma::fence_after_sync();
             const uint8_t* sA = smem + kWgSmemA + stage * 32768;
-            const uint8_t* sB = smem + kWgSmemB + stage * kWgStageB<HID>;
+            const uint8_t* sB = smem + kWgSmemB<HID> + stage * kWgStageB<HID>;
             for (int s = 0; s < 8; ++s) {
                 const int reg = s >> 2, kk = s & 3;
                 const uint64_t ad = umma::sdesc_sw128(umma::smem_u32(sA + reg * 16384 + kk * 32));
@@ -1836,19 +1888,19 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
                 umma::mma_f16(tmem, ad, bd, id, tile > t0 || s > 0);
             }
             umma::mma_commit(&mb_mma[stage]);
-            if (tile + 2 < t1) {
+            if (tile + S < t1) {
                 // Refill this stage once its MMAs have read it.
                 ok = umma::mbar_wait(&mb_mma[stage], mmph[stage], kSpinLimit);
                 mmph[stage] ^= 1u;
                 if (!ok) break;
-                load(tile + 2, stage);
+                load(tile + S, stage);
             }
         }
         // One more commit tracks every MMA issued above; after a timeout the
         // loads still in flight are waited for as well (no copy lands after exit).
         umma::mma_commit(&mb_done);
         ok = umma::mbar_wait(&mb_done, 0, kSpinLimit) && ok;
-        for (int k = 0; k < 2; ++k)
+        for (int k = 0; k < S; ++k)
             if (ld_pending[k]) umma::mbar_wait(&mb_ld[k], ldph[k], kSpinLimit);
     }
     ok = all_ok(ok);
@@ -1908,6 +1960,12 @@ struct AdamArgs {
     uint32_t min_n;
     int update;                    // 0: only re-pack (after loading parameters)
     int live0;                     // live input columns of layer 0 (the rest stay zero)
+    // When set, the last block to finish ends the step as k_tick does (step
+    // counter, Adam time, running loss); `done` counts the finished blocks.
+    int tick;
+    uint32_t* done;
+    const float* loss_sum;
+    float inv_count;
 };
 
 template <int NL, int HID>
@@ -1919,47 +1977,73 @@ __device__ __forceinline__ void layer_of(int i, int& l, int& r, int& c) {
     c = j % cols_h<HID>(l);
 }
 
+// Ends a step: advance the step counter and Adam time, keep a running loss.
+__device__ __forceinline__ void tick_state(uint32_t* state, const float* loss_sum, float inv_count, uint32_t min_n) {
+    const uint32_t n = state[S_NAVAIL];
+    if (n < min_n || n == 0) return;
+    state[S_STEP] += 1u;
+    state[S_ADAM_T] += 1u;
+    const float loss = *loss_sum * inv_count;
+    float ema = __uint_as_float(state[S_LOSS_EMA]);
+    ema = (state[S_ADAM_T] == 1u) ? loss : 0.9f * ema + 0.1f * loss;
+    state[S_LOSS_EMA] = __float_as_uint(ema);
+}
+
 template <int NL, int HID>
 __global__ void k_adam(AdamArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= params_h<HID>(NL)) return;
-    int l, r, c;
-    layer_of<NL, HID>(i, l, r, c);
-    // Padded entries (output rows 3..15, input columns past the encoding of layer 0) stay zero.
-    const bool live = !(l == NL - 1 && r >= 3) && !(l == 0 && c >= a.live0);
-    float w = a.w[i];
-    float e = a.ema[i];
-    const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
-    const float tn = (float)(a.state[S_ADAM_T] + (update ? 1u : 0u));
-    if (update && live) {
-        const float bc1 = 1.0f - powf(a.beta1, tn), bc2 = 1.0f - powf(a.beta2, tn);
-        float gs = 0.0f;
-        for (uint32_t k = 0; k < a.groups; ++k) gs += a.part[(size_t)k * params_h<HID>(NL) + i];
-        const float g = gs * a.grad_scale;
-        const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
-        const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
-        a.m[i] = m;
-        a.v[i] = v;
-        w -= a.lr * (m / bc1) / (sqrtf(v / bc2) + a.eps);
-        e = a.decay * e + (1.0f - a.decay) * w;
-        a.w[i] = w;
-        a.ema[i] = e;
+    if (i < params_h<HID>(NL)) {
+        int l, r, c;
+        layer_of<NL, HID>(i, l, r, c);
+        // Padded entries (output rows 3..15, input columns past the encoding of layer 0) stay zero.
+        const bool live = !(l == NL - 1 && r >= 3) && !(l == 0 && c >= a.live0);
+        float w = a.w[i];
+        float e = a.ema[i];
+        const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
+        const float tn = (float)(a.state[S_ADAM_T] + (update ? 1u : 0u));
+        if (update && live) {
+            const float bc1 = 1.0f - powf(a.beta1, tn), bc2 = 1.0f - powf(a.beta2, tn);
+            float gs = 0.0f;
+            for (uint32_t k = 0; k < a.groups; ++k) gs += a.part[(size_t)k * params_h<HID>(NL) + i];
+            const float g = gs * a.grad_scale;
+            const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
+            const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
+            a.m[i] = m;
+            a.v[i] = v;
+            w -= a.lr * (m / bc1) / (sqrtf(v / bc2) + a.eps);
+            e = a.decay * e + (1.0f - a.decay) * w;
+            a.w[i] = w;
+            a.ema[i] = e;
+        }
+        if (!live) { w = 0.0f; e = 0.0f; }
+        const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
+        const float ew = ema_debias > 0.0f ? e / ema_debias : w;
+        // forward / inference images: row r, K index c
+        const int rows = rows_h<HID>(NL, l);
+        const uint32_t off = (uint32_t)foff_h<HID>(NL, l) + (uint32_t)(c >> 6) * rows * 128 +
+                             umma::sw128_offset(r, (c & 63) >> 3) + 2 * (c & 7);
+        *reinterpret_cast<__half*>(a.fwd + off) = __float2half_rn(w);
+        *reinterpret_cast<__half*>(a.inf + off) = __float2half_rn(ew);
+        *reinterpret_cast<__nv_bfloat16*>(a.inf_bf + off) = __float2bfloat16_rn(ew);
+        if (l >= 1) {
+            // backward image: W^T, row = c (input unit), K index = r (output unit)
+            const uint32_t boff = (uint32_t)boff_h<HID>(NL, l) + (uint32_t)(r >> 6) * (HID * 128) +
+                                  umma::sw128_offset(c, (r & 63) >> 3) + 2 * (r & 7);
+            *reinterpret_cast<__nv_bfloat16*>(a.bwd + boff) = __float2bfloat16_rn(w);
+        }
     }
-    if (!live) { w = 0.0f; e = 0.0f; }
-    const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
-    const float ew = ema_debias > 0.0f ? e / ema_debias : w;
-    // forward / inference images: row r, K index c
-    const int rows = rows_h<HID>(NL, l);
-    const uint32_t off = (uint32_t)foff_h<HID>(NL, l) + (uint32_t)(c >> 6) * rows * 128 +
-                         umma::sw128_offset(r, (c & 63) >> 3) + 2 * (c & 7);
-    *reinterpret_cast<__half*>(a.fwd + off) = __float2half_rn(w);
-    *reinterpret_cast<__half*>(a.inf + off) = __float2half_rn(ew);
-    *reinterpret_cast<__nv_bfloat16*>(a.inf_bf + off) = __float2bfloat16_rn(ew);
-    if (l >= 1) {
-        // backward image: W^T, row = c (input unit), K index = r (output unit)
-        const uint32_t boff = (uint32_t)boff_h<HID>(NL, l) + (uint32_t)(r >> 6) * (HID * 128) +
-                              umma::sw128_offset(c, (r & 63) >> 3) + 2 * (r & 7);
-        *reinterpret_cast<__nv_bfloat16*>(a.bwd + boff) = __float2bfloat16_rn(w);
+    if (!a.tick) return;
+    // Every block has read S_ADAM_T (its image stores depend on the value)
+    // before it counts itself done, so the last one may advance it; the state
+    // words are written by that block alone.
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const uint32_t prev = atomicAdd(a.done, 1u);
+        if (prev == gridDim.x - 1) {
+            __threadfence();
+            *a.done = 0u;
+            tick_state(const_cast<uint32_t*>(a.state), a.loss_sum, a.inv_count, a.min_n);
+        }
     }
 }
 
@@ -2128,17 +2212,11 @@ __global__ void k_hash_init(float* w, size_t count, uint64_t seed) {
     }
 }
 
-// After a step: advance the step counter and Adam time, keep a running loss.
+// After a step of a model with hash-grid tables (whose table update reads
+// the Adam time after k_adam): the same end of step as k_adam's last block.
 __global__ void k_tick(uint32_t* state, const float* loss_sum, float inv_count, uint32_t min_n) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const uint32_t n = state[S_NAVAIL];
-    if (n < min_n || n == 0) return;
-    state[S_STEP] += 1u;
-    state[S_ADAM_T] += 1u;
-    const float loss = *loss_sum * inv_count;
-    float ema = __uint_as_float(state[S_LOSS_EMA]);
-    ema = (state[S_ADAM_T] == 1u) ? loss : 0.9f * ema + 0.1f * loss;
-    state[S_LOSS_EMA] = __float_as_uint(ema);
+    tick_state(state, loss_sum, inv_count, min_n);
 }
 
 // ------------------------------------------------------------------ cache gate
@@ -2318,7 +2396,7 @@ uint64_t splitmix(uint64_t& s) {
     return z ^ (z >> 31);
 }
 
-int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
+int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n, bool tick) {
     mlp::AdamArgs a;
     a.w = n->w; a.m = n->m; a.v = n->v; a.ema = n->ema; a.grad = n->grad;
     a.part = update ? n->wpart : nullptr;
@@ -2330,6 +2408,10 @@ int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n) {
     a.min_n = min_n;
     a.update = update ? 1 : 0;
     a.live0 = n->hlevels ? mlp::kHashLive : mlp::kFreqLive;
+    a.tick = tick ? 1 : 0;
+    a.done = n->dstate + mlp::S_DONE;
+    a.loss_sum = n->loss;
+    a.inv_count = 1.0f / (3.0f * (float)n->batch);
     with_width(n, [&](auto c, auto w) {
         constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
         mlp::k_adam<NL, HID><<<(mlp::params_h<HID>(NL) + 255) / 256, 256, 0, s>>>(a);
@@ -2434,7 +2516,10 @@ int enqueue_wgrad_sum(ColorMlp* n, uint32_t min_n, cudaStream_t s) {
 
 // Forward/backward, weight gradients (and, with `update`, Adam + tick) of one
 // step whose record count and seed are already in the device state.
-int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool update, cudaStream_t s) {
+// One training step.  `navail`: records available, given by the host (0:
+// already in S_NAVAIL, as a frame leaves it).
+int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool update, cudaStream_t s,
+                 uint32_t navail = 0) {
     const uint32_t tiles = n->batch / mlp::kTile;
     cudaError_t e = cudaMemsetAsync(n->loss, 0, sizeof(float), s);
     if (e != cudaSuccess) return cuda_fail(e, "mlp step");
@@ -2442,12 +2527,13 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     ta.buf = buf; ta.state = n->dstate; ta.min_n = min_n; ta.batch = n->batch;
     ta.bounds = n->bounds; ta.fwd = n->fwd; ta.bwd = n->bwd; ta.loss = n->loss;
     ta.hg = hash_view(n, true);
+    ta.navail = navail;
     for (int l = 0; l < mlp::kMaxLayers; ++l) { ta.hT[l] = n->hT[l]; ta.zT[l] = n->zT[l]; }
     with_width(n, [&](auto c, auto w) {
         constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
         const uint32_t grid = std::min<uint32_t>(tiles, (uint32_t)n->sms);
         if constexpr (HID == 128) mlp::k_train128<NL><<<grid, 128, mlp::kT128Smem + 1024, s>>>(ta);
-        else mlp::k_train<NL><<<grid, 128, mlp::kTrainSmem + 1024, s>>>(ta);
+        else mlp::k_train<NL><<<grid, mlp::kTrainThreads, mlp::kTrainSmem + 1024, s>>>(ta);
         return 0;
     });
     e = cudaGetLastError();
@@ -2463,10 +2549,14 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
         if (e != cudaSuccess) return cuda_fail(e, "mlp step: table gradient");
     }
     if (!update) return enqueue_wgrad_sum(n, min_n, s);
-    if (int rc = repack(n, s, true, min_n)) return rc;
-    mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n);
-    e = cudaGetLastError();
-    if (e != cudaSuccess) return cuda_fail(e, "mlp step: tick");
+    // Without tables the Adam kernel's last block ends the step; the table
+    // update reads the Adam time after it, so with tables k_tick does.
+    if (int rc = repack(n, s, true, min_n, n->hlevels == 0)) return rc;
+    if (n->hlevels) {
+        mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return cuda_fail(e, "mlp step: tick");
+    }
     return ok();
 }
 
@@ -2935,7 +3025,7 @@ int create_model(uint32_t n_in, uint32_t n_out, uint32_t batch, uint64_t seed, i
     if (e == cudaSuccess) e = cudaMemset(n->v, 0, pb);
     if (e == cudaSuccess) e = cudaMemset(n->grad, 0, pb);
     if (e != cudaSuccess) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return tfg::cuda_fail(e, "tfgMlpCreate"); }
-    if (int rc = tfg::repack(n, 0, false, 1)) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return rc; }
+    if (int rc = tfg::repack(n, 0, false, 1, false)) { tfgMlpDestroy(reinterpret_cast<TfgColorMLP*>(n)); return rc; }
     static bool attrs = false;
     if (!attrs) {
         set_kernel_attrs<4>();
@@ -3185,8 +3275,7 @@ extern "C" int tfgMlpTrainStep(TfgColorMLP* h, const TfgDatosMLP* buffer, uint32
     if (n_available < 100) return tfg::ok();   // mlp.cpp:96: too few samples, no step
     cudaStream_t s = (cudaStream_t)stream;
     if (int rc = tfg::mlp_prepare(n)) return rc;
-    if (int rc = tfg::set_word(n, M::S_NAVAIL, n_available, s)) return rc;
-    if (int rc = tfg::enqueue_step(n, buffer, 100, true, s)) return rc;
+    if (int rc = tfg::enqueue_step(n, buffer, 100, true, s, n_available)) return rc;
     if (loss_out) {
         float l = 0.0f;
         cudaError_t e = cudaMemcpyAsync(&l, n->loss, sizeof(float), cudaMemcpyDeviceToHost, s);
@@ -3229,7 +3318,7 @@ extern "C" int tfgMlpSetParams(TfgColorMLP* h, const float* host, uint32_t count
         if (e == cudaSuccess) e = cudaMemset(n->hgrad, 0, hb);
     }
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetParams");
-    if (int rc = tfg::repack(n, 0, false, 1)) return rc;
+    if (int rc = tfg::repack(n, 0, false, 1, false)) return rc;
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpSetParams");
     return tfg::ok();
@@ -3403,7 +3492,7 @@ extern "C" int tfgMlpLoad(TfgColorMLP* h, const char* path) {
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpLoad");
     n->bounds = M::Bounds{{lo[0], lo[1], lo[2]}, {hi[0], hi[1], hi[2]}};
     n->lr = hyper[0]; n->beta1 = hyper[1]; n->beta2 = hyper[2]; n->eps = hyper[3]; n->decay = hyper[4];
-    if (int rc = tfg::repack(n, 0, false, 1)) return rc;   // operand images of the loaded arrays
+    if (int rc = tfg::repack(n, 0, false, 1, false)) return rc;   // operand images of the loaded arrays
     e = cudaDeviceSynchronize();
     if (e != cudaSuccess) return tfg::cuda_fail(e, "tfgMlpLoad");
     return tfg::ok();
