@@ -192,6 +192,14 @@ def replicas_value(paths_per_rank: int, ms_max: float, world: int) -> float:
     return world * paths_per_rank / (ms_max * 1e-3) / 1e6
 
 
+def replica_frame(rank: int, step: int, steps: int) -> int:
+    """First frame number of timed step `step` on `rank`: every replica renders
+    its own frames (rank r's steps are frames 1 + SPP * (r * steps + s) ..),
+    so N ranks trace N distinct 64-spp frames per step; rank 0's are the
+    single-GPU run's."""
+    return 1 + SPP * (rank * steps + step)
+
+
 def cpu_oracle_sample(scene, hb, rows: int, nthreads: int, frame: int = 1) -> tuple[float, int]:
     """Time the CPU oracle (a restatement of the reference path tracer) on a
     band of `rows` image rows at 1 spp; returns (seconds, paths)."""
@@ -972,7 +980,7 @@ def main():
         for s in range(args.steps):
             flush.fill_(s & 0xFF)
             accum.zero_()
-            pt.render_pass(ds, timed, 1 + SPP * s, None, accum)
+            pt.render_pass(ds, timed, replica_frame(rank, s, args.steps), None, accum)
         ev1.record(stream)
         torch.cuda.synchronize()
     ms = ev0.elapsed_time(ev1)
