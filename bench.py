@@ -1130,12 +1130,10 @@ def main():
             "tuning": tuning.__dict__, "seconds": round(tune_s, 2), "spp_per_pass": min(SPP, 16),
             "pass_ms_start": round(tune_table[0][1], 3), "pass_ms_tuned": round(tuned_ms, 3),
             "candidates": [[t.wavefront_paths, t.trace_threads, t.trace_warps_per_sm, t.refill_min,
-                            t.shadow_one_lane, t.refill_min_primary, t.overlap_shadow, t.shadow_postpone,
-                            round(ms, 3)]
+                            t.shadow_one_lane, t.refill_min_primary, t.overlap_shadow, round(ms, 3)]
                            for t, ms in tune_table],
             "candidate_fields": ["wavefront_paths", "trace_threads", "trace_warps_per_sm", "refill_min",
-                                 "shadow_one_lane", "refill_min_primary", "overlap_shadow", "shadow_postpone",
-                                 "ms_per_pass"],
+                                 "shadow_one_lane", "refill_min_primary", "overlap_shadow", "ms_per_pass"],
         },
         "gpu_launches": launches,
         "clocks": clocks,

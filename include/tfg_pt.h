@@ -342,9 +342,7 @@ typedef struct TfgRenderTuning {
                                    in 8 x 4 pixel tiles; 32 = whole-warp batches), 0 (default) = refill_min */
     int32_t overlap_shadow;     /* 1 (default): each bounce's shadow rays run on a second stream beside the
                                    next bounce's closest-hit trace; 0: one stream */
-    int32_t shadow_postpone;    /* a shadow ray's triangle tests wait (on its stack) until at least this many
-                                   lanes of its warp test triangles together, 0 (default) = never wait;
-                                   0..32.  Occlusion does not depend on the test order */
+    int32_t reserved[1];
 } TfgRenderTuning;
 
 void tfgRenderTuningDefault(TfgRenderTuning* t);
@@ -364,7 +362,7 @@ typedef struct TfgTuneRecord {
  * call's spp capped at 16) under candidate tunings with CUDA events on
  * `stream`, one setting at a time starting from the current one (queue size,
  * then CTA size, warps per SM, refill threshold, shadow lanes, first-bounce
- * refill threshold, shadow / trace overlap, shadow triangle postponing), `repeats`
+ * refill threshold, shadow / trace overlap), `repeats`
  * timed passes per candidate after one warm-up (0 = 3).  A candidate must be
  * at least 1% faster to replace the best.  Sets the winner on the current
  * device and returns it in `out`.  `num_records` (optional) gets the number

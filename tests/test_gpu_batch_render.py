@@ -81,8 +81,7 @@ def test_batch_pass_under_tuning(dss):
     total = sum(d.scene.width * d.scene.height for d in dss)
     for t in (pt.RenderTuning(wavefront_paths=1024), pt.RenderTuning(wavefront_paths=total + 333),
               pt.RenderTuning(wavefront_paths=4 * total, trace_threads=64, refill_min=3),
-              pt.RenderTuning(wavefront_paths=2 * total, overlap_shadow=1),
-              pt.RenderTuning(shadow_postpone=8)):
+              pt.RenderTuning(wavefront_paths=2 * total, overlap_shadow=1)):
         pt.set_tuning(t)
         got_i, got_a = _batch(dss, p, 3)
         for gi, ga, wi, wa in zip(got_i, got_a, want_i, want_a):

@@ -1,6 +1,6 @@
 """Launch tuning and the autotuners.  A tuning changes how paths are scheduled
 (wavefront size, CTA size and residency, refill threshold, lanes per shadow
-query, the order of a shadow ray's triangle tests), never what a path computes, so every tuning must give the same
+query), never what a path computes, so every tuning must give the same
 image bit for bit -- plain passes, cache frames (eager and captured as CUDA
 graphs) and the allocation-free pass.  The model autotuner must leave the
 model's state untouched."""
@@ -58,10 +58,6 @@ TUNINGS = [
     pt.RenderTuning(refill_min=1),
     pt.RenderTuning(refill_min=32),
     pt.RenderTuning(shadow_one_lane=1),
-    pt.RenderTuning(shadow_postpone=32),                 # triangle tests postponed whenever a lane is missing
-    pt.RenderTuning(shadow_postpone=8, shadow_one_lane=1),
-    pt.RenderTuning(shadow_postpone=12, trace_threads=64),
-    pt.RenderTuning(shadow_postpone=4, shadow_one_lane=1, wavefront_paths=3 * N + 7, overlap_shadow=0),
     pt.RenderTuning(refill_min_primary=32),
     pt.RenderTuning(refill_min_primary=2, refill_min=29),
     pt.RenderTuning(overlap_shadow=0),
@@ -91,17 +87,15 @@ def test_reference_triangles_and_profile_counts_under_tuning(scene):
     p = pt.RenderParams(**{**PARAMS.__dict__, "tri_format": pt.TRIS_REF, "spp": 2, "accumulate": 1,
                            "profile": pt.PROFILE_COUNTS})
     outs = []
-    for t in (pt.RenderTuning.default(), pt.RenderTuning(wavefront_paths=4096, trace_threads=64, shadow_one_lane=1),
-              pt.RenderTuning(shadow_one_lane=1, shadow_postpone=8)):
+    for t in (pt.RenderTuning.default(), pt.RenderTuning(wavefront_paths=4096, trace_threads=64, shadow_one_lane=1)):
         pt.set_tuning(t)
         pt.profile_reset()
         acc = torch.zeros(N * 3, dtype=torch.float32, device="cuda")
         pt.render_pass(ds, p, 3, None, acc)
         prof = pt.profile_get()
         outs.append((acc.cpu().numpy(), prof["rays"], prof["shadow_rays"], prof["nodes"]))
-    for o in outs[1:]:
-        np.testing.assert_array_equal(o[0], outs[0][0])
-        assert o[1:] == outs[0][1:]            # the same rays, shadow rays and closest-hit nodes
+    np.testing.assert_array_equal(outs[0][0], outs[1][0])
+    assert outs[0][1:] == outs[1][1:]          # the same rays, shadow rays and nodes
 
 
 def test_static_pass_under_tuning(built):
@@ -111,8 +105,7 @@ def test_static_pass_under_tuning(built):
     n = 64 * 48
     acc0 = torch.zeros(n * 3, device="cuda")
     pt.render_pass(ds, p, 5, None, acc0)
-    for t in (pt.RenderTuning(wavefront_paths=1024), pt.RenderTuning(wavefront_paths=4 * n, trace_threads=256),
-              pt.RenderTuning(shadow_one_lane=1, shadow_postpone=16)):
+    for t in (pt.RenderTuning(wavefront_paths=1024), pt.RenderTuning(wavefront_paths=4 * n, trace_threads=256)):
         pt.set_tuning(t)
         acc = torch.zeros(n * 3, device="cuda")
         pt.render_pass_static(ds, p, 5, None, acc)
@@ -145,8 +138,7 @@ def test_cache_frames_under_tuning(scene, graph):
     want = frames([d, d, d])
     got = frames([pt.RenderTuning(wavefront_paths=4000, overlap_shadow=1),
                   pt.RenderTuning(wavefront_paths=4 * N, trace_threads=64),
-                  pt.RenderTuning(wavefront_paths=N // 3, shadow_one_lane=1, shadow_postpone=8, refill_min=3,
-                                  overlap_shadow=1)])
+                  pt.RenderTuning(wavefront_paths=N // 3, shadow_one_lane=1, refill_min=3, overlap_shadow=1)])
     for g, w in zip(got, want):
         assert np.isfinite(g).all()
         np.testing.assert_array_equal(g, w)
@@ -156,9 +148,7 @@ def test_bad_tunings_are_rejected(built):
     for bad in (pt.RenderTuning(wavefront_paths=100), pt.RenderTuning(wavefront_paths=(1 << 26) + 1),
                 pt.RenderTuning(trace_threads=96), pt.RenderTuning(refill_min=0), pt.RenderTuning(refill_min=33),
                 pt.RenderTuning(trace_warps_per_sm=-1), pt.RenderTuning(shadow_one_lane=2),
-                pt.RenderTuning(shadow_one_lane=-1), pt.RenderTuning(shadow_postpone=-1),
-                pt.RenderTuning(shadow_postpone=33), pt.RenderTuning(refill_min_primary=33),
-                pt.RenderTuning(overlap_shadow=2)):
+                pt.RenderTuning(refill_min_primary=33), pt.RenderTuning(overlap_shadow=2)):
         with pytest.raises(TfgError):
             pt.set_tuning(bad)
     assert pt.get_tuning() == pt.RenderTuning.default()

@@ -5,8 +5,8 @@
 // scheduled -- the wavefront (queue) size, the traversal CTA size and
 // residency, the refill threshold of the persistent traversal lanes, how
 // many lanes share a shading point's shadow rays, the first bounce's refill
-// threshold, whether the shadow stage overlaps the next trace, and how many
-// lanes a shadow ray's triangle tests wait for -- never what a path
+// threshold, and whether the shadow stage overlaps the next trace -- never
+// what a path
 // computes, so every candidate renders the same image.  The search is one
 // pass of coordinate descent in that order, starting from the device's
 // current setting; a candidate replaces the best only when it is at least 1%
@@ -75,7 +75,6 @@ std::vector<int32_t> candidates(int k, uint32_t npix, uint64_t paths) {
         case 4: v = {0, 1}; break;
         case 5: v = {0, 16, 24, 32}; break;
         case 6: v = {0, 1}; break;
-        case 7: v = {0, 8}; break;
     }
     return v;
 }
@@ -88,8 +87,7 @@ int32_t& field(TfgRenderTuning& t, int k) {
         case 3: return t.refill_min;
         case 4: return t.shadow_one_lane;
         case 5: return t.refill_min_primary;
-        case 6: return t.overlap_shadow;
-        default: return t.shadow_postpone;
+        default: return t.overlap_shadow;
     }
 }
 
@@ -141,7 +139,7 @@ extern "C" int tfgRenderAutotune(const TfgRenderParams* params, const TfgCamara*
     float best_ms = 0.0f;
     if (!rc) rc = time_tuning(dev, sc, best, repeats, s, e0, e1, &best_ms);
     if (!rc) record(best, best_ms);
-    for (int k = 0; k < 8 && !rc; ++k) {
+    for (int k = 0; k < 7 && !rc; ++k) {
         for (int32_t v : candidates(k, npix, paths)) {
             TfgRenderTuning cand = best;
             if (field(cand, k) == v) continue;

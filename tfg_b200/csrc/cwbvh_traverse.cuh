@@ -280,92 +280,6 @@ struct CwbvhRay {
     }
 };
 
-// Any-hit traversal for shadow segments, advanced one iteration at a time.
-// Its answer -- does some reachable triangle accept 0 < tmin < t < tmax --
-// does not depend on the order in which the triangles are tested: tmax stays
-// fixed until the first accepted triangle ends the traversal, so the set of
-// nodes whose boxes pass the slab test, and with it the set of triangles, is
-// the same in every order.  That frees the order for fuller warps:
-//  * a node's triangle group is tested at once only while at least
-//    `postpone_min` lanes of the warp are testing triangles in the same
-//    iteration and the lane has inner children left to descend; otherwise
-//    the rest of the group is pushed on the stack as a triangle group and the
-//    lane keeps descending (triangle postponing, Ylitie, Karras, Laine 2017,
-//    sec. 4.2), so lanes meet in the triangle loop instead of idling in it;
-//  * a triangle group popped from the stack is tested in full, which bounds
-//    the work: every group is postponed at most once.
-// Stack entries tell the two kinds apart: a node group always has a child bit
-// in bits 24..31, a triangle group only triangle bits (0..23).
-enum : int { kOccGoing = 0, kOccHit = 1, kOccClear = 2 };
-
-template <int TRI_FMT>
-struct CwbvhOcclusion {
-    V3 O, D, rD;
-    uint32_t octinv;
-    WtRay wr;
-    float tmin, tmax;
-    uint2 ng;
-    uint32_t sp, nsteps, ntris;
-
-    __device__ __forceinline__ void init(V3 O_, V3 D_, float tmin_, float tmax_) {
-        O = O_; D = D_; tmin = tmin_; tmax = tmax_;
-        rD = v3(slab_rcp(D.x), slab_rcp(D.y), slab_rcp(D.z));
-        octinv = 7u - ((D.x < 0.0f ? 4u : 0u) | (D.y < 0.0f ? 2u : 0u) | (D.z < 0.0f ? 1u : 0u));
-        if (TRI_FMT == 1) wr = wt_setup(D);
-        ng = make_uint2(0u, 0x80000000u);
-        sp = 0; nsteps = 0; ntris = 0;
-    }
-
-    // One iteration: decode the next inner node (or take a postponed
-    // triangle group off the stack) and test triangles.  Returns kOccHit as
-    // soon as a triangle is accepted, kOccClear once nothing is left.
-    __device__ __forceinline__ int step(const float4* __restrict__ nodes, const float4* __restrict__ tris,
-                                        TravStack& st, int postpone_min) {
-        if (nsteps >= kMaxNodeVisits) return kOccClear;
-        ++nsteps;
-        uint32_t tbase, tbits;
-        bool popped = false;
-        if (ng.y > 0x00FFFFFFu) {
-            const uint32_t bit = msb_index(ng.y);
-            const uint32_t imask_parent = ng.y & 0xFFu;
-            ng.y &= ~(1u << bit);
-            if (ng.y > 0x00FFFFFFu && sp < (uint32_t)kStackTotal) { st.put(sp, ng); ++sp; }
-            const uint32_t slot = (bit - 24u) ^ octinv;
-            const uint32_t rel = __popc(imask_parent & ~(0xFFFFFFFFu << slot));
-            uint32_t cbase, imask;
-            const uint32_t hm = decode_node(nodes, ng.x + rel, O, rD, octinv, tmax, cbase, tbase, imask);
-            ng = make_uint2(cbase, (hm & 0xFF000000u) | imask);
-            tbits = hm & 0x00FFFFFFu;
-        } else {
-            tbase = ng.x; tbits = ng.y; ng.y = 0u; popped = true;
-        }
-        while (tbits) {
-            if (!popped && ng.y > 0x00FFFFFFu && sp < (uint32_t)kStackTotal &&
-                __popc(__activemask()) < postpone_min) {
-                st.put(sp, make_uint2(tbase, tbits));
-                ++sp;
-                break;
-            }
-            ++ntris;
-            const uint32_t k = msb_index(tbits);
-            tbits &= ~(1u << k);
-            float t, u, v;
-            if (TRI_FMT == 0) {
-                uint32_t tid;
-                if (ref_hit(tris, tbase + 4u * k, O, D, tmin, tmax, t, u, v, tid)) return kOccHit;
-            } else {
-                if (wt_hit(tris, (tbase >> 2) + k, O, wr, tmin, tmax, t, u, v)) return kOccHit;
-            }
-        }
-        if (ng.y <= 0x00FFFFFFu) {
-            if (sp == 0) return kOccClear;
-            --sp;
-            ng = st.get(sp);
-        }
-        return kOccGoing;
-    }
-};
-
 // Whole traversal in one call.  tmax in: upper bound (exclusive); out: hit
 // distance when found.  Returns true on a hit; id / u / v are written only
 // then.  `cnt`, when not null, accumulates the work done.

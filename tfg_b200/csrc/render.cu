@@ -108,7 +108,6 @@ struct PassArgs {
     int refill_min;           // idle lanes that trigger a traversal warp's refill
     int refill_primary;       // the same for the first bounce
     int shadow_one_lane;      // 1: one lane traces all lights of a shading point
-    int shadow_postpone;      // triangle tests of a shadow ray wait until this many lanes test (0: never wait)
     Workspace ws;
 };
 
@@ -699,19 +698,16 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
             const TfgLuzPuntual* lights = a.lights;
             int lend = l_end;
             if constexpr (MS) { lights = tab.s[sc].lights; lend = tab.s[sc].nlights; }
-            const bool mesh = a.shadow_mesh && g.has_bvh;
             for (int l = l_begin; l < lend; ++l) {
                 LightRay lr;
                 if (!light_ray(lights[l], P, N, kd, lr)) continue;
                 if (STATS) ++nrays;
                 if (analytic_any(sprims, nsm, g.prims, g.nprims, lr.so, lr.dl, lr.dist)) continue;
-                if (mesh) {
-                    CwbvhOcclusion<TRI_FMT> r;
-                    r.init(lr.so, lr.dl, kEps, lr.dist);
-                    int res;
-                    do { res = r.step(g.nodes, g.tris, stck, a.shadow_postpone); } while (res == kOccGoing);
-                    if (STATS) { cnt.nodes += r.nsteps; cnt.tris += r.ntris; }
-                    if (res == kOccHit) continue;
+                if (a.shadow_mesh && g.has_bvh) {
+                    float tm = lr.dist, hu, hv;
+                    uint32_t hid;
+                    if (cwbvh_trace<TRI_FMT, true>(g.nodes, g.tris, lr.so, lr.dl, kEps, tm, hid, hu, hv, stck,
+                                                   STATS ? &cnt : nullptr)) continue;
                 }
                 // Each light's term is rounded before it is added, so one lane
                 // looping over the lights sums the same values in the same
@@ -925,7 +921,6 @@ int shapes_for(int dev, LaunchShapes& s) {
 struct Tuning {
     uint32_t wavefront = 0;
     int threads = 128, warps_per_sm = 0, refill = 8, refill_primary = 8, shadow_one_lane = 0, overlap_shadow = 0;
-    int shadow_postpone = 0;
 };
 
 Tuning resolve_tuning(int dev, uint32_t npix, int spp, bool nrc, uint32_t* generation) {
@@ -946,7 +941,6 @@ Tuning resolve_tuning(int dev, uint32_t npix, int spp, bool nrc, uint32_t* gener
     r.refill = t.refill_min;
     r.refill_primary = t.refill_min_primary > 0 ? t.refill_min_primary : t.refill_min;
     r.shadow_one_lane = t.shadow_one_lane;
-    r.shadow_postpone = t.shadow_postpone;
     r.overlap_shadow = t.overlap_shadow;
     return r;
 }
@@ -971,8 +965,6 @@ int render_tuning_check(const TfgRenderTuning& t) {
     if (t.refill_min < 1 || t.refill_min > 32) return fail(TFG_E_INVALID, "render tuning: refill_min must be in [1, 32]");
     if (t.shadow_one_lane != 0 && t.shadow_one_lane != 1)
         return fail(TFG_E_INVALID, "render tuning: shadow_one_lane must be 0 or 1");
-    if (t.shadow_postpone < 0 || t.shadow_postpone > 32)
-        return fail(TFG_E_INVALID, "render tuning: shadow_postpone must be in [0, 32]");
     if (t.refill_min_primary < 0 || t.refill_min_primary > 32)
         return fail(TFG_E_INVALID, "render tuning: refill_min_primary must be in [0, 32]");
     if (t.overlap_shadow != 0 && t.overlap_shadow != 1)
@@ -1233,7 +1225,6 @@ int enqueue_pass(PassArgs a, const TableOf<MS>& tab, const TfgRenderParams& prm,
     a.refill_min = tu.refill;
     a.refill_primary = tu.refill_primary;
     a.shadow_one_lane = tu.shadow_one_lane;
-    a.shadow_postpone = tu.shadow_postpone;
     const uint64_t total = (uint64_t)prm.spp * N;
     for (uint64_t q0 = 0; q0 < total; q0 += tu.wavefront) {
         a.nq = (uint32_t)std::min<uint64_t>(tu.wavefront, total - q0);
@@ -1427,7 +1418,6 @@ extern "C" void tfgRenderTuningDefault(TfgRenderTuning* t) {
     t->shadow_one_lane = 0;
     t->refill_min_primary = 0;
     t->overlap_shadow = 1;
-    t->shadow_postpone = 0;
 }
 
 extern "C" int tfgRenderTuningSet(const TfgRenderTuning* t) {

@@ -262,7 +262,6 @@ class RenderTuning:
     shadow_one_lane: int = 0      # 1: one lane traces all lights of a shading point
     refill_min_primary: int = 0   # first-bounce refill threshold; 0 = refill_min
     overlap_shadow: int = 1       # 1: shadow stage on a second stream beside the next trace
-    shadow_postpone: int = 0      # shadow triangle tests wait for this many lanes of the warp; 0 = never
 
     def c(self) -> CRenderTuning:
         t = CRenderTuning()
@@ -270,14 +269,13 @@ class RenderTuning:
                                                                     self.trace_warps_per_sm)
         t.refill_min, t.shadow_one_lane = self.refill_min, self.shadow_one_lane
         t.refill_min_primary, t.overlap_shadow = self.refill_min_primary, self.overlap_shadow
-        t.shadow_postpone = self.shadow_postpone
         return t
 
     @staticmethod
     def of(t: CRenderTuning) -> "RenderTuning":
         return RenderTuning(int(t.wavefront_paths), int(t.trace_threads), int(t.trace_warps_per_sm),
                             int(t.refill_min), int(t.shadow_one_lane), int(t.refill_min_primary),
-                            int(t.overlap_shadow), int(t.shadow_postpone))
+                            int(t.overlap_shadow))
 
     @staticmethod
     def default() -> "RenderTuning":

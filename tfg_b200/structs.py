@@ -117,7 +117,7 @@ class CRenderTuning(ctypes.Structure):
     _fields_ = [("wavefront_paths", ctypes.c_int32), ("trace_threads", ctypes.c_int32),
                 ("trace_warps_per_sm", ctypes.c_int32), ("refill_min", ctypes.c_int32),
                 ("shadow_one_lane", ctypes.c_int32), ("refill_min_primary", ctypes.c_int32),
-                ("overlap_shadow", ctypes.c_int32), ("shadow_postpone", ctypes.c_int32)]
+                ("overlap_shadow", ctypes.c_int32), ("reserved", ctypes.c_int32 * 1)]
 
 
 class CTuneRecord(ctypes.Structure):
