@@ -44,7 +44,7 @@ TRACE_DRAM_BYTES_PER_LAUNCH = {1: 38_063_296, 16: 505_144_128}
 # (smsp__thread_inst_executed_per_inst_executed.ratio / 32), over the pass's
 # 4,001,265 rays, weighted by duration and by instructions respectively.
 TRACE_L2_BYTES_PER_RAY = 508.0
-TRACE_ISSUE_FRAC = 0.565
+TRACE_ISSUE_FRAC = 0.561
 TRACE_SIMT_EFFICIENCY = 0.406
 
 
