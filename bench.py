@@ -46,6 +46,9 @@ TRACE_DRAM_BYTES_PER_LAUNCH = {1: 38_063_296, 16: 505_144_128}
 TRACE_L2_BYTES_PER_RAY = 508.0
 TRACE_ISSUE_FRAC = 0.561
 TRACE_SIMT_EFFICIENCY = 0.406
+# k_shadow's active lanes per instruction (of 32) on the first bounce of the
+# one-sample pass (profiles/k_shadow_spheres_terrain_1080p.md: 14.91).
+SHADOW_SIMT_EFFICIENCY = 0.466
 
 
 def l2_gather_peak(dev) -> dict:
@@ -957,6 +960,12 @@ def main():
     # Algorithmic bytes of one closest-hit ray (watertight layout): 80 B per node
     # decoded, 48 B per triangle tested, 32 B ray read, 16 B hit written.
     bytes_per_ray = 80.0 * nodes_per_ray + 48.0 * tris_per_ray + 32.0 + 16.0
+    # The same for a shadow ray (any hit): nodes and triangles, its share of the
+    # 64 B shading-point item and of the 16 B radiance update.
+    shadow_per_spp = work["shadow_rays"]
+    shadow_nodes = work["shadow_nodes"] / max(1, work["shadow_rays"])
+    shadow_tris = work["shadow_tri_tests"] / max(1, work["shadow_rays"])
+    shadow_bytes = 80.0 * shadow_nodes + 48.0 * shadow_tris + 64.0 + 16.0
 
     # The autotuner picks the wavefront size and launch shapes on this frame
     # (untimed, like the warm-up); the timed frames and the e2e calls use it.
@@ -1065,6 +1074,9 @@ def main():
     l2_achieved = (rays_timed * TRACE_L2_BYTES_PER_RAY / (trace_ms * 1e-3) / 1e9
                    if trace_ms > 0 and TRACE_L2_BYTES_PER_RAY else None)
     l2_peak = l2_gather_peak(dev)
+    shadow_ms = prof["ms"]["shadow"]
+    shadow_timed = shadow_per_spp * SPP * args.steps
+    shadow_achieved = shadow_timed * shadow_bytes / (shadow_ms * 1e-3) / 1e9 if shadow_ms > 0 else None
     launches = sum(prof["launches"].values())
     clocks = clk.summary()
 
@@ -1120,6 +1132,21 @@ def main():
             "rays_per_launch_avg": round(rays_timed / max(1, trace_launches), 1),
             "ms_per_launch_avg": round(trace_ms / max(1, trace_launches), 4),
             "stage_ms": {k: round(v, 2) for k, v in prof["ms"].items()},
+        },
+        # The shadow stage takes as much device time as the closest-hit one (launch list in
+        # profiles/launches_bench_1080p_64spp.md); its figures on the same terms.  Its CUDA-event
+        # time runs on the side stream beside the next bounce's trace, so `achieved` is low by
+        # the share of the GPU that trace holds meanwhile.
+        "roofline_shadow": {
+            "kernel": "k_shadow (CWBVH any hit, one lane per shading point)", "bound": "hbm",
+            "limiter": "instruction issue with divergent lanes (L2-resident scene)",
+            "simt_efficiency": SHADOW_SIMT_EFFICIENCY,
+            "achieved": round(shadow_achieved, 1) if shadow_achieved else None,
+            "peak": pk["hbm_gbs"], "unit": "GB/s",
+            "frac": round(shadow_achieved / pk["hbm_gbs"], 4) if shadow_achieved else None,
+            "algorithmic_bytes_per_ray": round(shadow_bytes, 1),
+            "nodes_per_ray": round(shadow_nodes, 3), "tri_tests_per_ray": round(shadow_tris, 3),
+            "rays_timed": shadow_timed, "ms": round(shadow_ms, 2),
         },
         "primary_rays": {"grays_per_s": round(primary_grays, 3), "rays_per_call": primary_samples * n_px,
                          "samples_per_call": primary_samples, "order": "8x4 tiles", "tri_test": "watertight",
