@@ -210,3 +210,21 @@ def test_gate_closes_when_the_lighting_changes(terrain):
     r.stream.synchronize()
     assert m.state()["gate"] > 0.5 * open0, (open0, m.state()["gate"])
     m.close()
+
+
+def test_bad_policy_settings_are_rejected(terrain):
+    from tfg_b200 import TfgError
+    s, ds = terrain
+    m = _mlp(s)
+    for kw in ({"footprint": -0.01}, {"footprint": float("nan")}, {"train_fraction": -0.1},
+               {"train_fraction": 1.5}, {"gate_threshold": -1.0}):
+        r = NrcRenderer(ds, m, PARAMS, train_steps=1, max_records=4096, min_records=64, use_graph=False, **kw)
+        with pytest.raises(TfgError):
+            r.frame(1, accumulate=False)
+    # the limits themselves are accepted
+    for kw in ({"footprint": 0.0}, {"train_fraction": 0.0}, {"train_fraction": 1.0}):
+        r = NrcRenderer(ds, m, PARAMS, train_steps=1, max_records=4096, min_records=64, use_graph=False, **kw)
+        r.frame(1, accumulate=False)
+        r.stream.synchronize()
+        assert np.isfinite(r.image().cpu().numpy()).all()
+    m.close()
