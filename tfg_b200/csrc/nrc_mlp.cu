@@ -154,7 +154,6 @@ enum : int {
     S_GATE = 3,      // open cells of the gate grid after the last gated frame
     S_LOSS_EMA = 4,  // running loss (float bits)
     S_F8_VER = 5,    // S_ADAM_T + 1 of the weights in the FP8 image (0: not packed)
-    S_DONE = 6,      // blocks of an Adam step finished so far (the last one resets it)
     S_WORDS = 8
 };
 
@@ -1824,7 +1823,26 @@ struct WgradArgs {
     uint32_t min_n;
     uint32_t ntiles;
     uint32_t tiles_per_cta;
+    // When set, CTA (0, 0) ends the step (step counter, Adam time, running
+    // loss, as k_tick): the forward / backward kernel that read the step's
+    // seed has finished, and nothing later in a step without hash tables
+    // reads the seed.
+    int tick;
+    const float* loss_sum;
+    float inv_count;
 };
+
+// Ends a step: advance the step counter and Adam time, keep a running loss.
+__device__ __forceinline__ void tick_state(uint32_t* state, const float* loss_sum, float inv_count, uint32_t min_n) {
+    const uint32_t n = state[S_NAVAIL];
+    if (n < min_n || n == 0) return;
+    state[S_STEP] += 1u;
+    state[S_ADAM_T] += 1u;
+    const float loss = *loss_sum * inv_count;
+    float ema = __uint_as_float(state[S_LOSS_EMA]);
+    ema = (state[S_ADAM_T] == 1u) ? loss : 0.9f * ema + 0.1f * loss;
+    state[S_LOSS_EMA] = __float_as_uint(ema);
+}
 
 template <int NL, int HID>
 __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
@@ -1839,6 +1857,8 @@ __global__ void __launch_bounds__(128) k_wgrad(WgradArgs a) {
     const uint32_t t0 = blockIdx.x * a.tiles_per_cta;
     if (t0 >= a.ntiles || a.state[S_NAVAIL] < a.min_n || a.state[S_NAVAIL] == 0) return;
     const uint32_t t1 = min(a.ntiles, t0 + a.tiles_per_cta);
+    if (a.tick && t == 0 && blockIdx.x == 0 && blockIdx.y == 0)
+        tick_state(const_cast<uint32_t*>(a.state), a.loss_sum, a.inv_count, a.min_n);
     if (warp == 0) umma::tmem_alloc(&tslot, 128);
     if (t == 0) {
         for (int k = 0; k < S; ++k) { umma::mbar_init(&mb_ld[k], 1); umma::mbar_init(&mb_mma[k], 1); }
@@ -1960,12 +1980,7 @@ struct AdamArgs {
     uint32_t min_n;
     int update;                    // 0: only re-pack (after loading parameters)
     int live0;                     // live input columns of layer 0 (the rest stay zero)
-    // When set, the last block to finish ends the step as k_tick does (step
-    // counter, Adam time, running loss); `done` counts the finished blocks.
-    int tick;
-    uint32_t* done;
-    const float* loss_sum;
-    float inv_count;
+    int ticked;                    // the step's end already advanced S_ADAM_T (k_wgrad)
 };
 
 template <int NL, int HID>
@@ -1977,73 +1992,48 @@ __device__ __forceinline__ void layer_of(int i, int& l, int& r, int& c) {
     c = j % cols_h<HID>(l);
 }
 
-// Ends a step: advance the step counter and Adam time, keep a running loss.
-__device__ __forceinline__ void tick_state(uint32_t* state, const float* loss_sum, float inv_count, uint32_t min_n) {
-    const uint32_t n = state[S_NAVAIL];
-    if (n < min_n || n == 0) return;
-    state[S_STEP] += 1u;
-    state[S_ADAM_T] += 1u;
-    const float loss = *loss_sum * inv_count;
-    float ema = __uint_as_float(state[S_LOSS_EMA]);
-    ema = (state[S_ADAM_T] == 1u) ? loss : 0.9f * ema + 0.1f * loss;
-    state[S_LOSS_EMA] = __float_as_uint(ema);
-}
 
 template <int NL, int HID>
 __global__ void k_adam(AdamArgs a) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < params_h<HID>(NL)) {
-        int l, r, c;
-        layer_of<NL, HID>(i, l, r, c);
-        // Padded entries (output rows 3..15, input columns past the encoding of layer 0) stay zero.
-        const bool live = !(l == NL - 1 && r >= 3) && !(l == 0 && c >= a.live0);
-        float w = a.w[i];
-        float e = a.ema[i];
-        const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
-        const float tn = (float)(a.state[S_ADAM_T] + (update ? 1u : 0u));
-        if (update && live) {
-            const float bc1 = 1.0f - powf(a.beta1, tn), bc2 = 1.0f - powf(a.beta2, tn);
-            float gs = 0.0f;
-            for (uint32_t k = 0; k < a.groups; ++k) gs += a.part[(size_t)k * params_h<HID>(NL) + i];
-            const float g = gs * a.grad_scale;
-            const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
-            const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
-            a.m[i] = m;
-            a.v[i] = v;
-            w -= a.lr * (m / bc1) / (sqrtf(v / bc2) + a.eps);
-            e = a.decay * e + (1.0f - a.decay) * w;
-            a.w[i] = w;
-            a.ema[i] = e;
-        }
-        if (!live) { w = 0.0f; e = 0.0f; }
-        const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
-        const float ew = ema_debias > 0.0f ? e / ema_debias : w;
-        // forward / inference images: row r, K index c
-        const int rows = rows_h<HID>(NL, l);
-        const uint32_t off = (uint32_t)foff_h<HID>(NL, l) + (uint32_t)(c >> 6) * rows * 128 +
-                             umma::sw128_offset(r, (c & 63) >> 3) + 2 * (c & 7);
-        *reinterpret_cast<__half*>(a.fwd + off) = __float2half_rn(w);
-        *reinterpret_cast<__half*>(a.inf + off) = __float2half_rn(ew);
-        *reinterpret_cast<__nv_bfloat16*>(a.inf_bf + off) = __float2bfloat16_rn(ew);
-        if (l >= 1) {
-            // backward image: W^T, row = c (input unit), K index = r (output unit)
-            const uint32_t boff = (uint32_t)boff_h<HID>(NL, l) + (uint32_t)(r >> 6) * (HID * 128) +
-                                  umma::sw128_offset(c, (r & 63) >> 3) + 2 * (r & 7);
-            *reinterpret_cast<__nv_bfloat16*>(a.bwd + boff) = __float2bfloat16_rn(w);
-        }
+    if (i >= params_h<HID>(NL)) return;
+    int l, r, c;
+    layer_of<NL, HID>(i, l, r, c);
+    // Padded entries (output rows 3..15, input columns past the encoding of layer 0) stay zero.
+    const bool live = !(l == NL - 1 && r >= 3) && !(l == 0 && c >= a.live0);
+    float w = a.w[i];
+    float e = a.ema[i];
+    const bool update = a.update && a.state[S_NAVAIL] >= a.min_n && a.state[S_NAVAIL] > 0;
+    const float tn = (float)(a.state[S_ADAM_T] + ((update && !a.ticked) ? 1u : 0u));
+    if (update && live) {
+        const float bc1 = 1.0f - powf(a.beta1, tn), bc2 = 1.0f - powf(a.beta2, tn);
+        float gs = 0.0f;
+        for (uint32_t k = 0; k < a.groups; ++k) gs += a.part[(size_t)k * params_h<HID>(NL) + i];
+        const float g = gs * a.grad_scale;
+        const float m = a.beta1 * a.m[i] + (1.0f - a.beta1) * g;
+        const float v = a.beta2 * a.v[i] + (1.0f - a.beta2) * g * g;
+        a.m[i] = m;
+        a.v[i] = v;
+        w -= a.lr * (m / bc1) / (sqrtf(v / bc2) + a.eps);
+        e = a.decay * e + (1.0f - a.decay) * w;
+        a.w[i] = w;
+        a.ema[i] = e;
     }
-    if (!a.tick) return;
-    // Every block has read S_ADAM_T (its image stores depend on the value)
-    // before it counts itself done, so the last one may advance it; the state
-    // words are written by that block alone.
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const uint32_t prev = atomicAdd(a.done, 1u);
-        if (prev == gridDim.x - 1) {
-            __threadfence();
-            *a.done = 0u;
-            tick_state(const_cast<uint32_t*>(a.state), a.loss_sum, a.inv_count, a.min_n);
-        }
+    if (!live) { w = 0.0f; e = 0.0f; }
+    const float ema_debias = tn > 0.0f ? 1.0f - powf(a.decay, tn) : 0.0f;
+    const float ew = ema_debias > 0.0f ? e / ema_debias : w;
+    // forward / inference images: row r, K index c
+    const int rows = rows_h<HID>(NL, l);
+    const uint32_t off = (uint32_t)foff_h<HID>(NL, l) + (uint32_t)(c >> 6) * rows * 128 +
+                         umma::sw128_offset(r, (c & 63) >> 3) + 2 * (c & 7);
+    *reinterpret_cast<__half*>(a.fwd + off) = __float2half_rn(w);
+    *reinterpret_cast<__half*>(a.inf + off) = __float2half_rn(ew);
+    *reinterpret_cast<__nv_bfloat16*>(a.inf_bf + off) = __float2bfloat16_rn(ew);
+    if (l >= 1) {
+        // backward image: W^T, row = c (input unit), K index = r (output unit)
+        const uint32_t boff = (uint32_t)boff_h<HID>(NL, l) + (uint32_t)(r >> 6) * (HID * 128) +
+                              umma::sw128_offset(c, (r & 63) >> 3) + 2 * (r & 7);
+        *reinterpret_cast<__nv_bfloat16*>(a.bwd + boff) = __float2bfloat16_rn(w);
     }
 }
 
@@ -2212,8 +2202,8 @@ __global__ void k_hash_init(float* w, size_t count, uint64_t seed) {
     }
 }
 
-// After a step of a model with hash-grid tables (whose table update reads
-// the Adam time after k_adam): the same end of step as k_adam's last block.
+// After a step of a model with hash-grid tables (whose table gradient reads
+// the step's seed after k_wgrad): the same end of step as k_wgrad's.
 __global__ void k_tick(uint32_t* state, const float* loss_sum, float inv_count, uint32_t min_n) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
     tick_state(state, loss_sum, inv_count, min_n);
@@ -2396,7 +2386,7 @@ uint64_t splitmix(uint64_t& s) {
     return z ^ (z >> 31);
 }
 
-int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n, bool tick) {
+int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n, bool ticked) {
     mlp::AdamArgs a;
     a.w = n->w; a.m = n->m; a.v = n->v; a.ema = n->ema; a.grad = n->grad;
     a.part = update ? n->wpart : nullptr;
@@ -2408,10 +2398,7 @@ int repack(ColorMlp* n, cudaStream_t s, bool update, uint32_t min_n, bool tick) 
     a.min_n = min_n;
     a.update = update ? 1 : 0;
     a.live0 = n->hlevels ? mlp::kHashLive : mlp::kFreqLive;
-    a.tick = tick ? 1 : 0;
-    a.done = n->dstate + mlp::S_DONE;
-    a.loss_sum = n->loss;
-    a.inv_count = 1.0f / (3.0f * (float)n->batch);
+    a.ticked = ticked ? 1 : 0;
     with_width(n, [&](auto c, auto w) {
         constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
         mlp::k_adam<NL, HID><<<(mlp::params_h<HID>(NL) + 255) / 256, 256, 0, s>>>(a);
@@ -2482,13 +2469,16 @@ uint32_t infer_grid(const ColorMlp* n, uint32_t tiles) {
     return std::max<uint32_t>(1u, std::min<uint32_t>((tiles + mlp::kSlots - 1) / mlp::kSlots, cap));
 }
 
-int enqueue_wgrad(ColorMlp* n, uint32_t tiles_per_cta, uint32_t min_n, cudaStream_t s) {
+int enqueue_wgrad(ColorMlp* n, uint32_t tiles_per_cta, uint32_t min_n, cudaStream_t s, bool tick = false) {
     const uint32_t tiles = n->batch / mlp::kTile;
     mlp::WgradArgs wa;
     for (int l = 0; l < mlp::kMaxLayers; ++l) { wa.zT[l] = n->zT[l]; wa.hT[l] = n->hT[l]; }
     wa.part = n->wpart; wa.state = n->dstate; wa.min_n = min_n;
     wa.ntiles = tiles;
     wa.tiles_per_cta = std::max<uint32_t>(1u, tiles_per_cta);
+    wa.tick = tick ? 1 : 0;
+    wa.loss_sum = n->loss;
+    wa.inv_count = 1.0f / (3.0f * (float)n->batch);
     const uint32_t groups = (tiles + wa.tiles_per_cta - 1) / wa.tiles_per_cta;
     with_width(n, [&](auto c, auto w) {
         constexpr int NL = decltype(c)::value, HID = decltype(w)::value;
@@ -2538,7 +2528,11 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
     });
     e = cudaGetLastError();
     if (e != cudaSuccess) return cuda_fail(e, "mlp step: forward/backward");
-    if (int rc = enqueue_wgrad(n, wgrad_tiles_per_cta(n, tiles), min_n, s)) return rc;
+    // Without hash tables the weight-gradient kernel ends the step; the table
+    // gradient re-draws the step's samples from its seed, so with tables
+    // k_tick ends it after the table update.
+    const bool tick_early = update && n->hlevels == 0;
+    if (int rc = enqueue_wgrad(n, wgrad_tiles_per_cta(n, tiles), min_n, s, tick_early)) return rc;
     if (n->hlevels) {
         mlp::HashGradArgs ha;
         ha.buf = buf; ha.state = n->dstate; ha.min_n = min_n; ha.batch = n->batch; ha.bounds = n->bounds;
@@ -2549,9 +2543,7 @@ int enqueue_step(ColorMlp* n, const TfgDatosMLP* buf, uint32_t min_n, bool updat
         if (e != cudaSuccess) return cuda_fail(e, "mlp step: table gradient");
     }
     if (!update) return enqueue_wgrad_sum(n, min_n, s);
-    // Without tables the Adam kernel's last block ends the step; the table
-    // update reads the Adam time after it, so with tables k_tick does.
-    if (int rc = repack(n, s, true, min_n, n->hlevels == 0)) return rc;
+    if (int rc = repack(n, s, true, min_n, tick_early)) return rc;
     if (n->hlevels) {
         mlp::k_tick<<<1, 32, 0, s>>>(n->dstate, n->loss, 1.0f / (3.0f * (float)n->batch), min_n);
         e = cudaGetLastError();
