@@ -31,10 +31,13 @@ METRIC = "Mpaths/s & ms/frame @1080p"
 WORKLOAD = "plain path tracing, 1920x1080, 64 spp, depth 8, RR from depth 3, 16 displaced icospheres + fractal terrain (1,000,480 tris), 2 point lights"
 
 
-# DRAM bytes (read + write) per closest-hit launch, measured with ncu on
-# `bench.py --profile-pass --wavefront-samples K`, by K = image samples per
-# wavefront (profiles/k_trace_k_shadow_dram_1080p.md).
-TRACE_DRAM_BYTES_PER_LAUNCH = {1: 38_063_296, 16: 505_144_128}
+# DRAM bytes (read + write) per closest-hit ray, measured with ncu over the
+# eight closest-hit launches of `bench.py --profile-pass --wavefront-samples K`
+# (profiles/k_trace_k_shadow_dram_1080p.md, k_trace_l2_issue_1080p.md): 306.4 MB
+# over 4,001,265 rays with one sample per wavefront, 4,041 MB over 64,020,240
+# rays with 16; the cold first touch of the tree is shared by more rays in
+# larger wavefronts.
+TRACE_DRAM_BYTES_PER_RAY = {1: 76.57, 16: 63.12}
 
 
 # ncu counters of the closest-hit kernel on the bench frame (one-sample pass,
@@ -86,9 +89,12 @@ def l2_gather_peak(dev) -> dict:
             "how": "80 B records at hashed indices of a 64 MiB table, 1184 x 256 threads x 256 reads, best of 10"}
 
 
-def trace_traffic(wavefront_paths: int, n_px: int):
+def trace_traffic(wavefront_paths: int, n_px: int, rays_per_launch: float) -> int:
+    """DRAM bytes per closest-hit launch: the measured bytes per ray of the
+    nearest captured wavefront size (1 or 16 samples) times the rays of an
+    average launch."""
     k = max(1, wavefront_paths // n_px) if wavefront_paths else 1
-    return TRACE_DRAM_BYTES_PER_LAUNCH.get(k)
+    return int(round(TRACE_DRAM_BYTES_PER_RAY[1 if k < 4 else 16] * rays_per_launch))
 
 
 def peaks() -> dict:
@@ -1123,10 +1129,11 @@ def main():
             "peak": pk["hbm_gbs"], "unit": "GB/s",
             "frac": round(achieved / pk["hbm_gbs"], 4) if achieved else None,
             "peak_source": pk["source"],
-            # ncu dram__bytes_read.sum + dram__bytes_write.sum of the 8 closest-hit launches of one
-            # pass in the tuned wavefront size, per launch (profiles/k_trace_k_shadow_dram_1080p.md):
-            # the 64 MB CWBVH + triangles stay L2-resident, so DRAM sees ~6-8 % of the algorithmic bytes.
-            "traffic": trace_traffic(tuning.wavefront_paths, n_px), "traffic_unit": "bytes per launch",
+            # ncu dram__bytes_read.sum + dram__bytes_write.sum per closest-hit ray (eight launches of
+            # one pass, 1- and 16-sample wavefronts) times this run's rays per launch: the 64 MB CWBVH +
+            # triangles stay L2-resident, so DRAM sees ~6-8 % of the algorithmic bytes.
+            "traffic": trace_traffic(tuning.wavefront_paths, n_px, rays_timed / max(1, trace_launches)),
+            "traffic_unit": "bytes per launch",
             "algorithmic_bytes_per_ray": round(bytes_per_ray, 1),
             "nodes_per_ray": round(nodes_per_ray, 3), "tri_tests_per_ray": round(tris_per_ray, 3),
             "rays_per_launch_avg": round(rays_timed / max(1, trace_launches), 1),
