@@ -34,12 +34,15 @@ def main() -> None:
     args = ap.parse_args()
     ref = orc.ref()
     assert ref is not None and torch.cuda.is_available(), "needs a GPU and oracle/_ref/libtfgref.so"
-    W, H = 1920, 1080                      # multiples of 16: the reference kernel has no bounds guard
+    W, H = 1920, 1080
     scene = scenes.spheres_terrain(W, H)
     ds = pt.DeviceScene(scene, "cuda")
     img_ref = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
     img_ours = torch.zeros(W * H * 3, dtype=torch.float32, device="cuda")
-    nb = pt.NrcBuffers(W * H, "cuda")
+    # The reference kernel runs whole 16 x 16 blocks (68 block rows for 1080)
+    # and writes the throughput of every thread without a bounds check, so the
+    # per-pixel buffers get 16 spare rows.
+    nb = pt.NrcBuffers(W * H + 16 * W, "cuda")
 
     def run_ref(frame):
         assert ref.ref_render_tiny(ds.camera.data_ptr(), None, 0, ds.lights.data_ptr(), ds.n_lights, W, H, frame,
