@@ -822,6 +822,36 @@ def profile_mlp(width: int = 64, precision: str = "fp16"):
     print("profile mlp done")
 
 
+def profile_train(width: int = 64, steps: int = 30):
+    """`steps` eager training steps of 16,384 samples (5 hidden layers of
+    `width` units, frequency encoding) drawn from 65,536 seeded records, then
+    exit; the case for a warm launch list of the step's kernels (k_train,
+    k_wgrad, k_adam): skip the first steps' launches in ncu."""
+    import numpy as np
+    import torch
+
+    from tfg_b200.nrc import ColorMLP
+    from tfg_b200.structs import DATOS_MLP
+    n = 65536
+    rng = np.random.default_rng(0)
+    d = np.zeros(n, DATOS_MLP)
+    for k in "xyz":
+        d["posicion"][k] = rng.uniform(-5, 5, n)
+        d["direccion"][k] = rng.uniform(0, 1, n)
+        d["normal"][k] = rng.uniform(0, 1, n)
+    for k in "rgb":
+        d["difuso"][k] = rng.uniform(0, 1, n)
+        d["color"][k] = rng.uniform(0, 2, n)
+    dd = torch.from_numpy(d.view(np.uint8).copy()).cuda()
+    m = ColorMLP(batch=16384, seed=1, width=width)
+    m.set_bounds((-6, -6, -6), (6, 6, 6))
+    for _ in range(steps):
+        m.train_step(dd, n, read_loss=False)
+    torch.cuda.synchronize()
+    m.close()
+    print("profile train done")
+
+
 def profile_frame(encoding: str = "frequency", width: int = 64, frames: int = 6, footprint: float = 0.01):
     """`frames` cache frames of the 1920x1080 benchmark scene (the first
     four as warm-up frames, 4 x 16384 training samples each, launched
@@ -900,6 +930,8 @@ def main():
                     help="with --profile-mlp / --profile-frame: 64 or 128 units per hidden layer")
     ap.add_argument("--mlp-precision", default="fp16", choices=["fp16", "fp8"],
                     help="with --profile-mlp: fp8 adds a calibration pass and two FP8 inferences")
+    ap.add_argument("--profile-train", action="store_true",
+                    help="run 30 eager 16,384-sample training steps of the cache model, then exit (case for ncu)")
     ap.add_argument("--profile-frame", action="store_true",
                     help="run six eager cache frames of the workload and one more inference, then exit (case for ncu)")
     ap.add_argument("--mlp-encoding", default="frequency", choices=["frequency", "hashgrid"],
@@ -930,6 +962,9 @@ def main():
         return
     if args.profile_mlp:
         profile_mlp(args.mlp_width, args.mlp_precision)
+        return
+    if args.profile_train:
+        profile_train(args.mlp_width)
         return
     if args.measure_peaks:
         measure_peaks()
