@@ -1011,7 +1011,7 @@ def main():
     # The autotuner picks the wavefront size and launch shapes on this frame
     # (untimed, like the warm-up); the timed frames and the e2e calls use it.
     t_tune = time.perf_counter()
-    tuning, tune_table = pt.autotune(ds, base, repeats=2)
+    tuning, tune_table = pt.autotune(ds, base, repeats=3)
     tune_s = time.perf_counter() - t_tune
     tuned_ms = min(ms for t, ms in tune_table if t == tuning)
 
