@@ -654,6 +654,14 @@ __device__ __forceinline__ void add_direct(const PassArgs& a, uint32_t p, uint32
     }
 }
 
+// A 16-byte load that the compiler keeps where it is written (not hoisted out
+// of a loop and held in registers).
+__device__ __forceinline__ float4 ld_item(const float4* p) {
+    float4 v;
+    asm volatile("ld.global.v4.f32 {%0, %1, %2, %3}, [%4];" : "=f"(v.x), "=f"(v.y), "=f"(v.z), "=f"(v.w) : "l"(p));
+    return v;
+}
+
 template <int TRI_FMT, bool STATS, bool MS>
 __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<MS> tab) {
     extern __shared__ unsigned char smem_raw[];
@@ -684,23 +692,20 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
         const uint32_t i = base + lane / G;
         const bool have = i < n;
         V3 L = v3(0.0f, 0.0f, 0.0f);
-        V3 P, N, kd, cam;
-        uint32_t p = 0;
-        uint32_t dest = 0;   // bit 0: suffix radiance, bit 1: also the pixel's
+        // The item (shading point, albedo, throughput, pixel, destination) is
+        // read where it is used -- the point for every light, the rest after
+        // the traversals -- so that none of it is held in registers through a
+        // traversal (L1 serves the re-reads).
+        const float4* s = &a.ws.shadow[4 * (size_t)(have ? i : 0u)];
         if (have) {
-            const float4* s = &a.ws.shadow[4 * (size_t)i];
-            const float4 s0 = s[0], s1 = s[1], s2 = s[2], s3 = s[3];
-            P = xyz(s0); N = xyz(s1); kd = xyz(s2); cam = xyz(s3);
-            p = __float_as_uint(s0.w);
-            dest = __float_as_uint(s1.w);
-            const uint32_t sc = MS ? __float_as_uint(s2.w) : 0u;
+            const uint32_t sc = MS ? __float_as_uint(ld_item(s + 2).w) : 0u;
             const Geo g = geo_of<MS>(a, tab, sc);
             const TfgLuzPuntual* lights = a.lights;
             int lend = l_end;
             if constexpr (MS) { lights = tab.s[sc].lights; lend = tab.s[sc].nlights; }
             for (int l = l_begin; l < lend; ++l) {
                 LightRay lr;
-                if (!light_ray(lights[l], P, N, kd, lr)) continue;
+                if (!light_ray(lights[l], xyz(ld_item(s)), xyz(ld_item(s + 1)), xyz(ld_item(s + 2)), lr)) continue;
                 if (STATS) ++nrays;
                 if (analytic_any(sprims, nsm, g.prims, g.nprims, lr.so, lr.dl, lr.dist)) continue;
                 if (a.shadow_mesh && g.has_bvh) {
@@ -723,7 +728,10 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
             const float z = __shfl_sync(0xFFFFFFFFu, L.z, group0 + j);
             if (lg == 0u && (int)j < nl) L = L + v3(x, y, z);
         }
-        if (have && lg == 0u) add_direct(a, p, dest, cam, L);
+        if (have && lg == 0u) {
+            const float4 s0 = ld_item(s), s1 = ld_item(s + 1), s3 = ld_item(s + 3);
+            add_direct(a, __float_as_uint(s0.w), __float_as_uint(s1.w), xyz(s3), L);
+        }
     }
     if (STATS) flush_work(3, nrays, cnt);
 }
