@@ -50,8 +50,8 @@ TRACE_L2_BYTES_PER_RAY = 508.0
 TRACE_ISSUE_FRAC = 0.561
 TRACE_SIMT_EFFICIENCY = 0.406
 # k_shadow's active lanes per instruction (of 32) on the first bounce of the
-# one-sample pass (profiles/k_shadow_spheres_terrain_1080p.md: 14.91).
-SHADOW_SIMT_EFFICIENCY = 0.466
+# one-sample pass (profiles/k_trace_k_shadow_bounce0_full_1080p.md: 15.18).
+SHADOW_SIMT_EFFICIENCY = 0.474
 
 
 def l2_gather_peak(dev) -> dict:
