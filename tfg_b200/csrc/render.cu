@@ -698,12 +698,16 @@ __global__ void __launch_bounds__(256) k_shadow(PassArgs a, int bounce, TableOf<
         // traversal (L1 serves the re-reads).
         const float4* s = &a.ws.shadow[4 * (size_t)(have ? i : 0u)];
         if (have) {
-            const uint32_t sc = MS ? __float_as_uint(ld_item(s + 2).w) : 0u;
-            const Geo g = geo_of<MS>(a, tab, sc);
-            const TfgLuzPuntual* lights = a.lights;
-            int lend = l_end;
-            if constexpr (MS) { lights = tab.s[sc].lights; lend = tab.s[sc].nlights; }
-            for (int l = l_begin; l < lend; ++l) {
+            for (int l = l_begin;; ++l) {
+                // A batch's scene (its lights, primitives and tree) is looked
+                // up again for every light from the item's scene index, for
+                // the same reason.
+                const uint32_t sc = MS ? __float_as_uint(ld_item(s + 2).w) : 0u;
+                const Geo g = geo_of<MS>(a, tab, sc);
+                const TfgLuzPuntual* lights = a.lights;
+                int lend = l_end;
+                if constexpr (MS) { lights = tab.s[sc].lights; lend = tab.s[sc].nlights; }
+                if (l >= lend) break;
                 LightRay lr;
                 if (!light_ray(lights[l], xyz(ld_item(s)), xyz(ld_item(s + 1)), xyz(ld_item(s + 2)), lr)) continue;
                 if (STATS) ++nrays;
