@@ -347,6 +347,7 @@ __global__ void __launch_bounds__(256) k_trace(PassArgs a, int bounce, TableOf<M
     const uint32_t lane = lane_id(), lt = (1u << lane) - 1u;
     const int refill = bounce == 0 ? a.refill_primary : a.refill_min;
     CwbvhRay<TRI_FMT, false> r;
+    uint32_t csc = 0;   // a batch: the current ray's scene, whose tree is looked up again at every step
     uint32_t cur = kMissId, bid = kMissId;
     float best = 0.0f, bu = 0.0f, bv = 0.0f;
     bool exhausted = false;
@@ -365,13 +366,16 @@ __global__ void __launch_bounds__(256) k_trace(PassArgs a, int bounce, TableOf<M
                 cur = k;
                 const float4 o4 = rays[2 * k], d4 = rays[2 * k + 1];
                 const V3 O = xyz(o4), D = xyz(d4);
-                if constexpr (MS) { g = geo_of<MS>(a, tab, __float_as_uint(o4.w)); best = 1e9f; }
+                if constexpr (MS) { csc = __float_as_uint(o4.w); g = geo_of<MS>(a, tab, csc); best = 1e9f; }
                 else best = o4.w;
                 bu = 0.0f; bv = 0.0f; bid = kMissId;
                 const int ai = analytic_closest(sprims, nsm, g.prims, g.nprims, O, D, best, bu, bv);
                 if (ai >= 0) bid = kAnalyticBit | (uint32_t)ai;
                 r.init(O, D, 0.0f, best);
             }
+        }
+        if constexpr (MS) {
+            if (cur != kMissId) g = geo_of<MS>(a, tab, csc);
         }
         if (cur != kMissId && !(g.has_bvh && r.step(g.nodes, g.tris, st))) {
             if (g.has_bvh) {
